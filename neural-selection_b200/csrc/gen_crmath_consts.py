@@ -1,0 +1,107 @@
+"""Generate ns_crmath_consts.h: binary64 constants for the correctly rounded
+binary32 exp/log in ns_crmath.h.
+
+Every constant is computed with Python's decimal module at 80 significant
+digits and rounded to binary64 by float(str(...)), which rounds correctly.
+Double-double constants are (hi, lo) with hi = RN(v), lo = RN(v - hi).
+
+Run:  python neural-selection_b200/csrc/gen_crmath_consts.py
+"""
+from decimal import Decimal, getcontext
+from pathlib import Path
+
+getcontext().prec = 80
+TWO = Decimal(2)
+LN2 = TWO.ln()
+
+
+def rn(v):
+    return float(str(v))
+
+
+def dd(v):
+    hi = rn(v)
+    lo = rn(v - Decimal(hi))
+    return hi, lo
+
+
+def split_bits(v, bits):
+    """Round v to a binary64 with at most `bits` significant bits (truncated
+    toward zero), so products with small integers stay exact."""
+    hi = rn(v)
+    m, e = __import__('math').frexp(hi)
+    scale = 2 ** bits
+    t = int(m * scale) / scale
+    return __import__('math').ldexp(t, e)
+
+
+def hx(x):
+    return float.hex(x)
+
+
+lines = ["/* Generated by gen_crmath_consts.py; do not edit. */",
+         "#pragma once", ""]
+
+# 2^(j/128), j = 0..127, binary64 correctly rounded.
+vals = [rn(TWO ** (Decimal(j) / 128)) for j in range(128)]
+lines.append("#define NSX_EXP2_128_TABLE \\")
+for i in range(0, 128, 4):
+    chunk = ", ".join(hx(v) for v in vals[i:i + 4])
+    sep = ", \\" if i + 4 < 128 else ""
+    lines.append("    " + chunk + sep)
+lines.append("")
+
+inv = rn(Decimal(128) / LN2)
+lines.append(f"#define NSX_INV_LN2_128 {hx(inv)}")
+h, l = dd(LN2 / 128)
+lines.append(f"#define NSX_LN2_128_HI {hx(h)}")
+lines.append(f"#define NSX_LN2_128_LO {hx(l)}")
+lines.append(f"#define NSX_INV_LN2 {hx(rn(1 / LN2))}")
+# ln2 as a sum of three doubles whose first two have <= 45 significant
+# bits, so m*A and m*B are exact for |m| < 2^8.
+a = split_bits(LN2, 45)
+rest = LN2 - Decimal(a)
+b = split_bits(rest, 45)
+c = rn(rest - Decimal(b))
+lines.append(f"#define NSX_LN2_A {hx(a)}")
+lines.append(f"#define NSX_LN2_B {hx(b)}")
+lines.append(f"#define NSX_LN2_C {hx(c)}")
+# ln2 split for log: HI has 45 bits so e*HI is exact for |e| < 2^8.
+lhi = split_bits(LN2, 45)
+llo = rn(LN2 - Decimal(lhi))
+lines.append(f"#define NSX_LN2_LOG_HI {hx(lhi)}")
+lines.append(f"#define NSX_LN2_LOG_LO {hx(llo)}")
+lines.append("")
+
+# 1/n! for n = 0..24 as double-double (exp slow path).
+fact = Decimal(1)
+lines.append("#define NSX_INV_FACT_DD \\")
+ents = []
+for n in range(25):
+    if n:
+        fact *= n
+    h, l = dd(Decimal(1) / fact)
+    ents.append(f"{hx(h)}, {hx(l)}")
+for i, e in enumerate(ents):
+    lines.append("    " + e + (", \\" if i + 1 < len(ents) else ""))
+lines.append("#define NSX_INV_FACT_COUNT 25")
+lines.append("")
+
+# 1/(2n+1) for n = 0..23 as double-double (log slow path).
+lines.append("#define NSX_INV_ODD_DD \\")
+ents = []
+for n in range(24):
+    h, l = dd(Decimal(1) / Decimal(2 * n + 1))
+    ents.append(f"{hx(h)}, {hx(l)}")
+for i, e in enumerate(ents):
+    lines.append("    " + e + (", \\" if i + 1 < len(ents) else ""))
+lines.append("#define NSX_INV_ODD_COUNT 24")
+lines.append("")
+
+# sqrt(2) as binary64 (log argument reduction threshold; exactness is not
+# required, only a fixed comparison constant).
+lines.append(f"#define NSX_SQRT2 {hx(rn(TWO.sqrt()))}")
+
+out = Path(__file__).with_name("ns_crmath_consts.h")
+out.write_text("\n".join(lines) + "\n")
+print("wrote", out)

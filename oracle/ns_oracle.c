@@ -1,0 +1,817 @@
+/* ORACLE — test infrastructure only (see ns_oracle.h).
+ *
+ * Plain-C restatement of the reference neural tick. Each function cites the
+ * reference lines it follows. Arithmetic is written so every binary32
+ * operation happens in the reference's order (no contraction: build with
+ * -ffp-contract=off), which is what makes a bit-for-bit comparison with the
+ * reference's own compiled code meaningful.
+ *
+ * Exp/log binding: OR_LIBM builds call glibc expf/logf wherever the reference
+ * evaluates a state-dependent exponential (the reference host build does the
+ * same); constant-argument exponentials, which a C compiler folds to the
+ * correctly rounded value, are the correctly rounded constants in both modes.
+ * The default build binds every exponential to or_cr_expf/or_cr_logf.
+ */
+#include "ns_oracle.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef OR_LIBM
+#define OEXP expf
+#define OLOG logf
+#else
+#define OEXP or_cr_expf
+#define OLOG or_cr_logf
+#endif
+
+float or_bound_expf(float x) { return OEXP(x); }
+float or_bound_logf(float x) { return OLOG(x); }
+
+/* ---- units and fixed constants (src/physiology.cuh:15-25) ---------------- */
+#define DT 1.0f
+#define BRANCHES 4
+#define E_EXC 0.0f
+#define E_INH (-75.0f)
+#define MOD_NE 1
+#define MOD_5HT 2
+#define MOD_DA 4
+#define SUBSTEPS 4
+#define H_SUB (DT / SUBSTEPS)
+
+/* Correctly rounded constant exponentials, computed once (values a compiler
+ * folds `expf(constant)` to). */
+static float K_EXC_MS, K_INH_MS, K_EXC_SUB, K_INH_SUB, K_LTP, K_LTD, K_NE,
+    K_5HT, K_LFS_THR, K_LFS_OPEN[3], K_PRINZ_CA, K_DEND_OFFSET, K_LOG_UP, K_LOG_DOWN;
+static int consts_ready;
+
+static void init_consts(void) {
+    if (consts_ready) return;
+    K_EXC_MS = or_cr_expf(-DT / 3.0f);        /* physiology.cuh:309 */
+    K_INH_MS = or_cr_expf(-DT / 10.0f);       /* physiology.cuh:310 */
+    K_EXC_SUB = or_cr_expf(-H_SUB / 3.0f);    /* physiology.cuh:371 */
+    K_INH_SUB = or_cr_expf(-H_SUB / 10.0f);   /* physiology.cuh:372 */
+    K_LTP = or_cr_expf(-DT / 17.0f);          /* physiology.cuh:537 */
+    K_LTD = or_cr_expf(-DT / 34.0f);          /* physiology.cuh:538 */
+    K_NE = or_cr_expf(-DT / 7200.0f);         /* physiology.cuh:514 */
+    K_5HT = or_cr_expf(-DT / 3600.0f);        /* physiology.cuh:515 */
+    K_LFS_THR = or_cr_expf(-1.0f / 10.0f);    /* physiology.cuh:266 */
+    K_LFS_OPEN[0] = or_cr_expf(-1.0f / 10.0f);  /* physiology.cuh:262,271 */
+    K_LFS_OPEN[1] = or_cr_expf(-1.0f / 40.0f);
+    K_LFS_OPEN[2] = or_cr_expf(-1.0f / 750.0f);
+    K_PRINZ_CA = or_cr_expf(-0.025f / 200.0f);  /* prinz_cell.cuh:75 */
+    K_DEND_OFFSET = 5.0f / (1.0f + or_cr_expf(10.0f));  /* physiology.cuh:228 */
+    K_LOG_UP = or_cr_logf(1.92f);             /* physiology.cuh:249 */
+    K_LOG_DOWN = or_cr_logf(0.70f);           /* physiology.cuh:250 */
+    consts_ready = 1;
+}
+
+static inline float clampf(float x, float lo, float hi) { return fminf(hi, fmaxf(lo, x)); }
+
+/* ---- records ------------------------------------------------------------- */
+typedef struct {               /* src/physiology.cuh:29-45 */
+    float cap, gl, el, vt, slope, a, tau_w, b, vr, adp_b, adp_tau;
+    unsigned char type, active, modulator, inh_tx;
+    float lp_scale[4];         /* src/lp_cell.cuh:19-21 */
+    float prinz_g[8];          /* src/prinz_cell.cuh:17 */
+    float prinz_leak;
+    signed char sens;
+    float rec_base, rec_gain, rec_event, rec_decay, affinity;
+} ngene;
+
+typedef struct {               /* src/physiology.cuh:50-58 */
+    float v, w, adp, inh, depol, log_ampa;
+    float dend[BRANCHES];
+    float u[16];               /* LP x[16] | Prinz v,ca,m[7],h[4] | LFS v,thr,act[3],open[3] */
+    int total;
+    unsigned char spike;
+    float rec_ns;
+    uint32_t rec_rng;
+} nstate;
+
+typedef struct {               /* src/physiology.cuh:59-65 */
+    float w0, U, trec, tfac;
+    int pre, post;
+    unsigned char delay, active, plast, branch, sites, receptors;
+    float slow_rec, slow_depl;
+} sgene;
+
+typedef struct {               /* src/physiology.cuh:66-76 */
+    float w, ru, pre_tr, post_tr, el_ltp, el_ltd, da_age, spine, st_age, pre_age, post_age;
+    int64_t last;
+    uint64_t ready;
+    uint32_t rng;
+    unsigned char arrived;
+    float slow;
+} sstate;
+
+/* ---- neuron parameter profiles (src/physiology.cuh:82-176) --------------- */
+static ngene blank_gene(void) {
+    ngene g; memset(&g, 0, sizeof g);
+    g.sens = -1; g.rec_decay = 3.0f; g.affinity = 1.0f;
+    return g;
+}
+static ngene naud_profile(int inhibitory) {          /* 82-89 */
+    ngene g = blank_gene();
+    if (inhibitory) {
+        g.cap = 59; g.gl = 2.9f; g.el = -62; g.vt = -42; g.slope = 3.0f;
+        g.a = 1.8f; g.tau_w = 16; g.b = 61; g.vr = -54;
+        g.type = 1; g.active = 1; g.inh_tx = 1;
+    } else {
+        g.cap = 104; g.gl = 4.3f; g.el = -65; g.vt = -52; g.slope = 0.8f;
+        g.a = -0.8f; g.tau_w = 88; g.b = 65; g.vr = -53;
+        g.type = 0; g.active = 1;
+    }
+    return g;
+}
+static ngene profile_for_type(unsigned char type) {  /* 94-176 */
+    ngene g;
+    switch (type) {
+    case 0: g = naud_profile(0); g.vr = -68.0f; g.adp_b = 120.0f; g.adp_tau = 45.0f; break;
+    case 1: g = naud_profile(1); break;
+    case 2: g = naud_profile(1); g.type = 2;
+            for (int i = 0; i < 4; ++i) g.lp_scale[i] = 1; break;
+    case 3: g = naud_profile(1); g.type = 3;          /* prinz_cell.cuh:19-24 */
+            g.prinz_g[0] = 400 * 628.0f; g.prinz_g[1] = 2.5f * 628;
+            g.prinz_g[2] = 6 * 628.0f; g.prinz_g[3] = 50 * 628.0f;
+            g.prinz_g[4] = 10 * 628.0f; g.prinz_g[5] = 100 * 628.0f;
+            g.prinz_g[6] = .01f * 628; g.prinz_g[7] = 0; break;
+    case 4: g = naud_profile(0); g.type = 4; g.cap = 8.7f; g.gl = 8.7f / 12.0f;
+            g.el = -60.0f; g.vt = -40.0f; g.vr = -60.0f; g.a = 0; g.b = 0; break;
+    case 5: g = naud_profile(0); g.type = 5; g.cap = 10.0f; g.gl = 0.5f;
+            g.el = -60.0f; g.vt = -40.0f; g.vr = -60.0f; g.a = 0; g.b = 0;
+            g.rec_base = 7.0f; g.rec_gain = 43.0f; g.rec_event = 2.0f; g.rec_decay = 3.0f; break;
+    default: g = naud_profile(0); g.type = 6; g.cap = 1200.0f;
+            g.gl = 1000.0f / 65.6f; g.el = -45.1f; g.vt = -51.8f; break;
+    }
+    return g;
+}
+static int excitatory_kind(unsigned char t) { return t == 0 || t == 4 || t == 5; }  /* 165-167 */
+
+/* 32-bit integer hash seeding the xorshift streams (physiology.cuh:183-187, 395-399). */
+static uint32_t seed_hash(uint32_t seed) {
+    uint32_t x = seed ? seed : 1u;
+    x ^= x >> 16; x *= 0x7feb352du;
+    x ^= x >> 15; x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+static uint32_t xorshift32(uint32_t x) { x ^= x << 13; x ^= x >> 17; x ^= x << 5; return x; }
+
+/* ---- cell models ---------------------------------------------------------- */
+/* LP two-compartment model (src/lp_cell.cuh:23-113). */
+static void lp_initial(float *x) {
+    static const float init[16] = {-56, 0, .2f, 0, 1, 0, 0, 1, 0, 0, 1, 1, 0, .04f, .01f, -56};
+    memcpy(x, init, sizeof init);
+}
+static float lp_sig(float v, float mid, float slope) { return 1.0f / (1.0f + OEXP((v - mid) / slope)); }
+static float lp_ratio(float num, float den, float lim) { return fabsf(den) < 1e-5f ? lim : num / den; }
+static void lp_rates(const float *x, float i_na, const float *sc, float *d) {
+    const float va = x[0], vs = x[15];
+    const float na = x[1] * x[1] * x[1] * x[2] * 7.15f * (va - 50.0f);
+    const float kd = x[8] * x[8] * x[8] * x[8] * 1.43f * (va + 72.0f);
+    const float km = .2613041227f * x[14] * (va + 80.0f);
+    const float aleak = sc[3] * .001004288227f * (va + 50.0f);
+    const float cpl = .004017089073f * (vs - va);
+    d[0] = (-na - kd - km - aleak + cpl) / .1148312178f;
+    const float ev = OEXP(vs / 11.4866f);
+    const float ghk = fabsf(vs) < .001f ? 11.4866f * (x[13] - 15123.5f)
+                                        : vs * (x[13] * ev - 15123.5f) / (ev - 1.0f);
+    const float ca = sc[0] * (x[3] * x[4] * .1247796343f + x[5] * .07142141077f) * .00155982f * ghk * .9f;
+    const float kca = sc[1] * x[6] * x[7] * 1.663612026f * (vs + 72.0f) * .9f;
+    const float amix = lp_sig(vs, 55.0f, -15.0f);
+    const float ka = x[9] * x[9] * x[9] * .8008791415f * (vs + 72.0f) * (amix * x[10] + (1.0f - amix) * x[11]) * .9f;
+    const float ih = sc[2] * x[12] * .0126874385f * (vs + 20.0f) * .9f;
+    const float sleak = sc[3] * .0006901584324f * (vs + 50.0f);
+    d[15] = (-ca - kca - ka - ih - sleak - cpl + (i_na - 2.0f) * .01222505828f) / .0543909161f;
+    float a = lp_ratio(-16.64f - .32f * va, OEXP(-13.0f - va / 4.0f) - 1.0f, 1.28f);
+    float b = lp_ratio(.28f * va + 7.0f, OEXP(va / 5.0f + 5.0f) - 1.0f, 1.4f);
+    d[1] = a * (1.0f - x[1]) - b * x[1];
+    a = .128f * OEXP(-2.66666666667f - va / 18.0f);
+    b = 4.0f / (OEXP(-5.0f - va / 5.0f) + 1.0f);
+    d[2] = a * (1.0f - x[2]) - b * x[2];
+    a = lp_ratio(-1.6f - .032f * va, OEXP(-10.0f - va / 5.0f) - 1.0f, .16f);
+    b = .5f * OEXP(-1.375f - va / 40.0f);
+    d[8] = a * (1.0f - x[8]) - b * x[8];
+    d[3] = (lp_sig(vs, 15.0f, -9.8f) - x[3]) * .045f;
+    d[4] = (lp_sig(vs, -40.0f, 3.2f) - x[4]) * .02f * lp_sig(vs, -15.0f, -10.0f);
+    d[5] = (lp_sig(vs, 29.1336f, -4.43083f) - x[5]) * .0608644f;
+    const float cai = x[13];
+    const float kca_inf = lp_sig(vs, -.6f * cai, -23.0f) * lp_sig(vs, -16.0f - .6f * cai, -5.0f) * cai / (2.5f + cai);
+    d[6] = (kca_inf - x[6]) * .6f;
+    d[7] = (.7f / (.6f + cai) - x[7]) * .035f;
+    d[9] = (lp_sig(vs, -12.0f, -26.0f) - x[9]) * .14f;
+    const float ainf = lp_sig(vs, -62.0f, 6.0f);
+    d[10] = (ainf - x[10]) * .05f;
+    d[11] = (ainf - x[11]) * .0036f * lp_sig(vs, -40.0f, -12.0f);
+    d[12] = (lp_sig(vs, -70.0f, 8.0f) - x[12]) * .00033f / lp_sig(vs, -110.0f, -21.6f);
+    d[13] = -.05049639866f * ca - .01729930764f * (cai - .02f);
+    d[14] = (lp_sig(va, -26.9916223f, -5.957441281f) - x[14]) * .0001386796618f * lp_sig(va, -60.57875745f, -13.25674673f);
+}
+static void lp_integrate(float *x, float i_na, const float *sc) {  /* RK4, 20 x 0.05 ms */
+    const float dt = .05f;
+    for (int step = 0; step < 20; ++step) {
+        float k1[16], k2[16], k3[16], k4[16], y[16];
+        lp_rates(x, i_na, sc, k1);
+        for (int j = 0; j < 16; ++j) y[j] = x[j] + .5f * dt * k1[j];
+        lp_rates(y, i_na, sc, k2);
+        for (int j = 0; j < 16; ++j) y[j] = x[j] + .5f * dt * k2[j];
+        lp_rates(y, i_na, sc, k3);
+        for (int j = 0; j < 16; ++j) y[j] = x[j] + dt * k3[j];
+        lp_rates(y, i_na, sc, k4);
+        for (int j = 0; j < 16; ++j) x[j] += dt * (k1[j] + 2 * k2[j] + 2 * k3[j] + k4[j]) / 6.0f;
+    }
+}
+
+/* Prinz pacemaker (src/prinz_cell.cuh:45-121); u = {v, ca, m[7], h[4]}. */
+static float pz_gate(float v, float a, float b) { return 1.0f / (1.0f + OEXP((v + a) / b)); }
+static float pz_gate2(float v, float a, float b, float c, float d) { return 1.0f / (OEXP((v + a) / b) + OEXP((v + c) / d)); }
+static void pz_substep(float *u, const float *g, float ext_pa, float clamp_ns, float clamp_rev) {
+    const float dt = .025f;
+    float *m = u + 2, *h = u + 9;
+    const float v = u[0], ca = fmaxf(u[1], 0.000001f);
+    const float eca = (8.31451e3f * 283.0f / (2.0f * 96485.3415f)) * OLOG(3000.0f / ca);
+    const float c[8] = {g[0] * m[0] * m[0] * m[0] * h[0], g[1] * m[1] * m[1] * m[1] * h[1],
+                        g[2] * m[2] * m[2] * m[2] * h[2], g[3] * m[3] * m[3] * m[3] * h[3],
+                        g[4] * m[4] * m[4] * m[4] * m[4], g[5] * m[5] * m[5] * m[5] * m[5],
+                        g[6] * m[6], g[7]};
+    const float rev[8] = {50, eca, eca, -80, -80, -80, -20, -50};
+    float gt = clamp_ns, wsum = ext_pa + clamp_ns * clamp_rev;
+    for (int i = 0; i < 8; ++i) { gt += c[i]; wsum += c[i] * rev[i]; }
+    if (fabsf(gt) < .000001f) u[0] = v + dt * wsum / 628.3f;
+    else { const float tgt = wsum / gt; u[0] = tgt + (v - tgt) * OEXP(-dt * gt / 628.3f); }
+    const float ica = (c[1] + c[2]) * (v - eca) / 1000000.0f;
+    const float ca_t = .05f - 14961.0f * ica;
+    u[1] = fmaxf(.000001f, ca_t + (ca - ca_t) * K_PRINZ_CA);
+    const float mi[7] = {pz_gate(v, 25.5f, -5.29f), pz_gate(v, 27.1f, -7.2f), pz_gate(v, 33, -8.1f),
+                         pz_gate(v, 27.2f, -8.7f), (ca / (ca + 3)) * pz_gate(v, 28.3f, -12.6f),
+                         pz_gate(v, 12.3f, -11.8f), pz_gate(v, 75, 5.5f)};
+    const float mt[7] = {2.64f - 2.52f * pz_gate(v, 120, -25), 43.4f - 42.6f * pz_gate(v, 68.1f, -20.5f),
+                         2.8f + 14 * pz_gate2(v, 27, 10, 70, -13), 23.2f - 20.8f * pz_gate(v, 32.9f, -15.2f),
+                         180.6f - 150.2f * pz_gate(v, 46, -22.7f), 14.4f - 12.8f * pz_gate(v, 28.3f, -19.2f),
+                         2.0f / (OEXP(-14.59f - .086f * v) + OEXP(-1.87f + .0701f * v))};
+    for (int i = 0; i < 7; ++i) m[i] = mi[i] + (m[i] - mi[i]) * OEXP(-dt / mt[i]);
+    const float hi_[4] = {pz_gate(v, 48.9f, 5.18f), pz_gate(v, 32.1f, 5.5f), pz_gate(v, 60, 6.2f), pz_gate(v, 56.9f, 4.9f)};
+    const float ht[4] = {(1.34f / (1 + OEXP((v + 62.9f) / -10))) * (1.5f + 1 / (1 + OEXP((v + 34.9f) / 3.6f))),
+                         210 - 179.6f * pz_gate(v, 55, -16.9f), 120 + 300 * pz_gate2(v, 55, 9, 65, -16),
+                         77.2f - 58.4f * pz_gate(v, 38.9f, -26.5f)};
+    for (int i = 0; i < 4; ++i) h[i] = hi_[i] + (h[i] - hi_[i]) * OEXP(-dt / ht[i]);
+}
+static int pz_advance(float *u, const float *g, float ext_pa, float clamp_ns, float clamp_rev) {
+    int spiked = 0;
+    for (int i = 0; i < 40; ++i) {
+        const float before = u[0];
+        pz_substep(u, g, ext_pa, clamp_ns, clamp_rev);
+        spiked |= before < 0 && u[0] >= 0;
+    }
+    return spiked;
+}
+
+/* LFS integrate-and-fire (src/physiology.cuh:258-287); u = {v, thr, act[3], open[3]}. */
+static void lfs_step(const ngene *g, nstate *s, float cur, float exc, float inh) {
+    static const float wt[3] = {250.0f, 10.0f, 4.0f}, op[3] = {10.0f, 40.0f, 750.0f}, cl[3] = {50.0f, 750.0f, 2000.0f};
+    float *u = s->u, *act = u + 2, *open = u + 5;
+    u[1] = g->vt + (u[1] - g->vt) * K_LFS_THR;
+    float under = 0;
+    for (int j = 0; j < 3; ++j) {
+        open[j] += act[j] / op[j] - open[j] / cl[j];
+        act[j] *= K_LFS_OPEN[j];
+        under += wt[j] * open[j];
+    }
+    const float v = u[0];
+    const float i = g->gl * (g->el - v) + exc * (10.0f - v) + inh * (-60.0f - v) + under * (-80.0f - v) + cur;
+    u[0] = v + i / g->cap;
+    s->spike = u[0] >= u[1];
+    if (s->spike) {
+        u[1] = 200.0f;
+        for (int j = 0; j < 3; ++j) act[j] += 1.0f;
+        ++s->total;
+    }
+    s->v = u[0];
+}
+
+/* ---- neuron ---------------------------------------------------------------- */
+static nstate neuron_initial(const ngene *g, uint32_t seed) {     /* physiology.cuh:179-202 */
+    nstate s; memset(&s, 0, sizeof s);
+    s.v = g->el;
+    uint32_t x = seed_hash(seed);
+    s.rec_rng = x ? x : 1u;
+    if (g->type == 2) { lp_initial(s.u); s.v = s.u[15] - 9.342518882f; }
+    if (g->type == 3) {
+        memset(s.u, 0, sizeof s.u);
+        s.u[0] = -50.0f; s.u[1] = .05f;
+        for (int i = 0; i < 4; ++i) s.u[9 + i] = 1.0f;
+        s.v = s.u[0];
+    }
+    if (g->type == 6) { memset(s.u, 0, sizeof s.u); s.u[0] = g->el; s.u[1] = g->vt; }
+    return s;
+}
+
+static float receptor_drive(const ngene *g, nstate *s, float level) {  /* physiology.cuh:206-219 */
+    if (g->sens < 0 || g->rec_event <= 0) return 0;
+    float rate = clampf(g->rec_base + g->rec_gain * level, 0, 1000);
+    s->rec_rng = xorshift32(s->rec_rng);
+    float u = (float)(s->rec_rng >> 8) * (1.0f / 16777216.0f);
+    s->rec_ns *= OEXP(-DT / g->rec_decay);
+    if (u < rate * (DT / 1000.0f)) s->rec_ns += g->rec_event;
+    return s->rec_ns * (E_EXC - s->v);
+}
+
+static float branch_gain(float gs) {                               /* physiology.cuh:226-230 */
+    float regen = 5.0f / (1.0f + OEXP(-(gs - 4.0f) / 0.4f));
+    return fminf(11.0f, gs + regen - K_DEND_OFFSET);
+}
+
+static void homeostasis(const ngene *g, nstate *s, float elapsed, float hz) {  /* 243-253 */
+    if (g->type != 0) return;
+    float ratio = clampf(hz / 0.4f, 0.0f, 2.65f);
+    float change = ratio < 1.0f ? K_LOG_UP * (1.0f - ratio) : K_LOG_DOWN * ((ratio - 1.0f) / 1.65f);
+    s->log_ampa = clampf(s->log_ampa + change * (elapsed / 172800000.0f), -3.0f, 3.0f);
+}
+
+/* physiology.cuh:290-374 (clamp_leak = 0, clamp_reversal = -68 as every caller passes). */
+static void neuron_tick(const ngene *g, nstate *s, float cur, const float *exc_in, float inh_in) {
+    const float clamp_leak = 0.0f, clamp_rev = -68.0f;
+    for (int k = 0; k < BRANCHES; ++k) s->dend[k] += exc_in[k];
+    float sub = fmaxf(0.0f, fminf(s->v, -50.0f) - g->el);
+    s->depol += 0.1f * (sub - s->depol);
+    s->inh += inh_in;
+    s->spike = 0;
+    if (g->type == 6 || g->type == 2 || g->type == 3) {
+        float exc = 0;
+        for (int k = 0; k < BRANCHES; ++k) exc += s->dend[k];
+        if (g->type == 6) {
+            lfs_step(g, s, cur, exc, s->inh);
+        } else if (g->type == 2) {
+            float axon_before = s->u[0];
+            float ext = cur + exc * (E_EXC - s->v) + s->inh * (E_INH - s->v) - clamp_leak * (s->v - clamp_rev);
+            lp_integrate(s->u, ext / 1000.0f, g->lp_scale);
+            s->v = s->u[15] - 9.342518882f;
+            s->spike = axon_before < 0 && s->u[0] >= 0;
+            s->total += s->spike;
+        } else {
+            const float ext = cur + exc * (E_EXC - s->v) + s->inh * (E_INH - s->v);
+            s->spike = (unsigned char)pz_advance(s->u, g->prinz_g, ext, g->prinz_leak + clamp_leak, clamp_rev);
+            s->total += s->spike;
+            s->v = s->u[0];
+        }
+        for (int k = 0; k < BRANCHES; ++k) s->dend[k] *= K_EXC_MS;
+        s->inh *= K_INH_MS;
+        return;
+    }
+    for (int step = 0; step < SUBSTEPS; ++step) {
+        float v = s->v;
+        s->w += H_SUB * (g->a * (v - g->el) - s->w) / g->tau_w;
+        float expo = clampf((v - g->vt) / g->slope, -20.0f, 10.0f);
+        float soma = 0;
+        for (int k = 0; k < BRANCHES; ++k) soma += g->type == 0 ? branch_gain(s->dend[k]) : s->dend[k];
+        float dv = g->gl * (g->el - v) + g->gl * g->slope * OEXP(expo) + soma * (E_EXC - v) +
+                   s->inh * (E_INH - v) + cur + s->adp - s->w - clamp_leak * (v - clamp_rev);
+        s->v = v + H_SUB * dv / g->cap;
+        if (s->v >= 0.0f) {
+            s->spike = 1; ++s->total;
+            s->v = g->vr; s->w += g->b; s->adp += g->adp_b;
+        }
+        if (g->adp_tau > 0) s->adp *= OEXP(-H_SUB / g->adp_tau);
+        for (int k = 0; k < BRANCHES; ++k) s->dend[k] *= K_EXC_SUB;
+        s->inh *= K_INH_SUB;
+    }
+}
+
+/* ---- synapse ---------------------------------------------------------------- */
+static int sites_of(const sgene *g) { return g->sites ? (g->sites > 64 ? 64 : g->sites) : 14; }  /* 376-378 */
+static float uniform24(sstate *s) { s->rng = xorshift32(s->rng); return (float)(s->rng >> 8) * (1.0f / 16777216.0f); }
+
+static sstate synapse_initial(const sgene *g, uint32_t seed) {  /* 393-404 */
+    sstate s; memset(&s, 0, sizeof s);
+    uint32_t x = seed_hash(seed);
+    if (!x) x = 1;
+    int n = sites_of(g);
+    s.w = g->w0; s.da_age = -1; s.spine = 1; s.st_age = -1;
+    s.pre_age = 1000000; s.post_age = 1000000; s.last = -1000000;
+    s.ready = n == 64 ? ~(uint64_t)0 : (((uint64_t)1 << n) - 1);
+    s.rng = x; s.arrived = 0; s.slow = 1;
+    return s;
+}
+
+static float da_window(float age) {                     /* 408-412 */
+    if (age < 0 || age > 20000.0f) return 0;
+    float x = age / 2000.0f;
+    return x * x * x * x * OEXP(4.0f * (1.0f - x));
+}
+static float spine_window(float age) {                  /* 416-420 */
+    if (age < 0 || age > 5000.0f) return 0;
+    float x = age / 1000.0f;
+    return x * x * x * OEXP(3.0f * (1.0f - x));
+}
+
+static float release(const sgene *g, sstate *s, int64_t tick) {  /* 425-454 */
+    float p_rec = 0;
+    if (s->last > -1000000) {
+        float dt = (float)(tick - s->last) * DT;
+        p_rec = 1.0f - OEXP(-dt / g->trec);
+        if (g->tfac > 0) s->ru *= OEXP(-dt / g->tfac);
+        if (g->slow_rec > 0) s->slow = 1.0f - (1.0f - s->slow) * OEXP(-dt / g->slow_rec);
+    }
+    s->ru = g->tfac > 0 ? s->ru + g->U * (1.0f - s->ru) : g->U;
+    int released = 0, n = sites_of(g);
+    for (int site = 0; site < n; ++site) {
+        uint64_t bit = (uint64_t)1 << site;
+        if (!(s->ready & bit) && uniform24(s) < p_rec) s->ready |= bit;
+        if ((s->ready & bit) && uniform24(s) < s->ru) { s->ready &= ~bit; ++released; }
+    }
+    s->last = tick;
+    float out = s->w * (float)released / (float)n * s->slow;
+    if (g->slow_rec > 0) s->slow *= 1.0f - g->slow_depl;
+    return out;
+}
+
+/* physiology.cuh:459-555 with nmda/l-type/cp-AMPA/PKA all available. */
+static void plasticity_tick(const sgene *g, sstate *s, int arrived, int post_spike, int pair,
+                            float depol, unsigned char mod) {
+    if (!g->plast || !pair) return;
+    if (g->plast == 5) {
+        if (s->st_age >= 0) { s->st_age += DT; if (s->st_age > 5000.0f) s->st_age = -1; }
+        s->pre_age += DT;
+        if (arrived) s->pre_age = 0;
+        if (post_spike && s->pre_age <= 15.0f && s->st_age < 0) s->st_age = 0;
+        if ((mod & MOD_DA) && (g->receptors & MOD_DA))
+            s->spine = clampf(s->spine + 0.025f * spine_window(s->st_age), 1.0f, 2.0f);
+        return;
+    }
+    if (g->plast == 4) {
+        if (s->da_age >= 0) { s->da_age += DT; if (s->da_age > 20000.0f) s->da_age = -1; }
+        s->pre_age += DT;
+        if (arrived) s->pre_age = 0;
+        if (post_spike && s->pre_age <= 15.0f && (s->da_age < 0 || s->da_age > 30.0f)) {
+            s->da_age = 0;
+            s->w -= 0.005383f * g->w0;
+        }
+        if ((mod & MOD_DA) && (g->receptors & MOD_DA)) {
+            s->w += 0.00453f * da_window(s->da_age) * g->w0;
+            s->da_age = -1;
+        }
+        s->w = clampf(s->w, 0.0f, 2.0f * g->w0);
+        return;
+    }
+    if (g->plast == 3) {
+        s->el_ltp *= K_NE;
+        s->el_ltd *= K_5HT;
+        s->pre_age += DT; s->post_age += DT;
+        if (arrived) { if (s->post_age <= 15.0f) s->el_ltd += 1.0f; s->pre_age = 0; }
+        if (post_spike) { if (s->pre_age <= 15.0f) s->el_ltp += 1.0f; s->post_age = 0; }
+        if ((mod & MOD_NE) && (g->receptors & MOD_NE)) { s->w += 0.0048f * s->el_ltp * g->w0; s->el_ltp = 0; }
+        if ((mod & MOD_5HT) && (g->receptors & MOD_5HT)) { s->w -= 0.0075f * s->el_ltd * g->w0; s->el_ltd = 0; }
+        s->w = clampf(s->w, 0.0f, 2.0f * g->w0);
+        return;
+    }
+    s->pre_tr *= K_LTP;
+    s->post_tr *= K_LTD;
+    s->pre_age += DT; s->post_age += DT;
+    if (arrived) {
+        if (s->post_age <= (g->plast == 2 ? 50.0f : 20.0f)) s->w *= 1.0f - 0.004f * s->post_tr;
+        s->pre_tr += 1.0f;
+        s->pre_age = 0;
+    }
+    if (post_spike) {
+        if (s->pre_age <= 20.0f && (g->plast == 1 || depol >= 2.3f))
+            s->w += 0.016f * s->pre_tr * (2.0f * g->w0 - s->w);
+        s->post_tr += 1.0f;
+        s->post_age = 0;
+    }
+    s->w = clampf(s->w, 0.0f, 2.0f * g->w0);
+}
+
+/* physiology.cuh:559-586 */
+static void plasticity_quiet(const sgene *g, sstate *s, int ticks) {
+    if (ticks <= 0 || !g->plast) return;
+    float el = (float)ticks * DT;
+    if (g->plast == 5) {
+        if (s->st_age >= 0) { s->st_age += el; if (s->st_age > 5000.0f) s->st_age = -1; }
+        s->pre_age += el;
+    } else if (g->plast == 4) {
+        if (s->da_age >= 0) { s->da_age += el; if (s->da_age > 20000.0f) s->da_age = -1; }
+        s->pre_age += el;
+    } else if (g->plast == 3) {
+        s->el_ltp *= OEXP(-el / 7200.0f);
+        s->el_ltd *= OEXP(-el / 3600.0f);
+        s->pre_age += el; s->post_age += el;
+    } else {
+        s->pre_tr *= OEXP(-el / 17.0f);
+        s->post_tr *= OEXP(-el / 34.0f);
+        s->pre_age += el; s->post_age += el;
+    }
+}
+
+/* ---- brain (gym_adapter/native.cpp:23-38, core.cuh:12-75) ------------------ */
+#define RING 32
+struct or_brain {
+    int count, edges, channels, outputs, ring;
+    ngene *ng; sgene *sg; nstate *ns; sstate *ss;
+    int *motors, *sensory;
+    uint8_t *hist;              /* count x ring spike bytes, slot tick % ring */
+    float *exc, *inh; uint8_t *mod;
+    uint32_t *orig_n, *orig_s;
+    int64_t tick, events;
+};
+
+static int bad(char *err, int len, const char *msg) { if (err && len > 0) snprintf(err, (size_t)len, "%s", msg); return 0; }
+
+or_brain *or_create(int count, int edges, int channels, int outputs, const float *ngr,
+                    const float *sgr, const int *motors, int max_delay, char *err, int errlen) {
+    init_consts();
+    if (count < 1 || edges < 0 || channels < 1 || channels > 65535 || outputs < 1) {
+        bad(err, errlen, "Invalid brain dimensions"); return NULL;
+    }
+    if (max_delay < 1 || max_delay > RING - 1) { bad(err, errlen, "Invalid delay ring"); return NULL; }
+    or_brain *b = (or_brain *)calloc(1, sizeof *b);
+    b->count = count; b->edges = edges; b->channels = channels; b->outputs = outputs;
+    b->ring = max_delay + 1;
+    b->ng = (ngene *)calloc((size_t)count, sizeof(ngene));
+    b->sg = (sgene *)calloc((size_t)(edges ? edges : 1), sizeof(sgene));
+    b->ns = (nstate *)calloc((size_t)count, sizeof(nstate));
+    b->ss = (sstate *)calloc((size_t)(edges ? edges : 1), sizeof(sstate));
+    b->motors = (int *)calloc((size_t)outputs, sizeof(int));
+    b->sensory = (int *)calloc((size_t)count, sizeof(int));
+    b->hist = (uint8_t *)calloc((size_t)count * RING, 1);
+    b->exc = (float *)calloc((size_t)count * BRANCHES, sizeof(float));
+    b->inh = (float *)calloc((size_t)count, sizeof(float));
+    b->mod = (uint8_t *)calloc((size_t)count, 1);
+    for (int i = 0; i < count; ++i) {                          /* native.cpp:128-141 */
+        const float *p = ngr + (size_t)i * 10;
+        for (int f = 0; f < 10; ++f) if (p[f] != p[f]) { bad(err, errlen, "Invalid neuron gene"); or_destroy(b); return NULL; }
+        if (p[0] < 0 || p[0] > 6 || p[1] < -1 || p[1] >= channels || p[2] < 0 || p[2] > 1 || p[3] < 0 ||
+            p[3] > 1 || p[4] < 0 || p[4] > 3) { bad(err, errlen, "Invalid neuron gene"); or_destroy(b); return NULL; }
+        ngene g = profile_for_type((unsigned char)p[0]);
+        b->sensory[i] = (int)p[1];
+        g.sens = p[1] < 0 ? -1 : 0;
+        g.active = (unsigned char)p[2];
+        g.inh_tx = (unsigned char)p[3];
+        g.modulator = (unsigned char)p[4];
+        if (p[5] <= 0 || p[6] <= 0 || p[7] < -80 || p[7] > -20 || p[8] < 0 || p[9] < 0) {
+            bad(err, errlen, "Invalid membrane parameters"); or_destroy(b); return NULL;
+        }
+        g.cap *= p[5]; g.gl *= p[6]; g.vt = p[7];
+        g.rec_base = 0; g.rec_gain = p[8]; g.rec_event = p[9];
+        b->ng[i] = g;
+    }
+    for (int i = 0; i < edges; ++i) {                          /* native.cpp:142-150 */
+        const float *p = sgr + (size_t)i * 11;
+        for (int f = 0; f < 11; ++f) if (p[f] != p[f]) { bad(err, errlen, "Invalid synapse gene"); or_destroy(b); return NULL; }
+        if (p[0] < 0 || p[0] >= count || p[1] < 0 || p[1] >= count || p[2] < 0 || p[3] < 0 || p[3] > 1 ||
+            p[4] < 1 || p[4] > max_delay || p[5] < 0 || p[5] >= BRANCHES || p[6] <= 0 || p[6] > 1 ||
+            p[7] <= 0 || p[8] < 0 || p[9] < 0 || p[9] > 5 || p[10] < 0 || p[10] > 7) {
+            bad(err, errlen, "Invalid synapse gene"); or_destroy(b); return NULL;
+        }
+        sgene g; memset(&g, 0, sizeof g);
+        g.pre = (int)p[0]; g.post = (int)p[1]; g.w0 = p[2];
+        g.active = (unsigned char)p[3]; g.delay = (unsigned char)p[4]; g.branch = (unsigned char)p[5];
+        g.U = p[6]; g.trec = p[7]; g.tfac = p[8];
+        g.plast = (unsigned char)p[9]; g.receptors = (unsigned char)p[10]; g.sites = 14;
+        b->sg[i] = g;
+    }
+    for (int i = 0; i < outputs; ++i) {
+        if (motors[i] < 0 || motors[i] >= count) { bad(err, errlen, "Invalid motor index"); or_destroy(b); return NULL; }
+        b->motors[i] = motors[i];
+    }
+    return b;
+}
+
+void or_original_indices(or_brain *b, const uint32_t *neurons, const uint32_t *synapses) {
+    free(b->orig_n); free(b->orig_s);
+    b->orig_n = (uint32_t *)malloc((size_t)b->count * 4);
+    memcpy(b->orig_n, neurons, (size_t)b->count * 4);
+    b->orig_s = NULL;
+    if (b->edges) {
+        b->orig_s = (uint32_t *)malloc((size_t)b->edges * 4);
+        memcpy(b->orig_s, synapses, (size_t)b->edges * 4);
+    }
+}
+
+void or_destroy(or_brain *b) {
+    if (!b) return;
+    free(b->ng); free(b->sg); free(b->ns); free(b->ss); free(b->motors); free(b->sensory);
+    free(b->hist); free(b->exc); free(b->inh); free(b->mod); free(b->orig_n); free(b->orig_s);
+    free(b);
+}
+
+void or_reset(or_brain *b, uint32_t seed) {                    /* core.cuh:25-29, native.cpp:164-169 */
+    b->tick = 0;
+    for (int i = 0; i < b->count; ++i) {
+        uint32_t idx = b->orig_n ? b->orig_n[i] : (uint32_t)i;
+        b->ns[i] = neuron_initial(&b->ng[i], seed + idx * 7919u);
+        memset(b->hist + (size_t)i * RING, 0, RING);
+    }
+    for (int i = 0; i < b->edges; ++i) {
+        uint32_t idx = b->orig_s ? b->orig_s[i] : (uint32_t)i;
+        b->ss[i] = synapse_initial(&b->sg[i], seed + idx * 104729u);
+    }
+}
+
+static int edge_live(const or_brain *b, const sgene *g) {
+    return g->active && b->ng[g->pre].active && b->ng[g->post].active;
+}
+
+int or_step(or_brain *b, const float *input, int ticks, float gain, float *output,
+            uint8_t *raster, int stop_on_nonfinite) {                /* core.cuh:30-75 */
+    int failed = 0;
+    const int64_t tick0 = b->tick;
+    b->events = 0;
+    for (int j = 0; j < b->outputs; ++j) output[j] = 0;
+    for (int t = 0; t < ticks; ++t, ++b->tick) {
+        memset(b->exc, 0, sizeof(float) * (size_t)b->count * BRANCHES);
+        memset(b->inh, 0, sizeof(float) * (size_t)b->count);
+        memset(b->mod, 0, (size_t)b->count);
+        for (int j = 0; j < b->edges; ++j) {                     /* delivery, edge order */
+            const sgene *g = &b->sg[j]; sstate *s = &b->ss[j];
+            s->arrived = 0;
+            if (!edge_live(b, g)) continue;
+            s->arrived = b->tick >= g->delay &&
+                         b->hist[(size_t)g->pre * RING + (size_t)((b->tick - g->delay) % b->ring)];
+            if (!s->arrived) continue;
+            ++b->events;
+            const ngene *src = &b->ng[g->pre];
+            float rel = (!src->inh_tx || src->modulator) ? release(g, s, b->tick) : s->w;
+            if (src->modulator) { if (rel > 0) b->mod[g->post] |= (uint8_t)(1u << (src->modulator - 1)); }
+            else if (src->inh_tx) b->inh[g->post] += rel;
+            else b->exc[(size_t)g->post * BRANCHES + g->branch] += rel * OEXP(b->ns[g->post].log_ampa);
+        }
+        for (int j = 0; j < b->count; ++j) {                     /* neurons, index order */
+            const ngene *g = &b->ng[j]; nstate *s = &b->ns[j];
+            if (g->active) {
+                float cur = 0;
+                if (b->sensory[j] >= 0)
+                    cur = g->type == 5 ? receptor_drive(g, s, input[b->sensory[j]]) : gain * input[b->sensory[j]];
+                neuron_tick(g, s, cur, b->exc + (size_t)j * BRANCHES, b->inh[j]);
+                if (!isfinite(s->v)) {
+                    /* ns_step keeps its tick counter on failure (native.cpp:176-177) */
+                    if (stop_on_nonfinite) { b->tick = tick0; return -1; }
+                    failed = 1;
+                }
+            } else s->spike = 0;
+            b->hist[(size_t)j * RING + (size_t)(b->tick % b->ring)] = s->spike;
+            if (raster) raster[(size_t)t * b->count + j] = s->spike;
+        }
+        for (int j = 0; j < b->edges; ++j) {                     /* plasticity, edge order */
+            const sgene *g = &b->sg[j]; sstate *s = &b->ss[j];
+            if (!edge_live(b, g)) continue;
+            const ngene *a = &b->ng[g->pre], *z = &b->ng[g->post];
+            int pair = !a->inh_tx && excitatory_kind(a->type) && !a->modulator && !z->inh_tx && excitatory_kind(z->type);
+            plasticity_tick(g, s, s->arrived, b->ns[g->post].spike, pair, b->ns[g->post].depol, b->mod[g->post]);
+        }
+        for (int j = 0; j < b->outputs; ++j) output[j] += (float)b->ns[b->motors[j]].spike;
+    }
+    for (int j = 0; j < b->count; ++j)                            /* homeostasis, core.cuh:71-72 */
+        if (b->ng[j].active)
+            homeostasis(&b->ng[j], &b->ns[j], (float)ticks,
+                        (float)b->ns[j].total * 1000.0f / (float)(ticks > b->tick ? ticks : b->tick));
+    return failed ? -1 : 0;
+}
+
+static uint32_t fw(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+
+void or_dump(const or_brain *b, uint32_t *nw, uint32_t *sw, int64_t *tick) {
+    if (tick) *tick = b->tick;
+    if (nw) for (int i = 0; i < b->count; ++i) {
+        const nstate *s = &b->ns[i]; uint32_t *o = nw + (size_t)i * OR_NEURON_WORDS;
+        memset(o, 0, OR_NEURON_WORDS * 4);
+        o[0] = fw(s->v); o[1] = fw(s->w); o[2] = fw(s->adp); o[3] = fw(s->inh);
+        o[4] = fw(s->depol); o[5] = fw(s->log_ampa);
+        for (int k = 0; k < 4; ++k) o[6 + k] = fw(s->dend[k]);
+        for (int k = 0; k < 16; ++k) o[10 + k] = fw(s->u[k]);
+        o[26] = (uint32_t)s->total; o[27] = s->spike; o[28] = fw(s->rec_ns); o[29] = s->rec_rng;
+        uint32_t h = 0;   /* bit k = spike at tick - 1 - k, k < ring-1 (the readable window) */
+        for (int k = 0; k < b->ring - 1 && k < 31; ++k) {
+            int64_t t = b->tick - 1 - k;
+            if (t < 0) break;
+            if (b->hist[(size_t)i * RING + (size_t)(t % b->ring)]) h |= 1u << k;
+        }
+        o[30] = h;
+    }
+    if (sw) for (int i = 0; i < b->edges; ++i) {
+        const sstate *s = &b->ss[i]; uint32_t *o = sw + (size_t)i * OR_SYNAPSE_WORDS;
+        memset(o, 0, OR_SYNAPSE_WORDS * 4);
+        o[0] = fw(s->w); o[1] = fw(s->ru); o[2] = fw(s->pre_tr); o[3] = fw(s->post_tr);
+        o[4] = fw(s->el_ltp); o[5] = fw(s->el_ltd); o[6] = fw(s->da_age); o[7] = fw(s->spine);
+        o[8] = fw(s->st_age); o[9] = fw(s->pre_age); o[10] = fw(s->post_age);
+        o[11] = (uint32_t)(uint64_t)s->last; o[12] = (uint32_t)((uint64_t)s->last >> 32);
+        o[13] = (uint32_t)s->ready; o[14] = (uint32_t)(s->ready >> 32);
+        o[15] = s->rng; o[16] = s->arrived; o[17] = fw(s->slow);
+    }
+}
+
+int or_count(const or_brain *b) { return b->count; }
+int or_edges(const or_brain *b) { return b->edges; }
+int64_t or_last_events(const or_brain *b) { return b->events; }
+
+/* ---- reference protocol checks ------------------------------------------------
+ * Restated from tests/physiology.cpp, tests/event_synapses.cpp and
+ * tests/cuda_relay_parity.cu; the Python test applies the same windows. */
+static int step_current_spikes(const ngene *g, float pa, int *first_isi, int *last_isi) {
+    nstate s = neuron_initial(g, 1);
+    const float none[4] = {0, 0, 0, 0};
+    int n = 0, prev2 = -1, prev = -1;
+    *first_isi = *last_isi = 0;
+    for (int t = 0; t < 2000; ++t) {
+        neuron_tick(g, &s, pa, none, 0);
+        if (s.spike) {
+            if (n == 1) *first_isi = t - prev;
+            prev2 = prev; prev = t; ++n;
+            if (n >= 2) *last_isi = prev - prev2;
+        }
+    }
+    return n;
+}
+static float stdp_pairs(int interval, int exc_target, unsigned char prof, float depol, int pairs) {
+    sgene g; memset(&g, 0, sizeof g);
+    g.w0 = 1.0f; g.U = 0.55f; g.trec = 450.0f; g.active = 1; g.delay = 1; g.plast = prof; g.sites = 14;
+    sstate s = synapse_initial(&g, 1);
+    for (int t = 0; t < pairs * 1000; ++t) {
+        int ph = t % 1000;
+        plasticity_tick(&g, &s, ph == 100, ph == 100 + interval, exc_target, depol, 0);
+    }
+    return s.w;
+}
+int or_protocols(float *out, int n) {
+    init_consts();
+    float r[40]; memset(r, 0, sizeof r);
+    int fi, li;
+    ngene rs = naud_profile(0), cna = naud_profile(1);
+    r[0] = (float)step_current_spikes(&rs, 130, &fi, &li); r[1] = (float)fi; r[2] = (float)li;
+    r[3] = (float)step_current_spikes(&cna, 150, &fi, &li); r[4] = (float)fi; r[5] = (float)li;
+    r[6] = (float)step_current_spikes(&rs, 0, &fi, &li);
+    /* release means (physiology.cpp:177-192) */
+    sgene dep; memset(&dep, 0, sizeof dep);
+    dep.w0 = 1.0f; dep.U = 0.55f; dep.trec = 450.0f; dep.active = 1; dep.delay = 1; dep.sites = 14;
+    double first = 0, second = 0, rec = 0;
+    for (int trial = 1; trial <= 10000; ++trial) {
+        sstate s = synapse_initial(&dep, (uint32_t)trial);
+        first += release(&dep, &s, 0); second += release(&dep, &s, 50); rec += release(&dep, &s, 2050);
+    }
+    r[7] = (float)(first / 10000); r[8] = (float)(second / 10000); r[9] = (float)(rec / 10000);
+    /* STDP pairs (physiology.cpp:226-239) */
+    r[10] = stdp_pairs(10, 1, 1, 0, 60); r[11] = stdp_pairs(-10, 1, 1, 0, 60);
+    r[12] = stdp_pairs(50, 1, 1, 0, 60); r[13] = stdp_pairs(-50, 1, 1, 0, 60);
+    r[14] = stdp_pairs(10, 0, 1, 0, 60);
+    r[15] = stdp_pairs(10, 1, 2, 0, 50); r[16] = stdp_pairs(10, 1, 2, 3, 50);
+    /* homeostasis 48 h (physiology.cpp:288-315) */
+    nstate q = neuron_initial(&rs, 1), c = q, a = q;
+    for (int h = 0; h < 48; ++h) {
+        homeostasis(&rs, &q, 3600000.0f, 0.0f);
+        homeostasis(&rs, &c, 3600000.0f, 0.4f);
+        homeostasis(&rs, &a, 3600000.0f, 1.06f);
+    }
+    r[17] = (float)exp((double)q.log_ampa); r[18] = (float)exp((double)c.log_ampa); r[19] = (float)exp((double)a.log_ampa);
+    /* quiet-jump agreement (event_synapses.cpp:25-60): max relative difference */
+    float worst = 0;
+    for (int prof = 1; prof <= 5; ++prof) {
+        sgene g; memset(&g, 0, sizeof g);
+        g.plast = (unsigned char)prof; g.w0 = 1.0f; g.receptors = MOD_NE | MOD_5HT | MOD_DA;
+        sstate reg = synapse_initial(&g, 1), ev = reg;
+        int last = -1;
+        for (int t = 0; t < 8192; ++t) {
+            int arr = t % 23 == 4 || t % 137 == 5, post = t % 29 == 8 || t % 137 == 9;
+            unsigned char m = 0;
+            if (t % 67 == 13) m |= MOD_NE;
+            if (t % 71 == 17) m |= MOD_5HT;
+            if (t % 73 == 21) m |= MOD_DA;
+            plasticity_tick(&g, &reg, arr, post, 1, 3.0f, m);
+            if (arr || post || m) {
+                plasticity_quiet(&g, &ev, t - last - 1);
+                plasticity_tick(&g, &ev, arr, post, 1, 3.0f, m);
+                last = t;
+            }
+            if (t % 16 == 15) {
+                plasticity_quiet(&g, &ev, t - last);
+                last = t;
+                const float *x = &reg.w, *y = &ev.w;
+                for (int f = 0; f < 11; ++f) {
+                    float den = fmaxf(1.0f, fmaxf(fabsf(x[f]), fabsf(y[f])));
+                    float d = fabsf(x[f] - y[f]) / den;
+                    if (d > worst) worst = d;
+                }
+            }
+        }
+    }
+    r[20] = worst;
+    /* CPU relay (cuda_relay_parity.cu:15-40) */
+    ngene l5 = profile_for_type(0);
+    nstate cell = neuron_initial(&l5, 19);
+    sgene orn; memset(&orn, 0, sizeof orn);
+    orn.w0 = 29.0f / (60.0f * 0.75f); orn.U = 0.75f; orn.trec = 50.0f; orn.sites = 50;
+    orn.slow_rec = 7500.0f; orn.slow_depl = 0.023f;
+    sstate rel = synapse_initial(&orn, 31);
+    float peak = l5.el, released = 0; int arrivals = 0;
+    for (int t = 0; t < 2000; ++t) {
+        float e[4] = {0, 0, 0, 0};
+        if (t % 137 == 0) { e[0] = release(&orn, &rel, t); released += e[0]; ++arrivals; }
+        neuron_tick(&l5, &cell, 0, e, 0);
+        peak = fmaxf(peak, cell.v);
+    }
+    r[21] = (float)arrivals; r[22] = released; r[23] = peak; r[24] = cell.v; r[25] = (float)cell.total;
+    int m = n < 40 ? n : 40;
+    memcpy(out, r, (size_t)m * sizeof(float));
+    return m;
+}

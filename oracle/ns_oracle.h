@@ -1,0 +1,65 @@
+/* ORACLE — test infrastructure only. Nothing in the product library includes,
+ * links or calls this code; tests, the smoke check and the CPU-baseline leg of
+ * bench.py use it as the checker.
+ *
+ * A plain-C restatement of the reference's neural tick:
+ *   physiology  src/physiology.cuh:29-586, src/lp_cell.cuh:16-113,
+ *               src/prinz_cell.cuh:17-121
+ *   ordering    gym_adapter/core.cuh:25-75 (edge order per tick)
+ *   ABI rules   gym_adapter/native.cpp:121-183
+ * Parity pin: built in its libm mode (-DOR_LIBM) it reproduces the reference
+ * host executor compiled from the reference's own sources (oracle/_ref) bit for
+ * bit; in its default mode exp/log are correctly rounded (or_crmath.c), which
+ * is the arithmetic the CUDA engine implements.
+ */
+#ifndef NS_ORACLE_H
+#define NS_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Canonical state dump layout shared by oracle, reference harness and the
+ * CUDA engine's state readback (32-bit words). */
+enum { OR_NEURON_WORDS = 32, OR_SYNAPSE_WORDS = 20 };
+
+typedef struct or_brain or_brain;
+
+/* ns_create semantics (gym_adapter/native.cpp:121-157); max_delay is 8 for
+ * the reference ABI and up to 31 for the extended delay ring. Returns NULL and
+ * fills err on invalid input. */
+or_brain *or_create(int count, int edges, int channels, int outputs,
+                    const float *ng, const float *sg, const int *motors,
+                    int max_delay, char *err, int errlen);
+void or_original_indices(or_brain *b, const uint32_t *neurons, const uint32_t *synapses);
+void or_destroy(or_brain *b);
+void or_reset(or_brain *b, uint32_t seed);
+/* ns_step semantics: 0, or -1 on a non-finite voltage. When stop_on_nonfinite
+ * is 0 the step records the failure, keeps integrating (the CUDA batch
+ * semantics of gym_adapter/gpu.cu:255) and returns -1 at the end.
+ * raster (optional): ticks x count spike bytes. */
+int or_step(or_brain *b, const float *input, int ticks, float gain, float *output,
+            uint8_t *raster, int stop_on_nonfinite);
+/* Canonical dump: neurons count x 32 words, synapses edges x 20 words. */
+void or_dump(const or_brain *b, uint32_t *nw, uint32_t *sw, int64_t *tick);
+int or_count(const or_brain *b);
+int or_edges(const or_brain *b);
+/* Number of synapses that arrived (delivered a spike) during the last or_step. */
+int64_t or_last_events(const or_brain *b);
+
+/* Correctly rounded binary32 exp/log (or_crmath.c). */
+float or_cr_expf(float x);
+float or_cr_logf(float x);
+/* The exp/log this build binds the physiology to. */
+float or_bound_expf(float x);
+float or_bound_logf(float x);
+
+/* Reference protocol checks (tests/physiology.cpp, tests/event_synapses.cpp,
+ * tests/cuda_relay_parity.cu restated); results written as floats. */
+int or_protocols(float *out, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,183 @@
+"""ORACLE — test infrastructure only. ctypes drivers for the C oracle
+(oracle/_build) and for the reference host executor compiled from the
+reference's own sources (oracle/_ref). Used by tests/, the smoke check and the
+CPU-baseline leg of bench.py; never by the product library."""
+from __future__ import annotations
+
+import ctypes as ct
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+NW, SW = 32, 20
+
+_f = ct.POINTER(ct.c_float)
+_u8 = ct.POINTER(ct.c_uint8)
+_u32 = ct.POINTER(ct.c_uint32)
+_i32 = ct.POINTER(ct.c_int)
+_i64 = ct.POINTER(ct.c_int64)
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t)
+
+
+_libs = {}
+
+
+def oracle_lib(libm=False):
+    """The C restatement: correctly rounded exp/log (default) or glibc."""
+    name = "libns_oracle_libm.so" if libm else "libns_oracle.so"
+    if name not in _libs:
+        path = HERE / "_build" / name
+        if not path.exists():
+            from . import build as _b  # noqa
+        lib = ct.CDLL(str(path))
+        lib.or_create.restype = ct.c_void_p
+        lib.or_create.argtypes = [ct.c_int] * 4 + [_f, _f, _i32, ct.c_int, ct.c_char_p, ct.c_int]
+        lib.or_original_indices.argtypes = [ct.c_void_p, _u32, _u32]
+        lib.or_destroy.argtypes = [ct.c_void_p]
+        lib.or_reset.argtypes = [ct.c_void_p, ct.c_uint32]
+        lib.or_step.argtypes = [ct.c_void_p, _f, ct.c_int, ct.c_float, _f, _u8, ct.c_int]
+        lib.or_step.restype = ct.c_int
+        lib.or_dump.argtypes = [ct.c_void_p, _u32, _u32, _i64]
+        lib.or_count.argtypes = [ct.c_void_p]
+        lib.or_edges.argtypes = [ct.c_void_p]
+        lib.or_last_events.argtypes = [ct.c_void_p]
+        lib.or_last_events.restype = ct.c_int64
+        lib.or_cr_expf.argtypes = [ct.c_float]; lib.or_cr_expf.restype = ct.c_float
+        lib.or_cr_logf.argtypes = [ct.c_float]; lib.or_cr_logf.restype = ct.c_float
+        lib.or_bound_expf.argtypes = [ct.c_float]; lib.or_bound_expf.restype = ct.c_float
+        lib.or_protocols.argtypes = [_f, ct.c_int]; lib.or_protocols.restype = ct.c_int
+        _libs[name] = lib
+    return _libs[name]
+
+
+def ref_lib(cr=False):
+    """The reference host executor built from its own sources, or None."""
+    name = "libns_ref_cr.so" if cr else "libns_ref.so"
+    path = HERE / "_ref" / name
+    if not path.exists():
+        return None
+    if name not in _libs:
+        lib = ct.CDLL(str(path))
+        lib.ns_create.restype = ct.c_void_p
+        lib.ns_create.argtypes = [ct.c_int] * 4 + [_f, _f, _i32]
+        lib.ns_destroy.argtypes = [ct.c_void_p]
+        lib.ns_reset.argtypes = [ct.c_void_p, ct.c_uint32]
+        lib.ns_step.argtypes = [ct.c_void_p, _f, ct.c_int, ct.c_float, _f]
+        lib.ns_step.restype = ct.c_int
+        lib.ns_error.restype = ct.c_char_p
+        lib.ns_original_indices.argtypes = [ct.c_void_p, _u32, _u32]
+        lib.ref_dump.argtypes = [ct.c_void_p, _u32, _u32, _i64]
+        lib.ref_step_raster.argtypes = [ct.c_void_p, _f, ct.c_int, ct.c_float, _f, _u8]
+        lib.ref_step_raster.restype = ct.c_int
+        _libs[name] = lib
+    return _libs[name]
+
+
+class OracleBrain:
+    """One brain in the C oracle."""
+
+    def __init__(self, neuron_rows, synapse_rows, motors, channels, max_delay=8, libm=False):
+        self.lib = oracle_lib(libm)
+        ng = np.ascontiguousarray(neuron_rows, np.float32)
+        sg = np.ascontiguousarray(synapse_rows, np.float32).reshape(-1, 11)
+        mo = np.ascontiguousarray(motors, np.int32)
+        err = ct.create_string_buffer(128)
+        self.count, self.edges, self.outputs, self.channels = len(ng), len(sg), len(mo), channels
+        sgp = sg if len(sg) else np.zeros((1, 11), np.float32)
+        self.ptr = self.lib.or_create(self.count, self.edges, channels, self.outputs, _ptr(ng, _f),
+                                      _ptr(sgp, _f), _ptr(mo, _i32), max_delay, err, 128)
+        if not self.ptr:
+            raise ValueError(err.value.decode())
+
+    def reset(self, seed):
+        self.lib.or_reset(self.ptr, ct.c_uint32(seed))
+
+    def original_indices(self, neurons, synapses):
+        n = np.ascontiguousarray(neurons, np.uint32)
+        s = np.ascontiguousarray(synapses, np.uint32) if len(synapses) else np.zeros(1, np.uint32)
+        self.lib.or_original_indices(self.ptr, _ptr(n, _u32), _ptr(s, _u32))
+
+    def step(self, inputs, ticks, gain=230.0, raster=False, stop_on_nonfinite=True):
+        x = np.ascontiguousarray(inputs, np.float32)
+        out = np.zeros(self.outputs, np.float32)
+        r = np.zeros((ticks, self.count), np.uint8) if raster else None
+        rc = self.lib.or_step(self.ptr, _ptr(x, _f), ticks, gain, _ptr(out, _f),
+                              _ptr(r, _u8) if raster else None, 1 if stop_on_nonfinite else 0)
+        return rc, out, r
+
+    def events(self):
+        return self.lib.or_last_events(self.ptr)
+
+    def dump(self):
+        nw = np.zeros((self.count, NW), np.uint32)
+        sw = np.zeros((max(self.edges, 1), SW), np.uint32)
+        t = ct.c_int64(0)
+        self.lib.or_dump(self.ptr, _ptr(nw, _u32), _ptr(sw, _u32), ct.byref(t))
+        return nw, sw[: self.edges], t.value
+
+    def close(self):
+        if self.ptr:
+            self.lib.or_destroy(self.ptr)
+            self.ptr = None
+
+    __del__ = close
+
+
+class RefBrain:
+    """One brain in the reference host executor (gym_adapter/native.cpp)."""
+
+    def __init__(self, neuron_rows, synapse_rows, motors, channels, cr=False):
+        self.lib = ref_lib(cr)
+        if self.lib is None:
+            raise FileNotFoundError("reference build absent (oracle/_ref)")
+        ng = np.ascontiguousarray(neuron_rows, np.float32)
+        sg = np.ascontiguousarray(synapse_rows, np.float32).reshape(-1, 11)
+        mo = np.ascontiguousarray(motors, np.int32)
+        self.count, self.edges, self.outputs = len(ng), len(sg), len(mo)
+        sgp = sg if len(sg) else np.zeros((1, 11), np.float32)
+        self.ptr = self.lib.ns_create(self.count, self.edges, channels, self.outputs,
+                                      _ptr(ng, _f), _ptr(sgp, _f), _ptr(mo, _i32))
+        if not self.ptr:
+            raise ValueError(self.lib.ns_error().decode())
+
+    def reset(self, seed):
+        self.lib.ns_reset(self.ptr, ct.c_uint32(seed))
+
+    def original_indices(self, neurons, synapses):
+        n = np.ascontiguousarray(neurons, np.uint32)
+        s = np.ascontiguousarray(synapses, np.uint32) if len(synapses) else np.zeros(1, np.uint32)
+        self.lib.ns_original_indices(self.ptr, _ptr(n, _u32), _ptr(s, _u32))
+
+    def step(self, inputs, ticks, gain=230.0, raster=False):
+        x = np.ascontiguousarray(inputs, np.float32)
+        out = np.zeros(self.outputs, np.float32)
+        if raster:
+            r = np.zeros((ticks, self.count), np.uint8)
+            rc = self.lib.ref_step_raster(self.ptr, _ptr(x, _f), ticks, gain, _ptr(out, _f), _ptr(r, _u8))
+            return rc, out, r
+        rc = self.lib.ns_step(self.ptr, _ptr(x, _f), ticks, gain, _ptr(out, _f))
+        return rc, out, None
+
+    def dump(self):
+        nw = np.zeros((self.count, NW), np.uint32)
+        sw = np.zeros((max(self.edges, 1), SW), np.uint32)
+        t = ct.c_int64(0)
+        self.lib.ref_dump(self.ptr, _ptr(nw, _u32), _ptr(sw, _u32), ct.byref(t))
+        return nw, sw[: self.edges], t.value
+
+    def close(self):
+        if self.ptr:
+            self.lib.ns_destroy(self.ptr)
+            self.ptr = None
+
+    __del__ = close
+
+
+def protocols():
+    out = np.zeros(40, np.float32)
+    n = oracle_lib().or_protocols(_ptr(out, _f), 40)
+    return out[:n]
