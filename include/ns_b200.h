@@ -1,0 +1,108 @@
+/* C ABI of the B200 neural-tick library (libns_b200.so).
+ *
+ * Drop-in boundary. The first ten entry points keep the signatures, argument
+ * meaning, validation messages and return conventions of the reference's Gym
+ * bridge (mixic/neural-selection gym_adapter/native.cpp and gym_adapter/gpu.cu):
+ * gym_adapter/adapter.py and gym_adapter/gpu.py bind them with ctypes
+ * unchanged. All computation runs on the GPU (sm_100a). Exceptions never cross
+ * the ABI: failures return -1 or NULL and ns_error() returns the thread-local
+ * message. Brain handles share the reference's host layout, so ns_gpu_create
+ * accepts handles made by either library's ns_create.
+ *
+ * Entry points prefixed nsb_ are this library's extensions.
+ */
+#ifndef NS_B200_H
+#define NS_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Replaces ns_error, gym_adapter/native.cpp:120. */
+const char *ns_error(void);
+
+/* Replaces ns_create, gym_adapter/native.cpp:121-157. ng: count x 10 rows
+ * [profile 0-6, channel -1..channels-1, active, inhibitory, modulator 0-3,
+ * capacitance x, leak x, threshold mV, receptor Hz gain, receptor event nS];
+ * sg: edges x 11 rows [pre, post, weight nS, active, delay 1-8, branch 0-3,
+ * U, recovery ms, facilitation ms, plasticity 0-5, receptor mask 0-7];
+ * motors: outputs neuron indices. NULL on invalid input. */
+void *ns_create(int count, int edges, int channels, int outputs, const float *ng, const float *sg,
+                const int *motors);
+
+/* Replaces ns_original_indices, gym_adapter/native.cpp:158-162 (reset seeds
+ * use original indices after graph compilation). */
+void ns_original_indices(void *brain, const uint32_t *neurons, const uint32_t *synapses);
+
+/* Replaces ns_destroy, gym_adapter/native.cpp:163. */
+void ns_destroy(void *brain);
+
+/* Replaces ns_reset, gym_adapter/native.cpp:164-169: state seeded from
+ * seed + index*7919 (neurons) and seed + index*104729 (synapses). */
+void ns_reset(void *brain, uint32_t seed);
+
+/* Replaces ns_step, gym_adapter/native.cpp:170-183: `ticks` 1 ms ticks (1..10000),
+ * input[channels] in [0,1], output[outputs] = motor spikes during the call.
+ * 0, or -1 ("Nonfinite neural state", invalid interval or observation). */
+int ns_step(void *brain, const float *input, int ticks, float input_gain, float *output);
+
+/* Replaces ns_gpu_create, gym_adapter/gpu.cu:273-315: a device batch built from
+ * `count` brain handles with equal channels/outputs. Honours GYM_CUDA_THREADS
+ * validation (32/64/128/256). */
+void *ns_gpu_create(void **brains, int count);
+
+/* Replaces ns_gpu_destroy, gym_adapter/gpu.cu:316. */
+void ns_gpu_destroy(void *batch);
+
+/* Replaces ns_gpu_reset, gym_adapter/gpu.cu:317-319: reset brains with mask[i]. */
+int ns_gpu_reset(void *batch, const uint8_t *mask, const uint32_t *seeds);
+
+/* Replaces ns_gpu_step, gym_adapter/gpu.cu:320-329: synchronous; input
+ * count x channels, output count x outputs, status[i] = -1 on a non-finite
+ * voltage (-2: tick counter past 2^31). */
+int ns_gpu_step(void *batch, const float *input, const uint8_t *mask, int ticks, float gain, float *output,
+                int *status);
+
+/* ---- extensions (no reference counterpart) ---------------------------------- */
+
+/* ns_create with a delay ring of max_delay ticks (1..31). */
+void *nsb_create_ext(int count, int edges, int channels, int outputs, const float *ng, const float *sg,
+                     const int *motors, int max_delay);
+/* ns_gpu_create with an explicit delay ring floor and CTA size (128 or 256; 0 = default). */
+void *nsb_gpu_create_ext(void **brains, int count, int max_delay, int block);
+/* Device batch straight from concatenated Gym-ABI rows: brain i owns neuron rows
+ * [neuron_offsets[i], neuron_offsets[i+1]) and synapse rows likewise (pre/post
+ * brain-local); motors is brains x outputs. */
+void *nsb_gpu_create_rows(int brains, const int64_t *neuron_offsets, const int64_t *synapse_offsets,
+                          const float *ng, const float *sg, const int *motors, int channels, int outputs,
+                          int max_delay, int block);
+/* Asynchronous step on device memory (cudaStream_t passed as void*). */
+int nsb_gpu_step_device(void *batch, const float *d_input, const uint8_t *d_mask, int ticks, float gain,
+                        float *d_output, int *d_status, void *stream);
+/* Step on the batch's own device buffers, replayed from a captured CUDA graph. */
+int nsb_gpu_step_graph(void *batch, int ticks, float gain, void *stream);
+/* Copy host observations (count x channels) and/or mask (count) into the
+ * batch's own device buffers; either pointer may be NULL. */
+int nsb_gpu_upload(void *batch, const float *input, const uint8_t *mask);
+/* Copy the batch's device outputs and status to host memory (synchronises). */
+int nsb_gpu_download(void *batch, float *output, int *status);
+/* Device pointer of the batch's buffer: 0 input, 1 mask, 2 output, 3 status. */
+void *nsb_gpu_buffer(void *batch, int which);
+/* Canonical state of one brain: 32 words per neuron, 20 per synapse, in the
+ * brain's original order; tick after the last step. */
+int nsb_gpu_dump(void *batch, int brain, uint32_t *neuron_words, uint32_t *synapse_words, int64_t *tick);
+/* Same for a single ns_create brain. */
+int nsb_dump(void *brain, uint32_t *neuron_words, uint32_t *synapse_words, int64_t *tick);
+/* Load one batch brain's state from a brain handle's host records. */
+int nsb_gpu_load_state(void *batch, int brain, void *brain_handle);
+/* Layout facts: brains, units, big_units, neurons, synapses, heavy, max_unit_neurons,
+ * grid, block, smem_bytes, ctas_per_sm. Returns the count written (11). */
+int nsb_gpu_stats(void *batch, int *out);
+/* Synaptic arrivals counted on the device since the previous call. */
+long long nsb_gpu_take_events(void *batch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,2 +1,10 @@
-"""B200-native neural tick for Neural Selection (placeholder, filled below)."""
+"""B200-native neural tick of Neural Selection.
+
+libns_b200.so (csrc/, built by build.py) runs the reference's neural tick —
+AdEx/conductance neurons, delayed stochastic spike delivery with short-term
+plasticity, STDP and modulatory eligibility — as one persistent CUDA kernel per
+call on sm_100a, behind the reference's own C ABI (include/ns_b200.h).
+`native` binds that ABI; `workloads` builds seeded synthetic populations.
+"""
 from . import workloads  # noqa: F401
+from .native import Brain, GpuBatch, library  # noqa: F401

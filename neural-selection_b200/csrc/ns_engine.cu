@@ -1,0 +1,1020 @@
+// B200 neural-tick engine: planner, persistent fused tick kernel, reset and
+// state readback.
+//
+// Work decomposition. Synapses are partitioned by their POSTsynaptic neuron:
+// the thread that owns neuron j also owns every synapse onto j, stored
+// contiguously in ascending original edge order. Within one tick that thread
+// (1) delivers its incoming spikes — arrival test against a shared-memory
+// ring of spike bitmasks, stochastic release, and accumulation per dendritic
+// branch in ascending edge order, the reference's summation order
+// (gym_adapter/core.cuh:37-47, gym_adapter/gpu.cu:41-47); (2) integrates the
+// neuron; (3) publishes its spike with a warp ballot into the ring; and
+// (4) applies plasticity to its incoming synapses. Every input of (1), (2),
+// (4) is either its own state or a spike bit from an earlier tick, so one
+// __syncthreads per tick is the only synchronisation and no float atomics
+// exist. All ticks of a call run inside one launch: the CTA keeps neuron state
+// in registers and the spike ring in shared memory for the whole call.
+//
+// Work units. Brains of at most `block` neurons are packed (best-fit
+// decreasing) into units of at most `block` neurons, one neuron per thread.
+// A larger brain is a unit of its own; its threads step several neurons each,
+// keeping neuron state in global memory (L2-resident during the call). A
+// persistent grid pulls units from an atomic queue, largest first.
+//
+// Plasticity is applied lazily and exactly: a synapse is updated at each tick
+// where it has an arrival, a postsynaptic spike or a relevant modulator event;
+// the quiet ticks in between are replayed operation by operation
+// (plasticity_quiet), and a final pass at the end of the call brings every
+// plastic synapse to the last tick. The results equal tick-by-tick updating.
+#include "ns_engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <stdexcept>
+
+#include "ns_crmath.h"
+#include "ns_layout.h"
+#include "ns_physio.cuh"
+
+namespace nsb {
+
+#define NSB_CHECK(x)                                                                        \
+    do {                                                                                    \
+        cudaError_t e_ = (x);                                                               \
+        if (e_ != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+constexpr int kMetaCap = 6144;       // synapse meta words cached in shared memory per unit
+constexpr int kMaxUnitBrains = 128;  // brains packed into one small unit
+constexpr int kMaxBrainNeurons = 16384;
+
+struct Pools {
+    const float4 *ngene;     // N x 4
+    const uint32_t *nflags;  // N
+    const int *nsens;        // N
+    const int *nxidx;        // N (index into heavy arrays, -1)
+    const float *xgene;      // H x 16
+    float *xstate;           // H x 16
+    uint32_t *nstate;        // N x 16
+    const int *inptr;        // N + 1
+    const uint32_t *smeta;   // E
+    const uint32_t *sgene;   // E x 8
+    uint32_t *sstate;        // E x 16
+    uint8_t *sarrived;       // E
+    int16_t *slastp;         // E (-1 between calls)
+    const int *bn0, *be0;
+    int64_t *btick;
+    const int *bmotor;       // B x outputs, global neuron index
+    const int4 *units;       // {n0, nn, e0, ne}
+    const int2 *unitb;       // {first entry in ubrain, nb}
+    const int *ubrain;       // unit brain lists (caller brain indices), pool order
+    int n_units, channels, outputs, hw;
+    int *queue;
+    unsigned long long *events;
+};
+
+__device__ __forceinline__ uint32_t rotl32(uint32_t x, uint32_t r) { return __funnelshift_l(x, x, r); }
+__device__ __forceinline__ uint32_t rotr32(uint32_t x, uint32_t r) { return __funnelshift_r(x, x, r); }
+
+// Arrival of synapse with meta m at local tick t (gym_adapter/core.cuh:40).
+__device__ __forceinline__ bool arrives(uint32_t m, int t, int64_t tick0, const uint32_t *hist, int hw) {
+    if (!(m & M_LIVE)) return false;
+    const int d = (int)((m >> M_DELAY_SHIFT) & 31u);
+    if (tick0 + t < d) return false;
+    const uint32_t pre = m & M_PRE_MASK;
+    return (hist[((t - d) & 31) * hw + (pre >> 5)] >> (pre & 31u)) & 1u;
+}
+
+__device__ __forceinline__ void load_plast(const uint32_t *z, SynPlast &p) {
+    p.w = __uint_as_float(z[Z_W]); p.pre_tr = __uint_as_float(z[Z_PRETR]); p.post_tr = __uint_as_float(z[Z_POSTTR]);
+    p.eltp = __uint_as_float(z[Z_ELTP]); p.eltd = __uint_as_float(z[Z_ELTD]); p.da_age = __uint_as_float(z[Z_DAAGE]);
+    p.spine = __uint_as_float(z[Z_SPINE]); p.st_age = __uint_as_float(z[Z_STAGE]);
+    p.pre_age = __uint_as_float(z[Z_PREAGE]); p.post_age = __uint_as_float(z[Z_POSTAGE]);
+}
+__device__ __forceinline__ void store_plast(uint32_t *z, const SynPlast &p) {
+    z[Z_W] = __float_as_uint(p.w); z[Z_PRETR] = __float_as_uint(p.pre_tr); z[Z_POSTTR] = __float_as_uint(p.post_tr);
+    z[Z_ELTP] = __float_as_uint(p.eltp); z[Z_ELTD] = __float_as_uint(p.eltd); z[Z_DAAGE] = __float_as_uint(p.da_age);
+    z[Z_SPINE] = __float_as_uint(p.spine); z[Z_STAGE] = __float_as_uint(p.st_age);
+    z[Z_PREAGE] = __float_as_uint(p.pre_age); z[Z_POSTAGE] = __float_as_uint(p.post_age);
+}
+
+__device__ __forceinline__ void load_neuron(const uint32_t *r, NeuronRegs &s, float &log_ampa, uint32_t &hist) {
+    const uint4 *q = reinterpret_cast<const uint4 *>(r);
+    uint4 a = q[0], b = q[1], c = q[2], d = q[3];
+    s.v = __uint_as_float(a.x); s.w = __uint_as_float(a.y); s.adp = __uint_as_float(a.z); s.inh = __uint_as_float(a.w);
+    s.depol = __uint_as_float(b.x); log_ampa = __uint_as_float(b.y); s.rec_ns = __uint_as_float(b.z); s.rng = b.w;
+    s.d0 = __uint_as_float(c.x); s.d1 = __uint_as_float(c.y); s.d2 = __uint_as_float(c.z); s.d3 = __uint_as_float(c.w);
+    s.total = (int)d.x; s.spike = d.y; hist = d.z;
+}
+__device__ __forceinline__ void store_neuron(uint32_t *r, const NeuronRegs &s, float log_ampa, uint32_t hist,
+                                             uint32_t pad) {
+    uint4 *q = reinterpret_cast<uint4 *>(r);
+    q[0] = make_uint4(__float_as_uint(s.v), __float_as_uint(s.w), __float_as_uint(s.adp), __float_as_uint(s.inh));
+    q[1] = make_uint4(__float_as_uint(s.depol), __float_as_uint(log_ampa), __float_as_uint(s.rec_ns), s.rng);
+    q[2] = make_uint4(__float_as_uint(s.d0), __float_as_uint(s.d1), __float_as_uint(s.d2), __float_as_uint(s.d3));
+    q[3] = make_uint4((uint32_t)s.total, s.spike, hist, pad);
+}
+
+__device__ __forceinline__ void load_gene(const float4 *g4, float (&g)[16]) {
+    float4 a = g4[0], b = g4[1], c = g4[2], d = g4[3];
+    g[0] = a.x; g[1] = a.y; g[2] = a.z; g[3] = a.w; g[4] = b.x; g[5] = b.y; g[6] = b.z; g[7] = b.w;
+    g[8] = c.x; g[9] = c.y; g[10] = c.z; g[11] = c.w; g[12] = d.x; g[13] = d.y; g[14] = d.z; g[15] = d.w;
+}
+
+// Delivery + integration of one neuron for local tick t. Returns the
+// postsynaptic modulator bits and the number of arrivals.
+__device__ __forceinline__ void deliver_and_integrate(
+    const Pools &P, const float (&g)[16], uint32_t flags, int ib, int ie, int e0, const uint32_t *meta,
+    const uint32_t *hist, int t, int64_t tick0, float ampa, float level, float gain, NeuronRegs &s, int xidx,
+    int *status, const PhysConst &K, const double *tab, uint32_t &mod_out, int &narr_out) {
+    float e0s = 0.0f, e1s = 0.0f, e2s = 0.0f, e3s = 0.0f, inh = 0.0f;
+    uint32_t mod = 0;
+    int narr = 0;
+    const int64_t tick = tick0 + t;
+    for (int e = ib; e < ie; ++e) {
+        const uint32_t m = meta[e - e0];
+        if (!arrives(m, t, tick0, hist, P.hw)) continue;
+        ++narr;
+        const uint32_t kind = (m >> M_KIND_SHIFT) & 3u;
+        uint32_t *z = P.sstate + (size_t)e * Z_WORDS;
+        if (kind == KIND_INH) {             // inhibitory source: weight, no release
+            inh += __uint_as_float(z[Z_W]);
+            continue;
+        }
+        const float *y = reinterpret_cast<const float *>(P.sgene + (size_t)e * Y_WORDS);
+        SynRelease r;
+        r.w = __uint_as_float(z[Z_W]); r.ru = __uint_as_float(z[Z_RU]); r.slow = __uint_as_float(z[Z_SLOW]);
+        r.ready = ((uint64_t)z[Z_READYHI] << 32) | z[Z_READYLO];
+        r.rng = z[Z_RNG]; r.last = (int)z[Z_LAST];
+        const float rel = release(y, r, tick, tab);
+        z[Z_RU] = __float_as_uint(r.ru); z[Z_SLOW] = __float_as_uint(r.slow);
+        z[Z_READYLO] = (uint32_t)r.ready; z[Z_READYHI] = (uint32_t)(r.ready >> 32);
+        z[Z_RNG] = r.rng; z[Z_LAST] = (uint32_t)r.last;
+        if (kind == KIND_MOD) {
+            if (rel > 0) mod |= 1u << ((m >> M_MODID_SHIFT) & 3u);
+        } else {
+            const float c = rel * ampa;
+            switch ((m >> M_BRANCH_SHIFT) & 3u) {
+            case 0: e0s += c; break;
+            case 1: e1s += c; break;
+            case 2: e2s += c; break;
+            default: e3s += c; break;
+            }
+        }
+    }
+    const uint32_t type = flags & NF_TYPE_MASK;
+    float cur = 0.0f;
+    if (flags & NF_HAS_INPUT) cur = type == 5 ? receptor_drive(g, flags, s, level) : gain * level;
+    if (type == 2 || type == 3 || type == 6) {
+        heavy_tick(g, type, P.xgene + (size_t)xidx * 16, P.xstate + (size_t)xidx * 16, s, cur, e0s, e1s, e2s, e3s,
+                   inh, K, tab);
+    } else {
+        adex_tick(g, type, flags, s, cur, e0s, e1s, e2s, e3s, inh, K, tab);
+    }
+    if (!isfinite(s.v)) *status = -1;
+    mod_out = mod;
+    narr_out = narr;
+}
+
+// Plasticity for the incoming synapses of one neuron at local tick t.
+__device__ __forceinline__ void plasticity_events(const Pools &P, int ib, int ie, int e0, const uint32_t *meta,
+                                                  const uint32_t *hist, int t, int64_t tick0, bool post,
+                                                  uint32_t mod, float depol, const PhysConst &K,
+                                                  const double *tab) {
+    for (int e = ib; e < ie; ++e) {
+        const uint32_t m = meta[e - e0];
+        if (!(m & M_PLASTIC)) continue;
+        const bool arr = arrives(m, t, tick0, hist, P.hw);
+        const uint32_t prof = m >> M_PROF_SHIFT;
+        uint32_t receptors = 0;
+        if (mod) receptors = (P.sgene[(size_t)e * Y_WORDS + Y_INFO] >> 8) & 0xffu;
+        if (!arr && !post && !mod_relevant(prof, receptors, mod)) continue;
+        const float w0 = __uint_as_float(P.sgene[(size_t)e * Y_WORDS + Y_W0]);
+        uint32_t *z = P.sstate + (size_t)e * Z_WORDS;
+        SynPlast p;
+        load_plast(z, p);
+        const int last = P.slastp[e];
+        plasticity_quiet(prof, w0, p, t - last - 1, K);
+        plasticity_tick(prof, receptors, w0, p, arr, post, depol, mod, K, tab);
+        store_plast(z, p);
+        P.slastp[e] = (int16_t)t;
+    }
+}
+
+__device__ __forceinline__ int find_brain(const int *starts, int nb, int local) {
+    int lo = 0, hi = nb - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (starts[mid] <= local) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+extern __shared__ __align__(16) unsigned char g_smem[];
+
+__global__ void __launch_bounds__(256) tick_kernel(Pools P, const float *__restrict__ input,
+                                                   const uint8_t *__restrict__ mask, float *__restrict__ output,
+                                                   int *__restrict__ status, int ticks, float gain, PhysConst K) {
+    double *tab = reinterpret_cast<double *>(g_smem);                    // 128 doubles
+    int *s_meta_raw = reinterpret_cast<int *>(g_smem + 1024);
+    uint32_t *s_meta = reinterpret_cast<uint32_t *>(s_meta_raw);          // kMetaCap
+    uint32_t *hist = s_meta + kMetaCap;                                   // 32 * hw
+    int *cnt = reinterpret_cast<int *>(hist + 32 * P.hw);                // 32 * hw (spike counts)
+    int *s_bn0 = cnt + 32 * P.hw;                                         // kMaxUnitBrains
+    int *s_be0 = s_bn0 + kMaxUnitBrains;
+    int64_t *s_tick = reinterpret_cast<int64_t *>(s_be0 + kMaxUnitBrains);
+    int *s_mask = reinterpret_cast<int *>(s_tick + kMaxUnitBrains);
+    int *s_bid = s_mask + kMaxUnitBrains;                                 // caller brain index
+    __shared__ int s_unit;
+    __shared__ unsigned long long s_events;
+
+    const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarp = bs >> 5;
+    {
+        const double *src = nsx::exp2_table();
+        for (int i = tid; i < 128; i += bs) tab[i] = src[i];
+    }
+    for (;;) {
+        if (tid == 0) { s_unit = atomicAdd(P.queue, 1); s_events = 0; }
+        __syncthreads();
+        const int u = s_unit;
+        if (u >= P.n_units) break;
+        const int4 U = P.units[u];
+        const int2 UB = P.unitb[u];
+        const int n0 = U.x, nn = U.y, e0 = U.z, ne = U.w, b0 = UB.x, nb = UB.y;
+        for (int i = tid; i < nb; i += bs) {
+            const int b = P.ubrain[b0 + i];
+            s_bid[i] = b;
+            s_bn0[i] = P.bn0[b] - n0;
+            s_be0[i] = P.be0[b] - e0;
+            const int64_t t0 = P.btick[b];
+            s_tick[i] = t0;
+            // last-arrival ticks are stored as int32: refuse to step past 2^31
+            const bool in_range = t0 + (int64_t)ticks < 2147483647ll;
+            s_mask[i] = mask[b] && in_range;
+            status[b] = in_range ? 0 : -2;
+        }
+        const bool meta_smem = ne <= kMetaCap;
+        if (meta_smem)
+            for (int k = tid; k < ne; k += bs) s_meta[k] = P.smeta[e0 + k];
+        const uint32_t *meta = meta_smem ? s_meta : P.smeta + e0;
+        __syncthreads();
+        const int slots = (nn + bs - 1) / bs;
+        int my_events = 0;
+
+        if (slots == 1) {
+            // ---- register path: one neuron per thread, state in registers --------
+            const bool has = tid < nn;
+            const int bi = has ? find_brain(s_bn0, nb, tid) : 0;
+            const bool run = has && s_mask[bi] != 0;
+            const int64_t tick0 = s_tick[bi];
+            const int n = n0 + tid;
+            float g[16];
+            uint32_t flags = 0;
+            NeuronRegs s = {};
+            float log_ampa = 0.0f, ampa = 1.0f, level = 0.0f;
+            uint32_t h0 = 0;
+            int ib = 0, ie = 0, xidx = -1, count = 0;
+            if (run) {
+                load_gene(P.ngene + (size_t)n * 4, g);
+                flags = P.nflags[n];
+                load_neuron(P.nstate + (size_t)n * S_WORDS, s, log_ampa, h0);
+                ampa = crexp(log_ampa, tab);
+                if (flags & NF_HAS_INPUT) level = input[(size_t)s_bid[bi] * P.channels + P.nsens[n]];
+                ib = P.inptr[n]; ie = P.inptr[n + 1];
+                xidx = P.nxidx[n];
+            }
+            const uint32_t rot = run ? rotr32(h0, (uint32_t)(tick0 & 31)) : 0u;
+            for (int sl = 0; sl < 32; ++sl) {
+                const uint32_t w = __ballot_sync(0xffffffffu, (rot >> sl) & 1u);
+                if (lane == 0 && warp < P.hw) hist[sl * P.hw + warp] = w;
+            }
+            __syncthreads();
+            int *status_ptr = status + s_bid[bi];
+            for (int t = 0; t < ticks; ++t) {
+                uint32_t mod = 0;
+                int narr = 0;
+                if (run) {
+                    if (flags & NF_ACTIVE) {
+                        deliver_and_integrate(P, g, flags, ib, ie, e0, meta, hist, t, tick0, ampa, level, gain, s, xidx,
+                                              status_ptr, K, tab, mod, narr);
+                    } else {
+                        s.spike = 0;
+                    }
+                }
+                const uint32_t w = __ballot_sync(0xffffffffu, run && s.spike);
+                if (lane == 0 && warp < P.hw) hist[(t & 31) * P.hw + warp] = w;
+                if (run && (s.spike || mod || narr))
+                    plasticity_events(P, ib, ie, e0, meta, hist, t, tick0, s.spike != 0, mod, s.depol, K, tab);
+                count += run ? (int)s.spike : 0;
+                my_events += narr;
+                __syncthreads();
+            }
+            if (run) {
+                if (flags & NF_ACTIVE) {
+                    const int64_t t1 = tick0 + ticks;
+                    log_ampa = homeostasis(flags & NF_TYPE_MASK, log_ampa, (float)ticks,
+                                           (float)s.total * 1000.0f / (float)(ticks > t1 ? (int64_t)ticks : t1), K);
+                }
+                uint32_t L = 0;
+                for (int sl = 0; sl < 32; ++sl) L |= ((hist[sl * P.hw + warp] >> lane) & 1u) << sl;
+                store_neuron(P.nstate + (size_t)n * S_WORDS, s, log_ampa, rotl32(L, (uint32_t)(tick0 & 31)), 0u);
+            }
+            if (has) cnt[tid] = count;
+        } else {
+            // ---- global path: one brain, several neurons per thread, state in L2 ----
+            const bool run = s_mask[0] != 0;
+            const int64_t tick0 = s_tick[0];
+            int *status_ptr = status + s_bid[0];
+            for (int sl0 = 0; sl0 < slots; ++sl0) {
+                const int j = sl0 * bs + tid;
+                const bool has = j < nn;
+                uint32_t h0 = 0;
+                if (has && run) {
+                    uint32_t *r = P.nstate + (size_t)(n0 + j) * S_WORDS;
+                    h0 = r[S_HIST];
+                    // ampa for the call kept in the record's spare word
+                    r[S_PAD] = __float_as_uint(crexp(__uint_as_float(r[S_LOGAMPA]), tab));
+                }
+                const uint32_t rot = (has && run) ? rotr32(h0, (uint32_t)(tick0 & 31)) : 0u;
+                for (int sl = 0; sl < 32; ++sl) {
+                    const uint32_t w = __ballot_sync(0xffffffffu, (rot >> sl) & 1u);
+                    if (lane == 0) hist[sl * P.hw + sl0 * nwarp + warp] = w;
+                }
+                if (has) cnt[j] = 0;
+            }
+            __syncthreads();
+            for (int t = 0; t < ticks; ++t) {
+                for (int sl0 = 0; sl0 < slots; ++sl0) {
+                    const int j = sl0 * bs + tid;
+                    const bool has = j < nn && run;
+                    uint32_t spike = 0;
+                    if (has) {
+                        const int n = n0 + j;
+                        uint32_t *r = P.nstate + (size_t)n * S_WORDS;
+                        NeuronRegs s;
+                        float log_ampa;
+                        uint32_t hw0;
+                        load_neuron(r, s, log_ampa, hw0);
+                        const float ampa = __uint_as_float(r[S_PAD]);
+                        const uint32_t flags = P.nflags[n];
+                        uint32_t mod = 0;
+                        int narr = 0;
+                        const int ib = P.inptr[n], ie = P.inptr[n + 1];
+                        if (flags & NF_ACTIVE) {
+                            float g[16];
+                            load_gene(P.ngene + (size_t)n * 4, g);
+                            const float level = (flags & NF_HAS_INPUT) ? input[(size_t)s_bid[0] * P.channels + P.nsens[n]] : 0.0f;
+                            deliver_and_integrate(P, g, flags, ib, ie, e0, meta, hist, t, tick0, ampa, level, gain, s,
+                                                  P.nxidx[n], status_ptr, K, tab, mod, narr);
+                        } else {
+                            s.spike = 0;
+                        }
+                        store_neuron(r, s, log_ampa, hw0, __float_as_uint(ampa));
+                        spike = s.spike;
+                        if (spike || mod || narr)
+                            plasticity_events(P, ib, ie, e0, meta, hist, t, tick0, spike != 0, mod, s.depol, K, tab);
+                        cnt[j] += (int)spike;
+                        my_events += narr;
+                    }
+                    const uint32_t w = __ballot_sync(0xffffffffu, spike);
+                    if (lane == 0) hist[(t & 31) * P.hw + sl0 * nwarp + warp] = w;
+                }
+                __syncthreads();
+            }
+            for (int sl0 = 0; sl0 < slots; ++sl0) {
+                const int j = sl0 * bs + tid;
+                if (j < nn && run) {
+                    const int n = n0 + j;
+                    uint32_t *r = P.nstate + (size_t)n * S_WORDS;
+                    const uint32_t flags = P.nflags[n];
+                    float la = __uint_as_float(r[S_LOGAMPA]);
+                    if (flags & NF_ACTIVE) {
+                        const int total = (int)r[S_TOTAL];
+                        const int64_t t1 = tick0 + ticks;
+                        la = homeostasis(flags & NF_TYPE_MASK, la, (float)ticks,
+                                         (float)total * 1000.0f / (float)(ticks > t1 ? (int64_t)ticks : t1), K);
+                    }
+                    uint32_t L = 0;
+                    const int word = sl0 * nwarp + warp;
+                    for (int sl = 0; sl < 32; ++sl) L |= ((hist[sl * P.hw + word] >> lane) & 1u) << sl;
+                    r[S_LOGAMPA] = __float_as_uint(la);
+                    r[S_HIST] = rotl32(L, (uint32_t)(tick0 & 31));
+                    r[S_PAD] = 0u;
+                }
+            }
+        }
+        __syncthreads();
+        // ---- end of call: finish plasticity, record last-tick arrivals ---------------
+        for (int k = tid; k < ne; k += bs) {
+            const int bi = nb == 1 ? 0 : find_brain(s_be0, nb, k);
+            if (!s_mask[bi]) continue;
+            const int e = e0 + k;
+            const uint32_t m = meta[k];
+            const int64_t tick0 = s_tick[bi];
+            P.sarrived[e] = arrives(m, ticks - 1, tick0, hist, P.hw) ? 1 : 0;
+            if (m & M_PLASTIC) {
+                const int last = P.slastp[e];
+                const int q = ticks - 1 - last;
+                if (q > 0) {
+                    uint32_t *z = P.sstate + (size_t)e * Z_WORDS;
+                    SynPlast p;
+                    load_plast(z, p);
+                    plasticity_quiet(m >> M_PROF_SHIFT, __uint_as_float(P.sgene[(size_t)e * Y_WORDS + Y_W0]), p, q, K);
+                    store_plast(z, p);
+                }
+                if (last >= 0) P.slastp[e] = -1;
+            }
+        }
+        // ---- motor outputs (spikes per call) and tick counters --------------------
+        for (int i = tid; i < nb * P.outputs; i += bs) {
+            const int bi = i / P.outputs, b = s_bid[bi];
+            output[(size_t)b * P.outputs + (i - bi * P.outputs)] =
+                s_mask[bi] ? (float)cnt[P.bmotor[(size_t)b * P.outputs + (i - bi * P.outputs)] - n0] : 0.0f;
+        }
+        for (int i = tid; i < nb; i += bs)
+            if (s_mask[i]) P.btick[s_bid[i]] = s_tick[i] + ticks;
+        if (P.events) {
+            unsigned long long v = (unsigned long long)my_events;
+            for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (lane == 0 && v) atomicAdd(&s_events, v);
+            __syncthreads();
+            if (tid == 0 && s_events) atomicAdd(P.events, s_events);
+        }
+        __syncthreads();
+    }
+}
+
+// ---- reset (gym_adapter/gpu.cu:18-23 with physiology.cuh:179-202, 393-404) --------
+__device__ __forceinline__ uint32_t seed_hash(uint32_t seed) {
+    uint32_t x = seed ? seed : 1u;
+    x ^= x >> 16; x *= 0x7feb352du;
+    x ^= x >> 15; x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+__global__ void reset_neurons(Pools P, const int *nbrain, const uint32_t *norig, const uint8_t *mask,
+                              const uint32_t *seeds, int n_neurons) {
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_neurons; n += gridDim.x * blockDim.x) {
+        const int b = nbrain[n];
+        if (!mask[b]) continue;
+        const uint32_t flags = P.nflags[n];
+        const uint32_t type = flags & NF_TYPE_MASK;
+        const float el = P.ngene[(size_t)n * 4].z;
+        const uint32_t x = seed_hash(seeds[b] + norig[n] * 7919u);
+        uint32_t *r = P.nstate + (size_t)n * S_WORDS;
+        for (int k = 0; k < S_WORDS; ++k) r[k] = 0u;
+        float v = el;
+        const int xi = P.nxidx[n];
+        if (xi >= 0) {
+            float *xs = P.xstate + (size_t)xi * 16;
+            for (int k = 0; k < 16; ++k) xs[k] = 0.0f;
+            if (type == 2) {
+                const float init[16] = {-56, 0, .2f, 0, 1, 0, 0, 1, 0, 0, 1, 1, 0, .04f, .01f, -56};
+                for (int k = 0; k < 16; ++k) xs[k] = init[k];
+                v = xs[15] - 9.342518882f;
+            } else if (type == 3) {
+                xs[0] = -50.0f; xs[1] = .05f;
+                for (int k = 0; k < 4; ++k) xs[9 + k] = 1.0f;
+                v = xs[0];
+            } else if (type == 6) {
+                xs[0] = el;
+                xs[1] = P.ngene[(size_t)n * 4].w;   // threshold
+            }
+        }
+        r[S_V] = __float_as_uint(v);
+        r[S_RECRNG] = x ? x : 1u;
+    }
+}
+
+__global__ void reset_synapses(Pools P, const int *sbrain, const uint32_t *sorig, const uint8_t *mask,
+                               const uint32_t *seeds, int n_synapses) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_synapses; e += gridDim.x * blockDim.x) {
+        const int b = sbrain[e];
+        if (!mask[b]) continue;
+        uint32_t x = seed_hash(seeds[b] + sorig[e] * 104729u);
+        if (!x) x = 1u;
+        const uint32_t *y = P.sgene + (size_t)e * Y_WORDS;
+        const int n = (int)(y[Y_INFO] & 0xffu);
+        const uint64_t ready = n == 64 ? ~0ull : ((1ull << n) - 1ull);
+        uint32_t *z = P.sstate + (size_t)e * Z_WORDS;
+        z[Z_W] = y[Y_W0];
+        z[Z_RU] = 0u; z[Z_PRETR] = 0u; z[Z_POSTTR] = 0u; z[Z_ELTP] = 0u; z[Z_ELTD] = 0u;
+        z[Z_DAAGE] = __float_as_uint(-1.0f); z[Z_SPINE] = __float_as_uint(1.0f); z[Z_STAGE] = __float_as_uint(-1.0f);
+        z[Z_PREAGE] = __float_as_uint(1000000.0f); z[Z_POSTAGE] = __float_as_uint(1000000.0f);
+        z[Z_SLOW] = __float_as_uint(1.0f);
+        z[Z_READYLO] = (uint32_t)ready; z[Z_READYHI] = (uint32_t)(ready >> 32);
+        z[Z_RNG] = x; z[Z_LAST] = (uint32_t)(-1000000);
+        P.sarrived[e] = 0;
+    }
+}
+
+__global__ void reset_ticks(int64_t *btick, const uint8_t *mask, int n) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < n && mask[b]) btick[b] = 0;
+}
+
+// ---- host side ------------------------------------------------------------------
+static PhysConst make_constants() {
+    PhysConst K;
+    K.exc_ms = nsx::expf_cr(-1.0f / 3.0f);
+    K.inh_ms = nsx::expf_cr(-1.0f / 10.0f);
+    K.exc_sub = nsx::expf_cr(-0.25f / 3.0f);
+    K.inh_sub = nsx::expf_cr(-0.25f / 10.0f);
+    K.ltp = nsx::expf_cr(-1.0f / 17.0f);
+    K.ltd = nsx::expf_cr(-1.0f / 34.0f);
+    K.ne = nsx::expf_cr(-1.0f / 7200.0f);
+    K.sht = nsx::expf_cr(-1.0f / 3600.0f);
+    K.lfs_thr = nsx::expf_cr(-1.0f / 10.0f);
+    K.lfs_open[0] = nsx::expf_cr(-1.0f / 10.0f);
+    K.lfs_open[1] = nsx::expf_cr(-1.0f / 40.0f);
+    K.lfs_open[2] = nsx::expf_cr(-1.0f / 750.0f);
+    K.prinz_ca = nsx::expf_cr(-0.025f / 200.0f);
+    K.dend_offset = 5.0f / (1.0f + nsx::expf_cr(10.0f));
+    K.log_up = nsx::logf_cr(1.92f);
+    K.log_down = nsx::logf_cr(0.70f);
+    return K;
+}
+
+template <class T> T *Engine::alloc(size_t n) {
+    T *p = nullptr;
+    if (n == 0) n = 1;
+    NSB_CHECK(cudaMalloc(reinterpret_cast<void **>(&p), n * sizeof(T)));
+    allocations_.push_back(p);
+    return p;
+}
+
+static bool excitatory_type(unsigned char t) { return t == 0 || t == 4 || t == 5; }
+
+Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, const EngineConfig &cfg) {
+    if (brains.empty()) throw std::runtime_error("Empty GPU batch");
+    if (cfg.max_delay < 1 || cfg.max_delay > kMaxDelay) throw std::runtime_error("Invalid delay ring");
+    if (cfg.block != 128 && cfg.block != 256) throw std::runtime_error("Invalid CUDA block size");
+    n_brains_ = (int)brains.size();
+    channels_ = channels; outputs_ = outputs; max_delay_ = cfg.max_delay; block_ = cfg.block;
+    count_events_ = cfg.count_events;
+    // ---- validate and size ----
+    long long nsum = 0, esum = 0;
+    for (const auto &b : brains) {
+        if (b.count < 1 || b.edges < 0) throw std::runtime_error("Invalid brain dimensions");
+        if (b.count > kMaxBrainNeurons) throw std::runtime_error("Brain exceeds 16384 neurons");
+        for (int j = 0; j < b.edges; ++j) {
+            const auto &c = b.conns[j];
+            if (c.pre < 0 || c.pre >= b.count || c.post < 0 || c.post >= b.count)
+                throw std::runtime_error("Invalid synapse gene");
+            if (c.delay > max_delay_ || c.delay < 1) throw std::runtime_error("Synapse delay exceeds the delay ring");
+        }
+        for (int j = 0; j < outputs; ++j)
+            if (b.motors[j] < 0 || b.motors[j] >= b.count) throw std::runtime_error("Invalid motor index");
+        nsum += b.count; esum += b.edges;
+    }
+    if (nsum > (1ll << 30) || esum > (1ll << 30)) throw std::runtime_error("Pool exceeds 2^30 entries");
+    n_neurons_ = (int)nsum; n_synapses_ = (int)esum;
+
+    // ---- work units: big brains alone, small ones best-fit decreasing ----
+    std::vector<int> order(n_brains_);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return brains[a].count > brains[b].count; });
+    std::vector<std::vector<int>> unit_brains;
+    std::vector<int> unit_fill;
+    std::multimap<int, int> open;   // remaining capacity -> unit
+    for (int b : order) {
+        const int n = brains[b].count;
+        if (n > block_) {
+            unit_brains.push_back({b});
+            unit_fill.push_back(n);
+            continue;
+        }
+        auto it = open.lower_bound(n);
+        if (it != open.end()) {
+            const int uidx = it->second;
+            open.erase(it);
+            unit_brains[uidx].push_back(b);
+            unit_fill[uidx] += n;
+            const int rem = block_ - unit_fill[uidx];
+            if (rem > 0 && (int)unit_brains[uidx].size() < kMaxUnitBrains) open.emplace(rem, uidx);
+        } else {
+            unit_brains.push_back({b});
+            unit_fill.push_back(n);
+            const int rem = block_ - n;
+            if (rem > 0) open.emplace(rem, (int)unit_brains.size() - 1);
+        }
+    }
+    // queue order: by neuron count descending (big units first)
+    std::vector<int> uorder(unit_brains.size());
+    std::iota(uorder.begin(), uorder.end(), 0);
+    std::stable_sort(uorder.begin(), uorder.end(), [&](int a, int b) { return unit_fill[a] > unit_fill[b]; });
+    n_units_ = (int)unit_brains.size();
+
+    // ---- pool layout ----
+    h_bn0_.assign(n_brains_, 0); h_bnn_.assign(n_brains_, 0); h_be0_.assign(n_brains_, 0); h_bne_.assign(n_brains_, 0);
+    std::vector<int4> units(n_units_);
+    std::vector<int2> unitb(n_units_);
+    std::vector<int> brain_order;   // brains in pool order
+    std::vector<int> brain_pos(n_brains_);
+    int ncur = 0, ecur = 0;
+    for (int ui = 0; ui < n_units_; ++ui) {
+        const auto &ub = unit_brains[uorder[ui]];
+        units[ui] = make_int4(ncur, 0, ecur, 0);
+        unitb[ui] = make_int2((int)brain_order.size(), (int)ub.size());
+        for (int b : ub) {
+            brain_pos[b] = (int)brain_order.size();
+            brain_order.push_back(b);
+            h_bn0_[b] = ncur; h_bnn_[b] = brains[b].count;
+            h_be0_[b] = ecur; h_bne_[b] = brains[b].edges;
+            ncur += brains[b].count; ecur += brains[b].edges;
+        }
+        units[ui].y = ncur - units[ui].x;
+        units[ui].w = ecur - units[ui].z;
+        max_unit_neurons_ = std::max(max_unit_neurons_, units[ui].y);
+        if (units[ui].y > block_) ++n_big_units_;
+        max_unit_brains_ = std::max(max_unit_brains_, (int)ub.size());
+    }
+    // Spike-ring words per tick: whole CTA-sized neuron slots (a big unit's
+    // threads write one word per warp per slot).
+    hw_ = ((std::max(max_unit_neurons_, block_) + block_ - 1) / block_) * (block_ / 32);
+
+    // ---- per-neuron and per-synapse records ----
+    std::vector<float> ngene((size_t)n_neurons_ * 16);
+    h_nflags_.assign(n_neurons_, 0);
+    std::vector<int> nsens(n_neurons_), nbrain(n_neurons_);
+    h_nxidx_.assign(n_neurons_, -1);
+    std::vector<uint32_t> norig(n_neurons_);
+    std::vector<float> xgene;
+    std::vector<int> inptr(n_neurons_ + 1, 0);
+    std::vector<uint32_t> smeta(n_synapses_), sgene((size_t)n_synapses_ * Y_WORDS), sorig(n_synapses_);
+    std::vector<int> sbrain(n_synapses_);
+    h_syn_orig_.assign(n_synapses_, 0);
+    h_syn_pool_.assign(n_synapses_, 0);
+    h_sinfo_.assign(n_synapses_, 0);
+    h_w0_.assign(n_synapses_, 0.0f);
+    for (int ui = 0; ui < n_units_; ++ui) {
+        const int un0 = units[ui].x;
+        for (int k = 0; k < unitb[ui].y; ++k) {
+            const int b = brain_order[unitb[ui].x + k];
+            const BrainSpec &B = brains[b];
+            const int bn0 = h_bn0_[b], be0 = h_be0_[b];
+            for (int j = 0; j < B.count; ++j) {
+                const ref::NeuronGene &G = B.genes[j];
+                const int n = bn0 + j;
+                float *g = &ngene[(size_t)n * 16];
+                g[G_CAP] = G.cap; g[G_GL] = G.gl; g[G_EL] = G.el; g[G_VT] = G.vt;
+                g[G_SLOPE] = G.slope; g[G_A] = G.a; g[G_TAUW] = G.tau_w; g[G_B] = G.b;
+                g[G_VR] = G.vr; g[G_ADPB] = G.adp_b;
+                g[G_ADPDECAY] = G.adp_tau > 0 ? nsx::expf_cr(-0.25f / G.adp_tau) : 1.0f;
+                g[G_GLSLOPE] = G.gl * G.slope;
+                g[G_RECBASE] = G.rec_base; g[G_RECGAIN] = G.rec_gain; g[G_RECEVENT] = G.rec_event;
+                g[G_RECDECAY] = nsx::expf_cr(-1.0f / G.rec_decay);
+                if (G.type > 6) throw std::runtime_error("Invalid neuron gene");
+                uint32_t f = (uint32_t)G.type;
+                if (G.active) f |= NF_ACTIVE;
+                if (G.inh_tx) f |= NF_INH;
+                f |= (uint32_t)(G.modulator & 3u) << NF_MOD_SHIFT;
+                if (G.sensory_channel >= 0) f |= NF_GENE_SENS;
+                if (G.adp_tau > 0) f |= NF_ADP;
+                const int sens = B.sensory ? B.sensory[j] : -1;
+                if (sens >= 0) {
+                    if (sens >= channels) throw std::runtime_error("Invalid neuron gene");
+                    f |= NF_HAS_INPUT;
+                }
+                if (excitatory_type(G.type)) f |= NF_EXC_TYPE;
+                h_nflags_[n] = f;
+                nsens[n] = sens;
+                nbrain[n] = b;
+                norig[n] = B.orig_n ? B.orig_n[j] : (uint32_t)j;
+                if (G.type == 2 || G.type == 3 || G.type == 6) {
+                    h_nxidx_[n] = n_heavy_++;
+                    float xg[16] = {};
+                    if (G.type == 2) { xg[0] = G.lp.calcium; xg[1] = G.lp.calcium_k; xg[2] = G.lp.h; xg[3] = G.lp.leak; }
+                    if (G.type == 3) { for (int q = 0; q < 8; ++q) xg[q] = G.prinz.g[q]; xg[8] = G.prinz_leak; }
+                    xgene.insert(xgene.end(), xg, xg + 16);
+                }
+            }
+            // incoming CSR of this brain: stable counting sort by post
+            std::vector<int> cnt(B.count + 1, 0);
+            for (int j = 0; j < B.edges; ++j) ++cnt[B.conns[j].post + 1];
+            for (int j = 0; j < B.count; ++j) cnt[j + 1] += cnt[j];
+            std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+            for (int j = 0; j < B.edges; ++j) {
+                const ref::SynapseGene &C = B.conns[j];
+                const int e = be0 + pos[C.post]++;
+                const ref::NeuronGene &A = B.genes[C.pre], &Z = B.genes[C.post];
+                const bool live = C.active && A.active && Z.active;
+                const bool pair = !A.inh_tx && excitatory_type(A.type) && !A.modulator && !Z.inh_tx &&
+                                  excitatory_type(Z.type);
+                uint32_t kind = A.modulator ? KIND_MOD : (A.inh_tx ? KIND_INH : KIND_EXC);
+                const int pre_local = bn0 + C.pre - un0;
+                if (pre_local > 0xffff) throw std::runtime_error("Unit exceeds 65536 neurons");
+                if (C.plasticity > 7) throw std::runtime_error("Invalid synapse gene");
+                uint32_t m = (uint32_t)pre_local | ((uint32_t)C.delay << M_DELAY_SHIFT) |
+                             ((uint32_t)(C.branch & 3u) << M_BRANCH_SHIFT) | (kind << M_KIND_SHIFT) |
+                             ((uint32_t)((A.modulator ? A.modulator - 1 : 0) & 3u) << M_MODID_SHIFT) |
+                             ((uint32_t)C.plasticity << M_PROF_SHIFT);
+                if (live) m |= M_LIVE;
+                if (live && C.plasticity && pair) m |= M_PLASTIC;
+                smeta[e] = m;
+                const int sites = C.sites ? (C.sites > 64 ? 64 : C.sites) : 14;
+                uint32_t *y = &sgene[(size_t)e * Y_WORDS];
+                float yf[8] = {C.w0, C.U, C.trec, C.tfac, C.slow_rec, C.slow_depl, 0.0f, 0.0f};
+                std::memcpy(y, yf, sizeof yf);
+                y[Y_INFO] = (uint32_t)sites | ((uint32_t)C.receptors << 8);
+                h_sinfo_[e] = y[Y_INFO];
+                h_w0_[e] = C.w0;
+                sorig[e] = B.orig_s ? B.orig_s[j] : (uint32_t)j;
+                sbrain[e] = b;
+                h_syn_orig_[e] = j;
+                h_syn_pool_[be0 + j] = e;
+            }
+        }
+    }
+    // inptr[n] must be the start of neuron n's segment: rebuild as starts.
+    {
+        std::vector<int> starts(n_neurons_ + 1);
+        for (int b = 0; b < n_brains_; ++b) {
+            const int bn0 = h_bn0_[b], be0 = h_be0_[b];
+            std::vector<int> c(brains[b].count + 1, 0);
+            for (int j = 0; j < brains[b].edges; ++j) ++c[brains[b].conns[j].post + 1];
+            for (int j = 0; j < brains[b].count; ++j) c[j + 1] += c[j];
+            for (int j = 0; j <= brains[b].count; ++j) starts[bn0 + j] = be0 + c[j];
+        }
+        starts[n_neurons_] = n_synapses_;
+        inptr.swap(starts);
+    }
+    std::vector<int> bmotor((size_t)n_brains_ * outputs);
+    for (int b = 0; b < n_brains_; ++b)
+        for (int j = 0; j < outputs; ++j) bmotor[(size_t)b * outputs + j] = h_bn0_[b] + brains[b].motors[j];
+    // ---- device allocation and upload ----
+    NSB_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    auto up = [&](auto *dst, const auto &src) {
+        NSB_CHECK(cudaMemcpy(dst, src.data(), src.size() * sizeof(src[0]), cudaMemcpyHostToDevice));
+    };
+    d_ngene_ = alloc<float>(ngene.size()); up(d_ngene_, ngene);
+    d_nflags_ = alloc<uint32_t>(n_neurons_); up(d_nflags_, h_nflags_);
+    d_nsens_ = alloc<int>(n_neurons_); up(d_nsens_, nsens);
+    d_nxidx_ = alloc<int>(n_neurons_); up(d_nxidx_, h_nxidx_);
+    d_xgene_ = alloc<float>(std::max<size_t>(xgene.size(), 16)); if (!xgene.empty()) up(d_xgene_, xgene);
+    d_xstate_ = alloc<float>((size_t)std::max(n_heavy_, 1) * 16);
+    NSB_CHECK(cudaMemset(d_xstate_, 0, (size_t)std::max(n_heavy_, 1) * 16 * sizeof(float)));
+    d_nstate_ = alloc<uint32_t>((size_t)n_neurons_ * S_WORDS);
+    NSB_CHECK(cudaMemset(d_nstate_, 0, (size_t)n_neurons_ * S_WORDS * 4));
+    d_inptr_ = alloc<int>(n_neurons_ + 1); up(d_inptr_, inptr);
+    d_smeta_ = alloc<uint32_t>(n_synapses_); if (n_synapses_) up(d_smeta_, smeta);
+    d_sgene_ = alloc<uint32_t>((size_t)n_synapses_ * Y_WORDS); if (n_synapses_) up(d_sgene_, sgene);
+    d_sstate_ = alloc<uint32_t>((size_t)n_synapses_ * Z_WORDS);
+    NSB_CHECK(cudaMemset(d_sstate_, 0, (size_t)std::max(n_synapses_, 1) * Z_WORDS * 4));
+    d_sarrived_ = alloc<uint8_t>(n_synapses_);
+    NSB_CHECK(cudaMemset(d_sarrived_, 0, std::max(n_synapses_, 1)));
+    d_slastp_ = alloc<int16_t>(n_synapses_);
+    NSB_CHECK(cudaMemset(d_slastp_, 0xff, (size_t)std::max(n_synapses_, 1) * 2));
+    d_bn0_ = alloc<int>(n_brains_); up(d_bn0_, h_bn0_);
+    d_be0_ = alloc<int>(n_brains_); up(d_be0_, h_be0_);
+    d_btick_ = alloc<int64_t>(n_brains_); NSB_CHECK(cudaMemset(d_btick_, 0, n_brains_ * sizeof(int64_t)));
+    d_bmotor_ = alloc<int>(std::max<size_t>(bmotor.size(), 1)); up(d_bmotor_, bmotor);
+    d_ubrain_ = alloc<int>(n_brains_); up(d_ubrain_, brain_order);
+    d_units_ = alloc<int4>(n_units_); up(d_units_, units);
+    d_unitb_ = alloc<int2>(n_units_); up(d_unitb_, unitb);
+    d_queue_ = alloc<int>(1);
+    d_events_ = alloc<unsigned long long>(1); NSB_CHECK(cudaMemset(d_events_, 0, 8));
+    d_input_ = alloc<float>((size_t)n_brains_ * channels);
+    NSB_CHECK(cudaMemset(d_input_, 0, (size_t)n_brains_ * channels * 4));
+    d_mask_ = alloc<uint8_t>(n_brains_); NSB_CHECK(cudaMemset(d_mask_, 1, n_brains_));
+    d_output_ = alloc<float>((size_t)n_brains_ * outputs);
+    d_status_ = alloc<int>(n_brains_);
+    d_seeds_ = alloc<uint32_t>(n_brains_);
+    d_rmask_ = alloc<uint8_t>(n_brains_);
+    d_nbrain_ = alloc<int>(n_neurons_); up(d_nbrain_, nbrain);
+    d_norig_ = alloc<uint32_t>(n_neurons_); up(d_norig_, norig);
+    d_sbrain_ = alloc<int>(n_synapses_); if (n_synapses_) up(d_sbrain_, sbrain);
+    d_sorig_ = alloc<uint32_t>(n_synapses_); if (n_synapses_) up(d_sorig_, sorig);
+    h_tick_.assign(n_brains_, 0);
+
+    // ---- launch shape ----
+    smem_ = 1024 + (kMetaCap + 32 * hw_ * 2 + 2 * kMaxUnitBrains) * 4 + kMaxUnitBrains * 8 + 2 * kMaxUnitBrains * 4;
+    NSB_CHECK(cudaFuncSetAttribute(tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_));
+    int dev = 0, sms = 0;
+    NSB_CHECK(cudaGetDevice(&dev));
+    NSB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    int occ = 0;
+    NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tick_kernel, block_, smem_));
+    ctas_per_sm_ = cfg.ctas_per_sm > 0 ? std::min(cfg.ctas_per_sm, std::max(occ, 1)) : std::max(occ, 1);
+    grid_ = std::min(n_units_, sms * ctas_per_sm_);
+    K_ = make_constants();
+}
+
+Engine::~Engine() {
+    for (auto &g : graphs_) cudaGraphExecDestroy(g.exec);
+    for (void *p : allocations_) cudaFree(p);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+Stats Engine::stats() const {
+    return Stats{n_brains_, n_units_, n_big_units_, n_neurons_, n_synapses_, n_heavy_, max_unit_neurons_,
+                 grid_, block_, smem_, ctas_per_sm_};
+}
+
+static Pools make_pools(float *ngene, uint32_t *nflags, int *nsens, int *nxidx, float *xgene, float *xstate,
+                        uint32_t *nstate, int *inptr, uint32_t *smeta, uint32_t *sgene, uint32_t *sstate,
+                        uint8_t *sarrived, int16_t *slastp, int *bn0, int *be0, int64_t *btick, int *bmotor,
+                        int4 *units, int2 *unitb, int *ubrain, int n_units, int channels, int outputs, int hw,
+                        int *queue, unsigned long long *events) {
+    Pools P;
+    P.ngene = reinterpret_cast<const float4 *>(ngene); P.nflags = nflags; P.nsens = nsens; P.nxidx = nxidx;
+    P.xgene = xgene; P.xstate = xstate; P.nstate = nstate; P.inptr = inptr; P.smeta = smeta; P.sgene = sgene;
+    P.sstate = sstate; P.sarrived = sarrived; P.slastp = slastp; P.bn0 = bn0; P.be0 = be0; P.btick = btick;
+    P.bmotor = bmotor; P.units = units; P.unitb = unitb; P.ubrain = ubrain; P.n_units = n_units;
+    P.channels = channels; P.outputs = outputs; P.hw = hw; P.queue = queue; P.events = events;
+    return P;
+}
+
+void Engine::launch(const float *d_input, const uint8_t *d_mask, int ticks, float gain, float *d_output,
+                    int *d_status, cudaStream_t stream) {
+    Pools P = make_pools(d_ngene_, d_nflags_, d_nsens_, d_nxidx_, d_xgene_, d_xstate_, d_nstate_, d_inptr_,
+                         d_smeta_, d_sgene_, d_sstate_, d_sarrived_, d_slastp_, d_bn0_, d_be0_, d_btick_,
+                         d_bmotor_, d_units_, d_unitb_, d_ubrain_, n_units_, channels_, outputs_, hw_, d_queue_,
+                         count_events_ ? d_events_ : nullptr);
+    NSB_CHECK(cudaMemsetAsync(d_queue_, 0, sizeof(int), stream));
+    tick_kernel<<<grid_, block_, smem_, stream>>>(P, d_input, d_mask, d_output, d_status, ticks, gain, K_);
+    NSB_CHECK(cudaGetLastError());
+}
+
+void Engine::step_device(const float *d_input, const uint8_t *d_mask, int ticks, float gain, float *d_output,
+                         int *d_status, cudaStream_t stream) {
+    if (ticks < 1 || ticks > 10000 || !std::isfinite(gain) || gain < 0)
+        throw std::runtime_error("Invalid neural integration interval");
+    launch(d_input, d_mask, ticks, gain, d_output, d_status, stream ? stream : stream_);
+}
+
+void Engine::step_host(const float *input, const uint8_t *mask, int ticks, float gain, float *output, int *status) {
+    if (ticks < 1 || ticks > 10000 || !std::isfinite(gain) || gain < 0)
+        throw std::runtime_error("Invalid neural integration interval");
+    for (int i = 0; i < n_brains_; ++i)
+        if (mask[i])
+            for (int j = 0; j < channels_; ++j) {
+                const float v = input[(size_t)i * channels_ + j];
+                if (!std::isfinite(v) || v < 0 || v > 1) throw std::runtime_error("Invalid encoded observation");
+            }
+    NSB_CHECK(cudaMemcpyAsync(d_input_, input, (size_t)n_brains_ * channels_ * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    NSB_CHECK(cudaMemcpyAsync(d_mask_, mask, n_brains_, cudaMemcpyHostToDevice, stream_));
+    launch(d_input_, d_mask_, ticks, gain, d_output_, d_status_, stream_);
+    NSB_CHECK(cudaMemcpyAsync(output, d_output_, (size_t)n_brains_ * outputs_ * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+    NSB_CHECK(cudaMemcpyAsync(status, d_status_, n_brains_ * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    NSB_CHECK(cudaStreamSynchronize(stream_));
+    for (int i = 0; i < n_brains_; ++i)
+        if (mask[i] && status[i] != -2) h_tick_[i] += ticks;
+}
+
+void Engine::step_graph(int ticks, float gain, cudaStream_t stream) {
+    if (ticks < 1 || ticks > 10000 || !std::isfinite(gain) || gain < 0)
+        throw std::runtime_error("Invalid neural integration interval");
+    cudaStream_t s = stream ? stream : stream_;
+    for (auto &g : graphs_)
+        if (g.ticks == ticks && g.gain == gain) {
+            NSB_CHECK(cudaGraphLaunch(g.exec, s));
+            return;
+        }
+    cudaGraph_t graph;
+    NSB_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    launch(d_input_, d_mask_, ticks, gain, d_output_, d_status_, s);
+    NSB_CHECK(cudaStreamEndCapture(s, &graph));
+    cudaGraphExec_t exec;
+    NSB_CHECK(cudaGraphInstantiate(&exec, graph, 0));
+    cudaGraphDestroy(graph);
+    graphs_.push_back({ticks, gain, exec});
+    NSB_CHECK(cudaGraphLaunch(exec, s));
+}
+
+void Engine::reset_host(const uint8_t *mask, const uint32_t *seeds) {
+    NSB_CHECK(cudaMemcpyAsync(d_rmask_, mask, n_brains_, cudaMemcpyHostToDevice, stream_));
+    NSB_CHECK(cudaMemcpyAsync(d_seeds_, seeds, n_brains_ * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
+    Pools P = make_pools(d_ngene_, d_nflags_, d_nsens_, d_nxidx_, d_xgene_, d_xstate_, d_nstate_, d_inptr_,
+                         d_smeta_, d_sgene_, d_sstate_, d_sarrived_, d_slastp_, d_bn0_, d_be0_, d_btick_,
+                         d_bmotor_, d_units_, d_unitb_, d_ubrain_, n_units_, channels_, outputs_, hw_, d_queue_,
+                         nullptr);
+    int dev = 0, sms = 0;
+    NSB_CHECK(cudaGetDevice(&dev));
+    NSB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    reset_neurons<<<sms * 8, 256, 0, stream_>>>(P, d_nbrain_, d_norig_, d_rmask_, d_seeds_, n_neurons_);
+    if (n_synapses_) reset_synapses<<<sms * 8, 256, 0, stream_>>>(P, d_sbrain_, d_sorig_, d_rmask_, d_seeds_, n_synapses_);
+    reset_ticks<<<(n_brains_ + 255) / 256, 256, 0, stream_>>>(d_btick_, d_rmask_, n_brains_);
+    NSB_CHECK(cudaGetLastError());
+    NSB_CHECK(cudaStreamSynchronize(stream_));
+    for (int i = 0; i < n_brains_; ++i)
+        if (mask[i]) h_tick_[i] = 0;
+}
+
+void Engine::set_tick(int brain, int64_t tick) {
+    if (brain < 0 || brain >= n_brains_) throw std::runtime_error("Invalid brain index");
+    NSB_CHECK(cudaStreamSynchronize(stream_));
+    NSB_CHECK(cudaMemcpy(d_btick_ + brain, &tick, 8, cudaMemcpyHostToDevice));
+    h_tick_[brain] = tick;
+}
+
+unsigned long long Engine::take_events() {
+    unsigned long long v = 0;
+    NSB_CHECK(cudaMemcpy(&v, d_events_, 8, cudaMemcpyDeviceToHost));
+    NSB_CHECK(cudaMemset(d_events_, 0, 8));
+    return v;
+}
+
+void Engine::dump(int brain, uint32_t *nw, uint32_t *sw, int64_t *tick) {
+    if (brain < 0 || brain >= n_brains_) throw std::runtime_error("Invalid brain index");
+    NSB_CHECK(cudaStreamSynchronize(stream_));
+    NSB_CHECK(cudaDeviceSynchronize());
+    const int n0 = h_bn0_[brain], nn = h_bnn_[brain], e0 = h_be0_[brain], ne = h_bne_[brain];
+    std::vector<uint32_t> rec((size_t)nn * S_WORDS), srec((size_t)std::max(ne, 1) * Z_WORDS);
+    std::vector<uint8_t> arr(std::max(ne, 1));
+    int64_t t = 0;
+    NSB_CHECK(cudaMemcpy(rec.data(), d_nstate_ + (size_t)n0 * S_WORDS, rec.size() * 4, cudaMemcpyDeviceToHost));
+    if (ne) {
+        NSB_CHECK(cudaMemcpy(srec.data(), d_sstate_ + (size_t)e0 * Z_WORDS, (size_t)ne * Z_WORDS * 4, cudaMemcpyDeviceToHost));
+        NSB_CHECK(cudaMemcpy(arr.data(), d_sarrived_ + e0, ne, cudaMemcpyDeviceToHost));
+    }
+    NSB_CHECK(cudaMemcpy(&t, d_btick_ + brain, 8, cudaMemcpyDeviceToHost));
+    if (tick) *tick = t;
+    if (nw) {
+        for (int j = 0; j < nn; ++j) {
+            const uint32_t *r = &rec[(size_t)j * S_WORDS];
+            uint32_t *o = nw + (size_t)j * kDumpNeuronWords;
+            std::memset(o, 0, kDumpNeuronWords * 4);
+            o[0] = r[S_V]; o[1] = r[S_W]; o[2] = r[S_ADP]; o[3] = r[S_INH]; o[4] = r[S_DEPOL]; o[5] = r[S_LOGAMPA];
+            o[6] = r[S_D0]; o[7] = r[S_D1]; o[8] = r[S_D2]; o[9] = r[S_D3];
+            const int xi = h_nxidx_[n0 + j];
+            if (xi >= 0) NSB_CHECK(cudaMemcpy(o + 10, d_xstate_ + (size_t)xi * 16, 64, cudaMemcpyDeviceToHost));
+            o[26] = r[S_TOTAL]; o[27] = r[S_SPIKE]; o[28] = r[S_RECNS]; o[29] = r[S_RECRNG];
+            uint32_t h = 0;
+            for (int k = 0; k < max_delay_ && k < 31; ++k) {
+                const int64_t tau = t - 1 - k;
+                if (tau < 0) break;
+                if ((r[S_HIST] >> (tau & 31)) & 1u) h |= 1u << k;
+            }
+            o[30] = h;
+        }
+    }
+    if (sw) {
+        for (int j = 0; j < ne; ++j) {
+            const int e = h_syn_pool_[e0 + j] - e0;
+            const uint32_t *z = &srec[(size_t)e * Z_WORDS];
+            uint32_t *o = sw + (size_t)j * kDumpSynapseWords;
+            std::memset(o, 0, kDumpSynapseWords * 4);
+            for (int k = 0; k < 11; ++k) o[k] = z[k];   // w .. post_age share the order
+            const int64_t last = (int32_t)z[Z_LAST];
+            o[11] = (uint32_t)(uint64_t)last; o[12] = (uint32_t)((uint64_t)last >> 32);
+            o[13] = z[Z_READYLO]; o[14] = z[Z_READYHI]; o[15] = z[Z_RNG]; o[16] = arr[e]; o[17] = z[Z_SLOW];
+        }
+    }
+}
+
+void Engine::load_state(int brain, const ref::NeuronState *neurons, const ref::SynapseState *synapses,
+                        const unsigned char (*history)[9], int64_t tick) {
+    if (brain < 0 || brain >= n_brains_) throw std::runtime_error("Invalid brain index");
+    if (tick < 0 || tick >= 2147483647ll) throw std::runtime_error("Tick outside the engine range");
+    const int n0 = h_bn0_[brain], nn = h_bnn_[brain], e0 = h_be0_[brain], ne = h_bne_[brain];
+    NSB_CHECK(cudaDeviceSynchronize());
+    std::vector<uint32_t> rec((size_t)nn * S_WORDS, 0u), srec((size_t)std::max(ne, 1) * Z_WORDS, 0u);
+    std::vector<uint8_t> arr(std::max(ne, 1), 0);
+    auto fw = [](float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; };
+    for (int j = 0; j < nn; ++j) {
+        const ref::NeuronState &s = neurons[j];
+        uint32_t *r = &rec[(size_t)j * S_WORDS];
+        r[S_V] = fw(s.v); r[S_W] = fw(s.w); r[S_ADP] = fw(s.adp); r[S_INH] = fw(s.inh); r[S_DEPOL] = fw(s.depol);
+        r[S_LOGAMPA] = fw(s.log_ampa); r[S_RECNS] = fw(s.rec_ns); r[S_RECRNG] = s.rec_rng;
+        r[S_D0] = fw(s.dend[0]); r[S_D1] = fw(s.dend[1]); r[S_D2] = fw(s.dend[2]); r[S_D3] = fw(s.dend[3]);
+        r[S_TOTAL] = (uint32_t)s.total; r[S_SPIKE] = s.spike;
+        uint32_t h = 0;
+        if (history)
+            for (int k = 1; k <= 9; ++k) {
+                const int64_t tau = tick - k;
+                if (tau < 0) break;
+                if (history[j][tau % 9]) h |= 1u << (tau & 31);
+            }
+        r[S_HIST] = h;
+        const int xi = h_nxidx_[n0 + j];
+        if (xi >= 0) NSB_CHECK(cudaMemcpy(d_xstate_ + (size_t)xi * 16, s.cell, 64, cudaMemcpyHostToDevice));
+    }
+    for (int j = 0; j < ne; ++j) {
+        const ref::SynapseState &s = synapses[j];
+        const int e = h_syn_pool_[e0 + j] - e0;
+        uint32_t *z = &srec[(size_t)e * Z_WORDS];
+        const float f[11] = {s.w, s.ru, s.pre_tr, s.post_tr, s.eltp, s.eltd, s.da_age, s.spine, s.st_age, s.pre_age, s.post_age};
+        for (int k = 0; k < 11; ++k) z[k] = fw(f[k]);
+        z[Z_SLOW] = fw(s.slow);
+        z[Z_READYLO] = (uint32_t)s.ready; z[Z_READYHI] = (uint32_t)(s.ready >> 32);
+        z[Z_RNG] = s.rng;
+        int64_t last = s.last < -1000000 ? -1000000 : s.last;
+        if (last >= 2147483647ll) throw std::runtime_error("Last arrival outside the engine range");
+        z[Z_LAST] = (uint32_t)(int32_t)last;
+        arr[e] = s.arrived;
+    }
+    NSB_CHECK(cudaMemcpy(d_nstate_ + (size_t)n0 * S_WORDS, rec.data(), rec.size() * 4, cudaMemcpyHostToDevice));
+    if (ne) {
+        NSB_CHECK(cudaMemcpy(d_sstate_ + (size_t)e0 * Z_WORDS, srec.data(), (size_t)ne * Z_WORDS * 4, cudaMemcpyHostToDevice));
+        NSB_CHECK(cudaMemcpy(d_sarrived_ + e0, arr.data(), ne, cudaMemcpyHostToDevice));
+    }
+    NSB_CHECK(cudaMemcpy(d_btick_ + brain, &tick, 8, cudaMemcpyHostToDevice));
+    h_tick_[brain] = tick;
+}
+
+}  // namespace nsb

@@ -1,0 +1,119 @@
+// B200 neural-tick engine: batched brains, one persistent fused kernel per
+// call (all ticks of the call inside one launch).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <memory>
+#include <string>
+#include <vector>
+#include "ns_layout.h"
+#include "ns_refabi.h"
+
+namespace nsb {
+
+// One brain in the reference's host representation (gym_adapter/native.cpp:23-38).
+struct BrainSpec {
+    const ref::NeuronGene *genes = nullptr;
+    int count = 0;
+    const ref::SynapseGene *conns = nullptr;
+    int edges = 0;
+    const int *motors = nullptr;        // outputs entries, brain-local
+    const int *sensory = nullptr;       // count entries, ABI sensory index (-1 none)
+    const uint32_t *orig_n = nullptr;   // optional original neuron indices (reset seeds)
+    const uint32_t *orig_s = nullptr;   // optional original synapse indices
+};
+
+struct EngineConfig {
+    int max_delay = 8;          // 8 = the reference ABI; up to 31
+    int block = 256;            // threads per CTA = neurons per small work unit
+    int ctas_per_sm = 0;        // 0: from occupancy
+    bool count_events = true;   // count synaptic arrivals on the device
+};
+
+struct Stats {
+    int brains, units, big_units, neurons, synapses, heavy, max_unit_neurons;
+    int grid, block, smem_bytes, ctas_per_sm;
+};
+
+class Engine {
+public:
+    // Builds device pools for `brains`; throws std::runtime_error on invalid input.
+    Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, const EngineConfig &cfg);
+    ~Engine();
+    Engine(const Engine &) = delete;
+    Engine &operator=(const Engine &) = delete;
+
+    int brains() const { return n_brains_; }
+    int channels() const { return channels_; }
+    int outputs() const { return outputs_; }
+    Stats stats() const;
+
+    // ns_gpu_reset semantics with host arrays; synchronous.
+    void reset_host(const uint8_t *mask, const uint32_t *seeds);
+    // ns_gpu_step semantics with host arrays (validated); synchronous.
+    void step_host(const float *input, const uint8_t *mask, int ticks, float gain, float *output, int *status);
+    // Device-resident step: all pointers device memory, asynchronous on `stream`.
+    // No validation; ticks in [1, 10000], inputs in [0, 1].
+    void step_device(const float *d_input, const uint8_t *d_mask, int ticks, float gain, float *d_output,
+                     int *d_status, cudaStream_t stream);
+    // Captures step_device on the engine's own buffers into a CUDA graph and
+    // replays it (one graph per (ticks, gain)).
+    void step_graph(int ticks, float gain, cudaStream_t stream);
+    // Engine-owned device buffers for step_device / step_graph.
+    float *dev_input() { return d_input_; }
+    uint8_t *dev_mask() { return d_mask_; }
+    float *dev_output() { return d_output_; }
+    int *dev_status() { return d_status_; }
+
+    // Canonical state dump of one brain (oracle layout, original order).
+    void dump(int brain, uint32_t *neuron_words, uint32_t *synapse_words, int64_t *tick);
+    // Load one brain's state from reference records (checkpoint / host state).
+    void load_state(int brain, const ref::NeuronState *neurons, const ref::SynapseState *synapses,
+                    const unsigned char (*history)[9], int64_t tick);
+    // Synaptic arrivals counted since the last call to take_events().
+    unsigned long long take_events();
+    int64_t host_tick(int brain) const { return h_tick_[brain]; }
+    // Overwrite one brain's tick counter.
+    void set_tick(int brain, int64_t tick);
+
+private:
+    void launch(const float *d_input, const uint8_t *d_mask, int ticks, float gain, float *d_output,
+                int *d_status, cudaStream_t stream);
+    template <class T> T *alloc(size_t n);
+
+    int n_brains_ = 0, channels_ = 0, outputs_ = 0, max_delay_ = 8;
+    int n_neurons_ = 0, n_synapses_ = 0, n_heavy_ = 0, n_units_ = 0, n_big_units_ = 0;
+    int max_unit_neurons_ = 0, hw_ = 0, meta_cap_ = 0, max_unit_brains_ = 0;
+    int grid_ = 0, block_ = 256, smem_ = 0, ctas_per_sm_ = 0;
+    bool count_events_ = true;
+    std::vector<void *> allocations_;
+    // device pools
+    float *d_ngene_ = nullptr; uint32_t *d_nflags_ = nullptr; int *d_nsens_ = nullptr; int *d_nxidx_ = nullptr;
+    float *d_xgene_ = nullptr; float *d_xstate_ = nullptr; uint32_t *d_nstate_ = nullptr; int *d_inptr_ = nullptr;
+    uint32_t *d_smeta_ = nullptr; uint32_t *d_sgene_ = nullptr; uint32_t *d_sstate_ = nullptr;
+    uint8_t *d_sarrived_ = nullptr; int16_t *d_slastp_ = nullptr;
+    int *d_bn0_ = nullptr, *d_bnn_ = nullptr, *d_be0_ = nullptr, *d_bne_ = nullptr;
+    int64_t *d_btick_ = nullptr; int *d_bmotor_ = nullptr; int *d_bunit_ = nullptr;
+    int4 *d_units_ = nullptr; int2 *d_unitb_ = nullptr; int *d_ubrain_ = nullptr;
+    int *d_nbrain_ = nullptr; uint32_t *d_norig_ = nullptr; int *d_sbrain_ = nullptr; uint32_t *d_sorig_ = nullptr;
+    uint8_t *d_rmask_ = nullptr;
+    int *d_queue_ = nullptr; unsigned long long *d_events_ = nullptr;
+    float *d_input_ = nullptr; uint8_t *d_mask_ = nullptr; float *d_output_ = nullptr; int *d_status_ = nullptr;
+    uint32_t *d_seeds_ = nullptr;
+    // host mirrors for layout mapping
+    std::vector<int> h_bn0_, h_bnn_, h_be0_, h_bne_;
+    std::vector<int> h_syn_orig_;        // pool synapse -> brain-local original edge index
+    std::vector<int> h_syn_pool_;        // per brain: original edge -> pool index (concatenated by brain e0)
+    std::vector<int> h_nxidx_;
+    std::vector<uint32_t> h_nflags_;
+    std::vector<int64_t> h_tick_;
+    std::vector<uint32_t> h_sinfo_;      // per pool synapse: sites | receptors << 8
+    std::vector<float> h_w0_;
+    struct Graph { int ticks; float gain; cudaGraphExec_t exec; };
+    std::vector<Graph> graphs_;
+    cudaStream_t stream_ = nullptr;
+    PhysConst K_{};
+    unsigned long long events_host_ = 0;
+};
+
+}  // namespace nsb

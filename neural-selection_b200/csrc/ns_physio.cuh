@@ -1,0 +1,410 @@
+// Device physiology of the neural tick (CUDA, sm_100a).
+//
+// The arithmetic restates the reference model (mixic/neural-selection
+// src/physiology.cuh:206-586, src/lp_cell.cuh:28-113,
+// src/prinz_cell.cuh:45-121) operation for operation: every binary32 add,
+// multiply and divide happens in the reference's order with IEEE rounding
+// (built with --fmad=false; divisions and square roots are IEEE), and every
+// exponential/logarithm is correctly rounded (ns_crmath.h). Constant-argument
+// and gene-constant exponentials are precomputed on the host with the same
+// correctly rounded function. Together this makes the engine's results
+// bit-identical to the CPU oracle.
+#pragma once
+#include <stdint.h>
+#include "ns_crmath.h"
+#include "ns_layout.h"
+
+namespace nsb {
+
+struct NeuronRegs {
+    float v, w, adp, inh, depol, rec_ns;
+    uint32_t rng;
+    float d0, d1, d2, d3;
+    int total;
+    uint32_t spike;
+};
+
+__device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(hi, fmaxf(lo, x)); }
+
+__device__ __forceinline__ uint32_t xorshift32(uint32_t x) {
+    x ^= x << 13; x ^= x >> 17; x ^= x << 5; return x;
+}
+
+__device__ __forceinline__ float crexp(float x, const double *tab) { return nsx::expf_cr_tab(x, tab); }
+
+// physiology.cuh:226-230: thin-branch input/output curve (type 0 only).
+__device__ __forceinline__ float branch_gain(float gs, float offset, const double *tab) {
+    float regen = 5.0f / (1.0f + crexp(-(gs - 4.0f) / 0.4f, tab));
+    return fminf(11.0f, gs + regen - offset);
+}
+
+// physiology.cuh:206-219: receptor events (type 5 with a receptor channel).
+__device__ __forceinline__ float receptor_drive(const float *g, uint32_t flags, NeuronRegs &s,
+                                                float level) {
+    if (!(flags & NF_GENE_SENS) || !(g[G_RECEVENT] > 0)) return 0.0f;
+    float rate = clampf(g[G_RECBASE] + g[G_RECGAIN] * level, 0.0f, 1000.0f);
+    s.rng = xorshift32(s.rng);
+    float u = (float)(s.rng >> 8) * (1.0f / 16777216.0f);
+    s.rec_ns *= g[G_RECDECAY];
+    if (u < rate * (1.0f / 1000.0f)) s.rec_ns += g[G_RECEVENT];
+    return s.rec_ns * (0.0f - s.v);
+}
+
+// physiology.cuh:290-374, AdEx path (types 0, 1, 4, 5), four 0.25 ms substeps.
+// exc0..3/inh_in: this tick's summed synaptic input.
+__device__ __forceinline__ void adex_tick(const float *g, uint32_t type, uint32_t flags, NeuronRegs &s,
+                                          float cur, float e0, float e1, float e2, float e3, float inh_in,
+                                          const PhysConst &K, const double *tab) {
+    s.d0 += e0; s.d1 += e1; s.d2 += e2; s.d3 += e3;
+    float sub = fmaxf(0.0f, fminf(s.v, -50.0f) - g[G_EL]);
+    s.depol += 0.1f * (sub - s.depol);
+    s.inh += inh_in;
+    s.spike = 0;
+    const float h = 0.25f;
+    const float clamp_leak = 0.0f, clamp_rev = -68.0f;
+#pragma unroll 1
+    for (int step = 0; step < 4; ++step) {
+        float v = s.v;
+        s.w += h * (g[G_A] * (v - g[G_EL]) - s.w) / g[G_TAUW];
+        float expo = clampf((v - g[G_VT]) / g[G_SLOPE], -20.0f, 10.0f);
+        float soma;
+        if (type == 0) {
+            soma = 0.0f + branch_gain(s.d0, K.dend_offset, tab);
+            soma += branch_gain(s.d1, K.dend_offset, tab);
+            soma += branch_gain(s.d2, K.dend_offset, tab);
+            soma += branch_gain(s.d3, K.dend_offset, tab);
+        } else {
+            soma = 0.0f + s.d0;
+            soma += s.d1; soma += s.d2; soma += s.d3;
+        }
+        float dv = g[G_GL] * (g[G_EL] - v) + g[G_GLSLOPE] * crexp(expo, tab) + soma * (0.0f - v) +
+                   s.inh * (-75.0f - v) + cur + s.adp - s.w - clamp_leak * (v - clamp_rev);
+        s.v = v + h * dv / g[G_CAP];
+        if (s.v >= 0.0f) {
+            s.spike = 1; ++s.total;
+            s.v = g[G_VR]; s.w += g[G_B]; s.adp += g[G_ADPB];
+        }
+        if (flags & NF_ADP) s.adp *= g[G_ADPDECAY];
+        s.d0 *= K.exc_sub; s.d1 *= K.exc_sub; s.d2 *= K.exc_sub; s.d3 *= K.exc_sub;
+        s.inh *= K.inh_sub;
+    }
+}
+
+// ---- LFS cell (physiology.cuh:258-287); x = {v, thr, act[3], open[3]} -------------
+__device__ __noinline__ void lfs_tick(const float *g, NeuronRegs &s, float *x, float cur, float exc, float inh,
+                                      const PhysConst &K) {
+    const float wt[3] = {250.0f, 10.0f, 4.0f}, op[3] = {10.0f, 40.0f, 750.0f}, cl[3] = {50.0f, 750.0f, 2000.0f};
+    x[1] = g[G_VT] + (x[1] - g[G_VT]) * K.lfs_thr;
+    float under = 0;
+    for (int j = 0; j < 3; ++j) {
+        x[5 + j] += x[2 + j] / op[j] - x[5 + j] / cl[j];
+        x[2 + j] *= K.lfs_open[j];
+        under += wt[j] * x[5 + j];
+    }
+    const float v = x[0];
+    const float i = g[G_GL] * (g[G_EL] - v) + exc * (10.0f - v) + inh * (-60.0f - v) + under * (-80.0f - v) + cur;
+    x[0] = v + i / g[G_CAP];
+    s.spike = x[0] >= x[1] ? 1u : 0u;
+    if (s.spike) {
+        x[1] = 200.0f;
+        for (int j = 0; j < 3; ++j) x[2 + j] += 1.0f;
+        ++s.total;
+    }
+    s.v = x[0];
+}
+
+// ---- LP cell (lp_cell.cuh:28-113) --------------------------------------------------
+__device__ __forceinline__ float lp_sig(float v, float mid, float slope, const double *tab) {
+    return 1.0f / (1.0f + crexp((v - mid) / slope, tab));
+}
+__device__ __forceinline__ float lp_ratio(float num, float den, float lim) { return fabsf(den) < 1e-5f ? lim : num / den; }
+__device__ __noinline__ void lp_rates(const float *x, float i_na, const float *sc, float *d, const double *tab) {
+    const float va = x[0], vs = x[15];
+    const float na = x[1] * x[1] * x[1] * x[2] * 7.15f * (va - 50.0f);
+    const float kd = x[8] * x[8] * x[8] * x[8] * 1.43f * (va + 72.0f);
+    const float km = .2613041227f * x[14] * (va + 80.0f);
+    const float aleak = sc[3] * .001004288227f * (va + 50.0f);
+    const float cpl = .004017089073f * (vs - va);
+    d[0] = (-na - kd - km - aleak + cpl) / .1148312178f;
+    const float ev = crexp(vs / 11.4866f, tab);
+    const float ghk = fabsf(vs) < .001f ? 11.4866f * (x[13] - 15123.5f) : vs * (x[13] * ev - 15123.5f) / (ev - 1.0f);
+    const float ca = sc[0] * (x[3] * x[4] * .1247796343f + x[5] * .07142141077f) * .00155982f * ghk * .9f;
+    const float kca = sc[1] * x[6] * x[7] * 1.663612026f * (vs + 72.0f) * .9f;
+    const float amix = lp_sig(vs, 55.0f, -15.0f, tab);
+    const float ka = x[9] * x[9] * x[9] * .8008791415f * (vs + 72.0f) * (amix * x[10] + (1.0f - amix) * x[11]) * .9f;
+    const float ih = sc[2] * x[12] * .0126874385f * (vs + 20.0f) * .9f;
+    const float sleak = sc[3] * .0006901584324f * (vs + 50.0f);
+    d[15] = (-ca - kca - ka - ih - sleak - cpl + (i_na - 2.0f) * .01222505828f) / .0543909161f;
+    float a = lp_ratio(-16.64f - .32f * va, crexp(-13.0f - va / 4.0f, tab) - 1.0f, 1.28f);
+    float b = lp_ratio(.28f * va + 7.0f, crexp(va / 5.0f + 5.0f, tab) - 1.0f, 1.4f);
+    d[1] = a * (1.0f - x[1]) - b * x[1];
+    a = .128f * crexp(-2.66666666667f - va / 18.0f, tab);
+    b = 4.0f / (crexp(-5.0f - va / 5.0f, tab) + 1.0f);
+    d[2] = a * (1.0f - x[2]) - b * x[2];
+    a = lp_ratio(-1.6f - .032f * va, crexp(-10.0f - va / 5.0f, tab) - 1.0f, .16f);
+    b = .5f * crexp(-1.375f - va / 40.0f, tab);
+    d[8] = a * (1.0f - x[8]) - b * x[8];
+    d[3] = (lp_sig(vs, 15.0f, -9.8f, tab) - x[3]) * .045f;
+    d[4] = (lp_sig(vs, -40.0f, 3.2f, tab) - x[4]) * .02f * lp_sig(vs, -15.0f, -10.0f, tab);
+    d[5] = (lp_sig(vs, 29.1336f, -4.43083f, tab) - x[5]) * .0608644f;
+    const float cai = x[13];
+    const float kinf = lp_sig(vs, -.6f * cai, -23.0f, tab) * lp_sig(vs, -16.0f - .6f * cai, -5.0f, tab) * cai / (2.5f + cai);
+    d[6] = (kinf - x[6]) * .6f;
+    d[7] = (.7f / (.6f + cai) - x[7]) * .035f;
+    d[9] = (lp_sig(vs, -12.0f, -26.0f, tab) - x[9]) * .14f;
+    const float ainf = lp_sig(vs, -62.0f, 6.0f, tab);
+    d[10] = (ainf - x[10]) * .05f;
+    d[11] = (ainf - x[11]) * .0036f * lp_sig(vs, -40.0f, -12.0f, tab);
+    d[12] = (lp_sig(vs, -70.0f, 8.0f, tab) - x[12]) * .00033f / lp_sig(vs, -110.0f, -21.6f, tab);
+    d[13] = -.05049639866f * ca - .01729930764f * (cai - .02f);
+    d[14] = (lp_sig(va, -26.9916223f, -5.957441281f, tab) - x[14]) * .0001386796618f *
+            lp_sig(va, -60.57875745f, -13.25674673f, tab);
+}
+__device__ __noinline__ void lp_integrate(float *x, float i_na, const float *sc, const double *tab) {
+    const float dt = .05f;
+    float k1[16], k2[16], k3[16], k4[16], y[16];
+    for (int step = 0; step < 20; ++step) {
+        lp_rates(x, i_na, sc, k1, tab);
+        for (int j = 0; j < 16; ++j) y[j] = x[j] + .5f * dt * k1[j];
+        lp_rates(y, i_na, sc, k2, tab);
+        for (int j = 0; j < 16; ++j) y[j] = x[j] + .5f * dt * k2[j];
+        lp_rates(y, i_na, sc, k3, tab);
+        for (int j = 0; j < 16; ++j) y[j] = x[j] + dt * k3[j];
+        lp_rates(y, i_na, sc, k4, tab);
+        for (int j = 0; j < 16; ++j) x[j] += dt * (k1[j] + 2 * k2[j] + 2 * k3[j] + k4[j]) / 6.0f;
+    }
+}
+
+// ---- Prinz pacemaker (prinz_cell.cuh:45-121); u = {v, ca, m[7], h[4]} -------------
+__device__ __forceinline__ float pz_gate(float v, float a, float b, const double *tab) {
+    return 1.0f / (1.0f + crexp((v + a) / b, tab));
+}
+__device__ __forceinline__ float pz_gate2(float v, float a, float b, float c, float d, const double *tab) {
+    return 1.0f / (crexp((v + a) / b, tab) + crexp((v + c) / d, tab));
+}
+__device__ __noinline__ void pz_substep(float *u, const float *g, float ext, float clamp_ns, float clamp_rev,
+                                        const PhysConst &K, const double *tab) {
+    const float dt = .025f;
+    float *m = u + 2, *h = u + 9;
+    const float v = u[0], ca = fmaxf(u[1], 0.000001f);
+    const float eca = (8.31451e3f * 283.0f / (2.0f * 96485.3415f)) * nsx::logf_cr(3000.0f / ca);
+    const float c[8] = {g[0] * m[0] * m[0] * m[0] * h[0], g[1] * m[1] * m[1] * m[1] * h[1],
+                        g[2] * m[2] * m[2] * m[2] * h[2], g[3] * m[3] * m[3] * m[3] * h[3],
+                        g[4] * m[4] * m[4] * m[4] * m[4], g[5] * m[5] * m[5] * m[5] * m[5],
+                        g[6] * m[6], g[7]};
+    const float rev[8] = {50, eca, eca, -80, -80, -80, -20, -50};
+    float gt = clamp_ns, ws = ext + clamp_ns * clamp_rev;
+    for (int i = 0; i < 8; ++i) { gt += c[i]; ws += c[i] * rev[i]; }
+    if (fabsf(gt) < .000001f) u[0] = v + dt * ws / 628.3f;
+    else { const float tg = ws / gt; u[0] = tg + (v - tg) * crexp(-dt * gt / 628.3f, tab); }
+    const float ica = (c[1] + c[2]) * (v - eca) / 1000000.0f;
+    const float cat = .05f - 14961.0f * ica;
+    u[1] = fmaxf(.000001f, cat + (ca - cat) * K.prinz_ca);
+    const float mi[7] = {pz_gate(v, 25.5f, -5.29f, tab), pz_gate(v, 27.1f, -7.2f, tab), pz_gate(v, 33, -8.1f, tab),
+                         pz_gate(v, 27.2f, -8.7f, tab), (ca / (ca + 3)) * pz_gate(v, 28.3f, -12.6f, tab),
+                         pz_gate(v, 12.3f, -11.8f, tab), pz_gate(v, 75, 5.5f, tab)};
+    const float mt[7] = {2.64f - 2.52f * pz_gate(v, 120, -25, tab), 43.4f - 42.6f * pz_gate(v, 68.1f, -20.5f, tab),
+                         2.8f + 14 * pz_gate2(v, 27, 10, 70, -13, tab), 23.2f - 20.8f * pz_gate(v, 32.9f, -15.2f, tab),
+                         180.6f - 150.2f * pz_gate(v, 46, -22.7f, tab), 14.4f - 12.8f * pz_gate(v, 28.3f, -19.2f, tab),
+                         2.0f / (crexp(-14.59f - .086f * v, tab) + crexp(-1.87f + .0701f * v, tab))};
+    for (int i = 0; i < 7; ++i) m[i] = mi[i] + (m[i] - mi[i]) * crexp(-dt / mt[i], tab);
+    const float hi[4] = {pz_gate(v, 48.9f, 5.18f, tab), pz_gate(v, 32.1f, 5.5f, tab), pz_gate(v, 60, 6.2f, tab),
+                         pz_gate(v, 56.9f, 4.9f, tab)};
+    const float ht[4] = {(1.34f / (1 + crexp((v + 62.9f) / -10, tab))) * (1.5f + 1 / (1 + crexp((v + 34.9f) / 3.6f, tab))),
+                         210 - 179.6f * pz_gate(v, 55, -16.9f, tab), 120 + 300 * pz_gate2(v, 55, 9, 65, -16, tab),
+                         77.2f - 58.4f * pz_gate(v, 38.9f, -26.5f, tab)};
+    for (int i = 0; i < 4; ++i) h[i] = hi[i] + (h[i] - hi[i]) * crexp(-dt / ht[i], tab);
+}
+
+// Heavy cell types (2 LP, 3 Prinz, 6 LFS) on their extended state x (16 floats).
+__device__ __noinline__ void heavy_tick(const float *g, uint32_t type, const float *xg, float *x, NeuronRegs &s,
+                                        float cur, float e0, float e1, float e2, float e3, float inh_in,
+                                        const PhysConst &K, const double *tab) {
+    const float clamp_leak = 0.0f, clamp_rev = -68.0f;
+    s.d0 += e0; s.d1 += e1; s.d2 += e2; s.d3 += e3;
+    float sub = fmaxf(0.0f, fminf(s.v, -50.0f) - g[G_EL]);
+    s.depol += 0.1f * (sub - s.depol);
+    s.inh += inh_in;
+    s.spike = 0;
+    float exc = 0;
+    exc += s.d0; exc += s.d1; exc += s.d2; exc += s.d3;
+    if (type == 6) {
+        lfs_tick(g, s, x, cur, exc, s.inh, K);
+    } else if (type == 2) {
+        float axon_before = x[0];
+        float ext = cur + exc * (0.0f - s.v) + s.inh * (-75.0f - s.v) - clamp_leak * (s.v - clamp_rev);
+        lp_integrate(x, ext / 1000.0f, xg, tab);
+        s.v = x[15] - 9.342518882f;
+        s.spike = (axon_before < 0 && x[0] >= 0) ? 1u : 0u;
+        s.total += (int)s.spike;
+    } else {
+        const float ext = cur + exc * (0.0f - s.v) + s.inh * (-75.0f - s.v);
+        bool spiked = false;
+        for (int i = 0; i < 40; ++i) {
+            const float before = x[0];
+            pz_substep(x, xg, ext, xg[8] + clamp_leak, clamp_rev, K, tab);
+            spiked |= before < 0 && x[0] >= 0;
+        }
+        s.spike = spiked ? 1u : 0u;
+        s.total += (int)s.spike;
+        s.v = x[0];
+    }
+    s.d0 *= K.exc_ms; s.d1 *= K.exc_ms; s.d2 *= K.exc_ms; s.d3 *= K.exc_ms;
+    s.inh *= K.inh_ms;
+}
+
+// ---- homeostasis (physiology.cuh:243-253) ----------------------------------------
+__device__ __forceinline__ float homeostasis(uint32_t type, float log_ampa, float elapsed, float hz,
+                                             const PhysConst &K) {
+    if (type != 0) return log_ampa;
+    float ratio = clampf(hz / 0.4f, 0.0f, 2.65f);
+    float change = ratio < 1.0f ? K.log_up * (1.0f - ratio) : K.log_down * ((ratio - 1.0f) / 1.65f);
+    return clampf(log_ampa + change * (elapsed / 172800000.0f), -3.0f, 3.0f);
+}
+
+// ---- synapse -----------------------------------------------------------------------
+// Release (physiology.cuh:425-454) on a synapse state record in registers.
+struct SynRelease {
+    float w, ru, slow;
+    uint64_t ready;
+    uint32_t rng;
+    int last;
+};
+__device__ __forceinline__ float release(const float *y, SynRelease &s, int64_t tick, const double *tab) {
+    float p_rec = 0;
+    if (s.last > -1000000) {
+        float dt = (float)(tick - (int64_t)s.last) * 1.0f;
+        p_rec = 1.0f - crexp(-dt / y[Y_TREC], tab);
+        if (y[Y_TFAC] > 0) s.ru *= crexp(-dt / y[Y_TFAC], tab);
+        if (y[Y_SLOWREC] > 0) s.slow = 1.0f - (1.0f - s.slow) * crexp(-dt / y[Y_SLOWREC], tab);
+    }
+    s.ru = y[Y_TFAC] > 0 ? s.ru + y[Y_U] * (1.0f - s.ru) : y[Y_U];
+    const int n = (int)(__float_as_uint(y[Y_INFO]) & 0xffu);
+    int released = 0;
+    uint32_t rng = s.rng;
+    uint64_t ready = s.ready;
+    const float ru = s.ru;
+    for (int site = 0; site < n; ++site) {
+        uint64_t bit = 1ull << site;
+        if (!(ready & bit)) {
+            rng = xorshift32(rng);
+            if ((float)(rng >> 8) * (1.0f / 16777216.0f) < p_rec) ready |= bit;
+        }
+        if (ready & bit) {
+            rng = xorshift32(rng);
+            if ((float)(rng >> 8) * (1.0f / 16777216.0f) < ru) { ready &= ~bit; ++released; }
+        }
+    }
+    s.rng = rng; s.ready = ready;
+    s.last = (int)tick;
+    float out = s.w * (float)released / (float)n * s.slow;
+    if (y[Y_SLOWREC] > 0) s.slow *= 1.0f - y[Y_SLOWDEPL];
+    return out;
+}
+
+// Plasticity state in registers.
+struct SynPlast {
+    float w, pre_tr, post_tr, eltp, eltd, da_age, spine, st_age, pre_age, post_age;
+};
+
+__device__ __forceinline__ float da_window(float age, const double *tab) {
+    if (age < 0 || age > 20000.0f) return 0;
+    float x = age / 2000.0f;
+    return x * x * x * x * crexp(4.0f * (1.0f - x), tab);
+}
+__device__ __forceinline__ float spine_window(float age, const double *tab) {
+    if (age < 0 || age > 5000.0f) return 0;
+    float x = age / 1000.0f;
+    return x * x * x * crexp(3.0f * (1.0f - x), tab);
+}
+
+// One plasticity tick (physiology.cuh:459-555) for a plastic synapse
+// (plasticity != 0 and excitatory pair), all channels available.
+__device__ __forceinline__ void plasticity_tick(uint32_t prof, uint32_t receptors, float w0, SynPlast &s,
+                                                bool arrived, bool post, float depol, uint32_t mod,
+                                                const PhysConst &K, const double *tab) {
+    if (prof == 5) {
+        if (s.st_age >= 0) { s.st_age += 1.0f; if (s.st_age > 5000.0f) s.st_age = -1; }
+        s.pre_age += 1.0f;
+        if (arrived) s.pre_age = 0;
+        if (post && s.pre_age <= 15.0f && s.st_age < 0) s.st_age = 0;
+        if ((mod & 4u) && (receptors & 4u)) s.spine = clampf(s.spine + 0.025f * spine_window(s.st_age, tab), 1.0f, 2.0f);
+        return;
+    }
+    if (prof == 4) {
+        if (s.da_age >= 0) { s.da_age += 1.0f; if (s.da_age > 20000.0f) s.da_age = -1; }
+        s.pre_age += 1.0f;
+        if (arrived) s.pre_age = 0;
+        if (post && s.pre_age <= 15.0f && (s.da_age < 0 || s.da_age > 30.0f)) {
+            s.da_age = 0;
+            s.w -= 0.005383f * w0;
+        }
+        if ((mod & 4u) && (receptors & 4u)) {
+            s.w += 0.00453f * da_window(s.da_age, tab) * w0;
+            s.da_age = -1;
+        }
+        s.w = clampf(s.w, 0.0f, 2.0f * w0);
+        return;
+    }
+    if (prof == 3) {
+        s.eltp *= K.ne; s.eltd *= K.sht;
+        s.pre_age += 1.0f; s.post_age += 1.0f;
+        if (arrived) { if (s.post_age <= 15.0f) s.eltd += 1.0f; s.pre_age = 0; }
+        if (post) { if (s.pre_age <= 15.0f) s.eltp += 1.0f; s.post_age = 0; }
+        if ((mod & 1u) && (receptors & 1u)) { s.w += 0.0048f * s.eltp * w0; s.eltp = 0; }
+        if ((mod & 2u) && (receptors & 2u)) { s.w -= 0.0075f * s.eltd * w0; s.eltd = 0; }
+        s.w = clampf(s.w, 0.0f, 2.0f * w0);
+        return;
+    }
+    s.pre_tr *= K.ltp; s.post_tr *= K.ltd;
+    s.pre_age += 1.0f; s.post_age += 1.0f;
+    if (arrived) {
+        if (s.post_age <= (prof == 2 ? 50.0f : 20.0f)) s.w *= 1.0f - 0.004f * s.post_tr;
+        s.pre_tr += 1.0f;
+        s.pre_age = 0;
+    }
+    if (post) {
+        if (s.pre_age <= 20.0f && (prof == 1 || depol >= 2.3f)) s.w += 0.016f * s.pre_tr * (2.0f * w0 - s.w);
+        s.post_tr += 1.0f;
+        s.post_age = 0;
+    }
+    s.w = clampf(s.w, 0.0f, 2.0f * w0);
+}
+
+// k consecutive ticks with no arrival, no postsynaptic spike and no relevant
+// modulator event: exactly k applications of plasticity_tick's quiet branch
+// (each field evolves independently; the weight bound is idempotent).
+__device__ __forceinline__ void plasticity_quiet(uint32_t prof, float w0, SynPlast &s, int k, const PhysConst &K) {
+    if (k <= 0) return;
+    if (prof == 5) {
+        for (int i = 0; i < k; ++i) {
+            if (s.st_age >= 0) { s.st_age += 1.0f; if (s.st_age > 5000.0f) s.st_age = -1; }
+            s.pre_age += 1.0f;
+        }
+        return;
+    }
+    if (prof == 4) {
+        for (int i = 0; i < k; ++i) {
+            if (s.da_age >= 0) { s.da_age += 1.0f; if (s.da_age > 20000.0f) s.da_age = -1; }
+            s.pre_age += 1.0f;
+        }
+        s.w = clampf(s.w, 0.0f, 2.0f * w0);
+        return;
+    }
+    if (prof == 3) {
+        for (int i = 0; i < k; ++i) { s.eltp *= K.ne; s.eltd *= K.sht; s.pre_age += 1.0f; s.post_age += 1.0f; }
+        s.w = clampf(s.w, 0.0f, 2.0f * w0);
+        return;
+    }
+    for (int i = 0; i < k; ++i) { s.pre_tr *= K.ltp; s.post_tr *= K.ltd; s.pre_age += 1.0f; s.post_age += 1.0f; }
+    s.w = clampf(s.w, 0.0f, 2.0f * w0);
+}
+
+// Does a modulator bit set at the postsynaptic neuron affect this profile?
+__device__ __forceinline__ bool mod_relevant(uint32_t prof, uint32_t receptors, uint32_t mod) {
+    if (prof == 3) return (mod & receptors & 3u) != 0;
+    if (prof == 4 || prof == 5) return (mod & receptors & 4u) != 0;
+    return false;
+}
+
+}  // namespace nsb

@@ -1,0 +1,89 @@
+// Host-side record layouts that must match the reference byte for byte.
+//
+// The reference's Gym GPU entry point ns_gpu_create (gym_adapter/gpu.cu:66-109
+// of mixic/neural-selection) receives opaque `Brain*` handles made by the host
+// library's ns_create (gym_adapter/native.cpp:23-38) and reads their
+// std::vector members directly. For this library's ns_gpu_create to accept
+// those handles (and for its own ns_create handles to be accepted by the
+// reference), the structs below reproduce that layout: same member types in
+// the same order, so libstdc++ lays them out identically. Member names are
+// this project's own. Sizes and offsets are checked by static_assert against
+// the values of the reference built with g++ on x86-64 (NeuronGene 124 B,
+// NeuronState 120 B, SynapseGene 40 B, SynapseState 80 B).
+#pragma once
+#include <array>
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+namespace nsb {
+namespace ref {
+
+struct LpScale { float calcium, calcium_k, h, leak; };
+struct PrinzG { float g[8]; };
+
+struct NeuronGene {                     // src/physiology.cuh:29-45
+    float cap, gl, el, vt, slope, a, tau_w, b, vr, adp_b, adp_tau;
+    unsigned char type, active, modulator, inh_tx;
+    LpScale lp;
+    PrinzG prinz;
+    float prinz_leak;
+    signed char sensory_channel;
+    float rec_base, rec_gain, rec_event, rec_decay, affinity;
+};
+
+struct NeuronState {                    // src/physiology.cuh:50-58
+    float v, w, adp, inh, depol, log_ampa;
+    float dend[4];
+    float cell[16];                     // the LP / Prinz / LFS union (64 bytes)
+    int total;
+    unsigned char spike;
+    float rec_ns;
+    uint32_t rec_rng;
+};
+
+struct SynapseGene {                    // src/physiology.cuh:59-65
+    float w0, U, trec, tfac;
+    int pre, post;
+    unsigned char delay, active, plasticity, branch, sites, receptors;
+    float slow_rec, slow_depl;
+};
+
+struct SynapseState {                   // src/physiology.cuh:66-76
+    float w, ru, pre_tr, post_tr, eltp, eltd, da_age, spine, st_age, pre_age, post_age;
+    int64_t last;
+    uint64_t ready;
+    uint32_t rng;
+    unsigned char arrived;
+    float slow;
+};
+
+// gym_adapter/native.cpp:23-38
+struct Brain {
+    std::vector<NeuronGene> genes;
+    std::vector<SynapseGene> connections;
+    std::vector<NeuronState> neurons;
+    std::vector<SynapseState> synapses;
+    std::vector<int> motors;
+    std::vector<std::array<unsigned char, 9>> history;
+    std::vector<std::array<float, 4>> excitation;
+    std::vector<float> inhibition;
+    std::vector<unsigned char> modulation;
+    std::vector<int> sensory;
+    std::vector<uint32_t> original_neurons, original_synapses;
+    int channels;
+    int64_t tick = 0;
+};
+
+static_assert(sizeof(NeuronGene) == 124, "NeuronGene layout");
+static_assert(offsetof(NeuronGene, type) == 44 && offsetof(NeuronGene, lp) == 48, "NeuronGene layout");
+static_assert(offsetof(NeuronGene, sensory_channel) == 100 && offsetof(NeuronGene, rec_base) == 104, "NeuronGene layout");
+static_assert(sizeof(NeuronState) == 120 && offsetof(NeuronState, cell) == 40, "NeuronState layout");
+static_assert(offsetof(NeuronState, spike) == 108 && offsetof(NeuronState, rec_ns) == 112, "NeuronState layout");
+static_assert(sizeof(SynapseGene) == 40 && offsetof(SynapseGene, delay) == 24 && offsetof(SynapseGene, slow_rec) == 32,
+              "SynapseGene layout");
+static_assert(sizeof(SynapseState) == 80 && offsetof(SynapseState, last) == 48 && offsetof(SynapseState, rng) == 64 &&
+              offsetof(SynapseState, slow) == 72, "SynapseState layout");
+
+}  // namespace ref
+}  // namespace nsb

@@ -1,0 +1,257 @@
+"""ctypes bindings of libns_b200.so (include/ns_b200.h).
+
+`Brain` mirrors the host-executor entry points the reference's Gym adapter
+binds (gym_adapter/adapter.py:28-41: ns_create/ns_reset/ns_step/...), and
+`GpuBatch` the batched ones (gym_adapter/gpu.py:35-38: ns_gpu_*), with the same
+argument meaning and error behaviour (RuntimeError carrying ns_error()). All
+stepping runs on the GPU; there is no CPU fallback: if the library or a GPU is
+missing the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libns_b200.so"
+
+_f = ct.POINTER(ct.c_float)
+_u8 = ct.POINTER(ct.c_uint8)
+_u32 = ct.POINTER(ct.c_uint32)
+_i32 = ct.POINTER(ct.c_int)
+_i64 = ct.POINTER(ct.c_int64)
+_vp = ct.c_void_p
+
+_lib = None
+
+# Every symbol include/ns_b200.h declares, with (restype, argtypes).
+SIGNATURES = {
+    "ns_error": (ct.c_char_p, []),
+    "ns_create": (_vp, [ct.c_int] * 4 + [_f, _f, _i32]),
+    "ns_original_indices": (None, [_vp, _u32, _u32]),
+    "ns_destroy": (None, [_vp]),
+    "ns_reset": (None, [_vp, ct.c_uint32]),
+    "ns_step": (ct.c_int, [_vp, _f, ct.c_int, ct.c_float, _f]),
+    "ns_gpu_create": (_vp, [ct.POINTER(_vp), ct.c_int]),
+    "ns_gpu_destroy": (None, [_vp]),
+    "ns_gpu_reset": (ct.c_int, [_vp, _u8, _u32]),
+    "ns_gpu_step": (ct.c_int, [_vp, _f, _u8, ct.c_int, ct.c_float, _f, _i32]),
+    "nsb_create_ext": (_vp, [ct.c_int] * 4 + [_f, _f, _i32, ct.c_int]),
+    "nsb_gpu_create_ext": (_vp, [ct.POINTER(_vp), ct.c_int, ct.c_int, ct.c_int]),
+    "nsb_gpu_create_rows": (_vp, [ct.c_int, _i64, _i64, _f, _f, _i32, ct.c_int, ct.c_int, ct.c_int, ct.c_int]),
+    "nsb_gpu_step_device": (ct.c_int, [_vp, _vp, _vp, ct.c_int, ct.c_float, _vp, _vp, _vp]),
+    "nsb_gpu_step_graph": (ct.c_int, [_vp, ct.c_int, ct.c_float, _vp]),
+    "nsb_gpu_buffer": (_vp, [_vp, ct.c_int]),
+    "nsb_gpu_upload": (ct.c_int, [_vp, _f, _u8]),
+    "nsb_gpu_download": (ct.c_int, [_vp, _f, _i32]),
+    "nsb_gpu_dump": (ct.c_int, [_vp, ct.c_int, _u32, _u32, _i64]),
+    "nsb_dump": (ct.c_int, [_vp, _u32, _u32, _i64]),
+    "nsb_gpu_load_state": (ct.c_int, [_vp, ct.c_int, _vp]),
+    "nsb_gpu_stats": (ct.c_int, [_vp, _i32]),
+    "nsb_gpu_take_events": (ct.c_longlong, [_vp]),
+}
+
+
+def library(path=None):
+    """Load libns_b200.so (built by neural-selection_b200/build.py)."""
+    global _lib
+    if _lib is None or path is not None:
+        p = Path(path) if path else LIB_PATH
+        if not p.exists():
+            raise RuntimeError(f"{p.name} is not built; run neural-selection_b200/build.py (needs nvcc)")
+        lib = ct.CDLL(str(p))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def _err(lib):
+    return lib.ns_error().decode()
+
+
+NW, SW = 32, 20
+STATS = ("brains", "units", "big_units", "neurons", "synapses", "heavy", "max_unit_neurons", "grid", "block",
+         "smem_bytes", "ctas_per_sm")
+
+
+class Brain:
+    """One brain behind ns_create/ns_reset/ns_step (stepped on the GPU)."""
+
+    def __init__(self, neuron_rows, synapse_rows, motors, channels, max_delay=8):
+        self.lib = library()
+        ng = np.ascontiguousarray(neuron_rows, np.float32)
+        sg = np.ascontiguousarray(synapse_rows, np.float32).reshape(-1, 11)
+        mo = np.ascontiguousarray(motors, np.int32)
+        self.count, self.edges, self.outputs, self.channels = len(ng), len(sg), len(mo), channels
+        sgp = sg if len(sg) else np.zeros((1, 11), np.float32)
+        if max_delay == 8:
+            self.ptr = self.lib.ns_create(self.count, self.edges, channels, self.outputs, _p(ng, _f), _p(sgp, _f),
+                                          _p(mo, _i32))
+        else:
+            self.ptr = self.lib.nsb_create_ext(self.count, self.edges, channels, self.outputs, _p(ng, _f),
+                                               _p(sgp, _f), _p(mo, _i32), max_delay)
+        if not self.ptr:
+            raise ValueError(_err(self.lib))
+
+    def original_indices(self, neurons, synapses):
+        n = np.ascontiguousarray(neurons, np.uint32)
+        s = np.ascontiguousarray(synapses, np.uint32) if len(synapses) else np.zeros(1, np.uint32)
+        self.lib.ns_original_indices(self.ptr, _p(n, _u32), _p(s, _u32))
+
+    def reset(self, seed):
+        self.lib.ns_reset(self.ptr, ct.c_uint32(int(seed) & 0xFFFFFFFF))
+
+    def step(self, inputs, ticks=16, gain=230.0):
+        x = np.ascontiguousarray(inputs, np.float32)
+        out = np.zeros(self.outputs, np.float32)
+        if self.lib.ns_step(self.ptr, _p(x, _f), int(ticks), float(gain), _p(out, _f)):
+            raise RuntimeError(_err(self.lib))
+        return out
+
+    def dump(self):
+        nw = np.zeros((self.count, NW), np.uint32)
+        sw = np.zeros((max(self.edges, 1), SW), np.uint32)
+        t = ct.c_int64(0)
+        if self.lib.nsb_dump(self.ptr, _p(nw, _u32), _p(sw, _u32), ct.byref(t)):
+            raise RuntimeError(_err(self.lib))
+        return nw, sw[: self.edges], t.value
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            self.lib.ns_destroy(self.ptr)
+            self.ptr = None
+
+    __del__ = close
+
+
+class GpuBatch:
+    """A device batch behind ns_gpu_create/ns_gpu_reset/ns_gpu_step."""
+
+    def __init__(self, ptr, brains, channels, outputs, sizes=None):
+        self.lib = library()
+        self.ptr = ptr
+        self.count, self.channels, self.outputs = brains, channels, outputs
+        self.sizes = sizes
+        self._keep = None
+
+    @classmethod
+    def from_brains(cls, brains, max_delay=8, block=0):
+        lib = library()
+        arr = (ct.c_void_p * len(brains))(*[b.ptr for b in brains])
+        if max_delay == 8 and block == 0:
+            ptr = lib.ns_gpu_create(arr, len(brains))
+        else:
+            ptr = lib.nsb_gpu_create_ext(arr, len(brains), max_delay, block)
+        if not ptr:
+            raise RuntimeError(_err(lib))
+        sizes = [(b.count, b.edges) for b in brains]
+        return cls(ptr, len(brains), brains[0].channels, brains[0].outputs, sizes)
+
+    @classmethod
+    def from_rows(cls, batch, block=0):
+        """From a workloads.Batch of concatenated ABI rows."""
+        lib = library()
+        no = np.ascontiguousarray(batch.neuron_offsets, np.int64)
+        so = np.ascontiguousarray(batch.synapse_offsets, np.int64)
+        ng = np.ascontiguousarray(batch.neuron_rows, np.float32)
+        sg = np.ascontiguousarray(batch.synapse_rows, np.float32)
+        if len(sg) == 0:
+            sg = np.zeros((1, 11), np.float32)
+        mo = np.ascontiguousarray(batch.motors, np.int32)
+        ptr = lib.nsb_gpu_create_rows(batch.brains, _p(no, _i64), _p(so, _i64), _p(ng, _f), _p(sg, _f),
+                                      _p(mo, _i32), batch.channels, batch.outputs, batch.max_delay, block)
+        if not ptr:
+            raise RuntimeError(_err(lib))
+        sizes = list(zip(np.diff(no).tolist(), np.diff(so).tolist()))
+        return cls(ptr, batch.brains, batch.channels, batch.outputs, sizes)
+
+    def reset(self, seeds, mask=None):
+        seeds = np.ascontiguousarray(seeds, np.uint32)
+        mask = np.ones(self.count, np.uint8) if mask is None else np.ascontiguousarray(mask, np.uint8)
+        if seeds.shape != (self.count,) or mask.shape != (self.count,):
+            raise ValueError("Reset dimensions differ")
+        if self.lib.ns_gpu_reset(self.ptr, _p(mask, _u8), _p(seeds, _u32)):
+            raise RuntimeError(_err(self.lib))
+
+    def step(self, inputs, mask=None, ticks=16, gain=230.0):
+        x = np.ascontiguousarray(inputs, np.float32)
+        mask = np.ones(self.count, np.uint8) if mask is None else np.ascontiguousarray(mask, np.uint8)
+        if x.shape != (self.count, self.channels) or mask.shape != (self.count,):
+            raise ValueError("Batch dimensions differ")
+        out = np.zeros((self.count, self.outputs), np.float32)
+        status = np.zeros(self.count, np.int32)
+        if self.lib.ns_gpu_step(self.ptr, _p(x, _f), _p(mask, _u8), int(ticks), float(gain), _p(out, _f),
+                                _p(status, _i32)):
+            raise RuntimeError(_err(self.lib))
+        return out, status
+
+    def step_device(self, d_input, d_mask, ticks, gain, d_output, d_status, stream=0):
+        if self.lib.nsb_gpu_step_device(self.ptr, d_input, d_mask, int(ticks), float(gain), d_output, d_status,
+                                        stream):
+            raise RuntimeError(_err(self.lib))
+
+    def step_graph(self, ticks=16, gain=230.0, stream=0):
+        if self.lib.nsb_gpu_step_graph(self.ptr, int(ticks), float(gain), stream):
+            raise RuntimeError(_err(self.lib))
+
+    def upload(self, inputs=None, mask=None):
+        x = None if inputs is None else np.ascontiguousarray(inputs, np.float32)
+        m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+        if self.lib.nsb_gpu_upload(self.ptr, None if x is None else _p(x, _f), None if m is None else _p(m, _u8)):
+            raise RuntimeError(_err(self.lib))
+
+    def download(self):
+        out = np.zeros((self.count, self.outputs), np.float32)
+        status = np.zeros(self.count, np.int32)
+        if self.lib.nsb_gpu_download(self.ptr, _p(out, _f), _p(status, _i32)):
+            raise RuntimeError(_err(self.lib))
+        return out, status
+
+    def buffer(self, which):
+        return self.lib.nsb_gpu_buffer(self.ptr, {"input": 0, "mask": 1, "output": 2, "status": 3}[which])
+
+    def dump(self, brain):
+        n, e = self.sizes[brain]
+        nw = np.zeros((n, NW), np.uint32)
+        sw = np.zeros((max(e, 1), SW), np.uint32)
+        t = ct.c_int64(0)
+        if self.lib.nsb_gpu_dump(self.ptr, brain, _p(nw, _u32), _p(sw, _u32), ct.byref(t)):
+            raise RuntimeError(_err(self.lib))
+        return nw, sw[:e], t.value
+
+    def load_state(self, brain, handle):
+        if self.lib.nsb_gpu_load_state(self.ptr, brain, handle):
+            raise RuntimeError(_err(self.lib))
+
+    def stats(self):
+        out = np.zeros(16, np.int32)
+        n = self.lib.nsb_gpu_stats(self.ptr, _p(out, _i32))
+        return dict(zip(STATS, out[:n].tolist()))
+
+    def take_events(self):
+        v = self.lib.nsb_gpu_take_events(self.ptr)
+        if v < 0:
+            raise RuntimeError(_err(self.lib))
+        return int(v)
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            self.lib.ns_gpu_destroy(self.ptr)
+            self.ptr = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    __del__ = close

@@ -1,0 +1,158 @@
+"""GPU parity: the CUDA engine, called through the C ABI (libns_b200.so),
+against the C oracle with correctly rounded exp/log — bit-exact in every state
+word, motor output and status, over multi-call runs with masks and resets.
+The oracle itself is pinned bit-exactly to the reference's own host executor
+(tests/test_oracle.py, tests/test_golden.py)."""
+import numpy as np
+import pytest
+
+from oracle.pyoracle import OracleBrain
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracles(batch, delay):
+    out = []
+    for i in range(batch.brains):
+        ng, sg, mo = batch.brain(i)
+        out.append(OracleBrain(ng, sg, mo, batch.channels, delay))
+    return out
+
+
+def _assert_brain_equal(gpu, ora, i, what):
+    gn, gs, gt = gpu.dump(i)
+    on, os_, ot = ora.dump()
+    assert gt == ot, f"{what}: brain {i} tick {gt} != {ot}"
+    bad = np.argwhere(gn != on)
+    assert bad.size == 0, f"{what}: brain {i} neuron words differ at {bad[:6].tolist()}"
+    bad = np.argwhere(gs != os_)
+    assert bad.size == 0, f"{what}: brain {i} synapse words differ at {bad[:6].tolist()}"
+
+
+def run_parity(nsb, batch, calls, ticks=16, mask_fn=None, reset_at=(), seeds=None, check_every=1, block=0,
+               gain=None):
+    delay = batch.max_delay
+    gain = batch.gain if gain is None else gain
+    gpu = nsb.GpuBatch.from_rows(batch, block=block)
+    ora = _oracles(batch, delay)
+    seeds = np.arange(batch.brains, dtype=np.uint32) * 17 + 20 if seeds is None else seeds
+    gpu.reset(seeds)
+    for i, o in enumerate(ora):
+        o.reset(int(seeds[i]))
+    inputs = batch.inputs
+    for c in range(calls):
+        mask = np.ones(batch.brains, np.uint8) if mask_fn is None else mask_fn(c)
+        if c in reset_at:
+            rmask = (np.arange(batch.brains) % 3 == c % 3).astype(np.uint8)
+            gpu.reset(seeds + c, rmask)
+            for i, o in enumerate(ora):
+                if rmask[i]:
+                    o.reset(int(seeds[i] + c))
+        out, status = gpu.step(inputs, mask, ticks, gain)
+        for i, o in enumerate(ora):
+            if mask[i]:
+                rc, oo, _ = o.step(inputs[i], ticks, gain, stop_on_nonfinite=False)
+                assert status[i] == rc, f"call {c} brain {i} status {status[i]} != {rc}"
+                np.testing.assert_array_equal(out[i], oo, err_msg=f"call {c} brain {i} outputs")
+            else:
+                assert not out[i].any() and status[i] == 0
+        if (c + 1) % check_every == 0 or c == calls - 1:
+            for i, o in enumerate(ora):
+                _assert_brain_equal(gpu, o, i, f"call {c}")
+    return gpu, ora
+
+
+def test_parity_mix_every_profile_and_cell_type(nsb):
+    batch = nsb.workloads.parity_mix(brains=16)
+    gpu, _ = run_parity(nsb, batch, calls=8, mask_fn=lambda c: np.array(
+        [1 if (i + c) % 4 else 0 for i in range(batch.brains)], np.uint8), reset_at=(3, 6))
+    gpu.close()
+
+
+def test_plain_small_2000_ticks_bitexact(nsb):
+    batch = nsb.workloads.plain_small(brains=16)
+    gpu, ora = run_parity(nsb, batch, calls=125, check_every=25)
+    assert sum(o.dump()[0][:, 26].astype(np.int64).sum() for o in ora) > 0
+
+
+def test_extended_delays_and_large_brains(nsb):
+    """Delays up to 16 ms (ring of 17 in the oracle) and brains above the CTA
+    size, which take the multi-neuron-per-thread path."""
+    batch = nsb.workloads.batched_uneven(brains=48, total_neurons=48 * 160, total_synapses=48 * 320)
+    assert max(n for n, _ in zip(np.diff(batch.neuron_offsets), range(99))) > 256
+    gpu, _ = run_parity(nsb, batch, calls=6, check_every=2)
+    st = gpu.stats()
+    assert st["big_units"] >= 1
+
+
+def test_block_128_matches(nsb):
+    batch = nsb.workloads.parity_mix(brains=10, heavy_types=False)
+    run_parity(nsb, batch, calls=5, block=128)
+
+
+def test_single_brain_ns_step(nsb):
+    batch = nsb.workloads.parity_mix(brains=4)
+    for i in range(4):
+        ng, sg, mo = batch.brain(i)
+        b = nsb.Brain(ng, sg, mo, batch.channels)
+        o = OracleBrain(ng, sg, mo, batch.channels, 8)
+        on = np.arange(len(ng), dtype=np.uint32) * 3 + 1
+        os_ = np.arange(len(sg), dtype=np.uint32) * 5 + 2
+        b.original_indices(on, os_); o.original_indices(on, os_)
+        b.reset(2 ** 31 + 47); o.reset(2 ** 31 + 47)
+        for c in range(6):
+            out = b.step(batch.inputs[i], 1 + 3 * c, 150.0)
+            rc, oo, _ = o.step(batch.inputs[i], 1 + 3 * c, 150.0)
+            assert rc == 0
+            np.testing.assert_array_equal(out, oo)
+        gn, gs, gt = b.dump()
+        on_, os2, ot = o.dump()
+        np.testing.assert_array_equal(gn, on_)
+        np.testing.assert_array_equal(gs, os2)
+        assert gt == ot
+        b.close()
+
+
+def test_nonfinite_voltage_reports_status(nsb):
+    batch = nsb.workloads.parity_mix(brains=3, heavy_types=False)
+    gpu = nsb.GpuBatch.from_rows(batch)
+    ora = _oracles(batch, 8)
+    gpu.reset(np.arange(3, dtype=np.uint32))
+    for i, o in enumerate(ora):
+        o.reset(i)
+    out, status = gpu.step(batch.inputs, None, 4, 3.0e38)
+    for i, o in enumerate(ora):
+        rc, oo, _ = o.step(batch.inputs[i], 4, 3.0e38, stop_on_nonfinite=False)
+        assert status[i] == rc
+    assert (status == -1).any()
+
+
+def test_validation_messages(nsb):
+    batch = nsb.workloads.parity_mix(brains=2, heavy_types=False)
+    gpu = nsb.GpuBatch.from_rows(batch)
+    gpu.reset(np.zeros(2, np.uint32))
+    with pytest.raises(RuntimeError, match="Invalid neural integration interval"):
+        gpu.step(batch.inputs, None, 0)
+    bad = batch.inputs.copy(); bad[0, 0] = 1.5
+    with pytest.raises(RuntimeError, match="Invalid encoded observation"):
+        gpu.step(bad, None, 4)
+    # a masked-out brain's observation is not validated (gym_adapter/gpu.cu:324)
+    gpu.step(bad, np.array([0, 1], np.uint8), 4)
+
+
+def test_graph_replay_matches_host_step(nsb):
+    batch = nsb.workloads.plain_small(brains=8)
+    a = nsb.GpuBatch.from_rows(batch)
+    b = nsb.GpuBatch.from_rows(batch)
+    seeds = np.arange(8, dtype=np.uint32)
+    a.reset(seeds); b.reset(seeds)
+    b.upload(batch.inputs, np.ones(8, np.uint8))
+    for _ in range(5):
+        out_a, st_a = a.step(batch.inputs, None, 16, 230.0)
+        b.step_graph(16, 230.0)
+        out_b, st_b = b.download()
+        np.testing.assert_array_equal(out_a, out_b)
+        np.testing.assert_array_equal(st_a, st_b)
+    for i in range(8):
+        np.testing.assert_array_equal(a.dump(i)[0], b.dump(i)[0])
+        np.testing.assert_array_equal(a.dump(i)[1], b.dump(i)[1])
