@@ -102,6 +102,62 @@ lines.append("")
 # required, only a fixed comparison constant).
 lines.append(f"#define NSX_SQRT2 {hx(rn(TWO.sqrt()))}")
 
+# ---- binary32 float-float fast path of exp ----
+import struct
+
+
+def rnf(v):
+    """Round a Decimal to binary32 (via the correctly rounded binary64, then
+    exactly re-rounded with ties-to-even on the 24-bit significand)."""
+    d = Decimal(v)
+    if d == 0:
+        return 0.0
+    # exact binary32 rounding of an arbitrary decimal
+    import math
+    sign = -1 if d < 0 else 1
+    a = abs(d)
+    e = int(math.floor(float(a.ln() / LN2)))
+    while Decimal(2) ** e > a:
+        e -= 1
+    while Decimal(2) ** (e + 1) <= a:
+        e += 1
+    scale = Decimal(2) ** (23 - e)
+    m = a * scale
+    mi = int(m)
+    frac = m - mi
+    if frac > Decimal("0.5") or (frac == Decimal("0.5") and mi % 2 == 1):
+        mi += 1
+    return sign * float(Decimal(mi) / scale)
+
+
+def hxf(x):
+    return float.hex(x) + "f"
+
+
+tabf = []
+for j in range(128):
+    v = TWO ** (Decimal(j) / 128)
+    hi = rnf(v)
+    lo = rnf(v - Decimal(hi))
+    tabf += [hi, lo]
+lines.append("/* 2^(j/128) as binary32 pairs (hi, lo), j = 0..127 */")
+lines.append("#define NSX_EXP2F_128_TABLE \\")
+for i in range(0, 256, 4):
+    chunk = ", ".join(hxf(v) for v in tabf[i:i + 4])
+    lines.append("    " + chunk + (", \\" if i + 4 < 256 else ""))
+L = LN2 / 128
+# L1: ln2/128 truncated to 10 significant bits (k*L1 exact for |k| < 2^14)
+import math
+m, e = math.frexp(float(L))
+L1 = math.ldexp(math.floor(m * 2 ** 10) / 2 ** 10, e)
+L2 = rnf(L - Decimal(L1))
+L3 = rnf(L - Decimal(L1) - Decimal(L2))
+lines.append(f"#define NSX_F_INV_LN2_128 {hxf(rnf(Decimal(128) / LN2))}")
+lines.append(f"#define NSX_F_LN2_128_A {hxf(L1)}")
+lines.append(f"#define NSX_F_LN2_128_B {hxf(L2)}")
+lines.append(f"#define NSX_F_LN2_128_C {hxf(L3)}")
+lines.append("")
+
 out = Path(__file__).with_name("ns_crmath_consts.h")
 out.write_text("\n".join(lines) + "\n")
 print("wrote", out)

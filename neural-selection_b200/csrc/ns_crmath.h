@@ -36,8 +36,10 @@
 
 #if defined(__CUDACC__)
 #define NSX_HD __host__ __device__ __forceinline__
+#define NSX_COLD __host__ __device__ __noinline__
 #else
 #define NSX_HD static inline
+#define NSX_COLD static
 #include <string.h>
 #include <math.h>
 #endif
@@ -163,7 +165,9 @@ NSX_HD bool near_midpoint(double y, uint64_t margin) {
 static const double kInvFactDD_h[2 * NSX_INV_FACT_COUNT] = {NSX_INV_FACT_DD};
 static const double kInvOddDD_h[2 * NSX_INV_ODD_COUNT] = {NSX_INV_ODD_DD};
 static const double kExp2Tab_h[128] = {NSX_EXP2_128_TABLE};
+static const float kExp2F_h[256] = {NSX_EXP2F_128_TABLE};
 #if defined(__CUDACC__)
+static __device__ const float kExp2F_d[256] = {NSX_EXP2F_128_TABLE};
 static __device__ const double kInvFactDD_d[2 * NSX_INV_FACT_COUNT] = {NSX_INV_FACT_DD};
 static __device__ const double kInvOddDD_d[2 * NSX_INV_ODD_COUNT] = {NSX_INV_ODD_DD};
 static __device__ const double kExp2Tab_d[128] = {NSX_EXP2_128_TABLE};
@@ -182,6 +186,13 @@ NSX_HD const double *inv_odd_dd() {
     return kInvOddDD_h;
 #endif
 }
+NSX_HD const float *exp2f_table() {
+#if defined(__CUDA_ARCH__)
+    return kExp2F_d;
+#else
+    return kExp2F_h;
+#endif
+}
 NSX_HD const double *exp2_table() {
 #if defined(__CUDA_ARCH__)
     return kExp2Tab_d;
@@ -191,7 +202,7 @@ NSX_HD const double *exp2_table() {
 }
 
 // exp(x) for -104 < x < 88.8 in double-double, rounded to binary32.
-NSX_HD float expf_slow(float x) {
+NSX_COLD float expf_slow(float x) {
     double xd = (double)x;
     double md = round_shift(xd * NSX_INV_LN2);
     // r = x - m ln2 with ln2 = A + B + C; m*A and m*B are exact.
@@ -240,11 +251,66 @@ NSX_HD float expf_cr_tab(float x, const double *tab) {
     return (float)y;
 }
 
+NSX_HD float sfma(float a, float b, float c) {
+#if defined(__CUDA_ARCH__)
+    return __fmaf_rn(a, b, c);
+#else
+    return fmaf(a, b, c);
+#endif
+}
+
+// Binary64 path, out of line on the device (used for the rare arguments the
+// binary32 fast path below cannot decide).
+NSX_COLD float expf_cr_wide(float x) { return expf_cr_tab(x, exp2_table()); }
+
+// Correctly rounded exp, binary32 fast path. `tabf` is NSX_EXP2F_128_TABLE
+// (2^(j/128) as binary32 hi/lo pairs). Float-float evaluation on the FP32
+// pipes: x = k ln2/128 + r (Cody-Waite with a 10-bit first constant, so the
+// first product is exact, and an error-free product for the second),
+// exp(x) = 2^(k>>7) (T_hi + T_lo)(1 + r + q(r)); relative error below 2^-41.
+// The result is returned only if it is at least 2^-38 (relative) away from a
+// rounding midpoint; otherwise, and outside [-86, 88.5] (results near the
+// normal range limits, NaN, infinities), the binary64 path decides.
+NSX_HD float expf_cr_ff(float x, const float *tabf) {
+    if (!(x >= -86.0f && x <= 88.5f)) return expf_cr_wide(x);
+    const float shifter = 0x1.8p23f;
+    const float t = sfma(x, NSX_F_INV_LN2_128, shifter);
+    const int ki = (int)fbits(t) - 0x4B400000;
+    const float kf = t - shifter;
+    const float r1 = sfma(-kf, NSX_F_LN2_128_A, x);      // exact
+    const float p = kf * NSX_F_LN2_128_B;
+    const float pe = sfma(kf, NSX_F_LN2_128_B, -p);       // exact error of p
+    const float rh = r1 - p;                              // two-sum(r1, -p)
+    const float bb = rh - r1;
+    const float re = (r1 - (rh - bb)) + (-p - bb);
+    const float rl = (re - pe) - kf * NSX_F_LN2_128_C;
+    float h = sfma(rh, 1.0f / 120.0f, 1.0f / 24.0f);
+    h = sfma(rh, h, 1.0f / 6.0f);
+    h = sfma(rh, h, 0.5f);
+    const float q = (rh * rh) * h;                        // e^r - 1 - r, |q| < 2^-17
+    const float sm = sfma(rh, rl, rl) + q;                // rl (1 + rh) + q
+    const int j = ki & 127;
+    const float th = tabf[2 * j], tl = tabf[2 * j + 1];
+    const float ph = th * rh;
+    const float pl = sfma(th, rh, -ph);
+    const float low = sfma(th, sm, sfma(tl, rh, tl)) + pl;
+    const float sh = th + ph;                             // fast two-sum, |th| > |ph|
+    const float sl = ph - (sh - th);
+    const float c = sl + low;
+    const float y = sh + c;
+    const float d = (sh - y) + c;                         // residual below ulp(y)/2
+    const uint32_t yb = fbits(y);
+    const float half = bitsf((yb & 0x7f800000u) - (24u << 23));   // ulp(y)/2
+    const float gap = half - fabsf(d);
+    if ((yb & 0x007fffffu) == 0u || gap <= half * 0x1p-14f) return expf_cr_wide(x);
+    return bitsf((uint32_t)((int)yb + (ki >> 7) * (1 << 23)));
+}
+
 // Correctly rounded exp using the built-in table of the calling side.
-NSX_HD float expf_cr(float x) { return expf_cr_tab(x, exp2_table()); }
+NSX_HD float expf_cr(float x) { return expf_cr_ff(x, exp2f_table()); }
 
 // log(x) for finite x > 0, x != 1, in double-double, rounded to binary32.
-NSX_HD float logf_slow(double md, int e) {
+NSX_COLD float logf_slow(double md, int e) {
     // s = (m-1)/(m+1); m-1 and m+1 are exact.
     dd s = dd_div_d(md - 1.0, md + 1.0);
     dd z = dd_mul(s, s);

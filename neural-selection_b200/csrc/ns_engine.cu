@@ -47,6 +47,10 @@ namespace nsb {
         if (e_ != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e_)); \
     } while (0)
 
+#ifndef NSB_MIN_CTAS
+#define NSB_MIN_CTAS 2   // CTAs per SM the light kernel's register budget is sized for
+#endif
+
 constexpr int kMetaCap = 6144;       // synapse meta words cached in shared memory per unit
 constexpr int kMaxUnitBrains = 128;  // brains packed into one small unit
 constexpr int kMaxBrainNeurons = 16384;
@@ -65,14 +69,12 @@ struct Pools {
     uint32_t *sstate;        // E x 16
     uint8_t *sarrived;       // E
     int16_t *slastp;         // E (-1 between calls)
-    const int *bn0, *be0;
     int64_t *btick;
     const int *bmotor;       // B x outputs, global neuron index
     const int4 *units;       // {n0, nn, e0, ne}
     const int2 *unitb;       // {first entry in ubrain, nb}
     const int *ubrain;       // unit brain lists (caller brain indices), pool order
-    int n_units, channels, outputs, hw;
-    int *queue;
+    int channels, outputs, hw;
     unsigned long long *events;
 };
 
@@ -124,12 +126,31 @@ __device__ __forceinline__ void load_gene(const float4 *g4, float (&g)[16]) {
     g[8] = c.x; g[9] = c.y; g[10] = c.z; g[11] = c.w; g[12] = d.x; g[13] = d.y; g[14] = d.z; g[15] = d.w;
 }
 
+// Stochastic release of one arriving synapse (event path).
+__device__ __forceinline__ float release_event(uint32_t *sstate, const uint32_t *sgene, int e, int64_t tick,
+                                               const float *tab) {
+    uint32_t *z = sstate + (size_t)e * Z_WORDS;
+    const float *y = reinterpret_cast<const float *>(sgene + (size_t)e * Y_WORDS);
+    SynRelease r;
+    r.w = __uint_as_float(z[Z_W]); r.ru = __uint_as_float(z[Z_RU]); r.slow = __uint_as_float(z[Z_SLOW]);
+    r.ready = ((uint64_t)z[Z_READYHI] << 32) | z[Z_READYLO];
+    r.rng = z[Z_RNG]; r.last = (int)z[Z_LAST];
+    const float rel = release(y, r, tick, tab);
+    z[Z_RU] = __float_as_uint(r.ru); z[Z_SLOW] = __float_as_uint(r.slow);
+    z[Z_READYLO] = (uint32_t)r.ready; z[Z_READYHI] = (uint32_t)(r.ready >> 32);
+    z[Z_RNG] = r.rng; z[Z_LAST] = (uint32_t)r.last;
+    return rel;
+}
+
 // Delivery + integration of one neuron for local tick t. Returns the
-// postsynaptic modulator bits and the number of arrivals.
+// postsynaptic modulator bits and the number of arrivals. HEAVY builds also
+// integrate the LP, Prinz and LFS cell types (out-of-line calls, which cost
+// registers, so units without such cells use the light build).
+template <bool HEAVY>
 __device__ __forceinline__ void deliver_and_integrate(
     const Pools &P, const float (&g)[16], uint32_t flags, int ib, int ie, int e0, const uint32_t *meta,
-    const uint32_t *hist, int t, int64_t tick0, float ampa, float level, float gain, NeuronRegs &s, int xidx,
-    int *status, const PhysConst &K, const double *tab, uint32_t &mod_out, int &narr_out) {
+    const uint32_t *hist, int t, int64_t tick0, float ampa, float level, float gain, NeuronRegs &s, int n,
+    int *status, const float *tab, uint32_t &mod_out, int &narr_out) {
     float e0s = 0.0f, e1s = 0.0f, e2s = 0.0f, e3s = 0.0f, inh = 0.0f;
     uint32_t mod = 0;
     int narr = 0;
@@ -139,20 +160,11 @@ __device__ __forceinline__ void deliver_and_integrate(
         if (!arrives(m, t, tick0, hist, P.hw)) continue;
         ++narr;
         const uint32_t kind = (m >> M_KIND_SHIFT) & 3u;
-        uint32_t *z = P.sstate + (size_t)e * Z_WORDS;
         if (kind == KIND_INH) {             // inhibitory source: weight, no release
-            inh += __uint_as_float(z[Z_W]);
+            inh += __uint_as_float(P.sstate[(size_t)e * Z_WORDS + Z_W]);
             continue;
         }
-        const float *y = reinterpret_cast<const float *>(P.sgene + (size_t)e * Y_WORDS);
-        SynRelease r;
-        r.w = __uint_as_float(z[Z_W]); r.ru = __uint_as_float(z[Z_RU]); r.slow = __uint_as_float(z[Z_SLOW]);
-        r.ready = ((uint64_t)z[Z_READYHI] << 32) | z[Z_READYLO];
-        r.rng = z[Z_RNG]; r.last = (int)z[Z_LAST];
-        const float rel = release(y, r, tick, tab);
-        z[Z_RU] = __float_as_uint(r.ru); z[Z_SLOW] = __float_as_uint(r.slow);
-        z[Z_READYLO] = (uint32_t)r.ready; z[Z_READYHI] = (uint32_t)(r.ready >> 32);
-        z[Z_RNG] = r.rng; z[Z_LAST] = (uint32_t)r.last;
+        const float rel = release_event(P.sstate, P.sgene, e, tick, tab);
         if (kind == KIND_MOD) {
             if (rel > 0) mod |= 1u << ((m >> M_MODID_SHIFT) & 3u);
         } else {
@@ -168,64 +180,80 @@ __device__ __forceinline__ void deliver_and_integrate(
     const uint32_t type = flags & NF_TYPE_MASK;
     float cur = 0.0f;
     if (flags & NF_HAS_INPUT) cur = type == 5 ? receptor_drive(g, flags, s, level) : gain * level;
-    if (type == 2 || type == 3 || type == 6) {
-        heavy_tick(g, type, P.xgene + (size_t)xidx * 16, P.xstate + (size_t)xidx * 16, s, cur, e0s, e1s, e2s, e3s,
-                   inh, K, tab);
+    if (HEAVY && (type == 2 || type == 3 || type == 6)) {
+        const int xidx = P.nxidx[n];
+        s = heavy_tick(reinterpret_cast<const float *>(P.ngene + (size_t)n * 4), type, P.xgene + (size_t)xidx * 16,
+                       P.xstate + (size_t)xidx * 16, s, cur, e0s, e1s, e2s, e3s, inh, tab);
     } else {
-        adex_tick(g, type, flags, s, cur, e0s, e1s, e2s, e3s, inh, K, tab);
+        adex_tick(g, type, flags, s, cur, e0s, e1s, e2s, e3s, inh, tab);
     }
     if (!isfinite(s.v)) *status = -1;
     mod_out = mod;
     narr_out = narr;
 }
 
-// Plasticity for the incoming synapses of one neuron at local tick t.
-__device__ __forceinline__ void plasticity_events(const Pools &P, int ib, int ie, int e0, const uint32_t *meta,
-                                                  const uint32_t *hist, int t, int64_t tick0, bool post,
-                                                  uint32_t mod, float depol, const PhysConst &K,
-                                                  const double *tab) {
+// Plasticity for the incoming synapses of one neuron at local tick t (runs
+// only on ticks with an arrival, a postsynaptic spike or a modulator event).
+__device__ __forceinline__ void plasticity_events(uint32_t *sstate, const uint32_t *sgene, int16_t *slastp, int hw,
+                                                  int ib, int ie, int e0, const uint32_t *meta, const uint32_t *hist,
+                                                  int t, int64_t tick0, bool post, uint32_t mod, float depol,
+                                                  const float *tab) {
     for (int e = ib; e < ie; ++e) {
         const uint32_t m = meta[e - e0];
         if (!(m & M_PLASTIC)) continue;
-        const bool arr = arrives(m, t, tick0, hist, P.hw);
+        const bool arr = arrives(m, t, tick0, hist, hw);
         const uint32_t prof = m >> M_PROF_SHIFT;
         uint32_t receptors = 0;
-        if (mod) receptors = (P.sgene[(size_t)e * Y_WORDS + Y_INFO] >> 8) & 0xffu;
+        if (mod) receptors = (sgene[(size_t)e * Y_WORDS + Y_INFO] >> 8) & 0xffu;
         if (!arr && !post && !mod_relevant(prof, receptors, mod)) continue;
-        const float w0 = __uint_as_float(P.sgene[(size_t)e * Y_WORDS + Y_W0]);
-        uint32_t *z = P.sstate + (size_t)e * Z_WORDS;
+        const float w0 = __uint_as_float(sgene[(size_t)e * Y_WORDS + Y_W0]);
+        uint32_t *z = sstate + (size_t)e * Z_WORDS;
         SynPlast p;
         load_plast(z, p);
-        const int last = P.slastp[e];
-        plasticity_quiet(prof, w0, p, t - last - 1, K);
-        plasticity_tick(prof, receptors, w0, p, arr, post, depol, mod, K, tab);
+        const int last = slastp[e];
+        plasticity_quiet(prof, w0, p, t - last - 1);
+        plasticity_tick(prof, receptors, w0, p, arr, post, depol, mod, tab);
         store_plast(z, p);
-        P.slastp[e] = (int16_t)t;
+        slastp[e] = (int16_t)t;
     }
 }
 
-__device__ __forceinline__ int find_brain(const int *starts, int nb, int local) {
-    int lo = 0, hi = nb - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (starts[mid] <= local) lo = mid; else hi = mid - 1;
+// End of call for the incoming synapses of one neuron: bring plastic synapses
+// to the last tick and record the last tick's arrivals.
+__device__ __forceinline__ void finish_synapses(const Pools &P, int ib, int ie, int e0, const uint32_t *meta,
+                                                const uint32_t *hist, int ticks, int64_t tick0) {
+    for (int e = ib; e < ie; ++e) {
+        const uint32_t m = meta[e - e0];
+        P.sarrived[e] = arrives(m, ticks - 1, tick0, hist, P.hw) ? 1 : 0;
+        if (m & M_PLASTIC) {
+            const int last = P.slastp[e];
+            const int q = ticks - 1 - last;
+            if (q > 0) {
+                uint32_t *z = P.sstate + (size_t)e * Z_WORDS;
+                SynPlast p;
+                load_plast(z, p);
+                plasticity_quiet(m >> M_PROF_SHIFT, __uint_as_float(P.sgene[(size_t)e * Y_WORDS + Y_W0]), p, q);
+                store_plast(z, p);
+            }
+            if (last >= 0) P.slastp[e] = -1;
+        }
     }
-    return lo;
 }
 
 extern __shared__ __align__(16) unsigned char g_smem[];
 
-__global__ void __launch_bounds__(256) tick_kernel(Pools P, const float *__restrict__ input,
+// One launch steps every unit of [unit_begin, unit_end) through `ticks`
+// ticks. Units are pulled from `queue` (reset to 0 before the launch).
+template <bool HEAVY>
+__global__ void __launch_bounds__(256, HEAVY ? 1 : NSB_MIN_CTAS) tick_kernel(Pools P, int unit_begin, int unit_end, int *queue,
+                                                   const float *__restrict__ input,
                                                    const uint8_t *__restrict__ mask, float *__restrict__ output,
-                                                   int *__restrict__ status, int ticks, float gain, PhysConst K) {
-    double *tab = reinterpret_cast<double *>(g_smem);                    // 128 doubles
-    int *s_meta_raw = reinterpret_cast<int *>(g_smem + 1024);
-    uint32_t *s_meta = reinterpret_cast<uint32_t *>(s_meta_raw);          // kMetaCap
+                                                   int *__restrict__ status, int ticks, float gain) {
+    float *tab = reinterpret_cast<float *>(g_smem);                      // 2^(j/128) hi/lo pairs
+    uint32_t *s_meta = reinterpret_cast<uint32_t *>(g_smem + 1024);       // kMetaCap
     uint32_t *hist = s_meta + kMetaCap;                                   // 32 * hw
     int *cnt = reinterpret_cast<int *>(hist + 32 * P.hw);                // 32 * hw (spike counts)
-    int *s_bn0 = cnt + 32 * P.hw;                                         // kMaxUnitBrains
-    int *s_be0 = s_bn0 + kMaxUnitBrains;
-    int64_t *s_tick = reinterpret_cast<int64_t *>(s_be0 + kMaxUnitBrains);
+    int64_t *s_tick = reinterpret_cast<int64_t *>(cnt + 32 * P.hw);      // kMaxUnitBrains
     int *s_mask = reinterpret_cast<int *>(s_tick + kMaxUnitBrains);
     int *s_bid = s_mask + kMaxUnitBrains;                                 // caller brain index
     __shared__ int s_unit;
@@ -233,22 +261,20 @@ __global__ void __launch_bounds__(256) tick_kernel(Pools P, const float *__restr
 
     const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarp = bs >> 5;
     {
-        const double *src = nsx::exp2_table();
-        for (int i = tid; i < 128; i += bs) tab[i] = src[i];
+        const float *src = nsx::exp2f_table();
+        for (int i = tid; i < 256; i += bs) tab[i] = src[i];
     }
     for (;;) {
-        if (tid == 0) { s_unit = atomicAdd(P.queue, 1); s_events = 0; }
+        if (tid == 0) { s_unit = unit_begin + atomicAdd(queue, 1); s_events = 0; }
         __syncthreads();
         const int u = s_unit;
-        if (u >= P.n_units) break;
+        if (u >= unit_end) break;
         const int4 U = P.units[u];
         const int2 UB = P.unitb[u];
         const int n0 = U.x, nn = U.y, e0 = U.z, ne = U.w, b0 = UB.x, nb = UB.y;
         for (int i = tid; i < nb; i += bs) {
             const int b = P.ubrain[b0 + i];
             s_bid[i] = b;
-            s_bn0[i] = P.bn0[b] - n0;
-            s_be0[i] = P.be0[b] - e0;
             const int64_t t0 = P.btick[b];
             s_tick[i] = t0;
             // last-arrival ticks are stored as int32: refuse to step past 2^31
@@ -267,29 +293,27 @@ __global__ void __launch_bounds__(256) tick_kernel(Pools P, const float *__restr
         if (slots == 1) {
             // ---- register path: one neuron per thread, state in registers --------
             const bool has = tid < nn;
-            const int bi = has ? find_brain(s_bn0, nb, tid) : 0;
+            const int n = n0 + tid;
+            const uint32_t flags = has ? P.nflags[n] : 0u;
+            const int bi = (int)((flags >> NF_SLOT_SHIFT) & NF_SLOT_MASK);
             const bool run = has && s_mask[bi] != 0;
             const int64_t tick0 = s_tick[bi];
-            const int n = n0 + tid;
             float g[16];
-            uint32_t flags = 0;
             NeuronRegs s = {};
             float log_ampa = 0.0f, ampa = 1.0f, level = 0.0f;
             uint32_t h0 = 0;
-            int ib = 0, ie = 0, xidx = -1, count = 0;
+            int ib = 0, ie = 0, count = 0;
             if (run) {
                 load_gene(P.ngene + (size_t)n * 4, g);
-                flags = P.nflags[n];
                 load_neuron(P.nstate + (size_t)n * S_WORDS, s, log_ampa, h0);
                 ampa = crexp(log_ampa, tab);
                 if (flags & NF_HAS_INPUT) level = input[(size_t)s_bid[bi] * P.channels + P.nsens[n]];
                 ib = P.inptr[n]; ie = P.inptr[n + 1];
-                xidx = P.nxidx[n];
             }
             const uint32_t rot = run ? rotr32(h0, (uint32_t)(tick0 & 31)) : 0u;
             for (int sl = 0; sl < 32; ++sl) {
                 const uint32_t w = __ballot_sync(0xffffffffu, (rot >> sl) & 1u);
-                if (lane == 0 && warp < P.hw) hist[sl * P.hw + warp] = w;
+                if (lane == 0) hist[sl * P.hw + warp] = w;
             }
             __syncthreads();
             int *status_ptr = status + s_bid[bi];
@@ -298,16 +322,17 @@ __global__ void __launch_bounds__(256) tick_kernel(Pools P, const float *__restr
                 int narr = 0;
                 if (run) {
                     if (flags & NF_ACTIVE) {
-                        deliver_and_integrate(P, g, flags, ib, ie, e0, meta, hist, t, tick0, ampa, level, gain, s, xidx,
-                                              status_ptr, K, tab, mod, narr);
+                        deliver_and_integrate<HEAVY>(P, g, flags, ib, ie, e0, meta, hist, t, tick0, ampa, level, gain,
+                                                     s, n, status_ptr, tab, mod, narr);
                     } else {
                         s.spike = 0;
                     }
                 }
                 const uint32_t w = __ballot_sync(0xffffffffu, run && s.spike);
-                if (lane == 0 && warp < P.hw) hist[(t & 31) * P.hw + warp] = w;
+                if (lane == 0) hist[(t & 31) * P.hw + warp] = w;
                 if (run && (s.spike || mod || narr))
-                    plasticity_events(P, ib, ie, e0, meta, hist, t, tick0, s.spike != 0, mod, s.depol, K, tab);
+                    plasticity_events(P.sstate, P.sgene, P.slastp, P.hw, ib, ie, e0, meta, hist, t, tick0,
+                                      s.spike != 0, mod, s.depol, tab);
                 count += run ? (int)s.spike : 0;
                 my_events += narr;
                 __syncthreads();
@@ -316,11 +341,12 @@ __global__ void __launch_bounds__(256) tick_kernel(Pools P, const float *__restr
                 if (flags & NF_ACTIVE) {
                     const int64_t t1 = tick0 + ticks;
                     log_ampa = homeostasis(flags & NF_TYPE_MASK, log_ampa, (float)ticks,
-                                           (float)s.total * 1000.0f / (float)(ticks > t1 ? (int64_t)ticks : t1), K);
+                                           (float)s.total * 1000.0f / (float)(ticks > t1 ? (int64_t)ticks : t1));
                 }
                 uint32_t L = 0;
                 for (int sl = 0; sl < 32; ++sl) L |= ((hist[sl * P.hw + warp] >> lane) & 1u) << sl;
                 store_neuron(P.nstate + (size_t)n * S_WORDS, s, log_ampa, rotl32(L, (uint32_t)(tick0 & 31)), 0u);
+                finish_synapses(P, ib, ie, e0, meta, hist, ticks, tick0);
             }
             if (has) cnt[tid] = count;
         } else {
@@ -367,15 +393,16 @@ __global__ void __launch_bounds__(256) tick_kernel(Pools P, const float *__restr
                             float g[16];
                             load_gene(P.ngene + (size_t)n * 4, g);
                             const float level = (flags & NF_HAS_INPUT) ? input[(size_t)s_bid[0] * P.channels + P.nsens[n]] : 0.0f;
-                            deliver_and_integrate(P, g, flags, ib, ie, e0, meta, hist, t, tick0, ampa, level, gain, s,
-                                                  P.nxidx[n], status_ptr, K, tab, mod, narr);
+                            deliver_and_integrate<HEAVY>(P, g, flags, ib, ie, e0, meta, hist, t, tick0, ampa, level,
+                                                         gain, s, n, status_ptr, tab, mod, narr);
                         } else {
                             s.spike = 0;
                         }
                         store_neuron(r, s, log_ampa, hw0, __float_as_uint(ampa));
                         spike = s.spike;
                         if (spike || mod || narr)
-                            plasticity_events(P, ib, ie, e0, meta, hist, t, tick0, spike != 0, mod, s.depol, K, tab);
+                            plasticity_events(P.sstate, P.sgene, P.slastp, P.hw, ib, ie, e0, meta, hist, t, tick0,
+                                              spike != 0, mod, s.depol, tab);
                         cnt[j] += (int)spike;
                         my_events += narr;
                     }
@@ -395,7 +422,7 @@ __global__ void __launch_bounds__(256) tick_kernel(Pools P, const float *__restr
                         const int total = (int)r[S_TOTAL];
                         const int64_t t1 = tick0 + ticks;
                         la = homeostasis(flags & NF_TYPE_MASK, la, (float)ticks,
-                                         (float)total * 1000.0f / (float)(ticks > t1 ? (int64_t)ticks : t1), K);
+                                         (float)total * 1000.0f / (float)(ticks > t1 ? (int64_t)ticks : t1));
                     }
                     uint32_t L = 0;
                     const int word = sl0 * nwarp + warp;
@@ -403,31 +430,11 @@ __global__ void __launch_bounds__(256) tick_kernel(Pools P, const float *__restr
                     r[S_LOGAMPA] = __float_as_uint(la);
                     r[S_HIST] = rotl32(L, (uint32_t)(tick0 & 31));
                     r[S_PAD] = 0u;
+                    finish_synapses(P, P.inptr[n], P.inptr[n + 1], e0, meta, hist, ticks, tick0);
                 }
             }
         }
         __syncthreads();
-        // ---- end of call: finish plasticity, record last-tick arrivals ---------------
-        for (int k = tid; k < ne; k += bs) {
-            const int bi = nb == 1 ? 0 : find_brain(s_be0, nb, k);
-            if (!s_mask[bi]) continue;
-            const int e = e0 + k;
-            const uint32_t m = meta[k];
-            const int64_t tick0 = s_tick[bi];
-            P.sarrived[e] = arrives(m, ticks - 1, tick0, hist, P.hw) ? 1 : 0;
-            if (m & M_PLASTIC) {
-                const int last = P.slastp[e];
-                const int q = ticks - 1 - last;
-                if (q > 0) {
-                    uint32_t *z = P.sstate + (size_t)e * Z_WORDS;
-                    SynPlast p;
-                    load_plast(z, p);
-                    plasticity_quiet(m >> M_PROF_SHIFT, __uint_as_float(P.sgene[(size_t)e * Y_WORDS + Y_W0]), p, q, K);
-                    store_plast(z, p);
-                }
-                if (last >= 0) P.slastp[e] = -1;
-            }
-        }
         // ---- motor outputs (spikes per call) and tick counters --------------------
         for (int i = tid; i < nb * P.outputs; i += bs) {
             const int bi = i / P.outputs, b = s_bid[bi];
@@ -574,68 +581,69 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
     if (nsum > (1ll << 30) || esum > (1ll << 30)) throw std::runtime_error("Pool exceeds 2^30 entries");
     n_neurons_ = (int)nsum; n_synapses_ = (int)esum;
 
-    // ---- work units: big brains alone, small ones best-fit decreasing ----
-    std::vector<int> order(n_brains_);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return brains[a].count > brains[b].count; });
+    // ---- work units ------------------------------------------------------------
+    // Brains with LP/Prinz/LFS cells go to units of their own (stepped by the
+    // heavy kernel). Within each group a brain above the CTA size is a unit of
+    // its own; smaller brains are packed best-fit decreasing.
+    auto is_heavy_type = [](unsigned char t) { return t == 2 || t == 3 || t == 6; };
+    std::vector<char> brain_heavy(n_brains_, 0);
+    for (int b = 0; b < n_brains_; ++b)
+        for (int j = 0; j < brains[b].count; ++j)
+            if (is_heavy_type(brains[b].genes[j].type)) { brain_heavy[b] = 1; break; }
     std::vector<std::vector<int>> unit_brains;
     std::vector<int> unit_fill;
-    std::multimap<int, int> open;   // remaining capacity -> unit
-    for (int b : order) {
-        const int n = brains[b].count;
-        if (n > block_) {
-            unit_brains.push_back({b});
-            unit_fill.push_back(n);
-            continue;
-        }
-        auto it = open.lower_bound(n);
-        if (it != open.end()) {
-            const int uidx = it->second;
-            open.erase(it);
-            unit_brains[uidx].push_back(b);
-            unit_fill[uidx] += n;
-            const int rem = block_ - unit_fill[uidx];
-            if (rem > 0 && (int)unit_brains[uidx].size() < kMaxUnitBrains) open.emplace(rem, uidx);
-        } else {
-            unit_brains.push_back({b});
-            unit_fill.push_back(n);
-            const int rem = block_ - n;
-            if (rem > 0) open.emplace(rem, (int)unit_brains.size() - 1);
+    std::vector<char> unit_heavy;
+    for (int group = 0; group < 2; ++group) {
+        std::vector<int> order;
+        for (int b = 0; b < n_brains_; ++b)
+            if (brain_heavy[b] == group) order.push_back(b);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return brains[a].count > brains[b].count; });
+        std::multimap<int, int> open;   // remaining capacity -> unit
+        for (int b : order) {
+            const int n = brains[b].count;
+            if (n > block_) {
+                unit_brains.push_back({b}); unit_fill.push_back(n); unit_heavy.push_back((char)group);
+                continue;
+            }
+            auto it = open.lower_bound(n);
+            if (it != open.end()) {
+                const int uidx = it->second;
+                open.erase(it);
+                unit_brains[uidx].push_back(b);
+                unit_fill[uidx] += n;
+                const int rem = block_ - unit_fill[uidx];
+                if (rem > 0 && (int)unit_brains[uidx].size() < kMaxUnitBrains) open.emplace(rem, uidx);
+            } else {
+                unit_brains.push_back({b}); unit_fill.push_back(n); unit_heavy.push_back((char)group);
+                const int rem = block_ - n;
+                if (rem > 0) open.emplace(rem, (int)unit_brains.size() - 1);
+            }
         }
     }
-    // queue order: by neuron count descending (big units first)
+    // queue order: light units then heavy units, each by neuron count descending
     std::vector<int> uorder(unit_brains.size());
     std::iota(uorder.begin(), uorder.end(), 0);
-    std::stable_sort(uorder.begin(), uorder.end(), [&](int a, int b) { return unit_fill[a] > unit_fill[b]; });
+    std::stable_sort(uorder.begin(), uorder.end(), [&](int a, int b) {
+        if (unit_heavy[a] != unit_heavy[b]) return unit_heavy[a] < unit_heavy[b];
+        return unit_fill[a] > unit_fill[b];
+    });
     n_units_ = (int)unit_brains.size();
+    n_light_units_ = 0;
+    for (int u : uorder) n_light_units_ += unit_heavy[u] ? 0 : 1;
 
-    // ---- pool layout ----
-    h_bn0_.assign(n_brains_, 0); h_bnn_.assign(n_brains_, 0); h_be0_.assign(n_brains_, 0); h_bne_.assign(n_brains_, 0);
-    std::vector<int4> units(n_units_);
-    std::vector<int2> unitb(n_units_);
-    std::vector<int> brain_order;   // brains in pool order
-    std::vector<int> brain_pos(n_brains_);
-    int ncur = 0, ecur = 0;
-    for (int ui = 0; ui < n_units_; ++ui) {
-        const auto &ub = unit_brains[uorder[ui]];
-        units[ui] = make_int4(ncur, 0, ecur, 0);
-        unitb[ui] = make_int2((int)brain_order.size(), (int)ub.size());
-        for (int b : ub) {
-            brain_pos[b] = (int)brain_order.size();
-            brain_order.push_back(b);
-            h_bn0_[b] = ncur; h_bnn_[b] = brains[b].count;
-            h_be0_[b] = ecur; h_bne_[b] = brains[b].edges;
-            ncur += brains[b].count; ecur += brains[b].edges;
-        }
-        units[ui].y = ncur - units[ui].x;
-        units[ui].w = ecur - units[ui].z;
-        max_unit_neurons_ = std::max(max_unit_neurons_, units[ui].y);
-        if (units[ui].y > block_) ++n_big_units_;
-        max_unit_brains_ = std::max(max_unit_brains_, (int)ub.size());
+    // ---- per-brain bookkeeping (caller order) ----
+    h_noff_.assign(n_brains_ + 1, 0);
+    h_soff_.assign(n_brains_ + 1, 0);
+    for (int b = 0; b < n_brains_; ++b) {
+        h_noff_[b + 1] = h_noff_[b] + brains[b].count;
+        h_soff_[b + 1] = h_soff_[b] + brains[b].edges;
     }
-    // Spike-ring words per tick: whole CTA-sized neuron slots (a big unit's
-    // threads write one word per warp per slot).
-    hw_ = ((std::max(max_unit_neurons_, block_) + block_ - 1) / block_) * (block_ / 32);
+    h_npos_.assign(n_neurons_, 0);
+    h_spos_.assign(n_synapses_, 0);
+    h_bunit_.assign(n_brains_, 0);
+    h_units_.assign(n_units_, make_int4(0, 0, 0, 0));
+    std::vector<int2> unitb(n_units_);
+    std::vector<int> brain_order;   // unit brain lists (caller indices), pool order
 
     // ---- per-neuron and per-synapse records ----
     std::vector<float> ngene((size_t)n_neurons_ * 16);
@@ -647,105 +655,149 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
     std::vector<int> inptr(n_neurons_ + 1, 0);
     std::vector<uint32_t> smeta(n_synapses_), sgene((size_t)n_synapses_ * Y_WORDS), sorig(n_synapses_);
     std::vector<int> sbrain(n_synapses_);
-    h_syn_orig_.assign(n_synapses_, 0);
-    h_syn_pool_.assign(n_synapses_, 0);
-    h_sinfo_.assign(n_synapses_, 0);
-    h_w0_.assign(n_synapses_, 0.0f);
+    std::vector<int> bmotor((size_t)n_brains_ * outputs);
+
+    int ncur = 0, ecur = 0;
     for (int ui = 0; ui < n_units_; ++ui) {
-        const int un0 = units[ui].x;
-        for (int k = 0; k < unitb[ui].y; ++k) {
-            const int b = brain_order[unitb[ui].x + k];
+        const auto &ub = unit_brains[uorder[ui]];
+        const int un0 = ncur, ue0 = ecur;
+        unitb[ui] = make_int2((int)brain_order.size(), (int)ub.size());
+        // Neuron order inside the unit: active before inactive, then by cell
+        // class (type 0 | types 1,4 | type 5 | LP/Prinz/LFS), then by which
+        // dendritic branches receive excitatory synapses, so that a warp's
+        // lanes take the same path through the integrator.
+        struct Key { int inactive, cls, bmask, slot, j; };
+        std::vector<Key> keys;
+        for (int slot = 0; slot < (int)ub.size(); ++slot) {
+            const int b = ub[slot];
             const BrainSpec &B = brains[b];
-            const int bn0 = h_bn0_[b], be0 = h_be0_[b];
-            for (int j = 0; j < B.count; ++j) {
-                const ref::NeuronGene &G = B.genes[j];
-                const int n = bn0 + j;
-                float *g = &ngene[(size_t)n * 16];
-                g[G_CAP] = G.cap; g[G_GL] = G.gl; g[G_EL] = G.el; g[G_VT] = G.vt;
-                g[G_SLOPE] = G.slope; g[G_A] = G.a; g[G_TAUW] = G.tau_w; g[G_B] = G.b;
-                g[G_VR] = G.vr; g[G_ADPB] = G.adp_b;
-                g[G_ADPDECAY] = G.adp_tau > 0 ? nsx::expf_cr(-0.25f / G.adp_tau) : 1.0f;
-                g[G_GLSLOPE] = G.gl * G.slope;
-                g[G_RECBASE] = G.rec_base; g[G_RECGAIN] = G.rec_gain; g[G_RECEVENT] = G.rec_event;
-                g[G_RECDECAY] = nsx::expf_cr(-1.0f / G.rec_decay);
-                if (G.type > 6) throw std::runtime_error("Invalid neuron gene");
-                uint32_t f = (uint32_t)G.type;
-                if (G.active) f |= NF_ACTIVE;
-                if (G.inh_tx) f |= NF_INH;
-                f |= (uint32_t)(G.modulator & 3u) << NF_MOD_SHIFT;
-                if (G.sensory_channel >= 0) f |= NF_GENE_SENS;
-                if (G.adp_tau > 0) f |= NF_ADP;
-                const int sens = B.sensory ? B.sensory[j] : -1;
-                if (sens >= 0) {
-                    if (sens >= channels) throw std::runtime_error("Invalid neuron gene");
-                    f |= NF_HAS_INPUT;
-                }
-                if (excitatory_type(G.type)) f |= NF_EXC_TYPE;
-                h_nflags_[n] = f;
-                nsens[n] = sens;
-                nbrain[n] = b;
-                norig[n] = B.orig_n ? B.orig_n[j] : (uint32_t)j;
-                if (G.type == 2 || G.type == 3 || G.type == 6) {
-                    h_nxidx_[n] = n_heavy_++;
-                    float xg[16] = {};
-                    if (G.type == 2) { xg[0] = G.lp.calcium; xg[1] = G.lp.calcium_k; xg[2] = G.lp.h; xg[3] = G.lp.leak; }
-                    if (G.type == 3) { for (int q = 0; q < 8; ++q) xg[q] = G.prinz.g[q]; xg[8] = G.prinz_leak; }
-                    xgene.insert(xgene.end(), xg, xg + 16);
-                }
-            }
-            // incoming CSR of this brain: stable counting sort by post
-            std::vector<int> cnt(B.count + 1, 0);
-            for (int j = 0; j < B.edges; ++j) ++cnt[B.conns[j].post + 1];
-            for (int j = 0; j < B.count; ++j) cnt[j + 1] += cnt[j];
-            std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+            h_bunit_[b] = ui;
+            brain_order.push_back(b);
+            std::vector<int> bmask(B.count, 0);
             for (int j = 0; j < B.edges; ++j) {
                 const ref::SynapseGene &C = B.conns[j];
-                const int e = be0 + pos[C.post]++;
                 const ref::NeuronGene &A = B.genes[C.pre], &Z = B.genes[C.post];
-                const bool live = C.active && A.active && Z.active;
-                const bool pair = !A.inh_tx && excitatory_type(A.type) && !A.modulator && !Z.inh_tx &&
-                                  excitatory_type(Z.type);
-                uint32_t kind = A.modulator ? KIND_MOD : (A.inh_tx ? KIND_INH : KIND_EXC);
-                const int pre_local = bn0 + C.pre - un0;
-                if (pre_local > 0xffff) throw std::runtime_error("Unit exceeds 65536 neurons");
-                if (C.plasticity > 7) throw std::runtime_error("Invalid synapse gene");
-                uint32_t m = (uint32_t)pre_local | ((uint32_t)C.delay << M_DELAY_SHIFT) |
-                             ((uint32_t)(C.branch & 3u) << M_BRANCH_SHIFT) | (kind << M_KIND_SHIFT) |
-                             ((uint32_t)((A.modulator ? A.modulator - 1 : 0) & 3u) << M_MODID_SHIFT) |
-                             ((uint32_t)C.plasticity << M_PROF_SHIFT);
-                if (live) m |= M_LIVE;
-                if (live && C.plasticity && pair) m |= M_PLASTIC;
-                smeta[e] = m;
-                const int sites = C.sites ? (C.sites > 64 ? 64 : C.sites) : 14;
-                uint32_t *y = &sgene[(size_t)e * Y_WORDS];
-                float yf[8] = {C.w0, C.U, C.trec, C.tfac, C.slow_rec, C.slow_depl, 0.0f, 0.0f};
-                std::memcpy(y, yf, sizeof yf);
-                y[Y_INFO] = (uint32_t)sites | ((uint32_t)C.receptors << 8);
-                h_sinfo_[e] = y[Y_INFO];
-                h_w0_[e] = C.w0;
-                sorig[e] = B.orig_s ? B.orig_s[j] : (uint32_t)j;
-                sbrain[e] = b;
-                h_syn_orig_[e] = j;
-                h_syn_pool_[be0 + j] = e;
+                if (C.active && A.active && Z.active && !A.modulator && !A.inh_tx) bmask[C.post] |= 1 << (C.branch & 3);
+            }
+            for (int j = 0; j < B.count; ++j) {
+                const unsigned char t = B.genes[j].type;
+                const int cls = is_heavy_type(t) ? 3 : (t == 0 ? 0 : (t == 5 ? 2 : 1));
+                keys.push_back({B.genes[j].active ? 0 : 1, cls, t == 0 ? bmask[j] : 0, slot, j});
             }
         }
-    }
-    // inptr[n] must be the start of neuron n's segment: rebuild as starts.
-    {
-        std::vector<int> starts(n_neurons_ + 1);
-        for (int b = 0; b < n_brains_; ++b) {
-            const int bn0 = h_bn0_[b], be0 = h_be0_[b];
-            std::vector<int> c(brains[b].count + 1, 0);
-            for (int j = 0; j < brains[b].edges; ++j) ++c[brains[b].conns[j].post + 1];
-            for (int j = 0; j < brains[b].count; ++j) c[j + 1] += c[j];
-            for (int j = 0; j <= brains[b].count; ++j) starts[bn0 + j] = be0 + c[j];
+        std::stable_sort(keys.begin(), keys.end(), [](const Key &a, const Key &b) {
+            if (a.inactive != b.inactive) return a.inactive < b.inactive;
+            if (a.cls != b.cls) return a.cls < b.cls;
+            if (a.bmask != b.bmask) return a.bmask < b.bmask;
+            if (a.slot != b.slot) return a.slot < b.slot;
+            return a.j < b.j;
+        });
+        for (size_t q = 0; q < keys.size(); ++q) {
+            const int b = ub[keys[q].slot];
+            h_npos_[h_noff_[b] + keys[q].j] = un0 + (int)q;
         }
-        starts[n_neurons_] = n_synapses_;
-        inptr.swap(starts);
+        // neuron records
+        for (size_t q = 0; q < keys.size(); ++q) {
+            const int slot = keys[q].slot, j = keys[q].j, b = ub[slot];
+            const BrainSpec &B = brains[b];
+            const ref::NeuronGene &G = B.genes[j];
+            const int n = un0 + (int)q;
+            float *g = &ngene[(size_t)n * 16];
+            g[G_CAP] = G.cap; g[G_GL] = G.gl; g[G_EL] = G.el; g[G_VT] = G.vt;
+            g[G_SLOPE] = G.slope; g[G_A] = G.a; g[G_TAUW] = G.tau_w; g[G_B] = G.b;
+            g[G_VR] = G.vr; g[G_ADPB] = G.adp_b;
+            g[G_ADPDECAY] = G.adp_tau > 0 ? nsx::expf_cr(-0.25f / G.adp_tau) : 1.0f;
+            g[G_GLSLOPE] = G.gl * G.slope;
+            g[G_RECBASE] = G.rec_base; g[G_RECGAIN] = G.rec_gain; g[G_RECEVENT] = G.rec_event;
+            g[G_RECDECAY] = nsx::expf_cr(-1.0f / G.rec_decay);
+            if (G.type > 6) throw std::runtime_error("Invalid neuron gene");
+            uint32_t f = (uint32_t)G.type;
+            if (G.active) f |= NF_ACTIVE;
+            if (G.inh_tx) f |= NF_INH;
+            f |= (uint32_t)(G.modulator & 3u) << NF_MOD_SHIFT;
+            if (G.sensory_channel >= 0) f |= NF_GENE_SENS;
+            if (G.adp_tau > 0) f |= NF_ADP;
+            const int sens = B.sensory ? B.sensory[j] : -1;
+            if (sens >= 0) {
+                if (sens >= channels) throw std::runtime_error("Invalid neuron gene");
+                f |= NF_HAS_INPUT;
+            }
+            if (excitatory_type(G.type)) f |= NF_EXC_TYPE;
+            f |= (uint32_t)slot << NF_SLOT_SHIFT;
+            h_nflags_[n] = f;
+            nsens[n] = sens;
+            nbrain[n] = b;
+            norig[n] = B.orig_n ? B.orig_n[j] : (uint32_t)j;
+            if (is_heavy_type(G.type)) {
+                h_nxidx_[n] = n_heavy_++;
+                float xg[16] = {};
+                if (G.type == 2) { xg[0] = G.lp.calcium; xg[1] = G.lp.calcium_k; xg[2] = G.lp.h; xg[3] = G.lp.leak; }
+                if (G.type == 3) { for (int r = 0; r < 8; ++r) xg[r] = G.prinz.g[r]; xg[8] = G.prinz_leak; }
+                xgene.insert(xgene.end(), xg, xg + 16);
+            }
+        }
+        // synapses: grouped by postsynaptic pool position, then original edge order
+        struct SKey { int post, j, b; };
+        std::vector<SKey> sk;
+        for (int slot = 0; slot < (int)ub.size(); ++slot) {
+            const int b = ub[slot];
+            for (int j = 0; j < brains[b].edges; ++j)
+                sk.push_back({h_npos_[h_noff_[b] + brains[b].conns[j].post], j, b});
+        }
+        std::stable_sort(sk.begin(), sk.end(), [](const SKey &a, const SKey &b) {
+            return a.post != b.post ? a.post < b.post : a.j < b.j;
+        });
+        for (size_t q = 0; q < sk.size(); ++q) {
+            const int b = sk[q].b, j = sk[q].j;
+            const BrainSpec &B = brains[b];
+            const ref::SynapseGene &C = B.conns[j];
+            const int e = ue0 + (int)q;
+            h_spos_[h_soff_[b] + j] = e;
+            const ref::NeuronGene &A = B.genes[C.pre], &Z = B.genes[C.post];
+            const bool live = C.active && A.active && Z.active;
+            const bool pair = !A.inh_tx && excitatory_type(A.type) && !A.modulator && !Z.inh_tx &&
+                              excitatory_type(Z.type);
+            const uint32_t kind = A.modulator ? KIND_MOD : (A.inh_tx ? KIND_INH : KIND_EXC);
+            const int pre_local = h_npos_[h_noff_[b] + C.pre] - un0;
+            if (pre_local > 0xffff) throw std::runtime_error("Unit exceeds 65536 neurons");
+            if (C.plasticity > 7) throw std::runtime_error("Invalid synapse gene");
+            uint32_t m = (uint32_t)pre_local | ((uint32_t)C.delay << M_DELAY_SHIFT) |
+                         ((uint32_t)(C.branch & 3u) << M_BRANCH_SHIFT) | (kind << M_KIND_SHIFT) |
+                         ((uint32_t)((A.modulator ? A.modulator - 1 : 0) & 3u) << M_MODID_SHIFT) |
+                         ((uint32_t)C.plasticity << M_PROF_SHIFT);
+            if (live) m |= M_LIVE;
+            if (live && C.plasticity && pair) m |= M_PLASTIC;
+            smeta[e] = m;
+            const int sites = C.sites ? (C.sites > 64 ? 64 : C.sites) : 14;
+            uint32_t *y = &sgene[(size_t)e * Y_WORDS];
+            const float yf[8] = {C.w0, C.U, C.trec, C.tfac, C.slow_rec, C.slow_depl, 0.0f, 0.0f};
+            std::memcpy(y, yf, sizeof yf);
+            y[Y_INFO] = (uint32_t)sites | ((uint32_t)C.receptors << 8);
+            sorig[e] = B.orig_s ? B.orig_s[j] : (uint32_t)j;
+            sbrain[e] = b;
+        }
+        // incoming segment starts
+        int cursor = ue0;
+        size_t q = 0;
+        for (int n = un0; n < un0 + (int)keys.size(); ++n) {
+            inptr[n] = cursor;
+            while (q < sk.size() && sk[q].post == n) { ++q; ++cursor; }
+        }
+        ncur += (int)keys.size();
+        ecur += (int)sk.size();
+        h_units_[ui] = make_int4(un0, ncur - un0, ue0, ecur - ue0);
+        max_unit_neurons_ = std::max(max_unit_neurons_, ncur - un0);
+        if (ncur - un0 > block_) ++n_big_units_;
+        max_unit_brains_ = std::max(max_unit_brains_, (int)ub.size());
     }
-    std::vector<int> bmotor((size_t)n_brains_ * outputs);
+    inptr[n_neurons_] = n_synapses_;
     for (int b = 0; b < n_brains_; ++b)
-        for (int j = 0; j < outputs; ++j) bmotor[(size_t)b * outputs + j] = h_bn0_[b] + brains[b].motors[j];
+        for (int j = 0; j < outputs; ++j)
+            bmotor[(size_t)b * outputs + j] = h_npos_[h_noff_[b] + brains[b].motors[j]];
+    // Spike-ring words per tick: whole CTA-sized neuron slots (a big unit's
+    // threads write one word per warp per slot).
+    hw_ = ((std::max(max_unit_neurons_, block_) + block_ - 1) / block_) * (block_ / 32);
+
     // ---- device allocation and upload ----
     NSB_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     auto up = [&](auto *dst, const auto &src) {
@@ -769,14 +821,12 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
     NSB_CHECK(cudaMemset(d_sarrived_, 0, std::max(n_synapses_, 1)));
     d_slastp_ = alloc<int16_t>(n_synapses_);
     NSB_CHECK(cudaMemset(d_slastp_, 0xff, (size_t)std::max(n_synapses_, 1) * 2));
-    d_bn0_ = alloc<int>(n_brains_); up(d_bn0_, h_bn0_);
-    d_be0_ = alloc<int>(n_brains_); up(d_be0_, h_be0_);
     d_btick_ = alloc<int64_t>(n_brains_); NSB_CHECK(cudaMemset(d_btick_, 0, n_brains_ * sizeof(int64_t)));
     d_bmotor_ = alloc<int>(std::max<size_t>(bmotor.size(), 1)); up(d_bmotor_, bmotor);
     d_ubrain_ = alloc<int>(n_brains_); up(d_ubrain_, brain_order);
-    d_units_ = alloc<int4>(n_units_); up(d_units_, units);
+    d_units_ = alloc<int4>(n_units_); up(d_units_, h_units_);
     d_unitb_ = alloc<int2>(n_units_); up(d_unitb_, unitb);
-    d_queue_ = alloc<int>(1);
+    d_queue_ = alloc<int>(2);
     d_events_ = alloc<unsigned long long>(1); NSB_CHECK(cudaMemset(d_events_, 0, 8));
     d_input_ = alloc<float>((size_t)n_brains_ * channels);
     NSB_CHECK(cudaMemset(d_input_, 0, (size_t)n_brains_ * channels * 4));
@@ -792,16 +842,21 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
     h_tick_.assign(n_brains_, 0);
 
     // ---- launch shape ----
-    smem_ = 1024 + (kMetaCap + 32 * hw_ * 2 + 2 * kMaxUnitBrains) * 4 + kMaxUnitBrains * 8 + 2 * kMaxUnitBrains * 4;
-    NSB_CHECK(cudaFuncSetAttribute(tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_));
-    int dev = 0, sms = 0;
+    smem_ = 1024 + (kMetaCap + 32 * hw_ * 2) * 4 + kMaxUnitBrains * 8 + 2 * kMaxUnitBrains * 4;
+    NSB_CHECK(cudaFuncSetAttribute(tick_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_));
+    NSB_CHECK(cudaFuncSetAttribute(tick_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_));
+    int dev = 0;
     NSB_CHECK(cudaGetDevice(&dev));
-    NSB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    NSB_CHECK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
     int occ = 0;
-    NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tick_kernel, block_, smem_));
+    NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tick_kernel<false>, block_, smem_));
     ctas_per_sm_ = cfg.ctas_per_sm > 0 ? std::min(cfg.ctas_per_sm, std::max(occ, 1)) : std::max(occ, 1);
-    grid_ = std::min(n_units_, sms * ctas_per_sm_);
+    grid_ = std::min(std::max(n_light_units_, 1), sms_ * ctas_per_sm_);
+    int occh = 0;
+    NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occh, tick_kernel<true>, block_, smem_));
+    grid_heavy_ = std::min(std::max(n_units_ - n_light_units_, 1), sms_ * std::max(occh, 1));
     K_ = make_constants();
+    NSB_CHECK(cudaMemcpyToSymbol(c_K, &K_, sizeof(PhysConst)));
 }
 
 Engine::~Engine() {
@@ -815,28 +870,27 @@ Stats Engine::stats() const {
                  grid_, block_, smem_, ctas_per_sm_};
 }
 
-static Pools make_pools(float *ngene, uint32_t *nflags, int *nsens, int *nxidx, float *xgene, float *xstate,
-                        uint32_t *nstate, int *inptr, uint32_t *smeta, uint32_t *sgene, uint32_t *sstate,
-                        uint8_t *sarrived, int16_t *slastp, int *bn0, int *be0, int64_t *btick, int *bmotor,
-                        int4 *units, int2 *unitb, int *ubrain, int n_units, int channels, int outputs, int hw,
-                        int *queue, unsigned long long *events) {
+Pools Engine::pools(bool events) const {
     Pools P;
-    P.ngene = reinterpret_cast<const float4 *>(ngene); P.nflags = nflags; P.nsens = nsens; P.nxidx = nxidx;
-    P.xgene = xgene; P.xstate = xstate; P.nstate = nstate; P.inptr = inptr; P.smeta = smeta; P.sgene = sgene;
-    P.sstate = sstate; P.sarrived = sarrived; P.slastp = slastp; P.bn0 = bn0; P.be0 = be0; P.btick = btick;
-    P.bmotor = bmotor; P.units = units; P.unitb = unitb; P.ubrain = ubrain; P.n_units = n_units;
-    P.channels = channels; P.outputs = outputs; P.hw = hw; P.queue = queue; P.events = events;
+    P.ngene = reinterpret_cast<const float4 *>(d_ngene_); P.nflags = d_nflags_; P.nsens = d_nsens_;
+    P.nxidx = d_nxidx_; P.xgene = d_xgene_; P.xstate = d_xstate_; P.nstate = d_nstate_; P.inptr = d_inptr_;
+    P.smeta = d_smeta_; P.sgene = d_sgene_; P.sstate = d_sstate_; P.sarrived = d_sarrived_; P.slastp = d_slastp_;
+    P.btick = d_btick_; P.bmotor = d_bmotor_; P.units = d_units_; P.unitb = d_unitb_; P.ubrain = d_ubrain_;
+    P.channels = channels_; P.outputs = outputs_; P.hw = hw_;
+    P.events = events ? d_events_ : nullptr;
     return P;
 }
 
 void Engine::launch(const float *d_input, const uint8_t *d_mask, int ticks, float gain, float *d_output,
                     int *d_status, cudaStream_t stream) {
-    Pools P = make_pools(d_ngene_, d_nflags_, d_nsens_, d_nxidx_, d_xgene_, d_xstate_, d_nstate_, d_inptr_,
-                         d_smeta_, d_sgene_, d_sstate_, d_sarrived_, d_slastp_, d_bn0_, d_be0_, d_btick_,
-                         d_bmotor_, d_units_, d_unitb_, d_ubrain_, n_units_, channels_, outputs_, hw_, d_queue_,
-                         count_events_ ? d_events_ : nullptr);
-    NSB_CHECK(cudaMemsetAsync(d_queue_, 0, sizeof(int), stream));
-    tick_kernel<<<grid_, block_, smem_, stream>>>(P, d_input, d_mask, d_output, d_status, ticks, gain, K_);
+    const Pools P = pools(count_events_);
+    NSB_CHECK(cudaMemsetAsync(d_queue_, 0, 2 * sizeof(int), stream));
+    if (n_light_units_ > 0)
+        tick_kernel<false><<<grid_, block_, smem_, stream>>>(P, 0, n_light_units_, d_queue_, d_input, d_mask,
+                                                              d_output, d_status, ticks, gain);
+    if (n_units_ > n_light_units_)
+        tick_kernel<true><<<grid_heavy_, block_, smem_, stream>>>(P, n_light_units_, n_units_, d_queue_ + 1, d_input,
+                                                                   d_mask, d_output, d_status, ticks, gain);
     NSB_CHECK(cudaGetLastError());
 }
 
@@ -889,15 +943,9 @@ void Engine::step_graph(int ticks, float gain, cudaStream_t stream) {
 void Engine::reset_host(const uint8_t *mask, const uint32_t *seeds) {
     NSB_CHECK(cudaMemcpyAsync(d_rmask_, mask, n_brains_, cudaMemcpyHostToDevice, stream_));
     NSB_CHECK(cudaMemcpyAsync(d_seeds_, seeds, n_brains_ * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
-    Pools P = make_pools(d_ngene_, d_nflags_, d_nsens_, d_nxidx_, d_xgene_, d_xstate_, d_nstate_, d_inptr_,
-                         d_smeta_, d_sgene_, d_sstate_, d_sarrived_, d_slastp_, d_bn0_, d_be0_, d_btick_,
-                         d_bmotor_, d_units_, d_unitb_, d_ubrain_, n_units_, channels_, outputs_, hw_, d_queue_,
-                         nullptr);
-    int dev = 0, sms = 0;
-    NSB_CHECK(cudaGetDevice(&dev));
-    NSB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    reset_neurons<<<sms * 8, 256, 0, stream_>>>(P, d_nbrain_, d_norig_, d_rmask_, d_seeds_, n_neurons_);
-    if (n_synapses_) reset_synapses<<<sms * 8, 256, 0, stream_>>>(P, d_sbrain_, d_sorig_, d_rmask_, d_seeds_, n_synapses_);
+    const Pools P = pools(false);
+    reset_neurons<<<sms_ * 8, 256, 0, stream_>>>(P, d_nbrain_, d_norig_, d_rmask_, d_seeds_, n_neurons_);
+    if (n_synapses_) reset_synapses<<<sms_ * 8, 256, 0, stream_>>>(P, d_sbrain_, d_sorig_, d_rmask_, d_seeds_, n_synapses_);
     reset_ticks<<<(n_brains_ + 255) / 256, 256, 0, stream_>>>(d_btick_, d_rmask_, n_brains_);
     NSB_CHECK(cudaGetLastError());
     NSB_CHECK(cudaStreamSynchronize(stream_));
@@ -914,6 +962,7 @@ void Engine::set_tick(int brain, int64_t tick) {
 
 unsigned long long Engine::take_events() {
     unsigned long long v = 0;
+    NSB_CHECK(cudaDeviceSynchronize());
     NSB_CHECK(cudaMemcpy(&v, d_events_, 8, cudaMemcpyDeviceToHost));
     NSB_CHECK(cudaMemset(d_events_, 0, 8));
     return v;
@@ -921,27 +970,29 @@ unsigned long long Engine::take_events() {
 
 void Engine::dump(int brain, uint32_t *nw, uint32_t *sw, int64_t *tick) {
     if (brain < 0 || brain >= n_brains_) throw std::runtime_error("Invalid brain index");
-    NSB_CHECK(cudaStreamSynchronize(stream_));
     NSB_CHECK(cudaDeviceSynchronize());
-    const int n0 = h_bn0_[brain], nn = h_bnn_[brain], e0 = h_be0_[brain], ne = h_bne_[brain];
-    std::vector<uint32_t> rec((size_t)nn * S_WORDS), srec((size_t)std::max(ne, 1) * Z_WORDS);
-    std::vector<uint8_t> arr(std::max(ne, 1));
+    const int4 U = h_units_[h_bunit_[brain]];
+    const int un0 = U.x, unn = U.y, ue0 = U.z, une = U.w;
+    const int nn = h_noff_[brain + 1] - h_noff_[brain], ne = h_soff_[brain + 1] - h_soff_[brain];
+    std::vector<uint32_t> rec((size_t)unn * S_WORDS), srec((size_t)std::max(une, 1) * Z_WORDS);
+    std::vector<uint8_t> arr(std::max(une, 1));
     int64_t t = 0;
-    NSB_CHECK(cudaMemcpy(rec.data(), d_nstate_ + (size_t)n0 * S_WORDS, rec.size() * 4, cudaMemcpyDeviceToHost));
-    if (ne) {
-        NSB_CHECK(cudaMemcpy(srec.data(), d_sstate_ + (size_t)e0 * Z_WORDS, (size_t)ne * Z_WORDS * 4, cudaMemcpyDeviceToHost));
-        NSB_CHECK(cudaMemcpy(arr.data(), d_sarrived_ + e0, ne, cudaMemcpyDeviceToHost));
+    NSB_CHECK(cudaMemcpy(rec.data(), d_nstate_ + (size_t)un0 * S_WORDS, rec.size() * 4, cudaMemcpyDeviceToHost));
+    if (une) {
+        NSB_CHECK(cudaMemcpy(srec.data(), d_sstate_ + (size_t)ue0 * Z_WORDS, (size_t)une * Z_WORDS * 4, cudaMemcpyDeviceToHost));
+        NSB_CHECK(cudaMemcpy(arr.data(), d_sarrived_ + ue0, une, cudaMemcpyDeviceToHost));
     }
     NSB_CHECK(cudaMemcpy(&t, d_btick_ + brain, 8, cudaMemcpyDeviceToHost));
     if (tick) *tick = t;
     if (nw) {
         for (int j = 0; j < nn; ++j) {
-            const uint32_t *r = &rec[(size_t)j * S_WORDS];
+            const int n = h_npos_[h_noff_[brain] + j];
+            const uint32_t *r = &rec[(size_t)(n - un0) * S_WORDS];
             uint32_t *o = nw + (size_t)j * kDumpNeuronWords;
             std::memset(o, 0, kDumpNeuronWords * 4);
             o[0] = r[S_V]; o[1] = r[S_W]; o[2] = r[S_ADP]; o[3] = r[S_INH]; o[4] = r[S_DEPOL]; o[5] = r[S_LOGAMPA];
             o[6] = r[S_D0]; o[7] = r[S_D1]; o[8] = r[S_D2]; o[9] = r[S_D3];
-            const int xi = h_nxidx_[n0 + j];
+            const int xi = h_nxidx_[n];
             if (xi >= 0) NSB_CHECK(cudaMemcpy(o + 10, d_xstate_ + (size_t)xi * 16, 64, cudaMemcpyDeviceToHost));
             o[26] = r[S_TOTAL]; o[27] = r[S_SPIKE]; o[28] = r[S_RECNS]; o[29] = r[S_RECRNG];
             uint32_t h = 0;
@@ -955,7 +1006,7 @@ void Engine::dump(int brain, uint32_t *nw, uint32_t *sw, int64_t *tick) {
     }
     if (sw) {
         for (int j = 0; j < ne; ++j) {
-            const int e = h_syn_pool_[e0 + j] - e0;
+            const int e = h_spos_[h_soff_[brain] + j] - ue0;
             const uint32_t *z = &srec[(size_t)e * Z_WORDS];
             uint32_t *o = sw + (size_t)j * kDumpSynapseWords;
             std::memset(o, 0, kDumpSynapseWords * 4);
@@ -971,14 +1022,23 @@ void Engine::load_state(int brain, const ref::NeuronState *neurons, const ref::S
                         const unsigned char (*history)[9], int64_t tick) {
     if (brain < 0 || brain >= n_brains_) throw std::runtime_error("Invalid brain index");
     if (tick < 0 || tick >= 2147483647ll) throw std::runtime_error("Tick outside the engine range");
-    const int n0 = h_bn0_[brain], nn = h_bnn_[brain], e0 = h_be0_[brain], ne = h_bne_[brain];
     NSB_CHECK(cudaDeviceSynchronize());
-    std::vector<uint32_t> rec((size_t)nn * S_WORDS, 0u), srec((size_t)std::max(ne, 1) * Z_WORDS, 0u);
-    std::vector<uint8_t> arr(std::max(ne, 1), 0);
+    const int4 U = h_units_[h_bunit_[brain]];
+    const int un0 = U.x, unn = U.y, ue0 = U.z, une = U.w;
+    const int nn = h_noff_[brain + 1] - h_noff_[brain], ne = h_soff_[brain + 1] - h_soff_[brain];
+    std::vector<uint32_t> rec((size_t)unn * S_WORDS), srec((size_t)std::max(une, 1) * Z_WORDS);
+    std::vector<uint8_t> arr(std::max(une, 1));
+    NSB_CHECK(cudaMemcpy(rec.data(), d_nstate_ + (size_t)un0 * S_WORDS, rec.size() * 4, cudaMemcpyDeviceToHost));
+    if (une) {
+        NSB_CHECK(cudaMemcpy(srec.data(), d_sstate_ + (size_t)ue0 * Z_WORDS, (size_t)une * Z_WORDS * 4, cudaMemcpyDeviceToHost));
+        NSB_CHECK(cudaMemcpy(arr.data(), d_sarrived_ + ue0, une, cudaMemcpyDeviceToHost));
+    }
     auto fw = [](float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; };
     for (int j = 0; j < nn; ++j) {
         const ref::NeuronState &s = neurons[j];
-        uint32_t *r = &rec[(size_t)j * S_WORDS];
+        const int n = h_npos_[h_noff_[brain] + j];
+        uint32_t *r = &rec[(size_t)(n - un0) * S_WORDS];
+        std::memset(r, 0, S_WORDS * 4);
         r[S_V] = fw(s.v); r[S_W] = fw(s.w); r[S_ADP] = fw(s.adp); r[S_INH] = fw(s.inh); r[S_DEPOL] = fw(s.depol);
         r[S_LOGAMPA] = fw(s.log_ampa); r[S_RECNS] = fw(s.rec_ns); r[S_RECRNG] = s.rec_rng;
         r[S_D0] = fw(s.dend[0]); r[S_D1] = fw(s.dend[1]); r[S_D2] = fw(s.dend[2]); r[S_D3] = fw(s.dend[3]);
@@ -991,27 +1051,27 @@ void Engine::load_state(int brain, const ref::NeuronState *neurons, const ref::S
                 if (history[j][tau % 9]) h |= 1u << (tau & 31);
             }
         r[S_HIST] = h;
-        const int xi = h_nxidx_[n0 + j];
+        const int xi = h_nxidx_[n];
         if (xi >= 0) NSB_CHECK(cudaMemcpy(d_xstate_ + (size_t)xi * 16, s.cell, 64, cudaMemcpyHostToDevice));
     }
     for (int j = 0; j < ne; ++j) {
         const ref::SynapseState &s = synapses[j];
-        const int e = h_syn_pool_[e0 + j] - e0;
+        const int e = h_spos_[h_soff_[brain] + j] - ue0;
         uint32_t *z = &srec[(size_t)e * Z_WORDS];
         const float f[11] = {s.w, s.ru, s.pre_tr, s.post_tr, s.eltp, s.eltd, s.da_age, s.spine, s.st_age, s.pre_age, s.post_age};
         for (int k = 0; k < 11; ++k) z[k] = fw(f[k]);
         z[Z_SLOW] = fw(s.slow);
         z[Z_READYLO] = (uint32_t)s.ready; z[Z_READYHI] = (uint32_t)(s.ready >> 32);
         z[Z_RNG] = s.rng;
-        int64_t last = s.last < -1000000 ? -1000000 : s.last;
+        const int64_t last = s.last < -1000000 ? -1000000 : s.last;
         if (last >= 2147483647ll) throw std::runtime_error("Last arrival outside the engine range");
         z[Z_LAST] = (uint32_t)(int32_t)last;
         arr[e] = s.arrived;
     }
-    NSB_CHECK(cudaMemcpy(d_nstate_ + (size_t)n0 * S_WORDS, rec.data(), rec.size() * 4, cudaMemcpyHostToDevice));
-    if (ne) {
-        NSB_CHECK(cudaMemcpy(d_sstate_ + (size_t)e0 * Z_WORDS, srec.data(), (size_t)ne * Z_WORDS * 4, cudaMemcpyHostToDevice));
-        NSB_CHECK(cudaMemcpy(d_sarrived_ + e0, arr.data(), ne, cudaMemcpyHostToDevice));
+    NSB_CHECK(cudaMemcpy(d_nstate_ + (size_t)un0 * S_WORDS, rec.data(), rec.size() * 4, cudaMemcpyHostToDevice));
+    if (une) {
+        NSB_CHECK(cudaMemcpy(d_sstate_ + (size_t)ue0 * Z_WORDS, srec.data(), (size_t)une * Z_WORDS * 4, cudaMemcpyHostToDevice));
+        NSB_CHECK(cudaMemcpy(d_sarrived_ + ue0, arr.data(), une, cudaMemcpyHostToDevice));
     }
     NSB_CHECK(cudaMemcpy(d_btick_ + brain, &tick, 8, cudaMemcpyHostToDevice));
     h_tick_[brain] = tick;

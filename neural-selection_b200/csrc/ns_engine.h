@@ -11,6 +11,8 @@
 
 namespace nsb {
 
+struct Pools;
+
 // One brain in the reference's host representation (gym_adapter/native.cpp:23-38).
 struct BrainSpec {
     const ref::NeuronGene *genes = nullptr;
@@ -80,11 +82,12 @@ private:
     void launch(const float *d_input, const uint8_t *d_mask, int ticks, float gain, float *d_output,
                 int *d_status, cudaStream_t stream);
     template <class T> T *alloc(size_t n);
+    struct Pools pools(bool events) const;
 
     int n_brains_ = 0, channels_ = 0, outputs_ = 0, max_delay_ = 8;
     int n_neurons_ = 0, n_synapses_ = 0, n_heavy_ = 0, n_units_ = 0, n_big_units_ = 0;
     int max_unit_neurons_ = 0, hw_ = 0, meta_cap_ = 0, max_unit_brains_ = 0;
-    int grid_ = 0, block_ = 256, smem_ = 0, ctas_per_sm_ = 0;
+    int grid_ = 0, grid_heavy_ = 0, block_ = 256, smem_ = 0, ctas_per_sm_ = 0, sms_ = 0, n_light_units_ = 0;
     bool count_events_ = true;
     std::vector<void *> allocations_;
     // device pools
@@ -92,7 +95,6 @@ private:
     float *d_xgene_ = nullptr; float *d_xstate_ = nullptr; uint32_t *d_nstate_ = nullptr; int *d_inptr_ = nullptr;
     uint32_t *d_smeta_ = nullptr; uint32_t *d_sgene_ = nullptr; uint32_t *d_sstate_ = nullptr;
     uint8_t *d_sarrived_ = nullptr; int16_t *d_slastp_ = nullptr;
-    int *d_bn0_ = nullptr, *d_bnn_ = nullptr, *d_be0_ = nullptr, *d_bne_ = nullptr;
     int64_t *d_btick_ = nullptr; int *d_bmotor_ = nullptr; int *d_bunit_ = nullptr;
     int4 *d_units_ = nullptr; int2 *d_unitb_ = nullptr; int *d_ubrain_ = nullptr;
     int *d_nbrain_ = nullptr; uint32_t *d_norig_ = nullptr; int *d_sbrain_ = nullptr; uint32_t *d_sorig_ = nullptr;
@@ -101,9 +103,10 @@ private:
     float *d_input_ = nullptr; uint8_t *d_mask_ = nullptr; float *d_output_ = nullptr; int *d_status_ = nullptr;
     uint32_t *d_seeds_ = nullptr;
     // host mirrors for layout mapping
-    std::vector<int> h_bn0_, h_bnn_, h_be0_, h_bne_;
-    std::vector<int> h_syn_orig_;        // pool synapse -> brain-local original edge index
-    std::vector<int> h_syn_pool_;        // per brain: original edge -> pool index (concatenated by brain e0)
+    std::vector<int> h_noff_, h_soff_;   // caller-order prefix offsets of neurons / synapses per brain
+    std::vector<int> h_npos_, h_spos_;   // (brain, original index) -> pool index
+    std::vector<int> h_bunit_;           // brain -> work unit
+    std::vector<int4> h_units_;          // {n0, nn, e0, ne} per unit
     std::vector<int> h_nxidx_;
     std::vector<uint32_t> h_nflags_;
     std::vector<int64_t> h_tick_;

@@ -16,6 +16,10 @@
 
 namespace nsb {
 
+// Correctly rounded constant exponentials, identical for every engine (set by
+// the host once per device).
+static __constant__ PhysConst c_K;
+
 struct NeuronRegs {
     float v, w, adp, inh, depol, rec_ns;
     uint32_t rng;
@@ -30,10 +34,10 @@ __device__ __forceinline__ uint32_t xorshift32(uint32_t x) {
     x ^= x << 13; x ^= x >> 17; x ^= x << 5; return x;
 }
 
-__device__ __forceinline__ float crexp(float x, const double *tab) { return nsx::expf_cr_tab(x, tab); }
+__device__ __forceinline__ float crexp(float x, const float *tab) { return nsx::expf_cr_ff(x, tab); }
 
 // physiology.cuh:226-230: thin-branch input/output curve (type 0 only).
-__device__ __forceinline__ float branch_gain(float gs, float offset, const double *tab) {
+__device__ __forceinline__ float branch_gain(float gs, float offset, const float *tab) {
     float regen = 5.0f / (1.0f + crexp(-(gs - 4.0f) / 0.4f, tab));
     return fminf(11.0f, gs + regen - offset);
 }
@@ -54,7 +58,7 @@ __device__ __forceinline__ float receptor_drive(const float *g, uint32_t flags, 
 // exc0..3/inh_in: this tick's summed synaptic input.
 __device__ __forceinline__ void adex_tick(const float *g, uint32_t type, uint32_t flags, NeuronRegs &s,
                                           float cur, float e0, float e1, float e2, float e3, float inh_in,
-                                          const PhysConst &K, const double *tab) {
+                                          const float *tab) {
     s.d0 += e0; s.d1 += e1; s.d2 += e2; s.d3 += e3;
     float sub = fmaxf(0.0f, fminf(s.v, -50.0f) - g[G_EL]);
     s.depol += 0.1f * (sub - s.depol);
@@ -69,10 +73,15 @@ __device__ __forceinline__ void adex_tick(const float *g, uint32_t type, uint32_
         float expo = clampf((v - g[G_VT]) / g[G_SLOPE], -20.0f, 10.0f);
         float soma;
         if (type == 0) {
-            soma = 0.0f + branch_gain(s.d0, K.dend_offset, tab);
-            soma += branch_gain(s.d1, K.dend_offset, tab);
-            soma += branch_gain(s.d2, K.dend_offset, tab);
-            soma += branch_gain(s.d3, K.dend_offset, tab);
+            // branch_gain(0) is exactly +0 (its two exponentials are the same
+            // value) and soma >= +0, so a branch with no conductance adds
+            // nothing and is skipped; warps sorted by branch usage skip it
+            // together.
+            soma = 0.0f;
+            if (s.d0 != 0.0f) soma += branch_gain(s.d0, c_K.dend_offset, tab);
+            if (s.d1 != 0.0f) soma += branch_gain(s.d1, c_K.dend_offset, tab);
+            if (s.d2 != 0.0f) soma += branch_gain(s.d2, c_K.dend_offset, tab);
+            if (s.d3 != 0.0f) soma += branch_gain(s.d3, c_K.dend_offset, tab);
         } else {
             soma = 0.0f + s.d0;
             soma += s.d1; soma += s.d2; soma += s.d3;
@@ -85,20 +94,19 @@ __device__ __forceinline__ void adex_tick(const float *g, uint32_t type, uint32_
             s.v = g[G_VR]; s.w += g[G_B]; s.adp += g[G_ADPB];
         }
         if (flags & NF_ADP) s.adp *= g[G_ADPDECAY];
-        s.d0 *= K.exc_sub; s.d1 *= K.exc_sub; s.d2 *= K.exc_sub; s.d3 *= K.exc_sub;
-        s.inh *= K.inh_sub;
+        s.d0 *= c_K.exc_sub; s.d1 *= c_K.exc_sub; s.d2 *= c_K.exc_sub; s.d3 *= c_K.exc_sub;
+        s.inh *= c_K.inh_sub;
     }
 }
 
 // ---- LFS cell (physiology.cuh:258-287); x = {v, thr, act[3], open[3]} -------------
-__device__ __noinline__ void lfs_tick(const float *g, NeuronRegs &s, float *x, float cur, float exc, float inh,
-                                      const PhysConst &K) {
+__device__ __noinline__ void lfs_tick(const float *g, NeuronRegs &s, float *x, float cur, float exc, float inh) {
     const float wt[3] = {250.0f, 10.0f, 4.0f}, op[3] = {10.0f, 40.0f, 750.0f}, cl[3] = {50.0f, 750.0f, 2000.0f};
-    x[1] = g[G_VT] + (x[1] - g[G_VT]) * K.lfs_thr;
+    x[1] = g[G_VT] + (x[1] - g[G_VT]) * c_K.lfs_thr;
     float under = 0;
     for (int j = 0; j < 3; ++j) {
         x[5 + j] += x[2 + j] / op[j] - x[5 + j] / cl[j];
-        x[2 + j] *= K.lfs_open[j];
+        x[2 + j] *= c_K.lfs_open[j];
         under += wt[j] * x[5 + j];
     }
     const float v = x[0];
@@ -114,11 +122,11 @@ __device__ __noinline__ void lfs_tick(const float *g, NeuronRegs &s, float *x, f
 }
 
 // ---- LP cell (lp_cell.cuh:28-113) --------------------------------------------------
-__device__ __forceinline__ float lp_sig(float v, float mid, float slope, const double *tab) {
+__device__ __forceinline__ float lp_sig(float v, float mid, float slope, const float *tab) {
     return 1.0f / (1.0f + crexp((v - mid) / slope, tab));
 }
 __device__ __forceinline__ float lp_ratio(float num, float den, float lim) { return fabsf(den) < 1e-5f ? lim : num / den; }
-__device__ __noinline__ void lp_rates(const float *x, float i_na, const float *sc, float *d, const double *tab) {
+__device__ __noinline__ void lp_rates(const float *x, float i_na, const float *sc, float *d, const float *tab) {
     const float va = x[0], vs = x[15];
     const float na = x[1] * x[1] * x[1] * x[2] * 7.15f * (va - 50.0f);
     const float kd = x[8] * x[8] * x[8] * x[8] * 1.43f * (va + 72.0f);
@@ -160,7 +168,7 @@ __device__ __noinline__ void lp_rates(const float *x, float i_na, const float *s
     d[14] = (lp_sig(va, -26.9916223f, -5.957441281f, tab) - x[14]) * .0001386796618f *
             lp_sig(va, -60.57875745f, -13.25674673f, tab);
 }
-__device__ __noinline__ void lp_integrate(float *x, float i_na, const float *sc, const double *tab) {
+__device__ __noinline__ void lp_integrate(float *x, float i_na, const float *sc, const float *tab) {
     const float dt = .05f;
     float k1[16], k2[16], k3[16], k4[16], y[16];
     for (int step = 0; step < 20; ++step) {
@@ -176,14 +184,14 @@ __device__ __noinline__ void lp_integrate(float *x, float i_na, const float *sc,
 }
 
 // ---- Prinz pacemaker (prinz_cell.cuh:45-121); u = {v, ca, m[7], h[4]} -------------
-__device__ __forceinline__ float pz_gate(float v, float a, float b, const double *tab) {
+__device__ __forceinline__ float pz_gate(float v, float a, float b, const float *tab) {
     return 1.0f / (1.0f + crexp((v + a) / b, tab));
 }
-__device__ __forceinline__ float pz_gate2(float v, float a, float b, float c, float d, const double *tab) {
+__device__ __forceinline__ float pz_gate2(float v, float a, float b, float c, float d, const float *tab) {
     return 1.0f / (crexp((v + a) / b, tab) + crexp((v + c) / d, tab));
 }
 __device__ __noinline__ void pz_substep(float *u, const float *g, float ext, float clamp_ns, float clamp_rev,
-                                        const PhysConst &K, const double *tab) {
+                                        const float *tab) {
     const float dt = .025f;
     float *m = u + 2, *h = u + 9;
     const float v = u[0], ca = fmaxf(u[1], 0.000001f);
@@ -199,7 +207,7 @@ __device__ __noinline__ void pz_substep(float *u, const float *g, float ext, flo
     else { const float tg = ws / gt; u[0] = tg + (v - tg) * crexp(-dt * gt / 628.3f, tab); }
     const float ica = (c[1] + c[2]) * (v - eca) / 1000000.0f;
     const float cat = .05f - 14961.0f * ica;
-    u[1] = fmaxf(.000001f, cat + (ca - cat) * K.prinz_ca);
+    u[1] = fmaxf(.000001f, cat + (ca - cat) * c_K.prinz_ca);
     const float mi[7] = {pz_gate(v, 25.5f, -5.29f, tab), pz_gate(v, 27.1f, -7.2f, tab), pz_gate(v, 33, -8.1f, tab),
                          pz_gate(v, 27.2f, -8.7f, tab), (ca / (ca + 3)) * pz_gate(v, 28.3f, -12.6f, tab),
                          pz_gate(v, 12.3f, -11.8f, tab), pz_gate(v, 75, 5.5f, tab)};
@@ -217,9 +225,9 @@ __device__ __noinline__ void pz_substep(float *u, const float *g, float ext, flo
 }
 
 // Heavy cell types (2 LP, 3 Prinz, 6 LFS) on their extended state x (16 floats).
-__device__ __noinline__ void heavy_tick(const float *g, uint32_t type, const float *xg, float *x, NeuronRegs &s,
+__device__ __noinline__ NeuronRegs heavy_tick(const float *g, uint32_t type, const float *xg, float *x, NeuronRegs s,
                                         float cur, float e0, float e1, float e2, float e3, float inh_in,
-                                        const PhysConst &K, const double *tab) {
+                                        const float *tab) {
     const float clamp_leak = 0.0f, clamp_rev = -68.0f;
     s.d0 += e0; s.d1 += e1; s.d2 += e2; s.d3 += e3;
     float sub = fmaxf(0.0f, fminf(s.v, -50.0f) - g[G_EL]);
@@ -229,7 +237,7 @@ __device__ __noinline__ void heavy_tick(const float *g, uint32_t type, const flo
     float exc = 0;
     exc += s.d0; exc += s.d1; exc += s.d2; exc += s.d3;
     if (type == 6) {
-        lfs_tick(g, s, x, cur, exc, s.inh, K);
+        lfs_tick(g, s, x, cur, exc, s.inh);
     } else if (type == 2) {
         float axon_before = x[0];
         float ext = cur + exc * (0.0f - s.v) + s.inh * (-75.0f - s.v) - clamp_leak * (s.v - clamp_rev);
@@ -242,23 +250,23 @@ __device__ __noinline__ void heavy_tick(const float *g, uint32_t type, const flo
         bool spiked = false;
         for (int i = 0; i < 40; ++i) {
             const float before = x[0];
-            pz_substep(x, xg, ext, xg[8] + clamp_leak, clamp_rev, K, tab);
+            pz_substep(x, xg, ext, xg[8] + clamp_leak, clamp_rev, tab);
             spiked |= before < 0 && x[0] >= 0;
         }
         s.spike = spiked ? 1u : 0u;
         s.total += (int)s.spike;
         s.v = x[0];
     }
-    s.d0 *= K.exc_ms; s.d1 *= K.exc_ms; s.d2 *= K.exc_ms; s.d3 *= K.exc_ms;
-    s.inh *= K.inh_ms;
+    s.d0 *= c_K.exc_ms; s.d1 *= c_K.exc_ms; s.d2 *= c_K.exc_ms; s.d3 *= c_K.exc_ms;
+    s.inh *= c_K.inh_ms;
+    return s;
 }
 
 // ---- homeostasis (physiology.cuh:243-253) ----------------------------------------
-__device__ __forceinline__ float homeostasis(uint32_t type, float log_ampa, float elapsed, float hz,
-                                             const PhysConst &K) {
+__device__ __forceinline__ float homeostasis(uint32_t type, float log_ampa, float elapsed, float hz) {
     if (type != 0) return log_ampa;
     float ratio = clampf(hz / 0.4f, 0.0f, 2.65f);
-    float change = ratio < 1.0f ? K.log_up * (1.0f - ratio) : K.log_down * ((ratio - 1.0f) / 1.65f);
+    float change = ratio < 1.0f ? c_K.log_up * (1.0f - ratio) : c_K.log_down * ((ratio - 1.0f) / 1.65f);
     return clampf(log_ampa + change * (elapsed / 172800000.0f), -3.0f, 3.0f);
 }
 
@@ -270,7 +278,7 @@ struct SynRelease {
     uint32_t rng;
     int last;
 };
-__device__ __forceinline__ float release(const float *y, SynRelease &s, int64_t tick, const double *tab) {
+__device__ __forceinline__ float release(const float *y, SynRelease &s, int64_t tick, const float *tab) {
     float p_rec = 0;
     if (s.last > -1000000) {
         float dt = (float)(tick - (int64_t)s.last) * 1.0f;
@@ -307,12 +315,12 @@ struct SynPlast {
     float w, pre_tr, post_tr, eltp, eltd, da_age, spine, st_age, pre_age, post_age;
 };
 
-__device__ __forceinline__ float da_window(float age, const double *tab) {
+__device__ __forceinline__ float da_window(float age, const float *tab) {
     if (age < 0 || age > 20000.0f) return 0;
     float x = age / 2000.0f;
     return x * x * x * x * crexp(4.0f * (1.0f - x), tab);
 }
-__device__ __forceinline__ float spine_window(float age, const double *tab) {
+__device__ __forceinline__ float spine_window(float age, const float *tab) {
     if (age < 0 || age > 5000.0f) return 0;
     float x = age / 1000.0f;
     return x * x * x * crexp(3.0f * (1.0f - x), tab);
@@ -322,7 +330,7 @@ __device__ __forceinline__ float spine_window(float age, const double *tab) {
 // (plasticity != 0 and excitatory pair), all channels available.
 __device__ __forceinline__ void plasticity_tick(uint32_t prof, uint32_t receptors, float w0, SynPlast &s,
                                                 bool arrived, bool post, float depol, uint32_t mod,
-                                                const PhysConst &K, const double *tab) {
+                                                const float *tab) {
     if (prof == 5) {
         if (s.st_age >= 0) { s.st_age += 1.0f; if (s.st_age > 5000.0f) s.st_age = -1; }
         s.pre_age += 1.0f;
@@ -347,7 +355,7 @@ __device__ __forceinline__ void plasticity_tick(uint32_t prof, uint32_t receptor
         return;
     }
     if (prof == 3) {
-        s.eltp *= K.ne; s.eltd *= K.sht;
+        s.eltp *= c_K.ne; s.eltd *= c_K.sht;
         s.pre_age += 1.0f; s.post_age += 1.0f;
         if (arrived) { if (s.post_age <= 15.0f) s.eltd += 1.0f; s.pre_age = 0; }
         if (post) { if (s.pre_age <= 15.0f) s.eltp += 1.0f; s.post_age = 0; }
@@ -356,7 +364,7 @@ __device__ __forceinline__ void plasticity_tick(uint32_t prof, uint32_t receptor
         s.w = clampf(s.w, 0.0f, 2.0f * w0);
         return;
     }
-    s.pre_tr *= K.ltp; s.post_tr *= K.ltd;
+    s.pre_tr *= c_K.ltp; s.post_tr *= c_K.ltd;
     s.pre_age += 1.0f; s.post_age += 1.0f;
     if (arrived) {
         if (s.post_age <= (prof == 2 ? 50.0f : 20.0f)) s.w *= 1.0f - 0.004f * s.post_tr;
@@ -374,7 +382,7 @@ __device__ __forceinline__ void plasticity_tick(uint32_t prof, uint32_t receptor
 // k consecutive ticks with no arrival, no postsynaptic spike and no relevant
 // modulator event: exactly k applications of plasticity_tick's quiet branch
 // (each field evolves independently; the weight bound is idempotent).
-__device__ __forceinline__ void plasticity_quiet(uint32_t prof, float w0, SynPlast &s, int k, const PhysConst &K) {
+__device__ __forceinline__ void plasticity_quiet(uint32_t prof, float w0, SynPlast &s, int k) {
     if (k <= 0) return;
     if (prof == 5) {
         for (int i = 0; i < k; ++i) {
@@ -392,11 +400,11 @@ __device__ __forceinline__ void plasticity_quiet(uint32_t prof, float w0, SynPla
         return;
     }
     if (prof == 3) {
-        for (int i = 0; i < k; ++i) { s.eltp *= K.ne; s.eltd *= K.sht; s.pre_age += 1.0f; s.post_age += 1.0f; }
+        for (int i = 0; i < k; ++i) { s.eltp *= c_K.ne; s.eltd *= c_K.sht; s.pre_age += 1.0f; s.post_age += 1.0f; }
         s.w = clampf(s.w, 0.0f, 2.0f * w0);
         return;
     }
-    for (int i = 0; i < k; ++i) { s.pre_tr *= K.ltp; s.post_tr *= K.ltd; s.pre_age += 1.0f; s.post_age += 1.0f; }
+    for (int i = 0; i < k; ++i) { s.pre_tr *= c_K.ltp; s.post_tr *= c_K.ltd; s.pre_age += 1.0f; s.post_age += 1.0f; }
     s.w = clampf(s.w, 0.0f, 2.0f * w0);
 }
 
