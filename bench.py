@@ -1,0 +1,441 @@
+"""Benchmark of the B200 neural tick at full pools.
+
+Workload (one step = one world step = 16 ticks of 1 ms): 32,768 brains of
+uneven size (lognormal, median 96, sigma 1, clipped to 16-4,096 and rescaled to
+fill 4,194,304 neuron slots), 8,388,608 synapses in proportion to size,
+delays 1-16 ms, Poisson 10-40 Hz receptor drive; seeded synthetic inputs
+(Philox4x32-10, seed 2). All device state (1.4 GB) exceeds the 126 MB L2, so
+every step streams it from HBM.
+
+value : neuron-ticks/s with inputs resident on the device, one persistent
+        fused launch per step replayed from a captured CUDA graph, timed with
+        CUDA events on the launching stream (max over ranks).
+e2e   : the same metric through the reference's C ABI call ns_gpu_step with
+        pinned host buffers (host->device observations, device->host motor
+        outputs and status inside the timed region).
+--impl reference : the reference's own host executor (gym_adapter/native.cpp
+        built from its sources into oracle/_ref) on the host cores.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+       (N > 1 under torch.distributed.run: one full-pool replica per GPU).
+"""
+import argparse
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+ALGO_BYTES_PER_NEURON = 172    # per world step: gene 64 + log-AMPA 4 + state 2x48 + delay-ring 2x4
+ALGO_BYTES_PER_SYNAPSE = 176   # per world step: gene 40 + state 2x68
+METRIC = "neuron-ticks/s at full pools"
+UNIT = "neuron-ticks/s"
+
+
+def load_package():
+    name = "neural_selection_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    pkg = ROOT / "neural-selection_b200"
+    spec = importlib.util.spec_from_file_location(name, pkg / "__init__.py", submodule_search_locations=[str(pkg)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_launch():
+    """DRAM bytes per tick-kernel launch from the committed ncu summary."""
+    p = ROOT / "profiles" / "tick_kernel_full_pools.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_launch:"):
+            return float(line.split(":")[1].split()[0])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi SM clocks and throttle reasons sampled every 200 ms."""
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 6:
+                continue
+            try:
+                sm.append(float(parts[0])); mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[2:6]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def workload(nsb, seed):
+    cache = Path(os.environ.get("NSB_BENCH_CACHE", "/tmp")) / f"nsb_uneven_full_seed{seed}.npz"
+    W = nsb.workloads
+    if cache.exists():
+        z = np.load(cache)
+        return W.Batch(z["nr"], z["sr"], z["no"], z["so"], z["mo"], int(z["ch"]), int(z["md"]), "batched_uneven",
+                       z["inp"], 230.0, {})
+    b = W.batched_uneven(seed=seed)
+    try:
+        np.savez(cache, nr=b.neuron_rows, sr=b.synapse_rows, no=b.neuron_offsets, so=b.synapse_offsets,
+                 mo=b.motors, ch=b.channels, md=b.max_delay, inp=b.inputs)
+    except OSError:
+        pass
+    return b
+
+
+# ---- CPU: the reference host executor -------------------------------------------
+_WORKER_BRAINS = []
+
+
+def _cpu_init(jobs, use_ref):
+    sys.path.insert(0, str(ROOT))
+    from oracle import pyoracle
+    global _WORKER_BRAINS
+    _WORKER_BRAINS = []
+    for rows_n, rows_s, motors, channels, inputs in jobs:
+        if use_ref:
+            b = pyoracle.RefBrain(rows_n, rows_s, motors, channels)
+        else:
+            b = pyoracle.OracleBrain(rows_n, rows_s, motors, channels, 16, libm=True)
+        b.reset(7)
+        _WORKER_BRAINS.append((b, inputs, len(rows_n)))
+
+
+def _cpu_step(ticks):
+    t0 = time.perf_counter()
+    nt = 0
+    for b, inputs, n in _WORKER_BRAINS:
+        b.step(inputs, ticks, 230.0)
+        nt += n * ticks
+    return nt, time.perf_counter() - t0
+
+
+class CpuReference:
+    """The reference host executor (gym_adapter/native.cpp built from its
+    sources) over a strided sample of brains, the sample split across one
+    process per host core; each process keeps its brains between steps."""
+
+    def __init__(self, batch, stride, processes):
+        import multiprocessing as mp
+        sys.path.insert(0, str(ROOT))
+        from oracle import pyoracle
+        self.use_ref = pyoracle.ref_lib() is not None
+        idx = np.argsort(np.diff(batch.neuron_offsets), kind="stable")[::stride]
+        jobs = []
+        for i in idx:
+            ng, sg, mo = batch.brain(int(i))
+            sg = sg.copy()
+            if self.use_ref:   # the reference ABI accepts delays 1-8 only; fold longer ones
+                sg[:, 4] = (sg[:, 4] - 1) % 8 + 1
+            jobs.append((ng, sg, mo, batch.channels, batch.inputs[int(i)]))
+        self.processes = max(1, min(processes, len(jobs)))
+        parts = [jobs[k::self.processes] for k in range(self.processes)]
+        ctx = mp.get_context("spawn")
+        self.pools = [ctx.Pool(1, initializer=_cpu_init, initargs=(part, self.use_ref)) for part in parts]
+        self.kind = "reference" if self.use_ref else "port"
+        self.sample = (f"{len(jobs)} of {batch.brains} brains (every {stride}th by size, "
+                       f"{sum(len(j[0]) for j in jobs)} neurons), 16-tick steps; " +
+                       ("delays folded into 1-8 (the reference ABI accepts 1-8)" if self.use_ref else
+                        "oracle port with the delay-16 ring"))
+
+    def step(self, ticks=16):
+        res = [p.apply_async(_cpu_step, (ticks,)) for p in self.pools]
+        out = [r.get() for r in res]
+        return sum(o[0] for o in out), max(o[1] for o in out)
+
+    def close(self):
+        for p in self.pools:
+            p.terminate()
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    nsb = load_package()
+    batch = workload(nsb, 2)
+    ref = CpuReference(batch, 8, os.cpu_count() or 1)
+    for _ in range(args.warmup):
+        ref.step(16)
+    nt, secs = 0, 0.0
+    for _ in range(args.steps):
+        a, b = ref.step(16)
+        nt += a; secs += b
+    ref.close()
+    value = nt / secs
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (Philox4x32-10 seed 2)",
+            "config": {"workload": "batched_uneven_full_pools", "brains": batch.brains, "neurons": 4194304,
+                       "synapses": 8388608, "ticks_per_step": 16, "delays_ms": "1-16"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.processes, "kind": ref.kind,
+                             "sample": ref.sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_cuda(args, rank, world, local_rank):
+    """The reference's own CUDA batch (gym_adapter/gpu.cu: one CTA per brain,
+    ns_gpu_step through its C ABI, synchronous with host buffers) on the same
+    workload; delays folded into 1-8 because its ABI accepts 1-8 only."""
+    if rank != 0:
+        return
+    import ctypes as ct
+    import torch
+    sys.path.insert(0, str(ROOT))
+    from oracle import pyoracle
+    lib = pyoracle.ref_gpu_lib()
+    if lib is None:
+        print(json.dumps({"impl": "reference-cuda", "unavailable": "oracle/_ref/libns_ref_gpu.so not built"}))
+        return
+    nsb = load_package()
+    batch = workload(nsb, 2)
+    f, i32 = ct.POINTER(ct.c_float), ct.POINTER(ct.c_int)
+    handles = []
+    for b in range(batch.brains):
+        ng, sg, mo = batch.brain(b)
+        sg = np.ascontiguousarray(sg.copy())
+        sg[:, 4] = (sg[:, 4] - 1) % 8 + 1
+        ng = np.ascontiguousarray(ng); mo = np.ascontiguousarray(mo, np.int32)
+        h = lib.ns_create(len(ng), len(sg), batch.channels, batch.outputs, ng.ctypes.data_as(f),
+                          sg.ctypes.data_as(f), mo.ctypes.data_as(i32))
+        if not h:
+            raise RuntimeError(lib.ns_error().decode())
+        handles.append(h)
+    arr = (ct.c_void_p * len(handles))(*handles)
+    t0 = time.perf_counter()
+    gb = lib.ns_gpu_create(arr, len(handles))
+    create_s = time.perf_counter() - t0
+    for h in handles:
+        lib.ns_destroy(h)
+    if not gb:
+        raise RuntimeError(lib.ns_error().decode())
+    mask = np.ones(batch.brains, np.uint8)
+    seeds = np.arange(batch.brains, dtype=np.uint32)
+    lib.ns_gpu_reset(gb, mask.ctypes.data_as(ct.POINTER(ct.c_uint8)), seeds.ctypes.data_as(ct.POINTER(ct.c_uint32)))
+    inp = np.ascontiguousarray(batch.inputs)
+    out = np.zeros((batch.brains, batch.outputs), np.float32)
+    st = np.zeros(batch.brains, np.int32)
+
+    def step():
+        rc = lib.ns_gpu_step(gb, inp.ctypes.data_as(f), mask.ctypes.data_as(ct.POINTER(ct.c_uint8)), 16,
+                             batch.gain, out.ctypes.data_as(f), st.ctypes.data_as(i32))
+        if rc:
+            raise RuntimeError(lib.ns_error().decode())
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+    steps = max(3, min(args.steps, 20))
+    t0 = time.perf_counter()
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record(); torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    ms = e0.elapsed_time(e1) / steps
+    N = len(batch.neuron_rows)
+    value = N * 16 / (ms / 1e3)
+    line = {"impl": "reference-cuda", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (Philox4x32-10 seed 2)",
+            "config": {"workload": "batched_uneven_full_pools", "brains": batch.brains, "neurons": N,
+                       "synapses": len(batch.synapse_rows), "ticks_per_step": 16,
+                       "delays_ms": "1-16 folded into 1-8 (reference ABI limit)",
+                       "kernel": "gym_adapter/gpu.cu step_batch, 32 threads per brain, --fmad=false --prec-div=true --prec-sqrt=true, sm_100a",
+                       "ns_gpu_create_s": create_s},
+            "e2e": {"value": N * 16 * steps / wall, "unit": UNIT, "h2d_bytes_per_step": int(inp.nbytes + mask.nbytes),
+                    "d2h_bytes_per_step": int(out.nbytes + st.nbytes)}}
+    lib.ns_gpu_destroy(gb)
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    nsb = load_package()
+    batch = workload(nsb, 2 + rank)
+    N = len(batch.neuron_rows)
+    E = len(batch.synapse_rows)
+    gpu = nsb.GpuBatch.from_rows(batch)
+    st = gpu.stats()
+    gpu.reset(np.arange(batch.brains, dtype=np.uint32) + 1000 * rank)
+    gpu.upload(batch.inputs, np.ones(batch.brains, np.uint8))
+    stream = torch.cuda.Stream()
+    s = stream.cuda_stream
+    for _ in range(max(args.warmup, 3)):
+        gpu.step_graph(16, batch.gain, s)
+    torch.cuda.synchronize()
+    gpu.take_events()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            gpu.step_graph(16, batch.gain, s)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    events = gpu.take_events()
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ms_step = ms / args.steps
+    value = world * N * 16 * args.steps / (ms / 1e3)
+    events_per_s = world * events / (ms / 1e3)
+    launches_per_step = (1 if st["units"] > 0 else 0) + (1 if st.get("heavy", 0) else 0)
+
+    # e2e: reference-facing C ABI call with pinned host buffers
+    inp = torch.from_numpy(batch.inputs).pin_memory()
+    msk = torch.ones(batch.brains, dtype=torch.uint8).pin_memory()
+    out = torch.zeros((batch.brains, batch.outputs), dtype=torch.float32).pin_memory()
+    stat = torch.zeros(batch.brains, dtype=torch.int32).pin_memory()
+    import ctypes as ct
+    lib = nsb.native.library()
+    f = ct.POINTER(ct.c_float)
+
+    def abi_step():
+        rc = lib.ns_gpu_step(gpu.ptr, ct.cast(inp.data_ptr(), f), ct.cast(msk.data_ptr(), ct.POINTER(ct.c_uint8)), 16,
+                             batch.gain, ct.cast(out.data_ptr(), f), ct.cast(stat.data_ptr(), ct.POINTER(ct.c_int)))
+        if rc:
+            raise RuntimeError(lib.ns_error().decode())
+    for _ in range(2):
+        abi_step()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    e2e_steps = max(args.steps // 2, 3)
+    for _ in range(e2e_steps):
+        abi_step()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * N * 16 * e2e_steps / e2e_s
+    h2d = batch.inputs.nbytes + batch.brains
+    d2h = out.numel() * 4 + stat.numel() * 4
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        algo = ALGO_BYTES_PER_NEURON * N + ALGO_BYTES_PER_SYNAPSE * E
+        achieved = algo / (ms_step / 1e3) / 1e9
+        traffic = traffic_per_launch()
+        clocks = clk.summary()
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (Philox4x32-10, seed 2 + rank)",
+                "config": {"workload": "batched_uneven_full_pools", "brains": batch.brains, "neurons": N,
+                           "synapses": E, "ticks_per_step": 16, "delays_ms": "1-16", "parallelism": f"replicas x{world}",
+                           "units": st["units"], "grid": st["grid"], "block": st["block"],
+                           "l2": "device state 1.4 GB > 126 MB L2: each step streams it from HBM"},
+                "synaptic_events_per_s": events_per_s,
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                             "algorithmic_bytes_per_launch": algo},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+                "gpu_launches": launches_per_step * args.steps,
+                "clocks": clocks}
+        if not args.no_cpu_baseline:
+            ref = CpuReference(batch, 8, os.cpu_count() or 1)
+            ref.step(16)
+            nt, secs = 0, 0.0
+            for _ in range(2):
+                a, b = ref.step(16)
+                nt += a; secs += b
+            ref.close()
+            line["cpu_baseline"] = {"value": nt / secs, "unit": UNIT, "cores": ref.processes, "kind": ref.kind,
+                                    "sample": ref.sample + "; 2 timed steps after 1 warm-up"}
+        print(json.dumps(line), flush=True)
+    gpu.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-cuda"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", args.gpus if "RANK" in os.environ else 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    elif args.impl == "reference-cuda":
+        run_reference_cuda(args, rank, world, local_rank)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

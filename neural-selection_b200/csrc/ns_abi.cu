@@ -278,6 +278,7 @@ static void *gpu_create(void **handles, int count, int max_delay_floor, int bloc
     EngineConfig cfg;
     cfg.max_delay = delay_ring_for(specs, max_delay_floor);
     if (block) cfg.block = block;
+    if (const char *slots = std::getenv("NSB_UNIT_SLOTS")) cfg.unit_slots = std::max(1, std::atoi(slots));
     auto batch = std::make_unique<GpuBatch>();
     batch->engine = std::make_unique<Engine>(specs, channels, outputs, cfg);
     return batch.release();

@@ -48,7 +48,7 @@ namespace nsb {
     } while (0)
 
 #ifndef NSB_MIN_CTAS
-#define NSB_MIN_CTAS 2   // CTAs per SM the light kernel's register budget is sized for
+#define NSB_MIN_CTAS 3   // CTAs per SM the light kernel's register budget is sized for
 #endif
 
 constexpr int kMetaCap = 6144;       // synapse meta words cached in shared memory per unit
@@ -142,54 +142,62 @@ __device__ __forceinline__ float release_event(uint32_t *sstate, const uint32_t 
     return rel;
 }
 
-// Delivery + integration of one neuron for local tick t. Returns the
-// postsynaptic modulator bits and the number of arrivals. HEAVY builds also
-// integrate the LP, Prinz and LFS cell types (out-of-line calls, which cost
-// registers, so units without such cells use the light build).
-template <bool HEAVY>
-__device__ __forceinline__ void deliver_and_integrate(
-    const Pools &P, const float (&g)[16], uint32_t flags, int ib, int ie, int e0, const uint32_t *meta,
-    const uint32_t *hist, int t, int64_t tick0, float ampa, float level, float gain, NeuronRegs &s, int n,
-    int *status, const float *tab, uint32_t &mod_out, int &narr_out) {
-    float e0s = 0.0f, e1s = 0.0f, e2s = 0.0f, e3s = 0.0f, inh = 0.0f;
-    uint32_t mod = 0;
-    int narr = 0;
+// Delivery for one postsynaptic neuron at local tick t: arrival test,
+// stochastic release and per-branch accumulation in ascending edge order.
+struct Delivered {
+    float e0, e1, e2, e3, inh;
+    uint32_t mod;
+    int narr;
+};
+__device__ __forceinline__ Delivered deliver(const Pools &P, int ib, int ie, int e0, const uint32_t *meta,
+                                             const uint32_t *hist, int t, int64_t tick0, float ampa,
+                                             const float *tab) {
+    Delivered d = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0u, 0};
     const int64_t tick = tick0 + t;
     for (int e = ib; e < ie; ++e) {
         const uint32_t m = meta[e - e0];
         if (!arrives(m, t, tick0, hist, P.hw)) continue;
-        ++narr;
+        ++d.narr;
         const uint32_t kind = (m >> M_KIND_SHIFT) & 3u;
         if (kind == KIND_INH) {             // inhibitory source: weight, no release
-            inh += __uint_as_float(P.sstate[(size_t)e * Z_WORDS + Z_W]);
+            d.inh += __uint_as_float(P.sstate[(size_t)e * Z_WORDS + Z_W]);
             continue;
         }
         const float rel = release_event(P.sstate, P.sgene, e, tick, tab);
         if (kind == KIND_MOD) {
-            if (rel > 0) mod |= 1u << ((m >> M_MODID_SHIFT) & 3u);
+            if (rel > 0) d.mod |= 1u << ((m >> M_MODID_SHIFT) & 3u);
         } else {
             const float c = rel * ampa;
             switch ((m >> M_BRANCH_SHIFT) & 3u) {
-            case 0: e0s += c; break;
-            case 1: e1s += c; break;
-            case 2: e2s += c; break;
-            default: e3s += c; break;
+            case 0: d.e0 += c; break;
+            case 1: d.e1 += c; break;
+            case 2: d.e2 += c; break;
+            default: d.e3 += c; break;
             }
         }
     }
+    return d;
+}
+
+// Integration of one neuron with this tick's synaptic input. HEAVY builds
+// also integrate the LP, Prinz and LFS cell types (out-of-line calls, which
+// cost registers, so units without such cells use the light build).
+template <bool HEAVY>
+__device__ __forceinline__ void integrate(const Pools &P, int n, uint32_t flags, const Delivered &d, float level,
+                                          float gain, NeuronRegs &s, int *status, const float *tab) {
+    float g[16];
+    load_gene(P.ngene + (size_t)n * 4, g);
     const uint32_t type = flags & NF_TYPE_MASK;
     float cur = 0.0f;
     if (flags & NF_HAS_INPUT) cur = type == 5 ? receptor_drive(g, flags, s, level) : gain * level;
     if (HEAVY && (type == 2 || type == 3 || type == 6)) {
         const int xidx = P.nxidx[n];
         s = heavy_tick(reinterpret_cast<const float *>(P.ngene + (size_t)n * 4), type, P.xgene + (size_t)xidx * 16,
-                       P.xstate + (size_t)xidx * 16, s, cur, e0s, e1s, e2s, e3s, inh, tab);
+                       P.xstate + (size_t)xidx * 16, s, cur, d.e0, d.e1, d.e2, d.e3, d.inh, tab);
     } else {
-        adex_tick(g, type, flags, s, cur, e0s, e1s, e2s, e3s, inh, tab);
+        adex_tick(g, type, flags, s, cur, d.e0, d.e1, d.e2, d.e3, d.inh, tab);
     }
     if (!isfinite(s.v)) *status = -1;
-    mod_out = mod;
-    narr_out = narr;
 }
 
 // Plasticity for the incoming synapses of one neuron at local tick t (runs
@@ -289,150 +297,92 @@ __global__ void __launch_bounds__(256, HEAVY ? 1 : NSB_MIN_CTAS) tick_kernel(Poo
         __syncthreads();
         const int slots = (nn + bs - 1) / bs;
         int my_events = 0;
-
-        if (slots == 1) {
-            // ---- register path: one neuron per thread, state in registers --------
-            const bool has = tid < nn;
-            const int n = n0 + tid;
-            const uint32_t flags = has ? P.nflags[n] : 0u;
+        // Each thread steps neurons j = sl0*bs + tid, sl0 < slots; their state
+        // stays in global memory (L1/L2-resident for the call). The per-call
+        // AMPA scale exp(log_ampa) is kept in the record's spare word.
+        for (int sl0 = 0; sl0 < slots; ++sl0) {
+            const int j = sl0 * bs + tid;
+            const bool has = j < nn;
+            const uint32_t flags = has ? P.nflags[n0 + j] : 0u;
             const int bi = (int)((flags >> NF_SLOT_SHIFT) & NF_SLOT_MASK);
             const bool run = has && s_mask[bi] != 0;
-            const int64_t tick0 = s_tick[bi];
-            float g[16];
-            NeuronRegs s = {};
-            float log_ampa = 0.0f, ampa = 1.0f, level = 0.0f;
             uint32_t h0 = 0;
-            int ib = 0, ie = 0, count = 0;
             if (run) {
-                load_gene(P.ngene + (size_t)n * 4, g);
-                load_neuron(P.nstate + (size_t)n * S_WORDS, s, log_ampa, h0);
-                ampa = crexp(log_ampa, tab);
-                if (flags & NF_HAS_INPUT) level = input[(size_t)s_bid[bi] * P.channels + P.nsens[n]];
-                ib = P.inptr[n]; ie = P.inptr[n + 1];
+                uint32_t *r = P.nstate + (size_t)(n0 + j) * S_WORDS;
+                h0 = r[S_HIST];
+                r[S_PAD] = __float_as_uint(crexp(__uint_as_float(r[S_LOGAMPA]), tab));
             }
-            const uint32_t rot = run ? rotr32(h0, (uint32_t)(tick0 & 31)) : 0u;
+            const uint32_t rot = run ? rotr32(h0, (uint32_t)(s_tick[bi] & 31)) : 0u;
             for (int sl = 0; sl < 32; ++sl) {
                 const uint32_t w = __ballot_sync(0xffffffffu, (rot >> sl) & 1u);
-                if (lane == 0) hist[sl * P.hw + warp] = w;
+                if (lane == 0) hist[sl * P.hw + sl0 * nwarp + warp] = w;
             }
-            __syncthreads();
-            int *status_ptr = status + s_bid[bi];
-            for (int t = 0; t < ticks; ++t) {
-                uint32_t mod = 0;
-                int narr = 0;
+            if (has) cnt[j] = 0;
+        }
+        __syncthreads();
+        for (int t = 0; t < ticks; ++t) {
+            for (int sl0 = 0; sl0 < slots; ++sl0) {
+                const int j = sl0 * bs + tid;
+                const int n = n0 + j;
+                const uint32_t flags = j < nn ? P.nflags[n] : 0u;
+                const int bi = (int)((flags >> NF_SLOT_SHIFT) & NF_SLOT_MASK);
+                const bool run = j < nn && s_mask[bi] != 0;
+                uint32_t spike = 0;
                 if (run) {
+                    const int64_t tick0 = s_tick[bi];
+                    uint32_t *r = P.nstate + (size_t)n * S_WORDS;
+                    const int ib = P.inptr[n], ie = P.inptr[n + 1];
+                    Delivered d = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0u, 0};
+                    if (flags & NF_ACTIVE)
+                        d = deliver(P, ib, ie, e0, meta, hist, t, tick0, __uint_as_float(r[S_PAD]), tab);
+                    NeuronRegs s;
+                    float log_ampa;
+                    uint32_t hw0;
+                    load_neuron(r, s, log_ampa, hw0);
                     if (flags & NF_ACTIVE) {
-                        deliver_and_integrate<HEAVY>(P, g, flags, ib, ie, e0, meta, hist, t, tick0, ampa, level, gain,
-                                                     s, n, status_ptr, tab, mod, narr);
+                        const float level =
+                            (flags & NF_HAS_INPUT) ? input[(size_t)s_bid[bi] * P.channels + P.nsens[n]] : 0.0f;
+                        integrate<HEAVY>(P, n, flags, d, level, gain, s, status + s_bid[bi], tab);
                     } else {
                         s.spike = 0;
                     }
+                    // the record's spare word keeps the call's AMPA scale
+                    store_neuron(r, s, log_ampa, hw0, r[S_PAD]);
+                    spike = s.spike;
+                    if (spike || d.mod || d.narr)
+                        plasticity_events(P.sstate, P.sgene, P.slastp, P.hw, ib, ie, e0, meta, hist, t, tick0,
+                                          spike != 0, d.mod, s.depol, tab);
+                    cnt[j] += (int)spike;
+                    my_events += d.narr;
                 }
-                const uint32_t w = __ballot_sync(0xffffffffu, run && s.spike);
-                if (lane == 0) hist[(t & 31) * P.hw + warp] = w;
-                if (run && (s.spike || mod || narr))
-                    plasticity_events(P.sstate, P.sgene, P.slastp, P.hw, ib, ie, e0, meta, hist, t, tick0,
-                                      s.spike != 0, mod, s.depol, tab);
-                count += run ? (int)s.spike : 0;
-                my_events += narr;
-                __syncthreads();
-            }
-            if (run) {
-                if (flags & NF_ACTIVE) {
-                    const int64_t t1 = tick0 + ticks;
-                    log_ampa = homeostasis(flags & NF_TYPE_MASK, log_ampa, (float)ticks,
-                                           (float)s.total * 1000.0f / (float)(ticks > t1 ? (int64_t)ticks : t1));
-                }
-                uint32_t L = 0;
-                for (int sl = 0; sl < 32; ++sl) L |= ((hist[sl * P.hw + warp] >> lane) & 1u) << sl;
-                store_neuron(P.nstate + (size_t)n * S_WORDS, s, log_ampa, rotl32(L, (uint32_t)(tick0 & 31)), 0u);
-                finish_synapses(P, ib, ie, e0, meta, hist, ticks, tick0);
-            }
-            if (has) cnt[tid] = count;
-        } else {
-            // ---- global path: one brain, several neurons per thread, state in L2 ----
-            const bool run = s_mask[0] != 0;
-            const int64_t tick0 = s_tick[0];
-            int *status_ptr = status + s_bid[0];
-            for (int sl0 = 0; sl0 < slots; ++sl0) {
-                const int j = sl0 * bs + tid;
-                const bool has = j < nn;
-                uint32_t h0 = 0;
-                if (has && run) {
-                    uint32_t *r = P.nstate + (size_t)(n0 + j) * S_WORDS;
-                    h0 = r[S_HIST];
-                    // ampa for the call kept in the record's spare word
-                    r[S_PAD] = __float_as_uint(crexp(__uint_as_float(r[S_LOGAMPA]), tab));
-                }
-                const uint32_t rot = (has && run) ? rotr32(h0, (uint32_t)(tick0 & 31)) : 0u;
-                for (int sl = 0; sl < 32; ++sl) {
-                    const uint32_t w = __ballot_sync(0xffffffffu, (rot >> sl) & 1u);
-                    if (lane == 0) hist[sl * P.hw + sl0 * nwarp + warp] = w;
-                }
-                if (has) cnt[j] = 0;
+                const uint32_t w = __ballot_sync(0xffffffffu, spike);
+                if (lane == 0) hist[(t & 31) * P.hw + sl0 * nwarp + warp] = w;
             }
             __syncthreads();
-            for (int t = 0; t < ticks; ++t) {
-                for (int sl0 = 0; sl0 < slots; ++sl0) {
-                    const int j = sl0 * bs + tid;
-                    const bool has = j < nn && run;
-                    uint32_t spike = 0;
-                    if (has) {
-                        const int n = n0 + j;
-                        uint32_t *r = P.nstate + (size_t)n * S_WORDS;
-                        NeuronRegs s;
-                        float log_ampa;
-                        uint32_t hw0;
-                        load_neuron(r, s, log_ampa, hw0);
-                        const float ampa = __uint_as_float(r[S_PAD]);
-                        const uint32_t flags = P.nflags[n];
-                        uint32_t mod = 0;
-                        int narr = 0;
-                        const int ib = P.inptr[n], ie = P.inptr[n + 1];
-                        if (flags & NF_ACTIVE) {
-                            float g[16];
-                            load_gene(P.ngene + (size_t)n * 4, g);
-                            const float level = (flags & NF_HAS_INPUT) ? input[(size_t)s_bid[0] * P.channels + P.nsens[n]] : 0.0f;
-                            deliver_and_integrate<HEAVY>(P, g, flags, ib, ie, e0, meta, hist, t, tick0, ampa, level,
-                                                         gain, s, n, status_ptr, tab, mod, narr);
-                        } else {
-                            s.spike = 0;
-                        }
-                        store_neuron(r, s, log_ampa, hw0, __float_as_uint(ampa));
-                        spike = s.spike;
-                        if (spike || mod || narr)
-                            plasticity_events(P.sstate, P.sgene, P.slastp, P.hw, ib, ie, e0, meta, hist, t, tick0,
-                                              spike != 0, mod, s.depol, tab);
-                        cnt[j] += (int)spike;
-                        my_events += narr;
-                    }
-                    const uint32_t w = __ballot_sync(0xffffffffu, spike);
-                    if (lane == 0) hist[(t & 31) * P.hw + sl0 * nwarp + warp] = w;
-                }
-                __syncthreads();
+        }
+        for (int sl0 = 0; sl0 < slots; ++sl0) {
+            const int j = sl0 * bs + tid;
+            if (j >= nn) continue;
+            const int n = n0 + j;
+            const uint32_t flags = P.nflags[n];
+            const int bi = (int)((flags >> NF_SLOT_SHIFT) & NF_SLOT_MASK);
+            if (!s_mask[bi]) continue;
+            const int64_t tick0 = s_tick[bi];
+            uint32_t *r = P.nstate + (size_t)n * S_WORDS;
+            float la = __uint_as_float(r[S_LOGAMPA]);
+            if (flags & NF_ACTIVE) {
+                const int total = (int)r[S_TOTAL];
+                const int64_t t1 = tick0 + ticks;
+                la = homeostasis(flags & NF_TYPE_MASK, la, (float)ticks,
+                                 (float)total * 1000.0f / (float)(ticks > t1 ? (int64_t)ticks : t1));
             }
-            for (int sl0 = 0; sl0 < slots; ++sl0) {
-                const int j = sl0 * bs + tid;
-                if (j < nn && run) {
-                    const int n = n0 + j;
-                    uint32_t *r = P.nstate + (size_t)n * S_WORDS;
-                    const uint32_t flags = P.nflags[n];
-                    float la = __uint_as_float(r[S_LOGAMPA]);
-                    if (flags & NF_ACTIVE) {
-                        const int total = (int)r[S_TOTAL];
-                        const int64_t t1 = tick0 + ticks;
-                        la = homeostasis(flags & NF_TYPE_MASK, la, (float)ticks,
-                                         (float)total * 1000.0f / (float)(ticks > t1 ? (int64_t)ticks : t1));
-                    }
-                    uint32_t L = 0;
-                    const int word = sl0 * nwarp + warp;
-                    for (int sl = 0; sl < 32; ++sl) L |= ((hist[sl * P.hw + word] >> lane) & 1u) << sl;
-                    r[S_LOGAMPA] = __float_as_uint(la);
-                    r[S_HIST] = rotl32(L, (uint32_t)(tick0 & 31));
-                    r[S_PAD] = 0u;
-                    finish_synapses(P, P.inptr[n], P.inptr[n + 1], e0, meta, hist, ticks, tick0);
-                }
-            }
+            uint32_t L = 0;
+            const int word = sl0 * nwarp + warp;
+            for (int sl = 0; sl < 32; ++sl) L |= ((hist[sl * P.hw + word] >> lane) & 1u) << sl;
+            r[S_LOGAMPA] = __float_as_uint(la);
+            r[S_HIST] = rotl32(L, (uint32_t)(tick0 & 31));
+            r[S_PAD] = 0u;
+            finish_synapses(P, P.inptr[n], P.inptr[n + 1], e0, meta, hist, ticks, tick0);
         }
         __syncthreads();
         // ---- motor outputs (spikes per call) and tick counters --------------------
@@ -582,6 +532,7 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
     n_neurons_ = (int)nsum; n_synapses_ = (int)esum;
 
     // ---- work units ------------------------------------------------------------
+    unit_cap_ = block_ * std::max(1, cfg.unit_slots);
     // Brains with LP/Prinz/LFS cells go to units of their own (stepped by the
     // heavy kernel). Within each group a brain above the CTA size is a unit of
     // its own; smaller brains are packed best-fit decreasing.
@@ -601,7 +552,7 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
         std::multimap<int, int> open;   // remaining capacity -> unit
         for (int b : order) {
             const int n = brains[b].count;
-            if (n > block_) {
+            if (n > unit_cap_) {
                 unit_brains.push_back({b}); unit_fill.push_back(n); unit_heavy.push_back((char)group);
                 continue;
             }
@@ -611,11 +562,11 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
                 open.erase(it);
                 unit_brains[uidx].push_back(b);
                 unit_fill[uidx] += n;
-                const int rem = block_ - unit_fill[uidx];
+                const int rem = unit_cap_ - unit_fill[uidx];
                 if (rem > 0 && (int)unit_brains[uidx].size() < kMaxUnitBrains) open.emplace(rem, uidx);
             } else {
                 unit_brains.push_back({b}); unit_fill.push_back(n); unit_heavy.push_back((char)group);
-                const int rem = block_ - n;
+                const int rem = unit_cap_ - n;
                 if (rem > 0) open.emplace(rem, (int)unit_brains.size() - 1);
             }
         }
@@ -787,7 +738,7 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
         ecur += (int)sk.size();
         h_units_[ui] = make_int4(un0, ncur - un0, ue0, ecur - ue0);
         max_unit_neurons_ = std::max(max_unit_neurons_, ncur - un0);
-        if (ncur - un0 > block_) ++n_big_units_;
+        if (ncur - un0 > unit_cap_) ++n_big_units_;
         max_unit_brains_ = std::max(max_unit_brains_, (int)ub.size());
     }
     inptr[n_neurons_] = n_synapses_;

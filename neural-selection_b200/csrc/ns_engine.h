@@ -29,6 +29,7 @@ struct EngineConfig {
     int max_delay = 8;          // 8 = the reference ABI; up to 31
     int block = 256;            // threads per CTA = neurons per small work unit
     int ctas_per_sm = 0;        // 0: from occupancy
+    int unit_slots = 3;         // small brains are packed into units of block * unit_slots neurons
     bool count_events = true;   // count synaptic arrivals on the device
 };
 
@@ -86,7 +87,7 @@ private:
 
     int n_brains_ = 0, channels_ = 0, outputs_ = 0, max_delay_ = 8;
     int n_neurons_ = 0, n_synapses_ = 0, n_heavy_ = 0, n_units_ = 0, n_big_units_ = 0;
-    int max_unit_neurons_ = 0, hw_ = 0, meta_cap_ = 0, max_unit_brains_ = 0;
+    int max_unit_neurons_ = 0, hw_ = 0, meta_cap_ = 0, max_unit_brains_ = 0, unit_cap_ = 256;
     int grid_ = 0, grid_heavy_ = 0, block_ = 256, smem_ = 0, ctas_per_sm_ = 0, sms_ = 0, n_light_units_ = 0;
     bool count_events_ = true;
     std::vector<void *> allocations_;

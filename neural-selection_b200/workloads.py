@@ -218,7 +218,7 @@ def uneven_sizes(seed, brains, total, median, sigma, lo, hi):
 
 
 def batched_uneven(seed=2, brains=32768, total_neurons=4194304, total_synapses=8388608,
-                   sensory=8, outputs=5, max_delay=16, plastic_all=False):
+                   sensory=8, outputs=5, max_delay=16, plastic_all=False, median=96.0, sigma=1.0, lo=16, hi=4096):
     """Batched uneven brains at full pools: sizes lognormal(median 96,
     sigma 1) clipped to [16, 4096] and rescaled to fill 4,194,304 neuron slots;
     8,388,608 synapses in proportion to size (2 per neuron); delays 1-16 ms;
@@ -229,7 +229,7 @@ def batched_uneven(seed=2, brains=32768, total_neurons=4194304, total_synapses=8
     (U .55, tau_rec 450) except facilitating onto inhibitory targets (U .1,
     tau_rec 30, tau_fac 1700); pair STDP (profile 1) on excitatory pairs."""
     st = Stream(seed)
-    sizes = uneven_sizes(seed, brains, total_neurons, 96.0, 1.0, 16, 4096)
+    sizes = uneven_sizes(seed, brains, total_neurons, median, sigma, lo, hi)
     per = total_synapses // total_neurons
     edges = sizes * per
     rem = total_synapses - edges.sum()

@@ -77,6 +77,30 @@ def ref_lib(cr=False):
     return _libs[name]
 
 
+def ref_gpu_lib():
+    """The reference CUDA batch (gym_adapter/gpu.cu built from its sources
+    with its own flags for sm_100a), or None."""
+    path = HERE / "_ref" / "libns_ref_gpu.so"
+    if not path.exists():
+        return None
+    name = "libns_ref_gpu.so"
+    if name not in _libs:
+        lib = ct.CDLL(str(path))
+        lib.ns_create.restype = ct.c_void_p
+        lib.ns_create.argtypes = [ct.c_int] * 4 + [_f, _f, _i32]
+        lib.ns_destroy.argtypes = [ct.c_void_p]
+        lib.ns_error.restype = ct.c_char_p
+        lib.ns_gpu_create.restype = ct.c_void_p
+        lib.ns_gpu_create.argtypes = [ct.POINTER(ct.c_void_p), ct.c_int]
+        lib.ns_gpu_destroy.argtypes = [ct.c_void_p]
+        lib.ns_gpu_reset.argtypes = [ct.c_void_p, _u8, _u32]
+        lib.ns_gpu_reset.restype = ct.c_int
+        lib.ns_gpu_step.argtypes = [ct.c_void_p, _f, _u8, ct.c_int, ct.c_float, _f, _i32]
+        lib.ns_gpu_step.restype = ct.c_int
+        _libs[name] = lib
+    return _libs[name]
+
+
 class OracleBrain:
     """One brain in the C oracle."""
 
