@@ -304,6 +304,44 @@ def run_reference_cuda(args, rank, world, local_rank):
     lib.ns_gpu_destroy(gb)
     print(json.dumps(line), flush=True)
 
+    # The world simulator's neural stage (src/main.cu) in both of its forms.
+    wlib = pyoracle.ref_world_lib()
+    if wlib is None:
+        print(json.dumps({"impl": "reference-cuda-world", "unavailable": "oracle/_ref/libns_ref_world.so not built"}))
+        return
+    for mode, label in ((0, "fused global-slot kernels"), (1, "--block-brains tiers + global-slot fallback")):
+        no = np.ascontiguousarray(batch.neuron_offsets, np.int64)
+        so = np.ascontiguousarray(batch.synapse_offsets, np.int64)
+        w = wlib.ref_world_create(batch.brains, no.ctypes.data_as(ct.POINTER(ct.c_int64)),
+                                  so.ctypes.data_as(ct.POINTER(ct.c_int64)),
+                                  np.ascontiguousarray(batch.neuron_rows).ctypes.data_as(f),
+                                  np.ascontiguousarray(batch.synapse_rows).ctypes.data_as(f),
+                                  np.ascontiguousarray(batch.motors, np.int32).ctypes.data_as(i32),
+                                  batch.outputs, 7, mode)
+        if not w:
+            print(json.dumps({"impl": "reference-cuda-world", "unavailable": "pool setup failed"}))
+            continue
+        for _ in range(max(args.warmup, 3)):
+            assert wlib.ref_world_step(w) == 0
+        wlib.ref_world_sync()
+        t0 = time.perf_counter()
+        e0.record()
+        for _ in range(steps):
+            assert wlib.ref_world_step(w) == 0
+        e1.record(); torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        ms = e0.elapsed_time(e1) / steps
+        spikes = wlib.ref_world_total_spikes(w, N)
+        wlib.ref_world_destroy(w)
+        line = dict(line)
+        line.update({"impl": "reference-cuda-world", "value": N * 16 / (ms / 1e3), "ms_per_step": ms,
+                     "config": dict(line["config"], kernel=f"src/main.cu neural stage, {label}, --use_fast_math, sm_100a",
+                                    total_spikes_after=spikes),
+                     "e2e": {"value": N * 16 * steps / wall, "unit": UNIT, "h2d_bytes_per_step": 0,
+                             "d2h_bytes_per_step": 16}})
+        line["config"].pop("ns_gpu_create_s", None)
+        print(json.dumps(line), flush=True)
+
 
 def run_ours(args, rank, world, local_rank):
     import torch

@@ -88,6 +88,23 @@ def build_ref(verbose=False, gpu=True):
             _run(["nvcc", "-O3", "-std=c++17", "--fmad=false", "--prec-div=true", "--prec-sqrt=true",
                   "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC",
                   *inc, gpu_src, "-o", out, "--cudart", "shared"])
+        # The world simulator's neural kernels (src/main.cu) with the world
+        # binary's flags (CMakeLists.txt:8), for timing only.
+        world_src = REFERENCE / "src" / "main.cu"
+        out = REF_OUT / "libns_ref_world.so"
+        if _stale(out, [world_src, HERE / "ref_world_harness.cu"]):
+            stub = REF_OUT / "stub_include"
+            stub.mkdir(exist_ok=True)
+            (stub / "png.h").write_text(
+                "/* stub: the timing harness never writes images */\n#pragma once\n"
+                "typedef struct { unsigned version, width, height, format; char message[64]; } png_image;\n"
+                "#define PNG_IMAGE_VERSION 1\n#define PNG_FORMAT_RGB 2\n"
+                "static inline int png_image_write_to_file(png_image *, const char *, int, const void *, int,"
+                " const void *) { return 1; }\n")
+            _run(["nvcc", "-O3", "-std=c++17", "--use_fast_math", "-gencode", "arch=compute_100a,code=sm_100a",
+                  "-shared", "-Xcompiler", "-fPIC", "-I", stub, "-I", REFERENCE / "src",
+                  "-DLIVE_ASSET_DIR=\"/nonexistent\"", HERE / "ref_world_harness.cu", REFERENCE / "src" / "live_view.cpp",
+                  "-o", out, "-lz"])
     return REF_OUT
 
 

@@ -101,6 +101,27 @@ def ref_gpu_lib():
     return _libs[name]
 
 
+def ref_world_lib():
+    """The reference world simulator's neural kernels (src/main.cu) behind the
+    timing harness oracle/ref_world_harness.cu, or None."""
+    path = HERE / "_ref" / "libns_ref_world.so"
+    if not path.exists():
+        return None
+    name = "libns_ref_world.so"
+    if name not in _libs:
+        lib = ct.CDLL(str(path))
+        lib.ref_world_create.restype = ct.c_void_p
+        lib.ref_world_create.argtypes = [ct.c_int, _i64, _i64, _f, _f, _i32, ct.c_int, ct.c_uint32, ct.c_int]
+        lib.ref_world_step.argtypes = [ct.c_void_p]
+        lib.ref_world_step.restype = ct.c_int
+        lib.ref_world_sync.restype = ct.c_int
+        lib.ref_world_total_spikes.argtypes = [ct.c_void_p, ct.c_int]
+        lib.ref_world_total_spikes.restype = ct.c_longlong
+        lib.ref_world_destroy.argtypes = [ct.c_void_p]
+        _libs[name] = lib
+    return _libs[name]
+
+
 class OracleBrain:
     """One brain in the C oracle."""
 

@@ -1,0 +1,252 @@
+// ORACLE — test/benchmark infrastructure only.
+//
+// Times the reference world simulator's own neural-tick kernels on a given
+// population. src/main.cu is compiled from the reference tree with main()
+// renamed (the pattern of the reference's tests/plasticity_ablation.cu:6-8);
+// this file fills its Device pools (src/main.cu:105-140) with the population
+// and replays the neural part of its step loop (src/main.cu:2634-2728 and
+// 2751-2758): selection of occupied slots or block-brain tiers, then 16 ticks
+// of synapse_delivery / synapse_plasticity_delivery / neuron_step /
+// synapse_plasticity (global-slot form) or brain_block_step tiers, then
+// homeostasis. Built with the world binary's own flags (--use_fast_math,
+// CMakeLists.txt:8). Needs a stub png.h (no image is ever written).
+#define main ecological_application_main
+#include "main.cu"
+#undef main
+
+#include <cstring>
+
+namespace {
+using namespace sim;
+
+template <class T> T *dalloc(size_t n) {
+    T *p = nullptr;
+    if (cudaMalloc(reinterpret_cast<void **>(&p), sizeof(T) * (n ? n : 1)) != cudaSuccess) return nullptr;
+    cudaMemset(p, 0, sizeof(T) * (n ? n : 1));
+    return p;
+}
+
+struct World {
+    Device d{};
+    void *select_tmp = nullptr;
+    size_t select_bytes = 0;
+    int block_mode = 0;   // 0 fused global-slot, 1 block-brain tiers + global fallback
+    int64_t step = 0;
+};
+}  // namespace
+
+extern "C" {
+
+// One animal per brain, genomes given as the Gym ABI rows (neuron rows of 10,
+// synapse rows of 11 floats, brain-local pre/post), decoded into the
+// reference's NeuronGene / SynapseGene with the rules of ns_create
+// (gym_adapter/native.cpp:128-150) using the reference's own profiles. A
+// sensory neuron reads world sense `channel` when channel < S. Returns NULL if
+// the population exceeds the pools.
+void *ref_world_create(int brains, const int64_t *noff, const int64_t *soff, const float *neuron_rows,
+                       const float *synapse_rows, const int *motors, int outputs, uint32_t seed, int block_mode) {
+    if (brains > P || noff[brains] > NEURON_CAPACITY || soff[brains] > SYNAPSE_CAPACITY) return nullptr;
+    auto *w = new World;
+    w->block_mode = block_mode;
+    Device &d = w->d;
+    d.trace_animal = -1;
+    d.animals = dalloc<Animal>(P);
+    d.neurons = dalloc<NeuronGene>(NEURON_CAPACITY);
+    d.synapses = dalloc<SynapseGene>(SYNAPSE_CAPACITY);
+    d.neuron_state = dalloc<NeuronState>(NEURON_CAPACITY);
+    d.synapse_state = dalloc<SynapseState>(SYNAPSE_CAPACITY);
+    d.neuron_owner = dalloc<int>(NEURON_CAPACITY);
+    d.synapse_owner = dalloc<int>(SYNAPSE_CAPACITY);
+    d.occupied_neurons = dalloc<int>(NEURON_CAPACITY);
+    d.occupied_synapses = dalloc<int>(SYNAPSE_CAPACITY);
+    d.occupied_neuron_count = dalloc<int>(1);
+    d.occupied_synapse_count = dalloc<int>(1);
+    d.block_animals = dalloc<int>(P);
+    d.block_animal_count = dalloc<int>(1);
+    d.medium_animals = dalloc<int>(P);
+    d.medium_animal_count = dalloc<int>(1);
+    d.neuron_next = dalloc<int>(NEURON_CAPACITY);
+    d.synapse_next = dalloc<int>(SYNAPSE_CAPACITY);
+    d.neuron_port = dalloc<int>(NEURON_CAPACITY);
+    d.pending_exc = dalloc<float>((size_t)NEURON_CAPACITY * DENDRITES);
+    d.pending_inh = dalloc<float>(NEURON_CAPACITY);
+    d.mod_event_tick = dalloc<unsigned long long>((size_t)NEURON_CAPACITY * 6);
+    d.spike_history = dalloc<unsigned char>((size_t)HISTORY * NEURON_CAPACITY);
+    d.senses = dalloc<float>((size_t)P * S);
+    d.motors = dalloc<int>((size_t)P * M);
+    d.trace_exc_arrivals = dalloc<int>(M); d.trace_exc_releases = dalloc<int>(M);
+    d.trace_inh_arrivals = dalloc<int>(M); d.trace_exc_ns = dalloc<float>(M);
+    d.trace_inh_ns = dalloc<float>(M); d.trace_peak_mv = dalloc<float>(M);
+    if (!d.animals || !d.neurons || !d.synapses || !d.neuron_state || !d.synapse_state || !d.spike_history) {
+        delete w;
+        return nullptr;
+    }
+    const int64_t N = noff[brains], E = soff[brains];
+    std::vector<Animal> animals(P);
+    std::vector<NeuronGene> ng(N);
+    std::vector<SynapseGene> sg(E);
+    std::vector<NeuronState> ns(N);
+    std::vector<SynapseState> ss(E);
+    std::vector<int> nowner(NEURON_CAPACITY, -1), sowner(SYNAPSE_CAPACITY, -1);
+    std::vector<int> nnext(N, -1), snext(E, -1), port(N, -1);
+    std::vector<float> senses((size_t)P * S, 0.0f);
+    std::vector<int> sensory(N);
+    for (int64_t i = 0; i < N; ++i) {
+        const float *q = neuron_rows + i * 10;
+        NeuronGene g = initial_profile(static_cast<unsigned char>(q[0]));
+        sensory[i] = (int)q[1];
+        g.active = q[2]; g.inhibitory_transmitter = q[3]; g.modulator = q[4];
+        g.capacitance_pf *= q[5]; g.leak_ns *= q[6]; g.threshold_mv = q[7];
+        g.receptor_baseline_hz = 0; g.receptor_gain_hz = q[8]; g.receptor_event_ns = q[9];
+        ng[i] = g;
+    }
+    for (int64_t i = 0; i < E; ++i) {
+        const float *q = synapse_rows + i * 11;
+        SynapseGene g{};
+        g.pre = q[0]; g.post = q[1]; g.initial_weight_ns = q[2]; g.active = q[3]; g.delay = q[4];
+        g.branch = q[5]; g.utilization = q[6]; g.recovery_ms = q[7]; g.facilitation_ms = q[8];
+        g.plasticity = q[9]; g.mod_receptors = q[10]; g.release_sites = 14;
+        if (g.delay > D) g.delay = (unsigned char)((g.delay - 1) % D + 1);   // the world ring holds D = 8
+        sg[i] = g;
+    }
+    for (int a = 0; a < P; ++a) {
+        Animal &b = animals[a];
+        std::memset(&b, 0, sizeof b);
+        b.neuron_head = b.synapse_head = -1;
+        for (int p = 0; p < S + M; ++p) b.ports[p] = -1;
+        if (a >= brains) continue;
+        b.alive = 1; b.id = a; b.age = 1;
+        b.neuron_count = (int)(noff[a + 1] - noff[a]);
+        b.synapse_count = (int)(soff[a + 1] - soff[a]);
+        if (b.neuron_count) b.neuron_head = (int)noff[a];
+        if (b.synapse_count) b.synapse_head = (int)soff[a];
+        for (int64_t n = noff[a]; n < noff[a + 1]; ++n) {
+            nowner[n] = a;
+            nnext[n] = n + 1 < noff[a + 1] ? (int)(n + 1) : -1;
+            NeuronGene &g = ng[n];
+            const int ch = sensory[n];
+            // world senses: channels < S read senses[a*S + channel]
+            g.sensory_channel = ch >= 0 && ch < S ? (signed char)ch : (signed char)-1;
+            if (ch >= 0 && ch < S) senses[(size_t)a * S + ch] = 1.0f;
+            ns[n] = initial_neuron_state(g, seed + (uint32_t)n * 7919u);
+        }
+        for (int m = 0; m < outputs && m < M; ++m) {
+            const int64_t n = noff[a] + motors[(size_t)a * outputs + m];
+            port[n] = S + m;
+        }
+        for (int64_t e = soff[a]; e < soff[a + 1]; ++e) {
+            sowner[e] = a;
+            snext[e] = e + 1 < soff[a + 1] ? (int)(e + 1) : -1;
+            sg[e].pre += (int)noff[a];
+            sg[e].post += (int)noff[a];
+            ss[e] = initial_synapse_state(sg[e], seed + (uint32_t)e * 104729u);
+        }
+    }
+    cudaMemcpy(d.animals, animals.data(), sizeof(Animal) * P, cudaMemcpyHostToDevice);
+    cudaMemcpy(d.neurons, ng.data(), sizeof(NeuronGene) * N, cudaMemcpyHostToDevice);
+    cudaMemcpy(d.synapses, sg.data(), sizeof(SynapseGene) * E, cudaMemcpyHostToDevice);
+    cudaMemcpy(d.neuron_state, ns.data(), sizeof(NeuronState) * N, cudaMemcpyHostToDevice);
+    cudaMemcpy(d.synapse_state, ss.data(), sizeof(SynapseState) * E, cudaMemcpyHostToDevice);
+    cudaMemcpy(d.neuron_owner, nowner.data(), sizeof(int) * NEURON_CAPACITY, cudaMemcpyHostToDevice);
+    cudaMemcpy(d.synapse_owner, sowner.data(), sizeof(int) * SYNAPSE_CAPACITY, cudaMemcpyHostToDevice);
+    cudaMemcpy(d.neuron_next, nnext.data(), sizeof(int) * N, cudaMemcpyHostToDevice);
+    cudaMemcpy(d.synapse_next, snext.data(), sizeof(int) * E, cudaMemcpyHostToDevice);
+    cudaMemcpy(d.neuron_port, port.data(), sizeof(int) * N, cudaMemcpyHostToDevice);
+    cudaMemcpy(d.senses, senses.data(), sizeof(float) * P * S, cudaMemcpyHostToDevice);
+    auto slots = thrust::make_counting_iterator<int>(0);
+    size_t b1 = 0, b2 = 0, b3 = 0, b4 = 0, b5 = 0, b6 = 0;
+    cub::DeviceSelect::If(nullptr, b1, slots, d.occupied_neurons, d.occupied_neuron_count, NEURON_CAPACITY, OwnedSlot{d.neuron_owner});
+    cub::DeviceSelect::If(nullptr, b2, slots, d.occupied_synapses, d.occupied_synapse_count, SYNAPSE_CAPACITY, OwnedSlot{d.synapse_owner});
+    cub::DeviceSelect::If(nullptr, b3, slots, d.block_animals, d.block_animal_count, P, BlockAnimal{d.animals});
+    cub::DeviceSelect::If(nullptr, b4, slots, d.medium_animals, d.medium_animal_count, P, MediumAnimal{d.animals});
+    cub::DeviceSelect::If(nullptr, b5, slots, d.occupied_neurons, d.occupied_neuron_count, NEURON_CAPACITY, FallbackOwnedSlot{d.neuron_owner, d.animals});
+    cub::DeviceSelect::If(nullptr, b6, slots, d.occupied_synapses, d.occupied_synapse_count, SYNAPSE_CAPACITY, FallbackOwnedSlot{d.synapse_owner, d.animals});
+    w->select_bytes = std::max({b1, b2, b3, b4, b5, b6});
+    cudaMalloc(&w->select_tmp, w->select_bytes);
+    cudaFuncSetAttribute(brain_block_step<BLOCK_BRAIN_NEURONS, BLOCK_BRAIN_SYNAPSES, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         sizeof(BlockBrain<BLOCK_BRAIN_NEURONS, BLOCK_BRAIN_SYNAPSES, false>));
+    cudaFuncSetAttribute(brain_block_step<MEDIUM_BRAIN_NEURONS, MEDIUM_BRAIN_SYNAPSES, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         sizeof(BlockBrain<MEDIUM_BRAIN_NEURONS, MEDIUM_BRAIN_SYNAPSES, false>));
+    if (cudaDeviceSynchronize() != cudaSuccess) { delete w; return nullptr; }
+    return w;
+}
+
+// One world step of the neural stage; returns 0 or a CUDA error code.
+int ref_world_step(void *p) {
+    World &w = *static_cast<World *>(p);
+    Device &d = w.d;
+    const int64_t step = ++w.step;
+    auto slots = thrust::make_counting_iterator<int>(0);
+    int neuron_count = 0, synapse_count = 0, block_count = 0, medium_count = 0;
+    if (w.block_mode) {
+        cub::DeviceSelect::If(w.select_tmp, w.select_bytes, slots, d.block_animals, d.block_animal_count, P, BlockAnimal{d.animals});
+        cub::DeviceSelect::If(w.select_tmp, w.select_bytes, slots, d.medium_animals, d.medium_animal_count, P, MediumAnimal{d.animals});
+        cub::DeviceSelect::If(w.select_tmp, w.select_bytes, slots, d.occupied_neurons, d.occupied_neuron_count, NEURON_CAPACITY, FallbackOwnedSlot{d.neuron_owner, d.animals});
+        cub::DeviceSelect::If(w.select_tmp, w.select_bytes, slots, d.occupied_synapses, d.occupied_synapse_count, SYNAPSE_CAPACITY, FallbackOwnedSlot{d.synapse_owner, d.animals});
+    } else {
+        cub::DeviceSelect::If(w.select_tmp, w.select_bytes, slots, d.occupied_neurons, d.occupied_neuron_count, NEURON_CAPACITY, OwnedSlot{d.neuron_owner});
+        cub::DeviceSelect::If(w.select_tmp, w.select_bytes, slots, d.occupied_synapses, d.occupied_synapse_count, SYNAPSE_CAPACITY, OwnedSlot{d.synapse_owner});
+    }
+    cudaMemcpy(&neuron_count, d.occupied_neuron_count, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemcpy(&synapse_count, d.occupied_synapse_count, sizeof(int), cudaMemcpyDeviceToHost);
+    if (w.block_mode) {
+        cudaMemcpy(&block_count, d.block_animal_count, sizeof(int), cudaMemcpyDeviceToHost);
+        cudaMemcpy(&medium_count, d.medium_animal_count, sizeof(int), cudaMemcpyDeviceToHost);
+    }
+    if (block_count)
+        brain_block_step<BLOCK_BRAIN_NEURONS, BLOCK_BRAIN_SYNAPSES, false>
+            <<<block_count, 128, sizeof(BlockBrain<BLOCK_BRAIN_NEURONS, BLOCK_BRAIN_SYNAPSES, false>)>>>(
+                d, d.block_animals, block_count, (step - 1) * TICKS);
+    if (medium_count)
+        brain_block_step<MEDIUM_BRAIN_NEURONS, MEDIUM_BRAIN_SYNAPSES, false>
+            <<<medium_count, 128, sizeof(BlockBrain<MEDIUM_BRAIN_NEURONS, MEDIUM_BRAIN_SYNAPSES, false>)>>>(
+                d, d.medium_animals, medium_count, (step - 1) * TICKS);
+    for (int t = 0; t < TICKS; ++t) {
+        const int64_t tick = (step - 1) * TICKS + t;
+        if (synapse_count) {
+            if (t == 0)
+                synapse_delivery<<<(synapse_count + NEURAL_BLOCK - 1) / NEURAL_BLOCK, NEURAL_BLOCK>>>(d, tick, synapse_count);
+            else
+                synapse_plasticity_delivery<<<(synapse_count + NEURAL_BLOCK - 1) / NEURAL_BLOCK, NEURAL_BLOCK>>>(
+                    d, tick - 1, tick, synapse_count);
+        }
+        if (neuron_count)
+            neuron_step<<<(neuron_count + NEURAL_BLOCK - 1) / NEURAL_BLOCK, NEURAL_BLOCK>>>(d, tick, neuron_count);
+        if (synapse_count && t == TICKS - 1)
+            synapse_plasticity<<<(synapse_count + NEURAL_BLOCK - 1) / NEURAL_BLOCK, NEURAL_BLOCK>>>(d, tick, synapse_count);
+    }
+    if (neuron_count) homeostasis_step<<<(neuron_count + 255) / 256, 256>>>(d, neuron_count);
+    if (block_count) homeostasis_block_animals<<<(block_count + 127) / 128, 128>>>(d, d.block_animals, block_count);
+    if (medium_count) homeostasis_block_animals<<<(medium_count + 127) / 128, 128>>>(d, d.medium_animals, medium_count);
+    return (int)cudaGetLastError();
+}
+
+int ref_world_sync() { return (int)cudaDeviceSynchronize(); }
+
+// Sum of total_spikes over the first n neuron slots (activity check).
+long long ref_world_total_spikes(void *p, int n) {
+    World &w = *static_cast<World *>(p);
+    std::vector<NeuronState> s(n);
+    cudaMemcpy(s.data(), w.d.neuron_state, sizeof(NeuronState) * n, cudaMemcpyDeviceToHost);
+    long long t = 0;
+    for (auto &x : s) t += x.total_spikes;
+    return t;
+}
+
+void ref_world_destroy(void *p) {
+    World *w = static_cast<World *>(p);
+    Device &d = w->d;
+    void *ptrs[] = {d.animals, d.neurons, d.synapses, d.neuron_state, d.synapse_state, d.neuron_owner,
+                    d.synapse_owner, d.occupied_neurons, d.occupied_synapses, d.occupied_neuron_count,
+                    d.occupied_synapse_count, d.block_animals, d.block_animal_count, d.medium_animals,
+                    d.medium_animal_count, d.neuron_next, d.synapse_next, d.neuron_port, d.pending_exc,
+                    d.pending_inh, d.mod_event_tick, d.spike_history, d.senses, d.motors, d.trace_exc_arrivals,
+                    d.trace_exc_releases, d.trace_inh_arrivals, d.trace_exc_ns, d.trace_inh_ns, d.trace_peak_mv,
+                    w->select_tmp};
+    for (void *q : ptrs) cudaFree(q);
+    delete w;
+}
+
+}  // extern "C"
