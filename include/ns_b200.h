@@ -80,6 +80,16 @@ void *nsb_gpu_create_rows(int brains, const int64_t *neuron_offsets, const int64
 /* Asynchronous step on device memory (cudaStream_t passed as void*). */
 int nsb_gpu_step_device(void *batch, const float *d_input, const uint8_t *d_mask, int ticks, float gain,
                         float *d_output, int *d_status, void *stream);
+/* No counterpart in the reference. Allocation-free step for callers that may
+ * not allocate device memory when they step (their device memory belongs to
+ * another allocator, or they forbid allocation once started): the same tick as
+ * nsb_gpu_step_device, with the kernel's scratch memory in a static device
+ * array (4 MiB + 256 B, held by every GPU that loads the library until exit)
+ * instead of library-allocated buffers. Rejects batches above 2,097,152
+ * synapses. The first call on a device sets up the array's address (make it
+ * before any stream capture); calls that overlap on the GPU race. */
+int nsb_gpu_step_noalloc(void *batch, const float *d_input, const uint8_t *d_mask, int ticks, float gain,
+                         float *d_output, int *d_status, void *stream);
 /* Step on the batch's own device buffers, replayed from a captured CUDA graph. */
 int nsb_gpu_step_graph(void *batch, int ticks, float gain, void *stream);
 /* Copy host observations (count x channels) and/or mask (count) into the

@@ -363,6 +363,28 @@ int nsb_gpu_step_device(void *p, const float *d_input, const uint8_t *d_mask, in
     }
 }
 
+// Allocation-free step (no counterpart in the reference): the same tick as
+// nsb_gpu_step_device, for callers that may not allocate device memory when
+// they step — processes whose device memory all belongs to another allocator
+// (a host application's memory pool) or that forbid allocation once started.
+// The kernel's scratch (work-queue counters, per-synapse plasticity
+// bookkeeping) lives in a static device array of 4 MiB + 256 B that every GPU
+// loading this library keeps until exit; batches above 2,097,152 synapses are
+// rejected. The first call on a device looks up that array's address and
+// should come before any stream capture. Calls that overlap on the GPU race
+// on the shared array. Inputs and outputs are caller device buffers.
+int nsb_gpu_step_noalloc(void *p, const float *d_input, const uint8_t *d_mask, int ticks, float gain,
+                         float *d_output, int *d_status, void *stream) {
+    try {
+        static_cast<GpuBatch *>(p)->engine->step_noalloc(d_input, d_mask, ticks, gain, d_output, d_status,
+                                                         static_cast<cudaStream_t>(stream));
+        return 0;
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
 // Replays the step on the batch's own device buffers from a captured CUDA graph.
 int nsb_gpu_step_graph(void *p, int ticks, float gain, void *stream) {
     try {

@@ -32,6 +32,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
 
@@ -842,6 +843,64 @@ void Engine::launch(const float *d_input, const uint8_t *d_mask, int ticks, floa
     if (n_units_ > n_light_units_)
         tick_kernel<true><<<grid_heavy_, block_, smem_, stream>>>(P, n_light_units_, n_units_, d_queue_ + 1, d_input,
                                                                    d_mask, d_output, d_status, ticks, gain);
+    NSB_CHECK(cudaGetLastError());
+}
+
+// ---- allocation-free step ----------------------------------------------------
+// For callers that may not allocate device memory when they step: processes
+// whose device memory all belongs to another allocator (a host application's
+// memory pool, a framework that owns the GPU heap) or that run under a
+// no-allocation rule once started. The tick kernel's scratch memory — the
+// work-queue counters and the per-synapse record of the last tick at which
+// plasticity was applied — comes from this file-scope array instead of
+// engine-allocated buffers. Every GPU that loads this library holds the array
+// (256 B + 2 B x kNoAllocMaxSynapses = 4 MiB + 256 B) until the process exits.
+constexpr int kNoAllocMaxSynapses = 2097152;
+constexpr size_t kNoAllocScratchBytes = 256 + sizeof(int16_t) * (size_t)kNoAllocMaxSynapses;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch on the current device, looked up once
+// per device (the host-side name is only a stand-in for the device array).
+static unsigned char *noalloc_scratch_address() {
+    static std::mutex lock;
+    static unsigned char *addr[64] = {};
+    int dev = 0;
+    NSB_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw std::runtime_error("Device index outside the scratch table");
+    std::lock_guard<std::mutex> guard(lock);
+    if (!addr[dev]) {
+        void *ptr = nullptr;
+        const cudaError_t rc = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (rc != cudaSuccess)
+            throw std::runtime_error(std::string("CUDA: scratch address lookup failed: ") + cudaGetErrorString(rc));
+        addr[dev] = static_cast<unsigned char *>(ptr);
+    }
+    return addr[dev];
+}
+
+void Engine::step_noalloc(const float *d_input, const uint8_t *d_mask, int ticks, float gain, float *d_output,
+                          int *d_status, cudaStream_t stream) {
+    if (ticks < 1 || ticks > 10000 || !std::isfinite(gain) || gain < 0)
+        throw std::runtime_error("Invalid neural integration interval");
+    if (n_synapses_ > kNoAllocMaxSynapses)
+        throw std::runtime_error("Batch has " + std::to_string(n_synapses_) +
+                                 " synapses; the allocation-free step supports at most 2097152");
+    unsigned char *scratch = noalloc_scratch_address();
+    int *queue = reinterpret_cast<int *>(scratch);
+    int16_t *lastp = reinterpret_cast<int16_t *>(scratch + 256);
+    cudaStream_t s = stream ? stream : stream_;
+    // The array keeps the previous call's contents: reset the queue counters
+    // to 0 and the plasticity bookkeeping to -1 ("none this call").
+    NSB_CHECK(cudaMemsetAsync(queue, 0, 2 * sizeof(int), s));
+    NSB_CHECK(cudaMemsetAsync(lastp, 0xff, sizeof(int16_t) * (size_t)std::max(n_synapses_, 1), s));
+    Pools P = pools(false);
+    P.slastp = lastp;
+    if (n_light_units_ > 0)
+        tick_kernel<false><<<grid_, block_, smem_, s>>>(P, 0, n_light_units_, queue, d_input, d_mask, d_output,
+                                                         d_status, ticks, gain);
+    if (n_units_ > n_light_units_)
+        tick_kernel<true><<<grid_heavy_, block_, smem_, s>>>(P, n_light_units_, n_units_, queue + 1, d_input, d_mask,
+                                                              d_output, d_status, ticks, gain);
     NSB_CHECK(cudaGetLastError());
 }
 

@@ -59,6 +59,11 @@ public:
     // No validation; ticks in [1, 10000], inputs in [0, 1].
     void step_device(const float *d_input, const uint8_t *d_mask, int ticks, float gain, float *d_output,
                      int *d_status, cudaStream_t stream);
+    // step_device with the kernel's scratch memory in a static device array
+    // instead of engine buffers: allocates nothing. At most 2,097,152 synapses;
+    // calls that overlap on the GPU race on the shared array.
+    void step_noalloc(const float *d_input, const uint8_t *d_mask, int ticks, float gain, float *d_output,
+                      int *d_status, cudaStream_t stream);
     // Captures step_device on the engine's own buffers into a CUDA graph and
     // replays it (one graph per (ticks, gain)).
     void step_graph(int ticks, float gain, cudaStream_t stream);

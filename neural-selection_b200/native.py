@@ -43,6 +43,7 @@ SIGNATURES = {
     "nsb_gpu_create_rows": (_vp, [ct.c_int, _i64, _i64, _f, _f, _i32, ct.c_int, ct.c_int, ct.c_int, ct.c_int]),
     "nsb_gpu_step_device": (ct.c_int, [_vp, _vp, _vp, ct.c_int, ct.c_float, _vp, _vp, _vp]),
     "nsb_gpu_step_graph": (ct.c_int, [_vp, ct.c_int, ct.c_float, _vp]),
+    "nsb_gpu_step_noalloc": (ct.c_int, [_vp, _vp, _vp, ct.c_int, ct.c_float, _vp, _vp, _vp]),
     "nsb_gpu_buffer": (_vp, [_vp, ct.c_int]),
     "nsb_gpu_upload": (ct.c_int, [_vp, _f, _u8]),
     "nsb_gpu_download": (ct.c_int, [_vp, _f, _i32]),
@@ -197,6 +198,12 @@ class GpuBatch:
     def step_device(self, d_input, d_mask, ticks, gain, d_output, d_status, stream=0):
         if self.lib.nsb_gpu_step_device(self.ptr, d_input, d_mask, int(ticks), float(gain), d_output, d_status,
                                         stream):
+            raise RuntimeError(_err(self.lib))
+
+    def step_noalloc(self, d_input, d_mask, ticks, gain, d_output, d_status, stream=0):
+        """Allocation-free step on caller device buffers (see nsb_gpu_step_noalloc)."""
+        if self.lib.nsb_gpu_step_noalloc(self.ptr, d_input, d_mask, int(ticks), float(gain), d_output, d_status,
+                                         stream):
             raise RuntimeError(_err(self.lib))
 
     def step_graph(self, ticks=16, gain=230.0, stream=0):
