@@ -123,14 +123,19 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def workload(nsb, seed):
-    cache = Path(os.environ.get("NSB_BENCH_CACHE", "/tmp")) / f"nsb_uneven_full_seed{seed}.npz"
+def workload(nsb, seed, fraction=1):
+    """The full-pool workload, or with --fraction D a 1/D slice of it (brains,
+    neuron and synapse pools all divided by D; same size distribution) for
+    profiler captures that must stay small."""
+    tag = "full" if fraction == 1 else f"div{fraction}"
+    cache = Path(os.environ.get("NSB_BENCH_CACHE", "/tmp")) / f"nsb_uneven_{tag}_seed{seed}.npz"
     W = nsb.workloads
     if cache.exists():
         z = np.load(cache)
         return W.Batch(z["nr"], z["sr"], z["no"], z["so"], z["mo"], int(z["ch"]), int(z["md"]), "batched_uneven",
                        z["inp"], 230.0, {})
-    b = W.batched_uneven(seed=seed)
+    b = W.batched_uneven(seed=seed, brains=32768 // fraction, total_neurons=4194304 // fraction,
+                         total_synapses=8388608 // fraction)
     try:
         np.savez(cache, nr=b.neuron_rows, sr=b.synapse_rows, no=b.neuron_offsets, so=b.synapse_offsets,
                  mo=b.motors, ch=b.channels, md=b.max_delay, inp=b.inputs)
@@ -352,7 +357,7 @@ def run_ours(args, rank, world, local_rank):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     nsb = load_package()
-    batch = workload(nsb, 2 + rank)
+    batch = workload(nsb, 2 + rank, args.fraction)
     N = len(batch.neuron_rows)
     E = len(batch.synapse_rows)
     gpu = nsb.GpuBatch.from_rows(batch)
@@ -424,14 +429,17 @@ def run_ours(args, rank, world, local_rank):
         algo = ALGO_BYTES_PER_NEURON * N + ALGO_BYTES_PER_SYNAPSE * E
         achieved = algo / (ms_step / 1e3) / 1e9
         traffic = traffic_per_launch()
+        if traffic is not None:
+            traffic /= args.fraction
         clocks = clk.summary()
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (Philox4x32-10, seed 2 + rank)",
-                "config": {"workload": "batched_uneven_full_pools", "brains": batch.brains, "neurons": N,
+                "config": {"workload": "batched_uneven_full_pools" if args.fraction == 1 else
+                           f"batched_uneven_1/{args.fraction}_pools", "brains": batch.brains, "neurons": N,
                            "synapses": E, "ticks_per_step": 16, "delays_ms": "1-16", "parallelism": f"replicas x{world}",
                            "units": st["units"], "grid": st["grid"], "block": st["block"],
-                           "l2": "device state 1.4 GB > 126 MB L2: each step streams it from HBM"},
+                           "l2": f"device state {(120 * N + 108 * E) / 1e9:.2f} GB > 126 MB L2: inputs larger than L2"},
                 "synaptic_events_per_s": events_per_s,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
@@ -463,6 +471,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-cuda"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fraction", type=int, default=1, choices=[1, 2, 4, 8, 16],
+                    help="run a 1/D slice of the full pools (profiler captures only)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus if "RANK" in os.environ else 1))
