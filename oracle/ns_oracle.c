@@ -70,6 +70,11 @@ static void init_consts(void) {
 
 static inline float clampf(float x, float lo, float hi) { return fminf(hi, fmaxf(lo, x)); }
 
+/* Decisions of the last binary32 call, read by the FP64 shadow (further down)
+ * so that it follows the same spike, receptor-event and release outcomes. */
+static __thread int dec_rec_event, dec_released;
+static __thread unsigned dec_subspikes;
+
 /* ---- records ------------------------------------------------------------- */
 typedef struct {               /* src/physiology.cuh:29-45 */
     float cap, gl, el, vt, slope, a, tau_w, b, vr, adp_b, adp_tau;
@@ -285,6 +290,7 @@ static void lfs_step(const ngene *g, nstate *s, float cur, float exc, float inh)
     u[0] = v + i / g->cap;
     s->spike = u[0] >= u[1];
     if (s->spike) {
+        dec_subspikes = 1u;
         u[1] = 200.0f;
         for (int j = 0; j < 3; ++j) act[j] += 1.0f;
         ++s->total;
@@ -315,7 +321,8 @@ static float receptor_drive(const ngene *g, nstate *s, float level) {  /* physio
     s->rec_rng = xorshift32(s->rec_rng);
     float u = (float)(s->rec_rng >> 8) * (1.0f / 16777216.0f);
     s->rec_ns *= OEXP(-DT / g->rec_decay);
-    if (u < rate * (DT / 1000.0f)) s->rec_ns += g->rec_event;
+    dec_rec_event = u < rate * (DT / 1000.0f);
+    if (dec_rec_event) s->rec_ns += g->rec_event;
     return s->rec_ns * (E_EXC - s->v);
 }
 
@@ -339,6 +346,7 @@ static void neuron_tick(const ngene *g, nstate *s, float cur, const float *exc_i
     s->depol += 0.1f * (sub - s->depol);
     s->inh += inh_in;
     s->spike = 0;
+    dec_subspikes = 0;
     if (g->type == 6 || g->type == 2 || g->type == 3) {
         float exc = 0;
         for (int k = 0; k < BRANCHES; ++k) exc += s->dend[k];
@@ -371,6 +379,7 @@ static void neuron_tick(const ngene *g, nstate *s, float cur, const float *exc_i
                    s->inh * (E_INH - v) + cur + s->adp - s->w - clamp_leak * (v - clamp_rev);
         s->v = v + H_SUB * dv / g->cap;
         if (s->v >= 0.0f) {
+            dec_subspikes |= 1u << step;
             s->spike = 1; ++s->total;
             s->v = g->vr; s->w += g->b; s->adp += g->adp_b;
         }
@@ -423,6 +432,7 @@ static float release(const sgene *g, sstate *s, int64_t tick) {  /* 425-454 */
         if ((s->ready & bit) && uniform24(s) < s->ru) { s->ready &= ~bit; ++released; }
     }
     s->last = tick;
+    dec_released = released;
     float out = s->w * (float)released / (float)n * s->slow;
     if (g->slow_rec > 0) s->slow *= 1.0f - g->slow_depl;
     return out;
@@ -515,7 +525,30 @@ struct or_brain {
     float *exc, *inh; uint8_t *mod;
     uint32_t *orig_n, *orig_s;
     int64_t tick, events;
+    struct or_shadow *sh;       /* FP64 shadow, or NULL */
 };
+
+/* ---- FP64 shadow ----------------------------------------------------------------
+ * The same equations in binary64 (decimal constants, exp/log of libm in
+ * double), stepped beside the binary32 state. Every discrete outcome (spike
+ * and the substep it fell in, receptor event, released site count, modulator
+ * bits, the depolarisation gate of profile 2) is taken from the binary32 run,
+ * so the two trajectories differ only by rounding and the tracked maxima are
+ * the binary32 state's error against the FP64 model. LP and Prinz cells
+ * (types 2 and 3) have no shadow. */
+typedef struct { double v, w, adp, inh, depol, log_ampa, dend[BRANCHES], u[8], rec_ns; } dnstate;
+typedef struct { double w, ru, pre_tr, post_tr, el_ltp, el_ltd, da_age, spine, st_age, pre_age, post_age, slow; } dsstate;
+struct or_shadow {
+    dnstate *n; dsstate *s; double *exc, *inh;
+    double maxabs[OR_SHADOW_FIELDS], maxrel[OR_SHADOW_FIELDS];
+    int64_t ticks;
+};
+static void sh_sync(or_brain *b);
+static void sh_deliver(or_brain *b, int j, int64_t last0);
+static void sh_neuron(or_brain *b, int j, const float *input, float gain);
+static void sh_plast(or_brain *b, int j, int pair);
+static void sh_track(or_brain *b, int tick_end);
+static void sh_homeo(or_brain *b, int j, int ticks);
 
 static int bad(char *err, int len, const char *msg) { if (err && len > 0) snprintf(err, (size_t)len, "%s", msg); return 0; }
 
@@ -594,6 +627,7 @@ void or_destroy(or_brain *b) {
     if (!b) return;
     free(b->ng); free(b->sg); free(b->ns); free(b->ss); free(b->motors); free(b->sensory);
     free(b->hist); free(b->exc); free(b->inh); free(b->mod); free(b->orig_n); free(b->orig_s);
+    if (b->sh) { free(b->sh->n); free(b->sh->s); free(b->sh->exc); free(b->sh->inh); free(b->sh); }
     free(b);
 }
 
@@ -608,6 +642,7 @@ void or_reset(or_brain *b, uint32_t seed) {                    /* core.cuh:25-29
         uint32_t idx = b->orig_s ? b->orig_s[i] : (uint32_t)i;
         b->ss[i] = synapse_initial(&b->sg[i], seed + idx * 104729u);
     }
+    if (b->sh) sh_sync(b);
 }
 
 static int edge_live(const or_brain *b, const sgene *g) {
@@ -624,6 +659,10 @@ int or_step(or_brain *b, const float *input, int ticks, float gain, float *outpu
         memset(b->exc, 0, sizeof(float) * (size_t)b->count * BRANCHES);
         memset(b->inh, 0, sizeof(float) * (size_t)b->count);
         memset(b->mod, 0, (size_t)b->count);
+        if (b->sh) {
+            memset(b->sh->exc, 0, sizeof(double) * (size_t)b->count * BRANCHES);
+            memset(b->sh->inh, 0, sizeof(double) * (size_t)b->count);
+        }
         for (int j = 0; j < b->edges; ++j) {                     /* delivery, edge order */
             const sgene *g = &b->sg[j]; sstate *s = &b->ss[j];
             s->arrived = 0;
@@ -633,7 +672,9 @@ int or_step(or_brain *b, const float *input, int ticks, float gain, float *outpu
             if (!s->arrived) continue;
             ++b->events;
             const ngene *src = &b->ng[g->pre];
+            const int64_t last0 = s->last;
             float rel = (!src->inh_tx || src->modulator) ? release(g, s, b->tick) : s->w;
+            if (b->sh) sh_deliver(b, j, last0);
             if (src->modulator) { if (rel > 0) b->mod[g->post] |= (uint8_t)(1u << (src->modulator - 1)); }
             else if (src->inh_tx) b->inh[g->post] += rel;
             else b->exc[(size_t)g->post * BRANCHES + g->branch] += rel * OEXP(b->ns[g->post].log_ampa);
@@ -645,6 +686,7 @@ int or_step(or_brain *b, const float *input, int ticks, float gain, float *outpu
                 if (b->sensory[j] >= 0)
                     cur = g->type == 5 ? receptor_drive(g, s, input[b->sensory[j]]) : gain * input[b->sensory[j]];
                 neuron_tick(g, s, cur, b->exc + (size_t)j * BRANCHES, b->inh[j]);
+                if (b->sh) sh_neuron(b, j, input, gain);
                 if (!isfinite(s->v)) {
                     /* ns_step keeps its tick counter on failure (native.cpp:176-177) */
                     if (stop_on_nonfinite) { b->tick = tick0; return -1; }
@@ -660,14 +702,278 @@ int or_step(or_brain *b, const float *input, int ticks, float gain, float *outpu
             const ngene *a = &b->ng[g->pre], *z = &b->ng[g->post];
             int pair = !a->inh_tx && excitatory_kind(a->type) && !a->modulator && !z->inh_tx && excitatory_kind(z->type);
             plasticity_tick(g, s, s->arrived, b->ns[g->post].spike, pair, b->ns[g->post].depol, b->mod[g->post]);
+            if (b->sh) sh_plast(b, j, pair);
         }
         for (int j = 0; j < b->outputs; ++j) output[j] += (float)b->ns[b->motors[j]].spike;
+        if (b->sh) sh_track(b, 1);
     }
     for (int j = 0; j < b->count; ++j)                            /* homeostasis, core.cuh:71-72 */
-        if (b->ng[j].active)
+        if (b->ng[j].active) {
             homeostasis(&b->ng[j], &b->ns[j], (float)ticks,
                         (float)b->ns[j].total * 1000.0f / (float)(ticks > b->tick ? ticks : b->tick));
+            if (b->sh) sh_homeo(b, j, ticks);
+        }
+    if (b->sh) sh_track(b, 0);
     return failed ? -1 : 0;
+}
+
+/* ---- FP64 shadow: equations ------------------------------------------------ */
+static double dclamp(double x, double lo, double hi) { return fmin(hi, fmax(lo, x)); }
+
+static void sh_copy_neuron(dnstate *d, const nstate *s) {
+    d->v = s->v; d->w = s->w; d->adp = s->adp; d->inh = s->inh; d->depol = s->depol;
+    d->log_ampa = s->log_ampa; d->rec_ns = s->rec_ns;
+    for (int k = 0; k < BRANCHES; ++k) d->dend[k] = s->dend[k];
+    for (int k = 0; k < 8; ++k) d->u[k] = s->u[k];
+}
+static void sh_copy_synapse(dsstate *d, const sstate *s) {
+    d->w = s->w; d->ru = s->ru; d->pre_tr = s->pre_tr; d->post_tr = s->post_tr; d->el_ltp = s->el_ltp;
+    d->el_ltd = s->el_ltd; d->da_age = s->da_age; d->spine = s->spine; d->st_age = s->st_age;
+    d->pre_age = s->pre_age; d->post_age = s->post_age; d->slow = s->slow;
+}
+static void sh_sync(or_brain *b) {
+    for (int i = 0; i < b->count; ++i) sh_copy_neuron(&b->sh->n[i], &b->ns[i]);
+    for (int i = 0; i < b->edges; ++i) sh_copy_synapse(&b->sh->s[i], &b->ss[i]);
+}
+
+int or_shadow_enable(or_brain *b) {
+    for (int i = 0; i < b->count; ++i)
+        if (b->ng[i].active && (b->ng[i].type == 2 || b->ng[i].type == 3)) return -1;
+    if (!b->sh) {
+        struct or_shadow *sh = (struct or_shadow *)calloc(1, sizeof *sh);
+        sh->n = (dnstate *)calloc((size_t)b->count, sizeof(dnstate));
+        sh->s = (dsstate *)calloc((size_t)(b->edges ? b->edges : 1), sizeof(dsstate));
+        sh->exc = (double *)calloc((size_t)b->count * BRANCHES, sizeof(double));
+        sh->inh = (double *)calloc((size_t)b->count, sizeof(double));
+        b->sh = sh;
+    }
+    sh_sync(b);
+    return 0;
+}
+
+/* release() (physiology.cuh:425-454) with the released site count given. */
+static double sh_release(const sgene *g, dsstate *d, int64_t last0, int64_t tick, int released) {
+    if (last0 > -1000000) {
+        const double dt = (double)(tick - last0);
+        if (g->tfac > 0) d->ru *= exp(-dt / g->tfac);
+        if (g->slow_rec > 0) d->slow = 1.0 - (1.0 - d->slow) * exp(-dt / g->slow_rec);
+    }
+    d->ru = g->tfac > 0 ? d->ru + g->U * (1.0 - d->ru) : g->U;
+    const double out = d->w * (double)released / (double)sites_of(g) * d->slow;
+    if (g->slow_rec > 0) d->slow *= 1.0 - (double)g->slow_depl;
+    return out;
+}
+
+static void sh_deliver(or_brain *b, int j, int64_t last0) {
+    const sgene *g = &b->sg[j];
+    const ngene *src = &b->ng[g->pre];
+    dsstate *d = &b->sh->s[j];
+    const double rel = (!src->inh_tx || src->modulator) ? sh_release(g, d, last0, b->tick, dec_released) : d->w;
+    if (src->modulator) return;                 /* modulator bits come from the binary32 run */
+    if (src->inh_tx) b->sh->inh[g->post] += rel;
+    else b->sh->exc[(size_t)g->post * BRANCHES + g->branch] += rel * exp(b->sh->n[g->post].log_ampa);
+}
+
+static double sh_branch_gain(double gs) {
+    const double regen = 5.0 / (1.0 + exp(-(gs - 4.0) / 0.4));
+    return fmin(11.0, gs + regen - 5.0 / (1.0 + exp(10.0)));
+}
+
+/* neuron_tick (physiology.cuh:290-374) and lfs_advance (258-287) in binary64;
+ * spikes and receptor events as decided by the binary32 step just taken. */
+static void sh_neuron(or_brain *b, int j, const float *input, float gain) {
+    const ngene *g = &b->ng[j];
+    dnstate *d = &b->sh->n[j];
+    const double *exc_in = b->sh->exc + (size_t)j * BRANCHES;
+    double cur = 0;
+    if (b->sensory[j] >= 0) {
+        if (g->type == 5) {
+            if (g->sens >= 0 && g->rec_event > 0) {
+                d->rec_ns *= exp(-1.0 / g->rec_decay);
+                if (dec_rec_event) d->rec_ns += g->rec_event;
+                cur = d->rec_ns * (0.0 - d->v);
+            }
+        } else cur = (double)gain * (double)input[b->sensory[j]];
+    }
+    for (int k = 0; k < BRANCHES; ++k) d->dend[k] += exc_in[k];
+    const double sub = fmax(0.0, fmin(d->v, -50.0) - g->el);
+    d->depol += 0.1 * (sub - d->depol);
+    d->inh += b->sh->inh[j];
+    if (g->type == 6) {
+        static const double wt[3] = {250.0, 10.0, 4.0}, op[3] = {10.0, 40.0, 750.0}, cl[3] = {50.0, 750.0, 2000.0};
+        double *u = d->u, *act = u + 2, *open = u + 5, exc = 0, under = 0;
+        for (int k = 0; k < BRANCHES; ++k) exc += d->dend[k];
+        u[1] = g->vt + (u[1] - g->vt) * exp(-0.1);
+        for (int k = 0; k < 3; ++k) {
+            open[k] += act[k] / op[k] - open[k] / cl[k];
+            act[k] *= exp(-1.0 / op[k]);
+            under += wt[k] * open[k];
+        }
+        const double v = u[0];
+        const double i = g->gl * (g->el - v) + exc * (10.0 - v) + d->inh * (-60.0 - v) + under * (-80.0 - v) + cur;
+        u[0] = v + i / g->cap;
+        if (dec_subspikes & 1u) {
+            u[1] = 200.0;
+            for (int k = 0; k < 3; ++k) act[k] += 1.0;
+        }
+        d->v = u[0];
+        for (int k = 0; k < BRANCHES; ++k) d->dend[k] *= exp(-1.0 / 3.0);
+        d->inh *= exp(-1.0 / 10.0);
+        return;
+    }
+    const double h = 0.25;
+    for (int step = 0; step < SUBSTEPS; ++step) {
+        const double v = d->v;
+        d->w += h * (g->a * (v - g->el) - d->w) / g->tau_w;
+        const double expo = dclamp((v - g->vt) / g->slope, -20.0, 10.0);
+        double soma = 0;
+        for (int k = 0; k < BRANCHES; ++k) soma += g->type == 0 ? sh_branch_gain(d->dend[k]) : d->dend[k];
+        const double dv = g->gl * (g->el - v) + (double)g->gl * g->slope * exp(expo) + soma * (0.0 - v) +
+                          d->inh * (-75.0 - v) + cur + d->adp - d->w;
+        d->v = v + h * dv / g->cap;
+        if (dec_subspikes >> step & 1u) { d->v = g->vr; d->w += g->b; d->adp += g->adp_b; }
+        if (g->adp_tau > 0) d->adp *= exp(-h / g->adp_tau);
+        for (int k = 0; k < BRANCHES; ++k) d->dend[k] *= exp(-h / 3.0);
+        d->inh *= exp(-h / 10.0);
+    }
+}
+
+static double sh_da_window(double age) {
+    if (age < 0 || age > 20000.0) return 0;
+    const double x = age / 2000.0;
+    return x * x * x * x * exp(4.0 * (1.0 - x));
+}
+static double sh_spine_window(double age) {
+    if (age < 0 || age > 5000.0) return 0;
+    const double x = age / 1000.0;
+    return x * x * x * exp(3.0 * (1.0 - x));
+}
+
+/* plasticity_tick (physiology.cuh:459-555) in binary64. Ages are whole
+ * milliseconds in both precisions, so their comparisons agree exactly; the
+ * profile-2 depolarisation gate reads the binary32 depolarisation. */
+static void sh_plast(or_brain *b, int j, int pair) {
+    const sgene *g = &b->sg[j];
+    if (!g->plast || !pair) return;
+    dsstate *d = &b->sh->s[j];
+    const int arrived = b->ss[j].arrived, post_spike = b->ns[g->post].spike;
+    const unsigned char mod = b->mod[g->post];
+    const double w0 = g->w0;
+    if (g->plast == 5) {
+        if (d->st_age >= 0) { d->st_age += 1.0; if (d->st_age > 5000.0) d->st_age = -1; }
+        d->pre_age += 1.0;
+        if (arrived) d->pre_age = 0;
+        if (post_spike && d->pre_age <= 15.0 && d->st_age < 0) d->st_age = 0;
+        if ((mod & MOD_DA) && (g->receptors & MOD_DA))
+            d->spine = dclamp(d->spine + 0.025 * sh_spine_window(d->st_age), 1.0, 2.0);
+        return;
+    }
+    if (g->plast == 4) {
+        if (d->da_age >= 0) { d->da_age += 1.0; if (d->da_age > 20000.0) d->da_age = -1; }
+        d->pre_age += 1.0;
+        if (arrived) d->pre_age = 0;
+        if (post_spike && d->pre_age <= 15.0 && (d->da_age < 0 || d->da_age > 30.0)) {
+            d->da_age = 0;
+            d->w -= 0.005383 * w0;
+        }
+        if ((mod & MOD_DA) && (g->receptors & MOD_DA)) {
+            d->w += 0.00453 * sh_da_window(d->da_age) * w0;
+            d->da_age = -1;
+        }
+        d->w = dclamp(d->w, 0.0, 2.0 * w0);
+        return;
+    }
+    if (g->plast == 3) {
+        d->el_ltp *= exp(-1.0 / 7200.0);
+        d->el_ltd *= exp(-1.0 / 3600.0);
+        d->pre_age += 1.0; d->post_age += 1.0;
+        if (arrived) { if (d->post_age <= 15.0) d->el_ltd += 1.0; d->pre_age = 0; }
+        if (post_spike) { if (d->pre_age <= 15.0) d->el_ltp += 1.0; d->post_age = 0; }
+        if ((mod & MOD_NE) && (g->receptors & MOD_NE)) { d->w += 0.0048 * d->el_ltp * w0; d->el_ltp = 0; }
+        if ((mod & MOD_5HT) && (g->receptors & MOD_5HT)) { d->w -= 0.0075 * d->el_ltd * w0; d->el_ltd = 0; }
+        d->w = dclamp(d->w, 0.0, 2.0 * w0);
+        return;
+    }
+    d->pre_tr *= exp(-1.0 / 17.0);
+    d->post_tr *= exp(-1.0 / 34.0);
+    d->pre_age += 1.0; d->post_age += 1.0;
+    if (arrived) {
+        if (d->post_age <= (g->plast == 2 ? 50.0 : 20.0)) d->w *= 1.0 - 0.004 * d->post_tr;
+        d->pre_tr += 1.0;
+        d->pre_age = 0;
+    }
+    if (post_spike) {
+        if (d->pre_age <= 20.0 && (g->plast == 1 || b->ns[g->post].depol >= 2.3f))
+            d->w += 0.016 * d->pre_tr * (2.0 * w0 - d->w);
+        d->post_tr += 1.0;
+        d->post_age = 0;
+    }
+    d->w = dclamp(d->w, 0.0, 2.0 * w0);
+}
+
+/* homeostatic_advance (physiology.cuh:243-253) in binary64. */
+static void sh_homeo(or_brain *b, int j, int ticks) {
+    const ngene *g = &b->ng[j];
+    if (g->type != 0) return;
+    dnstate *d = &b->sh->n[j];
+    const double elapsed = ticks;
+    const double hz = (double)b->ns[j].total * 1000.0 / (double)(ticks > b->tick ? ticks : b->tick);
+    const double ratio = dclamp(hz / 0.4, 0.0, 2.65);
+    const double change = ratio < 1.0 ? log(1.92) * (1.0 - ratio) : log(0.70) * ((ratio - 1.0) / 1.65);
+    d->log_ampa = dclamp(d->log_ampa + change * (elapsed / 172800000.0), -3.0, 3.0);
+}
+
+/* Fields: see or_shadow_field. Relative error = |x32 - x64| / max(|x64|, floor). */
+static const char *const SH_NAMES[OR_SHADOW_FIELDS] = {
+    "V_mV", "w_adapt_pA", "adp_pA", "g_inh_nS", "g_dend_nS", "log_ampa", "depol_mV", "g_receptor_nS",
+    "syn_w_nS", "syn_u", "syn_slow", "syn_pre_trace", "syn_post_trace", "syn_eligibility",
+    "V_subthreshold_mV"};
+static const double SH_FLOOR[OR_SHADOW_FIELDS] = {1.0, 1.0, 1.0, 1e-3, 1e-3, 1e-3, 1.0, 1e-3,
+                                                 1e-3, 1e-3, 1e-3, 1e-3, 1e-3, 1e-3, 1.0};
+const char *or_shadow_field(int i) { return i >= 0 && i < OR_SHADOW_FIELDS ? SH_NAMES[i] : ""; }
+
+static void sh_err(struct or_shadow *sh, int f, float x32, double x64) {
+    if (!isfinite(x32) || !isfinite(x64)) return;
+    const double e = fabs((double)x32 - x64);
+    const double r = e / fmax(fabs(x64), SH_FLOOR[f]);
+    if (e > sh->maxabs[f]) sh->maxabs[f] = e;
+    if (r > sh->maxrel[f]) sh->maxrel[f] = r;
+}
+
+static void sh_track(or_brain *b, int tick_end) {
+    struct or_shadow *sh = b->sh;
+    sh->ticks += tick_end;
+    for (int i = 0; i < b->count; ++i) {
+        const ngene *g = &b->ng[i];
+        if (!g->active) continue;
+        const nstate *s = &b->ns[i]; const dnstate *d = &sh->n[i];
+        sh_err(sh, 0, s->v, d->v); sh_err(sh, 1, s->w, d->w);
+        if (d->v < g->vt) sh_err(sh, 14, s->v, d->v); sh_err(sh, 2, s->adp, d->adp);
+        sh_err(sh, 3, s->inh, d->inh);
+        for (int k = 0; k < BRANCHES; ++k) sh_err(sh, 4, s->dend[k], d->dend[k]);
+        sh_err(sh, 5, s->log_ampa, d->log_ampa); sh_err(sh, 6, s->depol, d->depol);
+        sh_err(sh, 7, s->rec_ns, d->rec_ns);
+    }
+    for (int i = 0; i < b->edges; ++i) {
+        if (!edge_live(b, &b->sg[i])) continue;
+        const sstate *s = &b->ss[i]; const dsstate *d = &sh->s[i];
+        sh_err(sh, 8, s->w, d->w); sh_err(sh, 9, s->ru, d->ru); sh_err(sh, 10, s->slow, d->slow);
+        sh_err(sh, 11, s->pre_tr, d->pre_tr); sh_err(sh, 12, s->post_tr, d->post_tr);
+        sh_err(sh, 13, s->el_ltp, d->el_ltp); sh_err(sh, 13, s->el_ltd, d->el_ltd);
+    }
+}
+
+void or_shadow_dump(const or_brain *b, double *v, double *syn_w) {
+    if (!b->sh) return;
+    if (v) for (int i = 0; i < b->count; ++i) v[i] = b->sh->n[i].v;
+    if (syn_w) for (int i = 0; i < b->edges; ++i) syn_w[i] = b->sh->s[i].w;
+}
+
+int64_t or_shadow_stats(const or_brain *b, double *maxabs, double *maxrel) {
+    if (!b->sh) return -1;
+    memcpy(maxabs, b->sh->maxabs, sizeof b->sh->maxabs);
+    memcpy(maxrel, b->sh->maxrel, sizeof b->sh->maxrel);
+    return b->sh->ticks;
 }
 
 static uint32_t fw(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }

@@ -48,6 +48,24 @@ int or_edges(const or_brain *b);
 /* Number of synapses that arrived (delivered a spike) during the last or_step. */
 int64_t or_last_events(const or_brain *b);
 
+/* FP64 shadow: the same equations in binary64, stepped beside the binary32
+ * state with the binary32 run's discrete outcomes (spikes and their substep,
+ * receptor events, released sites, modulator bits), tracking after every tick
+ * the maximum absolute and relative error of each binary32 state field
+ * against it. or_shadow_enable returns -1 for brains with LP/Prinz cells. */
+enum { OR_SHADOW_FIELDS = 15 };
+int or_shadow_enable(or_brain *b);
+/* Maxima over all ticks since enabling; returns the number of ticks tracked
+ * (-1 without a shadow). Relative error = |x32 - x64| / max(|x64|, floor)
+ * with floor 1 for mV/pA fields and 1e-3 otherwise. V_subthreshold_mV counts
+ * only neurons whose FP64 voltage is below their threshold V_T, that is,
+ * outside the exponential upswing where the AdEx equation amplifies any
+ * rounding difference by up to ~200x per 0.25 ms substep. */
+int64_t or_shadow_stats(const or_brain *b, double *maxabs, double *maxrel);
+/* FP64 shadow voltages (count) and synaptic weights (edges), either may be NULL. */
+void or_shadow_dump(const or_brain *b, double *v, double *syn_w);
+const char *or_shadow_field(int i);
+
 /* Correctly rounded binary32 exp/log (or_crmath.c). */
 float or_cr_expf(float x);
 float or_cr_logf(float x);

@@ -50,6 +50,11 @@ def oracle_lib(libm=False):
         lib.or_cr_logf.argtypes = [ct.c_float]; lib.or_cr_logf.restype = ct.c_float
         lib.or_bound_expf.argtypes = [ct.c_float]; lib.or_bound_expf.restype = ct.c_float
         lib.or_protocols.argtypes = [_f, ct.c_int]; lib.or_protocols.restype = ct.c_int
+        lib.or_shadow_enable.argtypes = [ct.c_void_p]; lib.or_shadow_enable.restype = ct.c_int
+        _d = ct.POINTER(ct.c_double)
+        lib.or_shadow_stats.argtypes = [ct.c_void_p, _d, _d]; lib.or_shadow_stats.restype = ct.c_int64
+        lib.or_shadow_field.argtypes = [ct.c_int]; lib.or_shadow_field.restype = ct.c_char_p
+        lib.or_shadow_dump.argtypes = [ct.c_void_p, _d, _d]
         _libs[name] = lib
     return _libs[name]
 
@@ -156,6 +161,31 @@ class OracleBrain:
 
     def events(self):
         return self.lib.or_last_events(self.ptr)
+
+    SHADOW_FIELDS = 15
+
+    def enable_shadow(self):
+        """Start the FP64 shadow from the current state (ValueError for LP/Prinz cells)."""
+        if self.lib.or_shadow_enable(self.ptr):
+            raise ValueError("FP64 shadow: brain has LP/Prinz cells")
+
+    def shadow_stats(self):
+        """{field: (max abs error, max rel error)} of the binary32 state against
+        the FP64 shadow over every tick since enable_shadow, and the tick count."""
+        a = np.zeros(self.SHADOW_FIELDS, np.float64)
+        r = np.zeros(self.SHADOW_FIELDS, np.float64)
+        d = ct.POINTER(ct.c_double)
+        ticks = self.lib.or_shadow_stats(self.ptr, a.ctypes.data_as(d), r.ctypes.data_as(d))
+        names = [self.lib.or_shadow_field(i).decode() for i in range(self.SHADOW_FIELDS)]
+        return {n: (float(x), float(y)) for n, x, y in zip(names, a, r)}, int(ticks)
+
+    def shadow_dump(self):
+        """FP64 shadow voltages (count,) and synaptic weights (edges,)."""
+        v = np.zeros(self.count, np.float64)
+        w = np.zeros(max(self.edges, 1), np.float64)
+        d = ct.POINTER(ct.c_double)
+        self.lib.or_shadow_dump(self.ptr, v.ctypes.data_as(d), w.ctypes.data_as(d))
+        return v, w[: self.edges]
 
     def dump(self):
         nw = np.zeros((self.count, NW), np.uint32)

@@ -1,0 +1,143 @@
+"""Error of the binary32 neural state against an FP64 model over 2,000 ticks.
+
+The oracle's FP64 shadow steps the same equations in binary64 beside the
+binary32 state, taking every discrete outcome (spike substep, receptor event,
+released sites, modulator bits) from the binary32 run, and tracks per field the
+maximum absolute and relative error after every tick. The CUDA engine's state
+equals the binary32 oracle bit for bit (test_gpu_parity.py), so these are also
+the engine's errors; the GPU test below measures them on the engine's own
+readback.
+
+Bounds (relative error = |x32 - x64| / max(|x64|, floor); floor 1 mV / 1 pA /
+1e-3 for dimensionless and nS fields):
+- synaptic weight, release probability, traces, conductances: <= 1e-5
+  relative over 2,000 ticks (measured <= 8.4e-6, weights <= 5.5e-7);
+- membrane voltage below V_T: <= 5e-5 relative (measured up to 1.34e-5). The
+  excess over 1e-5 comes from the adaptation current w, which integrates the
+  voltage error of the preceding upswing and carries it past the reset;
+- membrane voltage including the exponential upswing: <= 0.05 mV absolute.
+  Above V_T the AdEx exponential amplifies a rounding difference by up to ~200x
+  per 0.25 ms substep until the spike resets both trajectories to V_r, so no
+  binary32 evaluation order can hold 1e-5 relative there.
+"""
+import numpy as np
+import pytest
+
+from oracle.pyoracle import OracleBrain
+
+REL_BOUND = 1e-5
+V_SUB_REL_BOUND = 5e-5
+V_ABS_BOUND = 0.05
+BOUNDED_REL = ["g_dend_nS", "g_inh_nS", "g_receptor_nS", "log_ampa", "syn_w_nS", "syn_u",
+               "syn_slow", "syn_pre_trace", "syn_post_trace", "syn_eligibility", "adp_pA"]
+
+
+def _shadow_run(batch, brains, calls=125, ticks=16, seed0=20):
+    worst = {}
+    for i in brains:
+        ng, sg, mo = batch.brain(i)
+        o = OracleBrain(ng, sg, mo, batch.channels, batch.max_delay)
+        o.reset(seed0 + i)
+        o.enable_shadow()
+        for _ in range(calls):
+            o.step(batch.inputs[i], ticks, batch.gain, stop_on_nonfinite=False)
+        st, n = o.shadow_stats()
+        assert n == calls * ticks
+        for k, (a, r) in st.items():
+            A, R = worst.get(k, (0.0, 0.0))
+            worst[k] = (max(A, a), max(R, r))
+        o.close()
+    return worst
+
+
+def _check(worst, label):
+    lines = [f"{label}: max abs / max rel error vs FP64 over 2,000 ticks"]
+    lines += [f"  {k:18s} {a:.3e} {r:.3e}" for k, (a, r) in worst.items()]
+    print("\n".join(lines))
+    for k in BOUNDED_REL:
+        assert worst[k][1] <= REL_BOUND, f"{label}: {k} relative error {worst[k][1]:.3e}"
+    assert worst["V_subthreshold_mV"][1] <= V_SUB_REL_BOUND, f"{label}: V below V_T rel {worst['V_subthreshold_mV'][1]:.3e}"
+    assert worst["V_mV"][0] <= V_ABS_BOUND, f"{label}: V abs error {worst['V_mV'][0]:.3e} mV"
+
+
+def test_shadow_does_not_change_binary32(nsb, oracle_built):
+    b = nsb.workloads.plain_small()
+    ng, sg, mo = b.brain(3)
+    runs = []
+    for shadow in (False, True):
+        o = OracleBrain(ng, sg, mo, b.channels, b.max_delay)
+        o.reset(9)
+        if shadow:
+            o.enable_shadow()
+        outs = [o.step(b.inputs[3], 16, b.gain)[1] for _ in range(20)]
+        runs.append((np.array(outs), o.dump()))
+    np.testing.assert_array_equal(runs[0][0], runs[1][0])
+    for a, c in zip(runs[0][1][:2], runs[1][1][:2]):
+        np.testing.assert_array_equal(a, c)
+
+
+def test_fp64_error_plain_small(nsb, oracle_built):
+    """64 brains x 48 neurons, 600 synapses each, pair STDP, Poisson 20 Hz."""
+    b = nsb.workloads.plain_small()
+    _check(_shadow_run(b, range(0, 64, 4)), "plain small")
+
+
+def test_fp64_error_batched_uneven_sample(nsb, oracle_built):
+    """Brains drawn like the full-pool workload (delays 1-16, 10-40 Hz drive)."""
+    b = nsb.workloads.batched_uneven(brains=48, total_neurons=6144, total_synapses=12288)
+    _check(_shadow_run(b, range(0, 48, 3)), "batched uneven sample")
+
+
+def test_fp64_shadow_rejects_lp_prinz(nsb, oracle_built):
+    b = nsb.workloads.parity_mix(seed=7, brains=24, heavy_types=True)
+    found = False
+    for i in range(b.brains):
+        ng, sg, mo = b.brain(i)
+        if np.isin(ng[:, 0], [2, 3]).any() and (ng[np.isin(ng[:, 0], [2, 3]), 2] > 0).any():
+            o = OracleBrain(ng, sg, mo, b.channels, b.max_delay)
+            with pytest.raises(ValueError):
+                o.enable_shadow()
+            found = True
+            break
+    assert found
+
+
+@pytest.mark.gpu
+def test_gpu_state_error_vs_fp64(nsb, oracle_built):
+    """The engine's own readback (V and synaptic weights after every 16-tick
+    call) against the FP64 shadow, over 2,000 ticks."""
+    b = nsb.workloads.plain_small()
+    brains = list(range(0, 64, 4))
+    sub = b.subset(brains)
+    gpu = nsb.GpuBatch.from_rows(sub)
+    seeds = np.array([20 + i for i in brains], np.uint32)
+    gpu.reset(seeds)
+    ora = []
+    for k, i in enumerate(brains):
+        ng, sg, mo = b.brain(i)
+        o = OracleBrain(ng, sg, mo, b.channels, b.max_delay)
+        o.reset(int(seeds[k]))
+        o.enable_shadow()
+        ora.append(o)
+    v_abs = v_sub_rel = w_rel = 0.0
+    for _ in range(125):
+        gpu.step(sub.inputs, None, 16, b.gain)
+        for k, o in enumerate(ora):
+            o.step(sub.inputs[k], 16, b.gain, stop_on_nonfinite=False)
+            nw, sw, _ = gpu.dump(k)
+            v32 = nw[:, 0].view(np.float32).astype(np.float64)
+            w32 = sw[:, 0].view(np.float32).astype(np.float64)
+            v64, w64 = o.shadow_dump()
+            dv = np.abs(v32 - v64)
+            v_abs = max(v_abs, float(dv.max()))
+            below = v64 < -55.0
+            if below.any():
+                v_sub_rel = max(v_sub_rel, float((dv[below] / np.maximum(np.abs(v64[below]), 1.0)).max()))
+            if len(w64):
+                w_rel = max(w_rel, float((np.abs(w32 - w64) / np.maximum(np.abs(w64), 1e-3)).max()))
+    gpu.close()
+    print(f"GPU vs FP64 over 2,000 ticks: V abs {v_abs:.3e} mV, V (below -55 mV) rel {v_sub_rel:.3e}, "
+          f"synaptic w rel {w_rel:.3e}")
+    assert v_abs <= V_ABS_BOUND
+    assert v_sub_rel <= V_SUB_REL_BOUND
+    assert w_rel <= REL_BOUND
