@@ -112,6 +112,45 @@ int nsb_gpu_stats(void *batch, int *out);
 /* Synaptic arrivals counted on the device since the previous call. */
 long long nsb_gpu_take_events(void *batch);
 
+/* ---- Serving loop. No counterpart in the reference: the reference evaluates
+ * episodes with Gymnasium environments on the host (gym_adapter/gpu.py:57-83);
+ * this server keeps episodes of different genomes and lengths on the device,
+ * with a pole-on-cart environment, the adapter's opponent-coded observation
+ * (gym_adapter/adapter.py:153-169) and its smoothed two-action decoding
+ * (gym_adapter/gpu.py:66-83), and batches them continuously into the tick
+ * kernel. */
+typedef struct {
+    uint64_t tag;
+    int32_t genome, steps, reward, failures; /* steps run; steps without a fall; falls */
+    uint32_t trace, seed;                    /* FNV-1a over (action, motor counts) of every step */
+    int32_t status, pad;                     /* 0, or -1 when the neural state went non-finite */
+    double arrival_s, admit_s, done_s;       /* server clock (seconds since creation) */
+} nsb_serve_result;
+/* Admission: first come first served while the neurons in flight stay within
+ * max_inflight_neurons and the bytes of admitted episodes within
+ * hbm_budget_bytes. Pools are sized for the in-flight cap. NULL on error. */
+void *nsb_serve_create(long long max_inflight_neurons, double hbm_budget_bytes, double synapses_per_neuron,
+                       int max_slots, int max_brain_neurons, int ticks, float gain, double smoothing);
+void nsb_serve_destroy(void *server);
+/* Genome in the ns_create row format with 8 channels and 2 motors; returns its id or -1. */
+int nsb_serve_register(void *server, int count, int edges, const float *neuron_rows, const float *synapse_rows,
+                       const int *motors);
+/* Queue n episodes (genome id, seed, steps, caller tag, arrival time on the server clock). */
+int nsb_serve_submit(void *server, int n, const int *genome, const uint32_t *seed, const int *steps,
+                     const uint64_t *tag, const double *arrival_s);
+/* Background loop thread. */
+int nsb_serve_start(void *server);
+int nsb_serve_stop(void *server);
+/* Run the loop on the calling thread until nothing is queued or in flight. */
+int nsb_serve_run(void *server, long long max_iterations);
+/* Finished episodes, oldest first (nsb_serve_result[max]); returns the count or -1. */
+int nsb_serve_poll(void *server, void *results, int max);
+double nsb_serve_now(void *server);
+/* steps, admitted, completed, queued, inflight, inflight_neurons, units,
+ * neuron_ticks, busy_s, elapsed_s, events, pool_neurons, pool_synapses,
+ * pool_bytes, inflight_bytes. Returns the count written (15). */
+int nsb_serve_stats(void *server, double *out);
+
 #ifdef __cplusplus
 }
 #endif

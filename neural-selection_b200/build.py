@@ -15,9 +15,8 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libns_b200.so"
-SOURCES = [CSRC / "ns_engine.cu", CSRC / "ns_abi.cu"]
-HEADERS = [CSRC / n for n in ("ns_crmath.h", "ns_crmath_consts.h", "ns_layout.h", "ns_physio.cuh",
-                              "ns_engine.h", "ns_refabi.h")]
+SOURCES = sorted(CSRC.glob("*.cu"))
+HEADERS = sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")))
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -26,6 +26,7 @@
 
 #include "ns_engine.h"
 #include "ns_refabi.h"
+#include "ns_serve.h"
 
 using namespace nsb;
 
@@ -478,6 +479,122 @@ int nsb_gpu_stats(void *p, int *out) {
 long long nsb_gpu_take_events(void *p) {
     try {
         return (long long)static_cast<GpuBatch *>(p)->engine->take_events();
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+// ---- serving loop (no counterpart in the reference) ----------------------------
+// Continuous batching of genome-evaluation episodes on a device-resident
+// pole-on-cart environment; see neural-selection_b200/csrc/ns_serve.h.
+
+static_assert(sizeof(ServeResult) == 64, "nsb_serve_result layout");
+
+void *nsb_serve_create(long long max_inflight_neurons, double hbm_budget_bytes, double synapses_per_neuron,
+                       int max_slots, int max_brain_neurons, int ticks, float gain, double smoothing) {
+    try {
+        ServeConfig cfg;
+        cfg.max_inflight_neurons = max_inflight_neurons;
+        cfg.hbm_budget_bytes = hbm_budget_bytes;
+        cfg.synapses_per_neuron = synapses_per_neuron;
+        cfg.max_slots = max_slots;
+        cfg.max_brain_neurons = max_brain_neurons;
+        cfg.ticks = ticks;
+        cfg.gain = gain;
+        cfg.smoothing = smoothing;
+        return new Server(cfg);
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return nullptr;
+    }
+}
+
+void nsb_serve_destroy(void *p) { delete static_cast<Server *>(p); }
+
+// Registers a genome in the Gym row format of ns_create (8 channels: the
+// opponent-coded pole-on-cart observation; 2 motors: push left, push right).
+int nsb_serve_register(void *p, int count, int edges, const float *neuron_rows, const float *synapse_rows,
+                       const int *motors) {
+    try {
+        std::unique_ptr<HostBrain> b(make_brain(count, edges, 8, 2, neuron_rows, synapse_rows, motors, 8));
+        return static_cast<Server *>(p)->register_genome(spec_of(*b));
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+int nsb_serve_submit(void *p, int n, const int *genome, const uint32_t *seed, const int *steps, const uint64_t *tag,
+                     const double *arrival_s) {
+    try {
+        static_cast<Server *>(p)->submit(n, genome, seed, steps, tag, arrival_s);
+        return 0;
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+int nsb_serve_start(void *p) {
+    try {
+        static_cast<Server *>(p)->start();
+        return 0;
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+int nsb_serve_stop(void *p) {
+    try {
+        Server &s = *static_cast<Server *>(p);
+        s.stop();
+        const std::string err = s.error();
+        if (!err.empty()) throw std::runtime_error(err);
+        return 0;
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+int nsb_serve_run(void *p, long long max_iterations) {
+    try {
+        static_cast<Server *>(p)->run_until_idle(max_iterations);
+        return 0;
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+int nsb_serve_poll(void *p, void *results, int max) {
+    try {
+        Server &s = *static_cast<Server *>(p);
+        const std::string err = s.error();
+        if (!err.empty()) throw std::runtime_error(err);
+        return s.poll(static_cast<ServeResult *>(results), max);
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+double nsb_serve_now(void *p) { return static_cast<Server *>(p)->now(); }
+
+// steps, admitted, completed, queued, inflight, inflight_neurons, units,
+// neuron_ticks, busy_s, elapsed_s, events, pool_neurons, pool_synapses,
+// pool_bytes, inflight_bytes
+int nsb_serve_stats(void *p, double *out) {
+    try {
+        const ServeStats s = static_cast<Server *>(p)->stats();
+        const double v[15] = {(double)s.steps, (double)s.admitted, (double)s.completed, (double)s.queued,
+                              (double)s.inflight, (double)s.inflight_neurons, (double)s.units, s.neuron_ticks,
+                              s.busy_s, s.elapsed_s, (double)s.events, (double)s.pool_neurons,
+                              (double)s.pool_synapses, s.pool_bytes, s.inflight_bytes};
+        std::memcpy(out, v, sizeof v);
+        return 15;
     } catch (const std::exception &e) {
         g_error = e.what();
         return -1;

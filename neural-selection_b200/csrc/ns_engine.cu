@@ -27,6 +27,7 @@
 // (plasticity_quiet), and a final pass at the end of the call brings every
 // plastic synapse to the last tick. The results equal tick-by-tick updating.
 #include "ns_engine.h"
+#include "ns_internal.h"
 
 #include <algorithm>
 #include <cmath>
@@ -39,45 +40,13 @@
 #include "ns_crmath.h"
 #include "ns_layout.h"
 #include "ns_physio.cuh"
+#include "ns_reset.cuh"
 
 namespace nsb {
-
-#define NSB_CHECK(x)                                                                        \
-    do {                                                                                    \
-        cudaError_t e_ = (x);                                                               \
-        if (e_ != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e_)); \
-    } while (0)
 
 #ifndef NSB_MIN_CTAS
 #define NSB_MIN_CTAS 3   // CTAs per SM the light kernel's register budget is sized for
 #endif
-
-constexpr int kMetaCap = 6144;       // synapse meta words cached in shared memory per unit
-constexpr int kMaxUnitBrains = 128;  // brains packed into one small unit
-constexpr int kMaxBrainNeurons = 16384;
-
-struct Pools {
-    const float4 *ngene;     // N x 4
-    const uint32_t *nflags;  // N
-    const int *nsens;        // N
-    const int *nxidx;        // N (index into heavy arrays, -1)
-    const float *xgene;      // H x 16
-    float *xstate;           // H x 16
-    uint32_t *nstate;        // N x 16
-    const int *inptr;        // N + 1
-    const uint32_t *smeta;   // E
-    const uint32_t *sgene;   // E x 8
-    uint32_t *sstate;        // E x 16
-    uint8_t *sarrived;       // E
-    int16_t *slastp;         // E (-1 between calls)
-    int64_t *btick;
-    const int *bmotor;       // B x outputs, global neuron index
-    const int4 *units;       // {n0, nn, e0, ne}
-    const int2 *unitb;       // {first entry in ubrain, nb}
-    const int *ubrain;       // unit brain lists (caller brain indices), pool order
-    int channels, outputs, hw;
-    unsigned long long *events;
-};
 
 __device__ __forceinline__ uint32_t rotl32(uint32_t x, uint32_t r) { return __funnelshift_l(x, x, r); }
 __device__ __forceinline__ uint32_t rotr32(uint32_t x, uint32_t r) { return __funnelshift_r(x, x, r); }
@@ -295,7 +264,12 @@ __global__ void __launch_bounds__(256, HEAVY ? 1 : NSB_MIN_CTAS) tick_kernel(Poo
         if (meta_smem)
             for (int k = tid; k < ne; k += bs) s_meta[k] = P.smeta[e0 + k];
         const uint32_t *meta = meta_smem ? s_meta : P.smeta + e0;
-        __syncthreads();
+        // A unit whose brains are all masked off does no work: outputs 0.
+        if (!__syncthreads_or(tid < nb && s_mask[tid] != 0)) {
+            for (int i = tid; i < nb * P.outputs; i += bs)
+                output[(size_t)s_bid[i / P.outputs] * P.outputs + (i % P.outputs)] = 0.0f;
+            continue;
+        }
         const int slots = (nn + bs - 1) / bs;
         int my_events = 0;
         // Each thread steps neurons j = sl0*bs + tid, sl0 < slots; their state
@@ -406,45 +380,14 @@ __global__ void __launch_bounds__(256, HEAVY ? 1 : NSB_MIN_CTAS) tick_kernel(Poo
 }
 
 // ---- reset (gym_adapter/gpu.cu:18-23 with physiology.cuh:179-202, 393-404) --------
-__device__ __forceinline__ uint32_t seed_hash(uint32_t seed) {
-    uint32_t x = seed ? seed : 1u;
-    x ^= x >> 16; x *= 0x7feb352du;
-    x ^= x >> 15; x *= 0x846ca68bu;
-    x ^= x >> 16;
-    return x;
-}
-
 __global__ void reset_neurons(Pools P, const int *nbrain, const uint32_t *norig, const uint8_t *mask,
                               const uint32_t *seeds, int n_neurons) {
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_neurons; n += gridDim.x * blockDim.x) {
         const int b = nbrain[n];
         if (!mask[b]) continue;
-        const uint32_t flags = P.nflags[n];
-        const uint32_t type = flags & NF_TYPE_MASK;
-        const float el = P.ngene[(size_t)n * 4].z;
-        const uint32_t x = seed_hash(seeds[b] + norig[n] * 7919u);
-        uint32_t *r = P.nstate + (size_t)n * S_WORDS;
-        for (int k = 0; k < S_WORDS; ++k) r[k] = 0u;
-        float v = el;
         const int xi = P.nxidx[n];
-        if (xi >= 0) {
-            float *xs = P.xstate + (size_t)xi * 16;
-            for (int k = 0; k < 16; ++k) xs[k] = 0.0f;
-            if (type == 2) {
-                const float init[16] = {-56, 0, .2f, 0, 1, 0, 0, 1, 0, 0, 1, 1, 0, .04f, .01f, -56};
-                for (int k = 0; k < 16; ++k) xs[k] = init[k];
-                v = xs[15] - 9.342518882f;
-            } else if (type == 3) {
-                xs[0] = -50.0f; xs[1] = .05f;
-                for (int k = 0; k < 4; ++k) xs[9 + k] = 1.0f;
-                v = xs[0];
-            } else if (type == 6) {
-                xs[0] = el;
-                xs[1] = P.ngene[(size_t)n * 4].w;   // threshold
-            }
-        }
-        r[S_V] = __float_as_uint(v);
-        r[S_RECRNG] = x ? x : 1u;
+        init_neuron(P.nstate + (size_t)n * S_WORDS, xi >= 0 ? P.xstate + (size_t)xi * 16 : nullptr,
+                    P.ngene + (size_t)n * 4, P.nflags[n], seeds[b], norig[n]);
     }
 }
 
@@ -453,19 +396,7 @@ __global__ void reset_synapses(Pools P, const int *sbrain, const uint32_t *sorig
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_synapses; e += gridDim.x * blockDim.x) {
         const int b = sbrain[e];
         if (!mask[b]) continue;
-        uint32_t x = seed_hash(seeds[b] + sorig[e] * 104729u);
-        if (!x) x = 1u;
-        const uint32_t *y = P.sgene + (size_t)e * Y_WORDS;
-        const int n = (int)(y[Y_INFO] & 0xffu);
-        const uint64_t ready = n == 64 ? ~0ull : ((1ull << n) - 1ull);
-        uint32_t *z = P.sstate + (size_t)e * Z_WORDS;
-        z[Z_W] = y[Y_W0];
-        z[Z_RU] = 0u; z[Z_PRETR] = 0u; z[Z_POSTTR] = 0u; z[Z_ELTP] = 0u; z[Z_ELTD] = 0u;
-        z[Z_DAAGE] = __float_as_uint(-1.0f); z[Z_SPINE] = __float_as_uint(1.0f); z[Z_STAGE] = __float_as_uint(-1.0f);
-        z[Z_PREAGE] = __float_as_uint(1000000.0f); z[Z_POSTAGE] = __float_as_uint(1000000.0f);
-        z[Z_SLOW] = __float_as_uint(1.0f);
-        z[Z_READYLO] = (uint32_t)ready; z[Z_READYHI] = (uint32_t)(ready >> 32);
-        z[Z_RNG] = x; z[Z_LAST] = (uint32_t)(-1000000);
+        init_synapse(P.sstate + (size_t)e * Z_WORDS, P.sgene + (size_t)e * Y_WORDS, seeds[b], sorig[e]);
         P.sarrived[e] = 0;
     }
 }
@@ -497,6 +428,38 @@ static PhysConst make_constants() {
     return K;
 }
 
+int spike_words(int max_unit_neurons, int block) {
+    // Whole CTA-sized neuron slots: a big unit's threads write one word per
+    // warp per slot.
+    return ((std::max(max_unit_neurons, block) + block - 1) / block) * (block / 32);
+}
+
+int tick_smem_bytes(int hw) {
+    return 1024 + (kMetaCap + 32 * hw * 2) * 4 + kMaxUnitBrains * 8 + 2 * kMaxUnitBrains * 4;
+}
+
+void prepare_tick_kernels(int smem) {
+    NSB_CHECK(cudaFuncSetAttribute(tick_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    NSB_CHECK(cudaFuncSetAttribute(tick_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const PhysConst K = make_constants();
+    NSB_CHECK(cudaMemcpyToSymbol(c_K, &K, sizeof(PhysConst)));
+}
+
+int tick_occupancy(int block, int smem) {
+    int occ = 0;
+    NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tick_kernel<false>, block, smem));
+    return std::max(occ, 1);
+}
+
+void launch_tick_light(const Pools &P, int n_units, int grid, int block, int smem, int *queue, const float *input,
+                       const uint8_t *mask, float *output, int *status, int ticks, float gain, cudaStream_t stream) {
+    NSB_CHECK(cudaMemsetAsync(queue, 0, sizeof(int), stream));
+    if (n_units > 0)
+        tick_kernel<false><<<grid, block, smem, stream>>>(P, 0, n_units, queue, input, mask, output, status, ticks,
+                                                          gain);
+    NSB_CHECK(cudaGetLastError());
+}
+
 template <class T> T *Engine::alloc(size_t n) {
     T *p = nullptr;
     if (n == 0) n = 1;
@@ -507,13 +470,9 @@ template <class T> T *Engine::alloc(size_t n) {
 
 static bool excitatory_type(unsigned char t) { return t == 0 || t == 4 || t == 5; }
 
-Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, const EngineConfig &cfg) {
-    if (brains.empty()) throw std::runtime_error("Empty GPU batch");
-    if (cfg.max_delay < 1 || cfg.max_delay > kMaxDelay) throw std::runtime_error("Invalid delay ring");
-    if (cfg.block != 128 && cfg.block != 256) throw std::runtime_error("Invalid CUDA block size");
-    n_brains_ = (int)brains.size();
-    channels_ = channels; outputs_ = outputs; max_delay_ = cfg.max_delay; block_ = cfg.block;
-    count_events_ = cfg.count_events;
+Plan make_plan(const std::vector<BrainSpec> &brains, int channels, int outputs, int max_delay, int unit_cap) {
+    Plan p;
+    const int n_brains = (int)brains.size();
     // ---- validate and size ----
     long long nsum = 0, esum = 0;
     for (const auto &b : brains) {
@@ -523,23 +482,22 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
             const auto &c = b.conns[j];
             if (c.pre < 0 || c.pre >= b.count || c.post < 0 || c.post >= b.count)
                 throw std::runtime_error("Invalid synapse gene");
-            if (c.delay > max_delay_ || c.delay < 1) throw std::runtime_error("Synapse delay exceeds the delay ring");
+            if (c.delay > max_delay || c.delay < 1) throw std::runtime_error("Synapse delay exceeds the delay ring");
         }
         for (int j = 0; j < outputs; ++j)
             if (b.motors[j] < 0 || b.motors[j] >= b.count) throw std::runtime_error("Invalid motor index");
         nsum += b.count; esum += b.edges;
     }
     if (nsum > (1ll << 30) || esum > (1ll << 30)) throw std::runtime_error("Pool exceeds 2^30 entries");
-    n_neurons_ = (int)nsum; n_synapses_ = (int)esum;
+    p.n_neurons = (int)nsum; p.n_synapses = (int)esum;
 
     // ---- work units ------------------------------------------------------------
-    unit_cap_ = block_ * std::max(1, cfg.unit_slots);
     // Brains with LP/Prinz/LFS cells go to units of their own (stepped by the
     // heavy kernel). Within each group a brain above the CTA size is a unit of
     // its own; smaller brains are packed best-fit decreasing.
     auto is_heavy_type = [](unsigned char t) { return t == 2 || t == 3 || t == 6; };
-    std::vector<char> brain_heavy(n_brains_, 0);
-    for (int b = 0; b < n_brains_; ++b)
+    std::vector<char> brain_heavy(n_brains, 0);
+    for (int b = 0; b < n_brains; ++b)
         for (int j = 0; j < brains[b].count; ++j)
             if (is_heavy_type(brains[b].genes[j].type)) { brain_heavy[b] = 1; break; }
     std::vector<std::vector<int>> unit_brains;
@@ -547,13 +505,13 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
     std::vector<char> unit_heavy;
     for (int group = 0; group < 2; ++group) {
         std::vector<int> order;
-        for (int b = 0; b < n_brains_; ++b)
+        for (int b = 0; b < n_brains; ++b)
             if (brain_heavy[b] == group) order.push_back(b);
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return brains[a].count > brains[b].count; });
         std::multimap<int, int> open;   // remaining capacity -> unit
         for (int b : order) {
             const int n = brains[b].count;
-            if (n > unit_cap_) {
+            if (n > unit_cap) {
                 unit_brains.push_back({b}); unit_fill.push_back(n); unit_heavy.push_back((char)group);
                 continue;
             }
@@ -563,11 +521,11 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
                 open.erase(it);
                 unit_brains[uidx].push_back(b);
                 unit_fill[uidx] += n;
-                const int rem = unit_cap_ - unit_fill[uidx];
+                const int rem = unit_cap - unit_fill[uidx];
                 if (rem > 0 && (int)unit_brains[uidx].size() < kMaxUnitBrains) open.emplace(rem, uidx);
             } else {
                 unit_brains.push_back({b}); unit_fill.push_back(n); unit_heavy.push_back((char)group);
-                const int rem = unit_cap_ - n;
+                const int rem = unit_cap - n;
                 if (rem > 0) open.emplace(rem, (int)unit_brains.size() - 1);
             }
         }
@@ -579,38 +537,45 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
         if (unit_heavy[a] != unit_heavy[b]) return unit_heavy[a] < unit_heavy[b];
         return unit_fill[a] > unit_fill[b];
     });
-    n_units_ = (int)unit_brains.size();
-    n_light_units_ = 0;
-    for (int u : uorder) n_light_units_ += unit_heavy[u] ? 0 : 1;
+    p.n_units = (int)unit_brains.size();
+    p.n_light_units = 0;
+    for (int u : uorder) p.n_light_units += unit_heavy[u] ? 0 : 1;
 
     // ---- per-brain bookkeeping (caller order) ----
-    h_noff_.assign(n_brains_ + 1, 0);
-    h_soff_.assign(n_brains_ + 1, 0);
-    for (int b = 0; b < n_brains_; ++b) {
+    auto &h_noff_ = p.noff, &h_soff_ = p.soff, &h_npos_ = p.npos, &h_spos_ = p.spos, &h_bunit_ = p.bunit;
+    h_noff_.assign(n_brains + 1, 0);
+    h_soff_.assign(n_brains + 1, 0);
+    for (int b = 0; b < n_brains; ++b) {
         h_noff_[b + 1] = h_noff_[b] + brains[b].count;
         h_soff_[b + 1] = h_soff_[b] + brains[b].edges;
     }
-    h_npos_.assign(n_neurons_, 0);
-    h_spos_.assign(n_synapses_, 0);
-    h_bunit_.assign(n_brains_, 0);
-    h_units_.assign(n_units_, make_int4(0, 0, 0, 0));
-    std::vector<int2> unitb(n_units_);
-    std::vector<int> brain_order;   // unit brain lists (caller indices), pool order
+    h_npos_.assign(p.n_neurons, 0);
+    h_spos_.assign(p.n_synapses, 0);
+    h_bunit_.assign(n_brains, 0);
+    p.units.assign(p.n_units, make_int4(0, 0, 0, 0));
+    p.unitb.assign(p.n_units, make_int2(0, 0));
+    auto &h_units_ = p.units;
+    auto &unitb = p.unitb;
+    auto &brain_order = p.brain_order;   // unit brain lists (caller indices), pool order
 
     // ---- per-neuron and per-synapse records ----
-    std::vector<float> ngene((size_t)n_neurons_ * 16);
-    h_nflags_.assign(n_neurons_, 0);
-    std::vector<int> nsens(n_neurons_), nbrain(n_neurons_);
-    h_nxidx_.assign(n_neurons_, -1);
-    std::vector<uint32_t> norig(n_neurons_);
-    std::vector<float> xgene;
-    std::vector<int> inptr(n_neurons_ + 1, 0);
-    std::vector<uint32_t> smeta(n_synapses_), sgene((size_t)n_synapses_ * Y_WORDS), sorig(n_synapses_);
-    std::vector<int> sbrain(n_synapses_);
-    std::vector<int> bmotor((size_t)n_brains_ * outputs);
+    const int n_neurons = p.n_neurons, n_synapses = p.n_synapses;
+    auto &ngene = p.ngene, &xgene = p.xgene;
+    auto &h_nflags_ = p.nflags, &norig = p.norig, &smeta = p.smeta, &sgene = p.sgene, &sorig = p.sorig;
+    auto &nsens = p.nsens, &nbrain = p.nbrain, &h_nxidx_ = p.nxidx, &inptr = p.inptr, &sbrain = p.sbrain,
+         &bmotor = p.bmotor;
+    ngene.assign((size_t)n_neurons * 16, 0.0f);
+    h_nflags_.assign(n_neurons, 0);
+    nsens.assign(n_neurons, 0); nbrain.assign(n_neurons, 0);
+    h_nxidx_.assign(n_neurons, -1);
+    norig.assign(n_neurons, 0);
+    inptr.assign(n_neurons + 1, 0);
+    smeta.assign(n_synapses, 0); sgene.assign((size_t)n_synapses * Y_WORDS, 0); sorig.assign(n_synapses, 0);
+    sbrain.assign(n_synapses, 0);
+    bmotor.assign((size_t)n_brains * outputs, 0);
 
     int ncur = 0, ecur = 0;
-    for (int ui = 0; ui < n_units_; ++ui) {
+    for (int ui = 0; ui < p.n_units; ++ui) {
         const auto &ub = unit_brains[uorder[ui]];
         const int un0 = ncur, ue0 = ecur;
         unitb[ui] = make_int2((int)brain_order.size(), (int)ub.size());
@@ -681,7 +646,7 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
             nbrain[n] = b;
             norig[n] = B.orig_n ? B.orig_n[j] : (uint32_t)j;
             if (is_heavy_type(G.type)) {
-                h_nxidx_[n] = n_heavy_++;
+                h_nxidx_[n] = p.n_heavy++;
                 float xg[16] = {};
                 if (G.type == 2) { xg[0] = G.lp.calcium; xg[1] = G.lp.calcium_k; xg[2] = G.lp.h; xg[3] = G.lp.leak; }
                 if (G.type == 3) { for (int r = 0; r < 8; ++r) xg[r] = G.prinz.g[r]; xg[8] = G.prinz_leak; }
@@ -738,17 +703,38 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
         ncur += (int)keys.size();
         ecur += (int)sk.size();
         h_units_[ui] = make_int4(un0, ncur - un0, ue0, ecur - ue0);
-        max_unit_neurons_ = std::max(max_unit_neurons_, ncur - un0);
-        if (ncur - un0 > unit_cap_) ++n_big_units_;
-        max_unit_brains_ = std::max(max_unit_brains_, (int)ub.size());
+        p.max_unit_neurons = std::max(p.max_unit_neurons, ncur - un0);
+        if (ncur - un0 > unit_cap) ++p.n_big_units;
+        p.max_unit_brains = std::max(p.max_unit_brains, (int)ub.size());
     }
-    inptr[n_neurons_] = n_synapses_;
-    for (int b = 0; b < n_brains_; ++b)
+    inptr[n_neurons] = n_synapses;
+    for (int b = 0; b < n_brains; ++b)
         for (int j = 0; j < outputs; ++j)
             bmotor[(size_t)b * outputs + j] = h_npos_[h_noff_[b] + brains[b].motors[j]];
-    // Spike-ring words per tick: whole CTA-sized neuron slots (a big unit's
-    // threads write one word per warp per slot).
-    hw_ = ((std::max(max_unit_neurons_, block_) + block_ - 1) / block_) * (block_ / 32);
+    return p;
+}
+
+Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, const EngineConfig &cfg) {
+    if (brains.empty()) throw std::runtime_error("Empty GPU batch");
+    if (cfg.max_delay < 1 || cfg.max_delay > kMaxDelay) throw std::runtime_error("Invalid delay ring");
+    if (cfg.block != 128 && cfg.block != 256) throw std::runtime_error("Invalid CUDA block size");
+    n_brains_ = (int)brains.size();
+    channels_ = channels; outputs_ = outputs; max_delay_ = cfg.max_delay; block_ = cfg.block;
+    count_events_ = cfg.count_events;
+    unit_cap_ = block_ * std::max(1, cfg.unit_slots);
+    Plan p = make_plan(brains, channels, outputs, max_delay_, unit_cap_);
+    n_neurons_ = p.n_neurons; n_synapses_ = p.n_synapses; n_units_ = p.n_units; n_light_units_ = p.n_light_units;
+    n_big_units_ = p.n_big_units; n_heavy_ = p.n_heavy; max_unit_neurons_ = p.max_unit_neurons;
+    max_unit_brains_ = p.max_unit_brains;
+    h_noff_ = std::move(p.noff); h_soff_ = std::move(p.soff); h_npos_ = std::move(p.npos);
+    h_spos_ = std::move(p.spos); h_bunit_ = std::move(p.bunit); h_units_ = p.units;
+    h_nflags_ = p.nflags; h_nxidx_ = p.nxidx;
+    const auto &ngene = p.ngene, &xgene = p.xgene;
+    const auto &norig = p.norig, &smeta = p.smeta, &sgene = p.sgene, &sorig = p.sorig;
+    const auto &nsens = p.nsens, &nbrain = p.nbrain, &inptr = p.inptr, &sbrain = p.sbrain, &bmotor = p.bmotor;
+    const auto &unitb = p.unitb;
+    const auto &brain_order = p.brain_order;
+    hw_ = spike_words(max_unit_neurons_, block_);
 
     // ---- device allocation and upload ----
     NSB_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
@@ -794,7 +780,7 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
     h_tick_.assign(n_brains_, 0);
 
     // ---- launch shape ----
-    smem_ = 1024 + (kMetaCap + 32 * hw_ * 2) * 4 + kMaxUnitBrains * 8 + 2 * kMaxUnitBrains * 4;
+    smem_ = tick_smem_bytes(hw_);
     NSB_CHECK(cudaFuncSetAttribute(tick_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_));
     NSB_CHECK(cudaFuncSetAttribute(tick_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_));
     int dev = 0;

@@ -52,6 +52,18 @@ SIGNATURES = {
     "nsb_gpu_load_state": (ct.c_int, [_vp, ct.c_int, _vp]),
     "nsb_gpu_stats": (ct.c_int, [_vp, _i32]),
     "nsb_gpu_take_events": (ct.c_longlong, [_vp]),
+    "nsb_serve_create": (_vp, [ct.c_longlong, ct.c_double, ct.c_double, ct.c_int, ct.c_int, ct.c_int, ct.c_float,
+                               ct.c_double]),
+    "nsb_serve_destroy": (None, [_vp]),
+    "nsb_serve_register": (ct.c_int, [_vp, ct.c_int, ct.c_int, _f, _f, _i32]),
+    "nsb_serve_submit": (ct.c_int, [_vp, ct.c_int, _i32, _u32, _i32, ct.POINTER(ct.c_uint64),
+                                    ct.POINTER(ct.c_double)]),
+    "nsb_serve_start": (ct.c_int, [_vp]),
+    "nsb_serve_stop": (ct.c_int, [_vp]),
+    "nsb_serve_run": (ct.c_int, [_vp, ct.c_longlong]),
+    "nsb_serve_poll": (ct.c_int, [_vp, _vp, ct.c_int]),
+    "nsb_serve_now": (ct.c_double, [_vp]),
+    "nsb_serve_stats": (ct.c_int, [_vp, ct.POINTER(ct.c_double)]),
 }
 
 

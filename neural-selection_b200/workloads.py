@@ -336,3 +336,74 @@ def parity_mix(seed=7, brains=24, min_n=8, max_n=160, fanin=8, channels=6, outpu
     motors = np.stack([st.integers(bi, 1000 + k, 40, 0, sizes) for k in range(outputs)], axis=1)
     inputs = st.uniform(np.repeat(bi, channels), np.tile(np.arange(channels), brains), 50).reshape(brains, channels)
     return _assemble("parity_mix", sizes, edges, channels, max_delay, nfn, sfn, motors, inputs, 230.0, {})
+
+
+def serving_library(seed=5, genomes=512, lo=32, hi=4096, per_neuron=8, channels=8, outputs=2, max_delay=8):
+    """Genomes of the serving workload (config 5): N log-uniform in [lo, hi],
+    per_neuron*N synapses. Ports follow the reference's random_genome
+    (gym_adapter/adapter.py:74-88): `channels` sensory neurons (profile 4,
+    channel i), `outputs` motor neurons (profile 4), hidden neurons of profile
+    0, 1 or 4 with 20% inhibitory transmitter; synapses as its synapse()
+    (weight U(1, 18) nS, branch 0-3, U .8, recovery 60 ms, facilitation 50 ms,
+    no plasticity) with pre uniform over all neurons, post uniform over
+    non-sensory neurons and delays 1-max_delay ms. Returns a Batch (inputs
+    zero: the server encodes observations itself)."""
+    st = Stream(seed, 0x73657276)
+    u = st.uniform(np.arange(genomes), 0, 0)
+    sizes = np.floor(np.exp(np.log(lo) + u * (np.log(hi + 1) - np.log(lo)))).astype(np.int64)
+    sizes = np.clip(sizes, max(lo, channels + outputs), hi)
+    edges = sizes * per_neuron
+
+    def nfn(no):
+        b, i = _brain_of(no)
+        rows = np.zeros((len(b), 10))
+        hidden = i >= channels + outputs
+        prof = np.where(hidden, np.array([0, 1, 4])[st.integers(b, i, 1, 0, 3)], 4)
+        inhib = hidden & (st.uniform(b, i, 2) < 0.2)
+        rows[:, 0] = prof
+        rows[:, 1] = np.where(i < channels, i, -1)
+        rows[:, 2] = 1
+        rows[:, 3] = inhib
+        rows[:, 5] = 1.0
+        rows[:, 6] = 1.0
+        rows[:, 7] = [THRESHOLD[int(p)] for p in prof]
+        rows[:, 8] = 43.0
+        rows[:, 9] = 2.0
+        return rows
+
+    def sfn(no, so):
+        b, e = _brain_of(so)
+        n = no[b + 1] - no[b]
+        rows = np.zeros((len(b), 11))
+        rows[:, 0] = st.integers(b, e, 10, 0, n)
+        rows[:, 1] = st.integers(b, e, 11, channels, n)
+        rows[:, 2] = 1.0 + 17.0 * st.uniform(b, e, 12)
+        rows[:, 3] = 1
+        rows[:, 4] = st.integers(b, e, 13, 1, max_delay + 1)
+        rows[:, 5] = st.integers(b, e, 14, 0, 4)
+        rows[:, 6] = 0.8
+        rows[:, 7] = 60.0
+        rows[:, 8] = 50.0
+        return rows
+
+    motors = np.tile(np.arange(channels, channels + outputs), (genomes, 1))
+    inputs = np.zeros((genomes, channels), np.float32)
+    return _assemble("serving_library", sizes, edges, channels, max_delay, nfn, sfn, motors, inputs, 230.0,
+                     {"per_neuron": per_neuron})
+
+
+def serving_schedule(seed, rate, seconds, genomes, lo_steps=200, hi_steps=2000, start=0.0):
+    """Poisson arrivals at `rate` per second over [start, start + seconds):
+    returns dict of arrays arrival (s), genome (uniform over the library), seed,
+    steps (uniform integer in [lo_steps, hi_steps]) and tag (request index)."""
+    st = Stream(seed, 0x61727276)
+    n_max = int(rate * seconds + 10 * np.sqrt(rate * seconds + 1) + 16)
+    idx = np.arange(n_max)
+    gaps = -np.log(1.0 - st.uniform(idx, 0, 0)) / rate
+    arrival = start + np.cumsum(gaps)
+    keep = arrival < start + seconds
+    idx = idx[keep]
+    return {"arrival": arrival[keep], "genome": st.integers(idx, 0, 1, 0, genomes).astype(np.int32),
+            "seed": st.bits(idx, 0, 2)[:, 0].astype(np.uint32),
+            "steps": st.integers(idx, 0, 3, lo_steps, hi_steps + 1).astype(np.int32),
+            "tag": idx.astype(np.uint64)}

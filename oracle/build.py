@@ -47,11 +47,11 @@ def build_oracle(verbose=False):
     cr_obj = BUILD / "or_crmath.o"
     if _stale(cr_obj, [HERE / "or_crmath.c"]):
         _run(["gcc", *CFLAGS, "-c", HERE / "or_crmath.c", "-o", cr_obj])
-    srcs = [HERE / "ns_oracle.c", HERE / "ns_oracle.h", cr_obj]
+    srcs = [HERE / "ns_oracle.c", HERE / "or_episode.c", HERE / "ns_oracle.h", cr_obj]
     for name, extra in (("libns_oracle.so", []), ("libns_oracle_libm.so", ["-DOR_LIBM"])):
         out = BUILD / name
         if _stale(out, srcs):
-            _run(["gcc", *CFLAGS, *extra, "-shared", HERE / "ns_oracle.c", cr_obj,
+            _run(["gcc", *CFLAGS, *extra, "-shared", HERE / "ns_oracle.c", HERE / "or_episode.c", cr_obj,
                   "-o", out, "-lquadmath", "-lm"])
     ex = BUILD / "exhaustive_math"
     if _stale(ex, [HERE / "exhaustive_math.cpp", cr_obj, CSRC / "ns_crmath.h"]):

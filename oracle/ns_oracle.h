@@ -73,6 +73,19 @@ float or_cr_logf(float x);
 float or_bound_expf(float x);
 float or_bound_logf(float x);
 
+/* One genome-evaluation episode (or_episode.c): reset with `seed`, then
+ * `steps` environment steps of `ticks` neural ticks on the pole-on-cart
+ * environment of the serving loop. out[5] = steps run, reward (steps without
+ * a fall), falls, trace (FNV-1a of action and motor counts per step), status
+ * (0, or -1 after a non-finite voltage). Returns 0, or -1 on bad arguments. */
+int or_episode(or_brain *b, uint32_t seed, int steps, int ticks, float gain, double smoothing, int32_t *out);
+/* The environment's binary64 elementary functions (or_episode.c). */
+double or_env_exp(double x);
+double or_env_tanh(double x);
+void or_env_sincos(double x, double *s, double *c);
+/* Fixed environment sequence for build comparisons (or_episode.c). */
+void or_env_sequence(uint64_t *out);
+
 /* Reference protocol checks (tests/physiology.cpp, tests/event_synapses.cpp,
  * tests/cuda_relay_parity.cu restated); results written as floats. */
 int or_protocols(float *out, int n);

@@ -55,6 +55,12 @@ def oracle_lib(libm=False):
         lib.or_shadow_stats.argtypes = [ct.c_void_p, _d, _d]; lib.or_shadow_stats.restype = ct.c_int64
         lib.or_shadow_field.argtypes = [ct.c_int]; lib.or_shadow_field.restype = ct.c_char_p
         lib.or_shadow_dump.argtypes = [ct.c_void_p, _d, _d]
+        lib.or_episode.argtypes = [ct.c_void_p, ct.c_uint32, ct.c_int, ct.c_int, ct.c_float, ct.c_double, _i32]
+        lib.or_episode.restype = ct.c_int
+        lib.or_env_exp.argtypes = [ct.c_double]; lib.or_env_exp.restype = ct.c_double
+        lib.or_env_tanh.argtypes = [ct.c_double]; lib.or_env_tanh.restype = ct.c_double
+        lib.or_env_sincos.argtypes = [ct.c_double, _d, _d]
+        lib.or_env_sequence.argtypes = [ct.POINTER(ct.c_uint64)]
         _libs[name] = lib
     return _libs[name]
 
@@ -178,6 +184,15 @@ class OracleBrain:
         ticks = self.lib.or_shadow_stats(self.ptr, a.ctypes.data_as(d), r.ctypes.data_as(d))
         names = [self.lib.or_shadow_field(i).decode() for i in range(self.SHADOW_FIELDS)]
         return {n: (float(x), float(y)) for n, x, y in zip(names, a, r)}, int(ticks)
+
+    def episode(self, seed, steps, ticks=16, gain=230.0, smoothing=0.4):
+        """One pole-on-cart episode from a reset with `seed` (or_episode.c)."""
+        out = np.zeros(5, np.int32)
+        if self.lib.or_episode(self.ptr, ct.c_uint32(seed), int(steps), int(ticks), float(gain), float(smoothing),
+                               _ptr(out, _i32)):
+            raise ValueError("or_episode: invalid arguments")
+        return {"steps": int(out[0]), "reward": int(out[1]), "failures": int(out[2]),
+                "trace": int(np.uint32(out[3].view(np.uint32))), "status": int(out[4])}
 
     def shadow_dump(self):
         """FP64 shadow voltages (count,) and synaptic weights (edges,)."""
