@@ -111,6 +111,13 @@ int nsb_gpu_load_state(void *batch, int brain, void *brain_handle);
 int nsb_gpu_stats(void *batch, int *out);
 /* Synaptic arrivals counted on the device since the previous call. */
 long long nsb_gpu_take_events(void *batch);
+/* Delivery mode of the tick kernel: 1 warp-cooperative stochastic release
+ * (dense, active brains), 0 serial per neuron; results are identical.
+ * Returns the previous mode, or -1. */
+int nsb_gpu_set_delivery(void *batch, int cooperative);
+/* Times both delivery modes on the batch's own buffers for a few steps
+ * (state restored afterwards) and keeps the faster; returns it, or -1. */
+int nsb_gpu_autotune(void *batch, int ticks, float gain, void *stream);
 
 /* ---- Serving loop. No counterpart in the reference: the reference evaluates
  * episodes with Gymnasium environments on the host (gym_adapter/gpu.py:57-83);

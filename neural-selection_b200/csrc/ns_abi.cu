@@ -485,6 +485,31 @@ long long nsb_gpu_take_events(void *p) {
     }
 }
 
+// Delivery mode of the light tick kernel: 1 warp-cooperative release, 0
+// serial per neuron. Returns the previous mode, or -1.
+int nsb_gpu_set_delivery(void *p, int cooperative) {
+    try {
+        Engine &e = *static_cast<GpuBatch *>(p)->engine;
+        const int old = e.cooperative() ? 1 : 0;
+        e.set_cooperative(cooperative != 0);
+        return old;
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+// Times both delivery modes on the batch's own buffers (state restored) and
+// keeps the faster; returns the chosen mode (1 cooperative, 0 serial) or -1.
+int nsb_gpu_autotune(void *p, int ticks, float gain, void *stream) {
+    try {
+        return static_cast<GpuBatch *>(p)->engine->autotune(ticks, gain, static_cast<cudaStream_t>(stream)) ? 1 : 0;
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
 // ---- serving loop (no counterpart in the reference) ----------------------------
 // Continuous batching of genome-evaluation episodes on a device-resident
 // pole-on-cart environment; see neural-selection_b200/csrc/ns_serve.h.

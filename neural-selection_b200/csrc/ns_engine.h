@@ -67,6 +67,15 @@ public:
     // Captures step_device on the engine's own buffers into a CUDA graph and
     // replays it (one graph per (ticks, gain)).
     void step_graph(int ticks, float gain, cudaStream_t stream);
+    // Delivery mode of the light tick kernel: serial per neuron, or
+    // warp-cooperative release (faster for dense, active brains). Both give
+    // identical results. The default is chosen from the synapse density.
+    bool cooperative() const { return coop_; }
+    void set_cooperative(bool coop);
+    // Times both delivery modes on the engine's own buffers (a few steps each,
+    // state restored afterwards, so the call has no visible effect on the
+    // brains) and keeps the faster one. Returns the chosen mode.
+    bool autotune(int ticks, float gain, cudaStream_t stream);
     // Engine-owned device buffers for step_device / step_graph.
     float *dev_input() { return d_input_; }
     uint8_t *dev_mask() { return d_mask_; }
@@ -95,6 +104,7 @@ private:
     int max_unit_neurons_ = 0, hw_ = 0, meta_cap_ = 0, max_unit_brains_ = 0, unit_cap_ = 256;
     int grid_ = 0, grid_heavy_ = 0, block_ = 256, smem_ = 0, ctas_per_sm_ = 0, sms_ = 0, n_light_units_ = 0;
     bool count_events_ = true;
+    bool coop_ = false;
     std::vector<void *> allocations_;
     // device pools
     float *d_ngene_ = nullptr; uint32_t *d_nflags_ = nullptr; int *d_nsens_ = nullptr; int *d_nxidx_ = nullptr;

@@ -32,6 +32,7 @@ enum : uint32_t {
     NF_ADP = 1u << 8,            // afterdepolarisation tau > 0
     NF_HAS_INPUT = 1u << 9,      // ABI sensory index >= 0
     NF_EXC_TYPE = 1u << 10,      // type in {0,4,5}
+    NF_PLASTIC_IN = 1u << 11,    // at least one incoming synapse is plastic
     NF_SLOT_SHIFT = 16,          // bits 16-22: the neuron's brain slot within its work unit
     NF_SLOT_MASK = 0x7fu,
 };

@@ -52,6 +52,8 @@ SIGNATURES = {
     "nsb_gpu_load_state": (ct.c_int, [_vp, ct.c_int, _vp]),
     "nsb_gpu_stats": (ct.c_int, [_vp, _i32]),
     "nsb_gpu_take_events": (ct.c_longlong, [_vp]),
+    "nsb_gpu_set_delivery": (ct.c_int, [_vp, ct.c_int]),
+    "nsb_gpu_autotune": (ct.c_int, [_vp, ct.c_int, ct.c_float, _vp]),
     "nsb_serve_create": (_vp, [ct.c_longlong, ct.c_double, ct.c_double, ct.c_int, ct.c_int, ct.c_int, ct.c_float,
                                ct.c_double]),
     "nsb_serve_destroy": (None, [_vp]),
@@ -261,6 +263,20 @@ class GpuBatch:
         if v < 0:
             raise RuntimeError(_err(self.lib))
         return int(v)
+
+    def set_delivery(self, cooperative):
+        """Tick-kernel delivery mode (True: warp-cooperative release). Returns the previous mode."""
+        v = self.lib.nsb_gpu_set_delivery(self.ptr, 1 if cooperative else 0)
+        if v < 0:
+            raise RuntimeError(_err(self.lib))
+        return bool(v)
+
+    def autotune(self, ticks=16, gain=230.0, stream=0):
+        """Time both delivery modes on the batch's own buffers (state restored); keep the faster."""
+        v = self.lib.nsb_gpu_autotune(self.ptr, int(ticks), float(gain), ct.c_void_p(stream))
+        if v < 0:
+            raise RuntimeError(_err(self.lib))
+        return bool(v)
 
     def close(self):
         if getattr(self, "ptr", None):

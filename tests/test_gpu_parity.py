@@ -45,10 +45,12 @@ def _assert_brain_equal(gpu, ora, i, what):
 
 
 def run_parity(nsb, batch, calls, ticks=16, mask_fn=None, reset_at=(), seeds=None, check_every=1, block=0,
-               gain=None):
+               gain=None, delivery=None, autotune_at=()):
     delay = batch.max_delay
     gain = batch.gain if gain is None else gain
     gpu = nsb.GpuBatch.from_rows(batch, block=block)
+    if delivery is not None:
+        gpu.set_delivery(delivery)
     ora = _oracles(batch, delay)
     seeds = np.arange(batch.brains, dtype=np.uint32) * 17 + 20 if seeds is None else seeds
     gpu.reset(seeds)
@@ -63,6 +65,9 @@ def run_parity(nsb, batch, calls, ticks=16, mask_fn=None, reset_at=(), seeds=Non
             for i, o in enumerate(ora):
                 if rmask[i]:
                     o.reset(int(seeds[i] + c))
+        if c in autotune_at:
+            gpu.upload(inputs, mask)
+            gpu.autotune(ticks, gain)      # times both modes; must leave the state untouched
         out, status = gpu.step(inputs, mask, ticks, gain)
         for i, o in enumerate(ora):
             if mask[i]:
@@ -77,10 +82,17 @@ def run_parity(nsb, batch, calls, ticks=16, mask_fn=None, reset_at=(), seeds=Non
     return gpu, ora
 
 
-def test_parity_mix_every_profile_and_cell_type(nsb):
+@pytest.mark.parametrize("delivery", [False, True])
+def test_parity_mix_every_profile_and_cell_type(nsb, delivery):
     batch = nsb.workloads.parity_mix(brains=16)
     gpu, _ = run_parity(nsb, batch, calls=8, mask_fn=lambda c: np.array(
-        [1 if (i + c) % 4 else 0 for i in range(batch.brains)], np.uint8), reset_at=(3, 6))
+        [1 if (i + c) % 4 else 0 for i in range(batch.brains)], np.uint8), reset_at=(3, 6), delivery=delivery)
+    gpu.close()
+
+
+def test_autotune_leaves_state_untouched(nsb):
+    batch = nsb.workloads.plain_small(brains=12)
+    gpu, _ = run_parity(nsb, batch, calls=6, autotune_at=(2, 4))
     gpu.close()
 
 
@@ -90,12 +102,13 @@ def test_plain_small_2000_ticks_bitexact(nsb):
     assert sum(o.dump()[0][:, 26].astype(np.int64).sum() for o in ora) > 0
 
 
-def test_extended_delays_and_large_brains(nsb):
+@pytest.mark.parametrize("delivery", [False, True])
+def test_extended_delays_and_large_brains(nsb, delivery):
     """Delays up to 16 ms (ring of 17 in the oracle) and brains above the CTA
     size, which take the multi-neuron-per-thread path."""
     batch = nsb.workloads.batched_uneven(brains=48, total_neurons=48 * 160, total_synapses=48 * 320)
     assert max(n for n, _ in zip(np.diff(batch.neuron_offsets), range(99))) > 256
-    gpu, _ = run_parity(nsb, batch, calls=6, check_every=2)
+    gpu, _ = run_parity(nsb, batch, calls=6, check_every=2, delivery=delivery)
     st = gpu.stats()
     assert st["big_units"] >= 1
 
