@@ -468,6 +468,112 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def run_serve(args, rank, world, local_rank):
+    """Serving loop (config 5): genome-evaluation episodes on the pole-on-cart
+    environment. Phases:
+      1. saturation: a backlog larger than the in-flight cap; peak batched
+         throughput = neuron-ticks launched per second over the last
+         `serve_seconds / 2` seconds, in episodes/s through the mean episode
+         work of the request mix;
+      2. open loop at --serve-load x peak (Poisson), then drain: p50/p99
+         latency (arrival -> result) of the requests that arrived after the
+         first quarter of the window, and the achieved fraction of peak;
+      3. open loop at --serve-rate (the configured 2,000 requests/s) for the
+         same window: what completes, at what latency, and the backlog left.
+    """
+    if rank != 0:
+        return
+    import torch
+    torch.cuda.set_device(local_rank)
+    nsb = load_package()
+    W = nsb.workloads
+    lib = W.serving_library(seed=5, genomes=args.serve_genomes)
+    sizes = np.diff(lib.neuron_offsets).astype(np.float64)
+    mean_steps = (200 + 2000) / 2.0
+    work_per_episode = sizes.mean() * mean_steps * 16      # neuron-ticks, library drawn uniformly
+
+    def server():
+        srv = nsb.Server(max_inflight_neurons=args.serve_cap, hbm_budget_bytes=150e9)
+        ids = np.array(srv.register_batch(lib), np.int32)
+        return srv, ids
+
+    def wait(srv, until, results):
+        while srv.now() < until:
+            time.sleep(0.2)
+            results.append(srv.poll())
+
+    T = args.serve_seconds
+    # 1. saturation
+    srv, ids = server()
+    n = int(max(20000, 3 * args.serve_cap / sizes.mean()))
+    sched = W.serving_schedule(11, 1e6, n / 1e6, len(ids))
+    srv.submit(ids[sched["genome"]], sched["seed"], sched["steps"], tag=sched["tag"], arrival=0.0)
+    srv.start()
+    res = []
+    wait(srv, T / 2, res)
+    a = srv.stats()
+    wait(srv, T, res)
+    b = srv.stats()
+    srv.stop()
+    srv.close()
+    peak_nt = (b["neuron_ticks_launched"] - a["neuron_ticks_launched"]) / (b["elapsed_s"] - a["elapsed_s"])
+    peak_eps = peak_nt / work_per_episode
+    peak_events = (b["events"] - a["events"]) / (b["elapsed_s"] - a["elapsed_s"])
+
+    def open_loop(rate, drain):
+        srv, ids = server()
+        sch = W.serving_schedule(13, rate, T, len(ids))
+        t0 = srv.now() + 0.5
+        srv.submit(ids[sch["genome"]], sch["seed"], sch["steps"], tag=sch["tag"], arrival=sch["arrival"] + t0)
+        srv.start()
+        res = []
+        wait(srv, t0 + T / 4, res)
+        s0 = srv.stats()
+        wait(srv, t0 + T, res)
+        s1 = srv.stats()
+        if drain:
+            deadline = t0 + T + 120
+            while srv.stats()["inflight"] + srv.stats()["queued"] > 0 and srv.now() < deadline:
+                time.sleep(0.2)
+                res.append(srv.poll())
+        s2 = srv.stats()
+        srv.stop()
+        res.append(srv.poll_all())
+        srv.close()
+        r = np.concatenate(res)
+        arr = r["arrival_s"] - t0
+        window = r[(arr >= T / 4) & (arr < T)]
+        lat = window["done_s"] - window["arrival_s"]
+        nt = (s1["neuron_ticks_launched"] - s0["neuron_ticks_launched"]) / (s1["elapsed_s"] - s0["elapsed_s"])
+        done_in_window = ((r["done_s"] - t0 >= T / 4) & (r["done_s"] - t0 < T)).sum()
+        out = {"offered_per_s": rate, "arrived": int(len(sch["arrival"])), "completed": int(len(r)),
+               "episodes_per_s": float(done_in_window / (0.75 * T)), "neuron_ticks_per_s": nt,
+               "frac_of_peak": nt / peak_nt,
+               "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
+               "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
+               "backlog_at_end": int(s1["queued"] + s1["inflight"]),
+               "nonfinite": int((r["status"] != 0).sum())}
+        if len(lat):
+            out["p99_over_p50"] = out["p99_s"] / out["p50_s"]
+        if not drain:
+            out["note"] = "latency of requests completed within the window only (overloaded: the rest are queued)"
+        return out
+
+    loaded = open_loop(args.serve_load * peak_eps, drain=True)
+    configured = open_loop(args.serve_rate, drain=False)
+    line = {"metric": "p99 episode latency, serving loop at the measured load", "value": loaded["p99_s"],
+            "unit": "s", "n_gpus": 1, "higher_is_better": False, "vs_baseline": None, "dtype": "f32",
+            "data": f"synthetic (Philox4x32-10): {len(ids)} genomes, N log-uniform 32-4096, 8 synapses/neuron; "
+                    "Poisson arrivals, episodes U[200, 2000] steps",
+            "config": {"workload": "serving_cartpole_episodes", "inflight_cap_neurons": args.serve_cap,
+                       "hbm_budget_bytes": 150e9, "window_s": T, "ticks_per_step": 16,
+                       "mean_episode_neuron_ticks": work_per_episode},
+            "peak": {"neuron_ticks_per_s": peak_nt, "episodes_per_s": peak_eps, "synaptic_events_per_s": peak_events,
+                     "busy_frac": (b["busy_s"] - a["busy_s"]) / (b["elapsed_s"] - a["elapsed_s"])},
+            "at_load": loaded, "at_configured_rate": configured}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -477,11 +583,19 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fraction", type=int, default=1, choices=[1, 2, 4, 8, 16],
                     help="run a 1/D slice of the full pools (profiler captures only)")
+    ap.add_argument("--serve", action="store_true", help="serving-loop latency/throughput (config 5)")
+    ap.add_argument("--serve-seconds", type=float, default=60.0)
+    ap.add_argument("--serve-load", type=float, default=0.85, help="offered load as a fraction of peak")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="configured arrival rate (requests/s)")
+    ap.add_argument("--serve-cap", type=int, default=4194304, help="neurons in flight")
+    ap.add_argument("--serve-genomes", type=int, default=512)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus if "RANK" in os.environ else 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
-    if args.impl == "reference":
+    if args.serve:
+        run_serve(args, rank, world, local_rank)
+    elif args.impl == "reference":
         run_reference(args, rank, world)
     elif args.impl == "reference-cuda":
         run_reference_cuda(args, rank, world, local_rank)

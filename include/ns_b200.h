@@ -154,8 +154,10 @@ int nsb_serve_run(void *server, long long max_iterations);
 int nsb_serve_poll(void *server, void *results, int max);
 double nsb_serve_now(void *server);
 /* steps, admitted, completed, queued, inflight, inflight_neurons, units,
- * neuron_ticks, busy_s, elapsed_s, events, pool_neurons, pool_synapses,
- * pool_bytes, inflight_bytes. Returns the count written (15). */
+ * neuron_ticks (of completed episodes), busy_s, elapsed_s, events,
+ * pool_neurons, pool_synapses, pool_bytes, inflight_bytes,
+ * neuron_ticks_launched (neurons in flight x ticks over launched steps).
+ * Returns the count written (16). */
 int nsb_serve_stats(void *server, double *out);
 
 #ifdef __cplusplus

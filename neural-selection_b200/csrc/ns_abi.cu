@@ -610,16 +610,16 @@ double nsb_serve_now(void *p) { return static_cast<Server *>(p)->now(); }
 
 // steps, admitted, completed, queued, inflight, inflight_neurons, units,
 // neuron_ticks, busy_s, elapsed_s, events, pool_neurons, pool_synapses,
-// pool_bytes, inflight_bytes
+// pool_bytes, inflight_bytes, neuron_ticks_launched
 int nsb_serve_stats(void *p, double *out) {
     try {
         const ServeStats s = static_cast<Server *>(p)->stats();
-        const double v[15] = {(double)s.steps, (double)s.admitted, (double)s.completed, (double)s.queued,
+        const double v[16] = {(double)s.steps, (double)s.admitted, (double)s.completed, (double)s.queued,
                               (double)s.inflight, (double)s.inflight_neurons, (double)s.units, s.neuron_ticks,
                               s.busy_s, s.elapsed_s, (double)s.events, (double)s.pool_neurons,
-                              (double)s.pool_synapses, s.pool_bytes, s.inflight_bytes};
+                              (double)s.pool_synapses, s.pool_bytes, s.inflight_bytes, s.neuron_ticks_launched};
         std::memcpy(out, v, sizeof v);
-        return 15;
+        return 16;
     } catch (const std::exception &e) {
         g_error = e.what();
         return -1;

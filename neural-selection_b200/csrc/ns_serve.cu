@@ -613,6 +613,7 @@ void Server::iteration() {
             reinterpret_cast<Ring *>(d_ring_[par]), keep_, smooth_);
         NSB_CHECK(cudaGetLastError());
         ++steps_run_;
+        launched_ticks_.store(launched_ticks_.load() + (double)inflight_neurons_.load() * cfg_.ticks);
         stepped = true;
     }
     NSB_CHECK(cudaEventRecord(ev_[par], stream_));
@@ -740,6 +741,7 @@ ServeStats Server::stats() {
     s.pool_synapses = ecap_;
     s.pool_bytes = ncap_ * kNeuronBytes + ecap_ * kSynapseBytes;
     s.inflight_bytes = inflight_bytes_;
+    s.neuron_ticks_launched = launched_ticks_;
     return s;
 }
 

@@ -68,6 +68,7 @@ struct ServeStats {
     unsigned long long events;
     long long pool_neurons, pool_synapses;
     double pool_bytes, inflight_bytes;
+    double neuron_ticks_launched;   // neurons in flight x ticks, summed over launched steps
 };
 
 class Server {
@@ -183,7 +184,7 @@ private:
     // counters written by the loop thread, read by stats()
     std::atomic<long long> inflight_neurons_{0}, inflight_{0}, admitted_{0}, completed_{0}, steps_run_{0},
         n_units_live_{0};
-    std::atomic<double> inflight_bytes_{0}, neuron_ticks_{0}, busy_s_{0};
+    std::atomic<double> inflight_bytes_{0}, neuron_ticks_{0}, busy_s_{0}, launched_ticks_{0};
     std::chrono::steady_clock::time_point epoch_;
     float keep_ = 0.6f, smooth_ = 0.4f;
 };

@@ -28,7 +28,8 @@ RESULT_DTYPE = np.dtype([("tag", np.uint64), ("genome", np.int32), ("steps", np.
                          ("done_s", np.float64)])
 assert RESULT_DTYPE.itemsize == 64
 STATS = ("steps", "admitted", "completed", "queued", "inflight", "inflight_neurons", "units", "neuron_ticks",
-         "busy_s", "elapsed_s", "events", "pool_neurons", "pool_synapses", "pool_bytes", "inflight_bytes")
+         "busy_s", "elapsed_s", "events", "pool_neurons", "pool_synapses", "pool_bytes", "inflight_bytes",
+         "neuron_ticks_launched")
 
 
 class Server:
