@@ -37,8 +37,13 @@ __device__ __forceinline__ uint32_t xorshift32(uint32_t x) {
 __device__ __forceinline__ float crexp(float x, const float *tab) { return nsx::expf_cr_ff(x, tab); }
 
 // physiology.cuh:226-230: thin-branch input/output curve (type 0 only).
+// When gs - 4 rounds to exactly -4 (|gs| below half an ulp of 4, about
+// 2.4e-7: a branch decaying after its last input), the exponent -(gs - 4)/0.4
+// is exactly 10, the same binary32 value as in the offset 5/(1 + exp(10)), so
+// regen equals the offset bit for bit and the exponential is skipped.
 __device__ __forceinline__ float branch_gain(float gs, float offset, const float *tab) {
-    float regen = 5.0f / (1.0f + crexp(-(gs - 4.0f) / 0.4f, tab));
+    const float t = gs - 4.0f;
+    const float regen = t == -4.0f ? offset : 5.0f / (1.0f + crexp(-t / 0.4f, tab));
     return fminf(11.0f, gs + regen - offset);
 }
 
