@@ -505,7 +505,7 @@ def run_serve(args, rank, world, local_rank):
     T = args.serve_seconds
     # 1. saturation
     srv, ids = server()
-    n = int(max(20000, 3 * args.serve_cap / sizes.mean()))
+    n = int(max(20000, 3 * args.serve_cap / sizes.mean(), 1000 * T))   # outlasts the window at any rate seen
     sched = W.serving_schedule(11, 1e6, n / 1e6, len(ids))
     srv.submit(ids[sched["genome"]], sched["seed"], sched["steps"], tag=sched["tag"], arrival=0.0)
     srv.start()
@@ -569,7 +569,8 @@ def run_serve(args, rank, world, local_rank):
                        "hbm_budget_bytes": 150e9, "window_s": T, "ticks_per_step": 16,
                        "mean_episode_neuron_ticks": work_per_episode},
             "peak": {"neuron_ticks_per_s": peak_nt, "episodes_per_s": peak_eps, "synaptic_events_per_s": peak_events,
-                     "busy_frac": (b["busy_s"] - a["busy_s"]) / (b["elapsed_s"] - a["elapsed_s"])},
+                     "busy_frac": (b["busy_s"] - a["busy_s"]) / (b["elapsed_s"] - a["elapsed_s"]),
+                     "queued_at_window_end": int(b["queued"])},
             "at_load": loaded, "at_configured_rate": configured}
     print(json.dumps(line), flush=True)
 

@@ -119,6 +119,25 @@ int nsb_gpu_set_delivery(void *batch, int cooperative);
  * (state restored afterwards) and keeps the faster; returns it, or -1. */
 int nsb_gpu_autotune(void *batch, int ticks, float gain, void *stream);
 
+/* ---- Checkpoint records. The world simulator saves the neural pools as
+ * CheckpointNeuron (344 B) and CheckpointSynapse (136 B) records, one per
+ * occupied slot in ascending slot order (src/main.cu:164-264, packed by
+ * pack_checkpoint_neurons/_synapses; stream order src/checkpoint_impl.cuh:190-211),
+ * under a header whose layout hash covers the build's sizes
+ * (src/checkpoint_impl.cuh:20-32). */
+/* The reference build's checkpoint layout hash (0x2b1cd1c766eebf82). */
+unsigned long long nsb_checkpoint_layout(void);
+/* Every brain of the batch as checkpoint records (neuron_records: sum of
+ * counts x 344 B, synapse_records: sum of edges x 136 B; brain i's neurons at
+ * slots [sum of earlier counts, ...), owner = brain index, next = next slot of
+ * the brain or -1, port = sensory channel, channels + motor index, or -1) and
+ * one tick per brain. Returns 0 or -1. */
+int nsb_gpu_checkpoint_export(void *batch, void *neuron_records, void *synapse_records, int64_t *ticks);
+/* Loads states, spike histories and ticks from records laid out as the export
+ * writes them; slots, owners and genes must describe this batch. */
+int nsb_gpu_checkpoint_import(void *batch, const void *neuron_records, long long neuron_count,
+                              const void *synapse_records, long long synapse_count, const int64_t *ticks);
+
 /* ---- Serving loop. No counterpart in the reference: the reference evaluates
  * episodes with Gymnasium environments on the host (gym_adapter/gpu.py:57-83);
  * this server keeps episodes of different genomes and lengths on the device,

@@ -176,6 +176,11 @@ Engine &brain_engine(HostBrain &b) {
 
 struct GpuBatch {
     std::unique_ptr<Engine> engine;
+    // Genes in the reference layout, kept for checkpoint records.
+    std::vector<ref::NeuronGene> genes;
+    std::vector<ref::SynapseGene> conns;
+    std::vector<int> noff, soff, motors, sensory;
+    int channels = 0, outputs = 0;
 };
 
 }  // namespace
@@ -282,6 +287,18 @@ static void *gpu_create(void **handles, int count, int max_delay_floor, int bloc
     if (const char *slots = std::getenv("NSB_UNIT_SLOTS")) cfg.unit_slots = std::max(1, std::atoi(slots));
     auto batch = std::make_unique<GpuBatch>();
     batch->engine = std::make_unique<Engine>(specs, channels, outputs, cfg);
+    batch->channels = channels;
+    batch->outputs = outputs;
+    batch->noff.push_back(0);
+    batch->soff.push_back(0);
+    for (const auto &sp : specs) {
+        batch->genes.insert(batch->genes.end(), sp.genes, sp.genes + sp.count);
+        batch->conns.insert(batch->conns.end(), sp.conns, sp.conns + sp.edges);
+        batch->motors.insert(batch->motors.end(), sp.motors, sp.motors + outputs);
+        batch->sensory.insert(batch->sensory.end(), sp.sensory, sp.sensory + sp.count);
+        batch->noff.push_back(batch->noff.back() + sp.count);
+        batch->soff.push_back(batch->soff.back() + sp.edges);
+    }
     return batch.release();
 }
 
@@ -504,6 +521,138 @@ int nsb_gpu_set_delivery(void *p, int cooperative) {
 int nsb_gpu_autotune(void *p, int ticks, float gain, void *stream) {
     try {
         return static_cast<GpuBatch *>(p)->engine->autotune(ticks, gain, static_cast<cudaStream_t>(stream)) ? 1 : 0;
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+}  // extern "C"
+
+// ---- checkpoint records (src/main.cu:164-264, src/checkpoint_impl.cuh) -----
+namespace {
+
+bool same_bits(float a, float b) { return std::memcmp(&a, &b, 4) == 0; }
+bool gene_equal(const ref::NeuronGene &a, const ref::NeuronGene &b) {
+    const float fa[] = {a.cap, a.gl, a.el, a.vt, a.slope, a.a, a.tau_w, a.b, a.vr, a.adp_b, a.adp_tau, a.lp.calcium,
+                        a.lp.calcium_k, a.lp.h, a.lp.leak, a.prinz_leak, a.rec_base, a.rec_gain, a.rec_event,
+                        a.rec_decay, a.affinity};
+    const float fb[] = {b.cap, b.gl, b.el, b.vt, b.slope, b.a, b.tau_w, b.b, b.vr, b.adp_b, b.adp_tau, b.lp.calcium,
+                        b.lp.calcium_k, b.lp.h, b.lp.leak, b.prinz_leak, b.rec_base, b.rec_gain, b.rec_event,
+                        b.rec_decay, b.affinity};
+    for (size_t i = 0; i < sizeof fa / sizeof fa[0]; ++i)
+        if (!same_bits(fa[i], fb[i])) return false;
+    for (int i = 0; i < 8; ++i)
+        if (!same_bits(a.prinz.g[i], b.prinz.g[i])) return false;
+    return a.type == b.type && a.active == b.active && a.modulator == b.modulator && a.inh_tx == b.inh_tx &&
+           a.sensory_channel == b.sensory_channel;
+}
+bool conn_equal(const ref::SynapseGene &a, const ref::SynapseGene &b) {
+    return same_bits(a.w0, b.w0) && same_bits(a.U, b.U) && same_bits(a.trec, b.trec) && same_bits(a.tfac, b.tfac) &&
+           a.pre == b.pre && a.post == b.post && a.delay == b.delay && a.active == b.active &&
+           a.plasticity == b.plasticity && a.branch == b.branch && a.sites == b.sites && a.receptors == b.receptors &&
+           same_bits(a.slow_rec, b.slow_rec) && same_bits(a.slow_depl, b.slow_depl);
+}
+int port_of(const GpuBatch &g, int brain, int j) {
+    const int sens = g.sensory[g.noff[brain] + j];
+    if (sens >= 0) return sens;
+    for (int k = 0; k < g.outputs; ++k)
+        if (g.motors[(size_t)brain * g.outputs + k] == j) return g.channels + k;
+    return -1;
+}
+
+}  // namespace
+
+extern "C" {
+
+// FNV-1a layout hash of the reference build's checkpoint (src/checkpoint_impl.cuh:20-32).
+unsigned long long nsb_checkpoint_layout() { return ref::layout_hash(); }
+
+// The state of every brain as the reference's checkpoint records: neuron
+// records (sum of counts x 344 B) and synapse records (sum of edges x 136 B)
+// in slot order, brain i's neurons at slots [sum of earlier counts, ...),
+// owner = brain index, next = the brain's next slot (-1 last), port = sensory
+// channel, or channels + motor index, or -1. Per-tick accumulators and the
+// world's modulatory timestamps are zero between steps. ticks: one per brain.
+int nsb_gpu_checkpoint_export(void *p, void *neuron_records, void *synapse_records, int64_t *ticks) {
+    try {
+        GpuBatch &g = *static_cast<GpuBatch *>(p);
+        auto *nr = static_cast<ref::CheckpointNeuron *>(neuron_records);
+        auto *sr = static_cast<ref::CheckpointSynapse *>(synapse_records);
+        const int brains = (int)g.noff.size() - 1;
+        for (int b = 0; b < brains; ++b) {
+            const int n = g.noff[b + 1] - g.noff[b], m = g.soff[b + 1] - g.soff[b];
+            std::vector<ref::NeuronState> ns(n);
+            std::vector<ref::SynapseState> ss(std::max(m, 1));
+            std::vector<std::array<unsigned char, 9>> hist(n);
+            int64_t tick = 0;
+            g.engine->export_state(b, ns.data(), ss.data(), reinterpret_cast<unsigned char (*)[9]>(hist.data()), &tick);
+            for (int j = 0; j < n; ++j) {
+                ref::CheckpointNeuron r;
+                std::memset(&r, 0, sizeof r);
+                r.slot = g.noff[b] + j;
+                r.owner = b;
+                r.next = j + 1 < n ? r.slot + 1 : -1;
+                r.port = port_of(g, b, j);
+                r.gene = g.genes[r.slot];
+                r.state = ns[j];
+                std::memcpy(r.spike_history, hist[j].data(), 9);
+                nr[r.slot] = r;
+            }
+            for (int j = 0; j < m; ++j) {
+                ref::CheckpointSynapse r;
+                std::memset(&r, 0, sizeof r);
+                r.slot = g.soff[b] + j;
+                r.owner = b;
+                r.next = j + 1 < m ? r.slot + 1 : -1;
+                r.gene = g.conns[r.slot];
+                r.state = ss[j];
+                sr[r.slot] = r;
+            }
+            if (ticks) ticks[b] = tick;
+        }
+        return 0;
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+// Loads every brain's state from checkpoint records laid out as the export
+// writes them. The records' slots, owners and genes must describe this
+// batch's brains; their states, spike histories and the ticks replace the
+// batch's.
+int nsb_gpu_checkpoint_import(void *p, const void *neuron_records, long long n_records, const void *synapse_records,
+                              long long e_records, const int64_t *ticks) {
+    try {
+        GpuBatch &g = *static_cast<GpuBatch *>(p);
+        const auto *nr = static_cast<const ref::CheckpointNeuron *>(neuron_records);
+        const auto *sr = static_cast<const ref::CheckpointSynapse *>(synapse_records);
+        const int brains = (int)g.noff.size() - 1;
+        if (n_records != g.noff.back() || e_records != g.soff.back())
+            throw std::runtime_error("Checkpoint record counts differ from the batch");
+        for (int b = 0; b < brains; ++b) {
+            const int n = g.noff[b + 1] - g.noff[b], m = g.soff[b + 1] - g.soff[b];
+            std::vector<ref::NeuronState> ns(n);
+            std::vector<ref::SynapseState> ss(std::max(m, 1));
+            std::vector<std::array<unsigned char, 9>> hist(n);
+            for (int j = 0; j < n; ++j) {
+                const auto &r = nr[g.noff[b] + j];
+                if (r.slot != g.noff[b] + j || r.owner != b) throw std::runtime_error("Invalid checkpoint neuron record");
+                if (!gene_equal(r.gene, g.genes[r.slot])) throw std::runtime_error("Checkpoint genes differ from the batch");
+                ns[j] = r.state;
+                std::memcpy(hist[j].data(), r.spike_history, 9);
+            }
+            for (int j = 0; j < m; ++j) {
+                const auto &r = sr[g.soff[b] + j];
+                if (r.slot != g.soff[b] + j || r.owner != b) throw std::runtime_error("Invalid checkpoint synapse record");
+                if (!conn_equal(r.gene, g.conns[r.slot])) throw std::runtime_error("Checkpoint genes differ from the batch");
+                ss[j] = r.state;
+            }
+            g.engine->load_state(b, ns.data(), ss.data(), reinterpret_cast<const unsigned char (*)[9]>(hist.data()),
+                                 ticks ? ticks[b] : 0);
+        }
+        return 0;
     } catch (const std::exception &e) {
         g_error = e.what();
         return -1;

@@ -1184,6 +1184,62 @@ void Engine::dump(int brain, uint32_t *nw, uint32_t *sw, int64_t *tick) {
     }
 }
 
+void Engine::export_state(int brain, ref::NeuronState *neurons, ref::SynapseState *synapses,
+                          unsigned char (*history)[9], int64_t *tick_out) {
+    if (brain < 0 || brain >= n_brains_) throw std::runtime_error("Invalid brain index");
+    NSB_CHECK(cudaDeviceSynchronize());
+    const int4 U = h_units_[h_bunit_[brain]];
+    const int un0 = U.x, unn = U.y, ue0 = U.z, une = U.w;
+    const int nn = h_noff_[brain + 1] - h_noff_[brain], ne = h_soff_[brain + 1] - h_soff_[brain];
+    std::vector<uint32_t> rec((size_t)unn * S_WORDS), srec((size_t)std::max(une, 1) * Z_WORDS);
+    std::vector<uint8_t> arr(std::max(une, 1));
+    int64_t tick = 0;
+    NSB_CHECK(cudaMemcpy(rec.data(), d_nstate_ + (size_t)un0 * S_WORDS, rec.size() * 4, cudaMemcpyDeviceToHost));
+    if (une) {
+        NSB_CHECK(cudaMemcpy(srec.data(), d_sstate_ + (size_t)ue0 * Z_WORDS, (size_t)une * Z_WORDS * 4, cudaMemcpyDeviceToHost));
+        NSB_CHECK(cudaMemcpy(arr.data(), d_sarrived_ + ue0, une, cudaMemcpyDeviceToHost));
+    }
+    NSB_CHECK(cudaMemcpy(&tick, d_btick_ + brain, 8, cudaMemcpyDeviceToHost));
+    auto uf = [](uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; };
+    for (int j = 0; j < nn; ++j) {
+        const int n = h_npos_[h_noff_[brain] + j];
+        const uint32_t *r = &rec[(size_t)(n - un0) * S_WORDS];
+        ref::NeuronState s;
+        std::memset(&s, 0, sizeof s);
+        s.v = uf(r[S_V]); s.w = uf(r[S_W]); s.adp = uf(r[S_ADP]); s.inh = uf(r[S_INH]); s.depol = uf(r[S_DEPOL]);
+        s.log_ampa = uf(r[S_LOGAMPA]); s.rec_ns = uf(r[S_RECNS]); s.rec_rng = r[S_RECRNG];
+        s.dend[0] = uf(r[S_D0]); s.dend[1] = uf(r[S_D1]); s.dend[2] = uf(r[S_D2]); s.dend[3] = uf(r[S_D3]);
+        s.total = (int)r[S_TOTAL]; s.spike = (unsigned char)r[S_SPIKE];
+        const int xi = h_nxidx_[n];
+        if (xi >= 0) NSB_CHECK(cudaMemcpy(s.cell, d_xstate_ + (size_t)xi * 16, 64, cudaMemcpyDeviceToHost));
+        neurons[j] = s;
+        if (history) {
+            std::memset(history[j], 0, 9);
+            for (int k = 1; k <= 9; ++k) {
+                const int64_t tau = tick - k;
+                if (tau < 0) break;
+                history[j][tau % 9] = (unsigned char)((r[S_HIST] >> (tau & 31)) & 1u);
+            }
+        }
+    }
+    for (int j = 0; j < ne; ++j) {
+        const int e = h_spos_[h_soff_[brain] + j] - ue0;
+        const uint32_t *z = &srec[(size_t)e * Z_WORDS];
+        ref::SynapseState s;
+        std::memset(&s, 0, sizeof s);
+        s.w = uf(z[Z_W]); s.ru = uf(z[Z_RU]); s.pre_tr = uf(z[Z_PRETR]); s.post_tr = uf(z[Z_POSTTR]);
+        s.eltp = uf(z[Z_ELTP]); s.eltd = uf(z[Z_ELTD]); s.da_age = uf(z[Z_DAAGE]); s.spine = uf(z[Z_SPINE]);
+        s.st_age = uf(z[Z_STAGE]); s.pre_age = uf(z[Z_PREAGE]); s.post_age = uf(z[Z_POSTAGE]);
+        s.last = (int64_t)(int32_t)z[Z_LAST];
+        s.ready = ((uint64_t)z[Z_READYHI] << 32) | z[Z_READYLO];
+        s.rng = z[Z_RNG];
+        s.arrived = arr[e];
+        s.slow = uf(z[Z_SLOW]);
+        synapses[j] = s;
+    }
+    if (tick_out) *tick_out = tick;
+}
+
 void Engine::load_state(int brain, const ref::NeuronState *neurons, const ref::SynapseState *synapses,
                         const unsigned char (*history)[9], int64_t tick) {
     if (brain < 0 || brain >= n_brains_) throw std::runtime_error("Invalid brain index");

@@ -87,6 +87,10 @@ public:
     // Load one brain's state from reference records (checkpoint / host state).
     void load_state(int brain, const ref::NeuronState *neurons, const ref::SynapseState *synapses,
                     const unsigned char (*history)[9], int64_t tick);
+    // Inverse of load_state: one brain's state as reference records, its
+    // 9-slot spike history ring (index tick % 9) and tick.
+    void export_state(int brain, ref::NeuronState *neurons, ref::SynapseState *synapses,
+                      unsigned char (*history)[9], int64_t *tick);
     // Synaptic arrivals counted since the last call to take_events().
     unsigned long long take_events();
     int64_t host_tick(int brain) const { return h_tick_[brain]; }

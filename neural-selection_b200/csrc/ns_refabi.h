@@ -75,6 +75,41 @@ struct Brain {
     int64_t tick = 0;
 };
 
+// World checkpoint records of the neural pools (src/main.cu:164-177): packed
+// per occupied slot, ascending slot order (src/checkpoint_impl.cuh:190-211).
+struct CheckpointNeuron {
+    int slot, owner, next, port;
+    NeuronGene gene;
+    NeuronState state;
+    float pending_exc[4], pending_inh;
+    unsigned long long mod_event_tick[6];
+    unsigned char spike_history[9];
+};
+struct CheckpointSynapse {
+    int slot, owner, next;
+    SynapseGene gene;
+    SynapseState state;
+};
+
+// The 20 build constants the reference's checkpoint layout hash covers
+// (src/checkpoint_impl.cuh:20-32): P, neuron and synapse capacities, S, M, W,
+// H, DENDRITES, HISTORY, TICKS (src/main.cu:33-47, src/physiology.cuh:17),
+// then the sizes of Animal, NeuronGene, NeuronState, SynapseGene,
+// SynapseState, CheckpointNeuron, CheckpointSynapse, BehaviorTotals,
+// LifeRecord and BiteEvent as the reference builds them with nvcc on x86-64.
+constexpr uint64_t kLayoutValues[20] = {32768, 4194304, 8388608, 19, 5, 128, 128, 4, 9, 16,
+                                        472, 124, 120, 40, 80, 344, 136, 528, 504, 24};
+// FNV-1a over those values (the reference's checkpoint_layout()).
+constexpr uint64_t layout_hash() {
+    uint64_t h = 1469598103934665603ull;
+    for (uint64_t v : kLayoutValues) {
+        h ^= v;
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+static_assert(layout_hash() == 0x2b1cd1c766eebf82ull, "checkpoint layout hash");
+
 static_assert(sizeof(NeuronGene) == 124, "NeuronGene layout");
 static_assert(offsetof(NeuronGene, type) == 44 && offsetof(NeuronGene, lp) == 48, "NeuronGene layout");
 static_assert(offsetof(NeuronGene, sensory_channel) == 100 && offsetof(NeuronGene, rec_base) == 104, "NeuronGene layout");
@@ -84,6 +119,12 @@ static_assert(sizeof(SynapseGene) == 40 && offsetof(SynapseGene, delay) == 24 &&
               "SynapseGene layout");
 static_assert(sizeof(SynapseState) == 80 && offsetof(SynapseState, last) == 48 && offsetof(SynapseState, rng) == 64 &&
               offsetof(SynapseState, slow) == 72, "SynapseState layout");
+static_assert(sizeof(CheckpointNeuron) == 344 && offsetof(CheckpointNeuron, gene) == 16 &&
+              offsetof(CheckpointNeuron, state) == 140 && offsetof(CheckpointNeuron, pending_exc) == 260 &&
+              offsetof(CheckpointNeuron, pending_inh) == 276 && offsetof(CheckpointNeuron, mod_event_tick) == 280 &&
+              offsetof(CheckpointNeuron, spike_history) == 328, "CheckpointNeuron layout");
+static_assert(sizeof(CheckpointSynapse) == 136 && offsetof(CheckpointSynapse, gene) == 12 &&
+              offsetof(CheckpointSynapse, state) == 56, "CheckpointSynapse layout");
 
 }  // namespace ref
 }  // namespace nsb

@@ -53,6 +53,9 @@ SIGNATURES = {
     "nsb_gpu_stats": (ct.c_int, [_vp, _i32]),
     "nsb_gpu_take_events": (ct.c_longlong, [_vp]),
     "nsb_gpu_set_delivery": (ct.c_int, [_vp, ct.c_int]),
+    "nsb_checkpoint_layout": (ct.c_ulonglong, []),
+    "nsb_gpu_checkpoint_export": (ct.c_int, [_vp, _vp, _vp, _i64]),
+    "nsb_gpu_checkpoint_import": (ct.c_int, [_vp, _vp, ct.c_longlong, _vp, ct.c_longlong, _i64]),
     "nsb_gpu_autotune": (ct.c_int, [_vp, ct.c_int, ct.c_float, _vp]),
     "nsb_serve_create": (_vp, [ct.c_longlong, ct.c_double, ct.c_double, ct.c_int, ct.c_int, ct.c_int, ct.c_float,
                                ct.c_double]),
@@ -94,6 +97,7 @@ def _err(lib):
 
 
 NW, SW = 32, 20
+CHECKPOINT_NEURON_BYTES, CHECKPOINT_SYNAPSE_BYTES = 344, 136
 STATS = ("brains", "units", "big_units", "neurons", "synapses", "heavy", "max_unit_neurons", "grid", "block",
          "smem_bytes", "ctas_per_sm")
 
@@ -263,6 +267,29 @@ class GpuBatch:
         if v < 0:
             raise RuntimeError(_err(self.lib))
         return int(v)
+
+    def checkpoint_export(self):
+        """Reference checkpoint records of every brain: (neuron records as a
+        uint8 array of N x 344, synapse records E x 136, ticks per brain)."""
+        n = sum(c for c, _ in self.sizes)
+        e = sum(m for _, m in self.sizes)
+        nr = np.zeros((max(n, 1), CHECKPOINT_NEURON_BYTES), np.uint8)
+        sr = np.zeros((max(e, 1), CHECKPOINT_SYNAPSE_BYTES), np.uint8)
+        ticks = np.zeros(self.count, np.int64)
+        if self.lib.nsb_gpu_checkpoint_export(self.ptr, nr.ctypes.data_as(ct.c_void_p), sr.ctypes.data_as(ct.c_void_p),
+                                              _p(ticks, _i64)):
+            raise RuntimeError(_err(self.lib))
+        return nr[:n], sr[:e], ticks
+
+    def checkpoint_import(self, neuron_records, synapse_records, ticks):
+        nr = np.ascontiguousarray(neuron_records, np.uint8).reshape(-1, CHECKPOINT_NEURON_BYTES)
+        sr = np.ascontiguousarray(synapse_records, np.uint8).reshape(-1, CHECKPOINT_SYNAPSE_BYTES)
+        t = np.ascontiguousarray(ticks, np.int64)
+        nrp = nr if len(nr) else np.zeros((1, CHECKPOINT_NEURON_BYTES), np.uint8)
+        srp = sr if len(sr) else np.zeros((1, CHECKPOINT_SYNAPSE_BYTES), np.uint8)
+        if self.lib.nsb_gpu_checkpoint_import(self.ptr, nrp.ctypes.data_as(ct.c_void_p), len(nr),
+                                              srp.ctypes.data_as(ct.c_void_p), len(sr), _p(t, _i64)):
+            raise RuntimeError(_err(self.lib))
 
     def set_delivery(self, cooperative):
         """Tick-kernel delivery mode (True: warp-cooperative release). Returns the previous mode."""

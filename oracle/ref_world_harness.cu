@@ -249,4 +249,22 @@ void ref_world_destroy(void *p) {
     delete w;
 }
 
+// Layout facts of the reference build: the 20 values its checkpoint layout
+// hash covers (src/checkpoint_impl.cuh:20-32), the hash, and the offsets of
+// the neural checkpoint records (src/main.cu:164-177).
+int ref_world_layout(uint64_t *values, uint64_t *hash, uint64_t *offsets) {
+    const uint64_t v[] = {P, NEURON_CAPACITY, SYNAPSE_CAPACITY, S, M, W, H, DENDRITES, HISTORY, TICKS,
+                          sizeof(Animal), sizeof(NeuronGene), sizeof(NeuronState), sizeof(SynapseGene),
+                          sizeof(SynapseState), sizeof(CheckpointNeuron), sizeof(CheckpointSynapse),
+                          sizeof(BehaviorTotals), sizeof(LifeRecord), sizeof(BiteEvent)};
+    for (int i = 0; i < 20; ++i) values[i] = v[i];
+    *hash = checkpoint_layout();
+    const uint64_t o[] = {offsetof(CheckpointNeuron, gene), offsetof(CheckpointNeuron, state),
+                          offsetof(CheckpointNeuron, pending_exc), offsetof(CheckpointNeuron, pending_inh),
+                          offsetof(CheckpointNeuron, mod_event_tick), offsetof(CheckpointNeuron, spike_history),
+                          offsetof(CheckpointSynapse, gene), offsetof(CheckpointSynapse, state)};
+    for (int i = 0; i < 8; ++i) offsets[i] = o[i];
+    return 20;
+}
+
 }  // extern "C"
