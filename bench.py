@@ -123,10 +123,15 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def workload(nsb, seed, fraction=1):
+def workload(nsb, seed, fraction=1, kind="batched_uneven"):
     """The full-pool workload, or with --fraction D a 1/D slice of it (brains,
     neuron and synapse pools all divided by D; same size distribution) for
-    profiler captures that must stay small."""
+    profiler captures that must stay small. kind "plasticity_heavy": the same
+    pools with every synapse on the triplet/dopamine profile (config 4)."""
+    if kind == "plasticity_heavy":
+        return nsb.workloads.plasticity_heavy(seed=seed + 2, brains=32768 // fraction,
+                                              total_neurons=4194304 // fraction,
+                                              total_synapses=8388608 // fraction)
     tag = "full" if fraction == 1 else f"div{fraction}"
     cache = Path(os.environ.get("NSB_BENCH_CACHE", "/tmp")) / f"nsb_uneven_{tag}_seed{seed}.npz"
     W = nsb.workloads
@@ -148,7 +153,7 @@ def workload(nsb, seed, fraction=1):
 _WORKER_BRAINS = []
 
 
-def _cpu_init(jobs, use_ref):
+def _cpu_init(jobs, use_ref, pulse):
     sys.path.insert(0, str(ROOT))
     from oracle import pyoracle
     global _WORKER_BRAINS
@@ -158,6 +163,8 @@ def _cpu_init(jobs, use_ref):
             b = pyoracle.RefBrain(rows_n, rows_s, motors, channels)
         else:
             b = pyoracle.OracleBrain(rows_n, rows_s, motors, channels, 16, libm=True)
+            if pulse:
+                b.set_pulse(*pulse)
         b.reset(7)
         _WORKER_BRAINS.append((b, inputs, len(rows_n)))
 
@@ -180,7 +187,9 @@ class CpuReference:
         import multiprocessing as mp
         sys.path.insert(0, str(ROOT))
         from oracle import pyoracle
-        self.use_ref = pyoracle.ref_lib() is not None
+        pulse = (batch.meta["pulse_period"], batch.meta["pulse_mod"]) if "pulse_period" in batch.meta else None
+        # The reference has no profile 6 (triplet/dopamine): that workload runs on the oracle port.
+        self.use_ref = pyoracle.ref_lib() is not None and pulse is None
         idx = np.argsort(np.diff(batch.neuron_offsets), kind="stable")[::stride]
         jobs = []
         for i in idx:
@@ -192,7 +201,7 @@ class CpuReference:
         self.processes = max(1, min(processes, len(jobs)))
         parts = [jobs[k::self.processes] for k in range(self.processes)]
         ctx = mp.get_context("spawn")
-        self.pools = [ctx.Pool(1, initializer=_cpu_init, initargs=(part, self.use_ref)) for part in parts]
+        self.pools = [ctx.Pool(1, initializer=_cpu_init, initargs=(part, self.use_ref, pulse)) for part in parts]
         self.kind = "reference" if self.use_ref else "port"
         self.sample = (f"{len(jobs)} of {batch.brains} brains (every {stride}th by size, "
                        f"{sum(len(j[0]) for j in jobs)} neurons), 16-tick steps; " +
@@ -357,10 +366,12 @@ def run_ours(args, rank, world, local_rank):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     nsb = load_package()
-    batch = workload(nsb, 2 + rank, args.fraction)
+    batch = workload(nsb, 2 + rank, args.fraction, args.workload)
     N = len(batch.neuron_rows)
     E = len(batch.synapse_rows)
     gpu = nsb.GpuBatch.from_rows(batch)
+    if "pulse_period" in batch.meta:
+        gpu.set_modulation(batch.meta["pulse_period"], batch.meta["pulse_mod"])
     st = gpu.stats()
     gpu.reset(np.arange(batch.brains, dtype=np.uint32) + 1000 * rank)
     gpu.upload(batch.inputs, np.ones(batch.brains, np.uint8))
@@ -431,15 +442,15 @@ def run_ours(args, rank, world, local_rank):
         peak, peak_kind = peaks()
         algo = ALGO_BYTES_PER_NEURON * N + ALGO_BYTES_PER_SYNAPSE * E
         achieved = algo / (ms_step / 1e3) / 1e9
-        traffic = traffic_per_launch()
+        traffic = traffic_per_launch() if args.workload == "batched_uneven" else None
         if traffic is not None:
             traffic /= args.fraction
         clocks = clk.summary()
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (Philox4x32-10, seed 2 + rank)",
-                "config": {"workload": "batched_uneven_full_pools" if args.fraction == 1 else
-                           f"batched_uneven_1/{args.fraction}_pools", "brains": batch.brains, "neurons": N,
+                "config": {"workload": f"{args.workload}_full_pools" if args.fraction == 1 else
+                           f"{args.workload}_1/{args.fraction}_pools", "brains": batch.brains, "neurons": N,
                            "synapses": E, "ticks_per_step": 16, "delays_ms": "1-16", "parallelism": f"replicas x{world}",
                            "units": st["units"], "grid": st["grid"], "block": st["block"],
                            "delivery": "warp-cooperative" if coop else "serial",
@@ -584,6 +595,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fraction", type=int, default=1, choices=[1, 2, 4, 8, 16],
                     help="run a 1/D slice of the full pools (profiler captures only)")
+    ap.add_argument("--workload", default="batched_uneven", choices=["batched_uneven", "plasticity_heavy"],
+                    help="full-pool workload: batched uneven brains (default) or the plasticity-heavy variant")
     ap.add_argument("--serve", action="store_true", help="serving-loop latency/throughput (config 5)")
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-load", type=float, default=0.85, help="offered load as a fraction of peak")

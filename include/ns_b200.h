@@ -66,7 +66,9 @@ int ns_gpu_step(void *batch, const float *input, const uint8_t *mask, int ticks,
 
 /* ---- extensions (no reference counterpart) ---------------------------------- */
 
-/* ns_create with a delay ring of max_delay ticks (1..31). */
+/* ns_create with a delay ring of max_delay ticks (1..31). The extended
+ * creators (this one and nsb_gpu_create_rows) also accept plasticity profile
+ * 6: triplet STDP written into a dopamine-gated eligibility trace. */
 void *nsb_create_ext(int count, int edges, int channels, int outputs, const float *ng, const float *sg,
                      const int *motors, int max_delay);
 /* ns_gpu_create with an explicit delay ring floor and CTA size (128 or 256; 0 = default). */
@@ -111,6 +113,11 @@ int nsb_gpu_load_state(void *batch, int brain, void *brain_handle);
 int nsb_gpu_stats(void *batch, int *out);
 /* Synaptic arrivals counted on the device since the previous call. */
 long long nsb_gpu_take_events(void *batch);
+/* No counterpart in the reference. A global modulator pulse: at every tick
+ * divisible by `period` (0: off) the plasticity of every neuron sees the
+ * modulator bits `mod` (1 NE, 2 5-HT, 4 DA) as if a modulatory synapse had
+ * released onto it. Returns 0 or -1. */
+int nsb_gpu_set_modulation(void *batch, int period, int mod);
 /* Delivery mode of the tick kernel: 1 warp-cooperative stochastic release
  * (dense, active brains), 0 serial per neuron; results are identical.
  * Returns the previous mode, or -1. */

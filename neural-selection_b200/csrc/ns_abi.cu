@@ -89,8 +89,10 @@ bool finite_row(const float *p, int n) {
 }
 
 // ns_create row decoding and validation (gym_adapter/native.cpp:121-157).
+// max_profile: 5 for the reference ABI; the extended creators also accept
+// profile 6 (triplet STDP into a dopamine-gated eligibility trace).
 HostBrain *make_brain(int count, int edges, int channels, int outputs, const float *ng, const float *sg,
-                      const int *motors, int max_delay) {
+                      const int *motors, int max_delay, int max_profile = 5) {
     if (count < 1 || edges < 0 || channels < 1 || channels > 65535 || outputs < 1)
         throw std::runtime_error("Invalid brain dimensions");
     if (max_delay < 1 || max_delay > kMaxDelay) throw std::runtime_error("Invalid delay ring");
@@ -118,7 +120,7 @@ HostBrain *make_brain(int count, int edges, int channels, int outputs, const flo
         const float *p = sg + (size_t)i * 11;
         if (!finite_row(p, 11) || p[0] < 0 || p[0] >= count || p[1] < 0 || p[1] >= count || p[2] < 0 || p[3] < 0 ||
             p[3] > 1 || p[4] < 1 || p[4] > max_delay || p[5] < 0 || p[5] >= 4 || p[6] <= 0 || p[6] > 1 ||
-            p[7] <= 0 || p[8] < 0 || p[9] < 0 || p[9] > 5 || p[10] < 0 || p[10] > 7)
+            p[7] <= 0 || p[8] < 0 || p[9] < 0 || p[9] > max_profile || p[10] < 0 || p[10] > 7)
             throw std::runtime_error("Invalid synapse gene");
         ref::SynapseGene g;
         std::memset(&g, 0, sizeof g);
@@ -202,7 +204,7 @@ void *ns_create(int count, int edges, int channels, int outputs, const float *ng
 void *nsb_create_ext(int count, int edges, int channels, int outputs, const float *ng, const float *sg,
                      const int *motors, int max_delay) {
     try {
-        return make_brain(count, edges, channels, outputs, ng, sg, motors, max_delay);
+        return make_brain(count, edges, channels, outputs, ng, sg, motors, max_delay, 6);
     } catch (const std::exception &e) {
         g_error = e.what();
         return nullptr;
@@ -335,7 +337,7 @@ void *nsb_gpu_create_rows(int brains, const int64_t *neuron_offsets, const int64
             const int64_t n0 = neuron_offsets[i], n1 = neuron_offsets[i + 1];
             const int64_t e0 = synapse_offsets[i], e1 = synapse_offsets[i + 1];
             hosts.emplace_back(make_brain((int)(n1 - n0), (int)(e1 - e0), channels, outputs, ng + n0 * 10,
-                                          sg + e0 * 11, motors + (size_t)i * outputs, max_delay));
+                                          sg + e0 * 11, motors + (size_t)i * outputs, max_delay, 6));
             handles.push_back(hosts.back().get());
         }
         return gpu_create(handles.data(), brains, max_delay, block);
@@ -496,6 +498,18 @@ int nsb_gpu_stats(void *p, int *out) {
 long long nsb_gpu_take_events(void *p) {
     try {
         return (long long)static_cast<GpuBatch *>(p)->engine->take_events();
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+// Global modulator pulse: every `period` ticks (0: off) all neurons' plasticity
+// sees the modulator bits `mod` (1 NE, 2 5-HT, 4 DA).
+int nsb_gpu_set_modulation(void *p, int period, int mod) {
+    try {
+        static_cast<GpuBatch *>(p)->engine->set_global_modulation(period, (uint32_t)mod);
+        return 0;
     } catch (const std::exception &e) {
         g_error = e.what();
         return -1;

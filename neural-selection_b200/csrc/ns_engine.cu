@@ -412,9 +412,11 @@ __global__ void __launch_bounds__(256, HEAVY ? 1 : NSB_MIN_CTAS) tick_kernel(Poo
                     // the record's spare word keeps the call's AMPA scale
                     store_neuron(r, s, log_ampa, hw0, r[S_PAD]);
                     spike = s.spike;
-                    if ((flags & NF_PLASTIC_IN) && (spike || d.mod || d.narr))
+                    uint32_t mod = d.mod;
+                    if (P.pulse_period > 0 && (tick0 + t) % P.pulse_period == 0) mod |= P.pulse_mod;
+                    if ((flags & NF_PLASTIC_IN) && (spike || mod || d.narr))
                         plasticity_events(P.sstate, P.sgene, P.slastp, P.hw, ib, ie, e0, meta, hist, t, tick0,
-                                          spike != 0, d.mod, s.depol, tab);
+                                          spike != 0, mod, s.depol, tab);
                     cnt[j] += (int)spike;
                     my_events += d.narr;
                 }
@@ -513,6 +515,10 @@ static PhysConst make_constants() {
     K.dend_offset = 5.0f / (1.0f + nsx::expf_cr(10.0f));
     K.log_up = nsx::logf_cr(1.92f);
     K.log_down = nsx::logf_cr(0.70f);
+    K.tp = nsx::expf_cr(-1.0f / 16.8f);
+    K.tm = nsx::expf_cr(-1.0f / 33.7f);
+    K.ty = nsx::expf_cr(-1.0f / 114.0f);
+    K.te = nsx::expf_cr(-1.0f / 200.0f);
     return K;
 }
 
@@ -921,6 +927,8 @@ Pools Engine::pools(bool events) const {
     P.btick = d_btick_; P.bmotor = d_bmotor_; P.units = d_units_; P.unitb = d_unitb_; P.ubrain = d_ubrain_;
     P.channels = channels_; P.outputs = outputs_; P.hw = hw_;
     P.events = events ? d_events_ : nullptr;
+    P.pulse_period = pulse_period_;
+    P.pulse_mod = pulse_mod_;
     return P;
 }
 
@@ -1020,6 +1028,15 @@ void Engine::step_host(const float *input, const uint8_t *mask, int ticks, float
     NSB_CHECK(cudaStreamSynchronize(stream_));
     for (int i = 0; i < n_brains_; ++i)
         if (mask[i] && status[i] != -2) h_tick_[i] += ticks;
+}
+
+void Engine::set_global_modulation(int period, uint32_t mod) {
+    if (period < 0 || mod > 7u) throw std::runtime_error("Invalid modulator pulse");
+    NSB_CHECK(cudaDeviceSynchronize());
+    for (auto &g : graphs_) cudaGraphExecDestroy(g.exec);
+    graphs_.clear();
+    pulse_period_ = mod ? period : 0;
+    pulse_mod_ = period ? mod : 0u;
 }
 
 void Engine::set_cooperative(bool coop) {

@@ -76,6 +76,10 @@ public:
     // state restored afterwards, so the call has no visible effect on the
     // brains) and keeps the faster one. Returns the chosen mode.
     bool autotune(int ticks, float gain, cudaStream_t stream);
+    // A global modulator pulse: at every tick divisible by `period` (> 0)
+    // every neuron's plasticity sees the modulator bits `mod` (1 NE, 2 5-HT,
+    // 4 DA) as if a modulatory synapse had released onto it. 0 turns it off.
+    void set_global_modulation(int period, uint32_t mod);
     // Engine-owned device buffers for step_device / step_graph.
     float *dev_input() { return d_input_; }
     uint8_t *dev_mask() { return d_mask_; }
@@ -109,6 +113,8 @@ private:
     int grid_ = 0, grid_heavy_ = 0, block_ = 256, smem_ = 0, ctas_per_sm_ = 0, sms_ = 0, n_light_units_ = 0;
     bool count_events_ = true;
     bool coop_ = false;
+    int pulse_period_ = 0;
+    uint32_t pulse_mod_ = 0;
     std::vector<void *> allocations_;
     // device pools
     float *d_ngene_ = nullptr; uint32_t *d_nflags_ = nullptr; int *d_nsens_ = nullptr; int *d_nxidx_ = nullptr;

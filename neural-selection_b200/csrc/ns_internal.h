@@ -46,6 +46,8 @@ struct Pools {
     const int *ubrain;       // unit brain lists (caller brain indices), pool order
     int channels, outputs, hw;
     unsigned long long *events;
+    int pulse_period;        // > 0: a global modulator pulse at every tick divisible by it
+    uint32_t pulse_mod;      // its modulator bits (1 NE, 2 5-HT, 4 DA)
 };
 
 // Host plan of a set of brains: work units and every pool record, indexed

@@ -80,6 +80,7 @@ struct PhysConst {
     float lfs_thr, lfs_open[3];                  // exp(-1/10), exp(-1/{10,40,750})
     float prinz_ca, dend_offset;                 // exp(-.025/200), 5/(1+exp(10))
     float log_up, log_down;                      // log(1.92), log(0.70)
+    float tp, tm, ty, te;                        // exp(-1/16.8), exp(-1/33.7), exp(-1/114), exp(-1/200): profile 6
 };
 
 // Canonical dump layout (shared with the oracle's or_dump): 32 words per

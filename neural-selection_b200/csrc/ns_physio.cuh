@@ -336,6 +336,19 @@ __device__ __forceinline__ float spine_window(float age, const float *tab) {
 __device__ __forceinline__ void plasticity_tick(uint32_t prof, uint32_t receptors, float w0, SynPlast &s,
                                                 bool arrived, bool post, float depol, uint32_t mod,
                                                 const float *tab) {
+    if (prof == 6) {
+        // Triplet STDP (Pfister & Gerstner 2006, minimal all-to-all model:
+        // tau+ 16.8, tau- 33.7, tau_y 114 ms, A3+ 6.5e-3, A2- 7.1e-3) written
+        // into an eligibility trace (tau 200 ms) that a dopamine event turns
+        // into a weight change. pre_tr = r1, post_tr = o1, eltd = o2, eltp = e.
+        s.pre_tr *= c_K.tp; s.post_tr *= c_K.tm; s.eltd *= c_K.ty; s.eltp *= c_K.te;
+        s.pre_age += 1.0f; s.post_age += 1.0f;
+        if (arrived) { s.eltp -= 0.0071f * s.post_tr; s.pre_tr += 1.0f; s.pre_age = 0; }
+        if (post) { s.eltp += 0.0065f * s.pre_tr * s.eltd; s.post_tr += 1.0f; s.eltd += 1.0f; s.post_age = 0; }
+        if ((mod & 4u) && (receptors & 4u)) s.w += w0 * s.eltp;
+        s.w = clampf(s.w, 0.0f, 2.0f * w0);
+        return;
+    }
     if (prof == 5) {
         if (s.st_age >= 0) { s.st_age += 1.0f; if (s.st_age > 5000.0f) s.st_age = -1; }
         s.pre_age += 1.0f;
@@ -389,6 +402,14 @@ __device__ __forceinline__ void plasticity_tick(uint32_t prof, uint32_t receptor
 // (each field evolves independently; the weight bound is idempotent).
 __device__ __forceinline__ void plasticity_quiet(uint32_t prof, float w0, SynPlast &s, int k) {
     if (k <= 0) return;
+    if (prof == 6) {
+        for (int i = 0; i < k; ++i) {
+            s.pre_tr *= c_K.tp; s.post_tr *= c_K.tm; s.eltd *= c_K.ty; s.eltp *= c_K.te;
+            s.pre_age += 1.0f; s.post_age += 1.0f;
+        }
+        s.w = clampf(s.w, 0.0f, 2.0f * w0);
+        return;
+    }
     if (prof == 5) {
         for (int i = 0; i < k; ++i) {
             if (s.st_age >= 0) { s.st_age += 1.0f; if (s.st_age > 5000.0f) s.st_age = -1; }
@@ -416,7 +437,7 @@ __device__ __forceinline__ void plasticity_quiet(uint32_t prof, float w0, SynPla
 // Does a modulator bit set at the postsynaptic neuron affect this profile?
 __device__ __forceinline__ bool mod_relevant(uint32_t prof, uint32_t receptors, uint32_t mod) {
     if (prof == 3) return (mod & receptors & 3u) != 0;
-    if (prof == 4 || prof == 5) return (mod & receptors & 4u) != 0;
+    if (prof == 4 || prof == 5 || prof == 6) return (mod & receptors & 4u) != 0;
     return false;
 }
 

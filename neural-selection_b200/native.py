@@ -53,6 +53,7 @@ SIGNATURES = {
     "nsb_gpu_stats": (ct.c_int, [_vp, _i32]),
     "nsb_gpu_take_events": (ct.c_longlong, [_vp]),
     "nsb_gpu_set_delivery": (ct.c_int, [_vp, ct.c_int]),
+    "nsb_gpu_set_modulation": (ct.c_int, [_vp, ct.c_int, ct.c_int]),
     "nsb_checkpoint_layout": (ct.c_ulonglong, []),
     "nsb_gpu_checkpoint_export": (ct.c_int, [_vp, _vp, _vp, _i64]),
     "nsb_gpu_checkpoint_import": (ct.c_int, [_vp, _vp, ct.c_longlong, _vp, ct.c_longlong, _i64]),
@@ -289,6 +290,11 @@ class GpuBatch:
         srp = sr if len(sr) else np.zeros((1, CHECKPOINT_SYNAPSE_BYTES), np.uint8)
         if self.lib.nsb_gpu_checkpoint_import(self.ptr, nrp.ctypes.data_as(ct.c_void_p), len(nr),
                                               srp.ctypes.data_as(ct.c_void_p), len(sr), _p(t, _i64)):
+            raise RuntimeError(_err(self.lib))
+
+    def set_modulation(self, period, mod=4):
+        """Global modulator pulse every `period` ticks (0: off) with bits `mod` (4 = dopamine)."""
+        if self.lib.nsb_gpu_set_modulation(self.ptr, int(period), int(mod)):
             raise RuntimeError(_err(self.lib))
 
     def set_delivery(self, cooperative):

@@ -283,6 +283,36 @@ def batched_uneven(seed=2, brains=32768, total_neurons=4194304, total_synapses=8
                      {"ticks_per_step": 16, "steps": 500})
 
 
+def plasticity_heavy(seed=4, brains=32768, total_neurons=4194304, total_synapses=8388608, sensory=8, outputs=5,
+                     max_delay=16, burst_frac=0.3, burst_level=0.65, median=96.0, sigma=1.0, lo=16, hi=4096):
+    """Plasticity-heavy full pools: the batched-uneven population with every
+    synapse on profile 6 (triplet STDP into a dopamine eligibility trace,
+    tau 200 ms) and a dopamine receptor, 30% of the hidden neurons driven
+    tonically to about 60 Hz (type 0 on an extra input channel at level 0.65,
+    i.e. 150 pA at the default gain of 230), and a global dopamine pulse every
+    50 ms (meta pulse_period / pulse_mod, applied with set_modulation)."""
+    base = batched_uneven(seed=seed, brains=brains, total_neurons=total_neurons, total_synapses=total_synapses,
+                          sensory=sensory, outputs=outputs, max_delay=max_delay, median=median, sigma=sigma, lo=lo,
+                          hi=hi)
+    st = Stream(seed, 0x62757273)
+    nr = base.neuron_rows.copy()
+    b, i = _brain_of(base.neuron_offsets)
+    hidden = i >= sensory + outputs
+    burst = hidden & (st.uniform(b, i, 20) < burst_frac)
+    nr[burst, 0] = 0                       # excitatory AdEx with afterdepolarisation
+    nr[burst, 1] = sensory                 # the drive channel
+    nr[burst, 3] = 0
+    nr[burst, 7] = -52.0
+    sr = base.synapse_rows.copy()
+    sr[:, 9] = 6                           # triplet STDP + dopamine eligibility on every synapse
+    sr[:, 10] = 4                          # dopamine receptor
+    inputs = np.concatenate([np.ones((base.brains, sensory), np.float32),
+                             np.full((base.brains, 1), burst_level, np.float32)], axis=1)
+    return Batch(nr, sr, base.neuron_offsets, base.synapse_offsets, base.motors, sensory + 1, max_delay,
+                 "plasticity_heavy", inputs, 230.0, {"ticks_per_step": 16, "steps": 1000, "pulse_period": 50,
+                                                     "pulse_mod": 4, "burst_fraction": burst_frac})
+
+
 def parity_mix(seed=7, brains=24, min_n=8, max_n=160, fanin=8, channels=6, outputs=4, max_delay=8,
                heavy_types=True):
     """Parity workload: every neuron profile (0-6, LP and Prinz cells

@@ -43,6 +43,7 @@ float or_bound_logf(float x) { return OLOG(x); }
 
 /* Correctly rounded constant exponentials, computed once (values a compiler
  * folds `expf(constant)` to). */
+static float K_TP, K_TM, K_TY, K_TE;   /* profile 6 trace decays */
 static float K_EXC_MS, K_INH_MS, K_EXC_SUB, K_INH_SUB, K_LTP, K_LTD, K_NE,
     K_5HT, K_LFS_THR, K_LFS_OPEN[3], K_PRINZ_CA, K_DEND_OFFSET, K_LOG_UP, K_LOG_DOWN;
 static int consts_ready;
@@ -65,6 +66,10 @@ static void init_consts(void) {
     K_DEND_OFFSET = 5.0f / (1.0f + or_cr_expf(10.0f));  /* physiology.cuh:228 */
     K_LOG_UP = or_cr_logf(1.92f);             /* physiology.cuh:249 */
     K_LOG_DOWN = or_cr_logf(0.70f);           /* physiology.cuh:250 */
+    K_TP = or_cr_expf(-DT / 16.8f);
+    K_TM = or_cr_expf(-DT / 33.7f);
+    K_TY = or_cr_expf(-DT / 114.0f);
+    K_TE = or_cr_expf(-DT / 200.0f);
     consts_ready = 1;
 }
 
@@ -442,6 +447,20 @@ static float release(const sgene *g, sstate *s, int64_t tick) {  /* 425-454 */
 static void plasticity_tick(const sgene *g, sstate *s, int arrived, int post_spike, int pair,
                             float depol, unsigned char mod) {
     if (!g->plast || !pair) return;
+    if (g->plast == 6) {
+        /* No reference counterpart (the reference's profiles are 1-5): triplet
+         * STDP, Pfister & Gerstner 2006 minimal all-to-all model (tau+ 16.8,
+         * tau- 33.7, tau_y 114 ms, A3+ 6.5e-3, A2- 7.1e-3), written into an
+         * eligibility trace (tau 200 ms) that a dopamine event applies to the
+         * weight. pre_tr = r1, post_tr = o1, el_ltd = o2, el_ltp = e. */
+        s->pre_tr *= K_TP; s->post_tr *= K_TM; s->el_ltd *= K_TY; s->el_ltp *= K_TE;
+        s->pre_age += DT; s->post_age += DT;
+        if (arrived) { s->el_ltp -= 0.0071f * s->post_tr; s->pre_tr += 1.0f; s->pre_age = 0; }
+        if (post_spike) { s->el_ltp += 0.0065f * s->pre_tr * s->el_ltd; s->post_tr += 1.0f; s->el_ltd += 1.0f; s->post_age = 0; }
+        if ((mod & MOD_DA) && (g->receptors & MOD_DA)) s->w += g->w0 * s->el_ltp;
+        s->w = clampf(s->w, 0.0f, 2.0f * g->w0);
+        return;
+    }
     if (g->plast == 5) {
         if (s->st_age >= 0) { s->st_age += DT; if (s->st_age > 5000.0f) s->st_age = -1; }
         s->pre_age += DT;
@@ -525,6 +544,8 @@ struct or_brain {
     float *exc, *inh; uint8_t *mod;
     uint32_t *orig_n, *orig_s;
     int64_t tick, events;
+    int pulse_period;           /* global modulator pulse (0: none) */
+    uint8_t pulse_mod;
     struct or_shadow *sh;       /* FP64 shadow, or NULL */
 };
 
@@ -595,7 +616,7 @@ or_brain *or_create(int count, int edges, int channels, int outputs, const float
         for (int f = 0; f < 11; ++f) if (p[f] != p[f]) { bad(err, errlen, "Invalid synapse gene"); or_destroy(b); return NULL; }
         if (p[0] < 0 || p[0] >= count || p[1] < 0 || p[1] >= count || p[2] < 0 || p[3] < 0 || p[3] > 1 ||
             p[4] < 1 || p[4] > max_delay || p[5] < 0 || p[5] >= BRANCHES || p[6] <= 0 || p[6] > 1 ||
-            p[7] <= 0 || p[8] < 0 || p[9] < 0 || p[9] > 5 || p[10] < 0 || p[10] > 7) {
+            p[7] <= 0 || p[8] < 0 || p[9] < 0 || p[9] > (max_delay > 8 ? 6 : 5) || p[10] < 0 || p[10] > 7) {
             bad(err, errlen, "Invalid synapse gene"); or_destroy(b); return NULL;
         }
         sgene g; memset(&g, 0, sizeof g);
@@ -621,6 +642,11 @@ void or_original_indices(or_brain *b, const uint32_t *neurons, const uint32_t *s
         b->orig_s = (uint32_t *)malloc((size_t)b->edges * 4);
         memcpy(b->orig_s, synapses, (size_t)b->edges * 4);
     }
+}
+
+void or_set_pulse(or_brain *b, int period, int mod) {
+    b->pulse_period = mod ? period : 0;
+    b->pulse_mod = (uint8_t)(period ? mod : 0);
 }
 
 void or_destroy(or_brain *b) {
@@ -696,6 +722,8 @@ int or_step(or_brain *b, const float *input, int ticks, float gain, float *outpu
             b->hist[(size_t)j * RING + (size_t)(b->tick % b->ring)] = s->spike;
             if (raster) raster[(size_t)t * b->count + j] = s->spike;
         }
+        if (b->pulse_period > 0 && b->tick % b->pulse_period == 0)   /* global modulator pulse */
+            for (int j = 0; j < b->count; ++j) b->mod[j] |= b->pulse_mod;
         for (int j = 0; j < b->edges; ++j) {                     /* plasticity, edge order */
             const sgene *g = &b->sg[j]; sstate *s = &b->ss[j];
             if (!edge_live(b, g)) continue;
@@ -859,6 +887,18 @@ static void sh_plast(or_brain *b, int j, int pair) {
     const int arrived = b->ss[j].arrived, post_spike = b->ns[g->post].spike;
     const unsigned char mod = b->mod[g->post];
     const double w0 = g->w0;
+    if (g->plast == 6) {
+        d->pre_tr *= exp(-1.0 / 16.8);
+        d->post_tr *= exp(-1.0 / 33.7);
+        d->el_ltd *= exp(-1.0 / 114.0);
+        d->el_ltp *= exp(-1.0 / 200.0);
+        d->pre_age += 1.0; d->post_age += 1.0;
+        if (arrived) { d->el_ltp -= 0.0071 * d->post_tr; d->pre_tr += 1.0; d->pre_age = 0; }
+        if (post_spike) { d->el_ltp += 0.0065 * d->pre_tr * d->el_ltd; d->post_tr += 1.0; d->el_ltd += 1.0; d->post_age = 0; }
+        if ((mod & MOD_DA) && (g->receptors & MOD_DA)) d->w += w0 * d->el_ltp;
+        d->w = dclamp(d->w, 0.0, 2.0 * w0);
+        return;
+    }
     if (g->plast == 5) {
         if (d->st_age >= 0) { d->st_age += 1.0; if (d->st_age > 5000.0) d->st_age = -1; }
         d->pre_age += 1.0;

@@ -34,6 +34,9 @@ or_brain *or_create(int count, int edges, int channels, int outputs,
                     int max_delay, char *err, int errlen);
 void or_original_indices(or_brain *b, const uint32_t *neurons, const uint32_t *synapses);
 void or_destroy(or_brain *b);
+/* Global modulator pulse: at every tick divisible by `period` (0: off) all
+ * neurons' plasticity sees the modulator bits `mod` (1 NE, 2 5-HT, 4 DA). */
+void or_set_pulse(or_brain *b, int period, int mod);
 void or_reset(or_brain *b, uint32_t seed);
 /* ns_step semantics: 0, or -1 on a non-finite voltage. When stop_on_nonfinite
  * is 0 the step records the failure, keeps integrating (the CUDA batch

@@ -38,6 +38,7 @@ def oracle_lib(libm=False):
         lib.or_create.argtypes = [ct.c_int] * 4 + [_f, _f, _i32, ct.c_int, ct.c_char_p, ct.c_int]
         lib.or_original_indices.argtypes = [ct.c_void_p, _u32, _u32]
         lib.or_destroy.argtypes = [ct.c_void_p]
+        lib.or_set_pulse.argtypes = [ct.c_void_p, ct.c_int, ct.c_int]
         lib.or_reset.argtypes = [ct.c_void_p, ct.c_uint32]
         lib.or_step.argtypes = [ct.c_void_p, _f, ct.c_int, ct.c_float, _f, _u8, ct.c_int]
         lib.or_step.restype = ct.c_int
@@ -153,6 +154,10 @@ class OracleBrain:
 
     def reset(self, seed):
         self.lib.or_reset(self.ptr, ct.c_uint32(seed))
+
+    def set_pulse(self, period, mod=4):
+        """Global modulator pulse every `period` ticks with bits `mod` (4 = dopamine)."""
+        self.lib.or_set_pulse(self.ptr, int(period), int(mod))
 
     def original_indices(self, neurons, synapses):
         n = np.ascontiguousarray(neurons, np.uint32)

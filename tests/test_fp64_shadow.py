@@ -50,14 +50,17 @@ def _shadow_run(batch, brains, calls=125, ticks=16, seed0=20):
     return worst
 
 
-def _check(worst, label):
+def _check(worst, label, rel=None, v_sub=V_SUB_REL_BOUND, v_abs=V_ABS_BOUND):
     lines = [f"{label}: max abs / max rel error vs FP64 over 2,000 ticks"]
     lines += [f"  {k:18s} {a:.3e} {r:.3e}" for k, (a, r) in worst.items()]
     print("\n".join(lines))
-    for k in BOUNDED_REL:
-        assert worst[k][1] <= REL_BOUND, f"{label}: {k} relative error {worst[k][1]:.3e}"
-    assert worst["V_subthreshold_mV"][1] <= V_SUB_REL_BOUND, f"{label}: V below V_T rel {worst['V_subthreshold_mV'][1]:.3e}"
-    assert worst["V_mV"][0] <= V_ABS_BOUND, f"{label}: V abs error {worst['V_mV'][0]:.3e} mV"
+    bounds = {k: REL_BOUND for k in BOUNDED_REL}
+    bounds.update(rel or {})
+    for k, bound in bounds.items():
+        assert worst[k][1] <= bound, f"{label}: {k} relative error {worst[k][1]:.3e}"
+    assert worst["V_subthreshold_mV"][1] <= v_sub, f"{label}: V below V_T rel {worst['V_subthreshold_mV'][1]:.3e}"
+    if v_abs is not None:
+        assert worst["V_mV"][0] <= v_abs, f"{label}: V abs error {worst['V_mV'][0]:.3e} mV"
 
 
 def test_shadow_does_not_change_binary32(nsb, oracle_built):
@@ -86,6 +89,35 @@ def test_fp64_error_batched_uneven_sample(nsb, oracle_built):
     """Brains drawn like the full-pool workload (delays 1-16, 10-40 Hz drive)."""
     b = nsb.workloads.batched_uneven(brains=48, total_neurons=6144, total_synapses=12288)
     _check(_shadow_run(b, range(0, 48, 3)), "batched uneven sample")
+
+
+def test_fp64_error_plasticity_heavy_sample(nsb, oracle_built):
+    """Profile 6 (triplet STDP into a dopamine eligibility trace) on every
+    synapse, 30% of neurons at ~60 Hz, dopamine pulses every 50 ms."""
+    b = nsb.workloads.plasticity_heavy(brains=48, total_neurons=6144, total_synapses=12288)
+    worst = {}
+    for i in range(0, 48, 6):
+        ng, sg, mo = b.brain(i)
+        o = OracleBrain(ng, sg, mo, b.channels, b.max_delay)
+        o.set_pulse(b.meta["pulse_period"], b.meta["pulse_mod"])
+        o.reset(20 + i)
+        o.enable_shadow()
+        for _ in range(125):
+            o.step(b.inputs[i], 16, b.gain, stop_on_nonfinite=False)
+        st, _ = o.shadow_stats()
+        for k, (a, r) in st.items():
+            A, R = worst.get(k, (0.0, 0.0))
+            worst[k] = (max(A, a), max(R, r))
+        o.close()
+    # Synaptic weights hold 1e-5. The eligibility trace sums potentiation and
+    # depression terms of opposite sign, so its relative error is that of a
+    # difference (bound 1e-3). Neurons firing at 60 Hz spend much of their
+    # time in the exponential upswing, where binary32 and binary64 voltages
+    # part by millivolts until the shared reset; the adaptation current
+    # and the afterdepolarisation current carry part of that below threshold
+    # (bounds 5e-4 and 1e-4); the voltage in the upswing is reported, not
+    # bounded.
+    _check(worst, "plasticity heavy sample", rel={"syn_eligibility": 1e-3, "adp_pA": 1e-4}, v_sub=5e-4, v_abs=None)
 
 
 def test_fp64_shadow_rejects_lp_prinz(nsb, oracle_built):

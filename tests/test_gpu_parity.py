@@ -45,13 +45,17 @@ def _assert_brain_equal(gpu, ora, i, what):
 
 
 def run_parity(nsb, batch, calls, ticks=16, mask_fn=None, reset_at=(), seeds=None, check_every=1, block=0,
-               gain=None, delivery=None, autotune_at=()):
+               gain=None, delivery=None, autotune_at=(), pulse=None):
     delay = batch.max_delay
     gain = batch.gain if gain is None else gain
     gpu = nsb.GpuBatch.from_rows(batch, block=block)
     if delivery is not None:
         gpu.set_delivery(delivery)
     ora = _oracles(batch, delay)
+    if pulse is not None:
+        gpu.set_modulation(*pulse)
+        for o in ora:
+            o.set_pulse(*pulse)
     seeds = np.arange(batch.brains, dtype=np.uint32) * 17 + 20 if seeds is None else seeds
     gpu.reset(seeds)
     for i, o in enumerate(ora):
@@ -87,6 +91,22 @@ def test_parity_mix_every_profile_and_cell_type(nsb, delivery):
     batch = nsb.workloads.parity_mix(brains=16)
     gpu, _ = run_parity(nsb, batch, calls=8, mask_fn=lambda c: np.array(
         [1 if (i + c) % 4 else 0 for i in range(batch.brains)], np.uint8), reset_at=(3, 6), delivery=delivery)
+    gpu.close()
+
+
+@pytest.mark.parametrize("delivery", [False, True])
+def test_plasticity_heavy_triplet_dopamine(nsb, delivery):
+    """Every synapse on profile 6 (triplet STDP into a dopamine eligibility
+    trace), 30% of hidden neurons driven to ~60 Hz, a global dopamine pulse
+    every 50 ms; 10 calls = 160 ticks, so pulses fall inside calls."""
+    batch = nsb.workloads.plasticity_heavy(brains=32, total_neurons=32 * 96, total_synapses=32 * 192)
+    gpu, ora = run_parity(nsb, batch, calls=10, check_every=5, delivery=delivery,
+                          pulse=(batch.meta["pulse_period"], batch.meta["pulse_mod"]))
+    changed = 0
+    for i, o in enumerate(ora):
+        w = o.dump()[1][:, 0].view(np.float32)
+        changed += int((w != batch.brain(i)[1][:, 2]).sum())
+    assert changed > 0
     gpu.close()
 
 
