@@ -366,7 +366,16 @@ def run_ours(args, rank, world, local_rank):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     nsb = load_package()
-    batch = workload(nsb, 2 + rank, args.fraction, args.workload)
+    if args.strong and world > 1:
+        # strong scaling: one population split across the ranks by neurons + synapses
+        full = workload(nsb, 2, args.fraction, args.workload)
+        lo, hi = nsb.sharding.shard_ranges(full.neuron_offsets, full.synapse_offsets, world)[rank]
+        batch = full.subset(range(lo, hi))
+        total_neurons = len(full.neuron_rows)
+        del full
+    else:
+        batch = workload(nsb, 2 + rank, args.fraction, args.workload)
+        total_neurons = world * len(batch.neuron_rows)
     N = len(batch.neuron_rows)
     E = len(batch.synapse_rows)
     gpu = nsb.GpuBatch.from_rows(batch)
@@ -398,13 +407,12 @@ def run_ours(args, rank, world, local_rank):
     ms = e0.elapsed_time(e1)
     events = gpu.take_events()
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = nsb.sharding.max_over_ranks(ms, dist, "cuda")
+        events = nsb.sharding.sum_over_ranks(events, dist, "cuda")
         dist.barrier()
     ms_step = ms / args.steps
-    value = world * N * 16 * args.steps / (ms / 1e3)
-    events_per_s = world * events / (ms / 1e3)
+    value = total_neurons * 16 * args.steps / (ms / 1e3)
+    events_per_s = events / (ms / 1e3)
     launches_per_step = (1 if st["units"] > 0 else 0) + (1 if st.get("heavy", 0) else 0)
 
     # e2e: reference-facing C ABI call with pinned host buffers
@@ -431,10 +439,8 @@ def run_ours(args, rank, world, local_rank):
         abi_step()
     e2e_s = time.perf_counter() - t0
     if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * N * 16 * e2e_steps / e2e_s
+        e2e_s = nsb.sharding.max_over_ranks(e2e_s, dist, "cuda")
+    e2e_value = total_neurons * 16 * e2e_steps / e2e_s
     h2d = batch.inputs.nbytes + batch.brains
     d2h = out.numel() * 4 + stat.numel() * 4
 
@@ -447,11 +453,12 @@ def run_ours(args, rank, world, local_rank):
             traffic /= args.fraction
         clocks = clk.summary()
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True,
+                "scaling": "strong" if args.strong and world > 1 else "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (Philox4x32-10, seed 2 + rank)",
                 "config": {"workload": f"{args.workload}_full_pools" if args.fraction == 1 else
                            f"{args.workload}_1/{args.fraction}_pools", "brains": batch.brains, "neurons": N,
-                           "synapses": E, "ticks_per_step": 16, "delays_ms": "1-16", "parallelism": f"replicas x{world}",
+                           "synapses": E, "ticks_per_step": 16, "delays_ms": "1-16", "parallelism": (f"shards x{world}" if args.strong and world > 1 else f"replicas x{world}"),
                            "units": st["units"], "grid": st["grid"], "block": st["block"],
                            "delivery": "warp-cooperative" if coop else "serial",
                            "l2": f"device state {(120 * N + 108 * E) / 1e9:.2f} GB > 126 MB L2: inputs larger than L2"},
@@ -597,6 +604,8 @@ def main():
                     help="run a 1/D slice of the full pools (profiler captures only)")
     ap.add_argument("--workload", default="batched_uneven", choices=["batched_uneven", "plasticity_heavy"],
                     help="full-pool workload: batched uneven brains (default) or the plasticity-heavy variant")
+    ap.add_argument("--strong", action="store_true",
+                    help="N > 1: split one full-pool population across the ranks (default: one replica per rank)")
     ap.add_argument("--serve", action="store_true", help="serving-loop latency/throughput (config 5)")
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-load", type=float, default=0.85, help="offered load as a fraction of peak")
