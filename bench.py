@@ -132,6 +132,12 @@ def workload(nsb, seed, fraction=1, kind="batched_uneven"):
         return nsb.workloads.plasticity_heavy(seed=seed + 2, brains=32768 // fraction,
                                               total_neurons=4194304 // fraction,
                                               total_synapses=8388608 // fraction)
+    if kind == "serving_population":
+        # the serving genomes (config 5) stepped as one static batch of 5,000
+        # genomes (about 4.1 M neurons, 33 M synapses), every channel at 0.5
+        b = nsb.workloads.serving_library(seed=5 + seed - 2, genomes=5000 // fraction)
+        b.inputs = np.full((b.brains, b.channels), 0.5, np.float32)
+        return b
     tag = "full" if fraction == 1 else f"div{fraction}"
     cache = Path(os.environ.get("NSB_BENCH_CACHE", "/tmp")) / f"nsb_uneven_{tag}_seed{seed}.npz"
     W = nsb.workloads
@@ -602,7 +608,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fraction", type=int, default=1, choices=[1, 2, 4, 8, 16],
                     help="run a 1/D slice of the full pools (profiler captures only)")
-    ap.add_argument("--workload", default="batched_uneven", choices=["batched_uneven", "plasticity_heavy"],
+    ap.add_argument("--workload", default="batched_uneven",
+                    choices=["batched_uneven", "plasticity_heavy", "serving_population"],
                     help="full-pool workload: batched uneven brains (default) or the plasticity-heavy variant")
     ap.add_argument("--strong", action="store_true",
                     help="N > 1: split one full-pool population across the ranks (default: one replica per rank)")
