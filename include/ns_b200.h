@@ -64,6 +64,15 @@ int ns_gpu_reset(void *batch, const uint8_t *mask, const uint32_t *seeds);
 int ns_gpu_step(void *batch, const float *input, const uint8_t *mask, int ticks, float gain, float *output,
                 int *status);
 
+/* gym_adapter/maze_gpu.cu:85-90. Steps the batch on the encoded observations
+ * of a device maze batch made by the reference's maze library (ns_maze_create
+ * in libgym_maze_gpu.so, whose MazeBatch starts {int count; int *grid; void
+ * *objects, *agents; unsigned char *observations; float *encoded, *lookup;
+ * ...}): mask host count, output host count x outputs, status host count.
+ * The batch must have 294 channels (7 x 7 x 3 x 2). Synchronous. */
+int ns_maze_brain_step(void *maze, void *batch, const unsigned char *mask, int ticks, float gain, float *output,
+                       int *status);
+
 /* ---- extensions (no reference counterpart) ---------------------------------- */
 
 /* ns_create with a delay ring of max_delay ticks (1..31). The extended

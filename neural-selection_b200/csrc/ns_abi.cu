@@ -504,6 +504,45 @@ long long nsb_gpu_take_events(void *p) {
     }
 }
 
+// The neural step of the reference's device maze batch
+// (gym_adapter/maze_gpu.cu:85-90): the maze library (built from the
+// reference sources) keeps the MiniGrid batch and its encoded observations on
+// the device; this entry point steps this library's GpuBatch on those
+// observations. Leading fields of the reference's MazeBatch, in its order.
+struct RefMazeBatch {
+    int count;
+    int *grid;
+    void *objects, *agents;
+    unsigned char *observations;
+    float *encoded, *lookup;
+};
+constexpr int kMazeChannels = 7 * 7 * 3 * 2;   // MS*MS*3*2 (gym_adapter/maze_gpu.cu:3)
+
+int ns_maze_brain_step(void *maze, void *brain, const unsigned char *mask, int ticks, float gain, float *output,
+                       int *status) {
+    try {
+        const RefMazeBatch &m = *static_cast<const RefMazeBatch *>(maze);
+        GpuBatch &g = *static_cast<GpuBatch *>(brain);
+        Engine &e = *g.engine;
+        if (e.brains() != m.count || e.channels() != kMazeChannels)
+            throw std::runtime_error("Maze/brain dimensions differ");
+        if (ticks < 1 || ticks > 10000 || !std::isfinite(gain) || gain < 0)
+            throw std::runtime_error("Invalid neural integration interval");
+        if (cudaMemcpy(e.dev_mask(), mask, (size_t)e.brains(), cudaMemcpyHostToDevice) != cudaSuccess)
+            throw std::runtime_error("CUDA: mask upload failed");
+        e.step_device(m.encoded, e.dev_mask(), ticks, gain, e.dev_output(), e.dev_status(), nullptr);
+        if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("CUDA: step failed");
+        if (cudaMemcpy(output, e.dev_output(), (size_t)e.brains() * e.outputs() * sizeof(float),
+                       cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(status, e.dev_status(), (size_t)e.brains() * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+            throw std::runtime_error("CUDA: output download failed");
+        return 0;
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
 // Global modulator pulse: every `period` ticks (0: off) all neurons' plasticity
 // sees the modulator bits `mod` (1 NE, 2 5-HT, 4 DA).
 int nsb_gpu_set_modulation(void *p, int period, int mod) {

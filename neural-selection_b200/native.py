@@ -38,6 +38,7 @@ SIGNATURES = {
     "ns_gpu_destroy": (None, [_vp]),
     "ns_gpu_reset": (ct.c_int, [_vp, _u8, _u32]),
     "ns_gpu_step": (ct.c_int, [_vp, _f, _u8, ct.c_int, ct.c_float, _f, _i32]),
+    "ns_maze_brain_step": (ct.c_int, [_vp, _vp, _u8, ct.c_int, ct.c_float, _f, _i32]),
     "nsb_create_ext": (_vp, [ct.c_int] * 4 + [_f, _f, _i32, ct.c_int]),
     "nsb_gpu_create_ext": (_vp, [ct.POINTER(_vp), ct.c_int, ct.c_int, ct.c_int]),
     "nsb_gpu_create_rows": (_vp, [ct.c_int, _i64, _i64, _f, _f, _i32, ct.c_int, ct.c_int, ct.c_int, ct.c_int]),

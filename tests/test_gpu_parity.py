@@ -214,3 +214,46 @@ def test_graph_replay_matches_host_step(nsb):
     for i in range(8):
         np.testing.assert_array_equal(a.dump(i)[0], b.dump(i)[0])
         np.testing.assert_array_equal(a.dump(i)[1], b.dump(i)[1])
+
+
+def test_maze_brain_step_matches_gpu_step(nsb):
+    """ns_maze_brain_step (gym_adapter/maze_gpu.cu:85-90) steps the batch on a
+    device maze batch's encoded observations; the reference's MazeBatch is
+    mirrored here by its leading fields. Same results as ns_gpu_step on the
+    same observations."""
+    import ctypes as ct
+    import torch
+    batch = nsb.workloads.parity_mix(brains=6, channels=294, heavy_types=False)
+    a = nsb.GpuBatch.from_rows(batch)
+    b = nsb.GpuBatch.from_rows(batch)
+    seeds = np.arange(6, dtype=np.uint32) + 3
+    a.reset(seeds); b.reset(seeds)
+    rng = np.random.default_rng(1)
+
+    class Maze(ct.Structure):
+        _fields_ = [("count", ct.c_int), ("grid", ct.c_void_p), ("objects", ct.c_void_p), ("agents", ct.c_void_p),
+                    ("observations", ct.c_void_p), ("encoded", ct.c_void_p), ("lookup", ct.c_void_p)]
+    lib = nsb.native.library()
+    for c in range(4):
+        x = rng.uniform(0, 1, (6, 294)).astype(np.float32)
+        mask = np.array([1, 1, 0, 1, 1, 1], np.uint8)
+        enc = torch.from_numpy(x).cuda()
+        torch.cuda.synchronize()
+        maze = Maze(6, None, None, None, None, enc.data_ptr(), None)
+        out = np.zeros((6, batch.outputs), np.float32)
+        status = np.zeros(6, np.int32)
+        rc = lib.ns_maze_brain_step(ct.byref(maze), a.ptr, mask.ctypes.data_as(ct.POINTER(ct.c_uint8)), 16, 230.0,
+                                    out.ctypes.data_as(ct.POINTER(ct.c_float)),
+                                    status.ctypes.data_as(ct.POINTER(ct.c_int32)))
+        assert rc == 0, lib.ns_error().decode()
+        ob, sb = b.step(x, mask, 16, 230.0)
+        np.testing.assert_array_equal(out, ob)
+        np.testing.assert_array_equal(status, sb)
+    for i in range(6):
+        np.testing.assert_array_equal(a.dump(i)[0], b.dump(i)[0])
+    bad = Maze(5, None, None, None, None, enc.data_ptr(), None)
+    assert lib.ns_maze_brain_step(ct.byref(bad), a.ptr, mask.ctypes.data_as(ct.POINTER(ct.c_uint8)), 16, 230.0,
+                                  out.ctypes.data_as(ct.POINTER(ct.c_float)),
+                                  status.ctypes.data_as(ct.POINTER(ct.c_int32))) == -1
+    assert lib.ns_error().decode() == "Maze/brain dimensions differ"
+    a.close(); b.close()
