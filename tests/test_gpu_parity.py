@@ -257,3 +257,63 @@ def test_maze_brain_step_matches_gpu_step(nsb):
                                   status.ctypes.data_as(ct.POINTER(ct.c_int32))) == -1
     assert lib.ns_error().decode() == "Maze/brain dimensions differ"
     a.close(); b.close()
+
+
+def test_handles_from_the_reference_library(nsb):
+    """ns_gpu_create accepts Brain handles made by the reference's own host
+    library (gym_adapter/native.cpp built from its sources, exp/log correctly
+    rounded): the batch then steps bit-identically to those brains stepped on
+    the reference host executor."""
+    import ctypes as ct
+    from oracle.pyoracle import RefBrain, ref_lib
+    if ref_lib(cr=True) is None:
+        pytest.skip("reference host build (oracle/_ref) absent")
+    batch = nsb.workloads.parity_mix(brains=6, heavy_types=True)
+    makers = [RefBrain(*batch.brain(i), batch.channels, cr=True) for i in range(6)]
+    lib = nsb.native.library()
+    arr = (ct.c_void_p * 6)(*[m.ptr for m in makers])
+    ptr = lib.ns_gpu_create(arr, 6)
+    assert ptr, lib.ns_error().decode()
+    gpu = nsb.GpuBatch(ptr, 6, batch.channels, batch.outputs,
+                       [(len(batch.brain(i)[0]), len(batch.brain(i)[1])) for i in range(6)])
+    for m in makers:                     # the batch deep-copied the genomes
+        m.close()
+    seeds = np.arange(6, dtype=np.uint32) + 11
+    gpu.reset(seeds)
+    refs = [RefBrain(*batch.brain(i), batch.channels, cr=True) for i in range(6)]
+    for i, r in enumerate(refs):
+        r.reset(int(seeds[i]))
+    for c in range(5):
+        out, status = gpu.step(batch.inputs, None, 16, batch.gain)
+        for i, r in enumerate(refs):
+            rc, ro, _ = r.step(batch.inputs[i], 16, batch.gain)
+            assert status[i] == rc
+            np.testing.assert_array_equal(out[i], ro)
+    for i, r in enumerate(refs):
+        gn, gs, gt = gpu.dump(i)
+        rn, rs, rt = r.dump()
+        assert gt == rt
+        assert (_nan_equivalent(gn, rn, _INT_WORDS)).all()
+        np.testing.assert_array_equal(gs, rs)
+    gpu.close()
+
+
+def test_edge_sizes(nsb):
+    """A one-neuron brain without synapses, a brain without synapses, and a
+    brain at the maximum size (16,384 neurons), in one batch."""
+    W = nsb.workloads
+    big = W.batched_uneven(seed=9, brains=1, total_neurons=16384, total_synapses=32768, lo=16, hi=16384)
+    tiny_n = np.array([[5, 0, 1, 0, 0, 1, 1, -40, 30, 2]], np.float32)
+    lone_n = np.array([[0, -1, 1, 0, 0, 1, 1, -52, 0, 0], [5, 1, 1, 0, 0, 1, 1, -40, 20, 2],
+                       [1, -1, 1, 1, 0, 1, 1, -42, 0, 0]], np.float32)
+    ch = big.channels
+    rows_n = np.concatenate([tiny_n, lone_n, big.neuron_rows])
+    rows_s = big.synapse_rows
+    no = np.array([0, 1, 4, 4 + len(big.neuron_rows)])
+    so = np.array([0, 0, 0, len(rows_s)])
+    motors = np.array([[0] * big.outputs, [0] * big.outputs, list(big.motors[0])], np.int32)
+    inputs = np.ones((3, ch), np.float32)
+    batch = W.Batch(rows_n, rows_s, no, so, motors, ch, big.max_delay, "edge_sizes", inputs, 230.0, {})
+    gpu, _ = run_parity(nsb, batch, calls=3)
+    assert gpu.stats()["max_unit_neurons"] == 16384
+    gpu.close()
