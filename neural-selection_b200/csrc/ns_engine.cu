@@ -29,6 +29,8 @@
 #include "ns_engine.h"
 #include "ns_internal.h"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -469,6 +471,183 @@ __global__ void __launch_bounds__(256, HEAVY ? 1 : NSB_MIN_CTAS) tick_kernel(Poo
     }
 }
 
+// ---- big brains: one brain per thread-block cluster -------------------------------
+// A brain above the CTA unit size is stepped by a cluster of C CTAs (C = 2, 4
+// or 8, from the launch). CTA rank r owns the brain's neurons [r*per,
+// min(nn, (r+1)*per)) with per a multiple of 32, so every spike-ring word has
+// one owner; each CTA caches the synapse meta words of its own neurons in
+// shared memory and keeps a full copy of the brain's spike ring, to which the
+// owner of each word writes its ballots (its own copy and, through
+// distributed shared memory, every other rank's). One cluster barrier per
+// tick replaces the CTA barrier of tick_kernel: tick t+1 reads only ring
+// slots of earlier ticks, which the barrier has made visible everywhere.
+// Every rank takes the same number of cluster barriers: the unit index comes
+// from rank 0 through distributed shared memory, and the mask, tick and tick
+// count that decide the work are the same values for every rank.
+template <bool COOP>
+__global__ void __launch_bounds__(256, NSB_MIN_CTAS) tick_kernel_cluster(Pools P, int unit_begin, int unit_end,
+                                                                         int *queue, const float *__restrict__ input,
+                                                                         const uint8_t *__restrict__ mask,
+                                                                         float *__restrict__ output,
+                                                                         int *__restrict__ status, int ticks,
+                                                                         float gain) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int C = (int)cluster.num_blocks();
+    const int rank = (int)cluster.block_rank();
+    float *tab = reinterpret_cast<float *>(g_smem);                      // 2^(j/128) hi/lo pairs
+    uint32_t *s_meta = reinterpret_cast<uint32_t *>(g_smem + 1024);       // kMetaCap
+    uint32_t *hist = s_meta + kMetaCap;                                   // 32 * hw
+    int *cnt = reinterpret_cast<int *>(hist + 32 * P.hw);                // 32 * hw (own neurons' spike counts)
+    int *s_ev = cnt + 32 * P.hw;                                          // 8 warps x kEvCap
+    uint32_t *s_evv = reinterpret_cast<uint32_t *>(s_ev + 8 * kEvCap);
+    __shared__ int s_unit;
+    __shared__ unsigned long long s_events;
+
+    const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    {
+        const float *src = nsx::exp2f_table();
+        for (int i = tid; i < 256; i += bs) tab[i] = src[i];
+    }
+    for (;;) {
+        if (tid == 0) {
+            if (rank == 0) s_unit = unit_begin + atomicAdd(queue, 1);
+            s_events = 0;
+        }
+        cluster.sync();
+        const int u = *cluster.map_shared_rank(&s_unit, 0);
+        cluster.sync();                                  // rank 0's s_unit is read before it changes
+        if (u >= unit_end) break;
+        const int4 U = P.units[u];
+        const int n0 = U.x, nn = U.y;
+        const int b = P.ubrain[P.unitb[u].x];           // a big unit holds one brain
+        const int64_t tick0 = P.btick[b];
+        const bool in_range = tick0 + (int64_t)ticks < 2147483647ll;
+        const bool run = mask[b] && in_range;
+        if (rank == 0 && tid == 0) status[b] = in_range ? 0 : -2;
+        if (!run) {
+            if (rank == 0)
+                for (int i = tid; i < P.outputs; i += bs) output[(size_t)b * P.outputs + i] = 0.0f;
+            continue;
+        }
+        const int per = (((nn + C - 1) / C) + 31) & ~31;
+        const int lo = min(nn, rank * per), hi = min(nn, lo + per);
+        const int e0 = P.inptr[n0 + lo], e1 = P.inptr[n0 + hi];
+        const bool meta_smem = e1 - e0 <= kMetaCap;
+        if (meta_smem)
+            for (int k = tid; k < e1 - e0; k += bs) s_meta[k] = P.smeta[e0 + k];
+        const uint32_t *meta = meta_smem ? s_meta : P.smeta + e0;
+        const int slots = (hi - lo + bs - 1) / bs;
+        int my_events = 0;
+        for (int sl0 = 0; sl0 < slots; ++sl0) {
+            const int j = lo + sl0 * bs + tid;
+            const bool has = j < hi;
+            uint32_t h0 = 0;
+            if (has) {
+                uint32_t *r = P.nstate + (size_t)(n0 + j) * S_WORDS;
+                h0 = r[S_HIST];
+                r[S_PAD] = __float_as_uint(crexp(__uint_as_float(r[S_LOGAMPA]), tab));
+            }
+            const uint32_t rot = has ? rotr32(h0, (uint32_t)(tick0 & 31)) : 0u;
+            const int word = (lo >> 5) + sl0 * (bs >> 5) + warp;
+            const bool word_in = lo + sl0 * bs + warp * 32 < hi;
+            for (int sl = 0; sl < 32; ++sl) {
+                const uint32_t w = __ballot_sync(0xffffffffu, (rot >> sl) & 1u);
+                if (lane == 0 && word_in)
+                    for (int q = 0; q < C; ++q) *cluster.map_shared_rank(hist + sl * P.hw + word, q) = w;
+            }
+            if (has) cnt[j - lo] = 0;
+        }
+        cluster.sync();
+        for (int t = 0; t < ticks; ++t) {
+            for (int sl0 = 0; sl0 < slots; ++sl0) {
+                const int j = lo + sl0 * bs + tid;
+                const int n = n0 + j;
+                const bool has = j < hi;
+                const uint32_t flags = has ? P.nflags[n] : 0u;
+                uint32_t spike = 0;
+                int ib = 0, ie = 0;
+                float ampa = 0.0f;
+                if (has) {
+                    ib = P.inptr[n];
+                    ie = P.inptr[n + 1];
+                    ampa = __uint_as_float(P.nstate[(size_t)n * S_WORDS + S_PAD]);
+                }
+                const bool dlv = has && (flags & NF_ACTIVE);
+                Delivered d = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0u, 0};
+                if (COOP)
+                    d = deliver_warp(P, dlv ? ib : 0, dlv ? ie : 0, e0, meta, hist, t, tick0, ampa, tab,
+                                     s_ev + warp * kEvCap, s_evv + warp * kEvCap, lane);
+                else if (dlv)
+                    d = deliver(P, ib, ie, e0, meta, hist, t, tick0, ampa, tab);
+                if (has) {
+                    uint32_t *r = P.nstate + (size_t)n * S_WORDS;
+                    NeuronRegs s;
+                    float log_ampa;
+                    uint32_t hw0;
+                    load_neuron(r, s, log_ampa, hw0);
+                    if (flags & NF_ACTIVE) {
+                        const float level =
+                            (flags & NF_HAS_INPUT) ? input[(size_t)b * P.channels + P.nsens[n]] : 0.0f;
+                        integrate<false>(P, n, flags, d, level, gain, s, status + b, tab);
+                    } else {
+                        s.spike = 0;
+                    }
+                    store_neuron(r, s, log_ampa, hw0, r[S_PAD]);
+                    spike = s.spike;
+                    uint32_t mod = d.mod;
+                    if (P.pulse_period > 0 && (tick0 + t) % P.pulse_period == 0) mod |= P.pulse_mod;
+                    if ((flags & NF_PLASTIC_IN) && (spike || mod || d.narr))
+                        plasticity_events(P.sstate, P.sgene, P.slastp, P.hw, ib, ie, e0, meta, hist, t, tick0,
+                                          spike != 0, mod, s.depol, tab);
+                    cnt[j - lo] += (int)spike;
+                    my_events += d.narr;
+                }
+                const uint32_t w = __ballot_sync(0xffffffffu, spike);
+                const int word = (lo >> 5) + sl0 * (bs >> 5) + warp;
+                if (lane == 0 && lo + sl0 * bs + warp * 32 < hi)
+                    for (int q = 0; q < C; ++q) *cluster.map_shared_rank(hist + (t & 31) * P.hw + word, q) = w;
+            }
+            cluster.sync();
+        }
+        for (int sl0 = 0; sl0 < slots; ++sl0) {
+            const int j = lo + sl0 * bs + tid;
+            if (j >= hi) continue;
+            const int n = n0 + j;
+            const uint32_t flags = P.nflags[n];
+            uint32_t *r = P.nstate + (size_t)n * S_WORDS;
+            float la = __uint_as_float(r[S_LOGAMPA]);
+            if (flags & NF_ACTIVE) {
+                const int total = (int)r[S_TOTAL];
+                const int64_t t1 = tick0 + ticks;
+                la = homeostasis(flags & NF_TYPE_MASK, la, (float)ticks,
+                                 (float)total * 1000.0f / (float)(ticks > t1 ? (int64_t)ticks : t1));
+            }
+            uint32_t L = 0;
+            const int word = j >> 5;
+            for (int sl = 0; sl < 32; ++sl) L |= ((hist[sl * P.hw + word] >> lane) & 1u) << sl;
+            r[S_LOGAMPA] = __float_as_uint(la);
+            r[S_HIST] = rotl32(L, (uint32_t)(tick0 & 31));
+            r[S_PAD] = 0u;
+            finish_synapses(P, P.inptr[n], P.inptr[n + 1], e0, meta, hist, ticks, tick0);
+        }
+        __syncthreads();
+        for (int k = tid; k < P.outputs; k += bs) {
+            const int m = P.bmotor[(size_t)b * P.outputs + k] - n0;
+            if (m >= lo && m < hi) output[(size_t)b * P.outputs + k] = (float)cnt[m - lo];
+        }
+        if (rank == 0 && tid == 0) P.btick[b] = tick0 + ticks;
+        if (P.events) {
+            unsigned long long v = (unsigned long long)my_events;
+            for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (lane == 0 && v) atomicAdd(&s_events, v);
+            __syncthreads();
+            if (tid == 0 && s_events) atomicAdd(P.events, s_events);
+        }
+        cluster.sync();                                  // ring copies are free for the next unit
+    }
+}
+
 // ---- reset (gym_adapter/gpu.cu:18-23 with physiology.cuh:179-202, 393-404) --------
 __global__ void reset_neurons(Pools P, const int *nbrain, const uint32_t *norig, const uint8_t *mask,
                               const uint32_t *seeds, int n_neurons) {
@@ -532,10 +711,67 @@ int tick_smem_bytes(int hw) {
     return 1024 + (kMetaCap + 32 * hw * 2) * 4 + kMaxUnitBrains * 8 + 2 * kMaxUnitBrains * 4 + 8 * kEvCap * 8;
 }
 
-static void set_tick_smem(int smem) {
-    NSB_CHECK(cudaFuncSetAttribute(tick_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    NSB_CHECK(cudaFuncSetAttribute(tick_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    NSB_CHECK(cudaFuncSetAttribute(tick_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+// The kernels' dynamic shared memory limit is a process-wide attribute: it is
+// set to the device's opt-in maximum, so that engines of different shapes in
+// one process never lower it under one another's launches.
+template <class K> static void allow_dynamic_smem(K kernel, int optin) {
+    cudaFuncAttributes fa;
+    NSB_CHECK(cudaFuncGetAttributes(&fa, kernel));
+    NSB_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   optin - (int)fa.sharedSizeBytes));
+}
+
+static void set_tick_smem(int) {
+    int dev = 0, optin = 0;
+    NSB_CHECK(cudaGetDevice(&dev));
+    NSB_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    allow_dynamic_smem(tick_kernel<false, false>, optin);
+    allow_dynamic_smem(tick_kernel<false, true>, optin);
+    allow_dynamic_smem(tick_kernel<true, false>, optin);
+    allow_dynamic_smem(tick_kernel_cluster<false>, optin);
+    allow_dynamic_smem(tick_kernel_cluster<true>, optin);
+}
+
+// Dynamic shared memory of the cluster kernel for hw ring words.
+static int cluster_smem_bytes(int hw) { return 1024 + (kMetaCap + 64 * hw) * 4 + 8 * kEvCap * 8; }
+
+static cudaLaunchConfig_t cluster_config(int C, int clusters, int block, int smem, cudaStream_t s,
+                                         cudaLaunchAttribute *attr) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(C * clusters), 1, 1);
+    cfg.blockDim = dim3((unsigned)block, 1, 1);
+    cfg.dynamicSmemBytes = (size_t)smem;
+    cfg.stream = s;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+// Co-resident clusters of C CTAs (the smaller of the two delivery modes).
+static int cluster_capacity(int C, int block, int smem) {
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = cluster_config(C, 1, block, smem, nullptr, attr);
+    int a = 0, b = 0;
+    NSB_CHECK(cudaOccupancyMaxActiveClusters(&a, tick_kernel_cluster<false>, &cfg));
+    NSB_CHECK(cudaOccupancyMaxActiveClusters(&b, tick_kernel_cluster<true>, &cfg));
+    return std::max(1, std::min(a, b));
+}
+
+static void launch_cluster(bool coop, int C, int clusters, int block, int smem, cudaStream_t s, const Pools &P,
+                           int ub, int ue, int *queue, const float *input, const uint8_t *mask, float *output,
+                           int *status, int ticks, float gain) {
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = cluster_config(C, clusters, block, smem, s, attr);
+    if (coop)
+        NSB_CHECK(cudaLaunchKernelEx(&cfg, tick_kernel_cluster<true>, P, ub, ue, queue, input, mask, output, status,
+                                     ticks, gain));
+    else
+        NSB_CHECK(cudaLaunchKernelEx(&cfg, tick_kernel_cluster<false>, P, ub, ue, queue, input, mask, output, status,
+                                     ticks, gain));
 }
 
 // Light units in either delivery mode (serial per lane, or warp-cooperative).
@@ -579,7 +815,8 @@ template <class T> T *Engine::alloc(size_t n) {
 
 static bool excitatory_type(unsigned char t) { return t == 0 || t == 4 || t == 5; }
 
-Plan make_plan(const std::vector<BrainSpec> &brains, int channels, int outputs, int max_delay, int unit_cap) {
+Plan make_plan(const std::vector<BrainSpec> &brains, int channels, int outputs, int max_delay, int unit_cap,
+               bool cluster_big) {
     Plan p;
     const int n_brains = (int)brains.size();
     // ---- validate and size ----
@@ -639,16 +876,32 @@ Plan make_plan(const std::vector<BrainSpec> &brains, int channels, int outputs, 
             }
         }
     }
-    // queue order: light units then heavy units, each by neuron count descending
+    // Queue order: light units stepped by clusters of 8, 4 and 2 CTAs (one
+    // brain above the CTA unit size each), light units of one CTA, heavy
+    // units; by neuron count descending within each group.
+    auto group_of = [&](int u) {
+        if (unit_heavy[u]) return 4;
+        if (!cluster_big || unit_fill[u] <= unit_cap) return 3;
+        if (unit_fill[u] <= 2 * unit_cap) return 2;
+        if (unit_fill[u] <= 4 * unit_cap) return 1;
+        return 0;
+    };
     std::vector<int> uorder(unit_brains.size());
     std::iota(uorder.begin(), uorder.end(), 0);
     std::stable_sort(uorder.begin(), uorder.end(), [&](int a, int b) {
-        if (unit_heavy[a] != unit_heavy[b]) return unit_heavy[a] < unit_heavy[b];
+        const int ga = group_of(a), gb = group_of(b);
+        if (ga != gb) return ga < gb;
         return unit_fill[a] > unit_fill[b];
     });
     p.n_units = (int)unit_brains.size();
     p.n_light_units = 0;
-    for (int u : uorder) p.n_light_units += unit_heavy[u] ? 0 : 1;
+    for (int u : uorder) {
+        const int g = group_of(u);
+        p.n_light_units += g < 4 ? 1 : 0;
+        if (g < 3) ++p.n_cluster[g];
+        int &mx = g < 3 ? p.max_big : (g == 3 ? p.max_small : p.max_heavy);
+        mx = std::max(mx, unit_fill[u]);
+    }
 
     // ---- per-brain bookkeeping (caller order) ----
     auto &h_noff_ = p.noff, &h_soff_ = p.soff, &h_npos_ = p.npos, &h_spos_ = p.spos, &h_bunit_ = p.bunit;
@@ -834,7 +1087,12 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
     channels_ = channels; outputs_ = outputs; max_delay_ = cfg.max_delay; block_ = cfg.block;
     count_events_ = cfg.count_events;
     unit_cap_ = block_ * std::max(1, cfg.unit_slots);
-    Plan p = make_plan(brains, channels, outputs, max_delay_, unit_cap_);
+    int dev0 = 0, sms0 = 0;
+    NSB_CHECK(cudaGetDevice(&dev0));
+    NSB_CHECK(cudaDeviceGetAttribute(&sms0, cudaDevAttrMultiProcessorCount, dev0));
+    Plan p = make_plan(brains, channels, outputs, max_delay_, unit_cap_, cfg.cluster_big == 1);
+    if (cfg.cluster_big < 0 && p.n_big_units > 0 && p.n_light_units < sms0 * NSB_MIN_CTAS)
+        p = make_plan(brains, channels, outputs, max_delay_, unit_cap_, true);
     n_neurons_ = p.n_neurons; n_synapses_ = p.n_synapses; n_units_ = p.n_units; n_light_units_ = p.n_light_units;
     n_big_units_ = p.n_big_units; n_heavy_ = p.n_heavy; max_unit_neurons_ = p.max_unit_neurons;
     max_unit_brains_ = p.max_unit_brains;
@@ -847,6 +1105,10 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
     const auto &unitb = p.unitb;
     const auto &brain_order = p.brain_order;
     hw_ = spike_words(max_unit_neurons_, block_);
+    for (int g = 0; g < 3; ++g) n_cluster_[g] = p.n_cluster[g];
+    hw_small_ = spike_words(p.max_small, block_);
+    hw_big_ = spike_words(p.max_big, block_);
+    hw_heavy_ = spike_words(p.max_heavy, block_);
     coop_ = n_synapses_ >= 4ll * n_neurons_;
 
     // ---- device allocation and upload ----
@@ -877,7 +1139,7 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
     d_ubrain_ = alloc<int>(n_brains_); up(d_ubrain_, brain_order);
     d_units_ = alloc<int4>(n_units_); up(d_units_, h_units_);
     d_unitb_ = alloc<int2>(n_units_); up(d_unitb_, unitb);
-    d_queue_ = alloc<int>(2);
+    d_queue_ = alloc<int>(8);
     d_events_ = alloc<unsigned long long>(1); NSB_CHECK(cudaMemset(d_events_, 0, 8));
     d_input_ = alloc<float>((size_t)n_brains_ * channels);
     NSB_CHECK(cudaMemset(d_input_, 0, (size_t)n_brains_ * channels * 4));
@@ -893,16 +1155,22 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
     h_tick_.assign(n_brains_, 0);
 
     // ---- launch shape ----
-    smem_ = tick_smem_bytes(hw_);
+    smem_ = tick_smem_bytes(hw_small_);
+    smem_big_ = cluster_smem_bytes(hw_big_);
+    smem_heavy_ = tick_smem_bytes(hw_heavy_);
     set_tick_smem(smem_);
     int dev = 0;
     NSB_CHECK(cudaGetDevice(&dev));
     NSB_CHECK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
     const int occ = tick_occupancy(block_, smem_);
     ctas_per_sm_ = cfg.ctas_per_sm > 0 ? std::min(cfg.ctas_per_sm, std::max(occ, 1)) : std::max(occ, 1);
-    grid_ = std::min(std::max(n_light_units_, 1), sms_ * ctas_per_sm_);
+    const int n_big = n_cluster_[0] + n_cluster_[1] + n_cluster_[2];
+    grid_ = std::min(std::max(n_light_units_ - n_big, 1), sms_ * ctas_per_sm_);
+    for (int g = 0; g < 3; ++g)
+        if (n_cluster_[g])
+            clusters_[g] = std::min(n_cluster_[g], cluster_capacity(kClusterSizes[g], block_, smem_big_));
     int occh = 0;
-    NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occh, tick_kernel<true, false>, block_, smem_));
+    NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occh, tick_kernel<true, false>, block_, smem_heavy_));
     grid_heavy_ = std::min(std::max(n_units_ - n_light_units_, 1), sms_ * std::max(occh, 1));
     K_ = make_constants();
     NSB_CHECK(cudaMemcpyToSymbol(c_K, &K_, sizeof(PhysConst)));
@@ -925,25 +1193,47 @@ Pools Engine::pools(bool events) const {
     P.nxidx = d_nxidx_; P.xgene = d_xgene_; P.xstate = d_xstate_; P.nstate = d_nstate_; P.inptr = d_inptr_;
     P.smeta = d_smeta_; P.sgene = d_sgene_; P.sstate = d_sstate_; P.sarrived = d_sarrived_; P.slastp = d_slastp_;
     P.btick = d_btick_; P.bmotor = d_bmotor_; P.units = d_units_; P.unitb = d_unitb_; P.ubrain = d_ubrain_;
-    P.channels = channels_; P.outputs = outputs_; P.hw = hw_;
+    P.channels = channels_; P.outputs = outputs_; P.hw = hw_small_;
     P.events = events ? d_events_ : nullptr;
     P.pulse_period = pulse_period_;
     P.pulse_mod = pulse_mod_;
     return P;
 }
 
+// Every unit group of a step, in queue order: big brains by clusters of 8, 4
+// and 2 CTAs, light units of one CTA, heavy units. queue: 8 zeroed counters.
+void Engine::launch_groups(const Pools &P0, int *queue, const float *d_input, const uint8_t *d_mask, int ticks,
+                           float gain, float *d_output, int *d_status, cudaStream_t stream) {
+    NSB_CHECK(cudaMemsetAsync(queue, 0, 8 * sizeof(int), stream));
+    int ub = 0;
+    for (int g = 0; g < 3; ++g) {
+        if (n_cluster_[g]) {
+            Pools P = P0;
+            P.hw = hw_big_;
+            launch_cluster(coop_, kClusterSizes[g], clusters_[g], block_, smem_big_, stream, P, ub, ub + n_cluster_[g],
+                           queue + 2 + g, d_input, d_mask, d_output, d_status, ticks, gain);
+        }
+        ub += n_cluster_[g];
+    }
+    if (n_light_units_ > ub) {
+        Pools P = P0;
+        P.hw = hw_small_;
+        launch_light(coop_, grid_, block_, smem_, stream, P, ub, n_light_units_, queue, d_input, d_mask, d_output,
+                     d_status, ticks, gain);
+    }
+    if (n_units_ > n_light_units_) {
+        Pools P = P0;
+        P.hw = hw_heavy_;
+        tick_kernel<true, false><<<grid_heavy_, block_, smem_heavy_, stream>>>(P, n_light_units_, n_units_, queue + 1,
+                                                                                d_input, d_mask, d_output, d_status,
+                                                                                ticks, gain);
+    }
+    NSB_CHECK(cudaGetLastError());
+}
+
 void Engine::launch(const float *d_input, const uint8_t *d_mask, int ticks, float gain, float *d_output,
                     int *d_status, cudaStream_t stream) {
-    const Pools P = pools(count_events_);
-    NSB_CHECK(cudaMemsetAsync(d_queue_, 0, 2 * sizeof(int), stream));
-    if (n_light_units_ > 0)
-        launch_light(coop_, grid_, block_, smem_, stream, P, 0, n_light_units_, d_queue_, d_input, d_mask, d_output,
-                     d_status, ticks, gain);
-    if (n_units_ > n_light_units_)
-        tick_kernel<true, false><<<grid_heavy_, block_, smem_, stream>>>(P, n_light_units_, n_units_, d_queue_ + 1,
-                                                                          d_input, d_mask, d_output, d_status, ticks,
-                                                                          gain);
-    NSB_CHECK(cudaGetLastError());
+    launch_groups(pools(count_events_), d_queue_, d_input, d_mask, ticks, gain, d_output, d_status, stream);
 }
 
 // ---- allocation-free step ----------------------------------------------------
@@ -989,19 +1279,14 @@ void Engine::step_noalloc(const float *d_input, const uint8_t *d_mask, int ticks
     int *queue = reinterpret_cast<int *>(scratch);
     int16_t *lastp = reinterpret_cast<int16_t *>(scratch + 256);
     cudaStream_t s = stream ? stream : stream_;
-    // The array keeps the previous call's contents: reset the queue counters
-    // to 0 and the plasticity bookkeeping to -1 ("none this call").
-    NSB_CHECK(cudaMemsetAsync(queue, 0, 2 * sizeof(int), s));
+    // The array keeps the previous call's contents: the plasticity
+    // bookkeeping is reset to -1 ("none this call") here, the queue counters
+    // to 0 by launch_groups.
+    // (launch_groups clears its eight queue counters at the start of the array.)
     NSB_CHECK(cudaMemsetAsync(lastp, 0xff, sizeof(int16_t) * (size_t)std::max(n_synapses_, 1), s));
     Pools P = pools(false);
     P.slastp = lastp;
-    if (n_light_units_ > 0)
-        launch_light(coop_, grid_, block_, smem_, s, P, 0, n_light_units_, queue, d_input, d_mask, d_output, d_status,
-                     ticks, gain);
-    if (n_units_ > n_light_units_)
-        tick_kernel<true, false><<<grid_heavy_, block_, smem_, s>>>(P, n_light_units_, n_units_, queue + 1, d_input,
-                                                                     d_mask, d_output, d_status, ticks, gain);
-    NSB_CHECK(cudaGetLastError());
+    launch_groups(P, queue, d_input, d_mask, ticks, gain, d_output, d_status, s);
 }
 
 void Engine::step_device(const float *d_input, const uint8_t *d_mask, int ticks, float gain, float *d_output,

@@ -31,6 +31,11 @@ struct EngineConfig {
     int ctas_per_sm = 0;        // 0: from occupancy
     int unit_slots = 3;         // small brains are packed into units of block * unit_slots neurons
     bool count_events = true;   // count synaptic arrivals on the device
+    // Brains above the unit size on thread-block clusters: 1 always, 0 never,
+    // -1 when the batch has too few units to fill the GPU (a latency mode: a
+    // big brain spread over up to 8 SMs; in full batches the one-CTA path
+    // has the higher throughput).
+    int cluster_big = -1;
 };
 
 struct Stats {
@@ -104,6 +109,8 @@ public:
 private:
     void launch(const float *d_input, const uint8_t *d_mask, int ticks, float gain, float *d_output,
                 int *d_status, cudaStream_t stream);
+    void launch_groups(const Pools &P, int *queue, const float *d_input, const uint8_t *d_mask, int ticks, float gain,
+                       float *d_output, int *d_status, cudaStream_t stream);
     template <class T> T *alloc(size_t n);
     struct Pools pools(bool events) const;
 
@@ -111,6 +118,9 @@ private:
     int n_neurons_ = 0, n_synapses_ = 0, n_heavy_ = 0, n_units_ = 0, n_big_units_ = 0;
     int max_unit_neurons_ = 0, hw_ = 0, meta_cap_ = 0, max_unit_brains_ = 0, unit_cap_ = 256;
     int grid_ = 0, grid_heavy_ = 0, block_ = 256, smem_ = 0, ctas_per_sm_ = 0, sms_ = 0, n_light_units_ = 0;
+    // big brains stepped by clusters of 8, 4, 2 CTAs (units first in queue order)
+    int n_cluster_[3] = {0, 0, 0}, clusters_[3] = {0, 0, 0};
+    int hw_small_ = 8, hw_big_ = 8, hw_heavy_ = 8, smem_big_ = 0, smem_heavy_ = 0;
     bool count_events_ = true;
     bool coop_ = false;
     int pulse_period_ = 0;

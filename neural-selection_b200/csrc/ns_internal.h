@@ -55,6 +55,11 @@ struct Pools {
 struct Plan {
     int n_neurons = 0, n_synapses = 0, n_units = 0, n_light_units = 0, n_big_units = 0, n_heavy = 0;
     int max_unit_neurons = 0, max_unit_brains = 0;
+    // Light units stepped by thread-block clusters of 8, 4 and 2 CTAs (big
+    // brains), first in queue order, then the light units of one CTA; the
+    // largest unit of each group.
+    int n_cluster[3] = {0, 0, 0};
+    int max_small = 0, max_big = 0, max_heavy = 0;
     std::vector<int4> units;              // {n0, nn, e0, ne}, light units first, each by size descending
     std::vector<int2> unitb;              // {first entry in brain_order, nb}
     std::vector<int> brain_order;         // unit brain lists (caller indices)
@@ -75,7 +80,10 @@ struct Plan {
 // a larger brain is a unit of its own; brains with LP/Prinz/LFS cells in
 // separate, heavy units) and lays out their records. Throws
 // std::runtime_error on invalid input with the reference's messages.
-Plan make_plan(const std::vector<BrainSpec> &brains, int channels, int outputs, int max_delay, int unit_cap);
+Plan make_plan(const std::vector<BrainSpec> &brains, int channels, int outputs, int max_delay, int unit_cap,
+               bool cluster_big = false);
+// Cluster sizes of the three big-brain groups, in queue order.
+constexpr int kClusterSizes[3] = {8, 4, 2};
 
 // Spike-ring words per tick for units of up to max_unit_neurons neurons.
 int spike_words(int max_unit_neurons, int block);

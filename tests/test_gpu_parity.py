@@ -317,3 +317,38 @@ def test_edge_sizes(nsb):
     gpu, _ = run_parity(nsb, batch, calls=3)
     assert gpu.stats()["max_unit_neurons"] == 16384
     gpu.close()
+
+
+def _concat(batches, name):
+    """One Batch of all brains of `batches`, in order."""
+    rows_n = np.concatenate([b.neuron_rows for b in batches])
+    rows_s = np.concatenate([b.synapse_rows for b in batches])
+    no, so = [0], [0]
+    for b in batches:
+        no.extend((no[-1] + np.asarray(b.neuron_offsets[1:]) - b.neuron_offsets[0]).tolist())
+        so.extend((so[-1] + np.asarray(b.synapse_offsets[1:]) - b.synapse_offsets[0]).tolist())
+    no, so = np.asarray(no, np.int64), np.asarray(so, np.int64)
+    motors = np.concatenate([b.motors for b in batches]).astype(np.int32)
+    inputs = np.concatenate([b.inputs for b in batches]).astype(np.float32)
+    b0 = batches[0]
+    return type(b0)(rows_n, rows_s, no, so, motors, b0.channels, b0.max_delay, name, inputs, b0.gain, {})
+
+
+@pytest.mark.parametrize("delivery,cluster", [(False, "1"), (True, "1"), (True, "0")])
+def test_big_brains_on_thread_block_clusters(nsb, monkeypatch, delivery, cluster):
+    """Brains above the 768-neuron unit are stepped by clusters of 2, 4 and 8
+    CTAs exchanging spikes through distributed shared memory (and, with
+    NSB_CLUSTER=0, by one CTA each): sizes 1,000
+    (2 CTAs), 2,000 (4), 3,500 and 6,500 (8, with 832 neurons per CTA), with
+    pair STDP on every excitatory pair, next to small brains, under masks and
+    partial resets."""
+    W = nsb.workloads
+    parts = [W.batched_uneven(seed=20 + k, brains=1, total_neurons=n, total_synapses=3 * n, lo=16, hi=16384,
+                              plastic_all=True) for k, n in enumerate([1000, 2000, 3500, 6500])]
+    parts.append(W.batched_uneven(seed=30, brains=6, total_neurons=6 * 120, total_synapses=6 * 300, plastic_all=True))
+    batch = _concat(parts, "big_brains")
+    monkeypatch.setenv("NSB_CLUSTER", cluster)     # "0": the same brains on one CTA each
+    gpu, _ = run_parity(nsb, batch, calls=6, check_every=2, delivery=delivery, reset_at=(3,),
+                        mask_fn=lambda c: np.array([1 if (i + c) % 5 else 0 for i in range(batch.brains)], np.uint8))
+    assert gpu.stats()["big_units"] == 4
+    gpu.close()
