@@ -116,6 +116,15 @@ def test_autotune_leaves_state_untouched(nsb):
     gpu.close()
 
 
+def test_plain_small_config_bitexact(nsb):
+    """The plain-small configuration as specified: 64 brains x 48 neurons, 600
+    synapses each, 200 world steps x 16 ticks = 3,200 ticks; outputs and
+    status every step, full state every 50 steps."""
+    batch = nsb.workloads.plain_small()
+    gpu, ora = run_parity(nsb, batch, calls=200, check_every=50)
+    gpu.close()
+
+
 def test_plain_small_2000_ticks_bitexact(nsb):
     batch = nsb.workloads.plain_small(brains=16)
     gpu, ora = run_parity(nsb, batch, calls=125, check_every=25)
