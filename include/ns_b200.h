@@ -135,6 +135,16 @@ int nsb_gpu_set_delivery(void *batch, int cooperative);
  * (state restored afterwards) and keeps the faster; returns it, or -1. */
 int nsb_gpu_autotune(void *batch, int ticks, float gain, void *stream);
 
+/* ---- World pool slots (src/main.cu:364-390). The reference claims neuron and
+ * synapse slots with an atomic first-free-bit search from a hint word; these
+ * replay the claims one after another, so the slots depend only on the
+ * bitmap and the hints. d_used: device bitmap of `capacity` bits. */
+/* slots[i] = the slot claimed for hints[i] (search from word hints[i] % words,
+ * lowest free bit first), or -1. Host arrays; synchronous. */
+int nsb_pool_claim(uint32_t *d_used, int capacity, const int *hints, int count, int *slots);
+/* Clears the bits of slots[0..count) (negative entries ignored). */
+int nsb_pool_release(uint32_t *d_used, const int *slots, int count);
+
 /* ---- Checkpoint records. The world simulator saves the neural pools as
  * CheckpointNeuron (344 B) and CheckpointSynapse (136 B) records, one per
  * occupied slot in ascending slot order (src/main.cu:164-264, packed by

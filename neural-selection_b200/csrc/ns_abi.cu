@@ -188,6 +188,10 @@ struct GpuBatch {
 
 }  // namespace
 
+namespace nsb {
+void set_error(const char *message) { g_error = message; }
+}  // namespace nsb
+
 extern "C" {
 
 const char *ns_error() { return g_error.c_str(); }

@@ -55,6 +55,8 @@ SIGNATURES = {
     "nsb_gpu_take_events": (ct.c_longlong, [_vp]),
     "nsb_gpu_set_delivery": (ct.c_int, [_vp, ct.c_int]),
     "nsb_gpu_set_modulation": (ct.c_int, [_vp, ct.c_int, ct.c_int]),
+    "nsb_pool_claim": (ct.c_int, [_vp, ct.c_int, _i32, ct.c_int, _i32]),
+    "nsb_pool_release": (ct.c_int, [_vp, _i32, ct.c_int]),
     "nsb_checkpoint_layout": (ct.c_ulonglong, []),
     "nsb_gpu_checkpoint_export": (ct.c_int, [_vp, _vp, _vp, _i64]),
     "nsb_gpu_checkpoint_import": (ct.c_int, [_vp, _vp, ct.c_longlong, _vp, ct.c_longlong, _i64]),

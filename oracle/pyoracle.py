@@ -132,6 +132,8 @@ def ref_world_lib():
         lib.ref_world_destroy.argtypes = [ct.c_void_p]
         lib.ref_world_layout.argtypes = [ct.POINTER(ct.c_uint64), ct.POINTER(ct.c_uint64), ct.POINTER(ct.c_uint64)]
         lib.ref_world_layout.restype = ct.c_int
+        lib.ref_world_claim_sequential.argtypes = [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int, ct.c_void_p]
+        lib.ref_world_claim_sequential.restype = ct.c_int
         _libs[name] = lib
     return _libs[name]
 

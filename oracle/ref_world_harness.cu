@@ -249,6 +249,17 @@ void ref_world_destroy(void *p) {
     delete w;
 }
 
+// The reference's slot allocator (src/main.cu:364-385) replayed on one
+// thread: claims for hints[0..count) in order on the device bitmap `used`.
+__global__ void ref_claim_kernel(uint32_t *used, int capacity, const int *hints, int count, int *slots) {
+    if (threadIdx.x || blockIdx.x) return;
+    for (int i = 0; i < count; ++i) slots[i] = claim_slot(used, capacity, hints[i]);
+}
+int ref_world_claim_sequential(uint32_t *d_used, int capacity, const int *d_hints, int count, int *d_slots) {
+    ref_claim_kernel<<<1, 1>>>(d_used, capacity, d_hints, count, d_slots);
+    return (int)cudaDeviceSynchronize();
+}
+
 // Layout facts of the reference build: the 20 values its checkpoint layout
 // hash covers (src/checkpoint_impl.cuh:20-32), the hash, and the offsets of
 // the neural checkpoint records (src/main.cu:164-177).
