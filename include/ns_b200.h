@@ -145,6 +145,65 @@ int nsb_pool_claim(uint32_t *d_used, int capacity, const int *hints, int count, 
 /* Clears the bits of slots[0..count) (negative entries ignored). */
 int nsb_pool_release(uint32_t *d_used, const int *slots, int count);
 
+/* ---- World neural stage. Replaces the neural part of the world simulator's
+ * step loop (src/main.cu:2634-2728: slot selection, the 16 ticks of
+ * synapse_delivery / synapse_plasticity_delivery / neuron_step /
+ * synapse_plasticity, or the brain_block_step tiers) and its homeostasis
+ * launches (src/main.cu:2751-2758), operating in place on the simulator's own
+ * device pools (struct Device, src/main.cu:105-140) in the reference record
+ * layouts: Animal 472 B, PlasticityCohort 80 B, NeuronGene 124 B,
+ * NeuronState 120 B, SynapseGene 40 B, SynapseState 80 B. Pointers are device
+ * pointers; capacities are the build's P, NEURON_CAPACITY and
+ * SYNAPSE_CAPACITY (spike_history is indexed [tick % 9][neuron_capacity]).
+ * World semantics (src/main.cu:659-801, 1122-1136, 1287-1300): only animals
+ * with alive == 1 step; an edge delivers only when active, its endpoints
+ * active and owned by the edge's animal; sensory neurons read
+ * senses[animal][channel], through receptor events for type 5 on channels
+ * below 6 and as channel level x 230 pA otherwise (silence flags zero them);
+ * spikes of neurons with port 19..23 add to motors[animal][port - 19];
+ * frozen plasticity cohorts skip plasticity and homeostasis; the traced
+ * animal's motor neurons feed the trace counters. Per post-synaptic branch the
+ * synaptic input is summed in the order of the animal's synapse list. */
+typedef struct NsbWorldPools {
+    const void *animals;            /* Animal[animal_capacity] */
+    const void *plasticity_cohort;  /* PlasticityCohort[animal_capacity] or NULL */
+    const void *neurons;            /* NeuronGene[neuron_capacity] */
+    const void *synapses;           /* SynapseGene[synapse_capacity] */
+    void *neuron_state;             /* NeuronState[neuron_capacity] */
+    void *synapse_state;            /* SynapseState[synapse_capacity] */
+    float *pending_exc;             /* [neuron_capacity][4] */
+    float *pending_inh;             /* [neuron_capacity] */
+    const float *senses;            /* [animal_capacity][19] */
+    unsigned long long *mod_event_tick; /* [neuron_capacity][6] */
+    unsigned char *spike_history;   /* [9][neuron_capacity] */
+    const int *neuron_owner, *synapse_owner, *neuron_next, *synapse_next, *neuron_port;
+    int *motors;                    /* [animal_capacity][5] */
+    int *trace_exc_arrivals, *trace_exc_releases, *trace_inh_arrivals;  /* [5] each */
+    float *trace_exc_ns, *trace_inh_ns, *trace_peak_mv;                 /* [5] each */
+    int trace_animal;               /* animal slot, or -1 */
+    int silence_senses, silence_contact;
+    int animal_capacity, neuron_capacity, synapse_capacity;
+} NsbWorldPools;
+/* A world stage over the given pools (copied; the pools stay the caller's).
+ * max_brain_neurons / max_brain_synapses bound one animal's brain (0: 4096 /
+ * 65536). NULL on invalid arguments. */
+void *nsb_world_create(const NsbWorldPools *pools, int max_brain_neurons, int max_brain_synapses);
+void nsb_world_destroy(void *world);
+/* The 16 ticks of world step `step` (ticks (step - 1) * 16 ... + 15) for
+ * every living animal, on the legacy default stream; returns 0, or -1 when an
+ * animal's lists disagree with its counts or exceed the maxima (ns_error()). */
+int nsb_world_neural_step(void *world, int64_t step);
+/* Homeostatic AMPA scaling after the world's body step: every active neuron
+ * of a living, unfrozen animal, elapsed max(16, age x 16) ms. */
+int nsb_world_homeostasis(void *world);
+/* Work of the last neural step: out[0] animals stepped, [1] neurons,
+ * [2] synapses, [3] synaptic events (arrivals). */
+int nsb_world_stats(void *world, long long *out);
+/* Layout facts the stage relies on: sizes of Animal, PlasticityCohort and the
+ * offsets of Animal.id, .age, .alive, .neuron_head, .synapse_head,
+ * .neuron_count, .synapse_count and PlasticityCohort.frozen (10 values). */
+int nsb_world_layout(uint64_t *out);
+
 /* ---- Checkpoint records. The world simulator saves the neural pools as
  * CheckpointNeuron (344 B) and CheckpointSynapse (136 B) records, one per
  * occupied slot in ascending slot order (src/main.cu:164-264, packed by

@@ -7,6 +7,6 @@ call on sm_100a, behind the reference's own C ABI (include/ns_b200.h).
 `native` binds that ABI; `serve` runs genome-evaluation episodes with
 continuous batching; `workloads` builds seeded synthetic populations.
 """
-from . import sharding, workloads  # noqa: F401
+from . import sharding, workloads, world  # noqa: F401
 from .native import Brain, GpuBatch, library  # noqa: F401
 from .serve import Server  # noqa: F401

@@ -14,9 +14,10 @@ from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
+INCLUDE = PKG.parent / "include"
 LIB = PKG / "libns_b200.so"
 SOURCES = sorted(CSRC.glob("*.cu"))
-HEADERS = sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")))
+HEADERS = sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h")))
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -29,7 +30,7 @@ def nvcc():
 
 def flags(extra=()):
     return ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-ffp-contract=off",
-            "-I", str(CSRC), *extra]
+            "-I", str(CSRC), "-I", str(INCLUDE), *extra]
 
 
 def build(force=False, verbose=False, ptxas_info=False):

@@ -36,7 +36,7 @@
 
 #if defined(__CUDACC__)
 #define NSX_HD __host__ __device__ __forceinline__
-#define NSX_COLD __host__ __device__ __noinline__
+#define NSX_COLD static __host__ __device__ __noinline__
 #else
 #define NSX_HD static inline
 #define NSX_COLD static

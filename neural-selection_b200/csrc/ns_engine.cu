@@ -676,7 +676,7 @@ __global__ void reset_ticks(int64_t *btick, const uint8_t *mask, int n) {
 }
 
 // ---- host side ------------------------------------------------------------------
-static PhysConst make_constants() {
+PhysConst make_constants() {
     PhysConst K;
     K.exc_ms = nsx::expf_cr(-1.0f / 3.0f);
     K.inh_ms = nsx::expf_cr(-1.0f / 10.0f);

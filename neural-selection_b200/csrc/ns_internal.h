@@ -85,6 +85,9 @@ Plan make_plan(const std::vector<BrainSpec> &brains, int channels, int outputs, 
 // Cluster sizes of the three big-brain groups, in queue order.
 constexpr int kClusterSizes[3] = {8, 4, 2};
 
+// Correctly rounded constant exponentials of the physiology (host side).
+PhysConst make_constants();
+
 // Spike-ring words per tick for units of up to max_unit_neurons neurons.
 int spike_words(int max_unit_neurons, int block);
 // Dynamic shared memory of the tick kernel for hw ring words.

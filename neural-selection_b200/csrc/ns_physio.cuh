@@ -105,7 +105,7 @@ __device__ __forceinline__ void adex_tick(const float *g, uint32_t type, uint32_
 }
 
 // ---- LFS cell (physiology.cuh:258-287); x = {v, thr, act[3], open[3]} -------------
-__device__ __noinline__ void lfs_tick(const float *g, NeuronRegs &s, float *x, float cur, float exc, float inh) {
+static __device__ __noinline__ void lfs_tick(const float *g, NeuronRegs &s, float *x, float cur, float exc, float inh) {
     const float wt[3] = {250.0f, 10.0f, 4.0f}, op[3] = {10.0f, 40.0f, 750.0f}, cl[3] = {50.0f, 750.0f, 2000.0f};
     x[1] = g[G_VT] + (x[1] - g[G_VT]) * c_K.lfs_thr;
     float under = 0;
@@ -131,7 +131,7 @@ __device__ __forceinline__ float lp_sig(float v, float mid, float slope, const f
     return 1.0f / (1.0f + crexp((v - mid) / slope, tab));
 }
 __device__ __forceinline__ float lp_ratio(float num, float den, float lim) { return fabsf(den) < 1e-5f ? lim : num / den; }
-__device__ __noinline__ void lp_rates(const float *x, float i_na, const float *sc, float *d, const float *tab) {
+static __device__ __noinline__ void lp_rates(const float *x, float i_na, const float *sc, float *d, const float *tab) {
     const float va = x[0], vs = x[15];
     const float na = x[1] * x[1] * x[1] * x[2] * 7.15f * (va - 50.0f);
     const float kd = x[8] * x[8] * x[8] * x[8] * 1.43f * (va + 72.0f);
@@ -173,7 +173,7 @@ __device__ __noinline__ void lp_rates(const float *x, float i_na, const float *s
     d[14] = (lp_sig(va, -26.9916223f, -5.957441281f, tab) - x[14]) * .0001386796618f *
             lp_sig(va, -60.57875745f, -13.25674673f, tab);
 }
-__device__ __noinline__ void lp_integrate(float *x, float i_na, const float *sc, const float *tab) {
+static __device__ __noinline__ void lp_integrate(float *x, float i_na, const float *sc, const float *tab) {
     const float dt = .05f;
     float k1[16], k2[16], k3[16], k4[16], y[16];
     for (int step = 0; step < 20; ++step) {
@@ -195,7 +195,7 @@ __device__ __forceinline__ float pz_gate(float v, float a, float b, const float 
 __device__ __forceinline__ float pz_gate2(float v, float a, float b, float c, float d, const float *tab) {
     return 1.0f / (crexp((v + a) / b, tab) + crexp((v + c) / d, tab));
 }
-__device__ __noinline__ void pz_substep(float *u, const float *g, float ext, float clamp_ns, float clamp_rev,
+static __device__ __noinline__ void pz_substep(float *u, const float *g, float ext, float clamp_ns, float clamp_rev,
                                         const float *tab) {
     const float dt = .025f;
     float *m = u + 2, *h = u + 9;
@@ -230,7 +230,7 @@ __device__ __noinline__ void pz_substep(float *u, const float *g, float ext, flo
 }
 
 // Heavy cell types (2 LP, 3 Prinz, 6 LFS) on their extended state x (16 floats).
-__device__ __noinline__ NeuronRegs heavy_tick(const float *g, uint32_t type, const float *xg, float *x, NeuronRegs s,
+static __device__ __noinline__ NeuronRegs heavy_tick(const float *g, uint32_t type, const float *xg, float *x, NeuronRegs s,
                                         float cur, float e0, float e1, float e2, float e3, float inh_in,
                                         const float *tab) {
     const float clamp_leak = 0.0f, clamp_rev = -68.0f;
@@ -277,13 +277,17 @@ __device__ __forceinline__ float homeostasis(uint32_t type, float log_ampa, floa
 
 // ---- synapse -----------------------------------------------------------------------
 // Release (physiology.cuh:425-454) on a synapse state record in registers.
-struct SynRelease {
+// L: type of the last-arrival tick (int in the batch pools, int64_t in the
+// world simulator's SynapseState records).
+template <class L> struct SynReleaseT {
     float w, ru, slow;
     uint64_t ready;
     uint32_t rng;
-    int last;
+    L last;
 };
-__device__ __forceinline__ float release(const float *y, SynRelease &s, int64_t tick, const float *tab) {
+using SynRelease = SynReleaseT<int>;
+template <class L>
+__device__ __forceinline__ float release(const float *y, SynReleaseT<L> &s, int64_t tick, const float *tab) {
     float p_rec = 0;
     if (s.last > -1000000) {
         float dt = (float)(tick - (int64_t)s.last) * 1.0f;
@@ -309,7 +313,7 @@ __device__ __forceinline__ float release(const float *y, SynRelease &s, int64_t 
         }
     }
     s.rng = rng; s.ready = ready;
-    s.last = (int)tick;
+    s.last = (L)tick;
     float out = s.w * (float)released / (float)n * s.slow;
     if (y[Y_SLOWREC] > 0) s.slow *= 1.0f - y[Y_SLOWDEPL];
     return out;

@@ -110,6 +110,32 @@ constexpr uint64_t layout_hash() {
 }
 static_assert(layout_hash() == 0x2b1cd1c766eebf82ull, "checkpoint layout hash");
 
+// World simulator records the neural stage reads (src/main.cu:71-100). Only
+// the members named here are read; the rest is carried as opaque bytes of the
+// same size (Behavior: 69 four-byte counters, src/main.cu:71-79).
+struct Animal {
+    float x, y, heading, energy, health, fullness, pain;
+    float taste[4];
+    float muscle[3];
+    unsigned long long rng;
+    int id, parent_id, generation, age, alive;
+    int neuron_head, synapse_head, neuron_count, synapse_count;
+    int ports[19 + 5];
+    int behavior[69];
+};
+struct PlasticityCohort {                // src/main.cu:96-104
+    int id, assigned, frozen, initial_age, initial_offspring;
+    int final_age, final_offspring, alive, death_cause;
+    int neurons, synapses, generation;
+    float initial_energy, initial_health;
+    int64_t start_step, observed_step, death_step;
+};
+static_assert(sizeof(Animal) == 472 && offsetof(Animal, id) == 64 && offsetof(Animal, age) == 76 &&
+              offsetof(Animal, alive) == 80 && offsetof(Animal, neuron_head) == 84 &&
+              offsetof(Animal, synapse_count) == 96, "Animal layout");
+static_assert(sizeof(PlasticityCohort) == 80 && offsetof(PlasticityCohort, frozen) == 8 &&
+              offsetof(PlasticityCohort, start_step) == 56, "PlasticityCohort layout");
+
 static_assert(sizeof(NeuronGene) == 124, "NeuronGene layout");
 static_assert(offsetof(NeuronGene, type) == 44 && offsetof(NeuronGene, lp) == 48, "NeuronGene layout");
 static_assert(offsetof(NeuronGene, sensory_channel) == 100 && offsetof(NeuronGene, rec_base) == 104, "NeuronGene layout");

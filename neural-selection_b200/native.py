@@ -61,6 +61,12 @@ SIGNATURES = {
     "nsb_gpu_checkpoint_export": (ct.c_int, [_vp, _vp, _vp, _i64]),
     "nsb_gpu_checkpoint_import": (ct.c_int, [_vp, _vp, ct.c_longlong, _vp, ct.c_longlong, _i64]),
     "nsb_gpu_autotune": (ct.c_int, [_vp, ct.c_int, ct.c_float, _vp]),
+    "nsb_world_create": (_vp, [_vp, ct.c_int, ct.c_int]),
+    "nsb_world_destroy": (None, [_vp]),
+    "nsb_world_neural_step": (ct.c_int, [_vp, ct.c_int64]),
+    "nsb_world_homeostasis": (ct.c_int, [_vp]),
+    "nsb_world_stats": (ct.c_int, [_vp, ct.POINTER(ct.c_longlong)]),
+    "nsb_world_layout": (ct.c_int, [ct.POINTER(ct.c_uint64)]),
     "nsb_serve_create": (_vp, [ct.c_longlong, ct.c_double, ct.c_double, ct.c_int, ct.c_int, ct.c_int, ct.c_float,
                                ct.c_double]),
     "nsb_serve_destroy": (None, [_vp]),

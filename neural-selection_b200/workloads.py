@@ -437,3 +437,89 @@ def serving_schedule(seed, rate, seconds, genomes, lo_steps=200, hi_steps=2000, 
             "seed": st.bits(idx, 0, 2)[:, 0].astype(np.uint32),
             "steps": st.integers(idx, 0, 3, lo_steps, hi_steps + 1).astype(np.int32),
             "tag": idx.astype(np.uint64)}
+
+
+def world_founders(seed=2, founders=2048, lo=32, hi=96, epn_lo=4, epn_hi=12, heavy_types=False):
+    """Founder brains of the world workload (config 2): `founders` animals of
+    N ~ U{lo..hi} neurons and N x U{epn_lo..epn_hi} synapses. Ports follow the
+    world simulator's layout (src/main.cu:36-42, 544-591): neurons 0-18 are
+    sensory on world channels 0-18 (type 5 receptor cells on the chemical
+    channels 0-5, type 4 relays on 6-18), neurons 19-23 the five motor
+    neurons (type 0), the rest hidden: type 0, 20% type 1 inhibitory, 5%
+    modulatory (NE / 5-HT / DA), and with heavy_types some LP, Prinz and LFS
+    cells. Synapses: pre uniform over all neurons, post uniform over
+    non-sensory neurons, weight U(1, 18) nS, delay 1-8 ms, branch 0-3,
+    facilitating or depressing release (src/main.cu:498-517), plasticity
+    profile 0-5 and modulator receptor mask 0-7 uniform. inputs: the world
+    senses, U(0, 1) per animal and channel."""
+    st = Stream(seed, 0x776f726c)
+    fi = np.arange(founders)
+    sizes = st.integers(fi, 0, 0, lo, hi + 1)
+    sizes = np.maximum(sizes, 25)
+    edges = sizes * st.integers(fi, 0, 1, epn_lo, epn_hi + 1)
+    channels, outputs = 19, 5
+
+    def nfn(no):
+        b, i = _brain_of(no)
+        rows = np.zeros((len(b), 10))
+        u = st.uniform(b, i, 1)
+        hidden = i >= channels + outputs
+        prof = np.where(i < 6, 5, np.where(i < channels, 4, 0))
+        inhib = hidden & (u < 0.2)
+        prof = np.where(inhib, 1, prof)
+        if heavy_types:
+            h = st.uniform(b, i, 2)
+            prof = np.where(hidden & ~inhib & (h < 0.03), 2, prof)
+            prof = np.where(hidden & ~inhib & (h >= 0.03) & (h < 0.06), 3, prof)
+            prof = np.where(hidden & ~inhib & (h >= 0.06) & (h < 0.09), 6, prof)
+        mod = np.where(hidden & ~inhib & (u >= 0.2) & (u < 0.25), st.integers(b, i, 3, 1, 4), 0)
+        rows[:, 0] = prof
+        rows[:, 1] = np.where(i < channels, i, -1)
+        rows[:, 2] = 1
+        rows[:, 3] = inhib
+        rows[:, 4] = mod
+        rows[:, 5] = 0.8 + 0.4 * st.uniform(b, i, 4)
+        rows[:, 6] = 0.8 + 0.4 * st.uniform(b, i, 5)
+        rows[:, 7] = [THRESHOLD[int(p)] for p in prof]
+        rows[:, 8] = np.where(prof == 5, 40.0 + 40.0 * st.uniform(b, i, 6), 0.0)
+        rows[:, 9] = np.where(prof == 5, 2.0, 0.0)
+        return rows
+
+    def sfn(no, so):
+        b, e = _brain_of(so)
+        n = no[b + 1] - no[b]
+        rows = np.zeros((len(b), 11))
+        rows[:, 0] = st.integers(b, e, 10, 0, n)
+        rows[:, 1] = st.integers(b, e, 11, channels, n)
+        rows[:, 2] = 1.0 + 17.0 * st.uniform(b, e, 12)
+        rows[:, 3] = 1
+        rows[:, 4] = st.integers(b, e, 13, 1, 9)
+        rows[:, 5] = st.integers(b, e, 14, 0, 4)
+        fac = st.uniform(b, e, 15) < 0.5
+        rows[:, 6] = np.where(fac, 0.1, 0.55)
+        rows[:, 7] = np.where(fac, 30.0, 450.0)
+        rows[:, 8] = np.where(fac, 1700.0, 0.0)
+        rows[:, 9] = st.integers(b, e, 16, 0, 6)
+        rows[:, 10] = st.integers(b, e, 17, 0, 8)
+        return rows
+
+    motors = np.tile(np.arange(channels, channels + outputs), (founders, 1))
+    inputs = st.uniform(np.repeat(fi, channels), np.tile(np.arange(channels), founders), 50).reshape(founders,
+                                                                                                      channels)
+    return _assemble("world_founders", sizes, edges, channels, 8, nfn, sfn, motors, inputs, 230.0,
+                     {"ticks_per_step": 16})
+
+
+def concat(batches, name="concat"):
+    """One Batch holding every brain of `batches`, in order (same channels,
+    outputs and delay ring)."""
+    no, so = [0], [0]
+    for b in batches:
+        no.extend((no[-1] + np.asarray(b.neuron_offsets[1:]) - b.neuron_offsets[0]).tolist())
+        so.extend((so[-1] + np.asarray(b.synapse_offsets[1:]) - b.synapse_offsets[0]).tolist())
+    b0 = batches[0]
+    inputs = None if b0.inputs is None else np.concatenate([b.inputs for b in batches]).astype(np.float32)
+    return Batch(np.concatenate([b.neuron_rows for b in batches]), np.concatenate([b.synapse_rows for b in batches]),
+                 np.asarray(no, np.int64), np.asarray(so, np.int64),
+                 np.concatenate([b.motors for b in batches]).astype(np.int32), b0.channels, b0.max_delay, name, inputs,
+                 b0.gain, {})

@@ -11,6 +11,10 @@ Outputs (all git-ignored):
   oracle/_ref/libns_ref_gpu.so        the reference CUDA batch
                                       (gym_adapter/gpu.cu) for sm_100a with the
                                       reference's flags (gym_adapter/gpu.py:19)
+  oracle/_ref/libns_ref_world.so      the reference world simulator's neural
+                                      kernels (src/main.cu) with its own flags
+  oracle/_ref/libns_ref_world_cr.so   the same kernels with IEEE arithmetic and
+                                      correctly rounded exp/log
 The _ref targets need the reference tree (REFERENCE_ROOT, default
 /root/reference) and are skipped when it is absent; prebuilt files are used as
 they are.
@@ -103,6 +107,16 @@ def build_ref(verbose=False, gpu=True):
                 " const void *) { return 1; }\n")
             _run(["nvcc", "-O3", "-std=c++17", "--use_fast_math", "-gencode", "arch=compute_100a,code=sm_100a",
                   "-shared", "-Xcompiler", "-fPIC", "-I", stub, "-I", REFERENCE / "src",
+                  "-DLIVE_ASSET_DIR=\"/nonexistent\"", HERE / "ref_world_harness.cu", REFERENCE / "src" / "live_view.cpp",
+                  "-o", out, "-lz"])
+        # The same kernels for the bit-exact comparison: IEEE division and
+        # square root, no FMA contraction, exp/log correctly rounded.
+        out = REF_OUT / "libns_ref_world_cr.so"
+        if _stale(out, [world_src, HERE / "ref_world_harness.cu", HERE / "ref_cr_shim_cuda.h", CSRC / "ns_crmath.h"]):
+            stub = REF_OUT / "stub_include"
+            _run(["nvcc", "-O3", "-std=c++17", "--fmad=false", "--prec-div=true", "--prec-sqrt=true",
+                  "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC,-ffp-contract=off",
+                  "-I", stub, "-I", REFERENCE / "src", "-I", CSRC, "-include", HERE / "ref_cr_shim_cuda.h",
                   "-DLIVE_ASSET_DIR=\"/nonexistent\"", HERE / "ref_world_harness.cu", REFERENCE / "src" / "live_view.cpp",
                   "-o", out, "-lz"])
     return REF_OUT

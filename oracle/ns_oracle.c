@@ -15,6 +15,7 @@
 #include "ns_oracle.h"
 
 #include <math.h>
+#include <stddef.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -1160,4 +1161,201 @@ int or_protocols(float *out, int n) {
     int m = n < 40 ? n : 40;
     memcpy(out, r, (size_t)m * sizeof(float));
     return m;
+}
+
+/* ---- World neural stage (src/main.cu:659-801, 1287-1300) ------------------------
+ * The reference world loop runs, per tick, synapse_delivery over every occupied
+ * synapse slot, neuron_step over every occupied neuron slot, then
+ * synapse_plasticity (src/main.cu:2696-2728; the fused
+ * synapse_plasticity_delivery kernel is plasticity(tick - 1) followed by
+ * delivery(tick) per synapse, the same sequence). Its per-branch sums are
+ * float atomics; this restatement fixes their order: each animal's synapse
+ * list order (the order of the animal's synapse_head/synapse_next chain).
+ * Trace float sums (observer-only) are fixed as: per neuron over the step in
+ * tick order, then added per motor port in the animal's neuron list order. */
+typedef struct {                   /* src/main.cu:81-91 */
+    float x, y, heading, energy, health, fullness, pain;
+    float taste[4];
+    float muscle[3];
+    unsigned long long rng;
+    int id, parent_id, generation, age, alive;
+    int neuron_head, synapse_head, neuron_count, synapse_count;
+    int ports[24];
+    int behavior[69];
+} or_animal;
+typedef struct {                   /* src/main.cu:96-104 */
+    int id, assigned, frozen, initial_age, initial_offspring;
+    int final_age, final_offspring, alive, death_cause;
+    int neurons, synapses, generation;
+    float initial_energy, initial_health;
+    int64_t start_step, observed_step, death_step;
+} or_cohort;
+
+#define W_S 19
+#define W_M 5
+#define W_HIST 9
+#define W_CONTACT 16
+
+static int or_w_frozen(const or_world_pools *w, int a) {       /* src/main.cu:142-146 */
+    const or_animal *A = (const or_animal *)w->animals;
+    const or_cohort *C = (const or_cohort *)w->plasticity_cohort;
+    return C && a >= 0 && C[a].assigned && C[a].frozen && C[a].id == A[a].id;
+}
+
+/* An edge delivers when active, owned endpoints of the same animal, genes active
+ * (src/main.cu:700-704). */
+static int or_w_valid(const or_world_pools *w, int a, const sgene *g) {
+    const ngene *NG = (const ngene *)w->neurons;
+    if (!g->active || g->pre < 0 || g->post < 0 || g->pre >= w->neuron_capacity || g->post >= w->neuron_capacity)
+        return 0;
+    return w->neuron_owner[g->pre] == a && w->neuron_owner[g->post] == a && NG[g->pre].active && NG[g->post].active;
+}
+
+int or_world_step(const or_world_pools *w, int64_t step) {
+    init_consts();
+    const or_animal *A = (const or_animal *)w->animals;
+    const ngene *NG = (const ngene *)w->neurons;
+    nstate *NS = (nstate *)w->neuron_state;
+    const sgene *SG = (const sgene *)w->synapses;
+    sstate *SS = (sstate *)w->synapse_state;
+    const int P = w->animal_capacity, NC = w->neuron_capacity;
+    const int64_t first = (step - 1) * 16;
+    float *tx = NULL, *ti = NULL;
+    const int tr = w->trace_animal;
+    if (tr >= 0 && tr < P && A[tr].alive == 1) {
+        tx = (float *)calloc((size_t)NC, sizeof(float));
+        ti = (float *)calloc((size_t)NC, sizeof(float));
+    }
+    /* gene checks the engine enforces on live edges */
+    for (int a = 0; a < P; ++a) {
+        if (A[a].alive != 1) continue;
+        for (int e = A[a].synapse_head; e >= 0; e = w->synapse_next[e]) {
+            const sgene *g = &SG[e];
+            if (!or_w_valid(w, a, g)) continue;
+            if (g->delay < 1 || g->delay > 8 || g->branch > 3 || g->plast > 7 || NG[g->pre].modulator > 3) {
+                free(tx); free(ti);
+                return -1;
+            }
+        }
+    }
+    for (int t = 0; t < 16; ++t) {
+        const int64_t tick = first + t;
+        for (int a = 0; a < P; ++a) {                                  /* delivery, src/main.cu:659-708 */
+            if (A[a].alive != 1) continue;
+            for (int e = A[a].synapse_head; e >= 0; e = w->synapse_next[e]) {
+                const sgene *g = &SG[e];
+                sstate *s = &SS[e];
+                if (!or_w_valid(w, a, g)) continue;
+                s->arrived = tick >= g->delay &&
+                             w->spike_history[(size_t)((tick - g->delay) % W_HIST) * NC + (size_t)g->pre];
+                if (!s->arrived) continue;
+                const ngene *src = &NG[g->pre];
+                const float rel = (!src->inh_tx || src->modulator) ? release(g, s, tick) : s->w;
+                const int motor = w->neuron_port[g->post] - W_S;
+                const int traced = a == tr && motor >= 0 && motor < W_M;
+                if (src->modulator) {
+                    if (rel > 0) {
+                        unsigned long long *q = &w->mod_event_tick[(size_t)g->post * 6 + (size_t)(src->modulator - 1) * 2 +
+                                                                   (size_t)(tick & 1)];
+                        if (*q < (unsigned long long)(tick + 1)) *q = (unsigned long long)(tick + 1);
+                    }
+                } else if (!src->inh_tx) {
+                    if (traced) {
+                        w->trace_exc_arrivals[motor] += 1;
+                        if (rel > 0) w->trace_exc_releases[motor] += 1;
+                        tx[g->post] += rel;
+                    }
+                    w->pending_exc[(size_t)g->post * 4 + g->branch] += rel * OEXP(NS[g->post].log_ampa);
+                } else {
+                    if (traced) {
+                        w->trace_inh_arrivals[motor] += 1;
+                        ti[g->post] += rel;
+                    }
+                    w->pending_inh[g->post] += rel;
+                }
+            }
+        }
+        for (int a = 0; a < P; ++a) {                                  /* neurons, src/main.cu:710-746 */
+            if (A[a].alive != 1) continue;
+            for (int n = A[a].neuron_head; n >= 0; n = w->neuron_next[n]) {
+                const ngene *g = &NG[n];
+                if (!g->active) continue;
+                nstate *s = &NS[n];
+                float exc[4];
+                for (int k = 0; k < 4; ++k) { exc[k] = w->pending_exc[(size_t)n * 4 + k]; w->pending_exc[(size_t)n * 4 + k] = 0; }
+                const float inh = w->pending_inh[n];
+                w->pending_inh[n] = 0;
+                const int port = w->neuron_port[n];
+                float cur = 0.0f;
+                if (g->sens >= 0 && g->sens < W_S) {
+                    const float level = (w->silence_senses || (w->silence_contact && g->sens >= W_CONTACT))
+                                            ? 0.0f : w->senses[(size_t)a * W_S + (size_t)g->sens];
+                    cur = g->type == 5 && g->sens < 6 ? receptor_drive(g, s, level) : level * 230.0f;
+                }
+                neuron_tick(g, s, cur, exc, inh);
+                if (a == tr && port >= W_S && port < W_S + W_M)
+                    w->trace_peak_mv[port - W_S] = fmaxf(w->trace_peak_mv[port - W_S], s->v);
+                if (s->spike && port >= W_S && port < W_S + W_M) w->motors[(size_t)a * W_M + (size_t)(port - W_S)] += 1;
+                w->spike_history[(size_t)(tick % W_HIST) * NC + (size_t)n] = s->spike;
+            }
+        }
+        for (int a = 0; a < P; ++a) {                                  /* plasticity, src/main.cu:748-767 */
+            if (A[a].alive != 1 || or_w_frozen(w, a)) continue;
+            for (int e = A[a].synapse_head; e >= 0; e = w->synapse_next[e]) {
+                const sgene *g = &SG[e];
+                if (!or_w_valid(w, a, g)) continue;
+                const ngene *x = &NG[g->pre], *z = &NG[g->post];
+                const int pair = !x->inh_tx && excitatory_kind(x->type) && x->modulator == 0 && !z->inh_tx &&
+                                 excitatory_kind(z->type);
+                const size_t target = (size_t)g->post * 6 + (size_t)(tick & 1);
+                unsigned char mod = 0;
+                if (w->mod_event_tick[target] == (unsigned long long)(tick + 1)) mod |= MOD_NE;
+                if (w->mod_event_tick[target + 2] == (unsigned long long)(tick + 1)) mod |= MOD_5HT;
+                if (w->mod_event_tick[target + 4] == (unsigned long long)(tick + 1)) mod |= MOD_DA;
+                plasticity_tick(g, &SS[e], SS[e].arrived, NS[g->post].spike, pair, NS[g->post].depol, mod);
+            }
+        }
+    }
+    if (tx) {
+        for (int n = A[tr].neuron_head; n >= 0; n = w->neuron_next[n]) {
+            const int port = w->neuron_port[n];
+            if (port < W_S || port >= W_S + W_M || !NG[n].active) continue;
+            w->trace_exc_ns[port - W_S] += tx[n];
+            w->trace_inh_ns[port - W_S] += ti[n];
+        }
+        free(tx); free(ti);
+    }
+    return 0;
+}
+
+void or_world_homeostasis(const or_world_pools *w) {          /* src/main.cu:1287-1300 */
+    init_consts();
+    const or_animal *A = (const or_animal *)w->animals;
+    const ngene *NG = (const ngene *)w->neurons;
+    nstate *NS = (nstate *)w->neuron_state;
+    for (int i = 0; i < w->neuron_capacity; ++i) {
+        const int a = w->neuron_owner[i];
+        if (a < 0 || a >= w->animal_capacity) continue;
+        if (A[a].alive != 1 || !NG[i].active || or_w_frozen(w, a)) continue;
+        const float elapsed = fmaxf(16.0f, (float)A[a].age * 16.0f);
+        homeostasis(&NG[i], &NS[i], 16.0f, (float)NS[i].total * 1000.0f / elapsed);
+    }
+}
+
+void or_records(const or_brain *b, void *neuron_genes, void *neuron_states, void *synapse_genes,
+                void *synapse_states) {
+    if (neuron_genes) memcpy(neuron_genes, b->ng, sizeof(ngene) * (size_t)b->count);
+    if (neuron_states) memcpy(neuron_states, b->ns, sizeof(nstate) * (size_t)b->count);
+    if (synapse_genes) memcpy(synapse_genes, b->sg, sizeof(sgene) * (size_t)b->edges);
+    if (synapse_states) memcpy(synapse_states, b->ss, sizeof(sstate) * (size_t)b->edges);
+}
+
+int or_world_layout(uint64_t *out) {
+    const uint64_t v[14] = {sizeof(or_animal), sizeof(or_cohort), sizeof(ngene), sizeof(nstate), sizeof(sgene),
+                            sizeof(sstate), offsetof(or_animal, id), offsetof(or_animal, age),
+                            offsetof(or_animal, alive), offsetof(or_animal, neuron_head),
+                            offsetof(or_animal, synapse_head), offsetof(or_animal, neuron_count),
+                            offsetof(or_animal, synapse_count), offsetof(or_cohort, frozen)};
+    for (int i = 0; i < 14; ++i) out[i] = v[i];
+    return 14;
 }

@@ -89,6 +89,38 @@ void or_env_sincos(double x, double *s, double *c);
 /* Fixed environment sequence for build comparisons (or_episode.c). */
 void or_env_sequence(uint64_t *out);
 
+/* World neural stage (src/main.cu:659-801 ordering; or_world_step follows the
+ * reference's tick-major order over every living animal, with the per-branch
+ * sums in each animal's synapse list order). Host pools in the reference
+ * record layouts, fields as the library's NsbWorldPools. */
+typedef struct or_world_pools {
+    const void *animals, *plasticity_cohort, *neurons, *synapses;
+    void *neuron_state, *synapse_state;
+    float *pending_exc, *pending_inh;
+    const float *senses;
+    unsigned long long *mod_event_tick;
+    unsigned char *spike_history;
+    const int *neuron_owner, *synapse_owner, *neuron_next, *synapse_next, *neuron_port;
+    int *motors;
+    int *trace_exc_arrivals, *trace_exc_releases, *trace_inh_arrivals;
+    float *trace_exc_ns, *trace_inh_ns, *trace_peak_mv;
+    int trace_animal, silence_senses, silence_contact;
+    int animal_capacity, neuron_capacity, synapse_capacity;
+} or_world_pools;
+/* One world step's 16 ticks; 0, or -1 on a live synapse gene the engine
+ * rejects (delay outside 1-8, branch above 3). */
+int or_world_step(const or_world_pools *w, int64_t step);
+/* Homeostasis after the body step (src/main.cu:1287-1300). */
+void or_world_homeostasis(const or_world_pools *w);
+/* The brain's records in the reference layouts (NeuronGene, NeuronState,
+ * SynapseGene, SynapseState); any pointer may be NULL. */
+void or_records(const or_brain *b, void *neuron_genes, void *neuron_states, void *synapse_genes,
+                void *synapse_states);
+/* sizeof Animal, PlasticityCohort, NeuronGene, NeuronState, SynapseGene,
+ * SynapseState, then offsets of Animal.id, .age, .alive, .neuron_head,
+ * .synapse_head, .neuron_count, .synapse_count, PlasticityCohort.frozen. */
+int or_world_layout(uint64_t *out);
+
 /* Reference protocol checks (tests/physiology.cpp, tests/event_synapses.cpp,
  * tests/cuda_relay_parity.cu restated); results written as floats. */
 int or_protocols(float *out, int n);

@@ -62,6 +62,12 @@ def oracle_lib(libm=False):
         lib.or_env_tanh.argtypes = [ct.c_double]; lib.or_env_tanh.restype = ct.c_double
         lib.or_env_sincos.argtypes = [ct.c_double, _d, _d]
         lib.or_env_sequence.argtypes = [ct.POINTER(ct.c_uint64)]
+        lib.or_world_step.argtypes = [ct.c_void_p, ct.c_int64]
+        lib.or_world_step.restype = ct.c_int
+        lib.or_world_homeostasis.argtypes = [ct.c_void_p]
+        lib.or_records.argtypes = [ct.c_void_p] * 5
+        lib.or_world_layout.argtypes = [ct.POINTER(ct.c_uint64)]
+        lib.or_world_layout.restype = ct.c_int
         _libs[name] = lib
     return _libs[name]
 
@@ -138,6 +144,40 @@ def ref_world_lib():
     return _libs[name]
 
 
+def world_step(pools, step):
+    """The oracle's world stage (or_world_step) on host WorldPools, in place."""
+    lib = oracle_lib()
+    st = pools.struct()
+    if lib.or_world_step(ct.byref(st), int(step)) != 0:
+        raise ValueError("oracle: invalid live synapse gene")
+
+
+def world_homeostasis(pools):
+    lib = oracle_lib()
+    st = pools.struct()
+    lib.or_world_homeostasis(ct.byref(st))
+
+
+def oracle_records(batch, seeds):
+    """Reset records of every brain of a workloads.Batch from the oracle, in
+    the reference layouts (neuron genes 124 B, states 120 B, synapse genes
+    40 B, states 80 B), concatenated in batch order."""
+    lib = oracle_lib()
+    N, E = int(batch.neuron_offsets[-1]), int(batch.synapse_offsets[-1])
+    ng = np.zeros((N, 124), np.uint8)
+    ns = np.zeros((N, 120), np.uint8)
+    sg = np.zeros((max(E, 1), 40), np.uint8)
+    ss = np.zeros((max(E, 1), 80), np.uint8)
+    for b in range(batch.brains):
+        n0, n1 = batch.neuron_offsets[b], batch.neuron_offsets[b + 1]
+        e0, e1 = batch.synapse_offsets[b], batch.synapse_offsets[b + 1]
+        o = OracleBrain(*batch.brain(b), batch.channels, batch.max_delay)
+        o.reset(int(seeds[b]))
+        lib.or_records(ct.c_void_p(o.ptr), ng[n0:].ctypes.data, ns[n0:].ctypes.data, sg[e0:].ctypes.data,
+                       ss[e0:].ctypes.data)
+    return ng, ns, sg[:E], ss[:E]
+
+
 class OracleBrain:
     """One brain in the C oracle."""
 
@@ -156,6 +196,16 @@ class OracleBrain:
 
     def reset(self, seed):
         self.lib.or_reset(self.ptr, ct.c_uint32(seed))
+
+    def records(self):
+        """(neuron genes, neuron states, synapse genes, synapse states) as
+        uint8 rows of the reference layouts (124, 120, 40, 80 bytes)."""
+        ng = np.zeros((self.count, 124), np.uint8)
+        ns = np.zeros((self.count, 120), np.uint8)
+        sg = np.zeros((max(self.edges, 1), 40), np.uint8)
+        ss = np.zeros((max(self.edges, 1), 80), np.uint8)
+        self.lib.or_records(ct.c_void_p(self.ptr), ng.ctypes.data, ns.ctypes.data, sg.ctypes.data, ss.ctypes.data)
+        return ng, ns, sg[:self.edges], ss[:self.edges]
 
     def set_pulse(self, period, mod=4):
         """Global modulator pulse every `period` ticks with bits `mod` (4 = dopamine)."""

@@ -14,6 +14,7 @@
 #include "main.cu"
 #undef main
 
+#include <algorithm>
 #include <cstring>
 
 namespace {
@@ -173,13 +174,46 @@ void *ref_world_create(int brains, const int64_t *noff, const int64_t *soff, con
     return w;
 }
 
-// One world step of the neural stage; returns 0 or a CUDA error code.
-int ref_world_step(void *p) {
-    World &w = *static_cast<World *>(p);
+}  // extern "C"
+
+namespace {
+// Selection buffers of a World whose pools are already set.
+bool alloc_selection(World &w) {
     Device &d = w.d;
-    const int64_t step = ++w.step;
+    d.occupied_neurons = dalloc<int>(NEURON_CAPACITY);
+    d.occupied_synapses = dalloc<int>(SYNAPSE_CAPACITY);
+    d.occupied_neuron_count = dalloc<int>(1);
+    d.occupied_synapse_count = dalloc<int>(1);
+    d.block_animals = dalloc<int>(P);
+    d.block_animal_count = dalloc<int>(1);
+    d.medium_animals = dalloc<int>(P);
+    d.medium_animal_count = dalloc<int>(1);
     auto slots = thrust::make_counting_iterator<int>(0);
-    int neuron_count = 0, synapse_count = 0, block_count = 0, medium_count = 0;
+    size_t b[6] = {};
+    cub::DeviceSelect::If(nullptr, b[0], slots, d.occupied_neurons, d.occupied_neuron_count, NEURON_CAPACITY, OwnedSlot{d.neuron_owner});
+    cub::DeviceSelect::If(nullptr, b[1], slots, d.occupied_synapses, d.occupied_synapse_count, SYNAPSE_CAPACITY, OwnedSlot{d.synapse_owner});
+    cub::DeviceSelect::If(nullptr, b[2], slots, d.block_animals, d.block_animal_count, P, BlockAnimal{d.animals});
+    cub::DeviceSelect::If(nullptr, b[3], slots, d.medium_animals, d.medium_animal_count, P, MediumAnimal{d.animals});
+    cub::DeviceSelect::If(nullptr, b[4], slots, d.occupied_neurons, d.occupied_neuron_count, NEURON_CAPACITY, FallbackOwnedSlot{d.neuron_owner, d.animals});
+    cub::DeviceSelect::If(nullptr, b[5], slots, d.occupied_synapses, d.occupied_synapse_count, SYNAPSE_CAPACITY, FallbackOwnedSlot{d.synapse_owner, d.animals});
+    w.select_bytes = *std::max_element(b, b + 6);
+    cudaMalloc(&w.select_tmp, w.select_bytes);
+    cudaFuncSetAttribute(brain_block_step<BLOCK_BRAIN_NEURONS, BLOCK_BRAIN_SYNAPSES, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         sizeof(BlockBrain<BLOCK_BRAIN_NEURONS, BLOCK_BRAIN_SYNAPSES, false>));
+    cudaFuncSetAttribute(brain_block_step<MEDIUM_BRAIN_NEURONS, MEDIUM_BRAIN_SYNAPSES, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         sizeof(BlockBrain<MEDIUM_BRAIN_NEURONS, MEDIUM_BRAIN_SYNAPSES, false>));
+    return d.occupied_neurons && d.occupied_synapses && w.select_tmp && cudaDeviceSynchronize() == cudaSuccess;
+}
+
+// The neural part of the world loop for `step` (src/main.cu:2634-2728):
+// selection, the device-to-host count reads, 16 ticks.
+int neural_stage(World &w, int64_t step, int &neuron_count, int &block_count, int &medium_count) {
+    Device &d = w.d;
+    auto slots = thrust::make_counting_iterator<int>(0);
+    int synapse_count = 0;
+    neuron_count = block_count = medium_count = 0;
     if (w.block_mode) {
         cub::DeviceSelect::If(w.select_tmp, w.select_bytes, slots, d.block_animals, d.block_animal_count, P, BlockAnimal{d.animals});
         cub::DeviceSelect::If(w.select_tmp, w.select_bytes, slots, d.medium_animals, d.medium_animal_count, P, MediumAnimal{d.animals});
@@ -217,10 +251,114 @@ int ref_world_step(void *p) {
         if (synapse_count && t == TICKS - 1)
             synapse_plasticity<<<(synapse_count + NEURAL_BLOCK - 1) / NEURAL_BLOCK, NEURAL_BLOCK>>>(d, tick, synapse_count);
     }
+    return (int)cudaGetLastError();
+}
+
+// Homeostasis launches of the world loop (src/main.cu:2751-2758).
+void homeostasis_stage(World &w, int neuron_count, int block_count, int medium_count) {
+    Device &d = w.d;
     if (neuron_count) homeostasis_step<<<(neuron_count + 255) / 256, 256>>>(d, neuron_count);
     if (block_count) homeostasis_block_animals<<<(block_count + 127) / 128, 128>>>(d, d.block_animals, block_count);
     if (medium_count) homeostasis_block_animals<<<(medium_count + 127) / 128, 128>>>(d, d.medium_animals, medium_count);
+}
+
+// Pool pointers in the layout of the library's NsbWorldPools.
+struct PoolsArg {
+    void *animals, *plasticity_cohort, *neurons, *synapses, *neuron_state, *synapse_state;
+    float *pending_exc, *pending_inh, *senses;
+    unsigned long long *mod_event_tick;
+    unsigned char *spike_history;
+    int *neuron_owner, *synapse_owner, *neuron_next, *synapse_next, *neuron_port, *motors;
+    int *trace_exc_arrivals, *trace_exc_releases, *trace_inh_arrivals;
+    float *trace_exc_ns, *trace_inh_ns, *trace_peak_mv;
+    int trace_animal, silence_senses, silence_contact, animal_capacity, neuron_capacity, synapse_capacity;
+};
+struct PoolsWorld {
+    World w;
+    int counts[3] = {0, 0, 0};
+};
+}  // namespace
+
+extern "C" {
+
+// One world step of the neural stage and its homeostasis; returns 0 or a CUDA error code.
+int ref_world_step(void *p) {
+    World &w = *static_cast<World *>(p);
+    int n = 0, b = 0, m = 0;
+    const int rc = neural_stage(w, ++w.step, n, b, m);
+    if (rc) return rc;
+    homeostasis_stage(w, n, b, m);
     return (int)cudaGetLastError();
+}
+
+// The reference's neural kernels on caller-owned pools (device pointers in
+// the library's NsbWorldPools layout, the build's full capacities). The
+// selection buffers are the harness's own. block_mode 0: the default fused
+// global-slot kernels; 1: the --block-brains tiers.
+void *ref_world_pools_create(const void *pools, int block_mode) {
+    const PoolsArg &p = *static_cast<const PoolsArg *>(pools);
+    if (p.animal_capacity != P || p.neuron_capacity != NEURON_CAPACITY || p.synapse_capacity != SYNAPSE_CAPACITY)
+        return nullptr;
+    auto *h = new PoolsWorld;
+    Device &d = h->w.d;
+    h->w.block_mode = block_mode;
+    d.trace_animal = p.trace_animal;
+    d.silence_senses = p.silence_senses != 0;
+    d.silence_contact = p.silence_contact != 0;
+    d.animals = static_cast<Animal *>(p.animals);
+    d.plasticity_cohort = static_cast<PlasticityCohort *>(p.plasticity_cohort);
+    d.neurons = static_cast<NeuronGene *>(p.neurons);
+    d.synapses = static_cast<SynapseGene *>(p.synapses);
+    d.neuron_state = static_cast<NeuronState *>(p.neuron_state);
+    d.synapse_state = static_cast<SynapseState *>(p.synapse_state);
+    d.pending_exc = p.pending_exc; d.pending_inh = p.pending_inh; d.senses = p.senses;
+    d.mod_event_tick = p.mod_event_tick; d.spike_history = p.spike_history;
+    d.neuron_owner = p.neuron_owner; d.synapse_owner = p.synapse_owner;
+    d.neuron_next = p.neuron_next; d.synapse_next = p.synapse_next; d.neuron_port = p.neuron_port;
+    d.motors = p.motors;
+    d.trace_exc_arrivals = p.trace_exc_arrivals; d.trace_exc_releases = p.trace_exc_releases;
+    d.trace_inh_arrivals = p.trace_inh_arrivals; d.trace_exc_ns = p.trace_exc_ns; d.trace_inh_ns = p.trace_inh_ns;
+    d.trace_peak_mv = p.trace_peak_mv;
+    if (!alloc_selection(h->w)) {
+        delete h;
+        return nullptr;
+    }
+    return h;
+}
+
+int ref_world_pools_step(void *p, long long step) {
+    auto *h = static_cast<PoolsWorld *>(p);
+    const int rc = neural_stage(h->w, step, h->counts[0], h->counts[1], h->counts[2]);
+    if (rc) return rc;
+    return (int)cudaDeviceSynchronize();
+}
+
+int ref_world_pools_homeostasis(void *p) {
+    auto *h = static_cast<PoolsWorld *>(p);
+    homeostasis_stage(h->w, h->counts[0], h->counts[1], h->counts[2]);
+    return (int)cudaDeviceSynchronize();
+}
+
+void ref_world_pools_destroy(void *p) {
+    auto *h = static_cast<PoolsWorld *>(p);
+    Device &d = h->w.d;
+    void *ptrs[] = {d.occupied_neurons, d.occupied_synapses, d.occupied_neuron_count, d.occupied_synapse_count,
+                    d.block_animals, d.block_animal_count, d.medium_animals, d.medium_animal_count, h->w.select_tmp};
+    for (void *q : ptrs) cudaFree(q);
+    delete h;
+}
+
+// Layout of the Animal and PlasticityCohort fields the neural stage reads, as
+// the reference builds them: sizes, then offsets of Animal.id, .age, .alive,
+// .neuron_head, .synapse_head, .neuron_count, .synapse_count and
+// PlasticityCohort.frozen.
+int ref_world_animal_layout(uint64_t *out) {
+    const uint64_t v[10] = {sizeof(Animal), sizeof(PlasticityCohort), offsetof(Animal, id), offsetof(Animal, age),
+                            offsetof(Animal, alive), offsetof(Animal, neuron_head), offsetof(Animal, synapse_head),
+                            offsetof(Animal, neuron_count), offsetof(Animal, synapse_count),
+                            offsetof(PlasticityCohort, frozen)};
+    for (int i = 0; i < 10; ++i) out[i] = v[i];
+    return 10;
 }
 
 int ref_world_sync() { return (int)cudaDeviceSynchronize(); }

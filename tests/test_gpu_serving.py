@@ -147,3 +147,18 @@ def test_serving_rejects_bad_input(nsb):
     with pytest.raises(RuntimeError, match="Invalid episode length"):
         srv.submit([g], 1, 0)
     srv.close()
+
+
+def test_request_that_can_never_fit_is_reported(nsb):
+    """A request larger than the server's synapse pool can never be admitted:
+    with nothing in flight the loop reports it instead of waiting forever."""
+    lib = _library(nsb)
+    sizes = np.diff(lib.neuron_offsets)
+    g = int(np.argmax(sizes))                      # ~4,000 neurons, ~32,000 synapses
+    srv = nsb.Server(max_inflight_neurons=int(sizes[g]), synapses_per_neuron=1.0, max_slots=16,
+                     max_brain_neurons=int(sizes[g]))
+    gid = srv.register(*lib.brain(g))
+    srv.submit([gid], 1, 10, tag=0, arrival=0.0)
+    with pytest.raises(RuntimeError, match="does not fit"):
+        srv.run()
+    srv.close()
