@@ -16,6 +16,9 @@ e2e   : the same metric through the reference's C ABI call ns_gpu_step with
 --impl reference : the reference's own host executor (gym_adapter/native.cpp
         built from its sources into oracle/_ref) on the host cores.
 
+--world : the world simulator's neural stage (config 2 founders, or --world-population
+        full) through nsb_world_*, then the reference's world kernels on the same pools.
+
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
        (N > 1 under torch.distributed.run: one full-pool replica per GPU).
 """
@@ -599,6 +602,163 @@ def run_serve(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def world_population(nsb, population):
+    """World pools at the reference build's capacities (32,768 animals,
+    4,194,304 neuron and 8,388,608 synapse slots). "founders": 2,048 founders
+    of 32-96 neurons with 4-12 synapses per neuron (config 2); "full": the
+    full-pool batched-uneven population as animals (delays folded into the
+    world's 1-8 ms ring, its 8 input channels as world senses 0-7)."""
+    W = nsb.world
+    if population == "founders":
+        batch = nsb.workloads.world_founders(seed=2, founders=2048)
+    else:
+        full = workload(nsb, 2)
+        sr = full.synapse_rows.copy()
+        sr[:, 4] = (sr[:, 4] - 1) % 8 + 1
+        senses = np.zeros((full.brains, 19), np.float32)
+        senses[:, :full.channels] = full.inputs
+        batch = nsb.workloads.Batch(full.neuron_rows, sr, full.neuron_offsets, full.synapse_offsets, full.motors, 19,
+                                    8, "batched_uneven_world", senses, 230.0, {})
+    recs = W.records_from_gpu(batch, np.arange(batch.brains, dtype=np.uint32) + 1)
+    pools = W.place_population(batch, *recs, animal_capacity=32768, neuron_capacity=4194304,
+                               synapse_capacity=8388608)
+    return batch, pools
+
+
+def run_world_stage(args, rank, world, local_rank):
+    """The world simulator's neural stage on world pools through
+    nsb_world_neural_step + nsb_world_homeostasis, then the reference's own
+    world kernels (src/main.cu, the world binary's flags) on the same pools.
+    Rank 0 only (one GPU)."""
+    import ctypes as ct
+    import torch
+    if rank != 0:
+        return
+    torch.cuda.set_device(local_rank)
+    sys.path.insert(0, str(ROOT))
+    nsb = load_package()
+    W = nsb.world
+    batch, pools = world_population(nsb, args.world_population)
+    N, E, B = int(batch.neuron_offsets[-1]), int(batch.synapse_offsets[-1]), batch.brains
+    stage = W.World(pools)
+    counter = [0]
+
+    def run(k):
+        for _ in range(k):
+            counter[0] += 1
+            stage.neural_step(counter[0])
+            stage.homeostasis()
+    t0 = time.perf_counter()
+    run(1)
+    first_step_s = time.perf_counter() - t0          # includes compiling every brain on the device
+    run(max(args.warmup, 3) - 1)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        t0 = time.perf_counter()
+        e0.record()
+        run(args.steps)
+        e1.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    ms = e0.elapsed_time(e1) / args.steps
+    st = stage.stats()
+    stage.close()
+    del stage
+    torch.cuda.empty_cache()
+    value = N * 16 / (ms / 1e3)
+    peak, peak_kind = peaks()
+    algo = ALGO_BYTES_PER_NEURON * N + ALGO_BYTES_PER_SYNAPSE * E
+    achieved = algo / (ms / 1e3) / 1e9
+    line = {"metric": "neuron-ticks/s of the world neural stage", "value": value, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (Philox4x32-10, seed 2)",
+            "config": {"workload": f"world_{args.world_population}", "animals": B, "neurons": N, "synapses": E,
+                       "ticks_per_step": 16, "delays_ms": "1-8",
+                       "pools": "reference layouts at the reference capacities (32,768 / 4,194,304 / 8,388,608)",
+                       "step": "nsb_world_neural_step + nsb_world_homeostasis (5 kernels, one host sync)",
+                       "first_step_s_with_compile": first_step_s,
+                       "l2": f"pools touched per step {(364 * N + 200 * E) / 1e9:.2f} GB"},
+            "synaptic_events_per_s": st["events"] / (ms / 1e3),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_source": peak_kind, "algorithmic_bytes_per_launch": algo},
+            "e2e": {"value": N * 16 * args.steps / wall, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 72},
+            "gpu_launches": 5 * args.steps,
+            "clocks": clk.summary()}
+    if not args.no_cpu_baseline:
+        from oracle import pyoracle
+        sub = batch.subset(range(0, B, max(1, B // 64)))
+        sp = W.place_population(sub, *W.records_from_gpu(sub, np.arange(sub.brains, dtype=np.uint32) + 1))
+        pyoracle.world_step(sp, 1)
+        t0 = time.perf_counter()
+        for k in (2, 3):
+            pyoracle.world_step(sp, k)
+            pyoracle.world_homeostasis(sp)
+        secs = time.perf_counter() - t0
+        n_sub = int(sub.neuron_offsets[-1])
+        line["cpu_baseline"] = {"value": n_sub * 16 * 2 / secs, "unit": UNIT, "cores": 1, "kind": "port",
+                                "sample": f"{sub.brains} of {B} animals ({n_sub} neurons), oracle world "
+                                          f"restatement, 2 steps after 1"}
+    print(json.dumps(line), flush=True)
+
+    # the reference's world kernels on the same initial pools
+    from oracle import pyoracle
+    wlib = pyoracle.ref_world_lib()
+    if wlib is None or not hasattr(wlib, "ref_world_pools_create"):
+        print(json.dumps({"impl": "reference-cuda-world", "unavailable": "oracle/_ref/libns_ref_world.so not built"}))
+        return
+    wlib.ref_world_pools_create.restype = ct.c_void_p
+    wlib.ref_world_pools_create.argtypes = [ct.c_void_p, ct.c_int]
+    wlib.ref_world_pools_step.argtypes = [ct.c_void_p, ct.c_longlong]
+    wlib.ref_world_pools_homeostasis.argtypes = [ct.c_void_p]
+    wlib.ref_world_pools_destroy.argtypes = [ct.c_void_p]
+    for mode, label in ((0, "fused global-slot kernels"), (1, "--block-brains tiers + global-slot fallback")):
+        dev = {}
+        stc = W.NsbWorldPools()
+        for n in W.ARRAYS:
+            a = getattr(pools, n)
+            dev[n] = None if a is None else torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).reshape(-1)).cuda()
+            setattr(stc, n, None if dev[n] is None else dev[n].data_ptr())
+        stc.trace_animal, stc.silence_senses, stc.silence_contact = -1, 0, 0
+        stc.animal_capacity, stc.neuron_capacity, stc.synapse_capacity = pools.capacities
+        h = wlib.ref_world_pools_create(ct.byref(stc), mode)
+        if not h:
+            print(json.dumps({"impl": "reference-cuda-world", "unavailable": "pool setup failed"}))
+            continue
+        k = 0
+        for _ in range(max(args.warmup, 3)):
+            k += 1
+            wlib.ref_world_pools_step(h, k)
+            wlib.ref_world_pools_homeostasis(h)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0.record()
+        for _ in range(args.steps):
+            k += 1
+            wlib.ref_world_pools_step(h, k)
+            wlib.ref_world_pools_homeostasis(h)
+        e1.record()
+        torch.cuda.synchronize()
+        rwall = time.perf_counter() - t0
+        rms = e0.elapsed_time(e1) / args.steps
+        wlib.ref_world_pools_destroy(h)
+        del dev
+        torch.cuda.empty_cache()
+        ref_line = {"impl": "reference-cuda-world", "metric": line["metric"], "value": N * 16 / (rms / 1e3),
+                    "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": rms,
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                    "data": line["data"],
+                    "config": dict(line["config"], kernel=f"src/main.cu neural stage, {label}, --use_fast_math, "
+                                                          f"sm_100a", step="selection + 16 ticks + homeostasis"),
+                    "e2e": {"value": N * 16 * args.steps / rwall, "unit": UNIT, "h2d_bytes_per_step": 0,
+                            "d2h_bytes_per_step": 16}}
+        ref_line["config"].pop("first_step_s_with_compile", None)
+        print(json.dumps(ref_line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -619,12 +779,17 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="configured arrival rate (requests/s)")
     ap.add_argument("--serve-cap", type=int, default=4194304, help="neurons in flight")
     ap.add_argument("--serve-genomes", type=int, default=512)
+    ap.add_argument("--world", action="store_true",
+                    help="the world simulator's neural stage on its own pools (config 2)")
+    ap.add_argument("--world-population", default="founders", choices=["founders", "full"])
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus if "RANK" in os.environ else 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.serve:
         run_serve(args, rank, world, local_rank)
+    elif args.world:
+        run_world_stage(args, rank, world, local_rank)
     elif args.impl == "reference":
         run_reference(args, rank, world)
     elif args.impl == "reference-cuda":
