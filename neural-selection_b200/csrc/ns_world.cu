@@ -127,10 +127,13 @@ __device__ __forceinline__ bool compiled(const WorldArgs &d, const Cache &c, int
 }
 
 // ---- selection: animals whose compiled brain is missing or stale --------------
-__global__ void world_select(WorldArgs d, Cache c, int *list, int *count) {
+// Also lists every living animal (order irrelevant: animals do not interact
+// within the neural stage).
+__global__ void world_select(WorldArgs d, Cache c, int *list, int *count, int *alive, int *nalive) {
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < d.P; a += gridDim.x * blockDim.x) {
-        if (d.animals[a].alive != 1 || compiled(d, c, a)) continue;
-        list[atomicAdd(count, 1)] = a;
+        if (d.animals[a].alive != 1) continue;
+        alive[atomicAdd(nalive, 1)] = a;
+        if (!compiled(d, c, a)) list[atomicAdd(count, 1)] = a;
     }
 }
 
@@ -308,21 +311,28 @@ __global__ void __launch_bounds__(32 * kCompileWarps) world_compile(WorldArgs d,
 // ---- the ticks ------------------------------------------------------------------------
 // Per-unit arrays (shared memory for small units, a global slab for big ones).
 struct UnitMem {
-    float *gene;       // [16][gs]
+    float *gene;       // [16][gs] engine gene records, word-major
     int gs;
     uint32_t *nflag;
     float *cur;        // receptor level, or level x 230 pA
     float *scale;      // exp(log AMPA scale) of the post-synaptic neuron
-    uint16_t *ring;    // spike history bits: bit k = history slot k
+    float *ndepol;     // this tick's recent depolarisation per neuron
+    float *rel;        // this tick's released conductance (or weight) per arriving synapse
+    float *trx, *tri;  // per-neuron trace sums (traced animal)
     const int *inptr;  // unit CSR offsets
     const uint32_t *cmeta;
     const int *cslot;
-    uint8_t *carr;
-    int8_t *clast;
+    int *ev;           // event list: arrivals, then plasticity events
+    int *counters;     // [0] arrivals, [1] plasticity events
     const int *nslot;
-    const uint8_t *nani;
-    float *trx, *tri;  // per-neuron trace sums (traced animal)
+    uint16_t *cpost;   // post-synaptic neuron of each synapse (unit-local)
+    uint16_t *ring;    // spike history bits: bit k = history slot k
+    uint8_t *carr;     // this tick's arrival flag per synapse
+    int8_t *clast;     // tick of the synapse's last plasticity update (-1: none this step)
+    uint8_t *nspk;     // this tick's spike per neuron
+    uint8_t *nmod;     // this tick's modulator bits per neuron
 };
+constexpr uint32_t WF_FROZEN = 1u << 18;   // the neuron's animal is a frozen plasticity cohort
 
 struct TraceRegs {
     int ea, er, ia;
@@ -339,9 +349,10 @@ __device__ __forceinline__ void gene_record(const ref::NeuronGene &G, float *g, 
     g[G_RECDECAY * stride] = crexp(-1.0f / G.rec_decay, tab);
 }
 
-// Static per-neuron setup for neuron n of animal a (pool slot `slot`).
+// Static per-neuron setup for neuron n of animal a (pool slot `slot`); also
+// marks the neuron's incoming synapses with their post-synaptic index.
 __device__ __forceinline__ void setup_neuron(const WorldArgs &d, const UnitMem &U, int n, int slot, int a,
-                                             bool traced, int base9, const float *tab) {
+                                             bool traced, bool frozen, const float *tab) {
     const ref::NeuronGene &G = d.ngene[slot];
     gene_record(G, U.gene + n, U.gs, tab);
     uint32_t f = (uint32_t)(G.type & 7u);
@@ -351,6 +362,7 @@ __device__ __forceinline__ void setup_neuron(const WorldArgs &d, const UnitMem &
     if (G.sensory_channel >= 0) f |= NF_GENE_SENS;
     if (G.adp_tau > 0) f |= NF_ADP;
     if (exc_type(G.type)) f |= NF_EXC_TYPE;
+    if (frozen) f |= WF_FROZEN;
     const int port = d.nport[slot];
     if (port >= kS && port < kS + kM) {
         f |= (uint32_t)(port - kS + 1) << WF_MOTOR_SHIFT;
@@ -374,7 +386,11 @@ __device__ __forceinline__ void setup_neuron(const WorldArgs &d, const UnitMem &
     U.ring[n] = r;
     U.trx[n] = 0.0f;
     U.tri[n] = 0.0f;
-    (void)base9;
+    for (int p = U.inptr[n]; p < U.inptr[n + 1]; ++p) {
+        U.cpost[p] = (uint16_t)n;
+        U.carr[p] = 0;
+        U.clast[p] = -1;
+    }
 }
 
 __device__ __forceinline__ void load_regs(const ref::NeuronState &S, NeuronRegs &s) {
@@ -413,14 +429,45 @@ __device__ __forceinline__ void store_plast_ref(ref::SynapseState &Z, const SynP
     Z.spine = p.spine; Z.st_age = p.st_age; Z.pre_age = p.pre_age; Z.post_age = p.post_age;
 }
 
-// One tick of neuron n (state in s): delivery of its live incoming synapses in
-// list order, integration, motor/trace/ring updates, plasticity events.
-// Returns the number of arrivals.
-__device__ __forceinline__ int neuron_tick(const WorldArgs &d, const UnitMem &U, int n, int t, int64_t tick,
-                                           int cur9, bool frozen, NeuronRegs &s, int *motor_cnt, TraceRegs &tr,
-                                           const float *tab) {
+// One tick runs in five barrier-separated phases over the unit:
+//   1 arrival test of every live synapse (ring of the source neuron at
+//     tick - delay), arriving synapses appended to the event list;
+//   2 release of the arriving synapses, one per thread (independent per
+//     synapse; inhibitory sources deliver their weight);
+//   3 per neuron: the arriving inputs summed in list order, integration,
+//     motor/trace/ring updates;
+//   4 plasticity events (arrival, post-synaptic spike or a relevant
+//     modulator) appended to the event list;
+//   5 plasticity of those synapses, quiet ticks since the last update replayed
+//     first.
+__device__ __forceinline__ void phase_arrivals(const UnitMem &U, int ne, int cur9, int64_t tick, int tid, int bs) {
+    for (int p = tid; p < ne; p += bs) {
+        const uint32_t m = U.cmeta[p];
+        const int dl = (int)((m >> M_DELAY_SHIFT) & 31u);
+        int r = cur9 - dl;
+        if (r < 0) r += kHist;
+        const bool arr = tick >= dl && ((U.ring[m & M_PRE_MASK] >> r) & 1u);
+        U.carr[p] = arr ? 1 : 0;
+        if (arr) U.ev[atomicAdd(&U.counters[0], 1)] = p;
+    }
+}
+
+__device__ __forceinline__ void phase_release(const WorldArgs &d, const UnitMem &U, int64_t tick, int tid, int bs,
+                                              const float *tab) {
+    const int n = U.counters[0];
+    for (int i = tid; i < n; i += bs) {
+        const int p = U.ev[i];
+        const int es = U.cslot[p];
+        U.rel[p] = ((U.cmeta[p] >> M_KIND_SHIFT) & 3u) == KIND_INH ? d.sstate[es].w : release_world(d, es, tick, tab);
+    }
+}
+
+// Phase 3 for neuron n (state in s).
+__device__ __forceinline__ void phase_neuron(const WorldArgs &d, const UnitMem &U, int n, int t, int64_t tick,
+                                             int cur9, NeuronRegs &s, int *motor_cnt, TraceRegs &tr,
+                                             const float *tab) {
     const uint32_t f = U.nflag[n];
-    if (!(f & NF_ACTIVE)) return 0;
+    if (!(f & NF_ACTIVE)) return;
     const int slot = U.nslot[n];
     const int ib = U.inptr[n], ie = U.inptr[n + 1];
     float e0 = 0.0f, e1 = 0.0f, e2 = 0.0f, e3 = 0.0f, inh = 0.0f;
@@ -430,28 +477,17 @@ __device__ __forceinline__ int neuron_tick(const WorldArgs &d, const UnitMem &U,
         inh = d.pinh[slot];
     }
     uint32_t mod = 0;
-    int narr = 0;
     const float scale = U.scale[n];
     const bool traced = (f & WF_TRACED) != 0;
     for (int p = ib; p < ie; ++p) {
+        if (!U.carr[p]) continue;
         const uint32_t m = U.cmeta[p];
-        const int dl = (int)((m >> M_DELAY_SHIFT) & 31u);
-        int r = cur9 - dl;
-        if (r < 0) r += kHist;
-        const bool arr = tick >= dl && ((U.ring[m & M_PRE_MASK] >> r) & 1u);
-        U.carr[p] = arr ? 1 : 0;
-        if (!arr) continue;
-        ++narr;
-        const int es = U.cslot[p];
+        const float v = U.rel[p];
         const uint32_t kind = (m >> M_KIND_SHIFT) & 3u;
         if (kind == KIND_INH) {
-            const float v = d.sstate[es].w;
             inh += v;
             if (traced) { ++tr.ia; tr.in += v; }
-            continue;
-        }
-        const float v = release_world(d, es, tick, tab);
-        if (kind == KIND_MOD) {
+        } else if (kind == KIND_MOD) {
             if (v > 0) {
                 const uint32_t id = (m >> M_MODID_SHIFT) & 3u;
                 mod |= 1u << id;
@@ -481,7 +517,9 @@ __device__ __forceinline__ int neuron_tick(const WorldArgs &d, const UnitMem &U,
         float xg[16] = {};
         if (type == 2) { xg[0] = G.lp.calcium; xg[1] = G.lp.calcium_k; xg[2] = G.lp.h; xg[3] = G.lp.leak; }
         if (type == 3) { for (int k = 0; k < 8; ++k) xg[k] = G.prinz.g[k]; xg[8] = G.prinz_leak; }
-        s = heavy_tick(g, type, xg, d.nstate[slot].cell, s, cur, e0, e1, e2, e3, inh, tab);
+        float gg[16];
+        for (int k = 0; k < 16; ++k) gg[k] = g[k];
+        s = heavy_tick(gg, type, xg, d.nstate[slot].cell, s, cur, e0, e1, e2, e3, inh, tab);
     } else {
         adex_tick(g, type, f, s, cur, e0, e1, e2, e3, inh, tab);
     }
@@ -492,49 +530,65 @@ __device__ __forceinline__ int neuron_tick(const WorldArgs &d, const UnitMem &U,
     }
     const uint16_t bit = (uint16_t)(1u << cur9);
     U.ring[n] = s.spike ? (uint16_t)(U.ring[n] | bit) : (uint16_t)(U.ring[n] & ~bit);
-    // plasticity (src/main.cu:748-767), events only
-    if (!frozen && ie > ib) {
-        const bool post = s.spike != 0;
-        for (int p = ib; p < ie; ++p) {
-            const uint32_t m = U.cmeta[p];
-            if (!(m & M_PLASTIC)) continue;
-            const bool arr = U.carr[p] != 0;
-            const uint32_t prof = m >> M_PROF_SHIFT;
-            const int es = U.cslot[p];
-            uint32_t receptors = 0;
-            if (mod) receptors = d.sgene[es].receptors;
-            if (!arr && !post && !mod_relevant(prof, receptors, mod)) continue;
-            const float w0 = d.sgene[es].w0;
-            ref::SynapseState &Z = d.sstate[es];
-            SynPlast pl;
-            load_plast_ref(Z, pl);
-            plasticity_quiet(prof, w0, pl, t - U.clast[p] - 1);
-            plasticity_tick(prof, receptors, w0, pl, arr, post, s.depol, mod, tab);
-            store_plast_ref(Z, pl);
-            U.clast[p] = (int8_t)t;
-        }
-    }
-    return narr;
+    U.nspk[n] = s.spike ? 1 : 0;
+    U.nmod[n] = (uint8_t)mod;
+    U.ndepol[n] = s.depol;
 }
 
-// End of the step for neuron n: state, cleared accumulators, history, the
-// last tick's arrival flags, plasticity caught up to the last tick.
-__device__ __forceinline__ void finish_neuron(const WorldArgs &d, const UnitMem &U, int n, int base9, bool frozen,
-                                              const NeuronRegs &s) {
-    const uint32_t f = U.nflag[n];
-    if (!(f & NF_ACTIVE)) return;
+__device__ __forceinline__ void phase_plastic_events(const WorldArgs &d, const UnitMem &U, int ne, int tid, int bs) {
+    for (int p = tid; p < ne; p += bs) {
+        const uint32_t m = U.cmeta[p];
+        if (!(m & M_PLASTIC)) continue;
+        const int post = U.cpost[p];
+        if (U.nflag[post] & WF_FROZEN) continue;
+        const uint32_t mod = U.nmod[post];
+        bool ev = U.carr[p] || U.nspk[post];
+        if (!ev && mod) ev = mod_relevant(m >> M_PROF_SHIFT, d.sgene[U.cslot[p]].receptors, mod);
+        if (ev) U.ev[atomicAdd(&U.counters[1], 1)] = p;
+    }
+}
+
+__device__ __forceinline__ void phase_plasticity(const WorldArgs &d, const UnitMem &U, int t, int tid, int bs,
+                                                 const float *tab) {
+    const int n = U.counters[1];
+    for (int i = tid; i < n; i += bs) {
+        const int p = U.ev[i];
+        const uint32_t m = U.cmeta[p];
+        const int post = U.cpost[p];
+        const int es = U.cslot[p];
+        const ref::SynapseGene &G = d.sgene[es];
+        const uint32_t mod = U.nmod[post];
+        const uint32_t receptors = mod ? (uint32_t)G.receptors : 0u;
+        const uint32_t prof = m >> M_PROF_SHIFT;
+        const float w0 = G.w0;
+        ref::SynapseState &Z = d.sstate[es];
+        SynPlast pl;
+        load_plast_ref(Z, pl);
+        plasticity_quiet(prof, w0, pl, t - U.clast[p] - 1);
+        plasticity_tick(prof, receptors, w0, pl, U.carr[p] != 0, U.nspk[post] != 0, U.ndepol[post], mod, tab);
+        store_plast_ref(Z, pl);
+        U.clast[p] = (int8_t)t;
+    }
+}
+
+// End of the step for neuron n: state, cleared accumulators, history.
+__device__ __forceinline__ void finish_neuron(const WorldArgs &d, const UnitMem &U, int n, const NeuronRegs &s) {
+    if (!(U.nflag[n] & NF_ACTIVE)) return;
     const int slot = U.nslot[n];
     store_regs(d.nstate[slot], s);
     for (int b = 0; b < 4; ++b) d.pexc[(size_t)slot * 4 + b] = 0.0f;
     d.pinh[slot] = 0.0f;
     const uint16_t r = U.ring[n];
     for (int k = 0; k < kHist; ++k) d.hist[(size_t)k * d.ncap + slot] = (unsigned char)((r >> k) & 1u);
-    const int ib = U.inptr[n], ie = U.inptr[n + 1];
-    for (int p = ib; p < ie; ++p) {
+}
+// End of the step for every synapse: the last tick's arrival flag, plasticity
+// caught up to the last tick.
+__device__ __forceinline__ void finish_synapses(const WorldArgs &d, const UnitMem &U, int ne, int tid, int bs) {
+    for (int p = tid; p < ne; p += bs) {
         const uint32_t m = U.cmeta[p];
         const int es = U.cslot[p];
         d.sstate[es].arrived = U.carr[p];
-        if (!frozen && (m & M_PLASTIC)) {
+        if ((m & M_PLASTIC) && !(U.nflag[U.cpost[p]] & WF_FROZEN)) {
             const int q = kTicks - 1 - U.clast[p];
             if (q > 0) {
                 ref::SynapseState &Z = d.sstate[es];
@@ -545,7 +599,6 @@ __device__ __forceinline__ void finish_neuron(const WorldArgs &d, const UnitMem 
             }
         }
     }
-    (void)base9;
 }
 
 // Global float max (trace peak); order-independent.
@@ -564,9 +617,12 @@ __device__ __forceinline__ void atomic_fmax(float *p, float v) {
 
 extern __shared__ __align__(16) unsigned char w_smem[];
 
+constexpr int kClaim = 4;   // animals taken from the living list per claim
+
 // Small units: animals with at most kBlock neurons and kUnitEdges live
 // synapses, packed in claim order; larger ones are appended to `big`.
-__global__ void __launch_bounds__(kBlock, 2) world_tick_small(WorldArgs d, Cache c, int64_t first_tick, int *queue,
+__global__ void __launch_bounds__(kBlock, 2) world_tick_small(WorldArgs d, Cache c, int64_t first_tick,
+                                                              const int *alive, const int *nalive, int *queue,
                                                               int *big, int *big_count, int *status,
                                                               Counters *stats) {
     float *tab = reinterpret_cast<float *>(w_smem);                         // 256
@@ -576,31 +632,39 @@ __global__ void __launch_bounds__(kBlock, 2) world_tick_small(WorldArgs d, Cache
     float *scale = curv + kBlock;
     float *trx = scale + kBlock;
     float *tri = trx + kBlock;
-    int *nslot = reinterpret_cast<int *>(tri + kBlock);
+    float *ndepol = tri + kBlock;
+    float *rel = ndepol + kBlock;                                           // kUnitEdges
+    int *nslot = reinterpret_cast<int *>(rel + kUnitEdges);                 // kBlock
     int *inptr = nslot + kBlock;                                            // kBlock + 4
     uint32_t *cmeta = reinterpret_cast<uint32_t *>(inptr + kBlock + 4);     // kUnitEdges
     int *cslot = reinterpret_cast<int *>(cmeta + kUnitEdges);
-    uint16_t *ring = reinterpret_cast<uint16_t *>(cslot + kUnitEdges);      // kBlock
+    int *ev = cslot + kUnitEdges;                                           // kUnitEdges
+    uint16_t *cpost = reinterpret_cast<uint16_t *>(ev + kUnitEdges);        // kUnitEdges
+    uint16_t *ring = cpost + kUnitEdges;                                    // kBlock
     uint8_t *nani = reinterpret_cast<uint8_t *>(ring + kBlock);             // kBlock
-    uint8_t *carr = nani + kBlock;                                          // kUnitEdges
+    uint8_t *nspk = nani + kBlock;                                          // kBlock
+    uint8_t *nmod = nspk + kBlock;                                          // kBlock
+    uint8_t *carr = nmod + kBlock;                                          // kUnitEdges
     int8_t *clast = reinterpret_cast<int8_t *>(carr + kUnitEdges);          // kUnitEdges
     __shared__ int ua_a[kUnitAnimals], ua_n0[kUnitAnimals + 1], ua_e0[kUnitAnimals + 1], ua_f[kUnitAnimals];
     __shared__ int ua_motor[kUnitAnimals * kM];
     __shared__ int q_a[32], q_nn[32], q_nl[32];
     __shared__ int q_n, q_i, q_done, s_nu, s_ntot, s_etot;
+    __shared__ int s_cnt[2];
     __shared__ unsigned long long s_events;
 
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31, warp = tid >> 5;
     {
         const float *src = nsx::exp2f_table();
-        for (int i = tid; i < 256; i += blockDim.x) tab[i] = src[i];
+        for (int i = tid; i < 256; i += bs) tab[i] = src[i];
     }
     if (tid == 0) { q_n = 0; q_i = 0; q_done = 0; }
     __syncthreads();
+    const int n_alive = *nalive;
     UnitMem U;
-    U.gene = gene; U.gs = kBlock; U.nflag = nflag; U.cur = curv; U.scale = scale; U.ring = ring; U.inptr = inptr;
-    U.cmeta = cmeta; U.cslot = cslot; U.carr = carr; U.clast = clast; U.nslot = nslot; U.nani = nani;
-    U.trx = trx; U.tri = tri;
+    U.gene = gene; U.gs = kBlock; U.nflag = nflag; U.cur = curv; U.scale = scale; U.ndepol = ndepol; U.rel = rel;
+    U.trx = trx; U.tri = tri; U.inptr = inptr; U.cmeta = cmeta; U.cslot = cslot; U.ev = ev; U.counters = s_cnt;
+    U.nslot = nslot; U.cpost = cpost; U.ring = ring; U.carr = carr; U.clast = clast; U.nspk = nspk; U.nmod = nmod;
     const int base9 = (int)(first_tick % kHist);
     for (;;) {
         // ---- form the next unit (warp 0) ----
@@ -609,14 +673,14 @@ __global__ void __launch_bounds__(kBlock, 2) world_tick_small(WorldArgs d, Cache
             for (;;) {
                 if (q_i >= q_n && !q_done) {
                     int base = 0;
-                    if (lane == 0) base = atomicAdd(queue, 32);
+                    if (lane == 0) base = atomicAdd(queue, kClaim);
                     base = __shfl_sync(0xffffffffu, base, 0);
-                    const int a = base + lane;
                     bool ok = false;
-                    int nn = 0, nl = 0;
-                    if (a < d.P && d.animals[a].alive == 1) {
+                    int a = -1, nn = 0, nl = 0;
+                    if (lane < kClaim && base + lane < n_alive) {
+                        a = alive[base + lane];
                         if (!compiled(d, c, a)) {
-                            atomicOr(status, ST_LIST);    // compile failed (status set there)
+                            atomicOr(status, ST_LIST);    // compile failed (its own status bit is set too)
                         } else {
                             nn = c.nn[a]; nl = c.nl[a];
                             if (nn > kBlock || nl > kUnitEdges) big[atomicAdd(big_count, 1)] = a;
@@ -629,7 +693,7 @@ __global__ void __launch_bounds__(kBlock, 2) world_tick_small(WorldArgs d, Cache
                         q_a[pos] = a; q_nn[pos] = nn; q_nl[pos] = nl;
                     }
                     __syncwarp();
-                    if (lane == 0) { q_n = __popc(mk); q_i = 0; if (base + 32 >= d.P) q_done = 1; }
+                    if (lane == 0) { q_n = __popc(mk); q_i = 0; if (base + kClaim >= n_alive) q_done = 1; }
                     __syncwarp();
                     continue;
                 }
@@ -646,24 +710,25 @@ __global__ void __launch_bounds__(kBlock, 2) world_tick_small(WorldArgs d, Cache
                     break;
                 }
             }
-            if (lane == 0) { s_nu = nu; s_ntot = ntot; s_etot = etot; ua_n0[nu] = ntot; ua_e0[nu] = etot; s_events = 0; }
+            if (lane == 0) {
+                s_nu = nu; s_ntot = ntot; s_etot = etot; ua_n0[nu] = ntot; ua_e0[nu] = etot;
+                s_events = 0; s_cnt[0] = 0; s_cnt[1] = 0;
+            }
         }
         __syncthreads();
-        const int nu = s_nu, ntot = s_ntot;
+        const int nu = s_nu, ntot = s_ntot, etot = s_etot;
         if (nu == 0) break;
         // ---- load the compiled animals ----
         for (int i = 0; i < nu; ++i) {
             const int a = ua_a[i], n0 = ua_n0[i], e0 = ua_e0[i];
             const int nn = ua_n0[i + 1] - n0, nl = ua_e0[i + 1] - e0;
             const int *R = c.arena + c.off[a];
-            for (int k = tid; k < nn; k += blockDim.x) { nslot[n0 + k] = R[k]; nani[n0 + k] = (uint8_t)i; }
-            for (int k = tid; k <= nn; k += blockDim.x) inptr[n0 + k] = e0 + R[nn + k];
-            const int *M = R + 2 * nn + 1;
-            for (int k = tid; k < nl; k += blockDim.x) {
-                cmeta[e0 + k] = (uint32_t)M[k] + (uint32_t)n0;    // pre index: animal-local -> unit-local
-                cslot[e0 + k] = M[nl + k];
-                carr[e0 + k] = 0;
-                clast[e0 + k] = -1;
+            for (int k = tid; k < nn; k += bs) { nslot[n0 + k] = R[k]; nani[n0 + k] = (uint8_t)i; }
+            for (int k = tid; k <= nn; k += bs) inptr[n0 + k] = e0 + R[nn + k];
+            const int *Mt = R + 2 * nn + 1;
+            for (int k = tid; k < nl; k += bs) {
+                cmeta[e0 + k] = (uint32_t)Mt[k] + (uint32_t)n0;    // pre index: animal-local -> unit-local
+                cslot[e0 + k] = Mt[nl + k];
             }
             if (tid < kM) ua_motor[i * kM + tid] = 0;
             if (tid == 0) ua_f[i] = (frozen_animal(d, a) ? UA_FROZEN : 0) | (a == d.trace ? UA_TRACED : 0);
@@ -671,23 +736,32 @@ __global__ void __launch_bounds__(kBlock, 2) world_tick_small(WorldArgs d, Cache
         __syncthreads();
         NeuronRegs s = {};
         TraceRegs tr = {0, 0, 0, 0.0f, 0.0f, -INFINITY};
-        bool fz = false;
         if (tid < ntot) {
-            const int i = nani[tid], a = ua_a[i];
-            fz = (ua_f[i] & UA_FROZEN) != 0;
-            setup_neuron(d, U, tid, nslot[tid], a, (ua_f[i] & UA_TRACED) != 0, base9, tab);
+            const int i = nani[tid];
+            setup_neuron(d, U, tid, nslot[tid], ua_a[i], (ua_f[i] & UA_TRACED) != 0, (ua_f[i] & UA_FROZEN) != 0, tab);
             load_regs(d.nstate[nslot[tid]], s);
         }
         __syncthreads();
         int narr = 0;
         for (int t = 0; t < kTicks; ++t) {
             const int cur9 = (base9 + t) % kHist;
-            if (tid < ntot)
-                narr += neuron_tick(d, U, tid, t, first_tick + t, cur9, fz, s, &ua_motor[nani[tid] * kM], tr, tab);
+            const int64_t tick = first_tick + t;
+            phase_arrivals(U, etot, cur9, tick, tid, bs);
+            __syncthreads();
+            if (tid == 0) { narr += s_cnt[0]; s_cnt[1] = 0; }
+            phase_release(d, U, tick, tid, bs, tab);
+            __syncthreads();
+            if (tid == 0) s_cnt[0] = 0;
+            if (tid < ntot) phase_neuron(d, U, tid, t, tick, cur9, s, &ua_motor[nani[tid] * kM], tr, tab);
+            __syncthreads();
+            phase_plastic_events(d, U, etot, tid, bs);
+            __syncthreads();
+            phase_plasticity(d, U, t, tid, bs, tab);
             __syncthreads();
         }
+        finish_synapses(d, U, etot, tid, bs);
         if (tid < ntot) {
-            finish_neuron(d, U, tid, base9, fz, s);
+            finish_neuron(d, U, tid, s);
             const uint32_t f = nflag[tid];
             if (f & WF_TRACED) {
                 const int m = (int)((f >> WF_MOTOR_SHIFT) & 7u) - 1;
@@ -699,8 +773,7 @@ __global__ void __launch_bounds__(kBlock, 2) world_tick_small(WorldArgs d, Cache
                 tri[tid] = tr.in;
             }
         }
-        for (int o = 16; o > 0; o >>= 1) narr += __shfl_down_sync(0xffffffffu, narr, o);
-        if (lane == 0 && narr) atomicAdd(&s_events, (unsigned long long)narr);
+        if (tid == 0 && narr) s_events = (unsigned long long)narr;
         __syncthreads();
         if (tid < nu) {
             const int a = ua_a[tid];
@@ -720,25 +793,27 @@ __global__ void __launch_bounds__(kBlock, 2) world_tick_small(WorldArgs d, Cache
         if (tid == 0) {
             atomicAdd(&stats->animals, (unsigned long long)nu);
             atomicAdd(&stats->neurons, (unsigned long long)ntot);
-            atomicAdd(&stats->synapses, (unsigned long long)s_etot);
+            atomicAdd(&stats->synapses, (unsigned long long)etot);
             atomicAdd(&stats->events, s_events);
         }
         __syncthreads();
     }
 }
 
-// Big animals: one per CTA, per-neuron arrays and register state in a global
-// slab, CSR read in place from the arena.
+// Big animals: one per CTA, per-neuron and per-synapse arrays and the
+// neurons' register state in a global slab, CSR read in place from the arena.
 struct BigSlab {
     float *gene;        // [16][max_n]
     uint32_t *nflag;
-    float *cur, *scale, *trx, *tri;
+    float *cur, *scale, *trx, *tri, *ndepol;
     uint16_t *ring;
-    uint8_t *nani;      // zeros
-    int *inptr;         // max_n + 1 (arena offsets converted)
-    uint8_t *carr;
-    int8_t *clast;
-    uint32_t *regs;     // [14][max_n] NeuronRegs words
+    uint8_t *nspk, *nmod;
+    float *rel;         // max_e
+    int *ev;            // max_e
+    uint16_t *cpost;    // max_e
+    uint8_t *carr;      // max_e
+    int8_t *clast;      // max_e
+    uint32_t *regs;     // [14][max_n] NeuronRegs words and the trace peak
     int max_n, max_e;
 };
 
@@ -762,33 +837,28 @@ __device__ __forceinline__ void slab_store(const BigSlab &B, int n, const Neuron
     B.regs[9 * M + n] = __float_as_uint(s.d2); B.regs[10 * M + n] = __float_as_uint(s.d3);
     B.regs[11 * M + n] = (uint32_t)s.total; B.regs[12 * M + n] = s.spike;
 }
-__device__ __forceinline__ void slab_trace_store(const BigSlab &B, int n, const TraceRegs &t) {
-    B.trx[n] = t.en; B.tri[n] = t.in;
-    const int M = B.max_n;
-    B.regs[13 * M + n] = __float_as_uint(t.pk);
-}
 
 __global__ void __launch_bounds__(kBigBlock) world_tick_big(WorldArgs d, Cache c, int64_t first_tick, const int *big,
                                                             const int *big_count, int *queue, BigSlab slab,
                                                             Counters *stats) {
     float *tab = reinterpret_cast<float *>(w_smem);
-    __shared__ int s_i, s_motor[kM];
+    __shared__ int s_i, s_motor[kM], s_cnt[2];
     __shared__ unsigned long long s_events;
-    const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31;
+    const int tid = threadIdx.x, bs = blockDim.x;
     {
         const float *src = nsx::exp2f_table();
         for (int i = tid; i < 256; i += bs) tab[i] = src[i];
     }
     BigSlab B = slab;
-    const size_t sn = (size_t)blockIdx.x;
-    B.gene += sn * 16 * slab.max_n; B.nflag += sn * slab.max_n; B.cur += sn * slab.max_n;
-    B.scale += sn * slab.max_n; B.trx += sn * slab.max_n; B.tri += sn * slab.max_n; B.ring += sn * slab.max_n;
-    B.nani += sn * slab.max_n; B.inptr += sn * (slab.max_n + 1); B.carr += sn * slab.max_e;
-    B.clast += sn * slab.max_e; B.regs += sn * 14 * slab.max_n;
+    const size_t sn = (size_t)blockIdx.x, MN = (size_t)slab.max_n, ME = (size_t)slab.max_e;
+    B.gene += sn * 16 * MN; B.nflag += sn * MN; B.cur += sn * MN; B.scale += sn * MN; B.trx += sn * MN;
+    B.tri += sn * MN; B.ndepol += sn * MN; B.ring += sn * MN; B.nspk += sn * MN; B.nmod += sn * MN;
+    B.rel += sn * ME; B.ev += sn * ME; B.cpost += sn * ME; B.carr += sn * ME; B.clast += sn * ME;
+    B.regs += sn * 14 * MN;
     const int nbig = *big_count;
     const int base9 = (int)(first_tick % kHist);
     for (;;) {
-        if (tid == 0) { s_i = atomicAdd(queue, 1); s_events = 0; }
+        if (tid == 0) { s_i = atomicAdd(queue, 1); s_events = 0; s_cnt[0] = 0; s_cnt[1] = 0; }
         if (tid < kM) s_motor[tid] = 0;
         __syncthreads();
         const int i = s_i;
@@ -798,50 +868,62 @@ __global__ void __launch_bounds__(kBigBlock) world_tick_big(WorldArgs d, Cache c
         const int *R = c.arena + c.off[a];
         const bool fz = frozen_animal(d, a), traced = a == d.trace;
         UnitMem U;
-        U.gene = B.gene; U.gs = B.max_n; U.nflag = B.nflag; U.cur = B.cur; U.scale = B.scale; U.ring = B.ring;
-        U.inptr = R + nn; U.cmeta = reinterpret_cast<const uint32_t *>(R + 2 * nn + 1); U.cslot = R + 2 * nn + 1 + nl;
-        U.carr = B.carr; U.clast = B.clast; U.nslot = R; U.nani = B.nani; U.trx = B.trx; U.tri = B.tri;
+        U.gene = B.gene; U.gs = B.max_n; U.nflag = B.nflag; U.cur = B.cur; U.scale = B.scale; U.ndepol = B.ndepol;
+        U.rel = B.rel; U.trx = B.trx; U.tri = B.tri; U.inptr = R + nn;
+        U.cmeta = reinterpret_cast<const uint32_t *>(R + 2 * nn + 1); U.cslot = R + 2 * nn + 1 + nl;
+        U.ev = B.ev; U.counters = s_cnt; U.nslot = R; U.cpost = B.cpost; U.ring = B.ring; U.carr = B.carr;
+        U.clast = B.clast; U.nspk = B.nspk; U.nmod = B.nmod;
         for (int n = tid; n < nn; n += bs) {
-            setup_neuron(d, U, n, R[n], a, traced, base9, tab);
+            setup_neuron(d, U, n, R[n], a, traced, fz, tab);
             NeuronRegs s;
             load_regs(d.nstate[R[n]], s);
             slab_store(B, n, s);
-            B.regs[13 * B.max_n + n] = __float_as_uint(-INFINITY);
+            B.regs[13 * MN + n] = __float_as_uint(-INFINITY);
         }
-        for (int p = tid; p < nl; p += bs) { B.carr[p] = 0; B.clast[p] = -1; }
         __syncthreads();
         int narr = 0;
         for (int t = 0; t < kTicks; ++t) {
             const int cur9 = (base9 + t) % kHist;
+            const int64_t tick = first_tick + t;
+            phase_arrivals(U, nl, cur9, tick, tid, bs);
+            __syncthreads();
+            if (tid == 0) { narr += s_cnt[0]; s_cnt[1] = 0; }
+            phase_release(d, U, tick, tid, bs, tab);
+            __syncthreads();
+            if (tid == 0) s_cnt[0] = 0;
             for (int n = tid; n < nn; n += bs) {
                 NeuronRegs s;
                 slab_load(B, n, s);
-                TraceRegs tr = {0, 0, 0, B.trx[n], B.tri[n], __uint_as_float(B.regs[13 * B.max_n + n])};
-                const int ea0 = 0;
-                narr += neuron_tick(d, U, n, t, first_tick + t, cur9, fz, s, s_motor, tr, tab);
+                TraceRegs tr = {0, 0, 0, B.trx[n], B.tri[n], __uint_as_float(B.regs[13 * MN + n])};
+                phase_neuron(d, U, n, t, tick, cur9, s, s_motor, tr, tab);
                 slab_store(B, n, s);
-                if (tr.ea != ea0 || tr.er || tr.ia) {
+                if (tr.ea || tr.er || tr.ia) {
                     const int m = (int)((U.nflag[n] >> WF_MOTOR_SHIFT) & 7u) - 1;
                     if (tr.ea) atomicAdd(&d.tr_ea[m], tr.ea);
                     if (tr.er) atomicAdd(&d.tr_er[m], tr.er);
                     if (tr.ia) atomicAdd(&d.tr_ia[m], tr.ia);
                 }
-                slab_trace_store(B, n, tr);
+                B.trx[n] = tr.en; B.tri[n] = tr.in;
+                B.regs[13 * MN + n] = __float_as_uint(tr.pk);
             }
             __syncthreads();
+            phase_plastic_events(d, U, nl, tid, bs);
+            __syncthreads();
+            phase_plasticity(d, U, t, tid, bs, tab);
+            __syncthreads();
         }
+        finish_synapses(d, U, nl, tid, bs);
         for (int n = tid; n < nn; n += bs) {
             NeuronRegs s;
             slab_load(B, n, s);
-            finish_neuron(d, U, n, base9, fz, s);
+            finish_neuron(d, U, n, s);
             const uint32_t f = U.nflag[n];
             if (f & WF_TRACED) {
                 const int m = (int)((f >> WF_MOTOR_SHIFT) & 7u) - 1;
-                atomic_fmax(&d.tr_pk[m], __uint_as_float(B.regs[13 * B.max_n + n]));
+                atomic_fmax(&d.tr_pk[m], __uint_as_float(B.regs[13 * MN + n]));
             }
         }
-        for (int o = 16; o > 0; o >>= 1) narr += __shfl_down_sync(0xffffffffu, narr, o);
-        if (lane == 0 && narr) atomicAdd(&s_events, (unsigned long long)narr);
+        if (tid == 0) s_events = (unsigned long long)narr;
         __syncthreads();
         if (tid == 0) {
             for (int m = 0; m < kM; ++m)
@@ -922,8 +1004,10 @@ public:
         NSB_CHECK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
         const PhysConst K = make_constants();
         NSB_CHECK(cudaMemcpyToSymbol(c_K, &K, sizeof(PhysConst)));
-        small_smem_ = 256 * 4 + 16 * kBlock * 4 + 5 * kBlock * 4 + kBlock * 4 + (kBlock + 4) * 4 + 2 * kUnitEdges * 4 +
-                      kBlock * 2 + kBlock + 2 * kUnitEdges;
+        // tab, gene records, 6 per-neuron floats, rel, nslot, inptr, cmeta, cslot,
+        // ev, cpost, ring, 3 per-neuron bytes, carr, clast
+        small_smem_ = 256 * 4 + 16 * kBlock * 4 + 6 * kBlock * 4 + kUnitEdges * 4 + kBlock * 4 + (kBlock + 4) * 4 +
+                      3 * kUnitEdges * 4 + kUnitEdges * 2 + kBlock * 2 + 3 * kBlock + 2 * kUnitEdges;
         NSB_CHECK(cudaFuncSetAttribute(world_tick_small, cudaFuncAttributeMaxDynamicSharedMemorySize, small_smem_));
         int occ = 0;
         NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, world_tick_small, kBlock, small_smem_));
@@ -955,16 +1039,21 @@ public:
         b_.scale = dev_alloc<float>(owned_, bg * max_n);
         b_.trx = dev_alloc<float>(owned_, bg * max_n);
         b_.tri = dev_alloc<float>(owned_, bg * max_n);
+        b_.ndepol = dev_alloc<float>(owned_, bg * max_n);
         b_.ring = dev_alloc<uint16_t>(owned_, bg * max_n);
-        b_.nani = dev_alloc<uint8_t>(owned_, bg * max_n);
-        NSB_CHECK(cudaMemset(b_.nani, 0, bg * max_n));
-        b_.inptr = dev_alloc<int>(owned_, bg * (max_n + 1));
+        b_.nspk = dev_alloc<uint8_t>(owned_, bg * max_n);
+        b_.nmod = dev_alloc<uint8_t>(owned_, bg * max_n);
+        b_.rel = dev_alloc<float>(owned_, bg * max_e);
+        b_.ev = dev_alloc<int>(owned_, bg * max_e);
+        b_.cpost = dev_alloc<uint16_t>(owned_, bg * max_e);
         b_.carr = dev_alloc<uint8_t>(owned_, bg * max_e);
         b_.clast = dev_alloc<int8_t>(owned_, bg * max_e);
         b_.regs = dev_alloc<uint32_t>(owned_, bg * 14 * max_n);
         list_ = dev_alloc<int>(owned_, P);
+        alive_ = dev_alloc<int>(owned_, P);
         big_ = dev_alloc<int>(owned_, P);
-        ints_ = dev_alloc<int>(owned_, 8);   // 0 compile count, 1 small queue, 2 big count, 3 big queue, 4 status
+        // 0 compile count, 1 small queue, 2 big count, 3 big queue, 4 status, 5 living animals
+        ints_ = dev_alloc<int>(owned_, 8);
         stats_ = dev_alloc<Counters>(owned_, 1);
         NSB_CHECK(cudaMallocHost(&h_ints_, 8 * sizeof(int)));
         NSB_CHECK(cudaMallocHost(&h_stats_, sizeof(Counters)));
@@ -982,10 +1071,11 @@ public:
         cudaStream_t st = 0;
         NSB_CHECK(cudaMemsetAsync(ints_, 0, 8 * sizeof(int), st));
         NSB_CHECK(cudaMemsetAsync(stats_, 0, sizeof(Counters), st));
-        world_select<<<std::max(1, std::min((d_.P + 255) / 256, sms_ * 8)), 256, 0, st>>>(d_, c_, list_, ints_);
+        world_select<<<std::max(1, std::min((d_.P + 255) / 256, sms_ * 8)), 256, 0, st>>>(d_, c_, list_, ints_,
+                                                                                            alive_, ints_ + 5);
         world_compile<<<compile_grid_, 32 * kCompileWarps, 0, st>>>(d_, c_, list_, ints_, s_, ints_ + 4);
-        world_tick_small<<<small_grid_, kBlock, small_smem_, st>>>(d_, c_, first_tick, ints_ + 1, big_, ints_ + 2,
-                                                                  ints_ + 4, stats_);
+        world_tick_small<<<small_grid_, kBlock, small_smem_, st>>>(d_, c_, first_tick, alive_, ints_ + 5, ints_ + 1,
+                                                                  big_, ints_ + 2, ints_ + 4, stats_);
         world_tick_big<<<big_grid_, kBigBlock, 1024, st>>>(d_, c_, first_tick, big_, ints_ + 2, ints_ + 3, b_, stats_);
         NSB_CHECK(cudaGetLastError());
         NSB_CHECK(cudaMemcpyAsync(h_ints_, ints_, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1026,7 +1116,7 @@ private:
     Scratch s_{};
     BigSlab b_{};
     std::vector<void *> owned_;
-    int *list_ = nullptr, *big_ = nullptr, *ints_ = nullptr, *h_ints_ = nullptr;
+    int *list_ = nullptr, *alive_ = nullptr, *big_ = nullptr, *ints_ = nullptr, *h_ints_ = nullptr;
     Counters *stats_ = nullptr, *h_stats_ = nullptr, last_{};
     int sms_ = 148, small_smem_ = 0, small_grid_ = 0, big_grid_ = 0, compile_grid_ = 0;
 };

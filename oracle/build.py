@@ -114,8 +114,11 @@ def build_ref(verbose=False, gpu=True):
         out = REF_OUT / "libns_ref_world_cr.so"
         if _stale(out, [world_src, HERE / "ref_world_harness.cu", HERE / "ref_cr_shim_cuda.h", CSRC / "ns_crmath.h"]):
             stub = REF_OUT / "stub_include"
+            # -maxrregcount=128: the reference launches 512-thread CTAs
+            # (NEURAL_BLOCK), which can hold at most 128 registers per thread.
             _run(["nvcc", "-O3", "-std=c++17", "--fmad=false", "--prec-div=true", "--prec-sqrt=true",
-                  "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC,-ffp-contract=off",
+                  "-maxrregcount=128", "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+                  "-Xcompiler", "-fPIC,-ffp-contract=off",
                   "-I", stub, "-I", REFERENCE / "src", "-I", CSRC, "-include", HERE / "ref_cr_shim_cuda.h",
                   "-DLIVE_ASSET_DIR=\"/nonexistent\"", HERE / "ref_world_harness.cu", REFERENCE / "src" / "live_view.cpp",
                   "-o", out, "-lz"])

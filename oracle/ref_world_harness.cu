@@ -229,28 +229,41 @@ int neural_stage(World &w, int64_t step, int &neuron_count, int &block_count, in
         cudaMemcpy(&block_count, d.block_animal_count, sizeof(int), cudaMemcpyDeviceToHost);
         cudaMemcpy(&medium_count, d.medium_animal_count, sizeof(int), cudaMemcpyDeviceToHost);
     }
+    // A failed launch returns 100 x the CUDA error + the launch site
+    // (1 selection, 2/3 block tiers, 4 delivery, 5 fused plasticity+delivery,
+    // 6 neuron_step, 7 plasticity).
+#define NS_SITE(k) do { const cudaError_t e_ = cudaGetLastError(); if (e_ != cudaSuccess) return 100 * (int)e_ + (k); } while (0)
+    NS_SITE(1);
     if (block_count)
         brain_block_step<BLOCK_BRAIN_NEURONS, BLOCK_BRAIN_SYNAPSES, false>
             <<<block_count, 128, sizeof(BlockBrain<BLOCK_BRAIN_NEURONS, BLOCK_BRAIN_SYNAPSES, false>)>>>(
                 d, d.block_animals, block_count, (step - 1) * TICKS);
+    NS_SITE(2);
     if (medium_count)
         brain_block_step<MEDIUM_BRAIN_NEURONS, MEDIUM_BRAIN_SYNAPSES, false>
             <<<medium_count, 128, sizeof(BlockBrain<MEDIUM_BRAIN_NEURONS, MEDIUM_BRAIN_SYNAPSES, false>)>>>(
                 d, d.medium_animals, medium_count, (step - 1) * TICKS);
+    NS_SITE(3);
     for (int t = 0; t < TICKS; ++t) {
         const int64_t tick = (step - 1) * TICKS + t;
         if (synapse_count) {
-            if (t == 0)
+            if (t == 0) {
                 synapse_delivery<<<(synapse_count + NEURAL_BLOCK - 1) / NEURAL_BLOCK, NEURAL_BLOCK>>>(d, tick, synapse_count);
-            else
+                NS_SITE(4);
+            } else {
                 synapse_plasticity_delivery<<<(synapse_count + NEURAL_BLOCK - 1) / NEURAL_BLOCK, NEURAL_BLOCK>>>(
                     d, tick - 1, tick, synapse_count);
+                NS_SITE(5);
+            }
         }
         if (neuron_count)
             neuron_step<<<(neuron_count + NEURAL_BLOCK - 1) / NEURAL_BLOCK, NEURAL_BLOCK>>>(d, tick, neuron_count);
+        NS_SITE(6);
         if (synapse_count && t == TICKS - 1)
             synapse_plasticity<<<(synapse_count + NEURAL_BLOCK - 1) / NEURAL_BLOCK, NEURAL_BLOCK>>>(d, tick, synapse_count);
+        NS_SITE(7);
     }
+#undef NS_SITE
     return (int)cudaGetLastError();
 }
 
@@ -346,6 +359,27 @@ void ref_world_pools_destroy(void *p) {
                     d.block_animals, d.block_animal_count, d.medium_animals, d.medium_animal_count, h->w.select_tmp};
     for (void *q : ptrs) cudaFree(q);
     delete h;
+}
+
+// Launch limits of the neural kernels as this build compiled them, 4 values
+// each (registers per thread, maximum threads per CTA, local bytes per
+// thread, static shared bytes): synapse_delivery, synapse_plasticity_delivery,
+// neuron_step, synapse_plasticity, then the two brain_block_step tiers.
+int ref_world_kernel_limits(int *out) {
+    const void *k[6] = {(const void *)synapse_delivery, (const void *)synapse_plasticity_delivery,
+                        (const void *)neuron_step, (const void *)synapse_plasticity,
+                        (const void *)brain_block_step<BLOCK_BRAIN_NEURONS, BLOCK_BRAIN_SYNAPSES, false>,
+                        (const void *)brain_block_step<MEDIUM_BRAIN_NEURONS, MEDIUM_BRAIN_SYNAPSES, false>};
+    for (int i = 0; i < 6; ++i) {
+        cudaFuncAttributes a{};
+        const cudaError_t e = cudaFuncGetAttributes(&a, k[i]);
+        if (e != cudaSuccess) return -(int)e;
+        out[4 * i] = a.numRegs;
+        out[4 * i + 1] = a.maxThreadsPerBlock;
+        out[4 * i + 2] = (int)a.localSizeBytes;
+        out[4 * i + 3] = (int)a.sharedSizeBytes;
+    }
+    return 6;
 }
 
 // Layout of the Animal and PlasticityCohort fields the neural stage reads, as
