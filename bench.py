@@ -602,7 +602,7 @@ def run_serve(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
-def world_population(nsb, population):
+def world_population(nsb, population, founders=2048):
     """World pools at the reference build's capacities (32,768 animals,
     4,194,304 neuron and 8,388,608 synapse slots). "founders": 2,048 founders
     of 32-96 neurons with 4-12 synapses per neuron (config 2); "full": the
@@ -610,7 +610,7 @@ def world_population(nsb, population):
     world's 1-8 ms ring, its 8 input channels as world senses 0-7)."""
     W = nsb.world
     if population == "founders":
-        batch = nsb.workloads.world_founders(seed=2, founders=2048)
+        batch = nsb.workloads.world_founders(seed=2, founders=founders)
     else:
         full = workload(nsb, 2)
         sr = full.synapse_rows.copy()
@@ -638,7 +638,7 @@ def run_world_stage(args, rank, world, local_rank):
     sys.path.insert(0, str(ROOT))
     nsb = load_package()
     W = nsb.world
-    batch, pools = world_population(nsb, args.world_population)
+    batch, pools = world_population(nsb, args.world_population, args.world_founders)
     N, E, B = int(batch.neuron_offsets[-1]), int(batch.synapse_offsets[-1]), batch.brains
     stage = W.World(pools)
     counter = [0]
@@ -675,7 +675,8 @@ def run_world_stage(args, rank, world, local_rank):
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (Philox4x32-10, seed 2)",
-            "config": {"workload": f"world_{args.world_population}", "animals": B, "neurons": N, "synapses": E,
+            "config": {"workload": (f"world_founders_{B}" if args.world_population == "founders" else "world_full"),
+                       "animals": B, "neurons": N, "synapses": E,
                        "ticks_per_step": 16, "delays_ms": "1-8",
                        "pools": "reference layouts at the reference capacities (32,768 / 4,194,304 / 8,388,608)",
                        "step": "nsb_world_neural_step + nsb_world_homeostasis (5 kernels, one host sync)",
@@ -782,6 +783,7 @@ def main():
     ap.add_argument("--world", action="store_true",
                     help="the world simulator's neural stage on its own pools (config 2)")
     ap.add_argument("--world-population", default="founders", choices=["founders", "full"])
+    ap.add_argument("--world-founders", type=int, default=2048, help="founders of the config-2 population")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus if "RANK" in os.environ else 1))

@@ -51,8 +51,17 @@ void set_error(const char *message);   // ns_abi.cu
 namespace {
 
 constexpr int kS = 19, kM = 5, kHist = 9, kTicks = 16, kContact = 16;
-constexpr int kBlock = 256;          // small units: one thread per neuron
-constexpr int kUnitEdges = 2048;     // live synapses of a small unit (shared memory)
+#ifndef NSB_WORLD_BLOCK
+#define NSB_WORLD_BLOCK 256
+#endif
+#ifndef NSB_WORLD_EDGES
+#define NSB_WORLD_EDGES 2048
+#endif
+#ifndef NSB_WORLD_MIN_CTAS
+#define NSB_WORLD_MIN_CTAS 2
+#endif
+constexpr int kBlock = NSB_WORLD_BLOCK;      // small units: one thread per neuron
+constexpr int kUnitEdges = NSB_WORLD_EDGES;  // live synapses of a small unit (shared memory)
 constexpr int kUnitAnimals = 32;
 constexpr int kBigBlock = 512;
 constexpr int kCompileWarps = 4;     // compile kernel: warps per CTA, one animal per warp at a time
@@ -621,7 +630,7 @@ constexpr int kClaim = 4;   // animals taken from the living list per claim
 
 // Small units: animals with at most kBlock neurons and kUnitEdges live
 // synapses, packed in claim order; larger ones are appended to `big`.
-__global__ void __launch_bounds__(kBlock, 2) world_tick_small(WorldArgs d, Cache c, int64_t first_tick,
+__global__ void __launch_bounds__(kBlock, NSB_WORLD_MIN_CTAS) world_tick_small(WorldArgs d, Cache c, int64_t first_tick,
                                                               const int *alive, const int *nalive, int *queue,
                                                               int *big, int *big_count, int *status,
                                                               Counters *stats) {
