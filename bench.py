@@ -602,7 +602,7 @@ def run_serve(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
-def world_population(nsb, population, founders=2048):
+def world_population(nsb, population, founders=2048, compact=False):
     """World pools at the reference build's capacities (32,768 animals,
     4,194,304 neuron and 8,388,608 synapse slots). "founders": 2,048 founders
     of 32-96 neurons with 4-12 synapses per neuron (config 2); "full": the
@@ -620,8 +620,13 @@ def world_population(nsb, population, founders=2048):
         batch = nsb.workloads.Batch(full.neuron_rows, sr, full.neuron_offsets, full.synapse_offsets, full.motors, 19,
                                     8, "batched_uneven_world", senses, 230.0, {})
     recs = W.records_from_gpu(batch, np.arange(batch.brains, dtype=np.uint32) + 1)
-    pools = W.place_population(batch, *recs, animal_capacity=32768, neuron_capacity=4194304,
-                               synapse_capacity=8388608)
+    if compact:     # pools sized to the population (profiler captures; the reference needs its full capacities)
+        N, E = int(batch.neuron_offsets[-1]), int(batch.synapse_offsets[-1])
+        pools = W.place_population(batch, *recs, animal_capacity=batch.brains + 64, neuron_capacity=N + 4096,
+                                   synapse_capacity=E + 8192)
+    else:
+        pools = W.place_population(batch, *recs, animal_capacity=32768, neuron_capacity=4194304,
+                                   synapse_capacity=8388608)
     return batch, pools
 
 
@@ -638,7 +643,7 @@ def run_world_stage(args, rank, world, local_rank):
     sys.path.insert(0, str(ROOT))
     nsb = load_package()
     W = nsb.world
-    batch, pools = world_population(nsb, args.world_population, args.world_founders)
+    batch, pools = world_population(nsb, args.world_population, args.world_founders, args.world_compact)
     N, E, B = int(batch.neuron_offsets[-1]), int(batch.synapse_offsets[-1]), batch.brains
     stage = W.World(pools)
     counter = [0]
@@ -678,7 +683,8 @@ def run_world_stage(args, rank, world, local_rank):
             "config": {"workload": (f"world_founders_{B}" if args.world_population == "founders" else "world_full"),
                        "animals": B, "neurons": N, "synapses": E,
                        "ticks_per_step": 16, "delays_ms": "1-8",
-                       "pools": "reference layouts at the reference capacities (32,768 / 4,194,304 / 8,388,608)",
+                       "pools": ("reference layouts sized to the population" if args.world_compact else
+                                 "reference layouts at the reference capacities (32,768 / 4,194,304 / 8,388,608)"),
                        "step": "nsb_world_neural_step + nsb_world_homeostasis (5 kernels, one host sync)",
                        "first_step_s_with_compile": first_step_s,
                        "l2": f"pools touched per step {(364 * N + 200 * E) / 1e9:.2f} GB"},
@@ -705,6 +711,8 @@ def run_world_stage(args, rank, world, local_rank):
                                           f"restatement, 2 steps after 1"}
     print(json.dumps(line), flush=True)
 
+    if args.world_compact:
+        return
     # the reference's world kernels on the same initial pools
     from oracle import pyoracle
     wlib = pyoracle.ref_world_lib()
@@ -784,6 +792,8 @@ def main():
                     help="the world simulator's neural stage on its own pools (config 2)")
     ap.add_argument("--world-population", default="founders", choices=["founders", "full"])
     ap.add_argument("--world-founders", type=int, default=2048, help="founders of the config-2 population")
+    ap.add_argument("--world-compact", action="store_true",
+                    help="pools sized to the population, no reference leg (profiler captures)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus if "RANK" in os.environ else 1))
