@@ -135,6 +135,18 @@ int nsb_gpu_set_delivery(void *batch, int cooperative);
  * (state restored afterwards) and keeps the faster; returns it, or -1. */
 int nsb_gpu_autotune(void *batch, int ticks, float gain, void *stream);
 
+/* Replaces compile_genome (gym_adapter/compile_graph.py:10-28), which the
+ * reference's SpikingPolicy applies before ns_create (gym_adapter/adapter.py:197-210):
+ * keeps the neurons with a causal path to a motor over active edges between
+ * active neurons, in ascending original order, and the synapses among them in
+ * original order with remapped endpoints. Outputs (any may be NULL except the
+ * counts): rows (count x 10, edges x 11 at most), motors (outputs), original
+ * indices for ns_original_indices. Host only; returns 0, or -1 on endpoints or
+ * motors outside the genome. */
+int nsb_compile_genome(int count, int edges, const float *neuron_rows, const float *synapse_rows, int outputs,
+                       const int *motors, float *out_neuron_rows, float *out_synapse_rows, int *out_motors,
+                       uint32_t *original_neurons, uint32_t *original_synapses, int *out_count, int *out_edges);
+
 /* ---- World pool slots (src/main.cu:364-390). The reference claims neuron and
  * synapse slots with an atomic first-free-bit search from a hint word; these
  * replay the claims one after another, so the slots depend only on the

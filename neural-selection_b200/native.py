@@ -61,6 +61,8 @@ SIGNATURES = {
     "nsb_gpu_checkpoint_export": (ct.c_int, [_vp, _vp, _vp, _i64]),
     "nsb_gpu_checkpoint_import": (ct.c_int, [_vp, _vp, ct.c_longlong, _vp, ct.c_longlong, _i64]),
     "nsb_gpu_autotune": (ct.c_int, [_vp, ct.c_int, ct.c_float, _vp]),
+    "nsb_compile_genome": (ct.c_int, [ct.c_int, ct.c_int, _f, _f, ct.c_int, _i32, _f, _f, _i32, _u32, _u32, _i32,
+                                      _i32]),
     "nsb_world_create": (_vp, [_vp, ct.c_int, ct.c_int]),
     "nsb_world_destroy": (None, [_vp]),
     "nsb_world_neural_step": (ct.c_int, [_vp, ct.c_int64]),
@@ -104,6 +106,31 @@ def _p(a, t):
 
 def _err(lib):
     return lib.ns_error().decode()
+
+
+def compile_genome(neuron_rows, synapse_rows, motors):
+    """The genome without neurons that have no causal path to a motor
+    (gym_adapter/compile_graph.py:10-28 of the reference, nsb_compile_genome):
+    (neuron rows, synapse rows, motors, original neuron indices, original
+    synapse indices). Pass the indices to Brain.original_indices so the reset
+    streams stay those of the full genome."""
+    lib = library()
+    ng = np.ascontiguousarray(neuron_rows, np.float32).reshape(-1, 10)
+    sg = np.ascontiguousarray(synapse_rows, np.float32).reshape(-1, 11)
+    mo = np.ascontiguousarray(motors, np.int32)
+    on = np.zeros((max(len(ng), 1), 10), np.float32)
+    os_ = np.zeros((max(len(sg), 1), 11), np.float32)
+    om = np.zeros(max(len(mo), 1), np.int32)
+    idn = np.zeros(max(len(ng), 1), np.uint32)
+    ids = np.zeros(max(len(sg), 1), np.uint32)
+    n, e = ct.c_int(0), ct.c_int(0)
+    sgp = sg if len(sg) else np.zeros((1, 11), np.float32)
+    ngp = ng if len(ng) else np.zeros((1, 10), np.float32)
+    mop = mo if len(mo) else np.zeros(1, np.int32)
+    if lib.nsb_compile_genome(len(ng), len(sg), _p(ngp, _f), _p(sgp, _f), len(mo), _p(mop, _i32), _p(on, _f),
+                              _p(os_, _f), _p(om, _i32), _p(idn, _u32), _p(ids, _u32), ct.byref(n), ct.byref(e)):
+        raise ValueError(_err(lib))
+    return on[:n.value], os_[:e.value], om[:len(mo)], idn[:n.value], ids[:e.value]
 
 
 NW, SW = 32, 20
