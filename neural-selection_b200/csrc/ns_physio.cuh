@@ -36,6 +36,18 @@ __device__ __forceinline__ uint32_t xorshift32(uint32_t x) {
 
 __device__ __forceinline__ float crexp(float x, const float *tab) { return nsx::expf_cr_ff(x, tab); }
 
+// The reference's uniform draws are u = (x >> 8) * 2^-24 for a 32-bit
+// xorshift state x (physiology.cuh:211-213, 384-391), tested as u < p. Both
+// u and p * 2^24 are exact binary32 values, so u < p holds exactly when the
+// 24-bit integer x >> 8 is below ceil(p * 2^24); a NaN or non-positive p
+// never passes. The integer test needs no int-to-float conversion per draw.
+__device__ __forceinline__ uint32_t draw_threshold(float p) {
+    const float t = p * 16777216.0f;
+    if (!(t > 0.0f)) return 0u;
+    if (t >= 16777216.0f) return 16777216u;
+    return (uint32_t)ceilf(t);
+}
+
 // physiology.cuh:226-230: thin-branch input/output curve (type 0 only).
 // When gs - 4 rounds to exactly -4 (|gs| below half an ulp of 4, about
 // 2.4e-7: a branch decaying after its last input), the exponent -(gs - 4)/0.4
@@ -53,9 +65,8 @@ __device__ __forceinline__ float receptor_drive(const float *g, uint32_t flags, 
     if (!(flags & NF_GENE_SENS) || !(g[G_RECEVENT] > 0)) return 0.0f;
     float rate = clampf(g[G_RECBASE] + g[G_RECGAIN] * level, 0.0f, 1000.0f);
     s.rng = xorshift32(s.rng);
-    float u = (float)(s.rng >> 8) * (1.0f / 16777216.0f);
     s.rec_ns *= g[G_RECDECAY];
-    if (u < rate * (1.0f / 1000.0f)) s.rec_ns += g[G_RECEVENT];
+    if ((s.rng >> 8) < draw_threshold(rate * (1.0f / 1000.0f))) s.rec_ns += g[G_RECEVENT];
     return s.rec_ns * (0.0f - s.v);
 }
 
@@ -300,16 +311,16 @@ __device__ __forceinline__ float release(const float *y, SynReleaseT<L> &s, int6
     int released = 0;
     uint32_t rng = s.rng;
     uint64_t ready = s.ready;
-    const float ru = s.ru;
+    const uint32_t t_rec = draw_threshold(p_rec), t_ru = draw_threshold(s.ru);
     for (int site = 0; site < n; ++site) {
         uint64_t bit = 1ull << site;
         if (!(ready & bit)) {
             rng = xorshift32(rng);
-            if ((float)(rng >> 8) * (1.0f / 16777216.0f) < p_rec) ready |= bit;
+            if ((rng >> 8) < t_rec) ready |= bit;
         }
         if (ready & bit) {
             rng = xorshift32(rng);
-            if ((float)(rng >> 8) * (1.0f / 16777216.0f) < ru) { ready &= ~bit; ++released; }
+            if ((rng >> 8) < t_ru) { ready &= ~bit; ++released; }
         }
     }
     s.rng = rng; s.ready = ready;
