@@ -272,3 +272,34 @@ def test_world_stage_matches_reference_kernels(nsb, block_mode):
         else:
             assert np.array_equal(_bits(x), _bits(y)), f"{name} differs from the reference kernels"
     assert got.motors.sum() > 0
+
+
+def test_world_stage_open_loop_2000_ticks(nsb, oracle_built):
+    """Config 2's gate: 125 world steps (2,000 ticks) of founders with new
+    world senses every step (open loop: the same senses fed to both sides),
+    motor counts compared every step and every pool at the end."""
+    W = nsb.world
+    batch = nsb.workloads.world_founders(seed=2, founders=128)
+    seeds = np.arange(batch.brains, dtype=np.uint32) + 1
+    pools = W.place_population(batch, *W.records_from_gpu(batch, seeds), scatter_seed=3)
+    world = W.World(pools)
+    ref = pools.copy()
+    rng = np.random.default_rng(4)
+    for step in range(1, 126):
+        senses = rng.random(ref.senses.shape).astype(np.float32)
+        ref.senses[:] = senses
+        world.upload("senses", senses.copy())
+        ref.motors[:] = 0
+        world.upload("motors", np.zeros_like(ref.motors))
+        world.neural_step(step)
+        world_step(ref, step)
+        got_motors = world.dev["motors"].cpu().numpy().view(np.int32).reshape(ref.motors.shape)
+        assert np.array_equal(got_motors, ref.motors), f"motor counts differ at step {step}"
+        ref.animals["age"][ref.animals["alive"] == 1] += 1
+        world.upload("animals", ref.animals.copy())
+        world.homeostasis()
+        world_homeostasis(ref)
+    got = world.download()
+    world.close()
+    _compare(got, ref)
+    assert got.neuron_state["total"].sum() > 0
