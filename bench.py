@@ -135,6 +135,9 @@ def workload(nsb, seed, fraction=1, kind="batched_uneven"):
         return nsb.workloads.plasticity_heavy(seed=seed + 2, brains=32768 // fraction,
                                               total_neurons=4194304 // fraction,
                                               total_synapses=8388608 // fraction)
+    if kind == "plain_small":
+        # config 1: 64 brains x 48 neurons, 600 synapses each, 20 Hz receptor drive
+        return nsb.workloads.plain_small(seed=seed)
     if kind == "serving_population":
         # the serving genomes (config 5) stepped as one static batch of 5,000
         # genomes (about 4.1 M neurons, 33 M synapses), every channel at 0.5
@@ -267,7 +270,7 @@ def run_reference_cuda(args, rank, world, local_rank):
         print(json.dumps({"impl": "reference-cuda", "unavailable": "oracle/_ref/libns_ref_gpu.so not built"}))
         return
     nsb = load_package()
-    batch = workload(nsb, 2)
+    batch = workload(nsb, 2, 1, args.workload if args.workload in ("batched_uneven", "plain_small") else "batched_uneven")
     f, i32 = ct.POINTER(ct.c_float), ct.POINTER(ct.c_int)
     handles = []
     for b in range(batch.brains):
@@ -317,7 +320,8 @@ def run_reference_cuda(args, rank, world, local_rank):
     line = {"impl": "reference-cuda", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (Philox4x32-10 seed 2)",
-            "config": {"workload": "batched_uneven_full_pools", "brains": batch.brains, "neurons": N,
+            "config": {"workload": ("batched_uneven_full_pools" if batch.brains == 32768 else batch.name),
+                       "brains": batch.brains, "neurons": N,
                        "synapses": len(batch.synapse_rows), "ticks_per_step": 16,
                        "delays_ms": "1-16 folded into 1-8 (reference ABI limit)",
                        "kernel": "gym_adapter/gpu.cu step_batch, 32 threads per brain, --fmad=false --prec-div=true --prec-sqrt=true, sm_100a",
@@ -328,6 +332,8 @@ def run_reference_cuda(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
     # The world simulator's neural stage (src/main.cu) in both of its forms.
+    if batch.brains != 32768:
+        return
     wlib = pyoracle.ref_world_lib()
     if wlib is None:
         print(json.dumps({"impl": "reference-cuda-world", "unavailable": "oracle/_ref/libns_ref_world.so not built"}))
@@ -465,12 +471,16 @@ def run_ours(args, rank, world, local_rank):
                 "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True,
                 "scaling": "strong" if args.strong and world > 1 else "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (Philox4x32-10, seed 2 + rank)",
-                "config": {"workload": f"{args.workload}_full_pools" if args.fraction == 1 else
-                           f"{args.workload}_1/{args.fraction}_pools", "brains": batch.brains, "neurons": N,
-                           "synapses": E, "ticks_per_step": 16, "delays_ms": "1-16", "parallelism": (f"shards x{world}" if args.strong and world > 1 else f"replicas x{world}"),
+                "config": {"workload": ("plain_small_64x48" if args.workload == "plain_small" else
+                                        f"{args.workload}_full_pools" if args.fraction == 1 else
+                                        f"{args.workload}_1/{args.fraction}_pools"), "brains": batch.brains, "neurons": N,
+                           "synapses": E, "ticks_per_step": 16, "delays_ms": f"1-{batch.max_delay}",
+                           "parallelism": (f"shards x{world}" if args.strong and world > 1 else f"replicas x{world}"),
                            "units": st["units"], "grid": st["grid"], "block": st["block"],
                            "delivery": "warp-cooperative" if coop else "serial",
-                           "l2": f"device state {(120 * N + 108 * E) / 1e9:.2f} GB > 126 MB L2: inputs larger than L2"},
+                           "l2": (f"device state {(120 * N + 108 * E) / 1e9:.2f} GB > 126 MB L2: inputs larger than L2"
+                                  if 120 * N + 108 * E > 126e6 else
+                                  f"device state {(120 * N + 108 * E) / 1e6:.1f} MB, L2-resident (not flushed)")},
                 "synaptic_events_per_s": events_per_s,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
@@ -778,7 +788,7 @@ def main():
     ap.add_argument("--fraction", type=int, default=1, choices=[1, 2, 4, 8, 16],
                     help="run a 1/D slice of the full pools (profiler captures only)")
     ap.add_argument("--workload", default="batched_uneven",
-                    choices=["batched_uneven", "plasticity_heavy", "serving_population"],
+                    choices=["batched_uneven", "plasticity_heavy", "serving_population", "plain_small"],
                     help="full-pool workload: batched uneven brains (default) or the plasticity-heavy variant")
     ap.add_argument("--strong", action="store_true",
                     help="N > 1: split one full-pool population across the ranks (default: one replica per rank)")

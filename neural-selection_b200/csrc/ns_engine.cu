@@ -1086,11 +1086,17 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
     n_brains_ = (int)brains.size();
     channels_ = channels; outputs_ = outputs; max_delay_ = cfg.max_delay; block_ = cfg.block;
     count_events_ = cfg.count_events;
-    unit_cap_ = block_ * std::max(1, cfg.unit_slots);
+    unit_cap_ = block_ * (cfg.unit_slots > 0 ? cfg.unit_slots : 3);
     int dev0 = 0, sms0 = 0;
     NSB_CHECK(cudaGetDevice(&dev0));
     NSB_CHECK(cudaDeviceGetAttribute(&sms0, cudaDevAttrMultiProcessorCount, dev0));
     Plan p = make_plan(brains, channels, outputs, max_delay_, unit_cap_, cfg.cluster_big == 1);
+    if (cfg.unit_slots <= 0 && p.n_light_units < sms0 * NSB_MIN_CTAS) {
+        // A batch too small to fill the GPU: one neuron per thread, so each
+        // unit's tick is one neuron update long instead of three.
+        unit_cap_ = block_;
+        p = make_plan(brains, channels, outputs, max_delay_, unit_cap_, cfg.cluster_big == 1);
+    }
     if (cfg.cluster_big < 0 && p.n_big_units > 0 && p.n_light_units < sms0 * NSB_MIN_CTAS)
         p = make_plan(brains, channels, outputs, max_delay_, unit_cap_, true);
     n_neurons_ = p.n_neurons; n_synapses_ = p.n_synapses; n_units_ = p.n_units; n_light_units_ = p.n_light_units;

@@ -29,7 +29,9 @@ struct EngineConfig {
     int max_delay = 8;          // 8 = the reference ABI; up to 31
     int block = 256;            // threads per CTA = neurons per small work unit
     int ctas_per_sm = 0;        // 0: from occupancy
-    int unit_slots = 3;         // small brains are packed into units of block * unit_slots neurons
+    // Small brains are packed into units of block * unit_slots neurons; 0:
+    // 3, or 1 when units of 3 cannot fill the GPU (lower per-tick latency).
+    int unit_slots = 0;
     bool count_events = true;   // count synaptic arrivals on the device
     // Brains above the unit size on thread-block clusters: 1 always, 0 never,
     // -1 when the batch has too few units to fill the GPU (a latency mode: a

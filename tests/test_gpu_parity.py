@@ -357,6 +357,7 @@ def test_big_brains_on_thread_block_clusters(nsb, monkeypatch, delivery, cluster
     parts.append(W.batched_uneven(seed=30, brains=6, total_neurons=6 * 120, total_synapses=6 * 300, plastic_all=True))
     batch = _concat(parts, "big_brains")
     monkeypatch.setenv("NSB_CLUSTER", cluster)     # "0": the same brains on one CTA each
+    monkeypatch.setenv("NSB_UNIT_SLOTS", "3")      # 768-neuron units, as in full batches
     gpu, _ = run_parity(nsb, batch, calls=6, check_every=2, delivery=delivery, reset_at=(3,),
                         mask_fn=lambda c: np.array([1 if (i + c) % 5 else 0 for i in range(batch.brains)], np.uint8))
     assert gpu.stats()["big_units"] == 4
