@@ -57,9 +57,6 @@ constexpr int kS = 19, kM = 5, kHist = 9, kTicks = 16, kContact = 16;
 #ifndef NSB_WORLD_EDGES
 #define NSB_WORLD_EDGES 2048
 #endif
-#ifndef NSB_WORLD_MIN_CTAS
-#define NSB_WORLD_MIN_CTAS 2
-#endif
 constexpr int kBlock = NSB_WORLD_BLOCK;      // small units: one thread per neuron
 constexpr int kUnitEdges = NSB_WORLD_EDGES;  // live synapses of a small unit (shared memory)
 constexpr int kUnitAnimals = 32;
@@ -104,6 +101,7 @@ struct WorldArgs {
 // neuron, list order within a neuron).
 struct Cache {
     int *id, *nn, *ne, *nl, *off, *cap;
+    int *hv;           // 1: the animal has an active LP, Prinz or LFS cell
     int *arena;
     long long arena_cap;
     unsigned long long *bump;
@@ -274,6 +272,12 @@ __device__ void compile_animal(const WorldArgs &d, const Cache &c, const Scratch
     }
     if (lane == 0) inptr[nn] = carry;
     const int nl = carry;
+    int hv = 0;
+    for (int k = lane; k < nn; k += 32) {
+        const ref::NeuronGene &G = d.ngene[nslot[k]];
+        if (G.active && (G.type == 2 || G.type == 3 || G.type == 6)) hv = 1;
+    }
+    hv = __any_sync(FULL, hv) ? 1 : 0;
     int *cmeta = inptr + nn + 1;
     int *cslot = cmeta + nl;
     __syncwarp();
@@ -295,7 +299,7 @@ __device__ void compile_animal(const WorldArgs &d, const Cache &c, const Scratch
     }
     __syncwarp();
     if (lane == 0) {
-        c.nn[a] = nn; c.ne[a] = ne; c.nl[a] = nl;
+        c.nn[a] = nn; c.ne[a] = ne; c.nl[a] = nl; c.hv[a] = hv;
         __threadfence();
         c.id[a] = A.id;
     }
@@ -472,6 +476,7 @@ __device__ __forceinline__ void phase_release(const WorldArgs &d, const UnitMem 
 }
 
 // Phase 3 for neuron n (state in s).
+template <bool HEAVY>
 __device__ __forceinline__ void phase_neuron(const WorldArgs &d, const UnitMem &U, int n, int t, int64_t tick,
                                              int cur9, NeuronRegs &s, int *motor_cnt, TraceRegs &tr,
                                              const float *tab) {
@@ -521,7 +526,7 @@ __device__ __forceinline__ void phase_neuron(const WorldArgs &d, const UnitMem &
     const uint32_t type = f & NF_TYPE_MASK;
     float cur = 0.0f;
     if (f & WF_SENSE) cur = (f & WF_RECEPTOR) ? receptor_drive(g, f, s, U.cur[n]) : U.cur[n];
-    if (type == 2 || type == 3 || type == 6) {
+    if (HEAVY && (type == 2 || type == 3 || type == 6)) {
         const ref::NeuronGene &G = d.ngene[slot];
         float xg[16] = {};
         if (type == 2) { xg[0] = G.lp.calcium; xg[1] = G.lp.calcium_k; xg[2] = G.lp.h; xg[3] = G.lp.leak; }
@@ -629,8 +634,14 @@ extern __shared__ __align__(16) unsigned char w_smem[];
 constexpr int kClaim = 4;   // animals taken from the living list per claim
 
 // Small units: animals with at most kBlock neurons and kUnitEdges live
-// synapses, packed in claim order; larger ones are appended to `big`.
-__global__ void __launch_bounds__(kBlock, NSB_WORLD_MIN_CTAS) world_tick_small(WorldArgs d, Cache c, int64_t first_tick,
+// synapses, packed in claim order. The light instantiation takes the animals
+// without LP, Prinz or LFS cells (no heavy-cell code: three CTAs per SM) and
+// appends the larger animals to `big`; the heavy one takes the rest.
+// MINB: CTAs per SM the register budget is sized for (the light kernel is
+// built for 3, at 79 registers, and for 2, at about 100, which steps each
+// unit faster when there are few units per CTA slot).
+template <bool HEAVY, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) world_tick_small(WorldArgs d, Cache c, int64_t first_tick,
                                                               const int *alive, const int *nalive, int *queue,
                                                               int *big, int *big_count, int *status,
                                                               Counters *stats) {
@@ -682,18 +693,21 @@ __global__ void __launch_bounds__(kBlock, NSB_WORLD_MIN_CTAS) world_tick_small(W
             for (;;) {
                 if (q_i >= q_n && !q_done) {
                     int base = 0;
-                    if (lane == 0) base = atomicAdd(queue, kClaim);
+                    if (lane == 0) base = atomicAdd(queue, HEAVY ? 32 : kClaim);
                     base = __shfl_sync(0xffffffffu, base, 0);
                     bool ok = false;
                     int a = -1, nn = 0, nl = 0;
-                    if (lane < kClaim && base + lane < n_alive) {
+                    if (lane < (HEAVY ? 32 : kClaim) && base + lane < n_alive) {
                         a = alive[base + lane];
                         if (!compiled(d, c, a)) {
-                            atomicOr(status, ST_LIST);    // compile failed (its own status bit is set too)
+                            if (!HEAVY) atomicOr(status, ST_LIST);    // compile failed (its own bit is set too)
                         } else {
                             nn = c.nn[a]; nl = c.nl[a];
-                            if (nn > kBlock || nl > kUnitEdges) big[atomicAdd(big_count, 1)] = a;
-                            else ok = nn > 0;
+                            if (nn > kBlock || nl > kUnitEdges) {
+                                if (!HEAVY) big[atomicAdd(big_count, 1)] = a;
+                            } else {
+                                ok = nn > 0 && (c.hv[a] != 0) == HEAVY;
+                            }
                         }
                     }
                     const unsigned mk = __ballot_sync(0xffffffffu, ok);
@@ -702,7 +716,7 @@ __global__ void __launch_bounds__(kBlock, NSB_WORLD_MIN_CTAS) world_tick_small(W
                         q_a[pos] = a; q_nn[pos] = nn; q_nl[pos] = nl;
                     }
                     __syncwarp();
-                    if (lane == 0) { q_n = __popc(mk); q_i = 0; if (base + kClaim >= n_alive) q_done = 1; }
+                    if (lane == 0) { q_n = __popc(mk); q_i = 0; if (base + (HEAVY ? 32 : kClaim) >= n_alive) q_done = 1; }
                     __syncwarp();
                     continue;
                 }
@@ -761,7 +775,7 @@ __global__ void __launch_bounds__(kBlock, NSB_WORLD_MIN_CTAS) world_tick_small(W
             phase_release(d, U, tick, tid, bs, tab);
             __syncthreads();
             if (tid == 0) s_cnt[0] = 0;
-            if (tid < ntot) phase_neuron(d, U, tid, t, tick, cur9, s, &ua_motor[nani[tid] * kM], tr, tab);
+            if (tid < ntot) phase_neuron<HEAVY>(d, U, tid, t, tick, cur9, s, &ua_motor[nani[tid] * kM], tr, tab);
             __syncthreads();
             phase_plastic_events(d, U, etot, tid, bs);
             __syncthreads();
@@ -904,7 +918,7 @@ __global__ void __launch_bounds__(kBigBlock) world_tick_big(WorldArgs d, Cache c
                 NeuronRegs s;
                 slab_load(B, n, s);
                 TraceRegs tr = {0, 0, 0, B.trx[n], B.tri[n], __uint_as_float(B.regs[13 * MN + n])};
-                phase_neuron(d, U, n, t, tick, cur9, s, s_motor, tr, tab);
+                phase_neuron<true>(d, U, n, t, tick, cur9, s, s_motor, tr, tab);
                 slab_store(B, n, s);
                 if (tr.ea || tr.er || tr.ia) {
                     const int m = (int)((U.nflag[n] >> WF_MOTOR_SHIFT) & 7u) - 1;
@@ -1017,15 +1031,25 @@ public:
         // ev, cpost, ring, 3 per-neuron bytes, carr, clast
         small_smem_ = 256 * 4 + 16 * kBlock * 4 + 6 * kBlock * 4 + kUnitEdges * 4 + kBlock * 4 + (kBlock + 4) * 4 +
                       3 * kUnitEdges * 4 + kUnitEdges * 2 + kBlock * 2 + 3 * kBlock + 2 * kUnitEdges;
-        NSB_CHECK(cudaFuncSetAttribute(world_tick_small, cudaFuncAttributeMaxDynamicSharedMemorySize, small_smem_));
         int occ = 0;
-        NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, world_tick_small, kBlock, small_smem_));
+        NSB_CHECK(cudaFuncSetAttribute(world_tick_small<false, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       small_smem_));
+        NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, world_tick_small<false, 3>, kBlock, small_smem_));
         small_grid_ = sms_ * std::max(occ, 1);
+        NSB_CHECK(cudaFuncSetAttribute(world_tick_small<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       small_smem_));
+        NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, world_tick_small<false, 2>, kBlock, small_smem_));
+        small2_grid_ = sms_ * std::max(occ, 1);
+        NSB_CHECK(cudaFuncSetAttribute(world_tick_small<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       small_smem_));
+        NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, world_tick_small<true, 2>, kBlock, small_smem_));
+        heavy_grid_ = sms_ * std::max(occ, 1);
         big_grid_ = sms_;
         compile_grid_ = sms_;
         const size_t P = (size_t)d_.P;
         c_.id = dev_alloc<int>(owned_, P); c_.nn = dev_alloc<int>(owned_, P); c_.ne = dev_alloc<int>(owned_, P);
         c_.nl = dev_alloc<int>(owned_, P); c_.off = dev_alloc<int>(owned_, P); c_.cap = dev_alloc<int>(owned_, P);
+        c_.hv = dev_alloc<int>(owned_, P);
         c_.arena_cap = 2 * (2LL * d_.ncap + (long long)d_.P + 2LL * d_.ecap);
         c_.arena = dev_alloc<int>(owned_, (size_t)c_.arena_cap);
         c_.bump = dev_alloc<unsigned long long>(owned_, 1);
@@ -1061,7 +1085,7 @@ public:
         list_ = dev_alloc<int>(owned_, P);
         alive_ = dev_alloc<int>(owned_, P);
         big_ = dev_alloc<int>(owned_, P);
-        // 0 compile count, 1 small queue, 2 big count, 3 big queue, 4 status, 5 living animals
+        // 0 compile count, 1 light queue, 2 big count, 3 big queue, 4 status, 5 living animals, 6 heavy queue
         ints_ = dev_alloc<int>(owned_, 8);
         stats_ = dev_alloc<Counters>(owned_, 1);
         NSB_CHECK(cudaMallocHost(&h_ints_, 8 * sizeof(int)));
@@ -1083,8 +1107,17 @@ public:
         world_select<<<std::max(1, std::min((d_.P + 255) / 256, sms_ * 8)), 256, 0, st>>>(d_, c_, list_, ints_,
                                                                                             alive_, ints_ + 5);
         world_compile<<<compile_grid_, 32 * kCompileWarps, 0, st>>>(d_, c_, list_, ints_, s_, ints_ + 4);
-        world_tick_small<<<small_grid_, kBlock, small_smem_, st>>>(d_, c_, first_tick, alive_, ints_ + 5, ints_ + 1,
-                                                                  big_, ints_ + 2, ints_ + 4, stats_);
+        // Few units per CTA slot (judged by the previous step's neurons): the
+        // 2-CTA build steps each unit faster; otherwise the 3-CTA build.
+        const bool few = last_.neurons > 0 && (long long)last_.neurons < 2LL * small_grid_ * kBlock;
+        if (few)
+            world_tick_small<false, 2><<<small2_grid_, kBlock, small_smem_, st>>>(
+                d_, c_, first_tick, alive_, ints_ + 5, ints_ + 1, big_, ints_ + 2, ints_ + 4, stats_);
+        else
+            world_tick_small<false, 3><<<small_grid_, kBlock, small_smem_, st>>>(
+                d_, c_, first_tick, alive_, ints_ + 5, ints_ + 1, big_, ints_ + 2, ints_ + 4, stats_);
+        world_tick_small<true, 2><<<heavy_grid_, kBlock, small_smem_, st>>>(d_, c_, first_tick, alive_, ints_ + 5,
+                                                                           ints_ + 6, big_, ints_ + 2, ints_ + 4, stats_);
         world_tick_big<<<big_grid_, kBigBlock, 1024, st>>>(d_, c_, first_tick, big_, ints_ + 2, ints_ + 3, b_, stats_);
         NSB_CHECK(cudaGetLastError());
         NSB_CHECK(cudaMemcpyAsync(h_ints_, ints_, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1127,7 +1160,8 @@ private:
     std::vector<void *> owned_;
     int *list_ = nullptr, *alive_ = nullptr, *big_ = nullptr, *ints_ = nullptr, *h_ints_ = nullptr;
     Counters *stats_ = nullptr, *h_stats_ = nullptr, last_{};
-    int sms_ = 148, small_smem_ = 0, small_grid_ = 0, big_grid_ = 0, compile_grid_ = 0;
+    int sms_ = 148, small_smem_ = 0, small_grid_ = 0, small2_grid_ = 0, heavy_grid_ = 0, big_grid_ = 0;
+    int compile_grid_ = 0;
 };
 
 }  // namespace nsb

@@ -15,7 +15,8 @@ world tick (src/main.cu:659-801):
 - input left pending from before the step;
 - spike history and modulatory timestamps from earlier ticks;
 - scattered, interleaved pool slots and list orders;
-- animals large enough for the one-animal-per-CTA path (by neurons and by synapses).
+- animals large enough for the one-animal-per-CTA path (by neurons and by synapses),
+  and animals exactly at the small path's capacity.
 
 The last test pins the stage to the reference simulator's own world kernels
 (src/main.cu built from its sources with IEEE arithmetic and correctly rounded
@@ -65,7 +66,9 @@ def _population(nsb, seed=6):
     W, wl = nsb.world, nsb.workloads
     batch = wl.concat([wl.world_founders(seed=seed, founders=40, heavy_types=True),
                        wl.world_founders(seed=seed + 1, founders=3, lo=300, hi=700),
-                       wl.world_founders(seed=seed + 2, founders=2, lo=190, hi=220, epn_lo=11, epn_hi=12)],
+                       wl.world_founders(seed=seed + 2, founders=2, lo=190, hi=220, epn_lo=11, epn_hi=12),
+                       # exactly the small path's capacity: 256 neurons, 8 synapses each (2,048)
+                       wl.world_founders(seed=seed + 3, founders=2, lo=256, hi=256, epn_lo=8, epn_hi=8)],
                       "world_mix")
     B = batch.brains
     N, E = int(batch.neuron_offsets[-1]), int(batch.synapse_offsets[-1])
