@@ -60,7 +60,7 @@ constexpr int kS = 19, kM = 5, kHist = 9, kTicks = 16, kContact = 16;
 constexpr int kBlock = NSB_WORLD_BLOCK;      // small units: one thread per neuron
 constexpr int kUnitEdges = NSB_WORLD_EDGES;  // live synapses of a small unit (shared memory)
 constexpr int kUnitAnimals = 32;
-constexpr int kBigBlock = 512;
+constexpr int kBigBlock = 256;
 constexpr int kCompileWarps = 4;     // compile kernel: warps per CTA, one animal per warp at a time
 
 // World neuron flags: bits 0-11 as the engine's NF_* (type, active,
@@ -861,9 +861,12 @@ __device__ __forceinline__ void slab_store(const BigSlab &B, int n, const Neuron
     B.regs[11 * M + n] = (uint32_t)s.total; B.regs[12 * M + n] = s.spike;
 }
 
-__global__ void __launch_bounds__(kBigBlock) world_tick_big(WorldArgs d, Cache c, int64_t first_tick, const int *big,
-                                                            const int *big_count, int *queue, BigSlab slab,
-                                                            Counters *stats) {
+// Big animals of one class (HEAVY: with an active LP, Prinz or LFS cell),
+// one per 256-thread CTA; each class has its own claim counter.
+template <bool HEAVY>
+__global__ void __launch_bounds__(kBigBlock, HEAVY ? 2 : 3) world_tick_big(WorldArgs d, Cache c, int64_t first_tick,
+                                                                          const int *big, const int *big_count,
+                                                                          int *queue, BigSlab slab, Counters *stats) {
     float *tab = reinterpret_cast<float *>(w_smem);
     __shared__ int s_i, s_motor[kM], s_cnt[2];
     __shared__ unsigned long long s_events;
@@ -881,7 +884,11 @@ __global__ void __launch_bounds__(kBigBlock) world_tick_big(WorldArgs d, Cache c
     const int nbig = *big_count;
     const int base9 = (int)(first_tick % kHist);
     for (;;) {
-        if (tid == 0) { s_i = atomicAdd(queue, 1); s_events = 0; s_cnt[0] = 0; s_cnt[1] = 0; }
+        if (tid == 0) {
+            int i = atomicAdd(queue, 1);
+            while (i < nbig && (c.hv[big[i]] != 0) != HEAVY) i = atomicAdd(queue, 1);
+            s_i = i; s_events = 0; s_cnt[0] = 0; s_cnt[1] = 0;
+        }
         if (tid < kM) s_motor[tid] = 0;
         __syncthreads();
         const int i = s_i;
@@ -918,7 +925,7 @@ __global__ void __launch_bounds__(kBigBlock) world_tick_big(WorldArgs d, Cache c
                 NeuronRegs s;
                 slab_load(B, n, s);
                 TraceRegs tr = {0, 0, 0, B.trx[n], B.tri[n], __uint_as_float(B.regs[13 * MN + n])};
-                phase_neuron<true>(d, U, n, t, tick, cur9, s, s_motor, tr, tab);
+                phase_neuron<HEAVY>(d, U, n, t, tick, cur9, s, s_motor, tr, tab);
                 slab_store(B, n, s);
                 if (tr.ea || tr.er || tr.ia) {
                     const int m = (int)((U.nflag[n] >> WF_MOTOR_SHIFT) & 7u) - 1;
@@ -1044,7 +1051,10 @@ public:
                                        small_smem_));
         NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, world_tick_small<true, 2>, kBlock, small_smem_));
         heavy_grid_ = sms_ * std::max(occ, 1);
-        big_grid_ = sms_;
+        NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, world_tick_big<false>, kBigBlock, 1024));
+        big_grid_ = sms_ * std::max(occ, 1);
+        NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, world_tick_big<true>, kBigBlock, 1024));
+        big_heavy_grid_ = sms_ * std::max(occ, 1);
         compile_grid_ = sms_;
         const size_t P = (size_t)d_.P;
         c_.id = dev_alloc<int>(owned_, P); c_.nn = dev_alloc<int>(owned_, P); c_.ne = dev_alloc<int>(owned_, P);
@@ -1064,7 +1074,7 @@ public:
         s_.skey = dev_alloc<int>(owned_, cw * pow2n);
         s_.sval = dev_alloc<int>(owned_, cw * pow2n);
         s_.cnt = dev_alloc<int>(owned_, cw * max_n);
-        const size_t bg = (size_t)big_grid_;
+        const size_t bg = (size_t)std::max(big_grid_, big_heavy_grid_);   // one slab per CTA
         b_.max_n = max_n; b_.max_e = max_e;
         b_.gene = dev_alloc<float>(owned_, bg * 16 * max_n);
         b_.nflag = dev_alloc<uint32_t>(owned_, bg * max_n);
@@ -1085,7 +1095,8 @@ public:
         list_ = dev_alloc<int>(owned_, P);
         alive_ = dev_alloc<int>(owned_, P);
         big_ = dev_alloc<int>(owned_, P);
-        // 0 compile count, 1 light queue, 2 big count, 3 big queue, 4 status, 5 living animals, 6 heavy queue
+        // 0 compile count, 1 light queue, 2 big count, 3 light big queue, 4 status, 5 living animals,
+        // 6 heavy queue, 7 heavy big queue
         ints_ = dev_alloc<int>(owned_, 8);
         stats_ = dev_alloc<Counters>(owned_, 1);
         NSB_CHECK(cudaMallocHost(&h_ints_, 8 * sizeof(int)));
@@ -1118,7 +1129,10 @@ public:
                 d_, c_, first_tick, alive_, ints_ + 5, ints_ + 1, big_, ints_ + 2, ints_ + 4, stats_);
         world_tick_small<true, 2><<<heavy_grid_, kBlock, small_smem_, st>>>(d_, c_, first_tick, alive_, ints_ + 5,
                                                                            ints_ + 6, big_, ints_ + 2, ints_ + 4, stats_);
-        world_tick_big<<<big_grid_, kBigBlock, 1024, st>>>(d_, c_, first_tick, big_, ints_ + 2, ints_ + 3, b_, stats_);
+        world_tick_big<false><<<big_grid_, kBigBlock, 1024, st>>>(d_, c_, first_tick, big_, ints_ + 2, ints_ + 3, b_,
+                                                                 stats_);
+        world_tick_big<true><<<big_heavy_grid_, kBigBlock, 1024, st>>>(d_, c_, first_tick, big_, ints_ + 2, ints_ + 7,
+                                                                       b_, stats_);
         NSB_CHECK(cudaGetLastError());
         NSB_CHECK(cudaMemcpyAsync(h_ints_, ints_, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
         NSB_CHECK(cudaMemcpyAsync(h_stats_, stats_, sizeof(Counters), cudaMemcpyDeviceToHost, st));
@@ -1161,6 +1175,7 @@ private:
     int *list_ = nullptr, *alive_ = nullptr, *big_ = nullptr, *ints_ = nullptr, *h_ints_ = nullptr;
     Counters *stats_ = nullptr, *h_stats_ = nullptr, last_{};
     int sms_ = 148, small_smem_ = 0, small_grid_ = 0, small2_grid_ = 0, heavy_grid_ = 0, big_grid_ = 0;
+    int big_heavy_grid_ = 0;
     int compile_grid_ = 0;
 };
 
