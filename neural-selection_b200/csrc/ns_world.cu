@@ -61,6 +61,7 @@ constexpr int kBlock = NSB_WORLD_BLOCK;      // small units: one thread per neur
 constexpr int kUnitEdges = NSB_WORLD_EDGES;  // live synapses of a small unit (shared memory)
 constexpr int kUnitAnimals = 32;
 constexpr int kBigBlock = 256;
+constexpr int kBigClasses = 4;       // big animals by size: above 2,048, 1,024, 512 neurons, the rest
 constexpr int kCompileWarps = 4;     // compile kernel: warps per CTA, one animal per warp at a time
 
 // World neuron flags: bits 0-11 as the engine's NF_* (type, active,
@@ -704,7 +705,10 @@ __global__ void __launch_bounds__(kBlock, MINB) world_tick_small(WorldArgs d, Ca
                         } else {
                             nn = c.nn[a]; nl = c.nl[a];
                             if (nn > kBlock || nl > kUnitEdges) {
-                                if (!HEAVY) big[atomicAdd(big_count, 1)] = a;
+                                if (!HEAVY) {
+                                    const int k = nn > 2048 ? 0 : nn > 1024 ? 1 : nn > 512 ? 2 : 3;
+                                    big[(size_t)k * d.P + atomicAdd(&big_count[k], 1)] = a;
+                                }
                             } else {
                                 ok = nn > 0 && (c.hv[a] != 0) == HEAVY;
                             }
@@ -881,19 +885,26 @@ __global__ void __launch_bounds__(kBigBlock, HEAVY ? 2 : 3) world_tick_big(World
     B.tri += sn * MN; B.ndepol += sn * MN; B.ring += sn * MN; B.nspk += sn * MN; B.nmod += sn * MN;
     B.rel += sn * ME; B.ev += sn * ME; B.cpost += sn * ME; B.carr += sn * ME; B.clast += sn * ME;
     B.regs += sn * 14 * MN;
-    const int nbig = *big_count;
+    int nbig = 0;
+    for (int k = 0; k < kBigClasses; ++k) nbig += big_count[k];
     const int base9 = (int)(first_tick % kHist);
     for (;;) {
         if (tid == 0) {
-            int i = atomicAdd(queue, 1);
-            while (i < nbig && (c.hv[big[i]] != 0) != HEAVY) i = atomicAdd(queue, 1);
-            s_i = i; s_events = 0; s_cnt[0] = 0; s_cnt[1] = 0;
+            int a = -1;
+            for (;;) {
+                int i = atomicAdd(queue, 1), k = 0;
+                if (i >= nbig) break;
+                while (i >= big_count[k]) { i -= big_count[k]; ++k; }
+                a = big[(size_t)k * d.P + i];
+                if ((c.hv[a] != 0) == HEAVY) break;
+                a = -1;
+            }
+            s_i = a; s_events = 0; s_cnt[0] = 0; s_cnt[1] = 0;
         }
         if (tid < kM) s_motor[tid] = 0;
         __syncthreads();
-        const int i = s_i;
-        if (i >= nbig) break;
-        const int a = big[i];
+        const int a = s_i;
+        if (a < 0) break;
         const int nn = c.nn[a], nl = c.nl[a];
         const int *R = c.arena + c.off[a];
         const bool fz = frozen_animal(d, a), traced = a == d.trace;
@@ -1094,12 +1105,12 @@ public:
         b_.regs = dev_alloc<uint32_t>(owned_, bg * 14 * max_n);
         list_ = dev_alloc<int>(owned_, P);
         alive_ = dev_alloc<int>(owned_, P);
-        big_ = dev_alloc<int>(owned_, P);
-        // 0 compile count, 1 light queue, 2 big count, 3 light big queue, 4 status, 5 living animals,
-        // 6 heavy queue, 7 heavy big queue
-        ints_ = dev_alloc<int>(owned_, 8);
+        big_ = dev_alloc<int>(owned_, (size_t)kBigClasses * P);
+        // 0 compile count, 1 light queue, 3 light big queue, 4 status, 5 living animals, 6 heavy queue,
+        // 7 heavy big queue, 8..11 big animals per size class
+        ints_ = dev_alloc<int>(owned_, kInts);
         stats_ = dev_alloc<Counters>(owned_, 1);
-        NSB_CHECK(cudaMallocHost(&h_ints_, 8 * sizeof(int)));
+        NSB_CHECK(cudaMallocHost(&h_ints_, kInts * sizeof(int)));
         NSB_CHECK(cudaMallocHost(&h_stats_, sizeof(Counters)));
         NSB_CHECK(cudaDeviceSynchronize());
     }
@@ -1113,7 +1124,7 @@ public:
         if (step < 1) throw std::runtime_error("Invalid world step");
         const int64_t first_tick = (step - 1) * kTicks;
         cudaStream_t st = 0;
-        NSB_CHECK(cudaMemsetAsync(ints_, 0, 8 * sizeof(int), st));
+        NSB_CHECK(cudaMemsetAsync(ints_, 0, kInts * sizeof(int), st));
         NSB_CHECK(cudaMemsetAsync(stats_, 0, sizeof(Counters), st));
         world_select<<<std::max(1, std::min((d_.P + 255) / 256, sms_ * 8)), 256, 0, st>>>(d_, c_, list_, ints_,
                                                                                             alive_, ints_ + 5);
@@ -1123,18 +1134,18 @@ public:
         const bool few = last_.neurons > 0 && (long long)last_.neurons < 2LL * small_grid_ * kBlock;
         if (few)
             world_tick_small<false, 2><<<small2_grid_, kBlock, small_smem_, st>>>(
-                d_, c_, first_tick, alive_, ints_ + 5, ints_ + 1, big_, ints_ + 2, ints_ + 4, stats_);
+                d_, c_, first_tick, alive_, ints_ + 5, ints_ + 1, big_, ints_ + 8, ints_ + 4, stats_);
         else
             world_tick_small<false, 3><<<small_grid_, kBlock, small_smem_, st>>>(
-                d_, c_, first_tick, alive_, ints_ + 5, ints_ + 1, big_, ints_ + 2, ints_ + 4, stats_);
+                d_, c_, first_tick, alive_, ints_ + 5, ints_ + 1, big_, ints_ + 8, ints_ + 4, stats_);
         world_tick_small<true, 2><<<heavy_grid_, kBlock, small_smem_, st>>>(d_, c_, first_tick, alive_, ints_ + 5,
-                                                                           ints_ + 6, big_, ints_ + 2, ints_ + 4, stats_);
-        world_tick_big<false><<<big_grid_, kBigBlock, 1024, st>>>(d_, c_, first_tick, big_, ints_ + 2, ints_ + 3, b_,
+                                                                           ints_ + 6, big_, ints_ + 8, ints_ + 4, stats_);
+        world_tick_big<false><<<big_grid_, kBigBlock, 1024, st>>>(d_, c_, first_tick, big_, ints_ + 8, ints_ + 3, b_,
                                                                  stats_);
-        world_tick_big<true><<<big_heavy_grid_, kBigBlock, 1024, st>>>(d_, c_, first_tick, big_, ints_ + 2, ints_ + 7,
+        world_tick_big<true><<<big_heavy_grid_, kBigBlock, 1024, st>>>(d_, c_, first_tick, big_, ints_ + 8, ints_ + 7,
                                                                        b_, stats_);
         NSB_CHECK(cudaGetLastError());
-        NSB_CHECK(cudaMemcpyAsync(h_ints_, ints_, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        NSB_CHECK(cudaMemcpyAsync(h_ints_, ints_, kInts * sizeof(int), cudaMemcpyDeviceToHost, st));
         NSB_CHECK(cudaMemcpyAsync(h_stats_, stats_, sizeof(Counters), cudaMemcpyDeviceToHost, st));
         NSB_CHECK(cudaStreamSynchronize(st));
         last_ = *h_stats_;
@@ -1176,6 +1187,7 @@ private:
     Counters *stats_ = nullptr, *h_stats_ = nullptr, last_{};
     int sms_ = 148, small_smem_ = 0, small_grid_ = 0, small2_grid_ = 0, heavy_grid_ = 0, big_grid_ = 0;
     int big_heavy_grid_ = 0;
+    static constexpr int kInts = 16;
     int compile_grid_ = 0;
 };
 
