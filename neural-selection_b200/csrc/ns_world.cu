@@ -16,19 +16,21 @@
 //    sort, owner/activity checks, a stable CSR of live synapses by
 //    post-synaptic neuron), into an arena keyed by (animal slot, animal id).
 //    Later steps read the compiled CSR with coalesced loads. Selection is a
-//    per-CTA claim over animal slots (alive == 1): no CUB pass, no host
-//    round trip inside the step.
-//  * One thread per post-synaptic neuron. It delivers the neuron's incoming
-//    synapses in list order (the per-branch sums of src/main.cu:680-690 in a
-//    fixed order instead of float atomics), integrates the neuron, and runs
-//    plasticity for the same synapses (lazy: quiet ticks are replayed exactly
-//    when the next event or the end of the step comes). Spikes cross threads
-//    only through the 9-tick history ring in shared memory: one barrier per
-//    tick.
+//    list of living animals that CTAs claim a few at a time: no CUB pass, no
+//    host round trip inside the step.
+//  * A tick runs in five barrier-separated phases over a unit: arrival test
+//    of every live synapse against the 9-tick spike-history ring; release of
+//    the arriving synapses from a compacted event list; per post-synaptic
+//    neuron (one thread each), the arriving inputs summed in list order (the
+//    per-branch sums of src/main.cu:680-690 in a fixed order instead of float
+//    atomics) and the integration; compaction of plasticity events; their
+//    plasticity, quiet ticks since the last update replayed exactly.
 //  * Small animals are packed into units of up to 256 neurons (one CTA,
 //    neuron genes, ring and CSR in shared memory, neuron state in registers);
-//    larger animals run one per CTA with their per-neuron arrays in a global
-//    scratch slab and the CSR read in place from the arena.
+//    larger animals run one per CTA, largest first, with their per-neuron
+//    arrays in a global scratch slab and the CSR read in place from the
+//    arena. Animals with LP, Prinz or LFS cells run in separate heavy builds
+//    of both kernels, so the light builds keep a small register budget.
 //  * Synapse state stays in the SynapseState records and is updated in place
 //    only when a synapse releases or its plasticity catches up.
 // Arithmetic is the engine's (ns_physio.cuh): bit-identical to the oracle.
