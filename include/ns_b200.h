@@ -206,7 +206,8 @@ void nsb_world_destroy(void *world);
  * animal's lists disagree with its counts or exceed the maxima (ns_error()). */
 int nsb_world_neural_step(void *world, int64_t step);
 /* Homeostatic AMPA scaling after the world's body step: every active neuron
- * of a living, unfrozen animal, elapsed max(16, age x 16) ms. */
+ * of a living, unfrozen animal, elapsed max(16, age x 16) ms. Launched on the
+ * legacy default stream; returns without waiting for it. */
 int nsb_world_homeostasis(void *world);
 /* Work of the last neural step: out[0] animals stepped, [1] neurons,
  * [2] synapses, [3] synaptic events (arrivals). */

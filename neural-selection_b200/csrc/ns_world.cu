@@ -1114,12 +1114,14 @@ public:
         stats_ = dev_alloc<Counters>(owned_, 1);
         NSB_CHECK(cudaMallocHost(&h_ints_, kInts * sizeof(int)));
         NSB_CHECK(cudaMallocHost(&h_stats_, sizeof(Counters)));
+        NSB_CHECK(cudaMallocHost(&h_bump_, sizeof(unsigned long long)));
         NSB_CHECK(cudaDeviceSynchronize());
     }
     ~WorldStage() {
         for (void *q : owned_) cudaFree(q);
         if (h_ints_) cudaFreeHost(h_ints_);
         if (h_stats_) cudaFreeHost(h_stats_);
+        if (h_bump_) cudaFreeHost(h_bump_);
     }
 
     void neural_step(int64_t step) {
@@ -1149,11 +1151,11 @@ public:
         NSB_CHECK(cudaGetLastError());
         NSB_CHECK(cudaMemcpyAsync(h_ints_, ints_, kInts * sizeof(int), cudaMemcpyDeviceToHost, st));
         NSB_CHECK(cudaMemcpyAsync(h_stats_, stats_, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+        NSB_CHECK(cudaMemcpyAsync(h_bump_, c_.bump, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
         NSB_CHECK(cudaStreamSynchronize(st));
         last_ = *h_stats_;
         const int status = h_ints_[4];
-        unsigned long long used = 0;
-        NSB_CHECK(cudaMemcpy(&used, c_.bump, sizeof used, cudaMemcpyDeviceToHost));
+        const unsigned long long used = *h_bump_;
         if (status & ST_ARENA || (long long)used > c_.arena_cap / 2) reset_cache();
         if (status & ST_SIZE) throw std::runtime_error("Animal brain larger than the world stage's maximum");
         if (status & ST_GENE) throw std::runtime_error("Invalid synapse gene in a living animal");
@@ -1161,10 +1163,11 @@ public:
         if (status & ST_LIST) throw std::runtime_error("Animal neuron/synapse lists disagree with its counts");
     }
 
+    // Launched on the legacy default stream, ordered before the caller's next
+    // launches there, as the reference's own homeostasis launches are.
     void homeostasis_step() {
         world_homeostasis<<<sms_ * 8, 256, 0, 0>>>(d_);
         NSB_CHECK(cudaGetLastError());
-        NSB_CHECK(cudaStreamSynchronize(0));
     }
 
     void stats(long long *out) const {
@@ -1187,6 +1190,7 @@ private:
     std::vector<void *> owned_;
     int *list_ = nullptr, *alive_ = nullptr, *big_ = nullptr, *ints_ = nullptr, *h_ints_ = nullptr;
     Counters *stats_ = nullptr, *h_stats_ = nullptr, last_{};
+    unsigned long long *h_bump_ = nullptr;
     int sms_ = 148, small_smem_ = 0, small_grid_ = 0, small2_grid_ = 0, heavy_grid_ = 0, big_grid_ = 0;
     int big_heavy_grid_ = 0;
     static constexpr int kInts = 16;
