@@ -306,3 +306,101 @@ def test_world_stage_open_loop_2000_ticks(nsb, oracle_built):
     world.close()
     _compare(got, ref)
     assert got.neuron_state["total"].sum() > 0
+
+
+
+def _genome_slots(pools, a):
+    """Pool slots of animal slot a's neuron and synapse lists, in list order."""
+    A = pools.animals[a]
+    n, q = [], int(A["neuron_head"])
+    while q >= 0:
+        n.append(q)
+        q = int(pools.neuron_next[q])
+    e, q = [], int(A["synapse_head"])
+    while q >= 0:
+        e.append(q)
+        q = int(pools.synapse_next[q])
+    return np.array(n), np.array(e)
+
+
+def _occupy(pools, a, genome, record, new_id):
+    """Animal slot a takes over a brain (its pool lists and state) as a new
+    animal: new id, age 1, owners rewritten, as a birth into a reused slot
+    does in the simulator (src/main.cu:1662-1732, which fills the lists from
+    freed pool slots)."""
+    nslots, eslots = genome
+    A = pools.animals
+    for f in ("neuron_head", "synapse_head", "neuron_count", "synapse_count", "ports"):
+        A[f][a] = record[f]
+    A["alive"][a] = 1
+    A["id"][a] = new_id
+    A["age"][a] = 1
+    pools.neuron_owner[nslots] = a
+    pools.synapse_owner[eslots] = a
+
+
+def test_world_stage_births_deaths_and_slot_reuse(nsb, oracle_built):
+    """Animals die and are born between steps, with every path of the
+    compiled-brain cache taken: a birth into a never-used animal slot, a
+    smaller brain taking over a dead animal's slot (its region rewritten in
+    place), a larger one (a new region), a brain moving through several slots
+    until the arena passes half full and the cache is reset, and the steps
+    after the reset that compile every living animal again. Every pool must
+    equal the oracle's after each phase."""
+    W, wl = nsb.world, nsb.workloads
+    batch = wl.concat([wl.world_founders(seed=9, founders=24),
+                       wl.world_founders(seed=10, founders=1, lo=230, hi=250, epn_lo=7, epn_hi=8),
+                       wl.world_founders(seed=11, founders=1, lo=20, hi=24)], "births")
+    seeds = np.arange(batch.brains, dtype=np.uint32) + 5
+    N, E = int(batch.neuron_offsets[-1]), int(batch.synapse_offsets[-1])
+    pools = W.place_population(batch, *W.records_from_gpu(batch, seeds), animal_capacity=32,
+                               neuron_capacity=N, synapse_capacity=E, scatter_seed=8)
+    big, small = 24, 25
+    genomes = {g: _genome_slots(pools, g) for g in range(batch.brains)}
+    records = {g: pools.animals[g].copy() for g in range(batch.brains)}
+    pools.animals["alive"][[big, small]] = 0          # not born yet
+    world = W.World(pools)
+    ref = pools.copy()
+    step = 0
+
+    def run(k):
+        nonlocal step
+        for _ in range(k):
+            step += 1
+            world.neural_step(step)
+            world_step(ref, step)
+            ref.animals["age"][ref.animals["alive"] == 1] += 1
+            world.upload("animals", ref.animals.copy())
+            world.homeostasis()
+            world_homeostasis(ref)
+        _compare(world.download(), ref, f"after step {step}: ")
+        assert world.stats()["animals"] == int((ref.animals["alive"] == 1).sum())
+
+    def publish():
+        for name in ("animals", "neuron_owner", "synapse_owner", "senses"):
+            world.upload(name, getattr(ref, name).copy())
+
+    run(2)
+    ref.animals["alive"][5] = 0                                   # a death
+    _occupy(ref, big, genomes[big], records[big], 5001)           # a birth into an unused slot
+    ref.senses[big] = batch.inputs[big]
+    publish()
+    run(2)
+    _occupy(ref, 5, genomes[small], records[small], 5002)         # smaller brain in a dead animal's slot
+    ref.senses[5] = batch.inputs[small]
+    ref.animals["alive"][big] = 0
+    _occupy(ref, 26, genomes[big], records[big], 5003)            # larger brain: a new region
+    ref.senses[26] = batch.inputs[big]
+    publish()
+    run(2)
+    next_id = 5004
+    for a in (27, 28, 29, 30):                                    # the arena passes half full
+        ref.animals["alive"][a - 1] = 0
+        _occupy(ref, a, genomes[big], records[big], next_id)
+        ref.senses[a] = batch.inputs[big]
+        next_id += 1
+        publish()
+        run(1)
+    run(2)                                                        # every living animal compiled again
+    world.close()
+    assert ref.motors.sum() > 0
