@@ -18,7 +18,11 @@ world tick (src/main.cu:659-801):
 - animals large enough for the one-animal-per-CTA path (by neurons and by synapses),
   and animals exactly at the small path's capacity.
 
-The last test pins the stage to the reference simulator's own world kernels
+A population that changes between steps (deaths, births, slots taken over
+by new animals) checks the compiled-brain cache, its arena reset included.
+
+test_world_stage_matches_reference_kernels pins the stage to the reference
+simulator's own world kernels
 (src/main.cu built from its sources with IEEE arithmetic and correctly rounded
 exp/log, oracle/ref_world_harness.cu) on a population whose float sums are
 order-independent: at most two live synapses per (post-synaptic neuron,
