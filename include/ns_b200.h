@@ -217,6 +217,41 @@ int nsb_world_stats(void *world, long long *out);
  * .neuron_count, .synapse_count and PlasticityCohort.frozen (10 values). */
 int nsb_world_layout(uint64_t *out);
 
+/* ---- World ecology stage: the rest of the world step around the neural
+ * stage (src/main.cu:612-657, 1138-1338; host loop order 2745-2770). The
+ * state beside the neural pools in the simulator's struct Device
+ * (src/main.cu:105-140). Grid 128 x 128 cells, row-major (y * 128 + x). */
+typedef struct NsbWorldEcology {
+    int *food, *kind;               /* [128 * 128]: food stock (0/1), kind 0-2 */
+    int *cell_head;                 /* [128 * 128] spatial index heads */
+    int *cell_next;                 /* [animal_capacity] */
+    unsigned char *bite_intent;     /* [animal_capacity] */
+    uint32_t *neuron_used, *synapse_used;   /* slot bitmaps, ceil(capacity / 32) words */
+    int *founder_motor_steps;       /* [5] */
+    int *founder_observed_steps, *deaths, *predation_deaths, *bites;
+    void *life_records;             /* LifeRecord[life_capacity] (504 B), or NULL */
+    int *life_count;
+    void *bite_events;              /* BiteEvent[2 * animal_capacity] (24 B), or NULL */
+    int *bite_event_count;
+    int initial_count;              /* animals with id below it count as founders */
+    int instant_motors;             /* motor force = spikes / 16 instead of the muscle model */
+    int life_capacity;
+} NsbWorldEcology;
+/* Contended steps (food harvests, spatial index order, bites, record slots)
+ * resolve as if the reference kernel's threads ran in ascending animal slot
+ * order: one legal execution of the reference's atomics, the same every run.
+ * All calls run on the legacy default stream and return after it finishes;
+ * -1 with ns_error() on invalid handles, lists that disagree with their
+ * counts, slots outside the capacities or a food kind outside 0-2. */
+void *nsb_world_ecology_create(const NsbWorldPools *pools, const NsbWorldEcology *ecology);
+void nsb_world_ecology_destroy(void *ecology);
+/* body_step, spatial index, bite_animals, finish_predation (src/main.cu:2745-2749). */
+int nsb_world_body_step(void *ecology, int64_t step);
+/* reclaim_dead_genomes (src/main.cu:2763): life records, genome release. */
+int nsb_world_reclaim(void *ecology, int64_t step);
+/* regrow, spatial index, update_senses (src/main.cu:2767-2770). */
+int nsb_world_regrow_and_sense(void *ecology, int64_t step, unsigned long long seed, float renewal_probability);
+
 /* ---- Checkpoint records. The world simulator saves the neural pools as
  * CheckpointNeuron (344 B) and CheckpointSynapse (136 B) records, one per
  * occupied slot in ascending slot order (src/main.cu:164-264, packed by

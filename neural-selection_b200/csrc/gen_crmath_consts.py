@@ -158,6 +158,40 @@ lines.append(f"#define NSX_F_LN2_128_B {hxf(L2)}")
 lines.append(f"#define NSX_F_LN2_128_C {hxf(L3)}")
 lines.append("")
 
+
+# ---- sin / cos argument reduction ----
+def pi_scaled(bits):
+    """floor(pi * 2^bits) - d with 0 <= d < 2, from Machin's formula
+    pi = 16 atan(1/5) - 4 atan(1/239) in integer arithmetic."""
+    guard = 32
+    one = 1 << (bits + guard)
+
+    def atan_inv(n):
+        total, term, k, n2 = 0, one // n, 0, n * n
+        while term:
+            total += term // (2 * k + 1) if k % 2 == 0 else -(term // (2 * k + 1))
+            term //= n2
+            k += 1
+        return total
+    return (16 * atan_inv(5) - 4 * atan_inv(239)) >> guard
+
+
+PI_BITS = 1200
+PI_INT = pi_scaled(PI_BITS)
+WORDS = 12
+# 2/pi = sum_i W[i] 2^(-32(i+1)): the first 32*WORDS fraction bits (2/pi < 1)
+two_over_pi = (1 << (PI_BITS + 1 + 32 * WORDS)) // PI_INT
+words = [(two_over_pi >> (32 * (WORDS - 1 - i))) & 0xffffffff for i in range(WORDS)]
+lines.append("/* 2/pi = sum_i W[i] 2^(-32 (i + 1)) */")
+lines.append("#define NSX_2OPI_WORDS \\")
+lines.append("    " + ", ".join(f"0x{w:08x}u" for w in words))
+lines.append(f"#define NSX_2OPI_COUNT {WORDS}")
+PIO2 = Decimal(PI_INT) / (Decimal(2) ** (PI_BITS + 1))
+h, l = dd(PIO2)
+lines.append(f"#define NSX_PIO2_HI {hx(h)}")
+lines.append(f"#define NSX_PIO2_LO {hx(l)}")
+lines.append("")
+
 out = Path(__file__).with_name("ns_crmath_consts.h")
 out.write_text("\n".join(lines) + "\n")
 print("wrote", out)

@@ -371,4 +371,194 @@ NSX_HD float logf_cr(float x) {
     return (float)y;
 }
 
+// ---- sin, cos, hypot ----------------------------------------------------------
+// The reference world's body and sense kernels (src/main.cu:619-657,
+// 1146-1249) call cosf, sinf and hypotf. They are evaluated here correctly
+// rounded as well, with the same fast-path / double-double strategy:
+//   reduction  |x| = (4j + q) pi/2 + r, |r| <= pi/4, by Payne and Hanek's
+//              method ("Radian reduction for trigonometric functions",
+//              SIGNUM Newsletter 18(1), 1983): the 24-bit significand times a
+//              192-bit window of 2/pi in integer arithmetic, keeping at least
+//              159 fraction bits, so r carries a relative error below 2^-100;
+//   fast path  Taylor polynomials of sin and cos to degree 17/18 in binary64
+//              (relative error below 2^-50), accepted unless within 2^-47 of a
+//              binary32 rounding midpoint;
+//   slow path  the Taylor series to degree 24 in double-double.
+// hypot: x^2 and y^2 are exact in binary64; sqrt(x^2 + y^2) in binary64 is
+// within 2^-52 (relative); near a midpoint the midpoint m is compared with the
+// exact sum of squares (m^2 has at most 50 significant bits).
+static const uint32_t k2OverPi_h[NSX_2OPI_COUNT] = {NSX_2OPI_WORDS};
+#if defined(__CUDACC__)
+static __device__ const uint32_t k2OverPi_d[NSX_2OPI_COUNT] = {NSX_2OPI_WORDS};
+#endif
+NSX_HD const uint32_t *two_over_pi() {
+#if defined(__CUDA_ARCH__)
+    return k2OverPi_d;
+#else
+    return k2OverPi_h;
+#endif
+}
+
+NSX_HD int clz32(uint32_t v) {   // v != 0
+#if defined(__CUDA_ARCH__)
+    return __clz((int)v);
+#else
+    return __builtin_clz(v);
+#endif
+}
+
+// Bits [lo, lo + 64) of the 256-bit little-endian value L (zero below bit 0).
+NSX_HD uint64_t window64(const uint32_t *L, int lo) {
+    int shift = 0;
+    if (lo < 0) {
+        if (lo <= -64) return 0;
+        shift = -lo;
+        lo = 0;
+    }
+    const int w = lo >> 5, s = lo & 31;
+    const uint64_t a = (uint64_t)L[w] | ((uint64_t)(w + 1 < 8 ? L[w + 1] : 0u) << 32);
+    const uint64_t c = w + 2 < 8 ? L[w + 2] : 0u;
+    const uint64_t v = s ? (a >> s) | (c << (64 - s)) : a;
+    return v << shift;
+}
+
+// |x| (binary32 bits u, finite, above pi/4) = (4j + q) pi/2 + r.
+NSX_COLD dd reduce_pio2(uint32_t u, int *quadrant) {
+    const uint32_t *W = two_over_pi();
+    const uint64_t m = (u & 0x7fffffu) | 0x800000u;
+    const int E = (int)(u >> 23) - 150;                 // |x| = m 2^E
+    const int i0 = E >= 2 ? (E - 2) >> 5 : 0;           // earlier words add multiples of 4
+    uint64_t p[6];
+    for (int k = 0; k < 6; ++k) p[k] = m * W[i0 + k];
+    uint32_t L[8];                                      // S = sum_k p[k] 2^(32 (5 - k))
+    uint64_t acc = 0;
+    for (int j = 0; j < 7; ++j) {
+        if (j <= 5) acc += p[5 - j] & 0xffffffffu;
+        if (j >= 1) acc += p[6 - j] >> 32;
+        L[j] = (uint32_t)acc;
+        acc >>= 32;
+    }
+    L[7] = (uint32_t)acc;
+    const int sh = 32 * (i0 + 6) - E;                   // fraction bits of S, 159..216
+    int q = (int)((L[sh >> 5] >> (sh & 31)) & 1u);
+    q |= (int)((L[(sh + 1) >> 5] >> ((sh + 1) & 31)) & 1u) << 1;
+    for (int j = 0; j < 8; ++j) {                       // keep the fraction F = S mod 2^sh
+        const int lo = 32 * j;
+        if (lo >= sh) L[j] = 0;
+        else if (lo + 32 > sh) L[j] &= (1u << (sh - lo)) - 1u;
+    }
+    const bool neg = (L[(sh - 1) >> 5] >> ((sh - 1) & 31)) & 1u;   // F >= 1/2: r = (F - 1) pi/2
+    if (neg) {
+        q = (q + 1) & 3;
+        uint64_t c = 1;                                 // 2^sh - F
+        for (int j = 0; j < 8; ++j) {
+            c += (uint64_t)(uint32_t)~L[j];
+            L[j] = (uint32_t)c;
+            c >>= 32;
+        }
+        for (int j = 0; j < 8; ++j) {
+            const int lo = 32 * j;
+            if (lo >= sh) L[j] = 0;
+            else if (lo + 32 > sh) L[j] &= (1u << (sh - lo)) - 1u;
+        }
+    }
+    *quadrant = q;
+    int top = -1;
+    for (int j = 7; j >= 0 && top < 0; --j)
+        if (L[j]) top = 32 * j + 31 - clz32(L[j]);
+    if (top < 0) return dd{0.0, 0.0};
+    const uint64_t mask53 = (1ull << 53) - 1ull;
+    const double a = (double)(window64(L, top - 52) & mask53);
+    const double b = (double)(window64(L, top - 105) & mask53);
+    const double fa = a * bitsd((uint64_t)(int64_t)(1023 + top - 52 - sh) << 52);
+    const double fb = b * bitsd((uint64_t)(int64_t)(1023 + top - 105 - sh) << 52);
+    dd r = dd_mul(fast_two_sum(fa, fb), dd{NSX_PIO2_HI, NSX_PIO2_LO});
+    if (neg) { r.hi = -r.hi; r.lo = -r.lo; }
+    return r;
+}
+
+// sin(r) (odd = 1) or cos(r) (odd = 0) for |r| <= pi/4 in double-double.
+NSX_COLD float sincos_slow(dd r, bool odd, bool negate) {
+    const double *c = inv_fact_dd();
+    const dd z = dd_mul(r, r);
+    int n = odd ? NSX_INV_FACT_COUNT - 2 : NSX_INV_FACT_COUNT - 1;   // 23 or 24
+    dd p = {c[2 * n], c[2 * n + 1]};
+    if ((n / 2) & 1) { p.hi = -p.hi; p.lo = -p.lo; }
+    for (n -= 2; n >= 0; n -= 2) {
+        dd t = {c[2 * n], c[2 * n + 1]};
+        if ((n / 2) & 1) { t.hi = -t.hi; t.lo = -t.lo; }
+        p = dd_add(dd_mul(p, z), t);
+    }
+    if (odd) p = dd_mul(p, r);
+    if (negate) { p.hi = -p.hi; p.lo = -p.lo; }
+    return round_dd_to_float(p.hi, p.lo);
+}
+
+// Correctly rounded sin (odd = 1) or cos (odd = 0) of binary32 x.
+NSX_HD float sincosf_cr(float x, bool want_sin) {
+    const uint32_t u = fbits(x) & 0x7fffffffu;
+    if (u >= 0x7f800000u) return (x - x) / (x - x);     // NaN, +-inf: NaN
+    if (u == 0u) return want_sin ? x : 1.0f;
+    const bool xneg = fbits(x) >> 31;
+    int q = 0;
+    dd r;
+    if (u <= 0x3f490fdau) r = dd{(double)bitsf(u), 0.0};  // |x| < pi/4
+    else r = reduce_pio2(u, &q);
+    const bool odd = want_sin ? (q & 1) == 0 : (q & 1) != 0;
+    bool negate = want_sin ? (q >= 2) != xneg : (q == 1 || q == 2);
+    const double rh = r.hi, rl = r.lo, z = rh * rh;
+    double y;
+    if (odd) {
+        double s = dfma(z, 1.0 / 355687428096000.0, -1.0 / 1307674368000.0);
+        s = dfma(z, s, 1.0 / 6227020800.0);
+        s = dfma(z, s, -1.0 / 39916800.0);
+        s = dfma(z, s, 1.0 / 362880.0);
+        s = dfma(z, s, -1.0 / 5040.0);
+        s = dfma(z, s, 1.0 / 120.0);
+        s = dfma(z, s, -1.0 / 6.0);
+        y = rh + dfma(rh * z, s, rl);                   // sin(rh + rl) ~ sin rh + rl
+    } else {
+        double s = dfma(z, 1.0 / 6402373705728000.0, -1.0 / 20922789888000.0);
+        s = dfma(z, s, 1.0 / 87178291200.0);
+        s = dfma(z, s, -1.0 / 479001600.0);
+        s = dfma(z, s, 1.0 / 3628800.0);
+        s = dfma(z, s, -1.0 / 40320.0);
+        s = dfma(z, s, 1.0 / 720.0);
+        s = dfma(z, s, -1.0 / 24.0);
+        s = dfma(z, s, 0.5);
+        y = 1.0 - dfma(z, s, rh * rl);                  // cos(rh + rl) ~ cos rh - rh rl
+    }
+    const double ay = y < 0 ? -y : y;
+    if (ay < 0x1p-126 || near_midpoint(ay, 64)) return sincos_slow(r, odd, negate);
+    return negate ? -(float)y : (float)y;
+}
+NSX_HD float sinf_cr(float x) { return sincosf_cr(x, true); }
+NSX_HD float cosf_cr(float x) { return sincosf_cr(x, false); }
+
+// Correctly rounded hypot of binary32 x, y (C99 special cases: an infinite
+// argument gives +inf even with a NaN, otherwise NaN propagates).
+NSX_HD float hypotf_cr(float x, float y) {
+    const uint32_t ux = fbits(x) & 0x7fffffffu, uy = fbits(y) & 0x7fffffffu;
+    if (ux == 0x7f800000u || uy == 0x7f800000u) return f32_inf();
+    if (ux > 0x7f800000u || uy > 0x7f800000u) return x + y;
+    const double a = (double)x * (double)x, b = (double)y * (double)y;   // exact
+    const double h = sqrt(a + b);
+    if (h >= 0x1p-126 && !near_midpoint(h, 16)) return (float)h;
+    if (h == 0.0) return 0.0f;
+    // The binary32 neighbours f, g around h and their midpoint (exact in
+    // binary64; +inf stands for 2^128 as round-to-nearest treats it).
+    const float f = (float)h;
+    const double fd = fbits(f) == 0x7f800000u ? 0x1p128 : (double)f;
+    if (fd == h) return f;
+    const float g = bitsf(fd < h ? fbits(f) + 1u : fbits(f) - 1u);
+    const double gd = fbits(g) == 0x7f800000u ? 0x1p128 : (double)g;
+    const double mid = 0.5 * (fd + gd);
+    const dd s = two_sum(a, b);                         // x^2 + y^2 exactly
+    const double d = mid * mid - s.hi;                  // exact: mid^2 has <= 50 bits, close to s.hi
+    const float below = fd < gd ? f : g, above = fd < gd ? g : f;
+    if (d > s.lo) return below;
+    if (d < s.lo) return above;
+    return (fbits(f) & 1u) ? g : f;                     // exact midpoint: even
+}
+
 }  // namespace nsx

@@ -110,9 +110,18 @@ constexpr uint64_t layout_hash() {
 }
 static_assert(layout_hash() == 0x2b1cd1c766eebf82ull, "checkpoint layout hash");
 
-// World simulator records the neural stage reads (src/main.cu:71-100). Only
-// the members named here are read; the rest is carried as opaque bytes of the
-// same size (Behavior: 69 four-byte counters, src/main.cu:71-79).
+// World simulator records (src/main.cu:66-104): the animal body with its
+// observer-only behaviour counters, the plasticity cohort, and the records the
+// world step appends (life records of reclaimed genomes, bite events).
+struct Behavior {                        // src/main.cu:66-74; age bins 0-99, 100-299, 300+
+    int opportunities[3][2][3];
+    int accepted[3][2][3];
+    int empty_steps[3][2], empty_eat[3][2];
+    float approach_progress[3][3];
+    float approach_travel[3][3];
+    int first_b_age, offspring, death_cause;
+};
+static_assert(sizeof(Behavior) == 276, "Behavior layout");
 struct Animal {
     float x, y, heading, energy, health, fullness, pain;
     float taste[4];
@@ -121,9 +130,22 @@ struct Animal {
     int id, parent_id, generation, age, alive;
     int neuron_head, synapse_head, neuron_count, synapse_count;
     int ports[19 + 5];
-    int behavior[69];
+    Behavior behavior;
 };
-struct PlasticityCohort {                // src/main.cu:96-104
+struct LifeRecord {                      // src/main.cu:85-90
+    Animal body;
+    int64_t death_step;
+    int active_neurons, active_synapses, modulatory_neurons, plastic_synapses;
+    float mean_abs_weight_change;
+};
+struct BiteEvent {                       // src/main.cu:91-95
+    int64_t step;
+    int attacker_id, prey_id;
+    float x, y;
+};
+static_assert(sizeof(LifeRecord) == 504 && offsetof(LifeRecord, death_step) == 472, "LifeRecord layout");
+static_assert(sizeof(BiteEvent) == 24, "BiteEvent layout");
+struct PlasticityCohort {                // src/main.cu:98-104
     int id, assigned, frozen, initial_age, initial_offspring;
     int final_age, final_offspring, alive, death_cause;
     int neurons, synapses, generation;

@@ -1,0 +1,686 @@
+// World ecology stage: the world simulator's per-step body, predation, genome
+// reclamation, food regrowth and senses (mixic/neural-selection
+// src/main.cu:612-657 and 1138-1338), on the simulator's own pools: the neural
+// pools of NsbWorldPools plus the food grid, spatial index, slot bitmaps and
+// counters of NsbWorldEcology.
+//
+// Order of one world step in the reference host loop (src/main.cu:2745-2770),
+// with the calls that replace each part:
+//   body_step, spatial reset, index_animals, bite_animals, finish_predation
+//                                                  nsb_world_body_step
+//   homeostasis                                    nsb_world_homeostasis
+//   reclaim_dead_genomes                           nsb_world_reclaim
+//   (reproduce, cohort observation: the caller's)
+//   regrow, spatial reset, index_animals, update_senses
+//                                                  nsb_world_regrow_and_sense
+//
+// Semantics. The reference runs each kernel one thread per animal (per cell
+// for regrowth) with atomics: food harvests, the spatial index's list order,
+// bites, and the slots of life records and bite events, so under contention
+// its results depend on thread timing. This stage computes the outcome of one
+// fixed legal execution: each kernel as if its threads ran one after another
+// in ascending animal slot order. It is computed in parallel:
+//   - harvests: an animal finds the food of its cell reduced by the eaters of
+//     lower slot in that cell (stock s, k such eaters: max(0, s - k)), which
+//     is what a slot-ordered sequence of harvests leaves; its 9 x 9 food scan
+//     reads the same quantity for each cell;
+//   - spatial index: each cell's list runs from the highest slot down, as
+//     ascending pushes onto the list head leave it (one warp ranks a cell);
+//   - bites only touch animals of the attacker's own cell, so each cell's
+//     attackers run in slot order on one thread, cells in parallel;
+//   - bite events and life records take consecutive indices in slot order
+//     (a scan over the animal slots).
+// Arithmetic: cosf, sinf and hypotf are the correctly rounded nsx functions,
+// sqrtf and division are IEEE (no contraction), so the results are those of
+// the reference's kernels built with IEEE arithmetic and the same correctly
+// rounded functions, bit for bit.
+#include <cuda_runtime.h>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "ns_b200.h"
+#include "ns_crmath.h"
+#include "ns_internal.h"
+#include "ns_refabi.h"
+
+namespace nsb {
+void set_error(const char *message);   // ns_abi.cu
+
+namespace {
+
+constexpr int kS = 19, kM = 5, kTicks = 16, kContact = 16;
+constexpr int kW = 128, kH = 128, kCells = kW * kH;
+constexpr float kBodyUpkeep = 0.003f;
+constexpr float kNeuronUpkeep = 0.00002f;
+constexpr float kBiteDamage = 2.0f;
+constexpr float kBiteCost = 0.02f;
+constexpr float kMeatFraction = 0.45f;
+constexpr float kMuscleDecay = 0.92311635f;   // exp(-16 / 200)
+constexpr float kMuscleTwitch = 0.30f;
+constexpr int kMaxAge = 10000;
+// Status bits, reported by the host as errors.
+enum : int { ES_LIST = 1, ES_SLOT = 2, ES_KIND = 4 };
+
+struct Eco {
+    ref::Animal *animals;
+    const ref::NeuronGene *ngene;
+    const ref::SynapseGene *sgene;
+    const ref::SynapseState *sstate;
+    int *nowner, *sowner;
+    const int *nnext, *snext;
+    float *senses;
+    int *motors;
+    int *food, *kind, *cell_head, *cell_next;
+    unsigned char *bite_intent;
+    uint32_t *nused, *sused;
+    int *f_motor, *f_observed, *deaths, *pred_deaths, *bites;
+    ref::LifeRecord *life;
+    int *life_count;
+    ref::BiteEvent *bite_events;
+    int *bite_count;
+    int initial_count, instant_motors, life_capacity;
+    int P, ncap, ecap;
+    // scratch
+    int *ecnt, *estart, *efill, *elist;          // eaters by food cell (slot order not kept)
+    int *acnt, *astart, *afill, *alist, *asort;  // living animals by cell; asort: highest slot first
+    unsigned char *flag;                         // per animal: bit, or reclaimed
+    int *prey, *rank, *base;                     // base[0]: first index of this call's records
+    int *status;
+};
+
+__device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(hi, fmaxf(lo, x)); }
+__device__ __forceinline__ int cell_of(float x, float y) {
+    const int ix = (int)floorf(clampf(x, 0.0f, (float)kW - 0.001f));
+    const int iy = (int)floorf(clampf(y, 0.0f, (float)kH - 0.001f));
+    return iy * kW + ix;
+}
+// xorshift64* and the seed hash of src/main.cu:331-346.
+__device__ __forceinline__ unsigned long long random64(unsigned long long &s) {
+    s ^= s >> 12; s ^= s << 25; s ^= s >> 27;
+    return s * 2685821657736338717ULL;
+}
+__device__ __forceinline__ float uniform(unsigned long long &s) {
+    return (float)((random64(s) >> 40) * (1.0 / 16777216.0));
+}
+__device__ __forceinline__ unsigned long long seed_for(unsigned long long seed, unsigned long long i) {
+    unsigned long long x = seed + 0x9e3779b97f4a7c15ULL * (i + 1);
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+    return (x ^ (x >> 31)) | 1ULL;
+}
+__device__ __forceinline__ bool excitatory(unsigned char t) { return t == 0 || t == 4 || t == 5; }
+
+// Food of cell c at animal a's turn: the stock minus the harvests of the
+// cell's eaters of lower slot (each takes one unit while any is left).
+__device__ int food_at(const Eco &e, int c, int a) {
+    const int f0 = e.food[c];
+    if (f0 <= 0) return f0;
+    const int n = e.ecnt[c];
+    if (!n) return f0;
+    const int *l = e.elist + e.estart[c];
+    int k = 0;
+    for (int i = 0; i < n; ++i) k += l[i] < a;
+    return k >= f0 ? 0 : f0 - k;
+}
+
+// ---- cell and slot scans (one CTA of 1024 threads) ------------------------------
+// out[i] = sum of in[0..i). With `accumulate`, base_out
+// receives *accumulate and *accumulate grows by the total.
+template <class T>
+__global__ void __launch_bounds__(1024) eco_scan(const T *in, int n, int *out, int *accumulate, int *base_out) {
+    __shared__ int warp_sum[32];
+    __shared__ int carry;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    if (t == 0) carry = 0;
+    __syncthreads();
+    for (int chunk = 0; chunk < n; chunk += 1024 * 16) {
+        int v[16], s = 0;
+        for (int k = 0; k < 16; ++k) {
+            const int i = chunk + t * 16 + k;
+            v[k] = i < n ? (int)in[i] : 0;
+            s += v[k];
+        }
+        int x = s;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_sum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            int w = warp_sum[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            warp_sum[lane] = w;
+        }
+        __syncthreads();
+        int b = carry + x - s + (warp ? warp_sum[warp - 1] : 0);
+        for (int k = 0; k < 16; ++k) {
+            const int i = chunk + t * 16 + k;
+            if (i < n) out[i] = b;
+            b += v[k];
+        }
+        __syncthreads();
+        if (t == 0) carry += warp_sum[31];
+        __syncthreads();
+    }
+    if (t == 0 && accumulate) {
+        base_out[0] = *accumulate;
+        *accumulate += carry;
+    }
+}
+
+// ---- body step (src/main.cu:1146-1249) -------------------------------------------
+__global__ void eco_count_eaters(Eco e) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
+        const ref::Animal &A = e.animals[a];
+        if (A.alive != 1 || e.motors[(size_t)a * kM + 3] <= 0) continue;
+        atomicAdd(&e.ecnt[cell_of(A.x, A.y)], 1);
+    }
+}
+__global__ void eco_place_eaters(Eco e) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
+        const ref::Animal &A = e.animals[a];
+        if (A.alive != 1 || e.motors[(size_t)a * kM + 3] <= 0) continue;
+        const int c = cell_of(A.x, A.y);
+        e.elist[e.estart[c] + atomicAdd(&e.efill[c], 1)] = a;
+    }
+}
+
+__global__ void __launch_bounds__(128) eco_body(Eco e) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
+        if (e.animals[a].alive != 1) continue;
+        ref::Animal b = e.animals[a];
+        ref::Behavior &bh = b.behavior;
+        const int age_bin = b.age < 100 ? 0 : (b.age < 300 ? 1 : 2);
+        const bool hungry = b.energy < 16.0f;
+        const float old_x = b.x, old_y = b.y;
+        int *mo = e.motors + (size_t)a * kM;
+        float force[3];
+        for (int m = 0; m < 3; ++m)
+            force[m] = e.instant_motors ? (float)mo[m] / (float)kTicks
+                                        : (b.muscle[m] = fminf(1.0f, b.muscle[m] * kMuscleDecay +
+                                                                     (float)mo[m] * kMuscleTwitch));
+        const float thrust = force[0], left = force[1], right = force[2];
+        const bool eat = mo[3] > 0;
+        const bool bite = mo[4] > 0;
+        e.bite_intent[a] = bite;
+        if (b.id < e.initial_count && b.age < 100) {
+            atomicAdd(e.f_observed, 1);
+            for (int m = 0; m < kM; ++m)
+                if (mo[m] > 0) atomicAdd(&e.f_motor[m], 1);
+        }
+        for (int m = 0; m < kM; ++m) mo[m] = 0;
+        b.heading += (right - left) * 1.2f;
+        b.x = clampf(b.x + nsx::cosf_cr(b.heading) * thrust * 1.5f, 0.0f, (float)kW - 0.001f);
+        b.y = clampf(b.y + nsx::sinf_cr(b.heading) * thrust * 1.5f, 0.0f, (float)kH - 0.001f);
+        const float travel = nsx::hypotf_cr(b.x - old_x, b.y - old_y);
+        if (hungry && travel > 0.0001f) {
+            float nearest[3] = {1e9f, 1e9f, 1e9f};
+            float tx[3] = {0.0f, 0.0f, 0.0f}, ty[3] = {0.0f, 0.0f, 0.0f};
+            const int cx = (int)old_x, cy = (int)old_y;
+            for (int dy = -4; dy <= 4; ++dy) {
+                const int y = cy + dy;
+                if (y < 0 || y >= kH) continue;
+                for (int dx = -4; dx <= 4; ++dx) {
+                    const int x = cx + dx;
+                    if (x < 0 || x >= kW) continue;
+                    const int c = y * kW + x;
+                    if (food_at(e, c, a) <= 0) continue;
+                    const int kind = e.kind[c];
+                    if (kind < 0 || kind > 2) { atomicOr(e.status, ES_KIND); continue; }
+                    const float fx = x + 0.5f, fy = y + 0.5f;
+                    const float distance = (fx - old_x) * (fx - old_x) + (fy - old_y) * (fy - old_y);
+                    if (distance < nearest[kind]) {
+                        nearest[kind] = distance;
+                        tx[kind] = fx;
+                        ty[kind] = fy;
+                    }
+                }
+            }
+            for (int kind = 0; kind < 3; ++kind)
+                if (nearest[kind] < 1e9f) {
+                    bh.approach_progress[age_bin][kind] += sqrtf(nearest[kind]) -
+                                                           nsx::hypotf_cr(tx[kind] - b.x, ty[kind] - b.y);
+                    bh.approach_travel[age_bin][kind] += travel;
+                }
+        }
+        int active = 0, walked = 0;
+        for (int n = b.neuron_head; n >= 0 && walked <= b.neuron_count; n = e.nnext[n], ++walked) {
+            if (n >= e.ncap) { atomicOr(e.status, ES_SLOT); break; }
+            active += e.ngene[n].active;
+        }
+        if (walked != b.neuron_count) atomicOr(e.status, ES_LIST);
+        b.energy -= kBodyUpkeep + (float)active * kNeuronUpkeep + thrust * 0.02f + (bite ? kBiteCost : 0.0f);
+        b.fullness = fmaxf(0.0f, b.fullness - 0.05f);
+        b.pain *= 0.8f;
+        for (int k = 0; k < 4; ++k) b.taste[k] *= 0.7f;
+        // Feed at the cell sensed before this decision; the harvest succeeds
+        // exactly when food is left at this animal's turn.
+        const int fc = cell_of(old_x, old_y);
+        const bool offered = food_at(e, fc, a) > 0;
+        const int hb = hungry ? 0 : 1;
+        int fkind = 0;
+        if (offered) {
+            fkind = e.kind[fc];
+            if (fkind < 0 || fkind > 2) { atomicOr(e.status, ES_KIND); fkind = 0; }
+            ++bh.opportunities[age_bin][hb][fkind];
+        } else {
+            ++bh.empty_steps[age_bin][hb];
+            bh.empty_eat[age_bin][hb] += eat;
+        }
+        if (eat && offered) {
+            ++bh.accepted[age_bin][hb][fkind];
+            if (fkind == 1 && bh.first_b_age == 0) bh.first_b_age = b.age + 1;
+            b.taste[fkind] = 1;
+            b.fullness += 1;
+            if (fkind == 0) b.energy = fminf(30, b.energy + 4);
+            if (fkind == 1) { b.energy = fminf(30, b.energy + 2); b.health -= 1.4f; b.pain += 1.4f; }
+            if (b.fullness > 8) { b.health -= 0.8f; b.pain += 0.8f; }
+        }
+        if (b.energy <= 0) { b.energy = 0; b.health -= 0.15f; b.pain += 0.15f; }
+        ++b.age;
+        if (b.health <= 0 || b.age >= kMaxAge) {
+            bh.death_cause = b.age >= kMaxAge ? 4 : (b.energy <= 0 ? 2 : 3);
+            b.alive = 0;
+            atomicAdd(e.deaths, 1);
+        }
+        e.animals[a] = b;
+    }
+}
+
+// Stock after every eater of the cell had its turn.
+__global__ void eco_commit_food(Eco e) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < kCells; c += gridDim.x * blockDim.x) {
+        const int f0 = e.food[c], n = e.ecnt[c];
+        if (f0 > 0 && n > 0) e.food[c] = n >= f0 ? 0 : f0 - n;
+    }
+}
+
+// ---- spatial index (src/main.cu:612-617) -----------------------------------------
+__global__ void eco_count_cells(Eco e) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
+        const ref::Animal &A = e.animals[a];
+        if (A.alive == 1) atomicAdd(&e.acnt[cell_of(A.x, A.y)], 1);
+    }
+}
+__global__ void eco_place_cells(Eco e) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
+        const ref::Animal &A = e.animals[a];
+        if (A.alive != 1) continue;
+        const int c = cell_of(A.x, A.y);
+        e.alist[e.astart[c] + atomicAdd(&e.afill[c], 1)] = a;
+    }
+}
+// One warp per cell: rank each member by the number of higher slots, then link
+// the list highest slot first (cell_next of animals not alive is untouched).
+__global__ void eco_link_cells(Eco e) {
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * blockDim.x / 32;
+    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) / 32; c < kCells; c += warps) {
+        const int n = e.acnt[c], s = e.astart[c];
+        for (int i = lane; i < n; i += 32) {
+            const int a = e.alist[s + i];
+            int r = 0;
+            for (int j = 0; j < n; ++j) r += e.alist[s + j] > a;
+            e.asort[s + r] = a;
+        }
+        __syncwarp();
+        for (int i = lane; i < n; i += 32) e.cell_next[e.asort[s + i]] = i + 1 < n ? e.asort[s + i + 1] : -1;
+        if (lane == 0) e.cell_head[c] = n ? e.asort[s] : -1;
+    }
+}
+
+// ---- predation (src/main.cu:1251-1285) --------------------------------------------
+// One thread per cell: the cell's attackers in ascending slot order, each
+// biting the first other living member in list order.
+__global__ void eco_bites(Eco e) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < kCells; c += gridDim.x * blockDim.x) {
+        const int n = e.acnt[c];
+        if (n < 2) continue;
+        const int *list = e.asort + e.astart[c];
+        for (int i = n - 1; i >= 0; --i) {
+            const int a = list[i];
+            if (e.animals[a].alive != 1 || !e.bite_intent[a]) continue;
+            for (int j = 0; j < n; ++j) {
+                const int prey = list[j];
+                if (prey == a || e.animals[prey].alive != 1) continue;
+                ref::Animal &p = e.animals[prey];
+                const float previous = p.health;
+                p.health = previous + -kBiteDamage;
+                p.pain = p.pain + kBiteDamage;
+                e.flag[a] = 1;
+                e.prey[a] = prey;
+                if (previous <= kBiteDamage) {
+                    p.alive = -2;
+                    ref::Animal &q = e.animals[a];
+                    q.energy = q.energy + fmaxf(0.0f, p.energy) * kMeatFraction;
+                    q.taste[3] = 1.0f;
+                    q.fullness = q.fullness + 1.0f;
+                }
+                break;
+            }
+        }
+    }
+}
+__global__ void eco_bite_events(Eco e, int64_t step) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
+        if (!e.flag[a]) continue;
+        atomicAdd(e.bites, 1);
+        if (!e.bite_events) continue;
+        const int event = e.base[0] + e.rank[a];
+        if (event < 2 * e.P) {
+            const ref::Animal &p = e.animals[e.prey[a]];
+            e.bite_events[event] = ref::BiteEvent{step, e.animals[a].id, p.id, p.x, p.y};
+        }
+    }
+}
+__global__ void eco_finish_predation(Eco e) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
+        if (e.animals[a].alive != -2) continue;
+        e.animals[a].behavior.death_cause = 1;
+        e.animals[a].alive = 0;
+        atomicAdd(e.deaths, 1);
+        atomicAdd(e.pred_deaths, 1);
+    }
+}
+
+// ---- genome reclamation (src/main.cu:1302-1338, 436-454) ------------------------
+__global__ void eco_reclaim_flags(Eco e) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
+        const ref::Animal &A = e.animals[a];
+        e.flag[a] = A.alive == 0 && (A.neuron_head >= 0 || A.synapse_head >= 0);
+    }
+}
+// Walks one list, bounded by its count; false if it disagrees with the count.
+__device__ bool list_ok(const int *next, int head, int count, int cap) {
+    int k = 0;
+    for (int q = head; q >= 0 && k <= count; q = next[q], ++k)
+        if (q >= cap) return false;
+    return k == count;
+}
+__global__ void eco_reclaim(Eco e, int64_t step) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
+        if (!e.flag[a]) continue;
+        ref::Animal body = e.animals[a];
+        if (!list_ok(e.nnext, body.neuron_head, body.neuron_count, e.ncap) ||
+            !list_ok(e.snext, body.synapse_head, body.synapse_count, e.ecap)) {
+            atomicOr(e.status, ES_LIST);
+            continue;
+        }
+        const int index = e.base[0] + e.rank[a];
+        if (e.life && index < e.life_capacity) {
+            ref::LifeRecord rec;
+            memset(&rec, 0, sizeof rec);
+            rec.body = body;
+            rec.death_step = step;
+            for (int n = body.neuron_head; n >= 0; n = e.nnext[n]) {
+                const ref::NeuronGene &g = e.ngene[n];
+                rec.active_neurons += g.active;
+                rec.modulatory_neurons += g.active && g.modulator != 0;
+            }
+            float total = 0;
+            for (int s = body.synapse_head; s >= 0; s = e.snext[s]) {
+                const ref::SynapseGene &g = e.sgene[s];
+                if ((unsigned)g.pre >= (unsigned)e.ncap || (unsigned)g.post >= (unsigned)e.ncap) {
+                    atomicOr(e.status, ES_SLOT);
+                    continue;
+                }
+                const ref::NeuronGene &pre = e.ngene[g.pre], &post = e.ngene[g.post];
+                const bool live = g.active && pre.active && post.active;
+                rec.active_synapses += live;
+                rec.plastic_synapses += live && g.plasticity != 0 && !pre.inh_tx && excitatory(pre.type) &&
+                                        pre.modulator == 0 && !post.inh_tx && excitatory(post.type);
+                if (live) total += fabsf(e.sstate[s].w - g.w0);
+            }
+            rec.mean_abs_weight_change = rec.active_synapses > 0 ? total / rec.active_synapses : 0;
+            e.life[index] = rec;
+        }
+        for (int s = body.synapse_head; s >= 0;) {
+            const int next = e.snext[s];
+            e.sowner[s] = -1;
+            atomicAnd(&e.sused[s / 32], ~(1u << (s % 32)));
+            s = next;
+        }
+        for (int n = body.neuron_head; n >= 0;) {
+            const int next = e.nnext[n];
+            e.nowner[n] = -1;
+            atomicAnd(&e.nused[n / 32], ~(1u << (n % 32)));
+            n = next;
+        }
+        body.neuron_head = body.synapse_head = -1;
+        body.neuron_count = body.synapse_count = 0;
+        for (int p = 0; p < kS + kM; ++p) body.ports[p] = -1;
+        e.animals[a] = body;
+    }
+}
+
+// ---- regrowth and senses (src/main.cu:1138-1144, 619-657) ------------------------
+__global__ void eco_regrow(Eco e, int64_t step, unsigned long long seed, float renewal) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < kCells; c += gridDim.x * blockDim.x) {
+        if (e.food[c] != 0) continue;
+        unsigned long long rng = seed_for(seed + (unsigned long long)step, (unsigned long long)c);
+        if (uniform(rng) < renewal) e.food[c] = 1;
+    }
+}
+
+__global__ void __launch_bounds__(128) eco_senses(Eco e) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
+        const ref::Animal &A = e.animals[a];
+        if (A.alive != 1) continue;
+        const float x = A.x, y = A.y, heading = A.heading;
+        float *out = e.senses + (size_t)a * kS;
+        for (int s = 0; s < 6; ++s) {
+            const float angle = heading + (s % 3 - 1) * 0.7f;
+            const float ca = nsx::cosf_cr(angle), sa = nsx::sinf_cr(angle);
+            float level = 0;
+            for (int range = 1; range <= 4; ++range) {
+                const int c = cell_of(x + ca * range, y + sa * range);
+                if (e.kind[c] == s / 3 && e.food[c] > 0) level += 0.25f;
+            }
+            out[s] = clampf(level, 0, 1);
+        }
+        out[6] = clampf((16.0f - A.energy) / 16.0f, 0, 1);
+        out[7] = clampf(A.fullness / 8.0f, 0, 1);
+        out[8] = clampf(A.pain / 3.0f, 0, 1);
+        for (int k = 0; k < 3; ++k) out[9 + k] = clampf(A.taste[k], 0, 1);
+        for (int direction = 0; direction < 3; ++direction) {
+            const float angle = heading + (direction - 1) * 0.7f;
+            const float ca = nsx::cosf_cr(angle), sa = nsx::sinf_cr(angle);
+            float level = 0;
+            for (int range = 1; range <= 4; ++range) {
+                const int c = cell_of(x + ca * range, y + sa * range);
+                const int *list = e.asort + e.astart[c];
+                for (int j = 0, n = e.acnt[c]; j < n; ++j)
+                    if (list[j] != a && e.animals[list[j]].alive == 1) level += 0.25f;
+            }
+            out[12 + direction] = clampf(level, 0, 1);
+        }
+        out[15] = clampf(A.taste[3], 0, 1);
+        const int cc = cell_of(x, y);
+        for (int kind = 0; kind < 3; ++kind)
+            out[kContact + kind] = e.food[cc] > 0 && e.kind[cc] == kind ? 1.0f : 0.0f;
+    }
+}
+
+template <class T> T *dev_zeros(std::vector<void *> &owned, size_t n) {
+    void *p = nullptr;
+    NSB_CHECK(cudaMalloc(&p, sizeof(T) * (n ? n : 1)));
+    owned.push_back(p);
+    NSB_CHECK(cudaMemset(p, 0, sizeof(T) * (n ? n : 1)));
+    return static_cast<T *>(p);
+}
+
+class EcologyStage {
+public:
+    EcologyStage(const NsbWorldPools &p, const NsbWorldEcology &x) {
+        if (!p.animals || !p.neurons || !p.synapses || !p.synapse_state || !p.neuron_owner || !p.synapse_owner ||
+            !p.neuron_next || !p.synapse_next || !p.senses || !p.motors || p.animal_capacity <= 0 ||
+            p.neuron_capacity <= 0 || p.synapse_capacity <= 0)
+            throw std::runtime_error("Invalid world pools");
+        if (!x.food || !x.kind || !x.cell_head || !x.cell_next || !x.bite_intent || !x.neuron_used ||
+            !x.synapse_used || !x.founder_motor_steps || !x.founder_observed_steps || !x.deaths ||
+            !x.predation_deaths || !x.bites || !x.life_count || !x.bite_event_count || x.life_capacity < 0)
+            throw std::runtime_error("Invalid world ecology");
+        x_.animals = static_cast<ref::Animal *>(const_cast<void *>(p.animals));
+        x_.ngene = static_cast<const ref::NeuronGene *>(p.neurons);
+        x_.sgene = static_cast<const ref::SynapseGene *>(p.synapses);
+        x_.sstate = static_cast<const ref::SynapseState *>(p.synapse_state);
+        x_.nowner = const_cast<int *>(p.neuron_owner);
+        x_.sowner = const_cast<int *>(p.synapse_owner);
+        x_.nnext = p.neuron_next;
+        x_.snext = p.synapse_next;
+        x_.senses = const_cast<float *>(p.senses);
+        x_.motors = p.motors;
+        x_.food = x.food; x_.kind = x.kind; x_.cell_head = x.cell_head; x_.cell_next = x.cell_next;
+        x_.bite_intent = x.bite_intent;
+        x_.nused = x.neuron_used; x_.sused = x.synapse_used;
+        x_.f_motor = x.founder_motor_steps; x_.f_observed = x.founder_observed_steps;
+        x_.deaths = x.deaths; x_.pred_deaths = x.predation_deaths; x_.bites = x.bites;
+        x_.life = static_cast<ref::LifeRecord *>(x.life_records);
+        x_.life_count = x.life_count;
+        x_.bite_events = static_cast<ref::BiteEvent *>(x.bite_events);
+        x_.bite_count = x.bite_event_count;
+        x_.initial_count = x.initial_count;
+        x_.instant_motors = x.instant_motors != 0;
+        x_.life_capacity = x.life_records ? x.life_capacity : 0;
+        x_.P = p.animal_capacity; x_.ncap = p.neuron_capacity; x_.ecap = p.synapse_capacity;
+        const size_t P = (size_t)p.animal_capacity;
+        x_.ecnt = dev_zeros<int>(owned_, kCells);
+        x_.estart = dev_zeros<int>(owned_, kCells);
+        x_.efill = dev_zeros<int>(owned_, kCells);
+        x_.elist = dev_zeros<int>(owned_, P);
+        x_.acnt = dev_zeros<int>(owned_, kCells);
+        x_.astart = dev_zeros<int>(owned_, kCells);
+        x_.afill = dev_zeros<int>(owned_, kCells);
+        x_.alist = dev_zeros<int>(owned_, P);
+        x_.asort = dev_zeros<int>(owned_, P);
+        x_.flag = dev_zeros<unsigned char>(owned_, P);
+        x_.prey = dev_zeros<int>(owned_, P);
+        x_.rank = dev_zeros<int>(owned_, P);
+        x_.base = dev_zeros<int>(owned_, 1);
+        x_.status = dev_zeros<int>(owned_, 1);
+        NSB_CHECK(cudaMallocHost(&h_status_, sizeof(int)));
+        int dev = 0;
+        NSB_CHECK(cudaGetDevice(&dev));
+        NSB_CHECK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
+    }
+    ~EcologyStage() {
+        for (void *q : owned_) cudaFree(q);
+        if (h_status_) cudaFreeHost(h_status_);
+    }
+
+    // body_step, spatial reset, index_animals, bite_animals, finish_predation.
+    void body_step(int64_t step) {
+        cudaStream_t st = 0;
+        NSB_CHECK(cudaMemsetAsync(x_.ecnt, 0, sizeof(int) * kCells, st));
+        eco_count_eaters<<<animal_grid(), 256, 0, st>>>(x_);
+        eco_scan<int><<<1, 1024, 0, st>>>(x_.ecnt, kCells, x_.estart, nullptr, nullptr);
+        NSB_CHECK(cudaMemsetAsync(x_.efill, 0, sizeof(int) * kCells, st));
+        eco_place_eaters<<<animal_grid(), 256, 0, st>>>(x_);
+        eco_body<<<(x_.P + 127) / 128, 128, 0, st>>>(x_);
+        eco_commit_food<<<kCells / 256, 256, 0, st>>>(x_);
+        index(st);
+        NSB_CHECK(cudaMemsetAsync(x_.flag, 0, (size_t)x_.P, st));
+        eco_bites<<<kCells / 128, 128, 0, st>>>(x_);
+        // the event counter advances only when events are recorded (src/main.cu:1262-1268)
+        eco_scan<unsigned char><<<1, 1024, 0, st>>>(x_.flag, x_.P, x_.rank, x_.bite_events ? x_.bite_count : nullptr,
+                                                    x_.base);
+        eco_bite_events<<<animal_grid(), 256, 0, st>>>(x_, step);
+        eco_finish_predation<<<animal_grid(), 256, 0, st>>>(x_);
+        finish(st);
+    }
+
+    void reclaim(int64_t step) {
+        cudaStream_t st = 0;
+        eco_reclaim_flags<<<animal_grid(), 256, 0, st>>>(x_);
+        eco_scan<unsigned char><<<1, 1024, 0, st>>>(x_.flag, x_.P, x_.rank, x_.life_count, x_.base);
+        eco_reclaim<<<animal_grid(), 256, 0, st>>>(x_, step);
+        finish(st);
+    }
+
+    // regrow, spatial reset, index_animals, update_senses.
+    void regrow_and_sense(int64_t step, unsigned long long seed, float renewal) {
+        cudaStream_t st = 0;
+        eco_regrow<<<kCells / 256, 256, 0, st>>>(x_, step, seed, renewal);
+        index(st);
+        eco_senses<<<(x_.P + 127) / 128, 128, 0, st>>>(x_);
+        finish(st);
+    }
+
+private:
+    int animal_grid() const { return std::min((x_.P + 255) / 256, sms_ * 8); }
+
+    void index(cudaStream_t st) {
+        NSB_CHECK(cudaMemsetAsync(x_.acnt, 0, sizeof(int) * kCells, st));
+        eco_count_cells<<<animal_grid(), 256, 0, st>>>(x_);
+        eco_scan<int><<<1, 1024, 0, st>>>(x_.acnt, kCells, x_.astart, nullptr, nullptr);
+        NSB_CHECK(cudaMemsetAsync(x_.afill, 0, sizeof(int) * kCells, st));
+        eco_place_cells<<<animal_grid(), 256, 0, st>>>(x_);
+        eco_link_cells<<<kCells * 32 / 256, 256, 0, st>>>(x_);
+    }
+
+    void finish(cudaStream_t st) {
+        NSB_CHECK(cudaGetLastError());
+        NSB_CHECK(cudaMemcpyAsync(h_status_, x_.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+        NSB_CHECK(cudaStreamSynchronize(st));
+        const int status = *h_status_;
+        if (status) {
+            NSB_CHECK(cudaMemset(x_.status, 0, sizeof(int)));
+            if (status & ES_LIST) throw std::runtime_error("Animal neuron/synapse lists disagree with its counts");
+            if (status & ES_SLOT) throw std::runtime_error("Pool slot outside the capacity");
+            throw std::runtime_error("Food kind outside 0-2");
+        }
+    }
+
+    Eco x_{};
+    std::vector<void *> owned_;
+    int *h_status_ = nullptr;
+    int sms_ = 148;
+};
+
+template <class F> int guarded(void *h, F f) {
+    try {
+        if (!h) throw std::runtime_error("Invalid world ecology handle");
+        f(*static_cast<EcologyStage *>(h));
+        return 0;
+    } catch (const std::exception &e) {
+        set_error(e.what());
+        return -1;
+    }
+}
+
+}  // namespace
+}  // namespace nsb
+
+extern "C" {
+
+void *nsb_world_ecology_create(const NsbWorldPools *pools, const NsbWorldEcology *ecology) {
+    try {
+        if (!pools || !ecology) throw std::runtime_error("Missing world pools or ecology");
+        return new nsb::EcologyStage(*pools, *ecology);
+    } catch (const std::exception &e) {
+        nsb::set_error(e.what());
+        return nullptr;
+    }
+}
+
+void nsb_world_ecology_destroy(void *ecology) { delete static_cast<nsb::EcologyStage *>(ecology); }
+
+int nsb_world_body_step(void *ecology, int64_t step) {
+    return nsb::guarded(ecology, [&](nsb::EcologyStage &s) { s.body_step(step); });
+}
+
+int nsb_world_reclaim(void *ecology, int64_t step) {
+    return nsb::guarded(ecology, [&](nsb::EcologyStage &s) { s.reclaim(step); });
+}
+
+int nsb_world_regrow_and_sense(void *ecology, int64_t step, unsigned long long seed, float renewal_probability) {
+    return nsb::guarded(ecology, [&](nsb::EcologyStage &s) { s.regrow_and_sense(step, seed, renewal_probability); });
+}
+
+}  // extern "C"

@@ -59,6 +59,27 @@ COHORT = np.dtype({"names": ["id", "assigned", "frozen", "initial_age", "initial
                    "offsets": [0, 4, 8, 12, 16, 20, 24, 28, 32, 36, 40, 44, 48, 52, 56, 64, 72], "itemsize": 80})
 
 
+BEHAVIOR = np.dtype({"names": ["opportunities", "accepted", "empty_steps", "empty_eat", "approach_progress",
+                               "approach_travel", "first_b_age", "offspring", "death_cause"],
+                     "formats": [("<i4", (3, 2, 3)), ("<i4", (3, 2, 3)), ("<i4", (3, 2)), ("<i4", (3, 2)),
+                                 ("<f4", (3, 3)), ("<f4", (3, 3)), "<i4", "<i4", "<i4"],
+                     "offsets": [0, 72, 144, 168, 192, 228, 264, 268, 272], "itemsize": 276})
+LIFE_RECORD = np.dtype({"names": ["body", "death_step", "active_neurons", "active_synapses", "modulatory_neurons",
+                                  "plastic_synapses", "mean_abs_weight_change"],
+                        "formats": [ANIMAL, "<i8", "<i4", "<i4", "<i4", "<i4", "<f4"],
+                        "offsets": [0, 472, 480, 484, 488, 492, 496], "itemsize": 504})
+BITE_EVENT = np.dtype({"names": ["step", "attacker_id", "prey_id", "x", "y"],
+                       "formats": ["<i8", "<i4", "<i4", "<f4", "<f4"], "offsets": [0, 8, 12, 16, 20],
+                       "itemsize": 24})
+GRID = 128
+CELLS = GRID * GRID
+
+
+def behavior(animals):
+    """The Behavior counters of Animal records, as a structured view."""
+    return animals["behavior"].view(np.uint8).reshape(len(animals), -1).view(BEHAVIOR).reshape(-1)
+
+
 class NsbWorldPools(ct.Structure):
     """include/ns_b200.h NsbWorldPools (pointers: device for the library,
     host for the oracle's or_world_pools, which has the same layout)."""
@@ -128,6 +149,125 @@ class WorldPools:
             self.silence_contact
         s.animal_capacity, s.neuron_capacity, s.synapse_capacity = self.capacities
         return s
+
+
+class NsbWorldEcology(ct.Structure):
+    """include/ns_b200.h NsbWorldEcology (device pointers for the library,
+    host pointers for the oracle's or_world_eco, which has the same layout)."""
+    _fields_ = [(n, ct.c_void_p) for n in (
+        "food", "kind", "cell_head", "cell_next", "bite_intent", "neuron_used", "synapse_used",
+        "founder_motor_steps", "founder_observed_steps", "deaths", "predation_deaths", "bites", "life_records",
+        "life_count", "bite_events", "bite_event_count")] + [(n, ct.c_int) for n in (
+        "initial_count", "instant_motors", "life_capacity")]
+
+
+ECO_ARRAYS = ("food", "kind", "cell_head", "cell_next", "bite_intent", "neuron_used", "synapse_used",
+              "founder_motor_steps", "founder_observed_steps", "deaths", "predation_deaths", "bites", "life_records",
+              "life_count", "bite_events", "bite_event_count")
+
+
+@dataclass
+class Ecology:
+    """Host copy of the world's ecology state beside the neural pools (the
+    food grid, spatial index, slot bitmaps, counters and appended records of
+    the simulator's struct Device, src/main.cu:105-140)."""
+    food: np.ndarray                 # (128 * 128,) i32
+    kind: np.ndarray                 # (128 * 128,) i32
+    cell_head: np.ndarray            # (128 * 128,) i32
+    cell_next: np.ndarray            # (animal_capacity,) i32
+    bite_intent: np.ndarray          # (animal_capacity,) u8
+    neuron_used: np.ndarray          # (ceil(neuron_capacity / 32),) u32
+    synapse_used: np.ndarray
+    founder_motor_steps: np.ndarray  # (5,) i32
+    founder_observed_steps: np.ndarray   # (1,) i32 each
+    deaths: np.ndarray
+    predation_deaths: np.ndarray
+    bites: np.ndarray
+    life_records: np.ndarray | None  # LIFE_RECORD
+    life_count: np.ndarray
+    bite_events: np.ndarray | None   # BITE_EVENT, 2 * animal_capacity
+    bite_event_count: np.ndarray
+    initial_count: int = 0
+    instant_motors: int = 0
+
+    def copy(self):
+        kw = {}
+        for f in fields(self):
+            v = getattr(self, f.name)
+            kw[f.name] = v.copy() if isinstance(v, np.ndarray) else v
+        return Ecology(**kw)
+
+    def struct(self):
+        """NsbWorldEcology over these host arrays (for the oracle)."""
+        s = NsbWorldEcology()
+        for n in ECO_ARRAYS:
+            a = getattr(self, n)
+            setattr(s, n, None if a is None else a.ctypes.data)
+        s.initial_count, s.instant_motors = self.initial_count, self.instant_motors
+        s.life_capacity = 0 if self.life_records is None else len(self.life_records)
+        return s
+
+
+def _seed_for(seed, i):
+    """src/main.cu:341-346 over numpy uint64 arrays."""
+    with np.errstate(over="ignore"):
+        x = np.uint64(seed) + np.uint64(0x9e3779b97f4a7c15) * (np.asarray(i, np.uint64) + np.uint64(1))
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xbf58476d1ce4e5b9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94d049bb133111eb)
+        return (x ^ (x >> np.uint64(31))) | np.uint64(1)
+
+
+def _uniform(s):
+    """xorshift64* step and uniform draw (src/main.cu:331-337); returns (u, s)."""
+    with np.errstate(over="ignore"):
+        s = s ^ (s >> np.uint64(12))
+        s = s ^ (s << np.uint64(25))
+        s = s ^ (s >> np.uint64(27))
+        r = s * np.uint64(2685821657736338717)
+    return ((r >> np.uint64(40)).astype(np.float64) * (1.0 / 16777216.0)).astype(np.float32), s
+
+
+def make_ecology(pools, seed, initial_count=None, life_capacity=None, bite_events=True, instant_motors=0):
+    """Ecology state for `pools`: the food grid of init_world
+    (src/main.cu:456-462, seed `seed`), slot bitmaps from the pool owners,
+    an empty spatial index and zero counters."""
+    P, NC, EC = pools.capacities
+    c = np.arange(CELLS, dtype=np.uint64)
+    s = _seed_for(seed, c + np.uint64(P))
+    u, s = _uniform(s)
+    kind = (u * np.float32(3)).astype(np.int32)
+    u, s = _uniform(s)
+    food = (u < np.float32(0.28)).astype(np.int32)
+
+    def bitmap(owner):
+        words = np.zeros((len(owner) + 31) // 32, np.uint32)
+        used = np.nonzero(owner >= 0)[0]
+        np.bitwise_or.at(words, used // 32, (np.uint32(1) << (used % 32).astype(np.uint32)))
+        return words
+
+    one = lambda: np.zeros(1, np.int32)
+    return Ecology(food=food, kind=kind, cell_head=np.full(CELLS, -1, np.int32), cell_next=np.full(P, -1, np.int32),
+                   bite_intent=np.zeros(P, np.uint8), neuron_used=bitmap(pools.neuron_owner),
+                   synapse_used=bitmap(pools.synapse_owner), founder_motor_steps=np.zeros(M, np.int32),
+                   founder_observed_steps=one(), deaths=one(), predation_deaths=one(), bites=one(),
+                   life_records=np.zeros(life_capacity if life_capacity is not None else 16 * P, LIFE_RECORD),
+                   life_count=one(), bite_events=np.zeros(2 * P, BITE_EVENT) if bite_events else None,
+                   bite_event_count=one(),
+                   initial_count=P if initial_count is None else int(initial_count), instant_motors=instant_motors)
+
+
+def place_bodies(pools, seed, energy=14.0, health=10.0):
+    """Bodies for the living animals as init_animals gives founders
+    (src/main.cu:527-541): uniform position and heading, energy 14, health 10."""
+    rng = np.random.default_rng(seed)
+    A = pools.animals
+    live = np.nonzero(A["alive"] == 1)[0]
+    A["x"][live] = rng.uniform(0, GRID - 1, len(live)).astype(np.float32)
+    A["y"][live] = rng.uniform(0, GRID - 1, len(live)).astype(np.float32)
+    A["heading"][live] = rng.uniform(0, 2 * np.pi, len(live)).astype(np.float32)
+    A["energy"][live] = energy
+    A["health"][live] = health
+    return pools
 
 
 def empty_pools(animal_capacity, neuron_capacity, synapse_capacity, cohort=False):
@@ -312,8 +452,62 @@ class World:
         return out
 
     def close(self):
+        if getattr(self, "eco", None):
+            self.lib.nsb_world_ecology_destroy(self.eco)
+            self.eco = None
         if getattr(self, "ptr", None):
             self.lib.nsb_world_destroy(self.ptr)
             self.ptr = None
 
     __del__ = close
+
+    # ---- ecology (the rest of the world step) ----
+    def attach_ecology(self, ecology: Ecology):
+        """Upload `ecology` and bind the library's ecology stage to it and to
+        this world's pools."""
+        torch = self.torch
+        dev = next(t for t in self.dev.values() if t is not None).device
+        self.eco_host = ecology
+        self.eco_dev = {}
+        for n in ECO_ARRAYS:
+            a = getattr(ecology, n)
+            self.eco_dev[n] = None if a is None else torch.from_numpy(
+                np.ascontiguousarray(a).view(np.uint8).reshape(-1).copy()).to(dev)
+        s = NsbWorldEcology()
+        for n in ECO_ARRAYS:
+            t = self.eco_dev[n]
+            setattr(s, n, None if t is None else t.data_ptr())
+        s.initial_count, s.instant_motors = ecology.initial_count, ecology.instant_motors
+        s.life_capacity = 0 if ecology.life_records is None else len(ecology.life_records)
+        self.eco_struct = s
+        self.eco = self.lib.nsb_world_ecology_create(ct.byref(self.struct), ct.byref(s))
+        if not self.eco:
+            raise RuntimeError(self.lib.ns_error().decode())
+
+    def _eco_call(self, rc):
+        if rc != 0:
+            raise RuntimeError(self.lib.ns_error().decode())
+
+    def body_step(self, step):
+        self._eco_call(self.lib.nsb_world_body_step(self.eco, int(step)))
+
+    def reclaim(self, step):
+        self._eco_call(self.lib.nsb_world_reclaim(self.eco, int(step)))
+
+    def regrow_and_sense(self, step, seed, renewal_probability):
+        self._eco_call(self.lib.nsb_world_regrow_and_sense(self.eco, int(step), int(seed),
+                                                            float(renewal_probability)))
+
+    def upload_ecology(self, name, array):
+        raw = np.ascontiguousarray(array).view(np.uint8).reshape(-1)
+        self.eco_dev[name].copy_(self.torch.from_numpy(raw))
+        setattr(self.eco_host, name, array)
+
+    def download_ecology(self) -> Ecology:
+        out = self.eco_host.copy()
+        for n in ECO_ARRAYS:
+            t = self.eco_dev[n]
+            if t is None:
+                continue
+            getattr(out, n).view(np.uint8).reshape(-1)[:] = t.cpu().numpy()
+        return out

@@ -23,9 +23,15 @@
 #ifdef OR_LIBM
 #define OEXP expf
 #define OLOG logf
+#define OCOS cosf
+#define OSIN sinf
+#define OHYPOT hypotf
 #else
 #define OEXP or_cr_expf
 #define OLOG or_cr_logf
+#define OCOS or_cr_cosf
+#define OSIN or_cr_sinf
+#define OHYPOT or_cr_hypotf
 #endif
 
 float or_bound_expf(float x) { return OEXP(x); }
@@ -1181,7 +1187,14 @@ typedef struct {                   /* src/main.cu:81-91 */
     int id, parent_id, generation, age, alive;
     int neuron_head, synapse_head, neuron_count, synapse_count;
     int ports[24];
-    int behavior[69];
+    struct {                       /* src/main.cu:66-74 */
+        int opportunities[3][2][3];
+        int accepted[3][2][3];
+        int empty_steps[3][2], empty_eat[3][2];
+        float approach_progress[3][3];
+        float approach_travel[3][3];
+        int first_b_age, offspring, death_cause;
+    } behavior;
 } or_animal;
 typedef struct {                   /* src/main.cu:96-104 */
     int id, assigned, frozen, initial_age, initial_offspring;
@@ -1358,4 +1371,284 @@ int or_world_layout(uint64_t *out) {
                             offsetof(or_animal, synapse_count), offsetof(or_cohort, frozen)};
     for (int i = 0; i < 14; ++i) out[i] = v[i];
     return 14;
+}
+
+
+/* ---- world ecology (src/main.cu:612-657, 1138-1338) ------------------------
+ * The reference kernels restated as loops over animal slots in ascending
+ * order (cells for regrowth): one thread after another, which fixes the
+ * outcome of every contended step (harvests, spatial list order, bites,
+ * record indices) as that sequential execution. */
+#define W_W 128
+#define W_H 128
+#define W_CELLS (W_W * W_H)
+
+typedef struct {                   /* src/main.cu:85-90 */
+    or_animal body;
+    int64_t death_step;
+    int active_neurons, active_synapses, modulatory_neurons, plastic_synapses;
+    float mean_abs_weight_change;
+} or_life;
+typedef struct {                   /* src/main.cu:91-95 */
+    int64_t step;
+    int attacker_id, prey_id;
+    float x, y;
+} or_bite;
+
+static float or_clamp(float x, float lo, float hi) { return fminf(hi, fmaxf(lo, x)); }
+static int or_cell(float x, float y) {                         /* src/main.cu:347-351 */
+    int ix = (int)floorf(or_clamp(x, 0.0f, W_W - 0.001f));
+    int iy = (int)floorf(or_clamp(y, 0.0f, W_H - 0.001f));
+    return iy * W_W + ix;
+}
+static unsigned long long or_random64(unsigned long long *s) {  /* src/main.cu:331-346 */
+    *s ^= *s >> 12; *s ^= *s << 25; *s ^= *s >> 27;
+    return *s * 2685821657736338717ULL;
+}
+static float or_uniform(unsigned long long *s) {
+    return (float)((or_random64(s) >> 40) * (1.0 / 16777216.0));
+}
+static unsigned long long or_seed_for(unsigned long long seed, unsigned long long i) {
+    unsigned long long x = seed + 0x9e3779b97f4a7c15ULL * (i + 1);
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+    return (x ^ (x >> 31)) | 1ULL;
+}
+static int or_excitatory(unsigned char t) { return t == 0 || t == 4 || t == 5; }
+
+static void or_index(const or_world_pools *w, const or_world_eco *x) {   /* src/main.cu:612-617 */
+    const or_animal *A = (const or_animal *)w->animals;
+    for (int c = 0; c < W_CELLS; ++c) x->cell_head[c] = -1;
+    for (int a = 0; a < w->animal_capacity; ++a) {
+        if (A[a].alive != 1) continue;
+        int c = or_cell(A[a].x, A[a].y);
+        x->cell_next[a] = x->cell_head[c];
+        x->cell_head[c] = a;
+    }
+}
+
+static void or_body(const or_world_pools *w, const or_world_eco *x, int a) {   /* src/main.cu:1146-1249 */
+    or_animal *A = (or_animal *)w->animals;
+    const ngene *NG = (const ngene *)w->neurons;
+    or_animal b = A[a];
+    const int age_bin = b.age < 100 ? 0 : (b.age < 300 ? 1 : 2);
+    const int hungry = b.energy < 16.0f;
+    const float old_x = b.x, old_y = b.y;
+    int *mo = w->motors + (size_t)a * W_M;
+    float force[3];
+    for (int m = 0; m < 3; ++m)
+        force[m] = x->instant_motors ? mo[m] / (float)16
+                                     : (b.muscle[m] = fminf(1.0f, b.muscle[m] * 0.92311635f + mo[m] * 0.30f));
+    float thrust = force[0], left = force[1], right = force[2];
+    int eat = mo[3] > 0;
+    x->bite_intent[a] = mo[4] > 0;
+    if (b.id < x->initial_count && b.age < 100) {
+        ++*x->founder_observed_steps;
+        for (int m = 0; m < W_M; ++m)
+            if (mo[m] > 0) ++x->founder_motor_steps[m];
+    }
+    for (int m = 0; m < W_M; ++m) mo[m] = 0;
+    b.heading += (right - left) * 1.2f;
+    b.x = or_clamp(b.x + OCOS(b.heading) * thrust * 1.5f, 0, W_W - 0.001f);
+    b.y = or_clamp(b.y + OSIN(b.heading) * thrust * 1.5f, 0, W_H - 0.001f);
+    float travel = OHYPOT(b.x - old_x, b.y - old_y);
+    if (hungry && travel > 0.0001f) {
+        float nearest[3] = {1e9f, 1e9f, 1e9f};
+        float target_x[3] = {0, 0, 0}, target_y[3] = {0, 0, 0};
+        int cx = (int)old_x, cy = (int)old_y;
+        for (int dy = -4; dy <= 4; ++dy) {
+            int y = cy + dy;
+            if (y < 0 || y >= W_H) continue;
+            for (int dx = -4; dx <= 4; ++dx) {
+                int xx = cx + dx;
+                if (xx < 0 || xx >= W_W || x->food[y * W_W + xx] <= 0) continue;
+                int kind = x->kind[y * W_W + xx];
+                float fx = xx + 0.5f, fy = y + 0.5f;
+                float distance = (fx - old_x) * (fx - old_x) + (fy - old_y) * (fy - old_y);
+                if (distance < nearest[kind]) {
+                    nearest[kind] = distance;
+                    target_x[kind] = fx;
+                    target_y[kind] = fy;
+                }
+            }
+        }
+        for (int kind = 0; kind < 3; ++kind)
+            if (nearest[kind] < 1e9f) {
+                b.behavior.approach_progress[age_bin][kind] +=
+                    sqrtf(nearest[kind]) - OHYPOT(target_x[kind] - b.x, target_y[kind] - b.y);
+                b.behavior.approach_travel[age_bin][kind] += travel;
+            }
+    }
+    int active_neurons = 0;
+    for (int n = b.neuron_head; n >= 0; n = w->neuron_next[n]) active_neurons += NG[n].active;
+    b.energy -= 0.003f + active_neurons * 0.00002f + thrust * 0.02f + (x->bite_intent[a] ? 0.02f : 0.0f);
+    b.fullness = fmaxf(0, b.fullness - 0.05f);
+    b.pain *= 0.8f;
+    for (int k = 0; k < 4; ++k) b.taste[k] *= 0.7f;
+    int food_cell = or_cell(old_x, old_y);
+    int food_offered = x->food[food_cell] > 0;
+    if (food_offered) {
+        int kind = x->kind[food_cell];
+        ++b.behavior.opportunities[age_bin][hungry ? 0 : 1][kind];
+    } else {
+        ++b.behavior.empty_steps[age_bin][hungry ? 0 : 1];
+        b.behavior.empty_eat[age_bin][hungry ? 0 : 1] += eat;
+    }
+    if (eat && x->food[food_cell] > 0) {                       /* harvest */
+        --x->food[food_cell];
+        int kind = x->kind[food_cell];
+        if (!food_offered) ++b.behavior.opportunities[age_bin][hungry ? 0 : 1][kind];
+        ++b.behavior.accepted[age_bin][hungry ? 0 : 1][kind];
+        if (kind == 1 && b.behavior.first_b_age == 0) b.behavior.first_b_age = b.age + 1;
+        b.taste[kind] = 1;
+        b.fullness += 1;
+        if (kind == 0) b.energy = fminf(30, b.energy + 4);
+        if (kind == 1) { b.energy = fminf(30, b.energy + 2); b.health -= 1.4f; b.pain += 1.4f; }
+        if (b.fullness > 8) { b.health -= 0.8f; b.pain += 0.8f; }
+    }
+    if (b.energy <= 0) { b.energy = 0; b.health -= 0.15f; b.pain += 0.15f; }
+    ++b.age;
+    if (b.health <= 0 || b.age >= 10000) {
+        b.behavior.death_cause = b.age >= 10000 ? 4 : (b.energy <= 0 ? 2 : 3);
+        b.alive = 0;
+        ++*x->deaths;
+    }
+    A[a] = b;
+}
+
+void or_world_body_step(const or_world_pools *w, const or_world_eco *x, int64_t step) {
+    or_animal *A = (or_animal *)w->animals;
+    const int P = w->animal_capacity;
+    for (int a = 0; a < P; ++a)
+        if (A[a].alive == 1) or_body(w, x, a);
+    or_index(w, x);
+    or_bite *events = (or_bite *)x->bite_events;
+    for (int a = 0; a < P; ++a) {                              /* src/main.cu:1251-1276 */
+        if (A[a].alive != 1 || !x->bite_intent[a]) continue;
+        int c = or_cell(A[a].x, A[a].y);
+        for (int prey = x->cell_head[c]; prey >= 0; prey = x->cell_next[prey]) {
+            if (prey == a || A[prey].alive != 1) continue;
+            float previous = A[prey].health;
+            A[prey].health = previous + -2.0f;
+            A[prey].pain += 2.0f;
+            ++*x->bites;
+            if (events) {
+                int event = (*x->bite_event_count)++;
+                if (event < 2 * P) {
+                    or_bite e = {step, A[a].id, A[prey].id, A[prey].x, A[prey].y};
+                    events[event] = e;
+                }
+            }
+            if (previous <= 2.0f && A[prey].alive == 1) {
+                A[prey].alive = -2;
+                A[a].energy += fmaxf(0.0f, A[prey].energy) * 0.45f;
+                A[a].taste[3] = 1.0f;
+                A[a].fullness += 1.0f;
+            }
+            break;
+        }
+    }
+    for (int a = 0; a < P; ++a) {                              /* src/main.cu:1278-1285 */
+        if (A[a].alive != -2) continue;
+        A[a].behavior.death_cause = 1;
+        A[a].alive = 0;
+        ++*x->deaths;
+        ++*x->predation_deaths;
+    }
+}
+
+void or_world_reclaim(const or_world_pools *w, const or_world_eco *x, int64_t step) {   /* 1302-1338 */
+    or_animal *A = (or_animal *)w->animals;
+    const ngene *NG = (const ngene *)w->neurons;
+    const sgene *SG = (const sgene *)w->synapses;
+    const sstate *SS = (const sstate *)w->synapse_state;
+    int *nowner = (int *)w->neuron_owner, *sowner = (int *)w->synapse_owner;
+    for (int a = 0; a < w->animal_capacity; ++a) {
+        if (A[a].alive != 0) continue;
+        or_animal body = A[a];
+        if (body.neuron_head < 0 && body.synapse_head < 0) continue;
+        int index = (*x->life_count)++;
+        if (x->life_records && index < x->life_capacity) {
+            or_life rec;
+            memset(&rec, 0, sizeof rec);
+            rec.body = body;
+            rec.death_step = step;
+            for (int n = body.neuron_head; n >= 0; n = w->neuron_next[n]) {
+                rec.active_neurons += NG[n].active;
+                rec.modulatory_neurons += NG[n].active && NG[n].modulator != 0;
+            }
+            float total = 0;
+            for (int e = body.synapse_head; e >= 0; e = w->synapse_next[e]) {
+                const sgene *g = &SG[e];
+                int active = g->active && NG[g->pre].active && NG[g->post].active;
+                rec.active_synapses += active;
+                rec.plastic_synapses += active && g->plast != 0 && !NG[g->pre].inh_tx &&
+                                        or_excitatory(NG[g->pre].type) && NG[g->pre].modulator == 0 &&
+                                        !NG[g->post].inh_tx && or_excitatory(NG[g->post].type);
+                if (active) total += fabsf(SS[e].w - g->w0);
+            }
+            rec.mean_abs_weight_change = rec.active_synapses > 0 ? total / rec.active_synapses : 0;
+            ((or_life *)x->life_records)[index] = rec;
+        }
+        for (int e = body.synapse_head; e >= 0;) {             /* release_genome, 436-454 */
+            int next = w->synapse_next[e];
+            sowner[e] = -1;
+            x->synapse_used[e / 32] &= ~(1u << (e % 32));
+            e = next;
+        }
+        for (int n = body.neuron_head; n >= 0;) {
+            int next = w->neuron_next[n];
+            nowner[n] = -1;
+            x->neuron_used[n / 32] &= ~(1u << (n % 32));
+            n = next;
+        }
+        body.neuron_head = body.synapse_head = -1;
+        body.neuron_count = body.synapse_count = 0;
+        for (int p = 0; p < W_S + W_M; ++p) body.ports[p] = -1;
+        A[a] = body;
+    }
+}
+
+void or_world_regrow_and_sense(const or_world_pools *w, const or_world_eco *x, int64_t step,
+                               unsigned long long seed, float renewal) {
+    for (int c = 0; c < W_CELLS; ++c) {                        /* regrow, 1138-1144 */
+        if (x->food[c] != 0) continue;
+        unsigned long long rng = or_seed_for(seed + (unsigned long long)step, (unsigned long long)c);
+        if (or_uniform(&rng) < renewal) x->food[c] = 1;
+    }
+    or_index(w, x);
+    const or_animal *A = (const or_animal *)w->animals;
+    float *senses = (float *)w->senses;
+    for (int a = 0; a < w->animal_capacity; ++a) {             /* update_senses, 619-657 */
+        if (A[a].alive != 1) continue;
+        or_animal b = A[a];
+        float *out = senses + (size_t)a * W_S;
+        for (int s = 0; s < 6; ++s) {
+            float angle = b.heading + (s % 3 - 1) * 0.7f;
+            float level = 0;
+            for (int range = 1; range <= 4; ++range) {
+                int c = or_cell(b.x + OCOS(angle) * range, b.y + OSIN(angle) * range);
+                if (x->kind[c] == s / 3 && x->food[c] > 0) level += 0.25f;
+            }
+            out[s] = or_clamp(level, 0, 1);
+        }
+        out[6] = or_clamp((16.0f - b.energy) / 16.0f, 0, 1);
+        out[7] = or_clamp(b.fullness / 8.0f, 0, 1);
+        out[8] = or_clamp(b.pain / 3.0f, 0, 1);
+        for (int k = 0; k < 3; ++k) out[9 + k] = or_clamp(b.taste[k], 0, 1);
+        for (int direction = 0; direction < 3; ++direction) {
+            float angle = b.heading + (direction - 1) * 0.7f;
+            float level = 0;
+            for (int range = 1; range <= 4; ++range) {
+                int c = or_cell(b.x + OCOS(angle) * range, b.y + OSIN(angle) * range);
+                for (int other = x->cell_head[c]; other >= 0; other = x->cell_next[other])
+                    if (other != a && A[other].alive == 1) level += 0.25f;
+            }
+            out[12 + direction] = or_clamp(level, 0, 1);
+        }
+        out[15] = or_clamp(b.taste[3], 0, 1);
+        int contact = or_cell(b.x, b.y);
+        for (int kind = 0; kind < 3; ++kind)
+            out[W_CONTACT + kind] = x->food[contact] > 0 && x->kind[contact] == kind ? 1.0f : 0.0f;
+    }
 }

@@ -72,6 +72,9 @@ const char *or_shadow_field(int i);
 /* Correctly rounded binary32 exp/log (or_crmath.c). */
 float or_cr_expf(float x);
 float or_cr_logf(float x);
+float or_cr_sinf(float x);
+float or_cr_cosf(float x);
+float or_cr_hypotf(float x, float y);
 /* The exp/log this build binds the physiology to. */
 float or_bound_expf(float x);
 float or_bound_logf(float x);
@@ -120,6 +123,29 @@ void or_records(const or_brain *b, void *neuron_genes, void *neuron_states, void
  * SynapseState, then offsets of Animal.id, .age, .alive, .neuron_head,
  * .synapse_head, .neuron_count, .synapse_count, PlasticityCohort.frozen. */
 int or_world_layout(uint64_t *out);
+
+/* World ecology (src/main.cu:612-657, 1138-1338), the reference kernels run
+ * as loops in ascending animal slot order. Fields as the library's
+ * NsbWorldEcology (host pointers). */
+typedef struct or_world_eco {
+    int *food, *kind, *cell_head, *cell_next;
+    unsigned char *bite_intent;
+    uint32_t *neuron_used, *synapse_used;
+    int *founder_motor_steps;
+    int *founder_observed_steps, *deaths, *predation_deaths, *bites;
+    void *life_records;
+    int *life_count;
+    void *bite_events;
+    int *bite_event_count;
+    int initial_count, instant_motors, life_capacity;
+} or_world_eco;
+/* body_step, spatial index, bite_animals, finish_predation. */
+void or_world_body_step(const or_world_pools *w, const or_world_eco *x, int64_t step);
+/* reclaim_dead_genomes with release_genome. */
+void or_world_reclaim(const or_world_pools *w, const or_world_eco *x, int64_t step);
+/* regrow, spatial index, update_senses. */
+void or_world_regrow_and_sense(const or_world_pools *w, const or_world_eco *x, int64_t step,
+                               unsigned long long seed, float renewal);
 
 /* Reference protocol checks (tests/physiology.cpp, tests/event_synapses.cpp,
  * tests/cuda_relay_parity.cu restated); results written as floats. */

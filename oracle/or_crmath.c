@@ -78,3 +78,53 @@ float or_cr_logf(float x) {
     if (ok) return r;
     abort();
 }
+
+/* sin, cos, hypot for the reference world's body and sense kernels
+ * (src/main.cu:619-657, 1146-1249), bracketed the same way: glibc binary64
+ * (error below 1 ulp of binary64), then x87 long double, then binary128. */
+float or_cr_sinf(float x) {
+    if (isnan(x) || isinf(x)) return (x - x) / (x - x);
+    if (x == 0) return x;
+    int ok;
+    float r = bracket_d(sin((double)x), 0x1p-48, &ok);
+    if (ok) return r;
+    r = bracket_ld(sinl((long double)x), 0x1p-58L, &ok);
+    if (ok) return r;
+    r = bracket_q(sinq((__float128)x), 0x1p-100Q, &ok);
+    if (ok) return r;
+    abort();
+}
+
+float or_cr_cosf(float x) {
+    if (isnan(x) || isinf(x)) return (x - x) / (x - x);
+    int ok;
+    float r = bracket_d(cos((double)x), 0x1p-48, &ok);
+    if (ok) return r;
+    r = bracket_ld(cosl((long double)x), 0x1p-58L, &ok);
+    if (ok) return r;
+    r = bracket_q(cosq((__float128)x), 0x1p-100Q, &ok);
+    if (ok) return r;
+    abort();
+}
+
+float or_cr_hypotf(float x, float y) {
+    if (isinf(x) || isinf(y)) return INFINITY;
+    if (isnan(x) || isnan(y)) return x + y;
+    if (x == 0 && y == 0) return 0.0f;
+    int ok;
+    float r = bracket_d(hypot((double)x, (double)y), 0x1p-48, &ok);
+    if (ok) return r;
+    r = bracket_ld(hypotl((long double)x, (long double)y), 0x1p-58L, &ok);
+    if (ok) return r;
+    /* x^2 and y^2 are exact in binary128; an exact midpoint (possible for
+     * sums of squares) is settled by comparing squares exactly. */
+    __float128 xq = x, yq = y, q = sqrtq(xq * xq + yq * yq);
+    r = bracket_q(q, 0x1p-100Q, &ok);
+    if (ok) return r;
+    float lo = (float)(q * (1 - 0x1p-100Q)), hi = (float)(q * (1 + 0x1p-100Q));
+    __float128 mid = ((__float128)lo + (__float128)hi) / 2, s = xq * xq + yq * yq;
+    if (mid * mid < s) return hi;
+    if (mid * mid > s) return lo;
+    uint32_t lb; memcpy(&lb, &lo, 4);
+    return (lb & 1u) ? hi : lo;
+}

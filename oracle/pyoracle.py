@@ -65,6 +65,13 @@ def oracle_lib(libm=False):
         lib.or_world_step.argtypes = [ct.c_void_p, ct.c_int64]
         lib.or_world_step.restype = ct.c_int
         lib.or_world_homeostasis.argtypes = [ct.c_void_p]
+        lib.or_world_body_step.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int64]
+        lib.or_world_reclaim.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int64]
+        lib.or_world_regrow_and_sense.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int64, ct.c_ulonglong,
+                                                  ct.c_float]
+        for fn in ("or_cr_sinf", "or_cr_cosf"):
+            getattr(lib, fn).argtypes = [ct.c_float]; getattr(lib, fn).restype = ct.c_float
+        lib.or_cr_hypotf.argtypes = [ct.c_float, ct.c_float]; lib.or_cr_hypotf.restype = ct.c_float
         lib.or_records.argtypes = [ct.c_void_p] * 5
         lib.or_world_layout.argtypes = [ct.POINTER(ct.c_uint64)]
         lib.or_world_layout.restype = ct.c_int
@@ -156,6 +163,23 @@ def world_homeostasis(pools):
     lib = oracle_lib()
     st = pools.struct()
     lib.or_world_homeostasis(ct.byref(st))
+
+
+def world_body_step(pools, eco, step):
+    """The oracle's body step, spatial index, bites and predation deaths
+    (or_world_body_step) on host WorldPools and Ecology, in place."""
+    oracle_lib().or_world_body_step(ct.byref(pools.struct()), ct.byref(eco.struct()), int(step))
+
+
+def world_reclaim(pools, eco, step):
+    """The oracle's reclaim_dead_genomes (or_world_reclaim), in place."""
+    oracle_lib().or_world_reclaim(ct.byref(pools.struct()), ct.byref(eco.struct()), int(step))
+
+
+def world_regrow_and_sense(pools, eco, step, seed, renewal_probability):
+    """The oracle's regrow, spatial index and update_senses, in place."""
+    oracle_lib().or_world_regrow_and_sense(ct.byref(pools.struct()), ct.byref(eco.struct()), int(step), int(seed),
+                                           float(renewal_probability))
 
 
 def oracle_records(batch, seeds):

@@ -1,11 +1,11 @@
 /* ORACLE — test infrastructure only.
  * Force-included (-include) when the reference world simulator's kernels are
  * compiled for the correctly rounded comparison (no fast math, no FMA
- * contraction): every expf/logf call in the reference sources, host or
- * device, resolves to a correctly rounded binary32 exp/log. The device
- * implementation is the library's nsx::expf_cr / nsx::logf_cr, whose results
- * the oracle's exhaustive test checks against an independent binary128
- * evaluation for all 2^32 inputs; a correctly rounded result is unique, so any
+ * contraction): every expf/logf/cosf/sinf/hypotf call in the reference
+ * sources, host or device, resolves to a correctly rounded binary32 function. The device
+ * implementation is the library's nsx::expf_cr / nsx::logf_cr (and the
+ * trigonometric and hypot functions beside them), whose results the oracle's
+ * sweeps check against an independent binary128 evaluation; a correctly rounded result is unique, so any
  * correct implementation gives the same bits. */
 #pragma once
 #include <cuda_runtime.h>
@@ -19,3 +19,6 @@
 #include "ns_crmath.h"
 #define expf(x) nsx::expf_cr(x)
 #define logf(x) nsx::logf_cr(x)
+#define cosf(x) nsx::cosf_cr(x)
+#define sinf(x) nsx::sinf_cr(x)
+#define hypotf(x, y) nsx::hypotf_cr(x, y)

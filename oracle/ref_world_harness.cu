@@ -450,4 +450,165 @@ int ref_world_layout(uint64_t *values, uint64_t *hash, uint64_t *offsets) {
     return 20;
 }
 
+
+// ---- the reference's world ecology kernels (src/main.cu:612-657, 1138-1338) ----
+// On caller-owned pools (NsbWorldPools layout) and ecology state
+// (NsbWorldEcology layout), the build's full capacities. sequential = 1
+// replays every contended kernel one animal at a time in ascending slot order
+// (body_step, index_animals, bite_animals, reclaim_dead_genomes): before each
+// launch the other candidates are relabelled (alive 1 -> 1000 or 0 -> 1001, or
+// their bite intent cleared), so the unmodified kernel acts for one animal,
+// and the labels are restored after it. sequential = 0 launches the kernels
+// as the host loop does (src/main.cu:2745-2770).
+struct EcoArg {
+    int *food, *kind, *cell_head, *cell_next;
+    unsigned char *bite_intent;
+    uint32_t *neuron_used, *synapse_used;
+    int *founder_motor_steps, *founder_observed_steps, *deaths, *predation_deaths, *bites;
+    void *life_records;
+    int *life_count;
+    void *bite_events;
+    int *bite_event_count;
+    int initial_count, instant_motors, life_capacity;
+};
+
+__global__ void ref_relabel(Device d, int keep, int from, int to) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < P && a != keep && d.animals[a].alive == from) d.animals[a].alive = to;
+}
+__global__ void ref_keep_intent(Device d, const unsigned char *saved, int keep) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < P) d.bite_intent[a] = a == keep ? saved[a] : 0;
+}
+
+struct EcoWorld {
+    Device d{};
+    unsigned char *saved_intent = nullptr;
+    std::vector<int> alive;
+};
+
+static void read_alive(EcoWorld &h) {
+    h.alive.resize(P);
+    cudaMemcpy2D(h.alive.data(), sizeof(int), &h.d.animals[0].alive, sizeof(Animal), sizeof(int), P,
+                 cudaMemcpyDeviceToHost);
+}
+static void index_stage(EcoWorld &h, int sequential) {
+    Device &d = h.d;
+    cudaMemset(d.cell_head, 0xff, W * H * sizeof(int));
+    if (!sequential) {
+        index_animals<<<(P + 127) / 128, 128>>>(d);
+        return;
+    }
+    read_alive(h);
+    for (int a = 0; a < P; ++a) {
+        if (h.alive[a] != 1) continue;
+        ref_relabel<<<(P + 255) / 256, 256>>>(d, a, 1, 1000);
+        index_animals<<<(P + 127) / 128, 128>>>(d);
+        ref_relabel<<<(P + 255) / 256, 256>>>(d, -1, 1000, 1);
+    }
+}
+
+void *ref_world_eco_create(const void *pools, const void *ecology) {
+    const PoolsArg &p = *static_cast<const PoolsArg *>(pools);
+    const EcoArg &x = *static_cast<const EcoArg *>(ecology);
+    if (p.animal_capacity != P || p.neuron_capacity != NEURON_CAPACITY || p.synapse_capacity != SYNAPSE_CAPACITY)
+        return nullptr;
+    if (x.life_records && x.life_capacity != LIFE_RECORD_CAPACITY) return nullptr;
+    auto *h = new EcoWorld;
+    Device &d = h->d;
+    d.initial_count = x.initial_count;
+    d.instant_motors = x.instant_motors != 0;
+    d.trace_animal = -1;
+    d.animals = static_cast<Animal *>(p.animals);
+    d.plasticity_cohort = static_cast<PlasticityCohort *>(p.plasticity_cohort);
+    d.neurons = static_cast<NeuronGene *>(p.neurons);
+    d.synapses = static_cast<SynapseGene *>(p.synapses);
+    d.neuron_state = static_cast<NeuronState *>(p.neuron_state);
+    d.synapse_state = static_cast<SynapseState *>(p.synapse_state);
+    d.pending_exc = p.pending_exc; d.pending_inh = p.pending_inh; d.senses = p.senses;
+    d.mod_event_tick = p.mod_event_tick; d.spike_history = p.spike_history;
+    d.neuron_owner = p.neuron_owner; d.synapse_owner = p.synapse_owner;
+    d.neuron_next = p.neuron_next; d.synapse_next = p.synapse_next; d.neuron_port = p.neuron_port;
+    d.motors = p.motors;
+    d.food = x.food; d.kind = x.kind; d.cell_head = x.cell_head; d.cell_next = x.cell_next;
+    d.bite_intent = x.bite_intent;
+    d.neuron_used = x.neuron_used; d.synapse_used = x.synapse_used;
+    d.founder_motor_steps = x.founder_motor_steps; d.founder_observed_steps = x.founder_observed_steps;
+    d.deaths = x.deaths; d.predation_deaths = x.predation_deaths; d.bites = x.bites;
+    d.life_records = static_cast<LifeRecord *>(x.life_records);
+    d.life_count = x.life_count;
+    d.bite_events = static_cast<BiteEvent *>(x.bite_events);
+    d.bite_event_count = x.bite_event_count;
+    if (cudaMalloc(&h->saved_intent, P) != cudaSuccess) {
+        delete h;
+        return nullptr;
+    }
+    return h;
+}
+
+int ref_world_eco_body(void *p, long long step, int sequential) {
+    EcoWorld &h = *static_cast<EcoWorld *>(p);
+    Device &d = h.d;
+    if (!sequential) {
+        body_step<<<(P + 127) / 128, 128>>>(d);
+    } else {
+        read_alive(h);
+        for (int a = 0; a < P; ++a) {
+            if (h.alive[a] != 1) continue;
+            ref_relabel<<<(P + 255) / 256, 256>>>(d, a, 1, 1000);
+            body_step<<<(P + 127) / 128, 128>>>(d);
+            ref_relabel<<<(P + 255) / 256, 256>>>(d, -1, 1000, 1);
+        }
+    }
+    index_stage(h, sequential);
+    if (!sequential) {
+        bite_animals<<<(P + 127) / 128, 128>>>(d, step);
+    } else {
+        std::vector<unsigned char> intent(P);
+        cudaMemcpy(h.saved_intent, d.bite_intent, P, cudaMemcpyDeviceToDevice);
+        cudaMemcpy(intent.data(), d.bite_intent, P, cudaMemcpyDeviceToHost);
+        for (int a = 0; a < P; ++a) {
+            if (!intent[a]) continue;
+            ref_keep_intent<<<(P + 255) / 256, 256>>>(d, h.saved_intent, a);
+            bite_animals<<<(P + 127) / 128, 128>>>(d, step);
+        }
+        cudaMemcpy(d.bite_intent, h.saved_intent, P, cudaMemcpyDeviceToDevice);
+    }
+    finish_predation<<<(P + 127) / 128, 128>>>(d);
+    return (int)cudaDeviceSynchronize();
+}
+
+int ref_world_eco_reclaim(void *p, long long step, int sequential) {
+    EcoWorld &h = *static_cast<EcoWorld *>(p);
+    Device &d = h.d;
+    if (!sequential) {
+        reclaim_dead_genomes<<<(P + 127) / 128, 128>>>(d, step);
+        return (int)cudaDeviceSynchronize();
+    }
+    read_alive(h);
+    for (int a = 0; a < P; ++a) {
+        if (h.alive[a] != 0) continue;
+        ref_relabel<<<(P + 255) / 256, 256>>>(d, a, 0, 1001);
+        reclaim_dead_genomes<<<(P + 127) / 128, 128>>>(d, step);
+        ref_relabel<<<(P + 255) / 256, 256>>>(d, -1, 1001, 0);
+    }
+    return (int)cudaDeviceSynchronize();
+}
+
+int ref_world_eco_regrow_and_sense(void *p, long long step, unsigned long long seed, float renewal,
+                                   int sequential) {
+    EcoWorld &h = *static_cast<EcoWorld *>(p);
+    Device &d = h.d;
+    regrow<<<(W * H + 255) / 256, 256>>>(d, step, seed, renewal);
+    index_stage(h, sequential);
+    update_senses<<<(P + 127) / 128, 128>>>(d);
+    return (int)cudaDeviceSynchronize();
+}
+
+void ref_world_eco_destroy(void *p) {
+    auto *h = static_cast<EcoWorld *>(p);
+    cudaFree(h->saved_intent);
+    delete h;
+}
+
 }  // extern "C"

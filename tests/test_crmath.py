@@ -1,7 +1,9 @@
-"""Correctly rounded exp/log: the product implementation (csrc/ns_crmath.h,
-built into oracle/_build/exhaustive_math) against the oracle's independent
-long-double/binary128 implementation, over a strided sample of all binary32
-inputs (the full 2^32 sweep is `oracle/_build/exhaustive_math exp 8 1`)."""
+"""Correctly rounded exp, log, sin, cos and hypot: the product implementation
+(csrc/ns_crmath.h, built into oracle/_build/exhaustive_math) against the
+oracle's independent long-double/binary128 implementation, over a strided
+sample of all binary32 inputs (the full 2^32 sweep is
+`oracle/_build/exhaustive_math exp 8 1`; hypot pairs each input with four
+partners, Pythagorean ratios among them)."""
 import json
 import subprocess
 
@@ -11,7 +13,7 @@ import pytest
 from oracle.pyoracle import oracle_lib
 
 
-@pytest.mark.parametrize("fn", ["exp", "log"])
+@pytest.mark.parametrize("fn", ["exp", "log", "sin", "cos", "hypot"])
 def test_sampled_sweep_matches_independent_cr(oracle_built, fn):
     from oracle.build import BUILD
     out = subprocess.run([str(BUILD / "exhaustive_math"), fn, "4", "1009"], capture_output=True, text=True)
@@ -51,3 +53,26 @@ def test_cr_exp_special_values(oracle_built):
     assert lib.or_cr_expf(-200.0) == 0.0
     assert np.isinf(lib.or_cr_expf(100.0))
     assert np.isnan(lib.or_cr_expf(float("nan")))
+
+
+def test_trig_special_values(oracle_built):
+    lib = oracle_lib()
+    import ctypes
+    for name in ("or_cr_sinf", "or_cr_cosf"):
+        getattr(lib, name).argtypes = [ctypes.c_float]
+        getattr(lib, name).restype = ctypes.c_float
+    lib.or_cr_hypotf.argtypes = [ctypes.c_float, ctypes.c_float]
+    lib.or_cr_hypotf.restype = ctypes.c_float
+    assert np.float32(lib.or_cr_sinf(-0.0)).tobytes() == np.float32(-0.0).tobytes()
+    assert lib.or_cr_cosf(0.0) == 1.0
+    assert np.isnan(lib.or_cr_sinf(float("inf"))) and np.isnan(lib.or_cr_cosf(float("nan")))
+    assert lib.or_cr_hypotf(3.0, 4.0) == 5.0
+    assert np.isinf(lib.or_cr_hypotf(float("nan"), float("-inf")))
+    assert np.isnan(lib.or_cr_hypotf(float("nan"), 1.0))
+    # headings far from the origin (the reference's headings grow without bound)
+    import mpmath
+    mpmath.mp.prec = 200
+    for x in (12007.25, -3.0e4, 1.0e30, 3.4e38, 7.853981e-1, 1.5707964):
+        xf = float(np.float32(x))
+        assert np.float32(lib.or_cr_sinf(xf)) == np.float32(float(mpmath.sin(xf))), x
+        assert np.float32(lib.or_cr_cosf(xf)) == np.float32(float(mpmath.cos(xf))), x
