@@ -18,6 +18,9 @@ e2e   : the same metric through the reference's C ABI call ns_gpu_step with
 
 --world : the world simulator's neural stage (config 2 founders, or --world-population
         full) through nsb_world_*, then the reference's world kernels on the same pools.
+--world-loop : the world step without reproduction (neural stage, body, bites,
+        homeostasis, reclamation, regrowth, senses), closed loop, then the
+        reference's kernels for the same steps on the same initial pools.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
        (N > 1 under torch.distributed.run: one full-pool replica per GPU).
@@ -778,6 +781,147 @@ def run_world_stage(args, rank, world, local_rank):
         print(json.dumps(ref_line), flush=True)
 
 
+def run_world_loop(args, rank, world, local_rank):
+    """The world step without reproduction, in the reference host loop's order
+    (src/main.cu:2634-2770): neural stage, body step with spatial index, bites
+    and predation deaths, homeostasis, genome reclamation, regrowth and senses,
+    closed loop (each step's senses drive the next). This library's stages,
+    then the reference's own kernels (the world binary's flags, launched as
+    its host loop launches them) on the same initial pools. Rank 0 only."""
+    import ctypes as ct
+    import torch
+    if rank != 0:
+        return
+    torch.cuda.set_device(local_rank)
+    sys.path.insert(0, str(ROOT))
+    nsb = load_package()
+    W = nsb.world
+    batch, pools = world_population(nsb, args.world_population, args.world_founders, False)
+    W.place_bodies(pools, 3)
+    seed, renewal = 2, 0.0006                     # the simulator's defaults (src/main.cu:1937)
+    eco = W.make_ecology(pools, seed=seed, initial_count=batch.brains, life_capacity=32768 * 16)
+    B = batch.brains
+    warm = max(args.warmup, 3)
+
+    def timed(step_fn, label):
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e = [None, torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)]
+        k = 0
+        for _ in range(warm):
+            k += 1
+            step_fn(k, None)
+        torch.cuda.synchronize()
+        eco_ms = 0.0
+        neurons = 0
+        with ClockSampler(local_rank) as clk:
+            start.record()
+            for _ in range(args.steps):
+                k += 1
+                neurons += step_fn(k, e)
+                eco_ms += e[1].elapsed_time(e[2])
+            end.record()
+            torch.cuda.synchronize()
+        return start.elapsed_time(end) / args.steps, eco_ms / args.steps, neurons, clk.summary()
+
+    def live_neurons(p):
+        A = p.animals
+        return int(A["neuron_count"][A["alive"] == 1].sum())
+
+    # ---- this library
+    stage = W.World(pools)
+    stage.attach_ecology(eco)
+    stage.regrow_and_sense(0, seed, 0.0)
+    alive_n = [live_neurons(pools)]
+
+    def ours(k, ev):
+        stage.neural_step(k)
+        if ev:
+            ev[1].record()
+        stage.body_step(k)
+        stage.homeostasis()
+        stage.reclaim(k)
+        stage.regrow_and_sense(k, seed, renewal)
+        if ev:
+            ev[2].record()
+            ev[2].synchronize()
+        n = stage.stats()["neurons"]
+        return n
+
+    ms, eco_ms, neuron_steps, clk = timed(ours, "ours")
+    fin = stage.download_ecology()
+    stage.close()
+    del stage
+    torch.cuda.empty_cache()
+    line = {"metric": "neuron-ticks/s of the world step (neural stage + ecology, no reproduction)",
+            "value": neuron_steps * 16 / (ms * args.steps / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": warm, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (Philox4x32-10, seed 2); food grid of init_world seed 2",
+            "config": {"workload": f"world_loop_founders_{B}" if args.world_population == "founders"
+                       else "world_loop_full", "animals": B, "neurons_at_start": alive_n[0],
+                       "food_renewal": renewal, "pools": "reference capacities (32,768 / 4,194,304 / 8,388,608)",
+                       "step": "neural_step, body_step, homeostasis, reclaim, regrow_and_sense (4 host syncs)"},
+            "ecology_ms_per_step": eco_ms,
+            "world_counts": {"deaths": int(fin.deaths[0]), "bites": int(fin.bites[0]),
+                             "life_records": int(fin.life_count[0])},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+    # ---- the reference's kernels on the same initial pools
+    from oracle import pyoracle
+    wlib = pyoracle.ref_world_lib()
+    if wlib is None or not hasattr(wlib, "ref_world_eco_create"):
+        print(json.dumps({"impl": "reference-cuda-world-loop", "unavailable": "oracle/_ref/libns_ref_world.so not built"}))
+        return
+    wlib.ref_world_pools_create.restype = ct.c_void_p
+    wlib.ref_world_pools_create.argtypes = [ct.c_void_p, ct.c_int]
+    wlib.ref_world_pools_step.argtypes = [ct.c_void_p, ct.c_longlong]
+    wlib.ref_world_pools_homeostasis.argtypes = [ct.c_void_p]
+    wlib.ref_world_pools_destroy.argtypes = [ct.c_void_p]
+    wlib.ref_world_eco_create.restype = ct.c_void_p
+    wlib.ref_world_eco_create.argtypes = [ct.c_void_p, ct.c_void_p]
+    wlib.ref_world_eco_body.argtypes = [ct.c_void_p, ct.c_longlong, ct.c_int]
+    wlib.ref_world_eco_reclaim.argtypes = [ct.c_void_p, ct.c_longlong, ct.c_int]
+    wlib.ref_world_eco_regrow_and_sense.argtypes = [ct.c_void_p, ct.c_longlong, ct.c_ulonglong, ct.c_float,
+                                                    ct.c_int]
+    wlib.ref_world_eco_destroy.argtypes = [ct.c_void_p]
+    for mode, label in ((0, "fused global-slot kernels"), (1, "--block-brains tiers + global-slot fallback")):
+        holder = W.World(pools)          # device copies of the pools and ecology, in the shared layouts
+        holder.attach_ecology(eco)
+        h = wlib.ref_world_pools_create(ct.byref(holder.struct), mode)
+        x = wlib.ref_world_eco_create(ct.byref(holder.struct), ct.byref(holder.eco_struct))
+        if not h or not x:
+            print(json.dumps({"impl": "reference-cuda-world-loop", "unavailable": "pool setup failed"}))
+            holder.close()
+            continue
+        wlib.ref_world_eco_regrow_and_sense(x, 0, seed, 0.0, 0)
+
+        def theirs(k, ev):
+            wlib.ref_world_pools_step(h, k)
+            if ev:
+                ev[1].record()
+            wlib.ref_world_eco_body(x, k, 0)
+            wlib.ref_world_pools_homeostasis(h)
+            wlib.ref_world_eco_reclaim(x, k, 0)
+            wlib.ref_world_eco_regrow_and_sense(x, k, seed, renewal, 0)
+            if ev:
+                ev[2].record()
+                ev[2].synchronize()
+            return 0
+
+        rms, reco_ms, _, rclk = timed(theirs, label)
+        wlib.ref_world_eco_destroy(x)
+        wlib.ref_world_pools_destroy(h)
+        holder.close()
+        del holder
+        torch.cuda.empty_cache()
+        print(json.dumps({"impl": "reference-cuda-world-loop", "metric": "ms per world step (neural stage + "
+                          "ecology, no reproduction)", "value": rms, "unit": "ms", "higher_is_better": False,
+                          "steps": args.steps, "warmup": warm, "ecology_ms_per_step": reco_ms,
+                          "ours_ms_per_step": ms, "ours_ecology_ms_per_step": eco_ms,
+                          "config": dict(line["config"], kernel=f"src/main.cu, {label}, --use_fast_math, sm_100a"),
+                          "clocks": rclk}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -804,12 +948,16 @@ def main():
     ap.add_argument("--world-founders", type=int, default=2048, help="founders of the config-2 population")
     ap.add_argument("--world-compact", action="store_true",
                     help="pools sized to the population, no reference leg (profiler captures)")
+    ap.add_argument("--world-loop", action="store_true",
+                    help="the world step without reproduction: neural stage + ecology, closed loop")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus if "RANK" in os.environ else 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.serve:
         run_serve(args, rank, world, local_rank)
+    elif args.world_loop:
+        run_world_loop(args, rank, world, local_rank)
     elif args.world:
         run_world_stage(args, rank, world, local_rank)
     elif args.impl == "reference":

@@ -87,6 +87,7 @@ struct Eco {
     int *acnt, *astart, *afill, *alist, *asort;  // living animals by cell; asort: highest slot first
     unsigned char *flag;                         // per animal: bit, or reclaimed
     int *prey, *rank, *base;                     // base[0]: first index of this call's records
+    int *active;                                 // active neurons per animal
     int *status;
 };
 
@@ -130,16 +131,21 @@ __device__ int food_at(const Eco &e, int c, int a) {
 // receives *accumulate and *accumulate grows by the total.
 template <class T>
 __global__ void __launch_bounds__(1024) eco_scan(const T *in, int n, int *out, int *accumulate, int *base_out) {
+    constexpr int kPer = 8, kChunk = 1024 * kPer;
+    __shared__ int buf[kChunk];
     __shared__ int warp_sum[32];
     __shared__ int carry;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     if (t == 0) carry = 0;
-    __syncthreads();
-    for (int chunk = 0; chunk < n; chunk += 1024 * 16) {
-        int v[16], s = 0;
-        for (int k = 0; k < 16; ++k) {
-            const int i = chunk + t * 16 + k;
-            v[k] = i < n ? (int)in[i] : 0;
+    for (int chunk = 0; chunk < n; chunk += kChunk) {
+        for (int k = 0; k < kPer; ++k) {                 // coalesced loads
+            const int i = chunk + k * 1024 + t;
+            buf[k * 1024 + t] = i < n ? (int)in[i] : 0;
+        }
+        __syncthreads();
+        int v[kPer], s = 0;
+        for (int k = 0; k < kPer; ++k) {
+            v[k] = buf[t * kPer + k];
             s += v[k];
         }
         int x = s;
@@ -159,12 +165,15 @@ __global__ void __launch_bounds__(1024) eco_scan(const T *in, int n, int *out, i
         }
         __syncthreads();
         int b = carry + x - s + (warp ? warp_sum[warp - 1] : 0);
-        for (int k = 0; k < 16; ++k) {
-            const int i = chunk + t * 16 + k;
-            if (i < n) out[i] = b;
+        for (int k = 0; k < kPer; ++k) {
+            buf[t * kPer + k] = b;
             b += v[k];
         }
         __syncthreads();
+        for (int k = 0; k < kPer; ++k) {                 // coalesced stores
+            const int i = chunk + k * 1024 + t;
+            if (i < n) out[i] = buf[k * 1024 + t];
+        }
         if (t == 0) carry += warp_sum[31];
         __syncthreads();
     }
@@ -188,6 +197,19 @@ __global__ void eco_place_eaters(Eco e) {
         if (A.alive != 1 || e.motors[(size_t)a * kM + 3] <= 0) continue;
         const int c = cell_of(A.x, A.y);
         e.elist[e.estart[c] + atomicAdd(&e.efill[c], 1)] = a;
+    }
+}
+
+// Active neurons of each living animal (its upkeep): over the neuron slots by
+// owner, which the simulator keeps equal to list membership (initialize_neuron
+// and release_genome / remove_hidden_neuron set and clear both together). An
+// integer sum, so the slot order of the additions does not matter.
+__global__ void eco_count_active(Eco e) {
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < e.ncap; n += gridDim.x * blockDim.x) {
+        const int a = e.nowner[n];
+        if (a < 0 || a >= e.P) continue;
+        const int on = e.ngene[n].active;
+        if (on && e.animals[a].alive == 1) atomicAdd(&e.active[a], on);
     }
 }
 
@@ -226,11 +248,20 @@ __global__ void __launch_bounds__(128) eco_body(Eco e) {
             for (int dy = -4; dy <= 4; ++dy) {
                 const int y = cy + dy;
                 if (y < 0 || y >= kH) continue;
-                for (int dx = -4; dx <= 4; ++dx) {
-                    const int x = cx + dx;
-                    if (x < 0 || x >= kW) continue;
+                int f[9], n[9];                                   // the row's stocks and eaters, loaded first
+#pragma unroll
+                for (int i = 0; i < 9; ++i) {
+                    const int x = cx - 4 + i;
+                    const bool in = x >= 0 && x < kW;
+                    f[i] = in ? e.food[y * kW + x] : 0;
+                    n[i] = in ? e.ecnt[y * kW + x] : 0;
+                }
+#pragma unroll
+                for (int i = 0; i < 9; ++i) {
+                    const int x = cx - 4 + i;
+                    if (x < 0 || x >= kW || f[i] <= 0) continue;
                     const int c = y * kW + x;
-                    if (food_at(e, c, a) <= 0) continue;
+                    if (n[i] && food_at(e, c, a) <= 0) continue;
                     const int kind = e.kind[c];
                     if (kind < 0 || kind > 2) { atomicOr(e.status, ES_KIND); continue; }
                     const float fx = x + 0.5f, fy = y + 0.5f;
@@ -249,12 +280,7 @@ __global__ void __launch_bounds__(128) eco_body(Eco e) {
                     bh.approach_travel[age_bin][kind] += travel;
                 }
         }
-        int active = 0, walked = 0;
-        for (int n = b.neuron_head; n >= 0 && walked <= b.neuron_count; n = e.nnext[n], ++walked) {
-            if (n >= e.ncap) { atomicOr(e.status, ES_SLOT); break; }
-            active += e.ngene[n].active;
-        }
-        if (walked != b.neuron_count) atomicOr(e.status, ES_LIST);
+        const int active = e.active[a];
         b.energy -= kBodyUpkeep + (float)active * kNeuronUpkeep + thrust * 0.02f + (bite ? kBiteCost : 0.0f);
         b.fullness = fmaxf(0.0f, b.fullness - 0.05f);
         b.pain *= 0.8f;
@@ -396,66 +422,65 @@ __global__ void eco_reclaim_flags(Eco e) {
         e.flag[a] = A.alive == 0 && (A.neuron_head >= 0 || A.synapse_head >= 0);
     }
 }
-// Walks one list, bounded by its count; false if it disagrees with the count.
-__device__ bool list_ok(const int *next, int head, int count, int cap) {
-    int k = 0;
-    for (int q = head; q >= 0 && k <= count; q = next[q], ++k)
-        if (q >= cap) return false;
-    return k == count;
-}
+// One pass over each list: the life record's sums and the release of the
+// slots together (release_genome only clears owners and bitmap bits, which
+// the record does not read). Walks stop after count + 1 entries; a list that
+// disagrees with its count is reported.
 __global__ void eco_reclaim(Eco e, int64_t step) {
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
         if (!e.flag[a]) continue;
         ref::Animal body = e.animals[a];
-        if (!list_ok(e.nnext, body.neuron_head, body.neuron_count, e.ncap) ||
-            !list_ok(e.snext, body.synapse_head, body.synapse_count, e.ecap)) {
-            atomicOr(e.status, ES_LIST);
-            continue;
-        }
         const int index = e.base[0] + e.rank[a];
-        if (e.life && index < e.life_capacity) {
-            ref::LifeRecord rec;
-            memset(&rec, 0, sizeof rec);
-            rec.body = body;
-            rec.death_step = step;
-            for (int n = body.neuron_head; n >= 0; n = e.nnext[n]) {
-                const ref::NeuronGene &g = e.ngene[n];
-                rec.active_neurons += g.active;
-                rec.modulatory_neurons += g.active && g.modulator != 0;
-            }
-            float total = 0;
-            for (int s = body.synapse_head; s >= 0; s = e.snext[s]) {
-                const ref::SynapseGene &g = e.sgene[s];
-                if ((unsigned)g.pre >= (unsigned)e.ncap || (unsigned)g.post >= (unsigned)e.ncap) {
-                    atomicOr(e.status, ES_SLOT);
-                    continue;
-                }
-                const ref::NeuronGene &pre = e.ngene[g.pre], &post = e.ngene[g.post];
-                const bool live = g.active && pre.active && post.active;
-                rec.active_synapses += live;
-                rec.plastic_synapses += live && g.plasticity != 0 && !pre.inh_tx && excitatory(pre.type) &&
-                                        pre.modulator == 0 && !post.inh_tx && excitatory(post.type);
-                if (live) total += fabsf(e.sstate[s].w - g.w0);
-            }
-            rec.mean_abs_weight_change = rec.active_synapses > 0 ? total / rec.active_synapses : 0;
-            e.life[index] = rec;
-        }
-        for (int s = body.synapse_head; s >= 0;) {
+        const bool record = e.life && index < e.life_capacity;
+        int active_n = 0, modulatory = 0, active_s = 0, plastic = 0, k = 0;
+        float total = 0;
+        for (int s = body.synapse_head; s >= 0 && k <= body.synapse_count; ++k) {
+            if (s >= e.ecap) { atomicOr(e.status, ES_SLOT); break; }
             const int next = e.snext[s];
+            if (record) {
+                const ref::SynapseGene &g = e.sgene[s];
+                if ((unsigned)g.pre < (unsigned)e.ncap && (unsigned)g.post < (unsigned)e.ncap) {
+                    const ref::NeuronGene &pre = e.ngene[g.pre], &post = e.ngene[g.post];
+                    const bool live = g.active && pre.active && post.active;
+                    active_s += live;
+                    plastic += live && g.plasticity != 0 && !pre.inh_tx && excitatory(pre.type) &&
+                               pre.modulator == 0 && !post.inh_tx && excitatory(post.type);
+                    if (live) total += fabsf(e.sstate[s].w - g.w0);
+                } else {
+                    atomicOr(e.status, ES_SLOT);
+                }
+            }
             e.sowner[s] = -1;
             atomicAnd(&e.sused[s / 32], ~(1u << (s % 32)));
             s = next;
         }
-        for (int n = body.neuron_head; n >= 0;) {
+        if (k != body.synapse_count) atomicOr(e.status, ES_LIST);
+        k = 0;
+        for (int n = body.neuron_head; n >= 0 && k <= body.neuron_count; ++k) {
+            if (n >= e.ncap) { atomicOr(e.status, ES_SLOT); break; }
             const int next = e.nnext[n];
+            const ref::NeuronGene &g = e.ngene[n];
+            active_n += g.active;
+            modulatory += g.active && g.modulator != 0;
             e.nowner[n] = -1;
             atomicAnd(&e.nused[n / 32], ~(1u << (n % 32)));
             n = next;
         }
-        body.neuron_head = body.synapse_head = -1;
-        body.neuron_count = body.synapse_count = 0;
-        for (int p = 0; p < kS + kM; ++p) body.ports[p] = -1;
-        e.animals[a] = body;
+        if (k != body.neuron_count) atomicOr(e.status, ES_LIST);
+        if (record) {
+            ref::LifeRecord &rec = e.life[index];
+            rec.body = body;
+            rec.death_step = step;
+            rec.active_neurons = active_n;
+            rec.active_synapses = active_s;
+            rec.modulatory_neurons = modulatory;
+            rec.plastic_synapses = plastic;
+            rec.mean_abs_weight_change = active_s > 0 ? total / active_s : 0;
+        }
+        ref::Animal &out = e.animals[a];
+        out.neuron_head = out.synapse_head = -1;
+        out.neuron_count = out.synapse_count = 0;
+        for (int p = 0; p < kS + kM; ++p) out.ports[p] = -1;
     }
 }
 
@@ -563,6 +588,7 @@ public:
         x_.prey = dev_zeros<int>(owned_, P);
         x_.rank = dev_zeros<int>(owned_, P);
         x_.base = dev_zeros<int>(owned_, 1);
+        x_.active = dev_zeros<int>(owned_, P);
         x_.status = dev_zeros<int>(owned_, 1);
         NSB_CHECK(cudaMallocHost(&h_status_, sizeof(int)));
         int dev = 0;
@@ -582,6 +608,8 @@ public:
         eco_scan<int><<<1, 1024, 0, st>>>(x_.ecnt, kCells, x_.estart, nullptr, nullptr);
         NSB_CHECK(cudaMemsetAsync(x_.efill, 0, sizeof(int) * kCells, st));
         eco_place_eaters<<<animal_grid(), 256, 0, st>>>(x_);
+        NSB_CHECK(cudaMemsetAsync(x_.active, 0, sizeof(int) * x_.P, st));
+        eco_count_active<<<sms_ * 8, 256, 0, st>>>(x_);
         eco_body<<<(x_.P + 127) / 128, 128, 0, st>>>(x_);
         eco_commit_food<<<kCells / 256, 256, 0, st>>>(x_);
         index(st);

@@ -149,15 +149,18 @@ def test_ecology_life_records_past_capacity_and_no_bite_events(nsb, oracle_built
 
 
 def test_ecology_reports_bad_lists(nsb):
+    """A dead animal whose neuron list is shorter than its count: reclamation
+    walks the list (at most count + 1 entries) and reports it."""
     W = nsb.world
     pools = _population(nsb, 41, founders=8, animal_capacity=16)
     A = pools.animals
+    A["alive"][3] = 0
     A["neuron_count"][3] += 2
     eco = W.make_ecology(pools, seed=1)
     world = W.World(pools)
     world.attach_ecology(eco)
     with pytest.raises(RuntimeError, match="lists disagree"):
-        world.body_step(1)
+        world.reclaim(1)
     world.close()
 
 
