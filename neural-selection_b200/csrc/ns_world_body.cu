@@ -88,6 +88,11 @@ struct Eco {
     unsigned char *flag;                         // per animal: bit, or reclaimed
     int *prey, *rank, *base;                     // base[0]: first index of this call's records
     int *active;                                 // active neurons per animal
+    // reclamation: per reclaimed animal its synapse slots (gathered by owner)
+    // and the life record's sums
+    int *goff, *gcount, *gslot, *dead, *stmp;
+    int *r_as, *r_ps, *r_an, *r_mn, *r_nc;
+    float *r_total;
     int *status;
 };
 
@@ -416,71 +421,216 @@ __global__ void eco_finish_predation(Eco e) {
 }
 
 // ---- genome reclamation (src/main.cu:1302-1338, 436-454) ------------------------
+// Reclamation. Counts and releases do not depend on list order, so they run
+// over the pool slots by owner (the simulator keeps owner equal to list
+// membership). Only the life record's float sum of weight changes follows
+// the synapse list order: each reclaimed animal's list is ranked in shared
+// memory by pointer jumping (Wyllie's list ranking) and the values are added
+// in that order.
+constexpr int kRankCap = 4096;                  // synapses ranked in shared memory; longer lists are walked
+constexpr int kRankSmem = (2 * kRankCap) * 8 + kRankCap * (4 + 16 + 4 + 1) + 64;
+
+__device__ __forceinline__ int dead_count(const Eco &e) { return e.rank[e.P - 1] + e.flag[e.P - 1]; }
+
 __global__ void eco_reclaim_flags(Eco e) {
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
         const ref::Animal &A = e.animals[a];
-        e.flag[a] = A.alive == 0 && (A.neuron_head >= 0 || A.synapse_head >= 0);
+        const bool f = A.alive == 0 && (A.neuron_head >= 0 || A.synapse_head >= 0);
+        e.flag[a] = f;
+        const bool sane = A.synapse_count >= 0 && A.synapse_count <= e.ecap;
+        if (f && !sane) atomicOr(e.status, ES_LIST);
+        e.stmp[a] = f && sane ? A.synapse_count : 0;
     }
 }
-// One pass over each list: the life record's sums and the release of the
-// slots together (release_genome only clears owners and bitmap bits, which
-// the record does not read). Walks stop after count + 1 entries; a list that
-// disagrees with its count is reported.
-__global__ void eco_reclaim(Eco e, int64_t step) {
+__global__ void eco_reclaim_list(Eco e) {
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
         if (!e.flag[a]) continue;
-        ref::Animal body = e.animals[a];
-        const int index = e.base[0] + e.rank[a];
-        const bool record = e.life && index < e.life_capacity;
-        int active_n = 0, modulatory = 0, active_s = 0, plastic = 0, k = 0;
-        float total = 0;
-        for (int s = body.synapse_head; s >= 0 && k <= body.synapse_count; ++k) {
-            if (s >= e.ecap) { atomicOr(e.status, ES_SLOT); break; }
-            const int next = e.snext[s];
-            if (record) {
-                const ref::SynapseGene &g = e.sgene[s];
-                if ((unsigned)g.pre < (unsigned)e.ncap && (unsigned)g.post < (unsigned)e.ncap) {
-                    const ref::NeuronGene &pre = e.ngene[g.pre], &post = e.ngene[g.post];
-                    const bool live = g.active && pre.active && post.active;
-                    active_s += live;
-                    plastic += live && g.plasticity != 0 && !pre.inh_tx && excitatory(pre.type) &&
-                               pre.modulator == 0 && !post.inh_tx && excitatory(post.type);
-                    if (live) total += fabsf(e.sstate[s].w - g.w0);
-                } else {
-                    atomicOr(e.status, ES_SLOT);
+        e.dead[e.rank[a]] = a;
+        e.gcount[a] = e.r_as[a] = e.r_ps[a] = e.r_an[a] = e.r_mn[a] = e.r_nc[a] = 0;
+        e.r_total[a] = 0.0f;
+    }
+}
+// Synapse slots of reclaimed animals: gathered (in no particular order) and released.
+__global__ void eco_gather_synapses(Eco e) {
+    if (dead_count(e) == 0) return;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < e.ecap; s += gridDim.x * blockDim.x) {
+        const int a = e.sowner[s];
+        if (a < 0 || a >= e.P || !e.flag[a]) continue;
+        const int pos = atomicAdd(&e.gcount[a], 1);
+        const int at = e.goff[a] + pos;
+        if (pos < e.stmp[a] && at >= 0 && at < e.ecap) e.gslot[at] = s;
+        e.sowner[s] = -1;
+        atomicAnd(&e.sused[s / 32], ~(1u << (s % 32)));
+    }
+}
+// Neuron slots of reclaimed animals: the record's counts, and released.
+__global__ void eco_release_neurons(Eco e) {
+    if (dead_count(e) == 0) return;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < e.ncap; n += gridDim.x * blockDim.x) {
+        const int a = e.nowner[n];
+        if (a < 0 || a >= e.P || !e.flag[a]) continue;
+        const ref::NeuronGene &g = e.ngene[n];
+        atomicAdd(&e.r_nc[a], 1);
+        if (g.active) atomicAdd(&e.r_an[a], g.active);
+        if (g.active && g.modulator != 0) atomicAdd(&e.r_mn[a], 1);
+        e.nowner[n] = -1;
+        atomicAnd(&e.nused[n / 32], ~(1u << (n % 32)));
+    }
+}
+
+// Contribution of synapse slot s to the life record (src/main.cu:1317-1328).
+__device__ __forceinline__ bool synapse_terms(const Eco &e, int s, bool &plastic, float &change) {
+    const ref::SynapseGene &g = e.sgene[s];
+    plastic = false;
+    change = 0.0f;
+    if ((unsigned)g.pre >= (unsigned)e.ncap || (unsigned)g.post >= (unsigned)e.ncap) {
+        atomicOr(e.status, ES_SLOT);
+        return false;
+    }
+    const ref::NeuronGene &pre = e.ngene[g.pre], &post = e.ngene[g.post];
+    const bool live = g.active && pre.active && post.active;
+    plastic = live && g.plasticity != 0 && !pre.inh_tx && excitatory(pre.type) && pre.modulator == 0 &&
+              !post.inh_tx && excitatory(post.type);
+    if (live) change = fabsf(e.sstate[s].w - g.w0);
+    return live;
+}
+__device__ __forceinline__ uint32_t slot_hash(int slot, int bits) {
+    return ((uint32_t)slot * 0x9E3779B1u) >> (32 - bits);
+}
+
+// One CTA per reclaimed animal (grid-stride over the list of reclaimed animals).
+__global__ void __launch_bounds__(256) eco_rank_synapses(Eco e) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    int *hkey = reinterpret_cast<int *>(sm);                 // 2 kRankCap: slot -> index table
+    int *hval = hkey + 2 * kRankCap;
+    int *slot = hval + 2 * kRankCap;                         // kRankCap each
+    int *succ0 = slot + kRankCap, *succ1 = succ0 + kRankCap;
+    int *dist0 = succ1 + kRankCap, *dist1 = dist0 + kRankCap;
+    float *val = reinterpret_cast<float *>(dist1 + kRankCap);
+    unsigned char *live = reinterpret_cast<unsigned char *>(val + kRankCap);
+    __shared__ int bad, head_index, n_live, n_plastic;
+    const int nd = dead_count(e);
+    for (int d = blockIdx.x; d < nd; d += gridDim.x) {
+        const int a = e.dead[d];
+        const ref::Animal &A = e.animals[a];
+        const int M = e.stmp[a];
+        if (threadIdx.x == 0) {
+            bad = e.gcount[a] != M || e.goff[a] < 0 || e.goff[a] > e.ecap - M;
+            head_index = -1;
+            n_live = n_plastic = 0;
+        }
+        __syncthreads();
+        if (bad || M == 0) {
+            if (threadIdx.x == 0 && bad) atomicOr(e.status, ES_LIST);
+            __syncthreads();
+            continue;
+        }
+        if (M > kRankCap) {                                   // long list: walked by one thread
+            if (threadIdx.x == 0) {
+                int k = 0, nl = 0, np = 0;
+                float total = 0;
+                for (int s = A.synapse_head; s >= 0 && k <= M; s = e.snext[s], ++k) {
+                    if (s >= e.ecap) { atomicOr(e.status, ES_SLOT); break; }
+                    bool pl;
+                    float ch;
+                    if (synapse_terms(e, s, pl, ch)) { ++nl; total += ch; }
+                    np += pl;
                 }
+                if (k != M) atomicOr(e.status, ES_LIST);
+                e.r_as[a] = nl; e.r_ps[a] = np; e.r_total[a] = total;
             }
-            e.sowner[s] = -1;
-            atomicAnd(&e.sused[s / 32], ~(1u << (s % 32)));
-            s = next;
+            __syncthreads();
+            continue;
         }
-        if (k != body.synapse_count) atomicOr(e.status, ES_LIST);
-        k = 0;
-        for (int n = body.neuron_head; n >= 0 && k <= body.neuron_count; ++k) {
-            if (n >= e.ncap) { atomicOr(e.status, ES_SLOT); break; }
-            const int next = e.nnext[n];
-            const ref::NeuronGene &g = e.ngene[n];
-            active_n += g.active;
-            modulatory += g.active && g.modulator != 0;
-            e.nowner[n] = -1;
-            atomicAnd(&e.nused[n / 32], ~(1u << (n % 32)));
-            n = next;
+        int bits = 1;
+        while ((1 << bits) < 2 * M) ++bits;
+        const int T = 1 << bits;
+        for (int i = threadIdx.x; i < T; i += blockDim.x) hkey[i] = -1;
+        __syncthreads();
+        const int *gs = e.gslot + e.goff[a];
+        for (int i = threadIdx.x; i < M; i += blockDim.x) {
+            const int k = gs[i];
+            slot[i] = k;
+            uint32_t h = slot_hash(k, bits);
+            for (int probe = 0; probe < T; ++probe, h = (h + 1) & (T - 1))
+                if (atomicCAS(&hkey[h], -1, k) == -1) { hval[h] = i; break; }
         }
-        if (k != body.neuron_count) atomicOr(e.status, ES_LIST);
-        if (record) {
+        __syncthreads();
+        auto lookup = [&](int k) {
+            uint32_t h = slot_hash(k, bits);
+            for (int probe = 0; probe < T; ++probe, h = (h + 1) & (T - 1)) {
+                const int key = hkey[h];
+                if (key == k) return hval[h];
+                if (key == -1) return -1;
+            }
+            return -1;
+        };
+        for (int i = threadIdx.x; i < M; i += blockDim.x) {
+            const int nx = e.snext[slot[i]];
+            const int j = nx < 0 ? -1 : lookup(nx);
+            if (nx >= 0 && j < 0) bad = 1;                    // successor outside this animal's slots
+            succ0[i] = j;
+            dist0[i] = j >= 0;
+        }
+        if (threadIdx.x == 0) head_index = A.synapse_head < 0 ? -1 : lookup(A.synapse_head);
+        __syncthreads();
+        int *sa = succ0, *sb = succ1, *da = dist0, *db = dist1;
+        for (int span = 1; span < M; span <<= 1) {            // pointer jumping: hops to the list end
+            for (int i = threadIdx.x; i < M; i += blockDim.x) {
+                const int j = sa[i];
+                db[i] = j >= 0 ? da[i] + da[j] : da[i];
+                sb[i] = j >= 0 ? sa[j] : -1;
+            }
+            __syncthreads();
+            int *t = sa; sa = sb; sb = t;
+            t = da; da = db; db = t;
+        }
+        // a single chain of M entries from the head: the head is M - 1 hops from the end
+        if (bad || head_index < 0 || da[head_index] != M - 1) {
+            if (threadIdx.x == 0) atomicOr(e.status, ES_LIST);
+            __syncthreads();
+            continue;
+        }
+        for (int i = threadIdx.x; i < M; i += blockDim.x) {
+            const int p = M - 1 - da[i];                      // list position
+            bool pl;
+            float ch;
+            const bool lv = synapse_terms(e, slot[i], pl, ch);
+            val[p] = ch;
+            live[p] = lv;
+            if (lv) atomicAdd(&n_live, 1);
+            if (pl) atomicAdd(&n_plastic, 1);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float total = 0;
+            for (int p = 0; p < M; ++p)
+                if (live[p]) total += val[p];
+            e.r_as[a] = n_live; e.r_ps[a] = n_plastic; e.r_total[a] = total;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void eco_reclaim_finish(Eco e, int64_t step) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
+        if (!e.flag[a]) continue;
+        ref::Animal &A = e.animals[a];
+        if (e.r_nc[a] != A.neuron_count) atomicOr(e.status, ES_LIST);
+        const int index = e.base[0] + e.rank[a];
+        if (e.life && index < e.life_capacity) {
             ref::LifeRecord &rec = e.life[index];
-            rec.body = body;
+            rec.body = A;
             rec.death_step = step;
-            rec.active_neurons = active_n;
-            rec.active_synapses = active_s;
-            rec.modulatory_neurons = modulatory;
-            rec.plastic_synapses = plastic;
-            rec.mean_abs_weight_change = active_s > 0 ? total / active_s : 0;
+            rec.active_neurons = e.r_an[a];
+            rec.active_synapses = e.r_as[a];
+            rec.modulatory_neurons = e.r_mn[a];
+            rec.plastic_synapses = e.r_ps[a];
+            rec.mean_abs_weight_change = e.r_as[a] > 0 ? e.r_total[a] / e.r_as[a] : 0;
         }
-        ref::Animal &out = e.animals[a];
-        out.neuron_head = out.synapse_head = -1;
-        out.neuron_count = out.synapse_count = 0;
-        for (int p = 0; p < kS + kM; ++p) out.ports[p] = -1;
+        A.neuron_head = A.synapse_head = -1;
+        A.neuron_count = A.synapse_count = 0;
+        for (int p = 0; p < kS + kM; ++p) A.ports[p] = -1;
     }
 }
 
@@ -589,6 +739,18 @@ public:
         x_.rank = dev_zeros<int>(owned_, P);
         x_.base = dev_zeros<int>(owned_, 1);
         x_.active = dev_zeros<int>(owned_, P);
+        x_.goff = dev_zeros<int>(owned_, P);
+        x_.gcount = dev_zeros<int>(owned_, P);
+        x_.gslot = dev_zeros<int>(owned_, (size_t)p.synapse_capacity);
+        x_.dead = dev_zeros<int>(owned_, P);
+        x_.stmp = dev_zeros<int>(owned_, P);
+        x_.r_as = dev_zeros<int>(owned_, P);
+        x_.r_ps = dev_zeros<int>(owned_, P);
+        x_.r_an = dev_zeros<int>(owned_, P);
+        x_.r_mn = dev_zeros<int>(owned_, P);
+        x_.r_nc = dev_zeros<int>(owned_, P);
+        x_.r_total = dev_zeros<float>(owned_, P);
+        NSB_CHECK(cudaFuncSetAttribute(eco_rank_synapses, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem));
         x_.status = dev_zeros<int>(owned_, 1);
         NSB_CHECK(cudaMallocHost(&h_status_, sizeof(int)));
         int dev = 0;
@@ -627,7 +789,12 @@ public:
         cudaStream_t st = 0;
         eco_reclaim_flags<<<animal_grid(), 256, 0, st>>>(x_);
         eco_scan<unsigned char><<<1, 1024, 0, st>>>(x_.flag, x_.P, x_.rank, x_.life_count, x_.base);
-        eco_reclaim<<<animal_grid(), 256, 0, st>>>(x_, step);
+        eco_scan<int><<<1, 1024, 0, st>>>(x_.stmp, x_.P, x_.goff, nullptr, nullptr);
+        eco_reclaim_list<<<animal_grid(), 256, 0, st>>>(x_);
+        eco_gather_synapses<<<sms_ * 8, 256, 0, st>>>(x_);
+        eco_release_neurons<<<sms_ * 8, 256, 0, st>>>(x_);
+        eco_rank_synapses<<<sms_, 256, kRankSmem, st>>>(x_);
+        eco_reclaim_finish<<<animal_grid(), 256, 0, st>>>(x_, step);
         finish(st);
     }
 

@@ -148,6 +148,27 @@ def test_ecology_life_records_past_capacity_and_no_bite_events(nsb, oracle_built
     assert not (ref.neuron_owner >= 0).any()
 
 
+def test_ecology_reclaims_long_and_short_lists(nsb, oracle_built):
+    """Every animal dies in the first body step: lists from a few synapses to
+    more than the 4,096 that are ranked in shared memory (those are walked),
+    all recorded and released."""
+    W, wl = nsb.world, nsb.workloads
+    batch = wl.concat([wl.world_founders(seed=61, founders=20, lo=4, hi=40, epn_lo=1, epn_hi=6),
+                       wl.world_founders(seed=62, founders=3, lo=380, hi=420, epn_lo=12, epn_hi=13)], "reclaim")
+    seeds = np.arange(batch.brains, dtype=np.uint32) + 9
+    N, E = int(batch.neuron_offsets[-1]), int(batch.synapse_offsets[-1])
+    pools = W.place_population(batch, *W.records_from_gpu(batch, seeds), animal_capacity=40,
+                               neuron_capacity=N + 100, synapse_capacity=E + 300, scatter_seed=63)
+    assert pools.animals["synapse_count"].max() > 4096
+    W.place_bodies(pools, 64)
+    pools.animals["health"][pools.animals["alive"] == 1] = 0.0
+    eco = W.make_ecology(pools, seed=3, life_capacity=64)
+    ref, ref_eco = _closed_loop(nsb, pools, eco, 1, seed=3, renewal=0.0, label="reclaim")
+    assert ref_eco.life_count[0] == batch.brains
+    assert ref_eco.life_records["active_synapses"][:batch.brains].max() > 4096
+    assert not (ref.synapse_owner >= 0).any() and not ref_eco.synapse_used.any()
+
+
 def test_ecology_reports_bad_lists(nsb):
     """A dead animal whose neuron list is shorter than its count: reclamation
     walks the list (at most count + 1 entries) and reports it."""
