@@ -236,6 +236,8 @@ typedef struct NsbWorldEcology {
     int initial_count;              /* animals with id below it count as founders */
     int instant_motors;             /* motor force = spikes / 16 instead of the muscle model */
     int life_capacity;
+    int *neuron_clone;              /* [neuron_capacity] reproduction scratch (parent slot -> child slot) */
+    int *births, *next_id;          /* birth counter, next animal id */
 } NsbWorldEcology;
 /* Contended steps (food harvests, spatial index order, bites, record slots)
  * resolve as if the reference kernel's threads ran in ascending animal slot
@@ -249,6 +251,10 @@ void nsb_world_ecology_destroy(void *ecology);
 int nsb_world_body_step(void *ecology, int64_t step);
 /* reclaim_dead_genomes (src/main.cu:2763): life records, genome release. */
 int nsb_world_reclaim(void *ecology, int64_t step);
+/* reproduce with mutate (src/main.cu:2765): parents (alive, energy >= 22)
+ * in ascending slot order, each birth complete before the next, slot claims
+ * as claim_slot run alone. */
+int nsb_world_reproduce(void *ecology);
 /* regrow, spatial index, update_senses (src/main.cu:2767-2770). */
 int nsb_world_regrow_and_sense(void *ecology, int64_t step, unsigned long long seed, float renewal_probability);
 

@@ -76,6 +76,15 @@ ref::NeuronGene profile_for_type(unsigned char type) {
     return g;
 }
 
+}  // namespace
+
+// initial_profile(0..6) (src/physiology.cuh:169-176), for device-side births.
+void nsb::neuron_profiles(ref::NeuronGene *out) {
+    for (int t = 0; t < 7; ++t) out[t] = profile_for_type(static_cast<unsigned char>(t));
+}
+
+namespace {
+
 // A host brain handle: the reference layout first, this library's extras after.
 struct HostBrain : ref::Brain {
     int max_delay = 8;

@@ -175,4 +175,7 @@ static_assert(sizeof(CheckpointSynapse) == 136 && offsetof(CheckpointSynapse, ge
               offsetof(CheckpointSynapse, state) == 56, "CheckpointSynapse layout");
 
 }  // namespace ref
+
+// initial_profile(0..6) of the reference (host; ns_abi.cu).
+void neuron_profiles(ref::NeuronGene *out);
 }  // namespace nsb

@@ -65,11 +65,11 @@ enum : int { ES_LIST = 1, ES_SLOT = 2, ES_KIND = 4 };
 
 struct Eco {
     ref::Animal *animals;
-    const ref::NeuronGene *ngene;
-    const ref::SynapseGene *sgene;
-    const ref::SynapseState *sstate;
+    ref::NeuronGene *ngene;
+    ref::SynapseGene *sgene;
+    ref::SynapseState *sstate;
     int *nowner, *sowner;
-    const int *nnext, *snext;
+    int *nnext, *snext;
     float *senses;
     int *motors;
     int *food, *kind, *cell_head, *cell_next;
@@ -93,6 +93,20 @@ struct Eco {
     int *goff, *gcount, *gslot, *dead, *stmp;
     int *r_as, *r_ps, *r_an, *r_mn, *r_nc;
     float *r_total;
+    // reproduction: the pools a birth writes, the parents' lists in list
+    // order, the child's lists (tail first: the last entry is the head)
+    ref::NeuronState *nstate;
+    int *nport;
+    float *pexc, *pinh;
+    unsigned long long *modtick;
+    unsigned char *hist;
+    int *neuron_clone, *births, *next_id;
+    const ref::NeuronGene *profiles;             // initial_profile(0..6)
+    unsigned char *pflag;
+    int *prank, *parents, *pn_off, *ps_off, *pn_cnt, *ps_cnt, *pn_tmp, *ps_tmp;
+    int *pn_g, *ps_g, *pn_list, *ps_list;
+    int *cn, *cs;
+    uint32_t *nseed, *sseed;
     int *status;
 };
 
@@ -682,6 +696,740 @@ __global__ void __launch_bounds__(128) eco_senses(Eco e) {
     }
 }
 
+// ---- reproduction with mutation (src/main.cu:364-525, 1340-1737) ----------------
+// Parents (alive, energy >= 22 when the step starts) reproduce one after
+// another in ascending slot order, each birth complete (copy, mutation, new
+// states) before the next, every slot claim as claim_slot run alone. A birth
+// is one CTA: the parent's lists come ranked in list order (gathered by owner,
+// ranked in shared memory as for reclamation); claims run 256 at a time in
+// parallel when each lands in its own hint word (claims in distinct words do
+// not see each other, so the result is that of the sequence), otherwise in
+// sequence on one thread; the RNG draws of the birth are taken in order by one
+// thread and the records written in parallel; mutation runs on one thread over
+// array copies of the child's lists, keeping the linked lists in global memory
+// exactly as the reference's list surgery leaves them.
+constexpr int kGrowth = 64;                      // list entries mutation may add (4 x at most 2)
+constexpr int kD = 8;
+
+__device__ __forceinline__ int randint(unsigned long long &s, int size) { return (int)(uniform(s) * size); }
+__device__ __forceinline__ uint32_t state_hash(uint32_t seed) {
+    uint32_t x = seed ? seed : 1u;
+    x ^= x >> 16; x *= 0x7feb352du;
+    x ^= x >> 15; x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+// initialize_neuron / initial_neuron_state (src/main.cu:408-422, src/physiology.cuh:179-202).
+__device__ void birth_state(const Eco &e, int n, uint32_t seed) {
+    const ref::NeuronGene &g = e.ngene[n];
+    ref::NeuronState s;
+    memset(&s, 0, sizeof s);
+    s.v = g.el;
+    const uint32_t x = state_hash(seed);
+    s.rec_rng = x ? x : 1u;
+    if (g.type == 2) {
+        const float init[16] = {-56, 0, .2f, 0, 1, 0, 0, 1, 0, 0, 1, 1, 0, .04f, .01f, -56};
+        for (int k = 0; k < 16; ++k) s.cell[k] = init[k];
+        s.v = s.cell[15] - 9.342518882f;
+    } else if (g.type == 3) {
+        s.cell[0] = -50.0f; s.cell[1] = .05f;
+        for (int k = 0; k < 4; ++k) s.cell[9 + k] = 1.0f;
+        s.v = s.cell[0];
+    } else if (g.type == 6) {
+        s.cell[0] = g.el;
+        s.cell[1] = g.vt;
+    }
+    e.nstate[n] = s;
+}
+__device__ void birth_neuron(const Eco &e, int n, int owner, int port, const ref::NeuronGene &g, int next,
+                             uint32_t seed) {
+    e.nowner[n] = owner;
+    e.nnext[n] = next;
+    e.nport[n] = port;
+    e.ngene[n] = g;
+    birth_state(e, n, seed);
+    for (int b = 0; b < 4; ++b) e.pexc[(size_t)n * 4 + b] = 0;
+    e.pinh[n] = 0;
+    for (int k = 0; k < 6; ++k) e.modtick[(size_t)n * 6 + k] = 0;
+    for (int h = 0; h < 9; ++h) e.hist[(size_t)h * e.ncap + n] = 0;
+}
+// initial_synapse_state (src/physiology.cuh:393-404).
+__device__ void birth_synapse_state(const Eco &e, int s, uint32_t seed) {
+    const ref::SynapseGene &g = e.sgene[s];
+    uint32_t x = state_hash(seed);
+    if (!x) x = 1;
+    const int n = g.sites ? (g.sites > 64 ? 64 : g.sites) : 14;
+    ref::SynapseState z;
+    memset(&z, 0, sizeof z);
+    z.w = g.w0;
+    z.da_age = -1; z.spine = 1; z.st_age = -1;
+    z.pre_age = 1000000; z.post_age = 1000000;
+    z.last = -1000000;
+    z.ready = n == 64 ? ~0ull : ((1ull << n) - 1ull);
+    z.rng = x;
+    z.slow = 1;
+    e.sstate[s] = z;
+}
+__device__ void birth_synapse(const Eco &e, int s, int owner, const ref::SynapseGene &g, int next, uint32_t seed) {
+    e.sowner[s] = owner;
+    e.snext[s] = next;
+    e.sgene[s] = g;
+    birth_synapse_state(e, s, seed);
+}
+// claim_slot run alone (src/main.cu:364-385).
+__device__ int claim_one(uint32_t *used, int capacity, int hint) {
+    const int words = (capacity + 31) / 32;
+    const int start = hint % words;
+    for (int off = 0; off < words; ++off) {
+        const int w = (start + off) % words;
+        const uint32_t occ = used[w];
+        if (~occ) {
+            const int bit = __ffs(~occ) - 1;
+            const int slot = w * 32 + bit;
+            if (slot >= capacity) return -1;
+            used[w] = occ | (1u << bit);
+            return slot;
+        }
+    }
+    return -1;
+}
+__device__ __forceinline__ void release_one(uint32_t *used, int slot) { used[slot >> 5] &= ~(1u << (slot & 31)); }
+
+// Claims for hints hint0 + k, k < K, in order, into out[k]; the number that
+// succeeded (K, or the index of the first failure). All threads of the CTA.
+__device__ int claim_run(uint32_t *used, int capacity, int hint0, int K, int *out) {
+    __shared__ int fail_at;
+    const int words = (capacity + 31) / 32;
+    const int t = threadIdx.x;
+    int done = 0;
+    while (done < K) {
+        const int B = min(min((int)blockDim.x, K - done), words);
+        int mine = -1;
+        bool flag = false;
+        if (t < B) {
+            const int w = (hint0 + done + t) % words;
+            const uint32_t occ = used[w];
+            if (~occ) {
+                const int slot = w * 32 + __ffs(~occ) - 1;
+                if (slot < capacity) mine = slot;
+                else flag = true;
+            } else {
+                flag = true;
+            }
+        }
+        if (__syncthreads_or(flag)) {
+            if (t == 0) {
+                fail_at = -1;
+                for (int i = 0; i < B; ++i) {
+                    const int slot = claim_one(used, capacity, hint0 + done + i);
+                    out[done + i] = slot;
+                    if (slot < 0) { fail_at = done + i; break; }
+                }
+            }
+            __syncthreads();
+            if (fail_at >= 0) return fail_at;
+        } else {
+            if (t < B) {
+                used[mine >> 5] |= 1u << (mine & 31);     // each lane owns its word in this round
+                out[done + t] = mine;
+            }
+            __syncthreads();
+        }
+        done += B;
+    }
+    return K;
+}
+
+__global__ void eco_parent_flags(Eco e) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
+        const ref::Animal &A = e.animals[a];
+        const bool f = A.alive == 1 && A.energy >= 22;
+        const bool sane = A.neuron_count >= 0 && A.neuron_count <= e.ncap && A.synapse_count >= 0 &&
+                          A.synapse_count <= e.ecap;
+        if (f && !sane) atomicOr(e.status, ES_LIST);
+        e.pflag[a] = f && sane;
+        e.pn_tmp[a] = f && sane ? A.neuron_count : 0;
+        e.ps_tmp[a] = f && sane ? A.synapse_count : 0;
+    }
+}
+__device__ __forceinline__ int parent_count(const Eco &e) { return e.prank[e.P - 1] + e.pflag[e.P - 1]; }
+__global__ void eco_parent_list(Eco e) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
+        if (!e.pflag[a]) continue;
+        e.parents[e.prank[a]] = a;
+        e.pn_cnt[a] = e.ps_cnt[a] = 0;
+    }
+}
+__global__ void eco_gather_parents(Eco e) {
+    if (parent_count(e) == 0) return;
+    const int stride = gridDim.x * blockDim.x;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < e.ncap; n += stride) {
+        const int a = e.nowner[n];
+        if (a < 0 || a >= e.P || !e.pflag[a]) continue;
+        const int pos = atomicAdd(&e.pn_cnt[a], 1), at = e.pn_off[a] + pos;
+        if (pos < e.pn_tmp[a] && at >= 0 && at < e.ncap) e.pn_g[at] = n;
+    }
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < e.ecap; s += stride) {
+        const int a = e.sowner[s];
+        if (a < 0 || a >= e.P || !e.pflag[a]) continue;
+        const int pos = atomicAdd(&e.ps_cnt[a], 1), at = e.ps_off[a] + pos;
+        if (pos < e.ps_tmp[a] && at >= 0 && at < e.ecap) e.ps_g[at] = s;
+    }
+}
+// Ranks one list of M slots gathered at g (in any order) whose head is `head`
+// and successors next[]: out[k] = the k-th slot in list order. All threads;
+// returns whether the slots form exactly that list. Lists above kRankCap are
+// walked by one thread.
+__device__ bool rank_list(const int *g, int M, int head, const int *next, int cap, int *out, unsigned char *sm) {
+    __shared__ int r_bad, r_head;
+    int *hkey = reinterpret_cast<int *>(sm);
+    int *hval = hkey + 2 * kRankCap;
+    int *slot = hval + 2 * kRankCap;
+    int *succ0 = slot + kRankCap, *succ1 = succ0 + kRankCap;
+    int *dist0 = succ1 + kRankCap, *dist1 = dist0 + kRankCap;
+    __syncthreads();
+    if (threadIdx.x == 0) { r_bad = 0; r_head = -1; }
+    if (M > kRankCap) {
+        if (threadIdx.x == 0) {
+            int k = 0;
+            for (int s = head; s >= 0 && k <= M; s = next[s], ++k) {
+                if (s >= cap) { r_bad = 1; break; }
+                if (k < M) out[k] = s;
+            }
+            if (k != M) r_bad = 1;
+        }
+        __syncthreads();
+        return !r_bad;
+    }
+    if (M == 0) {
+        __syncthreads();
+        return head < 0;
+    }
+    int bits = 1;
+    while ((1 << bits) < 2 * M) ++bits;
+    const int T = 1 << bits;
+    for (int i = threadIdx.x; i < T; i += blockDim.x) hkey[i] = -1;
+    __syncthreads();
+    for (int i = threadIdx.x; i < M; i += blockDim.x) {
+        const int k = g[i];
+        slot[i] = k;
+        uint32_t h = slot_hash(k, bits);
+        for (int probe = 0; probe < T; ++probe, h = (h + 1) & (T - 1))
+            if (atomicCAS(&hkey[h], -1, k) == -1) { hval[h] = i; break; }
+    }
+    __syncthreads();
+    auto lookup = [&](int k) {
+        uint32_t h = slot_hash(k, bits);
+        for (int probe = 0; probe < T; ++probe, h = (h + 1) & (T - 1)) {
+            const int key = hkey[h];
+            if (key == k) return hval[h];
+            if (key == -1) return -1;
+        }
+        return -1;
+    };
+    for (int i = threadIdx.x; i < M; i += blockDim.x) {
+        const int nx = next[slot[i]];
+        const int j = nx < 0 ? -1 : lookup(nx);
+        if (nx >= 0 && j < 0) r_bad = 1;
+        succ0[i] = j;
+        dist0[i] = j >= 0;
+    }
+    if (threadIdx.x == 0) r_head = head < 0 ? -1 : lookup(head);
+    __syncthreads();
+    int *sa = succ0, *sb = succ1, *da = dist0, *db = dist1;
+    for (int span = 1; span < M; span <<= 1) {
+        for (int i = threadIdx.x; i < M; i += blockDim.x) {
+            const int j = sa[i];
+            db[i] = j >= 0 ? da[i] + da[j] : da[i];
+            sb[i] = j >= 0 ? sa[j] : -1;
+        }
+        __syncthreads();
+        int *tmp = sa; sa = sb; sb = tmp;
+        tmp = da; da = db; db = tmp;
+    }
+    const bool ok = !r_bad && r_head >= 0 && da[r_head] == M - 1;
+    if (ok)
+        for (int i = threadIdx.x; i < M; i += blockDim.x) out[M - 1 - da[i]] = slot[i];
+    __syncthreads();
+    return ok;
+}
+__global__ void __launch_bounds__(256) eco_rank_parents(Eco e) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int np = parent_count(e);
+    for (int q = blockIdx.x; q < np; q += gridDim.x) {
+        const int a = e.parents[q];
+        const ref::Animal &A = e.animals[a];
+        const int N = e.pn_tmp[a], M = e.ps_tmp[a];
+        bool ok = e.pn_cnt[a] == N && e.ps_cnt[a] == M && e.pn_off[a] >= 0 && e.pn_off[a] <= e.ncap - N &&
+                  e.ps_off[a] >= 0 && e.ps_off[a] <= e.ecap - M;
+        ok = rank_list(e.pn_g + e.pn_off[a], ok ? N : 0, ok ? A.neuron_head : -1, e.nnext, e.ncap,
+                       e.pn_list + e.pn_off[a], sm) && ok;
+        ok = rank_list(e.ps_g + e.ps_off[a], ok ? M : 0, ok ? A.synapse_head : -1, e.snext, e.ecap,
+                       e.ps_list + e.ps_off[a], sm) && ok;
+        __syncthreads();
+        if (!ok && threadIdx.x == 0) {
+            atomicOr(e.status, ES_LIST);
+            e.pn_cnt[a] = -1;                                 // not reproduced
+        }
+        __syncthreads();
+    }
+}
+
+// ---- mutation on one thread (src/main.cu:1357-1660) --------------------------------
+// The child's lists as arrays, tail first (list position i is entry len-1-i).
+struct ChildLists {
+    int *n, *s;
+    int nn, ns;
+};
+__device__ int list_at(const int *l, int len, int ordinal) { return ordinal < len ? l[len - 1 - ordinal] : -1; }
+__device__ void list_remove(int *l, int &len, int idx) {
+    for (int i = idx; i + 1 < len; ++i) l[i] = l[i + 1];
+    --len;
+}
+__device__ int random_hidden(const Eco &e, const ChildLists &c, const ref::Animal &b, unsigned long long &rng) {
+    const int hidden = b.neuron_count - (kS + kM);
+    if (hidden <= 0) return -1;
+    int ordinal = randint(rng, hidden);
+    for (int i = c.nn - 1; i >= 0; --i) {
+        const int n = c.n[i];
+        if (e.nport[n] < 0 && ordinal-- == 0) return n;
+    }
+    return -1;
+}
+__device__ void remove_synapse_at(const Eco &e, ChildLists &c, ref::Animal &b, int target) {
+    for (int i = c.ns - 1; i >= 0; --i) {
+        if (c.s[i] != target) continue;
+        const int next = e.snext[target];
+        if (i == c.ns - 1) b.synapse_head = next;
+        else e.snext[c.s[i + 1]] = next;
+        --b.synapse_count;
+        e.sowner[target] = -1;
+        release_one(e.sused, target);
+        list_remove(c.s, c.ns, i);
+        return;
+    }
+}
+__device__ void remove_hidden(const Eco &e, ChildLists &c, ref::Animal &b, int target, int *scratch) {
+    if (target < 0 || e.nport[target] >= 0) return;
+    int k = 0;                                                // synapses touching it, in list order
+    for (int i = c.ns - 1; i >= 0; --i) {
+        const ref::SynapseGene &g = e.sgene[c.s[i]];
+        if (g.pre == target || g.post == target) scratch[k++] = c.s[i];
+    }
+    for (int j = 0; j < k; ++j) remove_synapse_at(e, c, b, scratch[j]);
+    for (int i = c.nn - 1; i >= 0; --i) {
+        if (c.n[i] != target) continue;
+        const int next = e.nnext[target];
+        if (i == c.nn - 1) b.neuron_head = next;
+        else e.nnext[c.n[i + 1]] = next;
+        --b.neuron_count;
+        e.nowner[target] = -1;
+        release_one(e.nused, target);
+        list_remove(c.n, c.nn, i);
+        return;
+    }
+}
+__device__ void random_synapse(const Eco &e, const ChildLists &c, ref::SynapseGene &g, int child,
+                               unsigned long long &rng) {
+    const ref::Animal &body = e.animals[child];
+    int active_sources = 0;
+    float target_weight = 0;
+    for (int i = c.nn - 1; i >= 0; --i) {
+        const int n = c.n[i];
+        const ref::NeuronGene &gene = e.ngene[n];
+        if (!gene.active) continue;
+        ++active_sources;
+        const int port = e.nport[n];
+        if (port < 0 || port >= kS) target_weight += gene.affinity;
+    }
+    g.pre = body.ports[0];
+    int source_choice = randint(rng, active_sources);
+    for (int i = c.nn - 1; i >= 0; --i)
+        if (e.ngene[c.n[i]].active && source_choice-- == 0) { g.pre = c.n[i]; break; }
+    g.post = body.ports[kS + randint(rng, kM)];
+    float target_choice = uniform(rng) * target_weight;
+    for (int i = c.nn - 1; i >= 0; --i) {
+        const int n = c.n[i];
+        const int port = e.nport[n];
+        if (!e.ngene[n].active || (port >= 0 && port < kS)) continue;
+        target_choice -= e.ngene[n].affinity;
+        if (target_choice <= 0) { g.post = n; break; }
+    }
+    g.delay = (unsigned char)(1 + randint(rng, kD));
+    g.branch = (unsigned char)randint(rng, 4);
+    g.w0 = 0.5f + uniform(rng) * 3.5f;
+    g.U = 0.55f;
+    g.trec = 450.0f;
+    g.tfac = 0;
+    g.sites = 14;
+    const bool pre_ok = (unsigned)g.pre < (unsigned)e.ncap, post_ok = (unsigned)g.post < (unsigned)e.ncap;
+    if (!pre_ok || !post_ok) atomicOr(e.status, ES_SLOT);
+    if (pre_ok && e.ngene[g.pre].type == 5) {
+        g.w0 = 29.0f / (60.0f * 0.75f);
+        g.U = 0.75f;
+        g.trec = 50.0f;
+        g.sites = 50;
+        g.slow_rec = 7500.0f;
+        g.slow_depl = 0.023f;
+    }
+    if (pre_ok && post_ok && e.ngene[g.pre].type == 0 && e.ngene[g.post].type == 1) {
+        g.U = 0.1f;
+        g.trec = 30.0f;
+        g.tfac = 1700.0f;
+    }
+    const float draw = uniform(rng);
+    g.plasticity = draw < 0.05f ? 5 : (draw < 0.10f ? 4 : (draw < 0.20f ? 3 : 2));
+    g.receptors = g.plasticity == 3 ? (1 | 2) : (g.plasticity >= 4 ? 4 : 0);
+    g.active = 1;
+}
+__device__ void prepend_neuron(const Eco &e, ChildLists &c, ref::Animal &b, int n, int child, const ref::NeuronGene &g,
+                               unsigned long long &rng) {
+    birth_neuron(e, n, child, -1, g, b.neuron_head, (uint32_t)random64(rng));
+    b.neuron_head = n;
+    ++b.neuron_count;
+    c.n[c.nn++] = n;
+}
+__device__ void prepend_synapse(const Eco &e, ChildLists &c, ref::Animal &b, int s, int child,
+                                const ref::SynapseGene &g, unsigned long long &rng) {
+    birth_synapse(e, s, child, g, b.synapse_head, (uint32_t)random64(rng));
+    b.synapse_head = s;
+    ++b.synapse_count;
+    c.s[c.ns++] = s;
+}
+__device__ void mutate(const Eco &e, ChildLists &c, int child, unsigned long long &rng, int *scratch) {
+    ref::NeuronGene *NG = e.ngene;
+    ref::SynapseGene *SG = e.sgene;
+    const int mutations = 1 + randint(rng, 4);
+    for (int m = 0; m < mutations; ++m) {
+        const int choice = randint(rng, 12);
+        ref::Animal body = e.animals[child];
+        const int n = random_hidden(e, c, body, rng);
+        const int syn = body.synapse_count ? list_at(c.s, c.ns, randint(rng, body.synapse_count)) : -1;
+        if (choice == 0) {
+            const float action = uniform(rng);
+            if (action < 1.0f / 3.0f) {
+                const int added = claim_one(e.nused, e.ncap, child * 131 + body.neuron_count);
+                const int incoming = added >= 0 ? claim_one(e.sused, e.ecap, child * 257 + body.synapse_count) : -1;
+                const int outgoing = incoming >= 0 ? claim_one(e.sused, e.ecap, child * 257 + body.synapse_count + 1) : -1;
+                if (added >= 0 && incoming >= 0 && outgoing >= 0 && syn >= 0) {
+                    int templ = syn;
+                    for (int attempt = 0; attempt < 8; ++attempt) {
+                        const int cand = list_at(c.s, c.ns, randint(rng, body.synapse_count));
+                        const ref::SynapseGene &cg = SG[cand];
+                        if ((unsigned)cg.pre >= (unsigned)e.ncap || (unsigned)cg.post >= (unsigned)e.ncap) {
+                            atomicOr(e.status, ES_SLOT);
+                            continue;
+                        }
+                        if (cg.active && NG[cg.pre].active && NG[cg.post].active) { templ = cand; break; }
+                    }
+                    const unsigned char type = (unsigned char)randint(rng, 7);
+                    ref::NeuronGene g = e.profiles[type];
+                    g.modulator = uniform(rng) < 0.12f ? (unsigned char)(1 + randint(rng, 3)) : 0;
+                    prepend_neuron(e, c, body, added, child, g, rng);
+                    ref::SynapseGene first = SG[templ], second = first;
+                    first.post = added;
+                    second.pre = added;
+                    first.active = second.active = 1;
+                    prepend_synapse(e, c, body, incoming, child, first, rng);
+                    prepend_synapse(e, c, body, outgoing, child, second, rng);
+                    e.animals[child] = body;
+                } else {
+                    if (outgoing >= 0) release_one(e.sused, outgoing);
+                    if (incoming >= 0) release_one(e.sused, incoming);
+                    if (added >= 0) release_one(e.nused, added);
+                }
+            } else if (action < 2.0f / 3.0f) {
+                if (n >= 0) { remove_hidden(e, c, body, n, scratch); e.animals[child] = body; }
+            } else if (n >= 0) {
+                NG[n].active ^= 1;
+            }
+        } else if (choice == 1 && n >= 0) {
+            const unsigned char active = NG[n].active;
+            const unsigned char type = (unsigned char)randint(rng, 7);
+            const unsigned char modulator = NG[n].modulator, inh = NG[n].inh_tx;
+            const float affinity = NG[n].affinity;
+            NG[n] = e.profiles[type];
+            NG[n].active = active;
+            NG[n].modulator = modulator;
+            NG[n].inh_tx = inh;
+            NG[n].affinity = affinity;
+        } else if (choice == 2) {
+            const int target = uniform(rng) < 0.2f ? body.ports[kS + randint(rng, kM)] : n;
+            if (target < 0) continue;
+            ref::NeuronGene &g = NG[target];
+            if (g.type == 2) {
+                float *scales = &g.lp.calcium;
+                const int channel = randint(rng, 4);
+                scales[channel] = clampf(scales[channel] * (0.9f + uniform(rng) * 0.2f), 0.2f, 3.0f);
+            } else if (g.type == 3) {
+                const int channel = randint(rng, 9);
+                float &conductance = channel == 8 ? g.prinz_leak : g.prinz.g[channel];
+                conductance = clampf((conductance + (channel >= 7 ? 2.0f : 0.0f)) * (0.9f + uniform(rng) * 0.2f), 0.0f,
+                                     channel >= 7 ? 200.0f : 500000.0f);
+            } else if (g.type == 5) {
+                const int parameter = randint(rng, 4);
+                if (parameter == 0) g.rec_base = clampf(g.rec_base + (uniform(rng) - 0.5f) * 2, 0, 30);
+                if (parameter == 1) g.rec_gain = clampf(g.rec_gain + (uniform(rng) - 0.5f) * 10, 0, 300);
+                if (parameter == 2) g.rec_event = clampf(g.rec_event * (0.9f + uniform(rng) * 0.2f), 0.5f, 6);
+                if (parameter == 3) g.rec_decay = clampf(g.rec_decay * (0.9f + uniform(rng) * 0.2f), 1, 20);
+            } else {
+                g.vt = clampf(g.vt + (uniform(rng) - 0.5f) * 2, -60, -35);
+            }
+        } else if (choice == 3) {
+            const float action = uniform(rng);
+            if (action < 1.0f / 3.0f) {
+                const int added = claim_one(e.sused, e.ecap, child * 257 + body.synapse_count);
+                if (added >= 0) {
+                    ref::SynapseGene g;
+                    memset(&g, 0, sizeof g);
+                    random_synapse(e, c, g, child, rng);
+                    prepend_synapse(e, c, body, added, child, g, rng);
+                    e.animals[child] = body;
+                }
+            } else if (action < 2.0f / 3.0f) {
+                if (syn >= 0) { remove_synapse_at(e, c, body, syn); e.animals[child] = body; }
+            } else if (syn >= 0) {
+                SG[syn].active ^= 1;
+            }
+        } else if (choice == 4 && syn >= 0) {
+            random_synapse(e, c, SG[syn], child, rng);
+        } else if (choice == 5 && syn >= 0) {
+            ref::SynapseGene &g = SG[syn];
+            g.w0 = clampf(g.w0 + (uniform(rng) - 0.5f) * 0.5f, 0.1f, 8);
+            g.sites = (unsigned char)clampf(g.sites + (uniform(rng) < 0.5f ? -1 : 1), 1, 64);
+        } else if (choice == 6 && syn >= 0) {
+            ref::SynapseGene &g = SG[syn];
+            g.plasticity = (unsigned char)randint(rng, 6);
+            g.receptors = g.plasticity == 3 ? (unsigned char)(1 + randint(rng, 3)) : (g.plasticity >= 4 ? 4 : 0);
+            g.U = clampf(g.U + (uniform(rng) - 0.5f) * 0.1f, 0.02f, 0.8f);
+            g.trec = clampf(g.trec + (uniform(rng) - 0.5f) * 50, 20, 1000);
+            if (uniform(rng) < 0.15f) {
+                g.slow_rec = g.slow_rec == 0 ? 7500.0f
+                           : (uniform(rng) < 0.1f ? 0.0f : clampf(g.slow_rec + (uniform(rng) - 0.5f) * 500, 1000.0f, 20000.0f));
+                g.slow_depl = g.slow_rec == 0 ? 0.0f : clampf(g.slow_depl + (uniform(rng) - 0.5f) * 0.01f, 0.0f, 0.1f);
+            }
+        } else if (choice == 7 && syn >= 0) {
+            ref::SynapseGene &g = SG[syn];
+            g.delay = (unsigned char)(1 + randint(rng, kD));
+            g.tfac = g.tfac == 0 ? 500.0f + uniform(rng) * 3500.0f
+                   : (uniform(rng) < 0.1f ? 0.0f : clampf(g.tfac + (uniform(rng) - 0.5f) * 200, 100, 4000));
+            if (n >= 0) NG[n].b = clampf(NG[n].b + (uniform(rng) - 0.5f) * 5, 0, 150);
+        } else if (choice == 8 && n >= 0) {
+            ref::NeuronGene &g = NG[n];
+            if (g.type == 0) {
+                g.adp_b = clampf(g.adp_b + (uniform(rng) - 0.5f) * 20, 0, 200);
+                g.adp_tau = clampf(g.adp_tau + (uniform(rng) - 0.5f) * 10, 10, 150);
+            }
+        } else if (choice == 9 && n >= 0) {
+            if (NG[n].type != 5 && uniform(rng) < 0.5f) NG[n].modulator = (unsigned char)randint(rng, 4);
+            else NG[n].inh_tx ^= 1;
+        } else if (choice == 10) {
+            const float action = uniform(rng);
+            int afferent = -1;
+            for (int attempt = 0; attempt < 12; ++attempt) {
+                const int h = random_hidden(e, c, body, rng);
+                if (h >= 0 && NG[h].sensory_channel >= 0) { afferent = h; break; }
+            }
+            if (action < 0.5f) {
+                const int added = claim_one(e.nused, e.ncap, child * 131 + body.neuron_count);
+                const int outgoing = added >= 0 ? claim_one(e.sused, e.ecap, child * 257 + body.synapse_count) : -1;
+                if (added >= 0 && outgoing >= 0) {
+                    int target = body.ports[kS + randint(rng, kM)];
+                    for (int attempt = 0; attempt < 8; ++attempt) {
+                        const int cand = list_at(c.n, c.nn, randint(rng, body.neuron_count));
+                        if (cand >= 0 && (e.nport[cand] < 0 || e.nport[cand] >= kS)) { target = cand; break; }
+                    }
+                    const int source = afferent >= 0 && uniform(rng) < 0.5f ? afferent : body.ports[randint(rng, kS)];
+                    if ((unsigned)source >= (unsigned)e.ncap) { atomicOr(e.status, ES_SLOT); continue; }
+                    ref::NeuronGene g = NG[source];
+                    g.modulator = 0;
+                    g.active = 1;
+                    prepend_neuron(e, c, body, added, child, g, rng);
+                    ref::SynapseGene edge;
+                    memset(&edge, 0, sizeof edge);
+                    edge.pre = added;
+                    edge.post = target;
+                    edge.delay = (unsigned char)(1 + randint(rng, kD));
+                    edge.branch = (unsigned char)randint(rng, 4);
+                    edge.w0 = g.type == 5 ? 29.0f / (60.0f * 0.75f) : 1.0f;
+                    edge.U = g.type == 5 ? 0.75f : 0.55f;
+                    edge.trec = g.type == 5 ? 50.0f : 450.0f;
+                    edge.sites = g.type == 5 ? 50 : 14;
+                    edge.slow_rec = g.type == 5 ? 7500.0f : 0.0f;
+                    edge.slow_depl = g.type == 5 ? 0.023f : 0.0f;
+                    edge.active = 1;
+                    prepend_synapse(e, c, body, outgoing, child, edge, rng);
+                    e.animals[child] = body;
+                } else {
+                    if (outgoing >= 0) release_one(e.sused, outgoing);
+                    if (added >= 0) release_one(e.nused, added);
+                }
+            } else if (action < 0.75f && afferent >= 0) {
+                remove_hidden(e, c, body, afferent, scratch);
+                e.animals[child] = body;
+            } else if (afferent >= 0) {
+                ref::NeuronGene &g = NG[afferent];
+                const int channel = randint(rng, kS);
+                const unsigned char active = g.active, inh = g.inh_tx;
+                const float affinity = g.affinity;
+                if (g.type == 5 && channel >= 6) g = e.profiles[0];
+                else if (g.type != 5 && channel < 6) g = e.profiles[5];
+                g.sensory_channel = (signed char)channel;
+                g.active = active;
+                g.inh_tx = inh;
+                g.affinity = affinity;
+            }
+        } else if (choice == 11) {
+            const int target = uniform(rng) < 0.3f ? body.ports[kS + randint(rng, kM)] : n;
+            if (target >= 0)
+                NG[target].affinity = clampf(NG[target].affinity * (uniform(rng) < 0.5f ? 0.5f : 2.0f), 0.125f, 256.0f);
+        }
+    }
+}
+
+// One CTA: the births of this step in ascending parent slot order (src/main.cu:1662-1737).
+__global__ void __launch_bounds__(256) eco_births(Eco e) {
+    __shared__ int s_child, s_n, s_s, s_start;
+    __shared__ unsigned long long s_rng;
+    __shared__ ref::Animal s_nb, s_parent;
+    const int t = threadIdx.x;
+    const int np = parent_count(e);
+    for (int q = 0; q < np; ++q) {
+        const int a = e.parents[q];
+        __syncthreads();
+        if (e.pn_cnt[a] < 0) continue;                         // its lists failed the ranking
+        if (t == 0) {
+            s_parent = e.animals[a];
+            unsigned long long r = s_parent.rng;
+            s_start = randint(r, e.P);
+            s_rng = r;
+            s_child = INT_MAX;
+        }
+        __syncthreads();
+        for (int base = 0; base < e.P; base += blockDim.x) {   // the first free animal slot from start
+            const int j = base + t;
+            if (j < e.P && e.animals[(s_start + j) % e.P].alive == 0) atomicMin(&s_child, j);
+            __syncthreads();
+            if (s_child != INT_MAX) break;
+        }
+        if (s_child == INT_MAX) {
+            if (t == 0) e.animals[a].rng = s_rng;
+            continue;
+        }
+        const int child = (s_start + s_child) % e.P;
+        if (t == 0) {
+            e.animals[child].alive = -1;
+            ref::Animal nb;
+            memset(&nb, 0, sizeof nb);
+            nb.neuron_head = nb.synapse_head = -1;
+            for (int p = 0; p < kS + kM; ++p) nb.ports[p] = -1;
+            unsigned long long r = s_rng;
+            nb.x = clampf(s_parent.x + (uniform(r) - 0.5f) * 2, 0, (float)kW - 0.001f);
+            nb.y = clampf(s_parent.y + (uniform(r) - 0.5f) * 2, 0, (float)kH - 0.001f);
+            nb.heading = uniform(r) * 2 * 3.14159265358979323846f;
+            nb.energy = 8;
+            nb.health = 10;
+            nb.generation = s_parent.generation + 1;
+            s_rng = r;
+            s_nb = nb;
+        }
+        __syncthreads();
+        const int N = e.pn_tmp[a], M = e.ps_tmp[a];
+        const int *pn = e.pn_list + e.pn_off[a], *ps = e.ps_list + e.ps_off[a];
+        // neurons: claims, draws in order, copies
+        const int n_ok = claim_run(e.nused, e.ncap, child * 131, N, e.cn);
+        if (t == 0) {
+            unsigned long long r = s_rng;
+            for (int k = 0; k < n_ok; ++k) e.nseed[k] = (uint32_t)random64(r);
+            s_rng = r;
+        }
+        __syncthreads();
+        for (int k = t; k < n_ok; k += blockDim.x) {
+            const int old = pn[k], n = e.cn[k];
+            birth_neuron(e, n, child, e.nport[old], e.ngene[old], k ? e.cn[k - 1] : -1, e.nseed[k]);
+            e.neuron_clone[old] = n;
+        }
+        __syncthreads();
+        int s_ok = 0;
+        if (n_ok == N) {
+            s_ok = claim_run(e.sused, e.ecap, child * 257, M, e.cs);
+            if (t == 0) {
+                unsigned long long r = s_rng;
+                for (int k = 0; k < s_ok; ++k) e.sseed[k] = (uint32_t)random64(r);
+                s_rng = r;
+            }
+            __syncthreads();
+            for (int k = t; k < s_ok; k += blockDim.x) {
+                ref::SynapseGene g = e.sgene[ps[k]];
+                if ((unsigned)g.pre >= (unsigned)e.ncap || (unsigned)g.post >= (unsigned)e.ncap) {
+                    atomicOr(e.status, ES_SLOT);
+                } else {
+                    g.pre = e.neuron_clone[g.pre];
+                    g.post = e.neuron_clone[g.post];
+                }
+                birth_synapse(e, e.cs[k], child, g, k ? e.cs[k - 1] : -1, e.sseed[k]);
+            }
+            __syncthreads();
+        }
+        if (n_ok < N || s_ok < M) {                            // pools full: the birth is undone
+            for (int k = t; k < s_ok; k += blockDim.x) {
+                e.sowner[e.cs[k]] = -1;
+                atomicAnd(&e.sused[e.cs[k] >> 5], ~(1u << (e.cs[k] & 31)));
+            }
+            for (int k = t; k < n_ok; k += blockDim.x) {
+                e.nowner[e.cn[k]] = -1;
+                atomicAnd(&e.nused[e.cn[k] >> 5], ~(1u << (e.cn[k] & 31)));
+            }
+            __syncthreads();
+            if (t == 0) {
+                e.animals[child].alive = 0;
+                e.animals[a].rng = s_rng;
+            }
+            continue;
+        }
+        if (t == 0) {
+            ref::Animal nb = s_nb;
+            for (int k = 0; k < n_ok; ++k) {
+                const int port = e.nport[e.cn[k]];
+                if (port >= 0 && port < kS + kM) nb.ports[port] = e.cn[k];
+            }
+            nb.neuron_head = n_ok ? e.cn[n_ok - 1] : -1;
+            nb.neuron_count = n_ok;
+            nb.synapse_head = s_ok ? e.cs[s_ok - 1] : -1;
+            nb.synapse_count = s_ok;
+            nb.id = atomicAdd(e.next_id, 1);
+            nb.parent_id = s_parent.id;
+            nb.alive = -1;
+            e.animals[child] = nb;
+            ChildLists c{e.cn, e.cs, n_ok, s_ok};
+            unsigned long long r = s_rng;
+            mutate(e, c, child, r, reinterpret_cast<int *>(e.sseed));   // sseed as scratch (reseeded below)
+            s_n = c.nn;
+            s_s = c.ns;
+            for (int i = c.nn - 1; i >= 0; --i) e.nseed[c.nn - 1 - i] = (uint32_t)random64(r);
+            for (int i = c.ns - 1; i >= 0; --i) e.sseed[c.ns - 1 - i] = (uint32_t)random64(r);
+            s_rng = r;
+        }
+        __syncthreads();
+        for (int k = t; k < s_n; k += blockDim.x) birth_state(e, e.cn[s_n - 1 - k], e.nseed[k]);
+        for (int k = t; k < s_s; k += blockDim.x) birth_synapse_state(e, e.cs[s_s - 1 - k], e.sseed[k]);
+        for (int k = t; k < kS; k += blockDim.x) e.senses[(size_t)child * kS + k] = 0;
+        for (int k = t; k < kM; k += blockDim.x) e.motors[(size_t)child * kM + k] = 0;
+        __syncthreads();
+        if (t == 0) {
+            e.animals[child].rng = s_rng;
+            ref::Animal p = s_parent;
+            p.energy -= 10;
+            ++p.behavior.offspring;
+            p.rng = s_rng;
+            e.animals[a] = p;
+            __threadfence();
+            e.animals[child].alive = 1;
+            atomicAdd(e.births, 1);
+        }
+    }
+}
+
 template <class T> T *dev_zeros(std::vector<void *> &owned, size_t n) {
     void *p = nullptr;
     NSB_CHECK(cudaMalloc(&p, sizeof(T) * (n ? n : 1)));
@@ -699,16 +1447,27 @@ public:
             throw std::runtime_error("Invalid world pools");
         if (!x.food || !x.kind || !x.cell_head || !x.cell_next || !x.bite_intent || !x.neuron_used ||
             !x.synapse_used || !x.founder_motor_steps || !x.founder_observed_steps || !x.deaths ||
-            !x.predation_deaths || !x.bites || !x.life_count || !x.bite_event_count || x.life_capacity < 0)
+            !x.predation_deaths || !x.bites || !x.life_count || !x.bite_event_count || x.life_capacity < 0 ||
+            !x.neuron_clone || !x.births || !x.next_id || !p.neuron_state || !p.neuron_port || !p.pending_exc ||
+            !p.pending_inh || !p.mod_event_tick || !p.spike_history)
             throw std::runtime_error("Invalid world ecology");
         x_.animals = static_cast<ref::Animal *>(const_cast<void *>(p.animals));
-        x_.ngene = static_cast<const ref::NeuronGene *>(p.neurons);
-        x_.sgene = static_cast<const ref::SynapseGene *>(p.synapses);
-        x_.sstate = static_cast<const ref::SynapseState *>(p.synapse_state);
+        x_.ngene = static_cast<ref::NeuronGene *>(const_cast<void *>(p.neurons));
+        x_.sgene = static_cast<ref::SynapseGene *>(const_cast<void *>(p.synapses));
+        x_.sstate = static_cast<ref::SynapseState *>(p.synapse_state);
         x_.nowner = const_cast<int *>(p.neuron_owner);
         x_.sowner = const_cast<int *>(p.synapse_owner);
-        x_.nnext = p.neuron_next;
-        x_.snext = p.synapse_next;
+        x_.nnext = const_cast<int *>(p.neuron_next);
+        x_.snext = const_cast<int *>(p.synapse_next);
+        x_.nstate = static_cast<ref::NeuronState *>(p.neuron_state);
+        x_.nport = const_cast<int *>(p.neuron_port);
+        x_.pexc = p.pending_exc;
+        x_.pinh = p.pending_inh;
+        x_.modtick = p.mod_event_tick;
+        x_.hist = p.spike_history;
+        x_.neuron_clone = x.neuron_clone;
+        x_.births = x.births;
+        x_.next_id = x.next_id;
         x_.senses = const_cast<float *>(p.senses);
         x_.motors = p.motors;
         x_.food = x.food; x_.kind = x.kind; x_.cell_head = x.cell_head; x_.cell_next = x.cell_next;
@@ -751,6 +1510,30 @@ public:
         x_.r_nc = dev_zeros<int>(owned_, P);
         x_.r_total = dev_zeros<float>(owned_, P);
         NSB_CHECK(cudaFuncSetAttribute(eco_rank_synapses, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem));
+        NSB_CHECK(cudaFuncSetAttribute(eco_rank_parents, cudaFuncAttributeMaxDynamicSharedMemorySize, kRankSmem));
+        const size_t NC = (size_t)p.neuron_capacity, EC = (size_t)p.synapse_capacity;
+        x_.pflag = dev_zeros<unsigned char>(owned_, P);
+        x_.prank = dev_zeros<int>(owned_, P);
+        x_.parents = dev_zeros<int>(owned_, P);
+        x_.pn_off = dev_zeros<int>(owned_, P);
+        x_.ps_off = dev_zeros<int>(owned_, P);
+        x_.pn_cnt = dev_zeros<int>(owned_, P);
+        x_.ps_cnt = dev_zeros<int>(owned_, P);
+        x_.pn_tmp = dev_zeros<int>(owned_, P);
+        x_.ps_tmp = dev_zeros<int>(owned_, P);
+        x_.pn_g = dev_zeros<int>(owned_, NC);
+        x_.ps_g = dev_zeros<int>(owned_, EC);
+        x_.pn_list = dev_zeros<int>(owned_, NC);
+        x_.ps_list = dev_zeros<int>(owned_, EC);
+        x_.cn = dev_zeros<int>(owned_, NC + kGrowth);
+        x_.cs = dev_zeros<int>(owned_, EC + kGrowth);
+        x_.nseed = dev_zeros<uint32_t>(owned_, NC + kGrowth);
+        x_.sseed = dev_zeros<uint32_t>(owned_, EC + kGrowth);
+        ref::NeuronGene prof[7];
+        neuron_profiles(prof);
+        auto *dprof = dev_zeros<ref::NeuronGene>(owned_, 7);
+        NSB_CHECK(cudaMemcpy(dprof, prof, sizeof prof, cudaMemcpyHostToDevice));
+        x_.profiles = dprof;
         x_.status = dev_zeros<int>(owned_, 1);
         NSB_CHECK(cudaMallocHost(&h_status_, sizeof(int)));
         int dev = 0;
@@ -795,6 +1578,20 @@ public:
         eco_release_neurons<<<sms_ * 8, 256, 0, st>>>(x_);
         eco_rank_synapses<<<sms_, 256, kRankSmem, st>>>(x_);
         eco_reclaim_finish<<<animal_grid(), 256, 0, st>>>(x_, step);
+        finish(st);
+    }
+
+    // reproduce (src/main.cu:2765): parents in ascending slot order.
+    void reproduce() {
+        cudaStream_t st = 0;
+        eco_parent_flags<<<animal_grid(), 256, 0, st>>>(x_);
+        eco_scan<unsigned char><<<1, 1024, 0, st>>>(x_.pflag, x_.P, x_.prank, nullptr, nullptr);
+        eco_scan<int><<<1, 1024, 0, st>>>(x_.pn_tmp, x_.P, x_.pn_off, nullptr, nullptr);
+        eco_scan<int><<<1, 1024, 0, st>>>(x_.ps_tmp, x_.P, x_.ps_off, nullptr, nullptr);
+        eco_parent_list<<<animal_grid(), 256, 0, st>>>(x_);
+        eco_gather_parents<<<sms_ * 8, 256, 0, st>>>(x_);
+        eco_rank_parents<<<sms_, 256, kRankSmem, st>>>(x_);
+        eco_births<<<1, 256, 0, st>>>(x_);
         finish(st);
     }
 
@@ -872,6 +1669,10 @@ int nsb_world_body_step(void *ecology, int64_t step) {
 
 int nsb_world_reclaim(void *ecology, int64_t step) {
     return nsb::guarded(ecology, [&](nsb::EcologyStage &s) { s.reclaim(step); });
+}
+
+int nsb_world_reproduce(void *ecology) {
+    return nsb::guarded(ecology, [&](nsb::EcologyStage &s) { s.reproduce(); });
 }
 
 int nsb_world_regrow_and_sense(void *ecology, int64_t step, unsigned long long seed, float renewal_probability) {

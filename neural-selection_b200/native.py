@@ -72,6 +72,7 @@ SIGNATURES = {
     "nsb_world_ecology_destroy": (None, [_vp]),
     "nsb_world_body_step": (ct.c_int, [_vp, ct.c_int64]),
     "nsb_world_reclaim": (ct.c_int, [_vp, ct.c_int64]),
+    "nsb_world_reproduce": (ct.c_int, [_vp]),
     "nsb_world_regrow_and_sense": (ct.c_int, [_vp, ct.c_int64, ct.c_ulonglong, ct.c_float]),
     "nsb_world_layout": (ct.c_int, [ct.POINTER(ct.c_uint64)]),
     "nsb_serve_create": (_vp, [ct.c_longlong, ct.c_double, ct.c_double, ct.c_int, ct.c_int, ct.c_int, ct.c_float,

@@ -158,12 +158,13 @@ class NsbWorldEcology(ct.Structure):
         "food", "kind", "cell_head", "cell_next", "bite_intent", "neuron_used", "synapse_used",
         "founder_motor_steps", "founder_observed_steps", "deaths", "predation_deaths", "bites", "life_records",
         "life_count", "bite_events", "bite_event_count")] + [(n, ct.c_int) for n in (
-        "initial_count", "instant_motors", "life_capacity")]
+        "initial_count", "instant_motors", "life_capacity")] + [(n, ct.c_void_p) for n in (
+        "neuron_clone", "births", "next_id")]
 
 
 ECO_ARRAYS = ("food", "kind", "cell_head", "cell_next", "bite_intent", "neuron_used", "synapse_used",
               "founder_motor_steps", "founder_observed_steps", "deaths", "predation_deaths", "bites", "life_records",
-              "life_count", "bite_events", "bite_event_count")
+              "life_count", "bite_events", "bite_event_count", "neuron_clone", "births", "next_id")
 
 
 @dataclass
@@ -187,6 +188,9 @@ class Ecology:
     life_count: np.ndarray
     bite_events: np.ndarray | None   # BITE_EVENT, 2 * animal_capacity
     bite_event_count: np.ndarray
+    neuron_clone: np.ndarray         # (neuron_capacity,) i32, reproduction scratch
+    births: np.ndarray
+    next_id: np.ndarray
     initial_count: int = 0
     instant_motors: int = 0
 
@@ -252,7 +256,8 @@ def make_ecology(pools, seed, initial_count=None, life_capacity=None, bite_event
                    founder_observed_steps=one(), deaths=one(), predation_deaths=one(), bites=one(),
                    life_records=np.zeros(life_capacity if life_capacity is not None else 16 * P, LIFE_RECORD),
                    life_count=one(), bite_events=np.zeros(2 * P, BITE_EVENT) if bite_events else None,
-                   bite_event_count=one(),
+                   bite_event_count=one(), neuron_clone=np.zeros(NC, np.int32), births=one(),
+                   next_id=np.array([int(pools.animals["id"].max()) + 1], np.int32),
                    initial_count=P if initial_count is None else int(initial_count), instant_motors=instant_motors)
 
 
@@ -493,6 +498,9 @@ class World:
 
     def reclaim(self, step):
         self._eco_call(self.lib.nsb_world_reclaim(self.eco, int(step)))
+
+    def reproduce(self):
+        self._eco_call(self.lib.nsb_world_reproduce(self.eco))
 
     def regrow_and_sense(self, step, seed, renewal_probability):
         self._eco_call(self.lib.nsb_world_regrow_and_sense(self.eco, int(step), int(seed),

@@ -1652,3 +1652,450 @@ void or_world_regrow_and_sense(const or_world_pools *w, const or_world_eco *x, i
             out[W_CONTACT + kind] = x->food[contact] > 0 && x->kind[contact] == kind ? 1.0f : 0.0f;
     }
 }
+
+/* ---- reproduction with mutation (src/main.cu:364-454, 464-525, 1340-1737) --
+ * Parents (alive, energy >= 22 when the step starts) reproduce one after
+ * another in ascending slot order; every slot claim runs alone. */
+#define W_D 8
+static int or_randint(unsigned long long *s, int size) { return (int)(or_uniform(s) * size); }
+
+static int or_claim(uint32_t *used, int capacity, int hint) {   /* claim_slot, 364-385 */
+    int words = (capacity + 31) / 32;
+    int start = hint % words;
+    for (int off = 0; off < words; ++off) {
+        int w = (start + off) % words;
+        uint32_t occ = used[w];
+        if (~occ) {
+            int bit = __builtin_ctz(~occ);
+            int slot = w * 32 + bit;
+            if (slot < capacity) { used[w] = occ | (1u << bit); return slot; }
+            return -1;
+        }
+    }
+    return -1;
+}
+static void or_release(uint32_t *used, int slot) { used[slot / 32] &= ~(1u << (slot % 32)); }
+
+typedef struct { const or_world_pools *w; const or_world_eco *x; } or_rw;
+
+static void or_init_neuron(or_rw r, int n, int owner, int port, const ngene *g, int next, uint32_t seed) {
+    const or_world_pools *w = r.w;
+    ((int *)w->neuron_owner)[n] = owner;
+    ((int *)w->neuron_next)[n] = next;
+    ((int *)w->neuron_port)[n] = port;
+    ((ngene *)w->neurons)[n] = *g;
+    ((nstate *)w->neuron_state)[n] = neuron_initial(g, seed);
+    for (int b = 0; b < 4; ++b) w->pending_exc[(size_t)n * 4 + b] = 0;
+    w->pending_inh[n] = 0;
+    for (int k = 0; k < 6; ++k) w->mod_event_tick[(size_t)n * 6 + k] = 0;
+    for (int h = 0; h < W_HIST; ++h) w->spike_history[(size_t)h * w->neuron_capacity + n] = 0;
+}
+static void or_init_synapse(or_rw r, int e, int owner, const sgene *g, int next, unsigned long long *rng) {
+    const or_world_pools *w = r.w;
+    ((int *)w->synapse_owner)[e] = owner;
+    ((int *)w->synapse_next)[e] = next;
+    ((sgene *)w->synapses)[e] = *g;
+    ((sstate *)w->synapse_state)[e] = synapse_initial(g, (uint32_t)or_random64(rng));
+}
+static void or_release_genome(or_rw r, or_animal *body) {            /* 436-454 */
+    const or_world_pools *w = r.w;
+    for (int e = body->synapse_head; e >= 0;) {
+        int next = w->synapse_next[e];
+        ((int *)w->synapse_owner)[e] = -1;
+        or_release(r.x->synapse_used, e);
+        e = next;
+    }
+    for (int n = body->neuron_head; n >= 0;) {
+        int next = w->neuron_next[n];
+        ((int *)w->neuron_owner)[n] = -1;
+        or_release(r.x->neuron_used, n);
+        n = next;
+    }
+    body->neuron_head = body->synapse_head = -1;
+    body->neuron_count = body->synapse_count = 0;
+    for (int p = 0; p < W_S + W_M; ++p) body->ports[p] = -1;
+}
+static int or_neuron_at(or_rw r, const or_animal *b, int ordinal) {
+    int n = b->neuron_head;
+    for (int j = 0; j < ordinal && n >= 0; ++j) n = r.w->neuron_next[n];
+    return n;
+}
+static int or_synapse_at(or_rw r, const or_animal *b, int ordinal) {
+    int e = b->synapse_head;
+    for (int j = 0; j < ordinal && e >= 0; ++j) e = r.w->synapse_next[e];
+    return e;
+}
+static int or_random_hidden(or_rw r, const or_animal *b, unsigned long long *rng) {
+    int hidden = b->neuron_count - (W_S + W_M);
+    if (hidden <= 0) return -1;
+    int ordinal = or_randint(rng, hidden);
+    for (int n = b->neuron_head; n >= 0; n = r.w->neuron_next[n])
+        if (r.w->neuron_port[n] < 0 && ordinal-- == 0) return n;
+    return -1;
+}
+static void or_random_synapse(or_rw r, sgene *g, int animal, unsigned long long *rng) {   /* 464-525 */
+    const or_world_pools *w = r.w;
+    const ngene *NG = (const ngene *)w->neurons;
+    or_animal body = ((or_animal *)w->animals)[animal];
+    int active_sources = 0;
+    float target_weight = 0;
+    for (int n = body.neuron_head; n >= 0; n = w->neuron_next[n]) {
+        if (!NG[n].active) continue;
+        ++active_sources;
+        int port = w->neuron_port[n];
+        if (port < 0 || port >= W_S) target_weight += NG[n].affinity;
+    }
+    g->pre = body.ports[0];
+    int source_choice = or_randint(rng, active_sources);
+    for (int n = body.neuron_head; n >= 0; n = w->neuron_next[n])
+        if (NG[n].active && source_choice-- == 0) { g->pre = n; break; }
+    g->post = body.ports[W_S + or_randint(rng, W_M)];
+    float target_choice = or_uniform(rng) * target_weight;
+    for (int n = body.neuron_head; n >= 0; n = w->neuron_next[n]) {
+        int port = w->neuron_port[n];
+        if (!NG[n].active || (port >= 0 && port < W_S)) continue;
+        target_choice -= NG[n].affinity;
+        if (target_choice <= 0) { g->post = n; break; }
+    }
+    g->delay = (unsigned char)(1 + or_randint(rng, W_D));
+    g->branch = (unsigned char)or_randint(rng, 4);
+    g->w0 = 0.5f + or_uniform(rng) * 3.5f;
+    g->U = 0.55f;
+    g->trec = 450.0f;
+    g->tfac = 0;
+    g->sites = 14;
+    if (NG[g->pre].type == 5) {
+        g->w0 = 29.0f / (60.0f * 0.75f);
+        g->U = 0.75f;
+        g->trec = 50.0f;
+        g->sites = 50;
+        g->slow_rec = 7500.0f;
+        g->slow_depl = 0.023f;
+    }
+    if (NG[g->pre].type == 0 && NG[g->post].type == 1) {
+        g->U = 0.1f;
+        g->trec = 30.0f;
+        g->tfac = 1700.0f;
+    }
+    float draw = or_uniform(rng);
+    g->plast = draw < 0.05f ? 5 : (draw < 0.10f ? 4 : (draw < 0.20f ? 3 : 2));
+    g->receptors = g->plast == 3 ? (MOD_NE | MOD_5HT) : (g->plast >= 4 ? 4 : 0);
+    g->active = 1;
+}
+static void or_remove_synapse(or_rw r, or_animal *body, int target) {   /* 1357-1372 */
+    int *next = (int *)r.w->synapse_next;
+    int previous = -1;
+    for (int e = body->synapse_head; e >= 0; e = next[e]) {
+        if (e != target) { previous = e; continue; }
+        int nx = next[e];
+        if (previous < 0) body->synapse_head = nx; else next[previous] = nx;
+        --body->synapse_count;
+        ((int *)r.w->synapse_owner)[e] = -1;
+        or_release(r.x->synapse_used, e);
+        return;
+    }
+}
+static void or_remove_hidden(or_rw r, or_animal *body, int target) {    /* 1374-1395 */
+    const sgene *SG = (const sgene *)r.w->synapses;
+    int *nnext = (int *)r.w->neuron_next;
+    if (target < 0 || r.w->neuron_port[target] >= 0) return;
+    for (int e = body->synapse_head; e >= 0;) {
+        int nx = r.w->synapse_next[e];
+        if (SG[e].pre == target || SG[e].post == target) or_remove_synapse(r, body, e);
+        e = nx;
+    }
+    int previous = -1;
+    for (int n = body->neuron_head; n >= 0; n = nnext[n]) {
+        if (n != target) { previous = n; continue; }
+        int nx = nnext[n];
+        if (previous < 0) body->neuron_head = nx; else nnext[previous] = nx;
+        --body->neuron_count;
+        ((int *)r.w->neuron_owner)[n] = -1;
+        or_release(r.x->neuron_used, n);
+        return;
+    }
+}
+static int or_random_afferent(or_rw r, const or_animal *b, unsigned long long *rng) {
+    const ngene *NG = (const ngene *)r.w->neurons;
+    for (int attempt = 0; attempt < 12; ++attempt) {
+        int n = or_random_hidden(r, b, rng);
+        if (n >= 0 && NG[n].sens >= 0) return n;
+    }
+    return -1;
+}
+
+static void or_mutate(or_rw r, int child, unsigned long long *rng) {    /* 1401-1660 */
+    const or_world_pools *w = r.w;
+    or_animal *A = (or_animal *)w->animals;
+    ngene *NG = (ngene *)w->neurons;
+    sgene *SG = (sgene *)w->synapses;
+    const int NC = w->neuron_capacity, EC = w->synapse_capacity;
+    int mutations = 1 + or_randint(rng, 4);
+    for (int m = 0; m < mutations; ++m) {
+        int choice = or_randint(rng, 12);
+        or_animal body = A[child];
+        int n = or_random_hidden(r, &body, rng);
+        int e = body.synapse_count ? or_synapse_at(r, &body, or_randint(rng, body.synapse_count)) : -1;
+        if (choice == 0) {
+            float action = or_uniform(rng);
+            if (action < 1.0f / 3.0f) {
+                int added = or_claim(r.x->neuron_used, NC, child * 131 + body.neuron_count);
+                int incoming = added >= 0 ? or_claim(r.x->synapse_used, EC, child * 257 + body.synapse_count) : -1;
+                int outgoing = incoming >= 0 ? or_claim(r.x->synapse_used, EC, child * 257 + body.synapse_count + 1) : -1;
+                if (added >= 0 && incoming >= 0 && outgoing >= 0 && e >= 0) {
+                    int template_e = e;
+                    for (int attempt = 0; attempt < 8; ++attempt) {
+                        int cand = or_synapse_at(r, &body, or_randint(rng, body.synapse_count));
+                        sgene cg = SG[cand];
+                        if (cg.active && NG[cg.pre].active && NG[cg.post].active) { template_e = cand; break; }
+                    }
+                    unsigned char type = (unsigned char)or_randint(rng, 7);
+                    ngene g = profile_for_type(type);
+                    g.modulator = or_uniform(rng) < 0.12f ? (unsigned char)(1 + or_randint(rng, 3)) : 0;
+                    or_init_neuron(r, added, child, -1, &g, body.neuron_head, (uint32_t)or_random64(rng));
+                    body.neuron_head = added;
+                    ++body.neuron_count;
+                    sgene first = SG[template_e], second = first;
+                    first.post = added;
+                    second.pre = added;
+                    first.active = second.active = 1;
+                    or_init_synapse(r, incoming, child, &first, body.synapse_head, rng);
+                    body.synapse_head = incoming;
+                    or_init_synapse(r, outgoing, child, &second, body.synapse_head, rng);
+                    body.synapse_head = outgoing;
+                    body.synapse_count += 2;
+                    A[child] = body;
+                } else {
+                    if (outgoing >= 0) or_release(r.x->synapse_used, outgoing);
+                    if (incoming >= 0) or_release(r.x->synapse_used, incoming);
+                    if (added >= 0) or_release(r.x->neuron_used, added);
+                }
+            } else if (action < 2.0f / 3.0f) {
+                if (n >= 0) { or_remove_hidden(r, &body, n); A[child] = body; }
+            } else if (n >= 0) NG[n].active ^= 1;
+        } else if (choice == 1 && n >= 0) {
+            unsigned char active = NG[n].active;
+            unsigned char type = (unsigned char)or_randint(rng, 7);
+            unsigned char modulator = NG[n].modulator, inh = NG[n].inh_tx;
+            float affinity = NG[n].affinity;
+            NG[n] = profile_for_type(type);
+            NG[n].active = active;
+            NG[n].modulator = modulator;
+            NG[n].inh_tx = inh;
+            NG[n].affinity = affinity;
+        } else if (choice == 2) {
+            int target = or_uniform(rng) < 0.2f ? body.ports[W_S + or_randint(rng, W_M)] : n;
+            if (target < 0) continue;
+            ngene *g = &NG[target];
+            if (g->type == 2) {
+                int channel = or_randint(rng, 4);
+                g->lp_scale[channel] = or_clamp(g->lp_scale[channel] * (0.9f + or_uniform(rng) * 0.2f), 0.2f, 3.0f);
+            } else if (g->type == 3) {
+                int channel = or_randint(rng, 9);
+                float *c = channel == 8 ? &g->prinz_leak : &g->prinz_g[channel];
+                *c = or_clamp((*c + (channel >= 7 ? 2.0f : 0.0f)) * (0.9f + or_uniform(rng) * 0.2f), 0.0f,
+                              channel >= 7 ? 200.0f : 500000.0f);
+            } else if (g->type == 5) {
+                int parameter = or_randint(rng, 4);
+                if (parameter == 0) g->rec_base = or_clamp(g->rec_base + (or_uniform(rng) - 0.5f) * 2, 0, 30);
+                if (parameter == 1) g->rec_gain = or_clamp(g->rec_gain + (or_uniform(rng) - 0.5f) * 10, 0, 300);
+                if (parameter == 2) g->rec_event = or_clamp(g->rec_event * (0.9f + or_uniform(rng) * 0.2f), 0.5f, 6);
+                if (parameter == 3) g->rec_decay = or_clamp(g->rec_decay * (0.9f + or_uniform(rng) * 0.2f), 1, 20);
+            } else {
+                g->vt = or_clamp(g->vt + (or_uniform(rng) - 0.5f) * 2, -60, -35);
+            }
+        } else if (choice == 3) {
+            float action = or_uniform(rng);
+            if (action < 1.0f / 3.0f) {
+                int added = or_claim(r.x->synapse_used, EC, child * 257 + body.synapse_count);
+                if (added >= 0) {
+                    sgene g; memset(&g, 0, sizeof g);
+                    or_random_synapse(r, &g, child, rng);
+                    or_init_synapse(r, added, child, &g, body.synapse_head, rng);
+                    body.synapse_head = added;
+                    ++body.synapse_count;
+                    A[child] = body;
+                }
+            } else if (action < 2.0f / 3.0f) {
+                if (e >= 0) { or_remove_synapse(r, &body, e); A[child] = body; }
+            } else if (e >= 0) SG[e].active ^= 1;
+        } else if (choice == 4 && e >= 0) {
+            or_random_synapse(r, &SG[e], child, rng);
+        } else if (choice == 5 && e >= 0) {
+            sgene *g = &SG[e];
+            g->w0 = or_clamp(g->w0 + (or_uniform(rng) - 0.5f) * 0.5f, 0.1f, 8);
+            g->sites = (unsigned char)or_clamp(g->sites + (or_uniform(rng) < 0.5f ? -1 : 1), 1, 64);
+        } else if (choice == 6 && e >= 0) {
+            sgene *g = &SG[e];
+            g->plast = (unsigned char)or_randint(rng, 6);
+            g->receptors = g->plast == 3 ? (unsigned char)(1 + or_randint(rng, 3)) : (g->plast >= 4 ? 4 : 0);
+            g->U = or_clamp(g->U + (or_uniform(rng) - 0.5f) * 0.1f, 0.02f, 0.8f);
+            g->trec = or_clamp(g->trec + (or_uniform(rng) - 0.5f) * 50, 20, 1000);
+            if (or_uniform(rng) < 0.15f) {
+                g->slow_rec = g->slow_rec == 0 ? 7500.0f :
+                    (or_uniform(rng) < 0.1f ? 0.0f : or_clamp(g->slow_rec + (or_uniform(rng) - 0.5f) * 500, 1000.0f, 20000.0f));
+                g->slow_depl = g->slow_rec == 0 ? 0.0f :
+                    or_clamp(g->slow_depl + (or_uniform(rng) - 0.5f) * 0.01f, 0.0f, 0.1f);
+            }
+        } else if (choice == 7 && e >= 0) {
+            sgene *g = &SG[e];
+            g->delay = (unsigned char)(1 + or_randint(rng, W_D));
+            g->tfac = g->tfac == 0 ? 500.0f + or_uniform(rng) * 3500.0f
+                    : (or_uniform(rng) < 0.1f ? 0.0f : or_clamp(g->tfac + (or_uniform(rng) - 0.5f) * 200, 100, 4000));
+            if (n >= 0) NG[n].b = or_clamp(NG[n].b + (or_uniform(rng) - 0.5f) * 5, 0, 150);
+        } else if (choice == 8 && n >= 0) {
+            ngene *g = &NG[n];
+            if (g->type == 0) {
+                g->adp_b = or_clamp(g->adp_b + (or_uniform(rng) - 0.5f) * 20, 0, 200);
+                g->adp_tau = or_clamp(g->adp_tau + (or_uniform(rng) - 0.5f) * 10, 10, 150);
+            }
+        } else if (choice == 9 && n >= 0) {
+            if (NG[n].type != 5 && or_uniform(rng) < 0.5f) NG[n].modulator = (unsigned char)or_randint(rng, 4);
+            else NG[n].inh_tx ^= 1;
+        } else if (choice == 10) {
+            float action = or_uniform(rng);
+            int afferent = or_random_afferent(r, &body, rng);
+            if (action < 0.5f) {
+                int added = or_claim(r.x->neuron_used, NC, child * 131 + body.neuron_count);
+                int outgoing = added >= 0 ? or_claim(r.x->synapse_used, EC, child * 257 + body.synapse_count) : -1;
+                if (added >= 0 && outgoing >= 0) {
+                    int target = body.ports[W_S + or_randint(rng, W_M)];
+                    for (int attempt = 0; attempt < 8; ++attempt) {
+                        int cand = or_neuron_at(r, &body, or_randint(rng, body.neuron_count));
+                        if (w->neuron_port[cand] < 0 || w->neuron_port[cand] >= W_S) { target = cand; break; }
+                    }
+                    int source = afferent >= 0 && or_uniform(rng) < 0.5f ? afferent : body.ports[or_randint(rng, W_S)];
+                    ngene g = NG[source];
+                    g.modulator = 0;
+                    g.active = 1;
+                    or_init_neuron(r, added, child, -1, &g, body.neuron_head, (uint32_t)or_random64(rng));
+                    body.neuron_head = added;
+                    ++body.neuron_count;
+                    sgene edge; memset(&edge, 0, sizeof edge);
+                    edge.pre = added;
+                    edge.post = target;
+                    edge.delay = (unsigned char)(1 + or_randint(rng, W_D));
+                    edge.branch = (unsigned char)or_randint(rng, 4);
+                    edge.w0 = g.type == 5 ? 29.0f / (60.0f * 0.75f) : 1.0f;
+                    edge.U = g.type == 5 ? 0.75f : 0.55f;
+                    edge.trec = g.type == 5 ? 50.0f : 450.0f;
+                    edge.sites = g.type == 5 ? 50 : 14;
+                    edge.slow_rec = g.type == 5 ? 7500.0f : 0.0f;
+                    edge.slow_depl = g.type == 5 ? 0.023f : 0.0f;
+                    edge.active = 1;
+                    or_init_synapse(r, outgoing, child, &edge, body.synapse_head, rng);
+                    body.synapse_head = outgoing;
+                    ++body.synapse_count;
+                    A[child] = body;
+                } else {
+                    if (outgoing >= 0) or_release(r.x->synapse_used, outgoing);
+                    if (added >= 0) or_release(r.x->neuron_used, added);
+                }
+            } else if (action < 0.75f && afferent >= 0) {
+                or_remove_hidden(r, &body, afferent);
+                A[child] = body;
+            } else if (afferent >= 0) {
+                ngene *g = &NG[afferent];
+                int channel = or_randint(rng, W_S);
+                unsigned char active = g->active, inh = g->inh_tx;
+                float affinity = g->affinity;
+                if (g->type == 5 && channel >= 6) *g = profile_for_type(0);
+                else if (g->type != 5 && channel < 6) *g = profile_for_type(5);
+                g->sens = (signed char)channel;
+                g->active = active;
+                g->inh_tx = inh;
+                g->affinity = affinity;
+            }
+        } else if (choice == 11) {
+            int target = or_uniform(rng) < 0.3f ? body.ports[W_S + or_randint(rng, W_M)] : n;
+            if (target >= 0)
+                NG[target].affinity = or_clamp(NG[target].affinity * (or_uniform(rng) < 0.5f ? 0.5f : 2.0f),
+                                               0.125f, 256.0f);
+        }
+    }
+}
+
+static void or_reproduce_one(or_rw r, int a) {                           /* 1662-1737 */
+    const or_world_pools *w = r.w;
+    const or_world_eco *x = r.x;
+    or_animal *A = (or_animal *)w->animals;
+    const int P = w->animal_capacity;
+    or_animal parent = A[a];
+    unsigned long long rng = parent.rng;
+    int start = or_randint(&rng, P);
+    int child = -1;
+    for (int j = 0; j < P; ++j) {
+        int cand = (start + j) % P;
+        if (A[cand].alive == 0) { A[cand].alive = -1; child = cand; break; }
+    }
+    if (child < 0) { A[a].rng = rng; return; }
+    or_animal nb; memset(&nb, 0, sizeof nb);
+    nb.neuron_head = nb.synapse_head = -1;
+    for (int p = 0; p < W_S + W_M; ++p) nb.ports[p] = -1;
+    nb.x = or_clamp(parent.x + (or_uniform(&rng) - 0.5f) * 2, 0, W_W - 0.001f);
+    nb.y = or_clamp(parent.y + (or_uniform(&rng) - 0.5f) * 2, 0, W_H - 0.001f);
+    nb.heading = or_uniform(&rng) * 2 * 3.14159265358979323846f;
+    nb.energy = 8;
+    nb.health = 10;
+    nb.generation = parent.generation + 1;
+    int complete = 1;
+    for (int old = parent.neuron_head; old >= 0; old = w->neuron_next[old]) {
+        int n = or_claim(x->neuron_used, w->neuron_capacity, child * 131 + nb.neuron_count);
+        if (n < 0) { complete = 0; break; }
+        int port = w->neuron_port[old];
+        ngene g = ((const ngene *)w->neurons)[old];
+        or_init_neuron(r, n, child, port, &g, nb.neuron_head, (uint32_t)or_random64(&rng));
+        x->neuron_clone[old] = n;
+        nb.neuron_head = n;
+        ++nb.neuron_count;
+        if (port >= 0) nb.ports[port] = n;
+    }
+    if (complete)
+        for (int old = parent.synapse_head; old >= 0; old = w->synapse_next[old]) {
+            int e = or_claim(x->synapse_used, w->synapse_capacity, child * 257 + nb.synapse_count);
+            if (e < 0) { complete = 0; break; }
+            sgene g = ((const sgene *)w->synapses)[old];
+            g.pre = x->neuron_clone[g.pre];
+            g.post = x->neuron_clone[g.post];
+            or_init_synapse(r, e, child, &g, nb.synapse_head, &rng);
+            nb.synapse_head = e;
+            ++nb.synapse_count;
+        }
+    if (!complete) {
+        or_release_genome(r, &nb);
+        A[child].alive = 0;
+        A[a].rng = rng;
+        return;
+    }
+    nb.id = (*x->next_id)++;
+    nb.parent_id = parent.id;
+    nb.alive = -1;
+    A[child] = nb;
+    or_mutate(r, child, &rng);
+    nb = A[child];
+    for (int n = nb.neuron_head; n >= 0; n = w->neuron_next[n])
+        ((nstate *)w->neuron_state)[n] = neuron_initial(&((const ngene *)w->neurons)[n], (uint32_t)or_random64(&rng));
+    for (int e = nb.synapse_head; e >= 0; e = w->synapse_next[e])
+        ((sstate *)w->synapse_state)[e] = synapse_initial(&((const sgene *)w->synapses)[e], (uint32_t)or_random64(&rng));
+    for (int s = 0; s < W_S; ++s) ((float *)w->senses)[(size_t)child * W_S + s] = 0;
+    for (int m = 0; m < W_M; ++m) w->motors[(size_t)child * W_M + m] = 0;
+    nb.rng = rng;
+    A[child] = nb;
+    parent.energy -= 10;
+    ++parent.behavior.offspring;
+    parent.rng = rng;
+    A[a] = parent;
+    A[child].alive = 1;
+    ++*x->births;
+}
+
+void or_world_reproduce(const or_world_pools *w, const or_world_eco *x) {
+    const or_animal *A = (const or_animal *)w->animals;
+    const int P = w->animal_capacity;
+    unsigned char *parent = (unsigned char *)calloc((size_t)P, 1);
+    for (int a = 0; a < P; ++a) parent[a] = A[a].alive == 1 && A[a].energy >= 22;
+    or_rw r = {w, x};
+    for (int a = 0; a < P; ++a)
+        if (parent[a]) or_reproduce_one(r, a);
+    free(parent);
+}

@@ -138,11 +138,15 @@ typedef struct or_world_eco {
     void *bite_events;
     int *bite_event_count;
     int initial_count, instant_motors, life_capacity;
+    int *neuron_clone;           /* [neuron_capacity] scratch of reproduce */
+    int *births, *next_id;
 } or_world_eco;
 /* body_step, spatial index, bite_animals, finish_predation. */
 void or_world_body_step(const or_world_pools *w, const or_world_eco *x, int64_t step);
 /* reclaim_dead_genomes with release_genome. */
 void or_world_reclaim(const or_world_pools *w, const or_world_eco *x, int64_t step);
+/* reproduce with mutate, parents in ascending slot order. */
+void or_world_reproduce(const or_world_pools *w, const or_world_eco *x);
 /* regrow, spatial index, update_senses. */
 void or_world_regrow_and_sense(const or_world_pools *w, const or_world_eco *x, int64_t step,
                                unsigned long long seed, float renewal);

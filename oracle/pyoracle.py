@@ -67,6 +67,7 @@ def oracle_lib(libm=False):
         lib.or_world_homeostasis.argtypes = [ct.c_void_p]
         lib.or_world_body_step.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int64]
         lib.or_world_reclaim.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int64]
+        lib.or_world_reproduce.argtypes = [ct.c_void_p, ct.c_void_p]
         lib.or_world_regrow_and_sense.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int64, ct.c_ulonglong,
                                                   ct.c_float]
         for fn in ("or_cr_sinf", "or_cr_cosf"):
@@ -174,6 +175,11 @@ def world_body_step(pools, eco, step):
 def world_reclaim(pools, eco, step):
     """The oracle's reclaim_dead_genomes (or_world_reclaim), in place."""
     oracle_lib().or_world_reclaim(ct.byref(pools.struct()), ct.byref(eco.struct()), int(step))
+
+
+def world_reproduce(pools, eco):
+    """The oracle's reproduce with mutate (or_world_reproduce), in place."""
+    oracle_lib().or_world_reproduce(ct.byref(pools.struct()), ct.byref(eco.struct()))
 
 
 def world_regrow_and_sense(pools, eco, step, seed, renewal_probability):

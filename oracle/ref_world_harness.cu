@@ -470,6 +470,7 @@ struct EcoArg {
     void *bite_events;
     int *bite_event_count;
     int initial_count, instant_motors, life_capacity;
+    int *neuron_clone, *births, *next_id;
 };
 
 __global__ void ref_relabel(Device d, int keep, int from, int to) {
@@ -539,6 +540,9 @@ void *ref_world_eco_create(const void *pools, const void *ecology) {
     d.life_count = x.life_count;
     d.bite_events = static_cast<BiteEvent *>(x.bite_events);
     d.bite_event_count = x.bite_event_count;
+    d.neuron_clone = x.neuron_clone;
+    d.births = x.births;
+    d.next_id = x.next_id;
     if (cudaMalloc(&h->saved_intent, P) != cudaSuccess) {
         delete h;
         return nullptr;
@@ -591,6 +595,28 @@ int ref_world_eco_reclaim(void *p, long long step, int sequential) {
         ref_relabel<<<(P + 255) / 256, 256>>>(d, a, 0, 1001);
         reclaim_dead_genomes<<<(P + 127) / 128, 128>>>(d, step);
         ref_relabel<<<(P + 255) / 256, 256>>>(d, -1, 1001, 0);
+    }
+    return (int)cudaDeviceSynchronize();
+}
+
+// reproduce (src/main.cu:1662-1737); sequential = 1: one parent at a time in
+// ascending slot order (the parents of this step relabelled 1 -> 1000 but one).
+int ref_world_eco_reproduce(void *p, int sequential) {
+    EcoWorld &h = *static_cast<EcoWorld *>(p);
+    Device &d = h.d;
+    if (!sequential) {
+        reproduce<<<(P + 127) / 128, 128>>>(d);
+        return (int)cudaDeviceSynchronize();
+    }
+    std::vector<Animal> a(P);
+    cudaMemcpy(a.data(), d.animals, sizeof(Animal) * P, cudaMemcpyDeviceToHost);
+    std::vector<int> parents;
+    for (int i = 0; i < P; ++i)
+        if (a[i].alive == 1 && a[i].energy >= 22) parents.push_back(i);
+    for (int q : parents) {
+        ref_relabel<<<(P + 255) / 256, 256>>>(d, q, 1, 1000);
+        reproduce<<<(P + 127) / 128, 128>>>(d);
+        ref_relabel<<<(P + 255) / 256, 256>>>(d, -1, 1000, 1);
     }
     return (int)cudaDeviceSynchronize();
 }

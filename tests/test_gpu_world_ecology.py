@@ -21,15 +21,16 @@ import numpy as np
 import pytest
 
 from oracle.pyoracle import (HERE, world_body_step, world_homeostasis, world_reclaim, world_regrow_and_sense,
-                             world_step)
+                             world_reproduce, world_step)
 
 pytestmark = pytest.mark.gpu
 
 POOLS = ("neurons", "synapses", "neuron_state", "synapse_state", "pending_exc", "pending_inh", "mod_event_tick",
-         "spike_history", "motors", "senses", "animals", "neuron_owner", "synapse_owner")
+         "spike_history", "motors", "senses", "animals", "neuron_owner", "synapse_owner", "neuron_next",
+         "synapse_next", "neuron_port")
 ECO = ("food", "cell_head", "cell_next", "bite_intent", "neuron_used", "synapse_used", "founder_motor_steps",
        "founder_observed_steps", "deaths", "predation_deaths", "bites", "life_records", "life_count", "bite_events",
-       "bite_event_count")
+       "bite_event_count", "neuron_clone", "births", "next_id")
 
 
 def _bits(a):
@@ -96,7 +97,7 @@ def _population(nsb, seed, founders, animal_capacity, neuron_capacity=None, syna
     return pools
 
 
-def _closed_loop(nsb, pools, eco, steps, seed, renewal, label):
+def _closed_loop(nsb, pools, eco, steps, seed, renewal, label, births=False):
     W = nsb.world
     world = W.World(pools)
     world.attach_ecology(eco)
@@ -114,6 +115,9 @@ def _closed_loop(nsb, pools, eco, steps, seed, renewal, label):
             world_homeostasis(ref)
             world.reclaim(step)
             world_reclaim(ref, ref_eco, step)
+            if births:
+                world.reproduce()
+                world_reproduce(ref, ref_eco)
             world.regrow_and_sense(step, seed, renewal)
             world_regrow_and_sense(ref, ref_eco, step, seed, renewal)
             _compare(world.download(), ref, world.download_ecology(), ref_eco, f"{label} step {step}")
@@ -167,6 +171,38 @@ def test_ecology_reclaims_long_and_short_lists(nsb, oracle_built):
     assert ref_eco.life_count[0] == batch.brains
     assert ref_eco.life_records["active_synapses"][:batch.brains].max() > 4096
     assert not (ref.synapse_owner >= 0).any() and not ref_eco.synapse_used.any()
+
+
+def test_reproduction_closed_loop_matches_oracle(nsb, oracle_built):
+    """Births with mutation in the closed loop: 30 of 120 founders well fed
+    (energy 100) reproduce every step, some in crowded cells and some of them
+    dying, so the births reuse reclaimed animal and pool slots. About 240
+    births over 8 steps draw every mutation choice."""
+    W = nsb.world
+    pools2 = _population(nsb, 71, founders=120, animal_capacity=400, neuron_capacity=60000,
+                         synapse_capacity=600000)
+    pools2.animals["energy"][np.nonzero(pools2.animals["alive"] == 1)[0][::4]] = 100.0
+    eco = W.make_ecology(pools2, seed=9, initial_count=60, life_capacity=256)
+    ref, ref_eco = _closed_loop(nsb, pools2, eco, 8, seed=9, renewal=0.01, label="births", births=True)
+    assert ref_eco.births[0] > 150
+    assert ref_eco.next_id[0] == eco.next_id[0] + ref_eco.births[0]
+    assert (ref.animals["generation"] > 0).sum() > 100
+    counts = ref.animals["neuron_count"][ref.animals["generation"] > 0]
+    assert len(np.unique(counts)) > 10                  # mutation changed brain sizes
+
+
+def test_reproduction_with_full_pools_undoes_births(nsb, oracle_built):
+    """Pools with little room: births that run out of neuron or synapse slots
+    midway are released again (src/main.cu:1712-1717)."""
+    W = nsb.world
+    pools = _population(nsb, 81, founders=40, animal_capacity=60)
+    pools.animals["energy"][pools.animals["alive"] == 1] = 60.0
+    eco = W.make_ecology(pools, seed=4, initial_count=0, life_capacity=64)
+    ref, ref_eco = _closed_loop(nsb, pools, eco, 2, seed=4, renewal=0.0, label="full", births=True)
+    assert 0 < ref_eco.births[0] < 80
+    # a parent left without offspring while animal slots were free: its birth was undone
+    A = ref.animals
+    assert (A["alive"] == 0).any() and ((A["alive"] == 1) & (A["energy"] > 55) & (A["generation"] == 0)).any()
 
 
 def test_ecology_reports_bad_lists(nsb):
