@@ -18,8 +18,8 @@ e2e   : the same metric through the reference's C ABI call ns_gpu_step with
 
 --world : the world simulator's neural stage (config 2 founders, or --world-population
         full) through nsb_world_*, then the reference's world kernels on the same pools.
---world-loop : the world step without reproduction (neural stage, body, bites,
-        homeostasis, reclamation, regrowth, senses), closed loop, then the
+--world-loop : the world step (neural stage, body, bites, homeostasis,
+        reclamation, reproduction, regrowth, senses), closed loop, then the
         reference's kernels for the same steps on the same initial pools.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -615,7 +615,7 @@ def run_serve(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
-def world_population(nsb, population, founders=2048, compact=False):
+def world_population(nsb, population, founders=2048, compact=False, scatter=None):
     """World pools at the reference build's capacities (32,768 animals,
     4,194,304 neuron and 8,388,608 synapse slots). "founders": 2,048 founders
     of 32-96 neurons with 4-12 synapses per neuron (config 2); "full": the
@@ -639,7 +639,7 @@ def world_population(nsb, population, founders=2048, compact=False):
                                    synapse_capacity=E + 8192)
     else:
         pools = W.place_population(batch, *recs, animal_capacity=32768, neuron_capacity=4194304,
-                                   synapse_capacity=8388608)
+                                   synapse_capacity=8388608, scatter_seed=scatter)
     return batch, pools
 
 
@@ -782,10 +782,11 @@ def run_world_stage(args, rank, world, local_rank):
 
 
 def run_world_loop(args, rank, world, local_rank):
-    """The world step without reproduction, in the reference host loop's order
-    (src/main.cu:2634-2770): neural stage, body step with spatial index, bites
-    and predation deaths, homeostasis, genome reclamation, regrowth and senses,
-    closed loop (each step's senses drive the next). This library's stages,
+    """The world step in the reference host loop's order (src/main.cu:2634-2770):
+    neural stage, body step with spatial index, bites and predation deaths,
+    homeostasis, genome reclamation, reproduction with mutation, regrowth and
+    senses, closed loop (each step's senses drive the next; cohort
+    observation, an observer, is left out). This library's stages,
     then the reference's own kernels (the world binary's flags, launched as
     its host loop launches them) on the same initial pools. Rank 0 only."""
     import ctypes as ct
@@ -796,8 +797,14 @@ def run_world_loop(args, rank, world, local_rank):
     sys.path.insert(0, str(ROOT))
     nsb = load_package()
     W = nsb.world
-    batch, pools = world_population(nsb, args.world_population, args.world_founders, False)
+    # slots spread over the pools, as the simulator's hinted claims spread them
+    # (init_animals, src/main.cu:547-611); packed slots would make every
+    # claim_slot scan long runs of full bitmap words
+    batch, pools = world_population(nsb, args.world_population, args.world_founders, False, scatter=3)
     W.place_bodies(pools, 3)
+    if args.world_parents > 0:                    # a fraction of well-fed animals: births every step
+        live = np.nonzero(pools.animals["alive"] == 1)[0]
+        pools.animals["energy"][live[:int(len(live) * args.world_parents)]] = 200.0
     seed, renewal = 2, 0.0006                     # the simulator's defaults (src/main.cu:1937)
     eco = W.make_ecology(pools, seed=seed, initial_count=batch.brains, life_capacity=32768 * 16)
     B = batch.brains
@@ -840,6 +847,7 @@ def run_world_loop(args, rank, world, local_rank):
         stage.body_step(k)
         stage.homeostasis()
         stage.reclaim(k)
+        stage.reproduce()
         stage.regrow_and_sense(k, seed, renewal)
         if ev:
             ev[2].record()
@@ -852,17 +860,19 @@ def run_world_loop(args, rank, world, local_rank):
     stage.close()
     del stage
     torch.cuda.empty_cache()
-    line = {"metric": "neuron-ticks/s of the world step (neural stage + ecology, no reproduction)",
+    line = {"metric": "neuron-ticks/s of the world step (neural stage + ecology)",
             "value": neuron_steps * 16 / (ms * args.steps / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": warm, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (Philox4x32-10, seed 2); food grid of init_world seed 2",
             "config": {"workload": f"world_loop_founders_{B}" if args.world_population == "founders"
                        else "world_loop_full", "animals": B, "neurons_at_start": alive_n[0],
-                       "food_renewal": renewal, "pools": "reference capacities (32,768 / 4,194,304 / 8,388,608)",
-                       "step": "neural_step, body_step, homeostasis, reclaim, regrow_and_sense (4 host syncs)"},
+                       "food_renewal": renewal,
+                       "pools": "reference capacities (32,768 / 4,194,304 / 8,388,608), slots scattered",
+                       "well_fed_fraction": args.world_parents,
+                       "step": "neural_step, body_step, homeostasis, reclaim, reproduce, regrow_and_sense (5 host syncs)"},
             "ecology_ms_per_step": eco_ms,
             "world_counts": {"deaths": int(fin.deaths[0]), "bites": int(fin.bites[0]),
-                             "life_records": int(fin.life_count[0])},
+                             "life_records": int(fin.life_count[0]), "births": int(fin.births[0])},
             "clocks": clk}
     print(json.dumps(line), flush=True)
 
@@ -884,6 +894,7 @@ def run_world_loop(args, rank, world, local_rank):
     wlib.ref_world_eco_regrow_and_sense.argtypes = [ct.c_void_p, ct.c_longlong, ct.c_ulonglong, ct.c_float,
                                                     ct.c_int]
     wlib.ref_world_eco_destroy.argtypes = [ct.c_void_p]
+    wlib.ref_world_eco_reproduce.argtypes = [ct.c_void_p, ct.c_int]
     for mode, label in ((0, "fused global-slot kernels"), (1, "--block-brains tiers + global-slot fallback")):
         holder = W.World(pools)          # device copies of the pools and ecology, in the shared layouts
         holder.attach_ecology(eco)
@@ -902,6 +913,7 @@ def run_world_loop(args, rank, world, local_rank):
             wlib.ref_world_eco_body(x, k, 0)
             wlib.ref_world_pools_homeostasis(h)
             wlib.ref_world_eco_reclaim(x, k, 0)
+            wlib.ref_world_eco_reproduce(x, 0)
             wlib.ref_world_eco_regrow_and_sense(x, k, seed, renewal, 0)
             if ev:
                 ev[2].record()
@@ -915,7 +927,7 @@ def run_world_loop(args, rank, world, local_rank):
         del holder
         torch.cuda.empty_cache()
         print(json.dumps({"impl": "reference-cuda-world-loop", "metric": "ms per world step (neural stage + "
-                          "ecology, no reproduction)", "value": rms, "unit": "ms", "higher_is_better": False,
+                          "ecology)", "value": rms, "unit": "ms", "higher_is_better": False,
                           "steps": args.steps, "warmup": warm, "ecology_ms_per_step": reco_ms,
                           "ours_ms_per_step": ms, "ours_ecology_ms_per_step": eco_ms,
                           "config": dict(line["config"], kernel=f"src/main.cu, {label}, --use_fast_math, sm_100a"),
@@ -948,8 +960,10 @@ def main():
     ap.add_argument("--world-founders", type=int, default=2048, help="founders of the config-2 population")
     ap.add_argument("--world-compact", action="store_true",
                     help="pools sized to the population, no reference leg (profiler captures)")
+    ap.add_argument("--world-parents", type=float, default=0.0,
+                    help="--world-loop: fraction of founders given energy 200 (they reproduce every step)")
     ap.add_argument("--world-loop", action="store_true",
-                    help="the world step without reproduction: neural stage + ecology, closed loop")
+                    help="the world step: neural stage + ecology with reproduction, closed loop")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus if "RANK" in os.environ else 1))

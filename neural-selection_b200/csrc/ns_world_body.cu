@@ -798,7 +798,7 @@ __device__ __forceinline__ void release_one(uint32_t *used, int slot) { used[slo
 // Claims for hints hint0 + k, k < K, in order, into out[k]; the number that
 // succeeded (K, or the index of the first failure). All threads of the CTA.
 __device__ int claim_run(uint32_t *used, int capacity, int hint0, int K, int *out) {
-    __shared__ int fail_at;
+    __shared__ int fail_at, found_off;
     const int words = (capacity + 31) / 32;
     const int t = threadIdx.x;
     int done = 0;
@@ -818,16 +818,36 @@ __device__ int claim_run(uint32_t *used, int capacity, int hint0, int K, int *ou
             }
         }
         if (__syncthreads_or(flag)) {
-            if (t == 0) {
-                fail_at = -1;
-                for (int i = 0; i < B; ++i) {
-                    const int slot = claim_one(used, capacity, hint0 + done + i);
-                    out[done + i] = slot;
-                    if (slot < 0) { fail_at = done + i; break; }
+            // one claim after another; the CTA searches 256 words at a time
+            // for the first word with a free bit, as claim_slot scans from its hint
+            if (t == 0) fail_at = -1;
+            for (int i = 0; i < B; ++i) {
+                const int start = (hint0 + done + i) % words;
+                if (t == 0) found_off = INT_MAX;
+                __syncthreads();
+                for (int base = 0; base < words; base += blockDim.x) {
+                    const int off = base + t;
+                    if (off < words && ~used[(start + off) % words]) atomicMin(&found_off, off);
+                    __syncthreads();
+                    if (found_off != INT_MAX) break;
                 }
+                if (t == 0) {
+                    int slot = -1;
+                    if (found_off != INT_MAX) {
+                        const int w = (start + found_off) % words;
+                        const uint32_t occ = used[w];
+                        const int cand = w * 32 + __ffs(~occ) - 1;
+                        if (cand < capacity) {
+                            used[w] = occ | (1u << (cand & 31));
+                            slot = cand;
+                        }
+                    }
+                    out[done + i] = slot;
+                    if (slot < 0) fail_at = done + i;
+                }
+                __syncthreads();
+                if (fail_at >= 0) return fail_at;
             }
-            __syncthreads();
-            if (fail_at >= 0) return fail_at;
         } else {
             if (t < B) {
                 used[mine >> 5] |= 1u << (mine & 31);     // each lane owns its word in this round

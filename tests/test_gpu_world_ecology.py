@@ -235,19 +235,27 @@ def _ref_eco_lib():
     for f in ("ref_world_eco_body", "ref_world_eco_reclaim", "ref_world_eco_regrow_and_sense"):
         getattr(lib, f).restype = ct.c_int
     lib.ref_world_eco_destroy.argtypes = [ct.c_void_p]
+    lib.ref_world_eco_reproduce.argtypes = [ct.c_void_p, ct.c_int]
+    lib.ref_world_eco_reproduce.restype = ct.c_int
     return lib
 
 
-def test_ecology_matches_reference_kernels(nsb):
+@pytest.mark.parametrize("births", [False, True])
+def test_ecology_matches_reference_kernels(nsb, births):
     """Both sides run this library's neural stage (pinned separately); the
     ecology kernels are this stage's on one copy of the pools and the
-    reference's own, replayed in slot order, on the other."""
+    reference's own, replayed in slot order, on the other. With births,
+    a third of the animals are well fed and reproduce every step (the
+    reference's reproduce with mutate, one parent at a time)."""
     ref = _ref_eco_lib()
     if ref is None:
         pytest.skip("oracle/_ref/libns_ref_world_cr.so not built")
     W = nsb.world
     pools = _population(nsb, 51, founders=72, animal_capacity=32768, neuron_capacity=4194304,
                         synapse_capacity=8388608)
+    if births:
+        live = np.nonzero(pools.animals["alive"] == 1)[0]
+        pools.animals["energy"][live[::3]] = 100.0
     eco = W.make_ecology(pools, seed=7, initial_count=40, life_capacity=32768 * 16)
     ours = W.World(pools)
     ours.attach_ecology(eco)
@@ -267,11 +275,15 @@ def test_ecology_matches_reference_kernels(nsb):
             theirs.homeostasis()
             ours.reclaim(step)
             assert ref.ref_world_eco_reclaim(h, step, 1) == 0
+            if births:
+                ours.reproduce()
+                assert ref.ref_world_eco_reproduce(h, 1) == 0
             ours.regrow_and_sense(step, 7, 0.05)
             assert ref.ref_world_eco_regrow_and_sense(h, step, 7, 0.05, 1) == 0
             want_eco = theirs.download_ecology()
             _compare(ours.download(), theirs.download(), ours.download_ecology(), want_eco, f"step {step}")
         assert want_eco.bites[0] > 0 and want_eco.deaths[0] > 0 and want_eco.life_count[0] > 0
+        assert want_eco.births[0] > (100 if births else -1)
     finally:
         ref.ref_world_eco_destroy(h)
         ours.close()
