@@ -107,6 +107,7 @@ struct Eco {
     int *pn_g, *ps_g, *pn_list, *ps_list;
     int *cn, *cs;
     uint32_t *nseed, *sseed;
+    const unsigned long long *jump;              // [kJumpLevels][64]: columns of M^(2^j), M the xorshift64 step
     int *status;
 };
 
@@ -712,6 +713,42 @@ constexpr int kGrowth = 64;                      // list entries mutation may ad
 constexpr int kD = 8;
 
 __device__ __forceinline__ int randint(unsigned long long &s, int size) { return (int)(uniform(s) * size); }
+// The xorshift64 state step (src/main.cu:331-334, before the output multiply)
+// is linear over GF(2): s' = M s. Columns of M^(2^j) let a thread reach the
+// state k steps ahead in log2(k) matrix-vector products, so the draws of a
+// birth are taken in parallel, each thread a contiguous run of the stream,
+// with the values the sequence gives.
+constexpr int kJumpLevels = 24;                  // jumps up to 2^24 draws
+__device__ __forceinline__ unsigned long long jump_state(const unsigned long long *jump, unsigned long long s,
+                                                         unsigned k) {
+    for (int level = 0; k; ++level, k >>= 1) {
+        if (!(k & 1u)) continue;
+        const unsigned long long *col = jump + level * 64;
+        unsigned long long acc[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int b = 0; b < 64; ++b) acc[b & 3] ^= col[b] & (0ull - ((s >> b) & 1ull));
+        s = (acc[0] ^ acc[1]) ^ (acc[2] ^ acc[3]);
+    }
+    return s;
+}
+// The draws k < count after state s0, (uint32)random64 each: k < na to
+// a[k], the rest to b[k - na]. All threads; each takes a contiguous run. The
+// state after the last draw goes to *final.
+__device__ void parallel_draws(const unsigned long long *jump, unsigned long long s0, int na, uint32_t *a, int nb,
+                               uint32_t *b, unsigned long long *final) {
+    const int count = na + nb;
+    const int chunk = (count + blockDim.x - 1) / blockDim.x;
+    const int k0 = threadIdx.x * chunk, k1 = min(count, k0 + chunk);
+    if (count == 0 && threadIdx.x == 0) *final = s0;
+    if (k0 >= k1) return;
+    unsigned long long st = jump_state(jump, s0, (unsigned)k0);
+    for (int k = k0; k < k1; ++k) {
+        const uint32_t v = (uint32_t)random64(st);
+        if (k < na) a[k] = v;
+        else b[k - na] = v;
+    }
+    if (k1 == count) *final = st;
+}
 __device__ __forceinline__ uint32_t state_hash(uint32_t seed) {
     uint32_t x = seed ? seed : 1u;
     x ^= x >> 16; x *= 0x7feb352du;
@@ -1010,9 +1047,14 @@ __device__ int random_hidden(const Eco &e, const ChildLists &c, const ref::Anima
     const int hidden = b.neuron_count - (kS + kM);
     if (hidden <= 0) return -1;
     int ordinal = randint(rng, hidden);
-    for (int i = c.nn - 1; i >= 0; --i) {
-        const int n = c.n[i];
-        if (e.nport[n] < 0 && ordinal-- == 0) return n;
+    for (int i = c.nn - 1; i >= 0; i -= 8) {                 // list order, eight loads before the tests
+        int nb[8], pt[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) nb[j] = i - j >= 0 ? c.n[i - j] : -1;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) pt[j] = nb[j] >= 0 ? e.nport[nb[j]] : 0;
+        for (int j = 0; j < 8 && i - j >= 0; ++j)
+            if (pt[j] < 0 && ordinal-- == 0) return nb[j];
     }
     return -1;
 }
@@ -1054,13 +1096,21 @@ __device__ void random_synapse(const Eco &e, const ChildLists &c, ref::SynapseGe
     const ref::Animal &body = e.animals[child];
     int active_sources = 0;
     float target_weight = 0;
-    for (int i = c.nn - 1; i >= 0; --i) {
-        const int n = c.n[i];
-        const ref::NeuronGene &gene = e.ngene[n];
-        if (!gene.active) continue;
-        ++active_sources;
-        const int port = e.nport[n];
-        if (port < 0 || port >= kS) target_weight += gene.affinity;
+    for (int i = c.nn - 1; i >= 0; i -= 8) {                 // list order, eight loads before the sums
+        int act[8], pt[8];
+        float aff[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int n = i - j >= 0 ? c.n[i - j] : -1;
+            act[j] = n >= 0 ? e.ngene[n].active : 0;
+            pt[j] = n >= 0 ? e.nport[n] : 0;
+            aff[j] = n >= 0 ? e.ngene[n].affinity : 0.0f;
+        }
+        for (int j = 0; j < 8 && i - j >= 0; ++j) {
+            if (!act[j]) continue;
+            ++active_sources;
+            if (pt[j] < 0 || pt[j] >= kS) target_weight += aff[j];
+        }
     }
     g.pre = body.ports[0];
     int source_choice = randint(rng, active_sources);
@@ -1310,10 +1360,12 @@ __device__ void mutate(const Eco &e, ChildLists &c, int child, unsigned long lon
 // One CTA: the births of this step in ascending parent slot order (src/main.cu:1662-1737).
 __global__ void __launch_bounds__(256) eco_births(Eco e) {
     __shared__ int s_child, s_n, s_s, s_start;
-    __shared__ unsigned long long s_rng;
+    __shared__ unsigned long long s_rng, s_final;
     __shared__ ref::Animal s_nb, s_parent;
+    __shared__ unsigned long long s_jump[kJumpLevels * 64];
     const int t = threadIdx.x;
     const int np = parent_count(e);
+    for (int i = t; i < kJumpLevels * 64; i += blockDim.x) s_jump[i] = e.jump[i];
     for (int q = 0; q < np; ++q) {
         const int a = e.parents[q];
         __syncthreads();
@@ -1357,12 +1409,13 @@ __global__ void __launch_bounds__(256) eco_births(Eco e) {
         const int N = e.pn_tmp[a], M = e.ps_tmp[a];
         const int *pn = e.pn_list + e.pn_off[a], *ps = e.ps_list + e.ps_off[a];
         // neurons: claims, draws in order, copies
+        // claims first (they draw nothing), then the birth's draws in the
+        // reference's order: one per copied neuron, then one per copied synapse
         const int n_ok = claim_run(e.nused, e.ncap, child * 131, N, e.cn);
-        if (t == 0) {
-            unsigned long long r = s_rng;
-            for (int k = 0; k < n_ok; ++k) e.nseed[k] = (uint32_t)random64(r);
-            s_rng = r;
-        }
+        const int s_ok = n_ok == N ? claim_run(e.sused, e.ecap, child * 257, M, e.cs) : 0;
+        parallel_draws(s_jump, s_rng, n_ok, e.nseed, s_ok, e.sseed, &s_final);
+        __syncthreads();
+        if (t == 0) s_rng = s_final;
         __syncthreads();
         for (int k = t; k < n_ok; k += blockDim.x) {
             const int old = pn[k], n = e.cn[k];
@@ -1370,15 +1423,7 @@ __global__ void __launch_bounds__(256) eco_births(Eco e) {
             e.neuron_clone[old] = n;
         }
         __syncthreads();
-        int s_ok = 0;
         if (n_ok == N) {
-            s_ok = claim_run(e.sused, e.ecap, child * 257, M, e.cs);
-            if (t == 0) {
-                unsigned long long r = s_rng;
-                for (int k = 0; k < s_ok; ++k) e.sseed[k] = (uint32_t)random64(r);
-                s_rng = r;
-            }
-            __syncthreads();
             for (int k = t; k < s_ok; k += blockDim.x) {
                 ref::SynapseGene g = e.sgene[ps[k]];
                 if ((unsigned)g.pre >= (unsigned)e.ncap || (unsigned)g.post >= (unsigned)e.ncap) {
@@ -1426,10 +1471,13 @@ __global__ void __launch_bounds__(256) eco_births(Eco e) {
             mutate(e, c, child, r, reinterpret_cast<int *>(e.sseed));   // sseed as scratch (reseeded below)
             s_n = c.nn;
             s_s = c.ns;
-            for (int i = c.nn - 1; i >= 0; --i) e.nseed[c.nn - 1 - i] = (uint32_t)random64(r);
-            for (int i = c.ns - 1; i >= 0; --i) e.sseed[c.ns - 1 - i] = (uint32_t)random64(r);
             s_rng = r;
         }
+        __syncthreads();
+        // new states: one draw per neuron, then per synapse, in list order
+        parallel_draws(s_jump, s_rng, s_n, e.nseed, s_s, e.sseed, &s_final);
+        __syncthreads();
+        if (t == 0) s_rng = s_final;
         __syncthreads();
         for (int k = t; k < s_n; k += blockDim.x) birth_state(e, e.cn[s_n - 1 - k], e.nseed[k]);
         for (int k = t; k < s_s; k += blockDim.x) birth_synapse_state(e, e.cs[s_s - 1 - k], e.sseed[k]);
@@ -1549,6 +1597,23 @@ public:
         x_.cs = dev_zeros<int>(owned_, EC + kGrowth);
         x_.nseed = dev_zeros<uint32_t>(owned_, NC + kGrowth);
         x_.sseed = dev_zeros<uint32_t>(owned_, EC + kGrowth);
+        {   // columns of M^(2^j) for the xorshift64 step
+            std::vector<unsigned long long> cols((size_t)kJumpLevels * 64);
+            auto step = [](unsigned long long v) { v ^= v >> 12; v ^= v << 25; v ^= v >> 27; return v; };
+            for (int b = 0; b < 64; ++b) cols[b] = step(1ull << b);
+            for (int level = 1; level < kJumpLevels; ++level) {
+                const unsigned long long *prev = &cols[(size_t)(level - 1) * 64];
+                for (int b = 0; b < 64; ++b) {
+                    unsigned long long v = prev[b], acc = 0;   // M^(2^(l-1)) applied to its own column
+                    for (int k = 0; k < 64; ++k)
+                        if ((v >> k) & 1ull) acc ^= prev[k];
+                    cols[(size_t)level * 64 + b] = acc;
+                }
+            }
+            auto *dj = dev_zeros<unsigned long long>(owned_, cols.size());
+            NSB_CHECK(cudaMemcpy(dj, cols.data(), cols.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+            x_.jump = dj;
+        }
         ref::NeuronGene prof[7];
         neuron_profiles(prof);
         auto *dprof = dev_zeros<ref::NeuronGene>(owned_, 7);
