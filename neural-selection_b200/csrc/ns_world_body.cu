@@ -1,8 +1,8 @@
 // World ecology stage: the world simulator's per-step body, predation, genome
-// reclamation, food regrowth and senses (mixic/neural-selection
-// src/main.cu:612-657 and 1138-1338), on the simulator's own pools: the neural
-// pools of NsbWorldPools plus the food grid, spatial index, slot bitmaps and
-// counters of NsbWorldEcology.
+// reclamation, reproduction with mutation, food regrowth and senses
+// (mixic/neural-selection src/main.cu:364-525, 612-657 and 1138-1737), on the
+// simulator's own pools: the neural pools of NsbWorldPools plus the food
+// grid, spatial index, slot bitmaps and counters of NsbWorldEcology.
 //
 // Order of one world step in the reference host loop (src/main.cu:2745-2770),
 // with the calls that replace each part:
@@ -10,7 +10,8 @@
 //                                                  nsb_world_body_step
 //   homeostasis                                    nsb_world_homeostasis
 //   reclaim_dead_genomes                           nsb_world_reclaim
-//   (reproduce, cohort observation: the caller's)
+//   reproduce                                      nsb_world_reproduce
+//   (cohort observation: the caller's)
 //   regrow, spatial reset, index_animals, update_senses
 //                                                  nsb_world_regrow_and_sense
 //
@@ -29,7 +30,9 @@
 //   - bites only touch animals of the attacker's own cell, so each cell's
 //     attackers run in slot order on one thread, cells in parallel;
 //   - bite events and life records take consecutive indices in slot order
-//     (a scan over the animal slots).
+//     (a scan over the animal slots);
+//   - births: parents one after another in slot order, each birth's slot
+//     claims as claim_slot run alone (below, reproduction).
 // Arithmetic: cosf, sinf and hypotf are the correctly rounded nsx functions,
 // sqrtf and division are IEEE (no contraction), so the results are those of
 // the reference's kernels built with IEEE arithmetic and the same correctly
@@ -704,11 +707,12 @@ __global__ void __launch_bounds__(128) eco_senses(Eco e) {
 // is one CTA: the parent's lists come ranked in list order (gathered by owner,
 // ranked in shared memory as for reclamation); claims run 256 at a time in
 // parallel when each lands in its own hint word (claims in distinct words do
-// not see each other, so the result is that of the sequence), otherwise in
-// sequence on one thread; the RNG draws of the birth are taken in order by one
-// thread and the records written in parallel; mutation runs on one thread over
-// array copies of the child's lists, keeping the linked lists in global memory
-// exactly as the reference's list surgery leaves them.
+// not see each other, so the result is that of the sequence), otherwise one
+// after another with the CTA searching for the first free word; the birth's
+// RNG draws are taken in parallel by jumping ahead in the stream, and the
+// records written in parallel; mutation runs on one thread over array copies
+// of the child's lists, keeping the linked lists in global memory exactly as
+// the reference's list surgery leaves them.
 constexpr int kGrowth = 64;                      // list entries mutation may add (4 x at most 2)
 constexpr int kD = 8;
 

@@ -2,8 +2,9 @@
 nsb_world_regrow_and_sense through the C ABI).
 
 A closed world loop: the neural stage, the body step, homeostasis, genome
-reclamation, regrowth and senses, with the senses of each step feeding the
-next step's neural stage (src/main.cu:2634-2770 without reproduction). Every
+reclamation, reproduction with mutation (where a test asks for births),
+regrowth and senses, with the senses of each step feeding the next step's
+neural stage (src/main.cu:2634-2770). Every
 pool and every ecology array must equal the oracle's (the reference kernels
 restated as loops in ascending slot order) after each step. The populations
 crowd animals into a few cells so that harvests of one food unit, bites, kills
