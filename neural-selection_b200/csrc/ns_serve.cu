@@ -518,7 +518,7 @@ void Server::upload_unit_table() {
     n_table_ = (int)active_units_.size();
     if (n_table_ == 0) { table_dirty_ = false; return; }
     const int par = (int)(iter_ & 1);
-    // The table goes at the end of this round's staging buffer.
+    // The table goes at the end of this admission round's staging buffer.
     const size_t bytes = (size_t)n_table_ * (sizeof(int4) + sizeof(int2));
     if (bytes > (size_t)cfg_.staging_bytes / 4) throw std::runtime_error("unit table exceeds the staging buffer");
     unsigned char *base = h_stage_[par] + (size_t)cfg_.staging_bytes - align16(bytes);
