@@ -1,7 +1,9 @@
 /* ORACLE — test infrastructure only (see ns_oracle.h).
  *
- * Plain-C restatement of the reference neural tick. Each function cites the
- * reference lines it follows. Arithmetic is written so every binary32
+ * Plain-C restatement of the reference neural tick, and of the world step
+ * around it (body, spatial index, bites, genome reclamation, reproduction with
+ * mutation, regrowth, senses: the reference kernels run as loops in ascending
+ * animal slot order). Each function cites the reference lines it follows. Arithmetic is written so every binary32
  * operation happens in the reference's order (no contraction: build with
  * -ffp-contract=off), which is what makes a bit-for-bit comparison with the
  * reference's own compiled code meaningful.
@@ -10,7 +12,8 @@
  * evaluates a state-dependent exponential (the reference host build does the
  * same); constant-argument exponentials, which a C compiler folds to the
  * correctly rounded value, are the correctly rounded constants in both modes.
- * The default build binds every exponential to or_cr_expf/or_cr_logf.
+ * The default build binds every exponential to or_cr_expf/or_cr_logf, and
+ * the world step's cosf/sinf/hypotf to or_cr_cosf/or_cr_sinf/or_cr_hypotf.
  */
 #include "ns_oracle.h"
 
