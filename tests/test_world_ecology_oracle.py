@@ -188,3 +188,54 @@ def test_reproduction_keeps_the_pools_consistent(nsb, oracle_built):
     world_reproduce(pools2, eco2)
     assert np.array_equal(pools.animals.view(np.uint8), pools2.animals.view(np.uint8))
     assert np.array_equal(eco.neuron_used, eco2.neuron_used)
+
+
+def test_body_step_death_causes_and_food_kind_one(nsb, oracle_built):
+    """Known answers of body_step (src/main.cu:1146-1249) in binary32:
+    starvation (cause 2), old age (cause 4), and a meal of food kind 1
+    (energy +2, health and pain 1.4, first_b_age)."""
+    W = nsb.world
+    pools = _pools(nsb)
+    A = pools.animals
+    f32 = np.float32
+    A["energy"][1], A["health"][1] = 0.001, 0.1          # starves
+    A["age"][2] = 9999                                   # dies of age
+    A["energy"][3], A["health"][3], A["age"][3] = 12.0, 10.0, 150
+    eco = W.make_ecology(pools, seed=1)
+    eco.food[:] = 0
+    c3 = int(A["y"][3]) * 128 + int(A["x"][3])
+    eco.food[c3], eco.kind[c3] = 1, 1
+    pools.motors[3, 3] = 2                               # eats
+    before = A[[1, 2, 3]].copy()
+    world_body_step(pools, eco, 1)
+    B = W.behavior(A)
+    assert A["alive"][1] == 0 and B["death_cause"][1] == 2 and A["energy"][1] == 0
+    assert A["health"][1] == f32(f32(0.1) - f32(0.15))
+    assert A["alive"][2] == 0 and B["death_cause"][2] == 4 and A["age"][2] == 10000
+    assert eco.deaths[0] == 2
+    # animal 3: upkeep first, then the meal (energy capped at 30)
+    active = int(pools.neurons["active"][pools.neuron_owner == 3].sum())
+    e = f32(12.0) - (f32(f32(0.003) + f32(active) * f32(0.00002)) + f32(0.0) * f32(0.02) + f32(0.0))
+    assert A["energy"][3] == min(f32(30), f32(e + f32(2)))
+    assert A["health"][3] == f32(f32(10.0) - f32(1.4)) and A["pain"][3] == f32(f32(before["pain"][2] * f32(0.8)) + f32(1.4))
+    assert B["first_b_age"][3] == 151 and B["accepted"][3, 1, 0, 1] == 1 and eco.food[c3] == 0
+    assert A["age"][3] == 151 and A["alive"][3] == 1
+
+
+def test_muscle_twitch_moves_along_the_heading(nsb, oracle_built):
+    """Thrust from three spikes on the thrust motor: muscle = min(1, 0.9231
+    m + 0.3 spikes) (src/main.cu:1152-1160); heading 0 moves along +x by
+    thrust x 1.5 (cos 0 = 1 exactly, sin 0 = 0)."""
+    W = nsb.world
+    pools = _pools(nsb)
+    A = pools.animals
+    f32 = np.float32
+    A["muscle"][4] = [0.5, 0.0, 0.0]
+    x0, y0 = A["x"][4], A["y"][4]
+    eco = W.make_ecology(pools, seed=1)
+    pools.motors[4, 0] = 3
+    world_body_step(pools, eco, 1)
+    m = min(f32(1.0), f32(f32(f32(0.5) * f32(0.92311635)) + f32(f32(3) * f32(0.30))))
+    assert A["muscle"][4, 0] == m
+    assert A["x"][4] == f32(x0 + f32(m * f32(1.5))) and A["y"][4] == y0
+    assert (pools.motors[4] == 0).all()
