@@ -905,8 +905,11 @@ __global__ void eco_parent_flags(Eco e) {
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.P; a += gridDim.x * blockDim.x) {
         const ref::Animal &A = e.animals[a];
         const bool f = A.alive == 1 && A.energy >= 22;
+        // (a birth draws one value per neuron and synapse, twice; the jump
+        // tables reach 2^kJumpLevels draws)
         const bool sane = A.neuron_count >= 0 && A.neuron_count <= e.ncap && A.synapse_count >= 0 &&
-                          A.synapse_count <= e.ecap;
+                          A.synapse_count <= e.ecap &&
+                          (long long)A.neuron_count + A.synapse_count + 2 * kGrowth < (1ll << kJumpLevels);
         if (f && !sane) atomicOr(e.status, ES_LIST);
         e.pflag[a] = f && sane;
         e.pn_tmp[a] = f && sane ? A.neuron_count : 0;
