@@ -868,9 +868,9 @@ __device__ int claim_run(uint32_t *used, int capacity, int hint0, int K, int *ou
                 __syncthreads();
                 for (int base = 0; base < words; base += blockDim.x) {
                     const int off = base + t;
-                    if (off < words && ~used[(start + off) % words]) atomicMin(&found_off, off);
-                    __syncthreads();
-                    if (found_off != INT_MAX) break;
+                    const bool hit = off < words && ~used[(start + off) % words];
+                    if (hit) atomicMin(&found_off, off);
+                    if (__syncthreads_or(hit)) break;          // the same answer for every thread
                 }
                 if (t == 0) {
                     int slot = -1;
@@ -1387,9 +1387,9 @@ __global__ void __launch_bounds__(256) eco_births(Eco e) {
         __syncthreads();
         for (int base = 0; base < e.P; base += blockDim.x) {   // the first free animal slot from start
             const int j = base + t;
-            if (j < e.P && e.animals[(s_start + j) % e.P].alive == 0) atomicMin(&s_child, j);
-            __syncthreads();
-            if (s_child != INT_MAX) break;
+            const bool hit = j < e.P && e.animals[(s_start + j) % e.P].alive == 0;
+            if (hit) atomicMin(&s_child, j);
+            if (__syncthreads_or(hit)) break;                  // the same answer for every thread
         }
         if (s_child == INT_MAX) {
             if (t == 0) e.animals[a].rng = s_rng;
