@@ -729,6 +729,7 @@ __global__ void __launch_bounds__(kBlock, MINB) world_tick_small(WorldArgs d, Ca
                 if (q_i >= q_n) break;
                 const int i = q_i, nn = q_nn[i], nl = q_nl[i];
                 if (nu < kUnitAnimals && ntot + nn <= kBlock && etot + nl <= kUnitEdges) {
+                    __syncwarp();                                   // every lane has read q_i
                     if (lane == 0) {
                         ua_a[nu] = q_a[i]; ua_n0[nu] = ntot; ua_e0[nu] = etot;
                         q_i = i + 1;
