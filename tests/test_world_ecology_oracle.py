@@ -239,3 +239,30 @@ def test_muscle_twitch_moves_along_the_heading(nsb, oracle_built):
     assert A["muscle"][4, 0] == m
     assert A["x"][4] == f32(x0 + f32(m * f32(1.5))) and A["y"][4] == y0
     assert (pools.motors[4] == 0).all()
+
+
+def test_place_population_and_make_ecology_are_consistent(nsb):
+    """Host helpers (world.py): scattered pools give each animal lists of its
+    own slots with ports on its sensory and motor neurons; the ecology's slot
+    bitmaps mark exactly the owned slots; record layouts match the reference
+    sizes (LifeRecord 504 B, BiteEvent 24 B, Behavior 276 B)."""
+    W = nsb.world
+    assert (W.LIFE_RECORD.itemsize, W.BITE_EVENT.itemsize, W.BEHAVIOR.itemsize) == (504, 24, 276)
+    assert W.LIFE_RECORD.fields["death_step"][1] == 472
+    pools = _pools(nsb, founders=10, capacity=16)
+    A = pools.animals
+    for a in range(10):
+        ns = _walk(pools.neuron_next, A["neuron_head"][a], A["neuron_count"][a])
+        es = _walk(pools.synapse_next, A["synapse_head"][a], A["synapse_count"][a])
+        assert len(ns) == A["neuron_count"][a] and len(es) == A["synapse_count"][a]
+        assert (pools.neuron_owner[ns] == a).all() and (pools.synapse_owner[es] == a).all()
+        ports = A["ports"][a]
+        assert (ports >= 0).all()                       # 19 channels and 5 motors in every founder
+        assert all(pools.neuron_port[ports[p]] == p for p in range(24))
+    assert (A["alive"][10:] == 0).all() and (A["neuron_head"][10:] == -1).all()
+    eco = W.make_ecology(pools, seed=3)
+    for owner, words in ((pools.neuron_owner, eco.neuron_used), (pools.synapse_owner, eco.synapse_used)):
+        used = np.unpackbits(words.view(np.uint8), bitorder="little")[:len(owner)].astype(bool)
+        assert np.array_equal(used, owner >= 0)
+    assert eco.next_id[0] == A["id"].max() + 1
+    assert (eco.cell_head == -1).all() and eco.food.sum() > 0.2 * 16384
