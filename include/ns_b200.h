@@ -19,10 +19,10 @@
 extern "C" {
 #endif
 
-/* Replaces ns_error, gym_adapter/native.cpp:120. */
+/* Replaces ns_error, gym_adapter/native.cpp:45 (thread-local message, :39). */
 const char *ns_error(void);
 
-/* Replaces ns_create, gym_adapter/native.cpp:121-157. ng: count x 10 rows
+/* Replaces ns_create, gym_adapter/native.cpp:46-82 (validation 49-76). ng: count x 10 rows
  * [profile 0-6, channel -1..channels-1, active, inhibitory, modulator 0-3,
  * capacitance x, leak x, threshold mV, receptor Hz gain, receptor event nS];
  * sg: edges x 11 rows [pre, post, weight nS, active, delay 1-8, branch 0-3,
@@ -31,34 +31,34 @@ const char *ns_error(void);
 void *ns_create(int count, int edges, int channels, int outputs, const float *ng, const float *sg,
                 const int *motors);
 
-/* Replaces ns_original_indices, gym_adapter/native.cpp:158-162 (reset seeds
+/* Replaces ns_original_indices, gym_adapter/native.cpp:83-87 (reset seeds
  * use original indices after graph compilation). */
 void ns_original_indices(void *brain, const uint32_t *neurons, const uint32_t *synapses);
 
-/* Replaces ns_destroy, gym_adapter/native.cpp:163. */
+/* Replaces ns_destroy, gym_adapter/native.cpp:88. */
 void ns_destroy(void *brain);
 
-/* Replaces ns_reset, gym_adapter/native.cpp:164-169: state seeded from
+/* Replaces ns_reset, gym_adapter/native.cpp:89-94: state seeded from
  * seed + index*7919 (neurons) and seed + index*104729 (synapses). */
 void ns_reset(void *brain, uint32_t seed);
 
-/* Replaces ns_step, gym_adapter/native.cpp:170-183: `ticks` 1 ms ticks (1..10000),
+/* Replaces ns_step, gym_adapter/native.cpp:95-108: `ticks` 1 ms ticks (1..10000),
  * input[channels] in [0,1], output[outputs] = motor spikes during the call.
  * 0, or -1 ("Nonfinite neural state", invalid interval or observation). */
 int ns_step(void *brain, const float *input, int ticks, float input_gain, float *output);
 
-/* Replaces ns_gpu_create, gym_adapter/gpu.cu:273-315: a device batch built from
+/* Replaces ns_gpu_create, gym_adapter/gpu.cu:67-109: a device batch built from
  * `count` brain handles with equal channels/outputs. Honours GYM_CUDA_THREADS
  * validation (32/64/128/256). */
 void *ns_gpu_create(void **brains, int count);
 
-/* Replaces ns_gpu_destroy, gym_adapter/gpu.cu:316. */
+/* Replaces ns_gpu_destroy, gym_adapter/gpu.cu:110. */
 void ns_gpu_destroy(void *batch);
 
-/* Replaces ns_gpu_reset, gym_adapter/gpu.cu:317-319: reset brains with mask[i]. */
+/* Replaces ns_gpu_reset, gym_adapter/gpu.cu:111-113: reset brains with mask[i]. */
 int ns_gpu_reset(void *batch, const uint8_t *mask, const uint32_t *seeds);
 
-/* Replaces ns_gpu_step, gym_adapter/gpu.cu:320-329: synchronous; input
+/* Replaces ns_gpu_step, gym_adapter/gpu.cu:114-123: synchronous; input
  * count x channels, output count x outputs, status[i] = -1 on a non-finite
  * voltage (-2: tick counter past 2^31). */
 int ns_gpu_step(void *batch, const float *input, const uint8_t *mask, int ticks, float gain, float *output,

@@ -2,7 +2,7 @@
 //
 // The ns_* and ns_gpu_* entry points keep the reference's signatures, argument
 // meaning, validation messages and return conventions
-// (gym_adapter/native.cpp:120-183 and gym_adapter/gpu.cu:272-330 of
+// (gym_adapter/native.cpp:45-108 and gym_adapter/gpu.cu:67-123 of
 // mixic/neural-selection), so gym_adapter/adapter.py and gym_adapter/gpu.py can
 // load this library in place of libgym_brain.so / libgym_brain_gpu.so. Brain
 // handles share the reference's host layout (ns_refabi.h), so ns_gpu_create
@@ -97,7 +97,7 @@ bool finite_row(const float *p, int n) {
     return true;
 }
 
-// ns_create row decoding and validation (gym_adapter/native.cpp:121-157).
+// ns_create row decoding and validation (gym_adapter/native.cpp:46-82).
 // max_profile: 5 for the reference ABI; the extended creators also accept
 // profile 6 (triplet STDP into a dopamine-gated eligibility trace).
 HostBrain *make_brain(int count, int edges, int channels, int outputs, const float *ng, const float *sg,
@@ -260,7 +260,7 @@ int ns_step(void *p, const float *input, int ticks, float input_gain, float *out
         e.step_host(input, &one, ticks, input_gain, output, &status);
         if (status == -2) throw std::runtime_error("Tick counter exceeds the engine range");
         if (status != 0) {
-            e.set_tick(0, b.tick);   // the reference keeps its tick on failure (native.cpp:176-177)
+            e.set_tick(0, b.tick);   // the reference keeps its tick on failure (native.cpp:101-102)
             throw std::runtime_error("Nonfinite neural state");
         }
         b.tick += ticks;

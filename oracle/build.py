@@ -15,8 +15,8 @@ Outputs (all git-ignored):
                                       kernels (src/main.cu) with its own flags
   oracle/_ref/libns_ref_world_cr.so   the same kernels with IEEE arithmetic and
                                       correctly rounded exp/log
-The _ref targets need the reference tree (REFERENCE_ROOT, default
-/root/reference) and are skipped when it is absent; prebuilt files are used as
+The _ref targets need the reference tree (REFERENCE_ROOT, default: a directory
+named "reference" beside this repository) and are skipped when it is absent; prebuilt files are used as
 they are.
 """
 import os
@@ -30,7 +30,7 @@ REPO = HERE.parent
 BUILD = HERE / "_build"
 REF_OUT = HERE / "_ref"
 CSRC = REPO / "neural-selection_b200" / "csrc"
-REFERENCE = Path(os.environ.get("REFERENCE_ROOT", "/root/reference"))
+REFERENCE = Path(os.environ.get("REFERENCE_ROOT", REPO.parent / "reference"))
 
 CFLAGS = ["-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math"]
 

@@ -603,7 +603,7 @@ or_brain *or_create(int count, int edges, int channels, int outputs, const float
     b->exc = (float *)calloc((size_t)count * BRANCHES, sizeof(float));
     b->inh = (float *)calloc((size_t)count, sizeof(float));
     b->mod = (uint8_t *)calloc((size_t)count, 1);
-    for (int i = 0; i < count; ++i) {                          /* native.cpp:128-141 */
+    for (int i = 0; i < count; ++i) {                          /* native.cpp:53-66 */
         const float *p = ngr + (size_t)i * 10;
         for (int f = 0; f < 10; ++f) if (p[f] != p[f]) { bad(err, errlen, "Invalid neuron gene"); or_destroy(b); return NULL; }
         if (p[0] < 0 || p[0] > 6 || p[1] < -1 || p[1] >= channels || p[2] < 0 || p[2] > 1 || p[3] < 0 ||
@@ -621,7 +621,7 @@ or_brain *or_create(int count, int edges, int channels, int outputs, const float
         g.rec_base = 0; g.rec_gain = p[8]; g.rec_event = p[9];
         b->ng[i] = g;
     }
-    for (int i = 0; i < edges; ++i) {                          /* native.cpp:142-150 */
+    for (int i = 0; i < edges; ++i) {                          /* native.cpp:67-75 */
         const float *p = sgr + (size_t)i * 11;
         for (int f = 0; f < 11; ++f) if (p[f] != p[f]) { bad(err, errlen, "Invalid synapse gene"); or_destroy(b); return NULL; }
         if (p[0] < 0 || p[0] >= count || p[1] < 0 || p[1] >= count || p[2] < 0 || p[3] < 0 || p[3] > 1 ||
@@ -667,7 +667,7 @@ void or_destroy(or_brain *b) {
     free(b);
 }
 
-void or_reset(or_brain *b, uint32_t seed) {                    /* core.cuh:25-29, native.cpp:164-169 */
+void or_reset(or_brain *b, uint32_t seed) {                    /* core.cuh:25-29, native.cpp:89-94 */
     b->tick = 0;
     for (int i = 0; i < b->count; ++i) {
         uint32_t idx = b->orig_n ? b->orig_n[i] : (uint32_t)i;
@@ -724,7 +724,7 @@ int or_step(or_brain *b, const float *input, int ticks, float gain, float *outpu
                 neuron_tick(g, s, cur, b->exc + (size_t)j * BRANCHES, b->inh[j]);
                 if (b->sh) sh_neuron(b, j, input, gain);
                 if (!isfinite(s->v)) {
-                    /* ns_step keeps its tick counter on failure (native.cpp:176-177) */
+                    /* ns_step keeps its tick counter on failure (native.cpp:101-102) */
                     if (stop_on_nonfinite) { b->tick = tick0; return -1; }
                     failed = 1;
                 }

@@ -6,7 +6,7 @@
  *   physiology  src/physiology.cuh:29-586, src/lp_cell.cuh:16-113,
  *               src/prinz_cell.cuh:17-121
  *   ordering    gym_adapter/core.cuh:25-75 (edge order per tick)
- *   ABI rules   gym_adapter/native.cpp:121-183
+ *   ABI rules   gym_adapter/native.cpp:46-108
  * Parity pin: built in its libm mode (-DOR_LIBM) it reproduces the reference
  * host executor compiled from the reference's own sources (oracle/_ref) bit for
  * bit; in its default mode exp/log are correctly rounded (or_crmath.c), which
@@ -26,7 +26,7 @@ enum { OR_NEURON_WORDS = 32, OR_SYNAPSE_WORDS = 20 };
 
 typedef struct or_brain or_brain;
 
-/* ns_create semantics (gym_adapter/native.cpp:121-157); max_delay is 8 for
+/* ns_create semantics (gym_adapter/native.cpp:46-82); max_delay is 8 for
  * the reference ABI and up to 31 for the extended delay ring. Returns NULL and
  * fills err on invalid input. */
 or_brain *or_create(int count, int edges, int channels, int outputs,
@@ -40,7 +40,7 @@ void or_set_pulse(or_brain *b, int period, int mod);
 void or_reset(or_brain *b, uint32_t seed);
 /* ns_step semantics: 0, or -1 on a non-finite voltage. When stop_on_nonfinite
  * is 0 the step records the failure, keeps integrating (the CUDA batch
- * semantics of gym_adapter/gpu.cu:255) and returns -1 at the end.
+ * semantics of gym_adapter/gpu.cu:49) and returns -1 at the end.
  * raster (optional): ticks x count spike bytes. */
 int or_step(or_brain *b, const float *input, int ticks, float gain, float *output,
             uint8_t *raster, int stop_on_nonfinite);

@@ -41,7 +41,7 @@ extern "C" {
 // One animal per brain, genomes given as the Gym ABI rows (neuron rows of 10,
 // synapse rows of 11 floats, brain-local pre/post), decoded into the
 // reference's NeuronGene / SynapseGene with the rules of ns_create
-// (gym_adapter/native.cpp:128-150) using the reference's own profiles. A
+// (gym_adapter/native.cpp:53-75) using the reference's own profiles. A
 // sensory neuron reads world sense `channel` when channel < S. Returns NULL if
 // the population exceeds the pools.
 void *ref_world_create(int brains, const int64_t *noff, const int64_t *soff, const float *neuron_rows,

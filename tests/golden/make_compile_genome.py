@@ -1,11 +1,11 @@
 """Golden vectors of the genome compiler (tests/test_compile_genome.py).
 
 Runs the reference's own compile_genome (gym_adapter/compile_graph.py of
-mixic/neural-selection, read from REFERENCE_ROOT, default /root/reference) on
-seeded genomes and writes inputs and outputs to compile_genome.npz. The
-reference module imports Genome from its adapter, which needs gymnasium; a
-stub package supplies a Genome with the same fields (neurons, synapses,
-motors, channels), which is all compile_genome uses.
+mixic/neural-selection, read from REFERENCE_ROOT, default: a directory named
+"reference" beside this repository) on seeded genomes and writes inputs and
+outputs to compile_genome.npz. The reference module imports Genome from its
+adapter, which needs gymnasium; a stub package supplies a Genome with the same
+fields (neurons, synapses, motors, channels), which is all compile_genome uses.
 
     python tests/golden/make_compile_genome.py
 """
@@ -20,7 +20,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REFERENCE = Path(os.environ.get("REFERENCE_ROOT", "/root/reference"))
+REFERENCE = Path(os.environ.get("REFERENCE_ROOT", ROOT.parent / "reference"))
 
 
 def reference_compiler():

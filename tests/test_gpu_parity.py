@@ -173,7 +173,7 @@ def test_single_brain_ns_step(nsb):
 def test_nonfinite_voltage_reports_status(nsb):
     """An LP cell (type 2) driven by an enormous tonic current integrates to a
     non-finite voltage; the batch reports status -1 for that brain only and
-    keeps stepping the others (gym_adapter/gpu.cu:255)."""
+    keeps stepping the others (gym_adapter/gpu.cu:49)."""
     W = nsb.workloads
     ng = np.array([[2, 0, 1, 0, 0, 1, 1, -42, 0, 0], [0, -1, 1, 0, 0, 1, 1, -52, 0, 0]], np.float32)
     sg = np.array([[0, 1, 3.0, 1, 2, 0, .5, 100, 0, 1, 0]], np.float32)
@@ -203,7 +203,7 @@ def test_validation_messages(nsb):
     bad = batch.inputs.copy(); bad[0, 0] = 1.5
     with pytest.raises(RuntimeError, match="Invalid encoded observation"):
         gpu.step(bad, None, 4)
-    # a masked-out brain's observation is not validated (gym_adapter/gpu.cu:324)
+    # a masked-out brain's observation is not validated (gym_adapter/gpu.cu:118)
     gpu.step(bad, np.array([0, 1], np.uint8), 4)
 
 
