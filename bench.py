@@ -13,8 +13,14 @@ value : neuron-ticks/s with inputs resident on the device, one persistent
 e2e   : the same metric through the reference's C ABI call ns_gpu_step with
         pinned host buffers (host->device observations, device->host motor
         outputs and status inside the timed region).
+reference_cuda : (N=1, default run) the reference's own CUDA forms on the
+        same batch and GPU after this library's buffers are freed: the Gym
+        batch kernel step_batch (gym_adapter/gpu.cu) and the world simulator's
+        neural stage (src/main.cu) as fused global-slot kernels and as
+        --block-brains tiers; best_ratio = value / the fastest form's.
 --impl reference : the reference's own host executor (gym_adapter/native.cpp
         built from its sources into oracle/_ref) on the host cores.
+--impl reference-cuda : the reference's CUDA forms alone, one line each.
 
 --world : the world simulator's neural stage (config 2 founders, or --world-population
         full) through nsb_world_*, then the reference's world kernels on the same pools.
@@ -258,90 +264,95 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def run_reference_cuda(args, rank, world, local_rank):
-    """The reference's own CUDA batch (gym_adapter/gpu.cu: one CTA per brain,
-    ns_gpu_step through its C ABI, synchronous with host buffers) on the same
-    workload; delays folded into 1-8 because its ABI accepts 1-8 only."""
-    if rank != 0:
-        return
+def reference_cuda_forms(batch, steps, warmup, gpu_index=0):
+    """The reference's own CUDA forms of the neural tick on `batch`, timed with
+    CUDA events on the default stream they launch on:
+      step_batch   : gym_adapter/gpu.cu (one CTA of 32 threads per brain),
+                     ns_gpu_step through its C ABI with host buffers, its flags
+                     --fmad=false --prec-div=true --prec-sqrt=true;
+      global_slot  : src/main.cu neural stage, fused global-slot kernels;
+      block_tiers  : src/main.cu neural stage, --block-brains tiers with the
+                     global-slot fallback (both --use_fast_math, as the world
+                     binary is built).
+    Delays are folded into 1-8 because the reference accepts 1-8 only; the
+    cost per tick does not depend on the delay. Returns (forms, notes): forms
+    maps a form to {ms_per_step, value, e2e_value, ...}; the world forms are
+    timed only for the full-pool batch. Nothing of this library runs here."""
     import ctypes as ct
     import torch
     sys.path.insert(0, str(ROOT))
     from oracle import pyoracle
+    forms, notes = {}, []
     lib = pyoracle.ref_gpu_lib()
-    if lib is None:
-        print(json.dumps({"impl": "reference-cuda", "unavailable": "oracle/_ref/libns_ref_gpu.so not built"}))
-        return
-    nsb = load_package()
-    batch = workload(nsb, 2, 1, args.workload if args.workload in ("batched_uneven", "plain_small") else "batched_uneven")
-    f, i32 = ct.POINTER(ct.c_float), ct.POINTER(ct.c_int)
-    handles = []
-    for b in range(batch.brains):
-        ng, sg, mo = batch.brain(b)
-        sg = np.ascontiguousarray(sg.copy())
-        sg[:, 4] = (sg[:, 4] - 1) % 8 + 1
-        ng = np.ascontiguousarray(ng); mo = np.ascontiguousarray(mo, np.int32)
-        h = lib.ns_create(len(ng), len(sg), batch.channels, batch.outputs, ng.ctypes.data_as(f),
-                          sg.ctypes.data_as(f), mo.ctypes.data_as(i32))
-        if not h:
-            raise RuntimeError(lib.ns_error().decode())
-        handles.append(h)
-    arr = (ct.c_void_p * len(handles))(*handles)
-    t0 = time.perf_counter()
-    gb = lib.ns_gpu_create(arr, len(handles))
-    create_s = time.perf_counter() - t0
-    for h in handles:
-        lib.ns_destroy(h)
-    if not gb:
-        raise RuntimeError(lib.ns_error().decode())
-    mask = np.ones(batch.brains, np.uint8)
-    seeds = np.arange(batch.brains, dtype=np.uint32)
-    lib.ns_gpu_reset(gb, mask.ctypes.data_as(ct.POINTER(ct.c_uint8)), seeds.ctypes.data_as(ct.POINTER(ct.c_uint32)))
-    inp = np.ascontiguousarray(batch.inputs)
-    out = np.zeros((batch.brains, batch.outputs), np.float32)
-    st = np.zeros(batch.brains, np.int32)
-
-    def step():
-        rc = lib.ns_gpu_step(gb, inp.ctypes.data_as(f), mask.ctypes.data_as(ct.POINTER(ct.c_uint8)), 16,
-                             batch.gain, out.ctypes.data_as(f), st.ctypes.data_as(i32))
-        if rc:
-            raise RuntimeError(lib.ns_error().decode())
-    for _ in range(max(args.warmup, 3)):
-        step()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
-    steps = max(3, min(args.steps, 20))
-    t0 = time.perf_counter()
-    e0.record()
-    for _ in range(steps):
-        step()
-    e1.record(); torch.cuda.synchronize()
-    wall = time.perf_counter() - t0
-    ms = e0.elapsed_time(e1) / steps
     N = len(batch.neuron_rows)
-    value = N * 16 / (ms / 1e3)
-    line = {"impl": "reference-cuda", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps,
-            "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (Philox4x32-10 seed 2)",
-            "config": {"workload": ("batched_uneven_full_pools" if batch.brains == 32768 else batch.name),
-                       "brains": batch.brains, "neurons": N,
-                       "synapses": len(batch.synapse_rows), "ticks_per_step": 16,
-                       "delays_ms": "1-16 folded into 1-8 (reference ABI limit)",
-                       "kernel": "gym_adapter/gpu.cu step_batch, 32 threads per brain, --fmad=false --prec-div=true --prec-sqrt=true, sm_100a",
-                       "ns_gpu_create_s": create_s},
-            "e2e": {"value": N * 16 * steps / wall, "unit": UNIT, "h2d_bytes_per_step": int(inp.nbytes + mask.nbytes),
-                    "d2h_bytes_per_step": int(out.nbytes + st.nbytes)}}
-    lib.ns_gpu_destroy(gb)
-    print(json.dumps(line), flush=True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if lib is None:
+        notes.append("oracle/_ref/libns_ref_gpu.so not built")
+    else:
+        f, i32 = ct.POINTER(ct.c_float), ct.POINTER(ct.c_int)
+        t_setup = time.perf_counter()
+        handles = []
+        for b in range(batch.brains):
+            ng, sg, mo = batch.brain(b)
+            sg = np.ascontiguousarray(sg.copy())
+            sg[:, 4] = (sg[:, 4] - 1) % 8 + 1
+            ng = np.ascontiguousarray(ng); mo = np.ascontiguousarray(mo, np.int32)
+            h = lib.ns_create(len(ng), len(sg), batch.channels, batch.outputs, ng.ctypes.data_as(f),
+                              sg.ctypes.data_as(f), mo.ctypes.data_as(i32))
+            if not h:
+                raise RuntimeError(lib.ns_error().decode())
+            handles.append(h)
+        arr = (ct.c_void_p * len(handles))(*handles)
+        t0 = time.perf_counter()
+        gb = lib.ns_gpu_create(arr, len(handles))
+        create_s = time.perf_counter() - t0
+        for h in handles:
+            lib.ns_destroy(h)
+        if not gb:
+            raise RuntimeError(lib.ns_error().decode())
+        mask = np.ones(batch.brains, np.uint8)
+        seeds = np.arange(batch.brains, dtype=np.uint32)
+        lib.ns_gpu_reset(gb, mask.ctypes.data_as(ct.POINTER(ct.c_uint8)),
+                         seeds.ctypes.data_as(ct.POINTER(ct.c_uint32)))
+        inp = np.ascontiguousarray(batch.inputs)
+        out = np.zeros((batch.brains, batch.outputs), np.float32)
+        st = np.zeros(batch.brains, np.int32)
 
-    # The world simulator's neural stage (src/main.cu) in both of its forms.
+        def step():
+            rc = lib.ns_gpu_step(gb, inp.ctypes.data_as(f), mask.ctypes.data_as(ct.POINTER(ct.c_uint8)), 16,
+                                 batch.gain, out.ctypes.data_as(f), st.ctypes.data_as(i32))
+            if rc:
+                raise RuntimeError(lib.ns_error().decode())
+        for _ in range(max(warmup, 3)):
+            step()
+        torch.cuda.synchronize()
+        with ClockSampler(gpu_index) as clk:
+            t0 = time.perf_counter()
+            e0.record()
+            for _ in range(steps):
+                step()
+            e1.record()
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+        ms = e0.elapsed_time(e1) / steps
+        lib.ns_gpu_destroy(gb)
+        forms["step_batch"] = {
+            "ms_per_step": ms, "value": N * 16 / (ms / 1e3), "e2e_value": N * 16 * steps / wall,
+            "kernel": "gym_adapter/gpu.cu step_batch, 32 threads per brain, --fmad=false --prec-div=true "
+                      "--prec-sqrt=true, sm_100a",
+            "h2d_bytes_per_step": int(inp.nbytes + mask.nbytes), "d2h_bytes_per_step": int(out.nbytes + st.nbytes),
+            "setup_s": time.perf_counter() - t_setup - wall, "ns_gpu_create_s": create_s, "steps": steps,
+            "clocks": clk.summary()}
     if batch.brains != 32768:
-        return
+        return forms, notes
     wlib = pyoracle.ref_world_lib()
     if wlib is None:
-        print(json.dumps({"impl": "reference-cuda-world", "unavailable": "oracle/_ref/libns_ref_world.so not built"}))
-        return
-    for mode, label in ((0, "fused global-slot kernels"), (1, "--block-brains tiers + global-slot fallback")):
+        notes.append("oracle/_ref/libns_ref_world.so not built")
+        return forms, notes
+    f, i32 = ct.POINTER(ct.c_float), ct.POINTER(ct.c_int)
+    for mode, key, label in ((0, "global_slot", "fused global-slot kernels"),
+                             (1, "block_tiers", "--block-brains tiers + global-slot fallback")):
         no = np.ascontiguousarray(batch.neuron_offsets, np.int64)
         so = np.ascontiguousarray(batch.synapse_offsets, np.int64)
         w = wlib.ref_world_create(batch.brains, no.ctypes.data_as(ct.POINTER(ct.c_int64)),
@@ -351,28 +362,55 @@ def run_reference_cuda(args, rank, world, local_rank):
                                   np.ascontiguousarray(batch.motors, np.int32).ctypes.data_as(i32),
                                   batch.outputs, 7, mode)
         if not w:
-            print(json.dumps({"impl": "reference-cuda-world", "unavailable": "pool setup failed"}))
+            notes.append(f"{key}: pool setup failed")
             continue
-        for _ in range(max(args.warmup, 3)):
+        for _ in range(max(warmup, 3)):
             assert wlib.ref_world_step(w) == 0
         wlib.ref_world_sync()
-        t0 = time.perf_counter()
-        e0.record()
-        for _ in range(steps):
-            assert wlib.ref_world_step(w) == 0
-        e1.record(); torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
+        with ClockSampler(gpu_index) as clk:
+            t0 = time.perf_counter()
+            e0.record()
+            for _ in range(steps):
+                assert wlib.ref_world_step(w) == 0
+            e1.record()
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
         ms = e0.elapsed_time(e1) / steps
         spikes = wlib.ref_world_total_spikes(w, N)
         wlib.ref_world_destroy(w)
-        line = dict(line)
-        line.update({"impl": "reference-cuda-world", "value": N * 16 / (ms / 1e3), "ms_per_step": ms,
-                     "config": dict(line["config"], kernel=f"src/main.cu neural stage, {label}, --use_fast_math, sm_100a",
-                                    total_spikes_after=spikes),
-                     "e2e": {"value": N * 16 * steps / wall, "unit": UNIT, "h2d_bytes_per_step": 0,
-                             "d2h_bytes_per_step": 16}})
-        line["config"].pop("ns_gpu_create_s", None)
+        forms[key] = {"ms_per_step": ms, "value": N * 16 / (ms / 1e3), "e2e_value": N * 16 * steps / wall,
+                      "kernel": f"src/main.cu neural stage, {label}, --use_fast_math, sm_100a",
+                      "total_spikes_after": int(spikes), "steps": steps, "clocks": clk.summary()}
+    return forms, notes
+
+
+def run_reference_cuda(args, rank, world, local_rank):
+    """The reference's own CUDA forms alone, one JSON line per form."""
+    if rank != 0:
+        return
+    import torch
+    torch.cuda.set_device(local_rank)
+    nsb = load_package()
+    batch = workload(nsb, 2, 1, args.workload if args.workload in ("batched_uneven", "plain_small") else "batched_uneven")
+    steps = max(3, min(args.steps, 20))
+    forms, notes = reference_cuda_forms(batch, steps, args.warmup, local_rank)
+    N = len(batch.neuron_rows)
+    for key, fm in forms.items():
+        line = {"impl": "reference-cuda" if key == "step_batch" else "reference-cuda-world", "metric": METRIC,
+                "value": fm["value"], "unit": UNIT, "n_gpus": 1, "steps": fm["steps"], "warmup": max(args.warmup, 3),
+                "ms_per_step": fm["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic (Philox4x32-10 seed 2)",
+                "config": {"workload": ("batched_uneven_full_pools" if batch.brains == 32768 else batch.name),
+                           "brains": batch.brains, "neurons": N, "synapses": len(batch.synapse_rows),
+                           "ticks_per_step": 16, "delays_ms": "1-16 folded into 1-8 (reference ABI limit)",
+                           "kernel": fm["kernel"]},
+                "e2e": {"value": fm["e2e_value"], "unit": UNIT,
+                        "h2d_bytes_per_step": fm.get("h2d_bytes_per_step", 0),
+                        "d2h_bytes_per_step": fm.get("d2h_bytes_per_step", 16)},
+                "clocks": fm["clocks"]}
         print(json.dumps(line), flush=True)
+    for n in notes:
+        print(json.dumps({"impl": "reference-cuda", "unavailable": n}), flush=True)
 
 
 def run_ours(args, rank, world, local_rank):
@@ -501,8 +539,27 @@ def run_ours(args, rank, world, local_rank):
             ref.close()
             line["cpu_baseline"] = {"value": nt / secs, "unit": UNIT, "cores": ref.processes, "kind": ref.kind,
                                     "sample": ref.sample + "; 2 timed steps after 1 warm-up"}
-        print(json.dumps(line), flush=True)
     gpu.close()
+    if rank == 0:
+        if (world == 1 and not args.no_reference_cuda and args.fraction == 1
+                and args.workload in ("batched_uneven", "plain_small")):
+            # The reference's own CUDA forms on the same batch and GPU, after
+            # this library's buffers are freed (none of its code runs there).
+            torch.cuda.synchronize()
+            forms, notes = reference_cuda_forms(batch, max(3, min(args.steps, 20)), args.warmup, local_rank)
+            rc = {k: {"ms_per_step": v["ms_per_step"], "value": v["value"], "e2e_value": v["e2e_value"],
+                      "kernel": v["kernel"], "steps": v["steps"], "clocks": v["clocks"]} for k, v in forms.items()}
+            if forms:
+                best = min(forms, key=lambda k: forms[k]["ms_per_step"])
+                rc["best_form"] = best
+                rc["best_ms_per_step"] = forms[best]["ms_per_step"]
+                rc["best_ratio"] = value / forms[best]["value"]
+                rc["best_e2e_ratio"] = e2e_value / max(v["e2e_value"] for v in forms.values())
+            rc["delays"] = "folded into 1-8 for the reference (its ABI accepts 1-8); cost per tick is delay-independent"
+            if notes:
+                rc["unavailable"] = notes
+            line["reference_cuda"] = rc
+        print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -941,6 +998,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-cuda"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip timing the reference's own CUDA forms on the same batch (N=1 only)")
     ap.add_argument("--fraction", type=int, default=1, choices=[1, 2, 4, 8, 16],
                     help="run a 1/D slice of the full pools (profiler captures only)")
     ap.add_argument("--workload", default="batched_uneven",

@@ -360,3 +360,127 @@ def protocols():
     out = np.zeros(40, np.float32)
     n = oracle_lib().or_protocols(_ptr(out, _f), 40)
     return out[:n]
+
+
+# ---- sampled stepping in worker processes (tests only) -------------------------
+def _step_brain_jobs(jobs, calls, ticks, gain, pulse):
+    """Steps each job's brain `calls` times from its reset in this process.
+    jobs: (index, neuron rows, synapse rows, motors, channels, max delay,
+    inputs, seed). Returns (index, outputs (calls x outputs), status (calls,),
+    neuron dump, synapse dump, tick) per job."""
+    out = []
+    for idx, ng, sg, mo, channels, max_delay, inputs, seed in jobs:
+        o = OracleBrain(ng, sg, mo, channels, max_delay)
+        if pulse is not None:
+            o.set_pulse(*pulse)
+        o.reset(int(seed))
+        outs = np.zeros((calls, len(mo)), np.float32)
+        status = np.zeros(calls, np.int32)
+        for c in range(calls):
+            rc, oo, _ = o.step(inputs, ticks, gain, stop_on_nonfinite=False)
+            outs[c] = oo
+            status[c] = rc
+        nw, sw, t = o.dump()
+        o.close()
+        out.append((idx, outs, status, nw, sw, t))
+    return out
+
+
+class SampledOracle:
+    """The oracle stepping a sample of a batch's brains, split across worker
+    processes (spawn start method, so the workers hold no CUDA state). Start it
+    before the GPU run and collect with result(): the two then overlap."""
+
+    def __init__(self, batch, indices, seeds, calls, ticks=16, gain=None, pulse=None, processes=None):
+        import concurrent.futures as cf
+        import multiprocessing as mp
+        import os
+        gain = batch.gain if gain is None else gain
+        jobs = []
+        for i in indices:
+            ng, sg, mo = batch.brain(int(i))
+            jobs.append((int(i), ng, sg, mo, batch.channels, batch.max_delay, batch.inputs[int(i)],
+                         int(seeds[int(i)])))
+        # largest brains first, dealt round-robin, so the workers finish together
+        jobs.sort(key=lambda j: -len(j[1]))
+        self.processes = max(1, min(processes or os.cpu_count() or 1, len(jobs)))
+        parts = [jobs[k::self.processes] for k in range(self.processes)]
+        self.pool = cf.ProcessPoolExecutor(self.processes, mp_context=mp.get_context("spawn"))
+        self.futures = [self.pool.submit(_step_brain_jobs, p, calls, ticks, gain, pulse) for p in parts]
+
+    def result(self):
+        """{index: (outputs, status, neuron dump, synapse dump, tick)}."""
+        res = {}
+        try:
+            for f in self.futures:
+                for idx, outs, status, nw, sw, t in f.result():
+                    res[idx] = (outs, status, nw, sw, t)
+        finally:
+            self.pool.shutdown()
+        return res
+
+
+def _host_package():
+    """The product's Python package loaded by path in a worker process, for
+    its host-side pool records (WorldPools) only; nothing here touches a GPU."""
+    import importlib.util
+    import sys
+    name = "neural_selection_b200"
+    if name not in sys.modules:
+        pkg = HERE.parent / "neural-selection_b200"
+        spec = importlib.util.spec_from_file_location(name, pkg / "__init__.py",
+                                                      submodule_search_locations=[str(pkg)])
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
+def _world_subset_run(fields_, subset, steps, senses_seed):
+    """The oracle's world stage over `steps` world steps for the animals in
+    `subset` only (every other animal marked not alive, so it is skipped): the
+    senses of every step are drawn from `senses_seed` for the whole
+    population, ages advance for living animals, homeostasis after each step.
+    fields_: the WorldPools fields as a dict. Returns the motor counts of every
+    step (steps x animals x 5) and the final pools as a dict."""
+    pools = _host_package().world.WorldPools(**fields_)
+    alive = pools.animals["alive"].copy()
+    keep = np.zeros(len(alive), bool)
+    keep[np.asarray(subset, np.int64)] = True
+    pools.animals["alive"][~keep & (alive == 1)] = 0
+    rng = np.random.default_rng(senses_seed)
+    motors = np.zeros((steps,) + pools.motors.shape, np.int32)
+    for step in range(1, steps + 1):
+        pools.senses[:] = rng.random(pools.senses.shape).astype(np.float32)
+        pools.motors[:] = 0
+        world_step(pools, step)
+        motors[step - 1] = pools.motors
+        pools.animals["age"][pools.animals["alive"] == 1] += 1
+        world_homeostasis(pools)
+    pools.animals["alive"][:] = alive
+    return motors, dict(pools.__dict__)
+
+
+class SubsetWorldOracle:
+    """The oracle's world stage on disjoint subsets of a population's animals
+    in worker processes (spawn). Animals do not interact within the neural
+    stage, so each subset's pools evolve exactly as in a run of the whole
+    population."""
+
+    def __init__(self, pools, steps, senses_seed, processes=None):
+        import concurrent.futures as cf
+        import multiprocessing as mp
+        import os
+        live = np.nonzero(pools.animals["alive"] == 1)[0]
+        self.processes = max(1, min(processes or os.cpu_count() or 1, len(live)))
+        self.subsets = [live[k::self.processes] for k in range(self.processes)]
+        fields_ = dict(pools.__dict__)
+        self.pool = cf.ProcessPoolExecutor(self.processes, mp_context=mp.get_context("spawn"))
+        self.futures = [self.pool.submit(_world_subset_run, fields_, s, steps, senses_seed) for s in self.subsets]
+
+    def result(self):
+        """[(subset, motors per step, final pool fields)] per worker."""
+        try:
+            return [(s, *f.result()) for s, f in zip(self.subsets, self.futures)]
+        finally:
+            self.pool.shutdown()
