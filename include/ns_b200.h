@@ -98,7 +98,10 @@ int nsb_gpu_step_device(void *batch, const float *d_input, const uint8_t *d_mask
  * array (4 MiB + 256 B, held by every GPU that loads the library until exit)
  * instead of library-allocated buffers. Rejects batches above 2,097,152
  * synapses. The first call on a device sets up the array's address (make it
- * before any stream capture); calls that overlap on the GPU race. */
+ * before any stream capture); the address is kept for the life of the
+ * process, so the device's context must live as long (no cudaDeviceReset
+ * between calls). Calls that overlap on the GPU race. Synaptic arrivals are
+ * counted as in the other steps. */
 int nsb_gpu_step_noalloc(void *batch, const float *d_input, const uint8_t *d_mask, int ticks, float gain,
                          float *d_output, int *d_status, void *stream);
 /* Step on the batch's own device buffers, replayed from a captured CUDA graph. */

@@ -114,13 +114,41 @@ __device__ __forceinline__ float release_event(uint32_t *sstate, const uint32_t 
     return rel;
 }
 
-// Delivery for one postsynaptic neuron at local tick t: arrival test,
-// stochastic release and per-branch accumulation in ascending edge order.
+// One tick's synaptic input of a postsynaptic neuron.
 struct Delivered {
     float e0, e1, e2, e3, inh;
     uint32_t mod;
     int narr;
 };
+
+// Fixed points of the input-free tick. A tick integrates a neuron from the
+// words below (voltage, adaptation, afterdepolarisation, inhibitory and
+// dendritic conductances, depolarisation trace) plus its input; the spike
+// word is written, never read, and a neuron without an input channel draws no
+// receptor events. So when a tick without input (no applied current, every
+// branch sum and the inhibitory sum exactly +0) leaves these words bit for
+// bit as they were and emits no spike, every later tick without input leaves
+// them unchanged too, and is skipped until an input arrives. The results are
+// those of integrating every tick; non-finite voltages and the LP, Prinz and
+// LFS cells, whose state lives elsewhere, are never treated as fixed.
+__device__ __forceinline__ bool no_input(uint32_t flags, const Delivered &d) {
+    return !(flags & NF_HAS_INPUT) &&
+           (__float_as_uint(d.e0) | __float_as_uint(d.e1) | __float_as_uint(d.e2) | __float_as_uint(d.e3) |
+            __float_as_uint(d.inh)) == 0u;
+}
+// Does the integrated state s leave the neuron record r (not yet overwritten)
+// as it was, with no spike and a finite voltage?
+__device__ __forceinline__ bool unchanged(const uint32_t *r, const NeuronRegs &s) {
+    const uint4 *q = reinterpret_cast<const uint4 *>(r);
+    const uint4 a = q[0], b = q[1], c = q[2];
+    return ((a.x ^ __float_as_uint(s.v)) | (a.y ^ __float_as_uint(s.w)) | (a.z ^ __float_as_uint(s.adp)) |
+            (a.w ^ __float_as_uint(s.inh)) | (b.x ^ __float_as_uint(s.depol)) | (c.x ^ __float_as_uint(s.d0)) |
+            (c.y ^ __float_as_uint(s.d1)) | (c.z ^ __float_as_uint(s.d2)) | (c.w ^ __float_as_uint(s.d3))) == 0u &&
+           s.spike == 0u && isfinite(s.v);
+}
+
+// Delivery for one postsynaptic neuron at local tick t: arrival test,
+// stochastic release and per-branch accumulation in ascending edge order.
 __device__ __forceinline__ Delivered deliver(const Pools &P, int ib, int ie, int e0, const uint32_t *meta,
                                              const uint32_t *hist, int t, int64_t tick0, float ampa,
                                              const float *tab) {
@@ -313,6 +341,7 @@ __global__ void __launch_bounds__(256, HEAVY ? 1 : NSB_MIN_CTAS) tick_kernel(Poo
     int *s_bid = s_mask + kMaxUnitBrains;                                 // caller brain index
     int *s_ev = s_bid + kMaxUnitBrains;                                   // 8 warps x kEvCap event synapses
     uint32_t *s_evv = reinterpret_cast<uint32_t *>(s_ev + 8 * kEvCap);    // 8 warps x kEvCap tick / value
+    float *s_heavy = reinterpret_cast<float *>(s_evv + 8 * kEvCap);       // 8 warps x kHeavyWarpScratch
     __shared__ int s_unit;
     __shared__ unsigned long long s_events;
 
@@ -374,6 +403,7 @@ __global__ void __launch_bounds__(256, HEAVY ? 1 : NSB_MIN_CTAS) tick_kernel(Poo
             if (has) cnt[j] = 0;
         }
         __syncthreads();
+        uint32_t fixed = 0;   // bit sl0: this thread's neuron of slot sl0 is at a fixed point (see unchanged)
         for (int t = 0; t < ticks; ++t) {
             for (int sl0 = 0; sl0 < slots; ++sl0) {
                 const int j = sl0 * bs + tid;
@@ -398,27 +428,84 @@ __global__ void __launch_bounds__(256, HEAVY ? 1 : NSB_MIN_CTAS) tick_kernel(Poo
                                      s_ev + warp * kEvCap, s_evv + warp * kEvCap, lane);
                 else if (dlv)
                     d = deliver(P, ib, ie, e0, meta, hist, t, tick0, ampa, tab);
+                uint32_t *r = P.nstate + (size_t)n * S_WORDS;
+                const uint32_t type = flags & NF_TYPE_MASK;
+                const uint32_t bit = sl0 < 32 ? 1u << sl0 : 0u;
+                uint32_t mod = d.mod;
+                float depol = 0.0f;
+                // HEAVY: an LP or Prinz cell whose model runs on the whole warp
+                bool pending = false;
+                NeuronRegs s;
+                float log_ampa = 0.0f, ext = 0.0f;
+                uint32_t hw0 = 0;
+                int xidx = 0;
                 if (run) {
-                    uint32_t *r = P.nstate + (size_t)n * S_WORDS;
-                    NeuronRegs s;
-                    float log_ampa;
-                    uint32_t hw0;
-                    load_neuron(r, s, log_ampa, hw0);
-                    if (flags & NF_ACTIVE) {
-                        const float level =
-                            (flags & NF_HAS_INPUT) ? input[(size_t)s_bid[bi] * P.channels + P.nsens[n]] : 0.0f;
-                        integrate<HEAVY>(P, n, flags, d, level, gain, s, status + s_bid[bi], tab);
-                    } else {
-                        s.spike = 0;
-                    }
-                    // the record's spare word keeps the call's AMPA scale
-                    store_neuron(r, s, log_ampa, hw0, r[S_PAD]);
-                    spike = s.spike;
-                    uint32_t mod = d.mod;
+                    const bool quiet = no_input(flags, d) && !(HEAVY && (type == 2 || type == 3 || type == 6));
                     if (P.pulse_period > 0 && (tick0 + t) % P.pulse_period == 0) mod |= P.pulse_mod;
+                    const bool plast = (flags & NF_PLASTIC_IN) && (mod || d.narr);
+                    if (quiet && (fixed & bit)) {
+                        // a fixed point without input: the record stays as it is
+                        depol = plast ? __uint_as_float(r[S_DEPOL]) : 0.0f;
+                    } else {
+                        load_neuron(r, s, log_ampa, hw0);
+                        if (flags & NF_ACTIVE) {
+                            const float level =
+                                (flags & NF_HAS_INPUT) ? input[(size_t)s_bid[bi] * P.channels + P.nsens[n]] : 0.0f;
+                            if (HEAVY && (type == 2 || type == 3)) {
+                                const float *g = reinterpret_cast<const float *>(P.ngene + (size_t)n * 4);
+                                const float cur = (flags & NF_HAS_INPUT) ? gain * level : 0.0f;
+                                ext = heavy_pre(g, type, s, cur, d.e0, d.e1, d.e2, d.e3, d.inh);
+                                xidx = P.nxidx[n];
+                                pending = true;
+                            } else {
+                                integrate<HEAVY>(P, n, flags, d, level, gain, s, status + s_bid[bi], tab);
+                            }
+                        } else {
+                            s.spike = 0;
+                        }
+                        if (!pending) {
+                            fixed = quiet && unchanged(r, s) ? fixed | bit : fixed & ~bit;
+                            // the record's spare word keeps the call's AMPA scale
+                            store_neuron(r, s, log_ampa, hw0, r[S_PAD]);
+                            spike = s.spike;
+                            depol = s.depol;
+                        }
+                    }
+                }
+                if (HEAVY) {
+                    // The warp's LP and Prinz cells, one after another, each on all 32 lanes.
+                    float axon_before = 0.0f;
+                    bool spiked = false;
+                    for (uint32_t pm = __ballot_sync(0xffffffffu, pending); pm; pm &= pm - 1u) {
+                        const int L = __ffs(pm) - 1;
+                        const int xi = __shfl_sync(0xffffffffu, xidx, L);
+                        const uint32_t ty = __shfl_sync(0xffffffffu, type, L);
+                        const float ex = __shfl_sync(0xffffffffu, ext, L);
+                        float *x = P.xstate + (size_t)xi * 16;
+                        const float *xg = P.xgene + (size_t)xi * 16;
+                        if (ty == 2) {
+                            const float ab = x[0];
+                            lp_integrate_warp(x, ex / 1000.0f, xg, s_heavy + warp * kHeavyWarpScratch, lane, tab);
+                            if (lane == L) axon_before = ab;
+                        } else {
+                            const bool sp = prinz_tick_warp(x, xg, ex, xg[8] + 0.0f, -68.0f,
+                                                            s_heavy + warp * kHeavyWarpScratch, lane, tab);
+                            if (lane == L) spiked = sp;
+                        }
+                    }
+                    if (pending) {
+                        heavy_post(type, s, P.xstate + (size_t)xidx * 16, axon_before, spiked);
+                        if (!isfinite(s.v)) status[s_bid[bi]] = -1;
+                        fixed &= ~bit;
+                        store_neuron(r, s, log_ampa, hw0, r[S_PAD]);
+                        spike = s.spike;
+                        depol = s.depol;
+                    }
+                }
+                if (run) {
                     if ((flags & NF_PLASTIC_IN) && (spike || mod || d.narr))
                         plasticity_events(P.sstate, P.sgene, P.slastp, P.hw, ib, ie, e0, meta, hist, t, tick0,
-                                          spike != 0, mod, s.depol, tab);
+                                          spike != 0, mod, depol, tab);
                     cnt[j] += (int)spike;
                     my_events += d.narr;
                 }
@@ -559,6 +646,7 @@ __global__ void __launch_bounds__(256, NSB_MIN_CTAS) tick_kernel_cluster(Pools P
             if (has) cnt[j - lo] = 0;
         }
         cluster.sync();
+        uint32_t fixed = 0;   // bit sl0: this thread's neuron of slot sl0 is at a fixed point (see unchanged)
         for (int t = 0; t < ticks; ++t) {
             for (int sl0 = 0; sl0 < slots; ++sl0) {
                 const int j = lo + sl0 * bs + tid;
@@ -582,24 +670,34 @@ __global__ void __launch_bounds__(256, NSB_MIN_CTAS) tick_kernel_cluster(Pools P
                     d = deliver(P, ib, ie, e0, meta, hist, t, tick0, ampa, tab);
                 if (has) {
                     uint32_t *r = P.nstate + (size_t)n * S_WORDS;
-                    NeuronRegs s;
-                    float log_ampa;
-                    uint32_t hw0;
-                    load_neuron(r, s, log_ampa, hw0);
-                    if (flags & NF_ACTIVE) {
-                        const float level =
-                            (flags & NF_HAS_INPUT) ? input[(size_t)b * P.channels + P.nsens[n]] : 0.0f;
-                        integrate<false>(P, n, flags, d, level, gain, s, status + b, tab);
-                    } else {
-                        s.spike = 0;
-                    }
-                    store_neuron(r, s, log_ampa, hw0, r[S_PAD]);
-                    spike = s.spike;
+                    const bool quiet = no_input(flags, d);
+                    const uint32_t bit = sl0 < 32 ? 1u << sl0 : 0u;
                     uint32_t mod = d.mod;
                     if (P.pulse_period > 0 && (tick0 + t) % P.pulse_period == 0) mod |= P.pulse_mod;
+                    const bool plast = (flags & NF_PLASTIC_IN) && (mod || d.narr);
+                    float depol;
+                    if (quiet && (fixed & bit)) {
+                        depol = plast ? __uint_as_float(r[S_DEPOL]) : 0.0f;
+                    } else {
+                        NeuronRegs s;
+                        float log_ampa;
+                        uint32_t hw0;
+                        load_neuron(r, s, log_ampa, hw0);
+                        if (flags & NF_ACTIVE) {
+                            const float level =
+                                (flags & NF_HAS_INPUT) ? input[(size_t)b * P.channels + P.nsens[n]] : 0.0f;
+                            integrate<false>(P, n, flags, d, level, gain, s, status + b, tab);
+                        } else {
+                            s.spike = 0;
+                        }
+                        fixed = quiet && unchanged(r, s) ? fixed | bit : fixed & ~bit;
+                        store_neuron(r, s, log_ampa, hw0, r[S_PAD]);
+                        spike = s.spike;
+                        depol = s.depol;
+                    }
                     if ((flags & NF_PLASTIC_IN) && (spike || mod || d.narr))
                         plasticity_events(P.sstate, P.sgene, P.slastp, P.hw, ib, ie, e0, meta, hist, t, tick0,
-                                          spike != 0, mod, s.depol, tab);
+                                          spike != 0, mod, depol, tab);
                     cnt[j - lo] += (int)spike;
                     my_events += d.narr;
                 }
@@ -708,7 +806,8 @@ int spike_words(int max_unit_neurons, int block) {
 }
 
 int tick_smem_bytes(int hw) {
-    return 1024 + (kMetaCap + 32 * hw * 2) * 4 + kMaxUnitBrains * 8 + 2 * kMaxUnitBrains * 4 + 8 * kEvCap * 8;
+    return 1024 + (kMetaCap + 32 * hw * 2) * 4 + kMaxUnitBrains * 8 + 2 * kMaxUnitBrains * 4 + 8 * kEvCap * 8 +
+           8 * kHeavyWarpScratch * 4;
 }
 
 // The kernels' dynamic shared memory limit is a process-wide attribute: it is
@@ -1256,7 +1355,9 @@ constexpr size_t kNoAllocScratchBytes = 256 + sizeof(int16_t) * (size_t)kNoAlloc
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 // Device address of g_noalloc_scratch on the current device, looked up once
-// per device (the host-side name is only a stand-in for the device array).
+// per device and kept for the life of the process (the host-side name is only
+// a stand-in for the device array). The cache assumes the device's primary
+// context lives as long: after a cudaDeviceReset the address would be stale.
 static unsigned char *noalloc_scratch_address() {
     static std::mutex lock;
     static unsigned char *addr[64] = {};
@@ -1290,7 +1391,8 @@ void Engine::step_noalloc(const float *d_input, const uint8_t *d_mask, int ticks
     // to 0 by launch_groups.
     // (launch_groups clears its eight queue counters at the start of the array.)
     NSB_CHECK(cudaMemsetAsync(lastp, 0xff, sizeof(int16_t) * (size_t)std::max(n_synapses_, 1), s));
-    Pools P = pools(false);
+    // Arrivals are counted into the engine's existing counter (no allocation).
+    Pools P = pools(count_events_);
     P.slastp = lastp;
     launch_groups(P, queue, d_input, d_mask, ticks, gain, d_output, d_status, s);
 }

@@ -278,6 +278,265 @@ static __device__ __noinline__ NeuronRegs heavy_tick(const float *g, uint32_t ty
     return s;
 }
 
+// ---- LP and Prinz cells on a whole warp ------------------------------------------
+// The same arithmetic as lp_integrate and pz_substep, spread over the 32 lanes
+// of a warp: every exponential (and the one logarithm) of a derivative
+// evaluation is computed by its own lane from the same operands in the same
+// order, and each state component is then assembled by one lane exactly as
+// the one-thread code assembles it. Each value is produced by the same binary32
+// operations as there, so the results are identical bit for bit; the latency
+// of an evaluation drops from some twenty dependent exponentials to one or
+// two. All 32 lanes call these functions together (converged); w is the
+// warp's 48-float shared-memory scratch.
+constexpr int kHeavyWarpScratch = 48;
+
+// lp_rates on the state y (w[0..15]) for lanes 0..15: returns d[lane].
+__device__ __forceinline__ float lp_rate_warp(const float *y, float i_na, const float *sc, float *T, int lane,
+                                              const float *tab) {
+    const float va = y[0], vs = y[15], cai = y[13];
+    float t = 0.0f;
+    switch (lane) {   // the transcendental terms, one per lane
+    case 0: t = crexp(vs / 11.4866f, tab); break;
+    case 1: t = lp_sig(vs, 55.0f, -15.0f, tab); break;
+    case 2: t = crexp(-13.0f - va / 4.0f, tab); break;
+    case 3: t = crexp(va / 5.0f + 5.0f, tab); break;
+    case 4: t = crexp(-2.66666666667f - va / 18.0f, tab); break;
+    case 5: t = crexp(-5.0f - va / 5.0f, tab); break;
+    case 6: t = crexp(-10.0f - va / 5.0f, tab); break;
+    case 7: t = crexp(-1.375f - va / 40.0f, tab); break;
+    case 8: t = lp_sig(vs, 15.0f, -9.8f, tab); break;
+    case 9: t = lp_sig(vs, -40.0f, 3.2f, tab); break;
+    case 10: t = lp_sig(vs, -15.0f, -10.0f, tab); break;
+    case 11: t = lp_sig(vs, 29.1336f, -4.43083f, tab); break;
+    case 12: t = lp_sig(vs, -.6f * cai, -23.0f, tab); break;
+    case 13: t = lp_sig(vs, -16.0f - .6f * cai, -5.0f, tab); break;
+    case 14: t = lp_sig(vs, -12.0f, -26.0f, tab); break;
+    case 15: t = lp_sig(vs, -62.0f, 6.0f, tab); break;
+    case 16: t = lp_sig(vs, -40.0f, -12.0f, tab); break;
+    case 17: t = lp_sig(vs, -70.0f, 8.0f, tab); break;
+    case 18: t = lp_sig(vs, -110.0f, -21.6f, tab); break;
+    case 19: t = lp_sig(va, -26.9916223f, -5.957441281f, tab); break;
+    case 20: t = lp_sig(va, -60.57875745f, -13.25674673f, tab); break;
+    default: break;
+    }
+    T[lane] = t;
+    __syncwarp();
+    const float *x = y;
+    float d = 0.0f, a, b;
+    switch (lane) {   // the derivative components, one per lane
+    case 0: {
+        const float na = x[1] * x[1] * x[1] * x[2] * 7.15f * (va - 50.0f);
+        const float kd = x[8] * x[8] * x[8] * x[8] * 1.43f * (va + 72.0f);
+        const float km = .2613041227f * x[14] * (va + 80.0f);
+        const float aleak = sc[3] * .001004288227f * (va + 50.0f);
+        const float cpl = .004017089073f * (vs - va);
+        d = (-na - kd - km - aleak + cpl) / .1148312178f;
+        break;
+    }
+    case 13:
+    case 15: {
+        const float ev = T[0];
+        const float ghk = fabsf(vs) < .001f ? 11.4866f * (x[13] - 15123.5f) : vs * (x[13] * ev - 15123.5f) / (ev - 1.0f);
+        const float ca = sc[0] * (x[3] * x[4] * .1247796343f + x[5] * .07142141077f) * .00155982f * ghk * .9f;
+        if (lane == 13) {
+            d = -.05049639866f * ca - .01729930764f * (cai - .02f);
+        } else {
+            const float cpl = .004017089073f * (vs - va);
+            const float kca = sc[1] * x[6] * x[7] * 1.663612026f * (vs + 72.0f) * .9f;
+            const float amix = T[1];
+            const float ka = x[9] * x[9] * x[9] * .8008791415f * (vs + 72.0f) * (amix * x[10] + (1.0f - amix) * x[11]) * .9f;
+            const float ih = sc[2] * x[12] * .0126874385f * (vs + 20.0f) * .9f;
+            const float sleak = sc[3] * .0006901584324f * (vs + 50.0f);
+            d = (-ca - kca - ka - ih - sleak - cpl + (i_na - 2.0f) * .01222505828f) / .0543909161f;
+        }
+        break;
+    }
+    case 1:
+        a = lp_ratio(-16.64f - .32f * va, T[2] - 1.0f, 1.28f);
+        b = lp_ratio(.28f * va + 7.0f, T[3] - 1.0f, 1.4f);
+        d = a * (1.0f - x[1]) - b * x[1];
+        break;
+    case 2:
+        a = .128f * T[4];
+        b = 4.0f / (T[5] + 1.0f);
+        d = a * (1.0f - x[2]) - b * x[2];
+        break;
+    case 8:
+        a = lp_ratio(-1.6f - .032f * va, T[6] - 1.0f, .16f);
+        b = .5f * T[7];
+        d = a * (1.0f - x[8]) - b * x[8];
+        break;
+    case 3: d = (T[8] - x[3]) * .045f; break;
+    case 4: d = (T[9] - x[4]) * .02f * T[10]; break;
+    case 5: d = (T[11] - x[5]) * .0608644f; break;
+    case 6: d = (T[12] * T[13] * cai / (2.5f + cai) - x[6]) * .6f; break;
+    case 7: d = (.7f / (.6f + cai) - x[7]) * .035f; break;
+    case 9: d = (T[14] - x[9]) * .14f; break;
+    case 10: d = (T[15] - x[10]) * .05f; break;
+    case 11: d = (T[15] - x[11]) * .0036f * T[16]; break;
+    case 12: d = (T[17] - x[12]) * .00033f / T[18]; break;
+    case 14: d = (T[19] - x[14]) * .0001386796618f * T[20]; break;
+    default: break;
+    }
+    __syncwarp();
+    return d;
+}
+
+// lp_integrate on x (16 floats, any memory the warp can read and write).
+static __device__ __noinline__ void lp_integrate_warp(float *x, float i_na, const float *sc, float *w, int lane,
+                                               const float *tab) {
+    const float dt = .05f;
+    float *y = w, *T = w + 16;
+    const float xj0 = lane < 16 ? x[lane] : 0.0f;
+    float xj = xj0;
+    if (lane < 16) y[lane] = xj;
+    __syncwarp();
+    for (int step = 0; step < 20; ++step) {
+        const float k1 = lp_rate_warp(y, i_na, sc, T, lane, tab);
+        if (lane < 16) y[lane] = xj + .5f * dt * k1;
+        __syncwarp();
+        const float k2 = lp_rate_warp(y, i_na, sc, T, lane, tab);
+        if (lane < 16) y[lane] = xj + .5f * dt * k2;
+        __syncwarp();
+        const float k3 = lp_rate_warp(y, i_na, sc, T, lane, tab);
+        if (lane < 16) y[lane] = xj + dt * k3;
+        __syncwarp();
+        const float k4 = lp_rate_warp(y, i_na, sc, T, lane, tab);
+        xj += dt * (k1 + 2 * k2 + 2 * k3 + k4) / 6.0f;
+        if (lane < 16) y[lane] = xj;
+        __syncwarp();
+    }
+    if (lane < 16) x[lane] = xj;
+    __syncwarp();
+}
+
+// One pz_substep on u (w[0..12]: v, ca, m[7], h[4]); returns nothing, u is
+// updated in place. T = w + 16 holds the lanes' transcendental terms.
+__device__ __forceinline__ void pz_substep_warp(float *u, const float *g, float ext, float clamp_ns, float clamp_rev,
+                                                float *T, int lane, const float *tab) {
+    const float dt = .025f;
+    const float *m = u + 2, *h = u + 9;
+    const float v = u[0], ca = fmaxf(u[1], 0.000001f);
+    float t = 0.0f;
+    switch (lane) {
+    case 0: t = nsx::logf_cr(3000.0f / ca); break;
+    case 1: t = pz_gate(v, 25.5f, -5.29f, tab); break;
+    case 2: t = pz_gate(v, 27.1f, -7.2f, tab); break;
+    case 3: t = pz_gate(v, 33, -8.1f, tab); break;
+    case 4: t = pz_gate(v, 27.2f, -8.7f, tab); break;
+    case 5: t = (ca / (ca + 3)) * pz_gate(v, 28.3f, -12.6f, tab); break;
+    case 6: t = pz_gate(v, 12.3f, -11.8f, tab); break;
+    case 7: t = pz_gate(v, 75, 5.5f, tab); break;
+    case 8: t = 2.64f - 2.52f * pz_gate(v, 120, -25, tab); break;
+    case 9: t = 43.4f - 42.6f * pz_gate(v, 68.1f, -20.5f, tab); break;
+    case 10: t = crexp((v + 27) / 10, tab); break;
+    case 11: t = crexp((v + 70) / -13, tab); break;
+    case 12: t = 23.2f - 20.8f * pz_gate(v, 32.9f, -15.2f, tab); break;
+    case 13: t = 180.6f - 150.2f * pz_gate(v, 46, -22.7f, tab); break;
+    case 14: t = 14.4f - 12.8f * pz_gate(v, 28.3f, -19.2f, tab); break;
+    case 15: t = crexp(-14.59f - .086f * v, tab); break;
+    case 16: t = crexp(-1.87f + .0701f * v, tab); break;
+    case 17: t = pz_gate(v, 48.9f, 5.18f, tab); break;
+    case 18: t = pz_gate(v, 32.1f, 5.5f, tab); break;
+    case 19: t = pz_gate(v, 60, 6.2f, tab); break;
+    case 20: t = pz_gate(v, 56.9f, 4.9f, tab); break;
+    case 21: t = crexp((v + 62.9f) / -10, tab); break;
+    case 22: t = crexp((v + 34.9f) / 3.6f, tab); break;
+    case 23: t = 210 - 179.6f * pz_gate(v, 55, -16.9f, tab); break;
+    case 24: t = crexp((v + 55) / 9, tab); break;
+    case 25: t = crexp((v + 65) / -16, tab); break;
+    case 26: t = 77.2f - 58.4f * pz_gate(v, 38.9f, -26.5f, tab); break;
+    default: break;
+    }
+    T[lane] = t;
+    __syncwarp();
+    float nv = 0.0f, nca = 0.0f;
+    if (lane == 0) {
+        const float eca = (8.31451e3f * 283.0f / (2.0f * 96485.3415f)) * T[0];
+        const float c[8] = {g[0] * m[0] * m[0] * m[0] * h[0], g[1] * m[1] * m[1] * m[1] * h[1],
+                            g[2] * m[2] * m[2] * m[2] * h[2], g[3] * m[3] * m[3] * m[3] * h[3],
+                            g[4] * m[4] * m[4] * m[4] * m[4], g[5] * m[5] * m[5] * m[5] * m[5],
+                            g[6] * m[6], g[7]};
+        const float rev[8] = {50, eca, eca, -80, -80, -80, -20, -50};
+        float gt = clamp_ns, ws = ext + clamp_ns * clamp_rev;
+        for (int i = 0; i < 8; ++i) { gt += c[i]; ws += c[i] * rev[i]; }
+        if (fabsf(gt) < .000001f) nv = v + dt * ws / 628.3f;
+        else { const float tg = ws / gt; nv = tg + (v - tg) * crexp(-dt * gt / 628.3f, tab); }
+        const float ica = (c[1] + c[2]) * (v - eca) / 1000000.0f;
+        const float cat = .05f - 14961.0f * ica;
+        nca = fmaxf(.000001f, cat + (ca - cat) * c_K.prinz_ca);
+    } else if (lane >= 2 && lane < 9) {
+        const int i = lane - 2;
+        const float mi = T[1 + i];
+        float mt;
+        if (i == 2) mt = 2.8f + 14 * (1.0f / (T[10] + T[11]));
+        else if (i == 6) mt = 2.0f / (T[15] + T[16]);
+        else mt = T[i < 2 ? 8 + i : 9 + i];
+        nv = mi + (m[i] - mi) * crexp(-dt / mt, tab);
+    } else if (lane >= 9 && lane < 13) {
+        const int i = lane - 9;
+        const float hi = T[17 + i];
+        float ht;
+        if (i == 0) ht = (1.34f / (1 + T[21])) * (1.5f + 1 / (1 + T[22]));
+        else if (i == 2) ht = 120 + 300 * (1.0f / (T[24] + T[25]));
+        else ht = T[i == 1 ? 23 : 26];
+        nv = hi + (h[i] - hi) * crexp(-dt / ht, tab);
+    }
+    __syncwarp();
+    if (lane == 0) { u[0] = nv; u[1] = nca; }
+    else if (lane >= 2 && lane < 13) u[lane] = nv;
+    __syncwarp();
+}
+
+// The Prinz cell's 40 substeps of one tick on x (13 state floats); returns
+// whether the voltage crossed 0 mV upwards in any substep (all lanes).
+static __device__ __noinline__ bool prinz_tick_warp(float *x, const float *xg, float ext, float clamp_ns,
+                                             float clamp_rev, float *w, int lane, const float *tab) {
+    float *u = w, *T = w + 16;
+    if (lane < 13) u[lane] = x[lane];
+    __syncwarp();
+    bool spiked = false;
+    for (int i = 0; i < 40; ++i) {
+        const float before = u[0];
+        pz_substep_warp(u, xg, ext, clamp_ns, clamp_rev, T, lane, tab);
+        spiked |= before < 0 && u[0] >= 0;
+    }
+    if (lane < 13) x[lane] = u[lane];
+    __syncwarp();
+    return spiked;
+}
+
+// heavy_tick in three parts for the warp form: heavy_pre and heavy_post run
+// on the cell's own lane, the cell model in between on the whole warp.
+// heavy_pre returns the external current the cell model receives (the LP
+// cell's is divided by 1000 there, as in heavy_tick).
+__device__ __forceinline__ float heavy_pre(const float *g, uint32_t type, NeuronRegs &s, float cur, float e0,
+                                           float e1, float e2, float e3, float inh_in) {
+    const float clamp_leak = 0.0f, clamp_rev = -68.0f;
+    s.d0 += e0; s.d1 += e1; s.d2 += e2; s.d3 += e3;
+    float sub = fmaxf(0.0f, fminf(s.v, -50.0f) - g[G_EL]);
+    s.depol += 0.1f * (sub - s.depol);
+    s.inh += inh_in;
+    s.spike = 0;
+    float exc = 0;
+    exc += s.d0; exc += s.d1; exc += s.d2; exc += s.d3;
+    if (type == 2) return cur + exc * (0.0f - s.v) + s.inh * (-75.0f - s.v) - clamp_leak * (s.v - clamp_rev);
+    return cur + exc * (0.0f - s.v) + s.inh * (-75.0f - s.v);
+}
+__device__ __forceinline__ void heavy_post(uint32_t type, NeuronRegs &s, const float *x, float axon_before,
+                                           bool spiked) {
+    if (type == 2) {
+        s.v = x[15] - 9.342518882f;
+        s.spike = (axon_before < 0 && x[0] >= 0) ? 1u : 0u;
+    } else {
+        s.spike = spiked ? 1u : 0u;
+        s.v = x[0];
+    }
+    s.total += (int)s.spike;
+    s.d0 *= c_K.exc_ms; s.d1 *= c_K.exc_ms; s.d2 *= c_K.exc_ms; s.d3 *= c_K.exc_ms;
+    s.inh *= c_K.inh_ms;
+}
+
 // ---- homeostasis (physiology.cuh:243-253) ----------------------------------------
 __device__ __forceinline__ float homeostasis(uint32_t type, float log_ampa, float elapsed, float hz) {
     if (type != 0) return log_ampa;

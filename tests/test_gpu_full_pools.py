@@ -134,7 +134,8 @@ def test_full_pools_2000_ticks(nsb, uneven, monkeypatch, delivery, cluster):
     if cluster == "1":
         assert stats["big_units"] > 0
     assert spikes > 0
-    assert max(np.diff(batch.neuron_offsets)[idx]) == 4096    # the largest brains are in the sample
+    sizes = np.diff(batch.neuron_offsets)
+    assert sizes[idx].max() == sizes.max()                   # the largest brains are in the sample
 
 
 def test_plasticity_heavy_full_pools_2000_ticks(nsb):

@@ -34,6 +34,8 @@ def test_noalloc_step_matches_regular_step_two_calls(nsb):
             np.testing.assert_array_equal(a[0], b[0])
             np.testing.assert_array_equal(a[1], b[1])
             assert a[2] == b[2]
+    # synaptic arrivals are counted by both steps alike
+    assert regular.take_events() == noalloc.take_events() > 0
     regular.close()
     noalloc.close()
 
