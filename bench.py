@@ -442,9 +442,11 @@ def run_ours(args, rank, world, local_rank):
     gpu.upload(batch.inputs, np.ones(batch.brains, np.uint8))
     stream = torch.cuda.Stream()
     s = stream.cuda_stream
-    # Delivery-mode autotune (untimed; state restored afterwards).
+    # Per-bucket autotune (untimed; state restored afterwards).
     coop = gpu.autotune(16, batch.gain, s)
     torch.cuda.synchronize()
+    plan = [{k: b[k] for k in ("name", "units", "max_neurons", "block", "cooperative", "cluster", "meta_cap", "grid")}
+            for b in gpu.buckets() if b["units"]]
     for _ in range(max(args.warmup, 3)):
         gpu.step_graph(16, batch.gain, s)
     torch.cuda.synchronize()
@@ -469,7 +471,7 @@ def run_ours(args, rank, world, local_rank):
     ms_step = ms / args.steps
     value = total_neurons * 16 * args.steps / (ms / 1e3)
     events_per_s = events / (ms / 1e3)
-    launches_per_step = (1 if st["units"] > 0 else 0) + (1 if st.get("heavy", 0) else 0)
+    launches_per_step = len(plan)          # one tick-kernel launch per non-empty bucket
 
     # e2e: reference-facing C ABI call with pinned host buffers
     inp = torch.from_numpy(batch.inputs).pin_memory()
@@ -519,6 +521,7 @@ def run_ours(args, rank, world, local_rank):
                            "parallelism": (f"shards x{world}" if args.strong and world > 1 else f"replicas x{world}"),
                            "units": st["units"], "grid": st["grid"], "block": st["block"],
                            "delivery": "warp-cooperative" if coop else "serial",
+                           "plan": plan,
                            "l2": (f"device state {(120 * N + 108 * E) / 1e9:.2f} GB > 126 MB L2: inputs larger than L2"
                                   if 120 * N + 108 * E > 126e6 else
                                   f"device state {(120 * N + 108 * E) / 1e6:.1f} MB, L2-resident (not flushed)")},

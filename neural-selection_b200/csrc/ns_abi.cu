@@ -584,11 +584,34 @@ int nsb_gpu_set_delivery(void *p, int cooperative) {
     }
 }
 
-// Times both delivery modes on the batch's own buffers (state restored) and
-// keeps the faster; returns the chosen mode (1 cooperative, 0 serial) or -1.
+// Per-bucket autotuner on the batch's own buffers (state restored); returns
+// the packed bucket's delivery mode (1 cooperative, 0 serial) or -1.
 int nsb_gpu_autotune(void *p, int ticks, float gain, void *stream) {
     try {
         return static_cast<GpuBatch *>(p)->engine->autotune(ticks, gain, static_cast<cudaStream_t>(stream)) ? 1 : 0;
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+int nsb_gpu_buckets(void *p, int *out) {
+    const auto &bs = static_cast<GpuBatch *>(p)->engine->buckets();
+    int k = 0;
+    for (const Bucket &B : bs) {
+        const int v[10] = {B.ub, B.units(), B.max_neurons, B.max_synapses, B.cfg.block, B.cfg.coop, B.cfg.cluster,
+                           B.cfg.meta_cap, B.smem, B.grid};
+        std::memcpy(out + k, v, sizeof v);
+        k += 10;
+    }
+    return k;
+}
+
+int nsb_gpu_set_bucket(void *p, int bucket, int block, int cooperative, int cluster, int meta_cap) {
+    try {
+        static_cast<GpuBatch *>(p)->engine->set_bucket(bucket, BucketConfig{block, cooperative ? 1 : 0, cluster,
+                                                                             meta_cap});
+        return 0;
     } catch (const std::exception &e) {
         g_error = e.what();
         return -1;

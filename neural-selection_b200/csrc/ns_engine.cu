@@ -333,8 +333,8 @@ __global__ void __launch_bounds__(256, HEAVY ? 1 : NSB_MIN_CTAS) tick_kernel(Poo
                                                    const uint8_t *__restrict__ mask, float *__restrict__ output,
                                                    int *__restrict__ status, int ticks, float gain) {
     float *tab = reinterpret_cast<float *>(g_smem);                      // 2^(j/128) hi/lo pairs
-    uint32_t *s_meta = reinterpret_cast<uint32_t *>(g_smem + 1024);       // kMetaCap
-    uint32_t *hist = s_meta + kMetaCap;                                   // 32 * hw
+    uint32_t *s_meta = reinterpret_cast<uint32_t *>(g_smem + 1024);       // P.meta_cap
+    uint32_t *hist = s_meta + P.meta_cap;                                   // 32 * hw
     int *cnt = reinterpret_cast<int *>(hist + 32 * P.hw);                // 32 * hw (spike counts)
     int64_t *s_tick = reinterpret_cast<int64_t *>(cnt + 32 * P.hw);      // kMaxUnitBrains
     int *s_mask = reinterpret_cast<int *>(s_tick + kMaxUnitBrains);
@@ -368,7 +368,7 @@ __global__ void __launch_bounds__(256, HEAVY ? 1 : NSB_MIN_CTAS) tick_kernel(Poo
             s_mask[i] = mask[b] && in_range;
             status[b] = in_range ? 0 : -2;
         }
-        const bool meta_smem = ne <= kMetaCap;
+        const bool meta_smem = ne <= P.meta_cap;
         if (meta_smem)
             for (int k = tid; k < ne; k += bs) s_meta[k] = P.smeta[e0 + k];
         const uint32_t *meta = meta_smem ? s_meta : P.smeta + e0;
@@ -558,6 +558,239 @@ __global__ void __launch_bounds__(256, HEAVY ? 1 : NSB_MIN_CTAS) tick_kernel(Poo
     }
 }
 
+// ---- light units with a per-tick integration list ---------------------------------
+// The light kernel splits each tick in two phases. Phase A: every thread
+// delivers the input of its own neurons (in ascending edge order, as above)
+// and decides whether each needs integrating; a neuron at a fixed point of
+// the input-free tick (see unchanged) with no input this tick does not, and
+// its plasticity, if an arrival or modulator calls for it, runs right there
+// with no postsynaptic spike. Neurons that do need integrating are appended,
+// with their delivered input, to a shared-memory list. Phase B: the CTA's
+// threads integrate the list, one entry each, so the integrations run at
+// full warp width however the needy neurons are spread over the unit; a
+// spike sets its bit in the current ring slot (atomicOr), which phase A of
+// the next tick reads. Each neuron's arithmetic is the same as when its owner
+// integrates it, so the results are identical bit for bit. Units above
+// kListCap neurons run the two phases per chunk of kListCap neurons.
+constexpr int kListCap = 768;
+
+template <bool COOP>
+__global__ void __launch_bounds__(256, NSB_MIN_CTAS) tick_kernel_list(Pools P, int unit_begin, int unit_end,
+                                                                      int *queue, const float *__restrict__ input,
+                                                                      const uint8_t *__restrict__ mask,
+                                                                      float *__restrict__ output,
+                                                                      int *__restrict__ status, int ticks,
+                                                                      float gain) {
+    float *tab = reinterpret_cast<float *>(g_smem);                      // 2^(j/128) hi/lo pairs
+    uint32_t *s_meta = reinterpret_cast<uint32_t *>(g_smem + 1024);       // P.meta_cap
+    uint32_t *hist = s_meta + P.meta_cap;                                   // 32 * hw
+    int *cnt = reinterpret_cast<int *>(hist + 32 * P.hw);                // 32 * hw (spike counts)
+    uint32_t *s_fixed = reinterpret_cast<uint32_t *>(cnt + 32 * P.hw);   // hw: neuron at a fixed point
+    int64_t *s_tick = reinterpret_cast<int64_t *>(s_fixed + ((P.hw + 1) & ~1));   // kMaxUnitBrains
+    int *s_mask = reinterpret_cast<int *>(s_tick + kMaxUnitBrains);
+    int *s_bid = s_mask + kMaxUnitBrains;                                 // caller brain index
+    int *s_ev = s_bid + kMaxUnitBrains;                                   // 8 warps x kEvCap event synapses
+    uint32_t *s_evv = reinterpret_cast<uint32_t *>(s_ev + 8 * kEvCap);    // 8 warps x kEvCap tick / value
+    int *l_j = reinterpret_cast<int *>(s_evv + 8 * kEvCap);              // the list: neuron, input, mod | narr << 8
+    float *l_e0 = reinterpret_cast<float *>(l_j + kListCap), *l_e1 = l_e0 + kListCap, *l_e2 = l_e1 + kListCap,
+          *l_e3 = l_e2 + kListCap, *l_inh = l_e3 + kListCap;
+    uint32_t *l_mn = reinterpret_cast<uint32_t *>(l_inh + kListCap);
+    __shared__ int s_unit, s_count[2];
+    __shared__ unsigned long long s_events;
+
+    const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarp = bs >> 5;
+    const int spc = kListCap / bs;                                         // slots per chunk
+    {
+        const float *src = nsx::exp2f_table();
+        for (int i = tid; i < 256; i += bs) tab[i] = src[i];
+    }
+    for (;;) {
+        if (tid == 0) { s_unit = unit_begin + atomicAdd(queue, 1); s_events = 0; s_count[0] = s_count[1] = 0; }
+        __syncthreads();
+        const int u = s_unit;
+        if (u >= unit_end) break;
+        const int4 U = P.units[u];
+        const int2 UB = P.unitb[u];
+        const int n0 = U.x, nn = U.y, e0 = U.z, ne = U.w, b0 = UB.x, nb = UB.y;
+        for (int i = tid; i < nb; i += bs) {
+            const int b = P.ubrain[b0 + i];
+            s_bid[i] = b;
+            const int64_t t0 = P.btick[b];
+            s_tick[i] = t0;
+            // last-arrival ticks are stored as int32: refuse to step past 2^31
+            const bool in_range = t0 + (int64_t)ticks < 2147483647ll;
+            s_mask[i] = mask[b] && in_range;
+            status[b] = in_range ? 0 : -2;
+        }
+        const bool meta_smem = ne <= P.meta_cap;
+        if (meta_smem)
+            for (int k = tid; k < ne; k += bs) s_meta[k] = P.smeta[e0 + k];
+        const uint32_t *meta = meta_smem ? s_meta : P.smeta + e0;
+        for (int w = tid; w < P.hw; w += bs) s_fixed[w] = 0u;
+        // A unit whose brains are all masked off does no work: outputs 0.
+        if (!__syncthreads_or(tid < nb && s_mask[tid] != 0)) {
+            for (int i = tid; i < nb * P.outputs; i += bs)
+                output[(size_t)s_bid[i / P.outputs] * P.outputs + (i % P.outputs)] = 0.0f;
+            continue;
+        }
+        const int slots = (nn + bs - 1) / bs;
+        int my_events = 0;
+        for (int sl0 = 0; sl0 < slots; ++sl0) {
+            const int j = sl0 * bs + tid;
+            const bool has = j < nn;
+            const uint32_t flags = has ? P.nflags[n0 + j] : 0u;
+            const int bi = (int)((flags >> NF_SLOT_SHIFT) & NF_SLOT_MASK);
+            const bool run = has && s_mask[bi] != 0;
+            uint32_t h0 = 0;
+            if (run) {
+                uint32_t *r = P.nstate + (size_t)(n0 + j) * S_WORDS;
+                h0 = r[S_HIST];
+                r[S_PAD] = __float_as_uint(crexp(__uint_as_float(r[S_LOGAMPA]), tab));
+            }
+            const uint32_t rot = run ? rotr32(h0, (uint32_t)(s_tick[bi] & 31)) : 0u;
+            for (int sl = 0; sl < 32; ++sl) {
+                const uint32_t w = __ballot_sync(0xffffffffu, (rot >> sl) & 1u);
+                if (lane == 0) hist[sl * P.hw + sl0 * nwarp + warp] = w;
+            }
+            if (has) cnt[j] = 0;
+        }
+        __syncthreads();
+        int seq = 0;   // chunks run so far (the list counter alternates between two words)
+        for (int t = 0; t < ticks; ++t) {
+            for (int c0 = 0; c0 < slots; c0 += spc, ++seq) {
+                const int par = seq & 1;
+                if (tid == 0) s_count[par ^ 1] = 0;                      // the next chunk's counter
+                // ---- phase A: delivery and the integration list --------------------
+                for (int sl0 = c0; sl0 < min(slots, c0 + spc); ++sl0) {
+                    const int j = sl0 * bs + tid;
+                    const int n = n0 + j;
+                    const uint32_t flags = j < nn ? P.nflags[n] : 0u;
+                    const int bi = (int)((flags >> NF_SLOT_SHIFT) & NF_SLOT_MASK);
+                    const bool run = j < nn && s_mask[bi] != 0;
+                    if (lane == 0) hist[(t & 31) * P.hw + sl0 * nwarp + warp] = 0u;   // filled in phase B
+                    int ib = 0, ie = 0;
+                    int64_t tick0 = 0;
+                    float ampa = 0.0f;
+                    if (run) {
+                        tick0 = s_tick[bi];
+                        ib = P.inptr[n];
+                        ie = P.inptr[n + 1];
+                        ampa = __uint_as_float(P.nstate[(size_t)n * S_WORDS + S_PAD]);
+                    }
+                    const bool dlv = run && (flags & NF_ACTIVE);
+                    Delivered d = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0u, 0};
+                    if (COOP)
+                        d = deliver_warp(P, dlv ? ib : 0, dlv ? ie : 0, e0, meta, hist, t, tick0, ampa, tab,
+                                         s_ev + warp * kEvCap, s_evv + warp * kEvCap, lane);
+                    else if (dlv)
+                        d = deliver(P, ib, ie, e0, meta, hist, t, tick0, ampa, tab);
+                    bool need = false;
+                    uint32_t mod = d.mod;
+                    if (run) {
+                        if (P.pulse_period > 0 && (tick0 + t) % P.pulse_period == 0) mod |= P.pulse_mod;
+                        my_events += d.narr;
+                        if (no_input(flags, d) && ((s_fixed[j >> 5] >> (j & 31)) & 1u)) {
+                            // a fixed point without input: the record stays as it is, no spike
+                            if ((flags & NF_PLASTIC_IN) && (mod || d.narr))
+                                plasticity_events(P.sstate, P.sgene, P.slastp, P.hw, ib, ie, e0, meta, hist, t,
+                                                  tick0, false, mod,
+                                                  __uint_as_float(P.nstate[(size_t)n * S_WORDS + S_DEPOL]), tab);
+                        } else {
+                            need = true;
+                        }
+                    }
+                    const uint32_t nm = __ballot_sync(0xffffffffu, need);
+                    int base = 0;
+                    if (lane == 0 && nm) base = atomicAdd(&s_count[par], __popc(nm));
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    if (need) {
+                        const int k = base + __popc(nm & ((1u << lane) - 1u));
+                        l_j[k] = j;
+                        l_e0[k] = d.e0; l_e1[k] = d.e1; l_e2[k] = d.e2; l_e3[k] = d.e3; l_inh[k] = d.inh;
+                        l_mn[k] = mod | ((uint32_t)d.narr << 8);
+                    }
+                }
+                __syncthreads();
+                // ---- phase B: the list's integrations, one per thread ---------------
+                const int count = s_count[par];
+                for (int k = tid; k < count; k += bs) {
+                    const int j = l_j[k];
+                    const int n = n0 + j;
+                    const uint32_t flags = P.nflags[n];
+                    const int bi = (int)((flags >> NF_SLOT_SHIFT) & NF_SLOT_MASK);
+                    const uint32_t mn = l_mn[k];
+                    const Delivered d = {l_e0[k], l_e1[k], l_e2[k], l_e3[k], l_inh[k], mn & 0xffu, (int)(mn >> 8)};
+                    uint32_t *r = P.nstate + (size_t)n * S_WORDS;
+                    NeuronRegs s;
+                    float log_ampa;
+                    uint32_t hw0;
+                    load_neuron(r, s, log_ampa, hw0);
+                    if (flags & NF_ACTIVE) {
+                        const float level =
+                            (flags & NF_HAS_INPUT) ? input[(size_t)s_bid[bi] * P.channels + P.nsens[n]] : 0.0f;
+                        integrate<false>(P, n, flags, d, level, gain, s, status + s_bid[bi], tab);
+                    } else {
+                        s.spike = 0;
+                    }
+                    if (no_input(flags, d) && unchanged(r, s)) atomicOr(&s_fixed[j >> 5], 1u << (j & 31));
+                    else atomicAnd(&s_fixed[j >> 5], ~(1u << (j & 31)));
+                    // the record's spare word keeps the call's AMPA scale
+                    store_neuron(r, s, log_ampa, hw0, r[S_PAD]);
+                    if (s.spike) {
+                        atomicOr(&hist[(t & 31) * P.hw + (j >> 5)], 1u << (j & 31));
+                        ++cnt[j];
+                    }
+                    if ((flags & NF_PLASTIC_IN) && (s.spike || d.mod || d.narr))
+                        plasticity_events(P.sstate, P.sgene, P.slastp, P.hw, P.inptr[n], P.inptr[n + 1], e0, meta,
+                                          hist, t, s_tick[bi], s.spike != 0, d.mod, s.depol, tab);
+                }
+                __syncthreads();
+            }
+        }
+        for (int sl0 = 0; sl0 < slots; ++sl0) {
+            const int j = sl0 * bs + tid;
+            if (j >= nn) continue;
+            const int n = n0 + j;
+            const uint32_t flags = P.nflags[n];
+            const int bi = (int)((flags >> NF_SLOT_SHIFT) & NF_SLOT_MASK);
+            if (!s_mask[bi]) continue;
+            const int64_t tick0 = s_tick[bi];
+            uint32_t *r = P.nstate + (size_t)n * S_WORDS;
+            float la = __uint_as_float(r[S_LOGAMPA]);
+            if (flags & NF_ACTIVE) {
+                const int total = (int)r[S_TOTAL];
+                const int64_t t1 = tick0 + ticks;
+                la = homeostasis(flags & NF_TYPE_MASK, la, (float)ticks,
+                                 (float)total * 1000.0f / (float)(ticks > t1 ? (int64_t)ticks : t1));
+            }
+            uint32_t L = 0;
+            const int word = sl0 * nwarp + warp;
+            for (int sl = 0; sl < 32; ++sl) L |= ((hist[sl * P.hw + word] >> lane) & 1u) << sl;
+            r[S_LOGAMPA] = __float_as_uint(la);
+            r[S_HIST] = rotl32(L, (uint32_t)(tick0 & 31));
+            r[S_PAD] = 0u;
+            finish_synapses(P, P.inptr[n], P.inptr[n + 1], e0, meta, hist, ticks, tick0);
+        }
+        __syncthreads();
+        // ---- motor outputs (spikes per call) and tick counters --------------------
+        for (int i = tid; i < nb * P.outputs; i += bs) {
+            const int bi = i / P.outputs, b = s_bid[bi];
+            output[(size_t)b * P.outputs + (i - bi * P.outputs)] =
+                s_mask[bi] ? (float)cnt[P.bmotor[(size_t)b * P.outputs + (i - bi * P.outputs)] - n0] : 0.0f;
+        }
+        for (int i = tid; i < nb; i += bs)
+            if (s_mask[i]) P.btick[s_bid[i]] = s_tick[i] + ticks;
+        if (P.events) {
+            unsigned long long v = (unsigned long long)my_events;
+            for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (lane == 0 && v) atomicAdd(&s_events, v);
+            __syncthreads();
+            if (tid == 0 && s_events) atomicAdd(P.events, s_events);
+        }
+        __syncthreads();
+    }
+}
+
 // ---- big brains: one brain per thread-block cluster -------------------------------
 // A brain above the CTA unit size is stepped by a cluster of C CTAs (C = 2, 4
 // or 8, from the launch). CTA rank r owns the brain's neurons [r*per,
@@ -583,8 +816,8 @@ __global__ void __launch_bounds__(256, NSB_MIN_CTAS) tick_kernel_cluster(Pools P
     const int C = (int)cluster.num_blocks();
     const int rank = (int)cluster.block_rank();
     float *tab = reinterpret_cast<float *>(g_smem);                      // 2^(j/128) hi/lo pairs
-    uint32_t *s_meta = reinterpret_cast<uint32_t *>(g_smem + 1024);       // kMetaCap
-    uint32_t *hist = s_meta + kMetaCap;                                   // 32 * hw
+    uint32_t *s_meta = reinterpret_cast<uint32_t *>(g_smem + 1024);       // P.meta_cap
+    uint32_t *hist = s_meta + P.meta_cap;                                   // 32 * hw
     int *cnt = reinterpret_cast<int *>(hist + 32 * P.hw);                // 32 * hw (own neurons' spike counts)
     int *s_ev = cnt + 32 * P.hw;                                          // 8 warps x kEvCap
     uint32_t *s_evv = reinterpret_cast<uint32_t *>(s_ev + 8 * kEvCap);
@@ -620,7 +853,7 @@ __global__ void __launch_bounds__(256, NSB_MIN_CTAS) tick_kernel_cluster(Pools P
         const int per = (((nn + C - 1) / C) + 31) & ~31;
         const int lo = min(nn, rank * per), hi = min(nn, lo + per);
         const int e0 = P.inptr[n0 + lo], e1 = P.inptr[n0 + hi];
-        const bool meta_smem = e1 - e0 <= kMetaCap;
+        const bool meta_smem = e1 - e0 <= P.meta_cap;
         if (meta_smem)
             for (int k = tid; k < e1 - e0; k += bs) s_meta[k] = P.smeta[e0 + k];
         const uint32_t *meta = meta_smem ? s_meta : P.smeta + e0;
@@ -805,8 +1038,15 @@ int spike_words(int max_unit_neurons, int block) {
     return ((std::max(max_unit_neurons, block) + block - 1) / block) * (block / 32);
 }
 
-int tick_smem_bytes(int hw) {
-    return 1024 + (kMetaCap + 32 * hw * 2) * 4 + kMaxUnitBrains * 8 + 2 * kMaxUnitBrains * 4 + 8 * kEvCap * 8 +
+// Dynamic shared memory of the light (list) kernel.
+int tick_smem_bytes(int hw, int meta_cap) {
+    return 1024 + (meta_cap + 32 * hw * 2 + ((hw + 1) & ~1)) * 4 + kMaxUnitBrains * 8 + 2 * kMaxUnitBrains * 4 +
+           8 * kEvCap * 8 + kListCap * 7 * 4;
+}
+
+// Dynamic shared memory of the heavy kernel for hw ring words.
+static int heavy_smem_bytes(int hw, int meta_cap = kMetaCap) {
+    return 1024 + (meta_cap + 32 * hw * 2) * 4 + kMaxUnitBrains * 8 + 2 * kMaxUnitBrains * 4 + 8 * kEvCap * 8 +
            8 * kHeavyWarpScratch * 4;
 }
 
@@ -824,15 +1064,17 @@ static void set_tick_smem(int) {
     int dev = 0, optin = 0;
     NSB_CHECK(cudaGetDevice(&dev));
     NSB_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    allow_dynamic_smem(tick_kernel<false, false>, optin);
-    allow_dynamic_smem(tick_kernel<false, true>, optin);
+    allow_dynamic_smem(tick_kernel_list<false>, optin);
+    allow_dynamic_smem(tick_kernel_list<true>, optin);
     allow_dynamic_smem(tick_kernel<true, false>, optin);
     allow_dynamic_smem(tick_kernel_cluster<false>, optin);
     allow_dynamic_smem(tick_kernel_cluster<true>, optin);
 }
 
 // Dynamic shared memory of the cluster kernel for hw ring words.
-static int cluster_smem_bytes(int hw) { return 1024 + (kMetaCap + 64 * hw) * 4 + 8 * kEvCap * 8; }
+static int cluster_smem_bytes(int hw, int meta_cap = kMetaCap) {
+    return 1024 + (meta_cap + 64 * hw) * 4 + 8 * kEvCap * 8;
+}
 
 static cudaLaunchConfig_t cluster_config(int C, int clusters, int block, int smem, cudaStream_t s,
                                          cudaLaunchAttribute *attr) {
@@ -850,14 +1092,26 @@ static cudaLaunchConfig_t cluster_config(int C, int clusters, int block, int sme
     return cfg;
 }
 
-// Co-resident clusters of C CTAs (the smaller of the two delivery modes).
-static int cluster_capacity(int C, int block, int smem) {
+// Occupancy queries for the autotuner: 0 when the shape cannot run (the
+// query's error, if any, is cleared so that it does not surface later).
+static int clusters_resident(int C, int block, int smem) {
     cudaLaunchAttribute attr[1];
     cudaLaunchConfig_t cfg = cluster_config(C, 1, block, smem, nullptr, attr);
     int a = 0, b = 0;
-    NSB_CHECK(cudaOccupancyMaxActiveClusters(&a, tick_kernel_cluster<false>, &cfg));
-    NSB_CHECK(cudaOccupancyMaxActiveClusters(&b, tick_kernel_cluster<true>, &cfg));
-    return std::max(1, std::min(a, b));
+    if (cudaOccupancyMaxActiveClusters(&a, tick_kernel_cluster<false>, &cfg) != cudaSuccess ||
+        cudaOccupancyMaxActiveClusters(&b, tick_kernel_cluster<true>, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return std::min(a, b);
+}
+template <class K> static int ctas_resident(K kernel, int block, int smem) {
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, block, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return occ;
 }
 
 static void launch_cluster(bool coop, int C, int clusters, int block, int smem, cudaStream_t s, const Pools &P,
@@ -878,9 +1132,9 @@ static void launch_light(bool coop, int grid, int block, int smem, cudaStream_t 
                          int *queue, const float *input, const uint8_t *mask, float *output, int *status, int ticks,
                          float gain) {
     if (coop)
-        tick_kernel<false, true><<<grid, block, smem, s>>>(P, ub, ue, queue, input, mask, output, status, ticks, gain);
+        tick_kernel_list<true><<<grid, block, smem, s>>>(P, ub, ue, queue, input, mask, output, status, ticks, gain);
     else
-        tick_kernel<false, false><<<grid, block, smem, s>>>(P, ub, ue, queue, input, mask, output, status, ticks, gain);
+        tick_kernel_list<false><<<grid, block, smem, s>>>(P, ub, ue, queue, input, mask, output, status, ticks, gain);
 }
 
 void prepare_tick_kernels(int smem) {
@@ -891,8 +1145,8 @@ void prepare_tick_kernels(int smem) {
 
 int tick_occupancy(int block, int smem) {
     int occ = 0, occ2 = 0;
-    NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tick_kernel<false, false>, block, smem));
-    NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, tick_kernel<false, true>, block, smem));
+    NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tick_kernel_list<false>, block, smem));
+    NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, tick_kernel_list<true>, block, smem));
     return std::max(std::min(occ, occ2), 1);
 }
 
@@ -1210,11 +1464,39 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
     const auto &unitb = p.unitb;
     const auto &brain_order = p.brain_order;
     hw_ = spike_words(max_unit_neurons_, block_);
-    for (int g = 0; g < 3; ++g) n_cluster_[g] = p.n_cluster[g];
-    hw_small_ = spike_words(p.max_small, block_);
-    hw_big_ = spike_words(p.max_big, block_);
-    hw_heavy_ = spike_words(p.max_heavy, block_);
     coop_ = n_synapses_ >= 4ll * n_neurons_;
+    // Light units are in queue order by size, largest first; a unit above the
+    // unit size holds one brain. Buckets by size class, then the heavy units.
+    const bool clustered = cfg.cluster_big == 1 ||
+                           (cfg.cluster_big < 0 && p.n_big_units > 0 && p.n_light_units < sms0 * NSB_MIN_CTAS);
+    buckets_.assign(kBuckets, Bucket{});
+    {
+        auto bucket_of = [&](int nn) { return nn > 4 * unit_cap_ ? 0 : nn > 2 * unit_cap_ ? 1 : nn > unit_cap_ ? 2 : 3; };
+        for (int b = 0; b < kBuckets; ++b) buckets_[b].ub = buckets_[b].ue = b == kBucketHeavy ? n_light_units_ : 0;
+        int cur = -1;
+        for (int u = 0; u < n_light_units_; ++u) {
+            const int b = bucket_of(p.units[u].y);
+            if (b < cur) throw std::runtime_error("Work units out of size order");
+            if (b != cur) { buckets_[b].ub = u; cur = b; }
+            buckets_[b].ue = u + 1;
+        }
+        buckets_[kBucketHeavy].ub = n_light_units_;
+        buckets_[kBucketHeavy].ue = n_units_;
+        buckets_[kBucketHeavy].heavy = true;
+        for (int b = 0; b < kBuckets; ++b) {
+            Bucket &B = buckets_[b];
+            if (B.ue < B.ub) B.ue = B.ub;
+            for (int u = B.ub; u < B.ue; ++u) {
+                B.max_neurons = std::max(B.max_neurons, p.units[u].y);
+                B.max_synapses = std::max(B.max_synapses, p.units[u].w);
+            }
+            B.cluster_size = b < 3 ? kClusterSizes[b] : 1;
+            B.cfg.block = block_;
+            B.cfg.coop = b == kBucketHeavy ? 0 : (int)coop_;
+            B.cfg.cluster = b < 3 && clustered ? B.cluster_size : 1;
+            B.cfg.meta_cap = kMetaCap;
+        }
+    }
 
     // ---- device allocation and upload ----
     NSB_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
@@ -1260,23 +1542,27 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
     h_tick_.assign(n_brains_, 0);
 
     // ---- launch shape ----
-    smem_ = tick_smem_bytes(hw_small_);
-    smem_big_ = cluster_smem_bytes(hw_big_);
-    smem_heavy_ = tick_smem_bytes(hw_heavy_);
-    set_tick_smem(smem_);
-    int dev = 0;
+    set_tick_smem(0);
+    int dev = 0, optin = 0;
     NSB_CHECK(cudaGetDevice(&dev));
     NSB_CHECK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
-    const int occ = tick_occupancy(block_, smem_);
-    ctas_per_sm_ = cfg.ctas_per_sm > 0 ? std::min(cfg.ctas_per_sm, std::max(occ, 1)) : std::max(occ, 1);
-    const int n_big = n_cluster_[0] + n_cluster_[1] + n_cluster_[2];
-    grid_ = std::min(std::max(n_light_units_ - n_big, 1), sms_ * ctas_per_sm_);
-    for (int g = 0; g < 3; ++g)
-        if (n_cluster_[g])
-            clusters_[g] = std::min(n_cluster_[g], cluster_capacity(kClusterSizes[g], block_, smem_big_));
-    int occh = 0;
-    NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occh, tick_kernel<true, false>, block_, smem_heavy_));
-    grid_heavy_ = std::min(std::max(n_units_ - n_light_units_, 1), sms_ * std::max(occh, 1));
+    NSB_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    smem_optin_ = optin - 1024;      // room for the kernels' static shared memory
+    ctas_cap_ = cfg.ctas_per_sm;
+    for (int b = 0; b < kBuckets; ++b) {
+        Bucket &B = buckets_[b];
+        if (!shape_bucket(B) && B.cfg.cluster > 1) {   // clusters that cannot run: one CTA per brain
+            B.cfg.cluster = 1;
+            if (!shape_bucket(B)) throw std::runtime_error("Work unit exceeds the device's shared memory");
+        } else if (B.units() && B.grid == 0) {
+            throw std::runtime_error("Work unit exceeds the device's shared memory");
+        }
+    }
+    for (int b = 0; b < kBuckets; ++b) {
+        NSB_CHECK(cudaStreamCreateWithFlags(&bstream_[b], cudaStreamNonBlocking));
+        NSB_CHECK(cudaEventCreateWithFlags(&join_[b], cudaEventDisableTiming));
+    }
+    NSB_CHECK(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
     K_ = make_constants();
     NSB_CHECK(cudaMemcpyToSymbol(c_K, &K_, sizeof(PhysConst)));
 }
@@ -1284,12 +1570,64 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
 Engine::~Engine() {
     for (auto &g : graphs_) cudaGraphExecDestroy(g.exec);
     for (void *p : allocations_) cudaFree(p);
+    for (int b = 0; b < kBuckets; ++b) {
+        if (bstream_[b]) cudaStreamDestroy(bstream_[b]);
+        if (join_[b]) cudaEventDestroy(join_[b]);
+    }
+    if (fork_) cudaEventDestroy(fork_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
 Stats Engine::stats() const {
+    const Bucket &B = buckets_[kBucketPacked];
+    const int occ = B.units() ? ctas_resident(tick_kernel_list<false>, B.cfg.block, B.smem) : 0;
     return Stats{n_brains_, n_units_, n_big_units_, n_neurons_, n_synapses_, n_heavy_, max_unit_neurons_,
-                 grid_, block_, smem_, ctas_per_sm_};
+                 B.grid, B.cfg.block, B.smem, occ};
+}
+
+bool Engine::shape_bucket(Bucket &B) const {
+    const BucketConfig &c = B.cfg;
+    if (c.block != 128 && c.block != 256) return false;
+    if (c.meta_cap < 0 || c.meta_cap % 32 != 0) return false;
+    if (B.heavy && (c.coop || c.cluster != 1)) return false;
+    if (c.cluster != 1 && c.cluster != B.cluster_size) return false;
+    B.hw = spike_words(B.max_neurons, c.block);
+    if (B.units() == 0) {
+        B.smem = 0;
+        B.grid = 0;
+        return true;
+    }
+    if (B.heavy) {
+        B.smem = heavy_smem_bytes(B.hw, c.meta_cap);
+        const int occ = B.smem <= smem_optin_ ? ctas_resident(tick_kernel<true, false>, c.block, B.smem) : 0;
+        B.grid = std::min(B.units(), sms_ * occ);
+    } else if (c.cluster > 1) {
+        B.smem = cluster_smem_bytes(B.hw, c.meta_cap);
+        B.grid = B.smem <= smem_optin_ ? std::min(B.units(), clusters_resident(c.cluster, c.block, B.smem)) : 0;
+    } else {
+        B.smem = tick_smem_bytes(B.hw, c.meta_cap);
+        int occ = B.smem <= smem_optin_ ? std::min(ctas_resident(tick_kernel_list<false>, c.block, B.smem),
+                                                   ctas_resident(tick_kernel_list<true>, c.block, B.smem))
+                                        : 0;
+        if (ctas_cap_ > 0) occ = std::min(occ, ctas_cap_);
+        B.grid = std::min(B.units(), sms_ * occ);
+    }
+    return B.grid > 0;
+}
+
+void Engine::set_bucket(int b, const BucketConfig &cfg) {
+    if (b < 0 || b >= kBuckets) throw std::runtime_error("Invalid bucket");
+    Bucket B = buckets_[b];
+    B.cfg = cfg;
+    if (!shape_bucket(B)) throw std::runtime_error("Bucket configuration cannot run on this device");
+    NSB_CHECK(cudaDeviceSynchronize());
+    buckets_[b] = B;
+    drop_graphs();
+}
+
+void Engine::drop_graphs() {
+    for (auto &g : graphs_) cudaGraphExecDestroy(g.exec);
+    graphs_.clear();
 }
 
 Pools Engine::pools(bool events) const {
@@ -1298,41 +1636,58 @@ Pools Engine::pools(bool events) const {
     P.nxidx = d_nxidx_; P.xgene = d_xgene_; P.xstate = d_xstate_; P.nstate = d_nstate_; P.inptr = d_inptr_;
     P.smeta = d_smeta_; P.sgene = d_sgene_; P.sstate = d_sstate_; P.sarrived = d_sarrived_; P.slastp = d_slastp_;
     P.btick = d_btick_; P.bmotor = d_bmotor_; P.units = d_units_; P.unitb = d_unitb_; P.ubrain = d_ubrain_;
-    P.channels = channels_; P.outputs = outputs_; P.hw = hw_small_;
+    P.channels = channels_; P.outputs = outputs_; P.hw = hw_;
     P.events = events ? d_events_ : nullptr;
     P.pulse_period = pulse_period_;
     P.pulse_mod = pulse_mod_;
     return P;
 }
 
-// Every unit group of a step, in queue order: big brains by clusters of 8, 4
-// and 2 CTAs, light units of one CTA, heavy units. queue: 8 zeroed counters.
-void Engine::launch_groups(const Pools &P0, int *queue, const float *d_input, const uint8_t *d_mask, int ticks,
+// One bucket's kernel over its units.
+void Engine::launch_bucket(const Bucket &B, const Pools &P0, int *queue, const float *d_input, const uint8_t *d_mask,
+                           int ticks, float gain, float *d_output, int *d_status, cudaStream_t stream) const {
+    Pools P = P0;
+    P.hw = B.hw;
+    P.meta_cap = B.cfg.meta_cap;
+    if (B.heavy)
+        tick_kernel<true, false><<<B.grid, B.cfg.block, B.smem, stream>>>(P, B.ub, B.ue, queue, d_input, d_mask,
+                                                                           d_output, d_status, ticks, gain);
+    else if (B.cfg.cluster > 1)
+        launch_cluster(B.cfg.coop != 0, B.cfg.cluster, B.grid, B.cfg.block, B.smem, stream, P, B.ub, B.ue, queue,
+                       d_input, d_mask, d_output, d_status, ticks, gain);
+    else
+        launch_light(B.cfg.coop != 0, B.grid, B.cfg.block, B.smem, stream, P, B.ub, B.ue, queue, d_input, d_mask,
+                     d_output, d_status, ticks, gain);
+}
+
+// Every bucket of a step, each on its own stream so that the buckets run
+// side by side: the big-brain and heavy buckets are launched first, the
+// packed bucket (on the caller's stream) fills the rest of the GPU.
+// queue: 8 counters, zeroed here.
+void Engine::launch_groups(const Pools &P, int *queue, const float *d_input, const uint8_t *d_mask, int ticks,
                            float gain, float *d_output, int *d_status, cudaStream_t stream) {
     NSB_CHECK(cudaMemsetAsync(queue, 0, 8 * sizeof(int), stream));
-    int ub = 0;
-    for (int g = 0; g < 3; ++g) {
-        if (n_cluster_[g]) {
-            Pools P = P0;
-            P.hw = hw_big_;
-            launch_cluster(coop_, kClusterSizes[g], clusters_[g], block_, smem_big_, stream, P, ub, ub + n_cluster_[g],
-                           queue + 2 + g, d_input, d_mask, d_output, d_status, ticks, gain);
+    int active = 0;
+    for (const Bucket &B : buckets_) active += B.units() > 0;
+    bool forked[kBuckets] = {};
+    if (active > 1) NSB_CHECK(cudaEventRecord(fork_, stream));
+    for (int b = 0; b < kBuckets; ++b) {
+        const Bucket &B = buckets_[b];
+        if (!B.units() || (active > 1 && b == kBucketPacked)) continue;
+        cudaStream_t s = stream;
+        if (active > 1) {
+            s = bstream_[b];
+            NSB_CHECK(cudaStreamWaitEvent(s, fork_, 0));
+            forked[b] = true;
         }
-        ub += n_cluster_[g];
+        launch_bucket(B, P, queue + b, d_input, d_mask, ticks, gain, d_output, d_status, s);
+        if (forked[b]) NSB_CHECK(cudaEventRecord(join_[b], s));
     }
-    if (n_light_units_ > ub) {
-        Pools P = P0;
-        P.hw = hw_small_;
-        launch_light(coop_, grid_, block_, smem_, stream, P, ub, n_light_units_, queue, d_input, d_mask, d_output,
-                     d_status, ticks, gain);
-    }
-    if (n_units_ > n_light_units_) {
-        Pools P = P0;
-        P.hw = hw_heavy_;
-        tick_kernel<true, false><<<grid_heavy_, block_, smem_heavy_, stream>>>(P, n_light_units_, n_units_, queue + 1,
-                                                                                d_input, d_mask, d_output, d_status,
-                                                                                ticks, gain);
-    }
+    if (active > 1 && buckets_[kBucketPacked].units())
+        launch_bucket(buckets_[kBucketPacked], P, queue + kBucketPacked, d_input, d_mask, ticks, gain, d_output,
+                      d_status, stream);
+    for (int b = 0; b < kBuckets; ++b)
+        if (forked[b]) NSB_CHECK(cudaStreamWaitEvent(stream, join_[b], 0));
     NSB_CHECK(cudaGetLastError());
 }
 
@@ -1426,25 +1781,24 @@ void Engine::step_host(const float *input, const uint8_t *mask, int ticks, float
 void Engine::set_global_modulation(int period, uint32_t mod) {
     if (period < 0 || mod > 7u) throw std::runtime_error("Invalid modulator pulse");
     NSB_CHECK(cudaDeviceSynchronize());
-    for (auto &g : graphs_) cudaGraphExecDestroy(g.exec);
-    graphs_.clear();
+    drop_graphs();
     pulse_period_ = mod ? period : 0;
     pulse_mod_ = period ? mod : 0u;
 }
 
 void Engine::set_cooperative(bool coop) {
-    if (coop == coop_) return;
     NSB_CHECK(cudaStreamSynchronize(stream_));
     NSB_CHECK(cudaDeviceSynchronize());
-    for (auto &g : graphs_) cudaGraphExecDestroy(g.exec);
-    graphs_.clear();
+    for (int b = 0; b < kBuckets; ++b)
+        if (!buckets_[b].heavy) buckets_[b].cfg.coop = coop ? 1 : 0;
     coop_ = coop;
+    drop_graphs();
 }
 
 bool Engine::autotune(int ticks, float gain, cudaStream_t stream) {
     if (ticks < 1 || ticks > 10000 || !std::isfinite(gain) || gain < 0)
         throw std::runtime_error("Invalid neural integration interval");
-    if (n_light_units_ == 0) return coop_;
+    if (n_light_units_ == 0) return cooperative();
     cudaStream_t s = stream ? stream : stream_;
     NSB_CHECK(cudaDeviceSynchronize());
     // Back up everything a step writes.
@@ -1453,6 +1807,7 @@ bool Engine::autotune(int ticks, float gain, cudaStream_t stream) {
         {d_nstate_, (size_t)n_neurons_ * S_WORDS * 4, nullptr},
         {d_sstate_, (size_t)n_synapses_ * Z_WORDS * 4, nullptr},
         {d_sarrived_, (size_t)n_synapses_, nullptr},
+        {d_slastp_, (size_t)n_synapses_ * 2, nullptr},
         {d_xstate_, (size_t)std::max(n_heavy_, 1) * 16 * 4, nullptr},
         {d_btick_, (size_t)n_brains_ * 8, nullptr},
         {d_output_, (size_t)n_brains_ * outputs_ * 4, nullptr},
@@ -1471,28 +1826,56 @@ bool Engine::autotune(int ticks, float gain, cudaStream_t stream) {
     cudaEvent_t e0, e1;
     NSB_CHECK(cudaEventCreate(&e0));
     NSB_CHECK(cudaEventCreate(&e1));
-    float best = 0;
-    bool best_mode = coop_;
-    const bool original = coop_;
-    for (int mode = 0; mode < 2; ++mode) {
-        coop_ = mode != 0;
-        launch(d_input_, d_mask_, ticks, gain, d_output_, d_status_, s);   // warm-up
-        NSB_CHECK(cudaEventRecord(e0, s));
-        for (int k = 0; k < 3; ++k) launch(d_input_, d_mask_, ticks, gain, d_output_, d_status_, s);
+    const Pools P = pools(count_events_);
+    // Times a bucket alone: one warm-up launch and three timed ones from the
+    // same restored state for every candidate.
+    auto time_bucket = [&](const Bucket &B) {
+        restore();
+        for (int k = 0; k < 4; ++k) {
+            if (k == 1) NSB_CHECK(cudaEventRecord(e0, s));
+            NSB_CHECK(cudaMemsetAsync(d_queue_, 0, 8 * sizeof(int), s));
+            launch_bucket(B, P, d_queue_, d_input_, d_mask_, ticks, gain, d_output_, d_status_, s);
+        }
         NSB_CHECK(cudaEventRecord(e1, s));
         NSB_CHECK(cudaEventSynchronize(e1));
+        NSB_CHECK(cudaGetLastError());
         float ms = 0;
         NSB_CHECK(cudaEventElapsedTime(&ms, e0, e1));
-        if (mode == 0 || ms < best) { best = ms; best_mode = coop_; }
-        restore();
+        return ms;
+    };
+    for (int b = 0; b < kBuckets; ++b) {
+        Bucket &cur = buckets_[b];
+        if (cur.heavy || cur.units() == 0) continue;
+        std::vector<int> caps = {kMetaCap};
+        // a deeper meta stage when the bucket's largest unit has more synapses
+        const int deep = std::min((cur.max_synapses + 31) & ~31, 32768);
+        if (deep > kMetaCap) caps.push_back(deep);
+        std::vector<BucketConfig> cands;
+        for (int block : {256, 128})
+            for (int coop : {0, 1})
+                for (int cap : caps) {
+                    cands.push_back(BucketConfig{block, coop, 1, cap});
+                    if (cur.cluster_size > 1) cands.push_back(BucketConfig{block, coop, cur.cluster_size, cap});
+                }
+        Bucket best = cur;
+        float best_ms = -1.0f;
+        for (const BucketConfig &c : cands) {
+            Bucket B = cur;
+            B.cfg = c;
+            if (!shape_bucket(B)) continue;
+            const float ms = time_bucket(B);
+            if (best_ms < 0 || ms < best_ms) { best_ms = ms; best = B; }
+        }
+        cur = best;
     }
+    restore();
     NSB_CHECK(cudaStreamSynchronize(s));
     for (auto &b : bufs)
         if (b.copy) cudaFree(b.copy);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    coop_ = original;
-    set_cooperative(best_mode);
+    coop_ = cooperative();
+    drop_graphs();
     return coop_;
 }
 

@@ -45,6 +45,30 @@ struct Stats {
     int grid, block, smem_bytes, ctas_per_sm;
 };
 
+// Launch configuration of one bucket of work units.
+struct BucketConfig {
+    int block = 256;         // threads per CTA: 128 or 256 (warps per unit: 4 or 8)
+    int coop = 0;            // warp-cooperative delivery
+    int cluster = 1;         // CTAs per unit: 1, or the bucket's cluster size (big units only)
+    int meta_cap = 6144;     // synapse meta words staged in shared memory per CTA
+};
+
+// Work units of one size class, launched together with one configuration.
+// Buckets, in order: units above 4, 2 and 1 times the unit size (one big
+// brain each; stepped by clusters of 8, 4 and 2 CTAs when clustered), packed
+// units of small brains, and units with LP, Prinz or LFS cells (heavy).
+constexpr int kBuckets = 5;
+constexpr int kBucketHeavy = 4, kBucketPacked = 3;
+struct Bucket {
+    int ub = 0, ue = 0;              // units [ub, ue) in queue order
+    int max_neurons = 0, max_synapses = 0;
+    int cluster_size = 1;            // the cluster a unit of this bucket would use (8, 4, 2), or 1
+    bool heavy = false;
+    BucketConfig cfg;
+    int hw = 8, smem = 0, grid = 0;  // launch shape derived from cfg (grid: CTAs, or clusters)
+    int units() const { return ue - ub; }
+};
+
 class Engine {
 public:
     // Builds device pools for `brains`; throws std::runtime_error on invalid input.
@@ -74,15 +98,24 @@ public:
     // Captures step_device on the engine's own buffers into a CUDA graph and
     // replays it (one graph per (ticks, gain)).
     void step_graph(int ticks, float gain, cudaStream_t stream);
-    // Delivery mode of the light tick kernel: serial per neuron, or
+    // Delivery mode of the light buckets: serial per neuron, or
     // warp-cooperative release (faster for dense, active brains). Both give
-    // identical results. The default is chosen from the synapse density.
-    bool cooperative() const { return coop_; }
+    // identical results. The default is chosen from the synapse density;
+    // set_cooperative sets every light bucket.
+    bool cooperative() const { return buckets_[kBucketPacked].cfg.coop != 0; }
     void set_cooperative(bool coop);
-    // Times both delivery modes on the engine's own buffers (a few steps each,
-    // state restored afterwards, so the call has no visible effect on the
-    // brains) and keeps the faster one. Returns the chosen mode.
+    // Per-bucket autotuner: for each bucket of work units, times candidate
+    // configurations (threads per CTA, delivery mode, meta staging depth, and
+    // one CTA or a cluster for big brains) on the engine's own buffers, a few
+    // launches each with the state restored afterwards (so the call has no
+    // visible effect on the brains), and keeps the fastest. Returns the
+    // packed bucket's delivery mode.
     bool autotune(int ticks, float gain, cudaStream_t stream);
+    // The buckets and their current configurations.
+    const std::vector<Bucket> &buckets() const { return buckets_; }
+    // Sets one bucket's configuration (validated against its units and the
+    // device's shared memory); throws std::runtime_error when it cannot run.
+    void set_bucket(int b, const BucketConfig &cfg);
     // A global modulator pulse: at every tick divisible by `period` (> 0)
     // every neuron's plasticity sees the modulator bits `mod` (1 NE, 2 5-HT,
     // 4 DA) as if a modulatory synapse had released onto it. 0 turns it off.
@@ -113,16 +146,23 @@ private:
                 int *d_status, cudaStream_t stream);
     void launch_groups(const Pools &P, int *queue, const float *d_input, const uint8_t *d_mask, int ticks, float gain,
                        float *d_output, int *d_status, cudaStream_t stream);
+    // One bucket's launch on `stream` (its queue counter already zeroed).
+    void launch_bucket(const Bucket &B, const Pools &P, int *queue, const float *d_input, const uint8_t *d_mask,
+                       int ticks, float gain, float *d_output, int *d_status, cudaStream_t stream) const;
+    // Derives hw, smem and grid from the bucket's configuration; false when
+    // the configuration cannot run on this device.
+    bool shape_bucket(Bucket &B) const;
+    void drop_graphs();
     template <class T> T *alloc(size_t n);
     struct Pools pools(bool events) const;
 
     int n_brains_ = 0, channels_ = 0, outputs_ = 0, max_delay_ = 8;
     int n_neurons_ = 0, n_synapses_ = 0, n_heavy_ = 0, n_units_ = 0, n_big_units_ = 0;
     int max_unit_neurons_ = 0, hw_ = 0, meta_cap_ = 0, max_unit_brains_ = 0, unit_cap_ = 256;
-    int grid_ = 0, grid_heavy_ = 0, block_ = 256, smem_ = 0, ctas_per_sm_ = 0, sms_ = 0, n_light_units_ = 0;
-    // big brains stepped by clusters of 8, 4, 2 CTAs (units first in queue order)
-    int n_cluster_[3] = {0, 0, 0}, clusters_[3] = {0, 0, 0};
-    int hw_small_ = 8, hw_big_ = 8, hw_heavy_ = 8, smem_big_ = 0, smem_heavy_ = 0;
+    int block_ = 256, sms_ = 0, smem_optin_ = 0, ctas_cap_ = 0, n_light_units_ = 0;
+    std::vector<Bucket> buckets_;
+    cudaStream_t bstream_[kBuckets] = {};
+    cudaEvent_t fork_ = nullptr, join_[kBuckets] = {};
     bool count_events_ = true;
     bool coop_ = false;
     int pulse_period_ = 0;

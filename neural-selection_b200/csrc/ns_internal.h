@@ -20,7 +20,7 @@ namespace nsb {
         if (e_ != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e_)); \
     } while (0)
 
-constexpr int kMetaCap = 6144;       // synapse meta words cached in shared memory per unit
+constexpr int kMetaCap = 6144;       // default synapse meta words staged in shared memory per unit
 constexpr int kMaxUnitBrains = 128;  // brains packed into one small unit
 constexpr int kMaxBrainNeurons = 16384;
 
@@ -48,6 +48,10 @@ struct Pools {
     unsigned long long *events;
     int pulse_period;        // > 0: a global modulator pulse at every tick divisible by it
     uint32_t pulse_mod;      // its modulator bits (1 NE, 2 5-HT, 4 DA)
+    // Synapse meta words a CTA stages in shared memory (a unit with more
+    // reads them from global memory); the launch's dynamic shared memory is
+    // sized for it.
+    int meta_cap = kMetaCap;
 };
 
 // Host plan of a set of brains: work units and every pool record, indexed
@@ -90,8 +94,9 @@ PhysConst make_constants();
 
 // Spike-ring words per tick for units of up to max_unit_neurons neurons.
 int spike_words(int max_unit_neurons, int block);
-// Dynamic shared memory of the tick kernel for hw ring words.
-int tick_smem_bytes(int hw);
+// Dynamic shared memory of the light tick kernel for hw ring words and
+// meta_cap staged synapse meta words.
+int tick_smem_bytes(int hw, int meta_cap = kMetaCap);
 // Binds the physiology constants and the tick kernels' shared-memory limit on
 // the current device (idempotent).
 void prepare_tick_kernels(int smem);

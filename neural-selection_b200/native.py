@@ -61,6 +61,8 @@ SIGNATURES = {
     "nsb_gpu_checkpoint_export": (ct.c_int, [_vp, _vp, _vp, _i64]),
     "nsb_gpu_checkpoint_import": (ct.c_int, [_vp, _vp, ct.c_longlong, _vp, ct.c_longlong, _i64]),
     "nsb_gpu_autotune": (ct.c_int, [_vp, ct.c_int, ct.c_float, _vp]),
+    "nsb_gpu_buckets": (ct.c_int, [_vp, _i32]),
+    "nsb_gpu_set_bucket": (ct.c_int, [_vp, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_int]),
     "nsb_compile_genome": (ct.c_int, [ct.c_int, ct.c_int, _f, _f, ct.c_int, _i32, _f, _f, _i32, _u32, _u32, _i32,
                                       _i32]),
     "nsb_world_create": (_vp, [_vp, ct.c_int, ct.c_int]),
@@ -347,11 +349,31 @@ class GpuBatch:
         return bool(v)
 
     def autotune(self, ticks=16, gain=230.0, stream=0):
-        """Time both delivery modes on the batch's own buffers (state restored); keep the faster."""
+        """Per-bucket autotuner: time candidate configurations of every
+        work-unit bucket on the batch's own buffers (state restored) and keep
+        the fastest. Returns the packed bucket's delivery mode."""
         v = self.lib.nsb_gpu_autotune(self.ptr, int(ticks), float(gain), ct.c_void_p(stream))
         if v < 0:
             raise RuntimeError(_err(self.lib))
         return bool(v)
+
+    BUCKETS = ("huge", "large", "big", "packed", "heavy")
+    BUCKET_FIELDS = ("first_unit", "units", "max_neurons", "max_synapses", "block", "cooperative", "cluster",
+                     "meta_cap", "smem_bytes", "grid")
+
+    def buckets(self):
+        """The five work-unit buckets and their launch configurations, as dicts."""
+        out = np.zeros(50, np.int32)
+        n = self.lib.nsb_gpu_buckets(self.ptr, _p(out, _i32))
+        rows = out[:n].reshape(-1, 10)
+        return [dict(name=name, **{f: int(v) for f, v in zip(self.BUCKET_FIELDS, row)})
+                for name, row in zip(self.BUCKETS, rows)]
+
+    def set_bucket(self, bucket, block=256, cooperative=False, cluster=1, meta_cap=6144):
+        """Set one bucket's configuration (RuntimeError when it cannot run)."""
+        if self.lib.nsb_gpu_set_bucket(self.ptr, int(bucket), int(block), 1 if cooperative else 0, int(cluster),
+                                       int(meta_cap)):
+            raise RuntimeError(_err(self.lib))
 
     def close(self):
         if getattr(self, "ptr", None):

@@ -206,6 +206,45 @@ def test_reproduction_with_full_pools_undoes_births(nsb, oracle_built):
     assert (A["alive"] == 0).any() and ((A["alive"] == 1) & (A["energy"] > 55) & (A["generation"] == 0)).any()
 
 
+def _words_for_long_scans(full_words, hints, min_run=300):
+    """A bitmap size in words, above full_words, for which at least three of
+    `hints` (taken modulo the size) start more than min_run full words before
+    the end of the packed run [0, full_words)."""
+    for words in range(full_words + 64, full_words + 4000):
+        if sum((h % words) < full_words - min_run for h in hints) >= 3:
+            return words
+    raise AssertionError("no bitmap size found")
+
+
+def test_births_search_past_the_first_256_candidates(nsb, oracle_built):
+    """Birth searches that need more than one round of 256 candidates (the
+    loops whose exits are decided by __syncthreads_or): 590 living animals in
+    600 slots with only the last ten free, so most parents' drawn starts lie
+    more than 256 live slots before a free one; neuron and synapse slots
+    packed, with pool sizes chosen so that several children's hint words
+    (child*131, child*257) start more than 300 full bitmap words before a
+    free bit. Twelve parents for ten free slots: the last two find no slot.
+    Every pool, bitmap and counter equals the oracle's after each step."""
+    W = nsb.world
+    batch = nsb.workloads.world_founders(seed=91, founders=590, lo=32, hi=40, epn_lo=4, epn_hi=5)
+    seeds = np.arange(batch.brains, dtype=np.uint32) * 3 + 7
+    N, E = int(batch.neuron_offsets[-1]), int(batch.synapse_offsets[-1])
+    children = range(590, 596)
+    nwords = _words_for_long_scans(N // 32, [c * 131 for c in children])
+    swords = _words_for_long_scans(E // 32, [c * 257 for c in children])
+    pools = W.place_population(batch, *W.records_from_gpu(batch, seeds), animal_capacity=600,
+                               neuron_capacity=32 * nwords, synapse_capacity=32 * swords)
+    W.place_bodies(pools, 93)
+    alive = np.nonzero(pools.animals["alive"] == 1)[0]
+    assert len(alive) == 590 and alive.max() == 589
+    pools.animals["id"][alive] = np.arange(len(alive))
+    pools.animals["energy"][alive[::49][:12]] = 100.0
+    eco = W.make_ecology(pools, seed=5, initial_count=0, life_capacity=64)
+    ref, ref_eco = _closed_loop(nsb, pools, eco, 2, seed=5, renewal=0.0, label="long searches", births=True)
+    assert ref_eco.births[0] == 10                         # every free slot filled, two parents without one
+    assert (ref.animals["alive"] == 1).sum() == 600
+
+
 def test_ecology_reports_bad_lists(nsb):
     """A dead animal whose neuron list is shorter than its count: reclamation
     walks the list (at most count + 1 entries) and reports it."""
