@@ -675,15 +675,17 @@ def run_serve(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
-def world_population(nsb, population, founders=2048, compact=False, scatter=None):
+def world_population(nsb, population, founders=2048, compact=False, scatter=None, heavy=False):
     """World pools at the reference build's capacities (32,768 animals,
     4,194,304 neuron and 8,388,608 synapse slots). "founders": 2,048 founders
-    of 32-96 neurons with 4-12 synapses per neuron (config 2); "full": the
+    of 32-96 neurons with 4-12 synapses per neuron (config 2; with `heavy`,
+    3 % each of the hidden excitatory neurons are LP, Prinz and LFS cells, as
+    mutation makes them, so nearly every animal carries one); "full": the
     full-pool batched-uneven population as animals (delays folded into the
     world's 1-8 ms ring, its 8 input channels as world senses 0-7)."""
     W = nsb.world
     if population == "founders":
-        batch = nsb.workloads.world_founders(seed=2, founders=founders)
+        batch = nsb.workloads.world_founders(seed=2, founders=founders, heavy_types=heavy)
     else:
         full = workload(nsb, 2)
         sr = full.synapse_rows.copy()
@@ -716,7 +718,8 @@ def run_world_stage(args, rank, world, local_rank):
     sys.path.insert(0, str(ROOT))
     nsb = load_package()
     W = nsb.world
-    batch, pools = world_population(nsb, args.world_population, args.world_founders, args.world_compact)
+    batch, pools = world_population(nsb, args.world_population, args.world_founders, args.world_compact,
+                                    heavy=args.world_heavy)
     N, E, B = int(batch.neuron_offsets[-1]), int(batch.synapse_offsets[-1]), batch.brains
     stage = W.World(pools)
     counter = [0]
@@ -860,7 +863,8 @@ def run_world_loop(args, rank, world, local_rank):
     # slots spread over the pools, as the simulator's hinted claims spread them
     # (init_animals, src/main.cu:547-611); packed slots would make every
     # claim_slot scan long runs of full bitmap words
-    batch, pools = world_population(nsb, args.world_population, args.world_founders, False, scatter=3)
+    batch, pools = world_population(nsb, args.world_population, args.world_founders, False, scatter=3,
+                                    heavy=args.world_heavy)
     W.place_bodies(pools, 3)
     if args.world_parents > 0:                    # a fraction of well-fed animals: births every step
         live = np.nonzero(pools.animals["alive"] == 1)[0]
@@ -1024,6 +1028,8 @@ def main():
                     help="pools sized to the population, no reference leg (profiler captures)")
     ap.add_argument("--world-parents", type=float, default=0.0,
                     help="--world-loop: fraction of founders given energy 200 (they reproduce every step)")
+    ap.add_argument("--world-heavy", action="store_true",
+                    help="--world / --world-loop founders with LP, Prinz and LFS cells (3 %% each of hidden cells)")
     ap.add_argument("--world-loop", action="store_true",
                     help="the world step: neural stage + ecology with reproduction, closed loop")
     args = ap.parse_args()

@@ -139,8 +139,9 @@ int nsb_gpu_set_delivery(void *batch, int cooperative);
  * kernels' size tiers at compile time (src/main.cu:49-52). Per-bucket
  * autotuner: for each bucket of work units (see nsb_gpu_buckets) it times
  * candidate configurations (threads per CTA 128/256, serial or cooperative
- * delivery, shared-memory staging depth of the synapse meta words, one CTA
- * or a thread-block cluster per big brain) on the batch's own buffers, a few
+ * delivery, shared-memory staging depth of the synapse meta words, list or
+ * per-thread integration, one CTA or a thread-block cluster per big brain)
+ * on the batch's own buffers, a few
  * launches each with the state restored afterwards, and keeps the fastest.
  * Results are identical under every configuration. Returns the packed
  * bucket's delivery mode (1 cooperative), or -1. */
@@ -148,16 +149,19 @@ int nsb_gpu_autotune(void *batch, int ticks, float gain, void *stream);
 /* No counterpart in the reference. The batch's five work-unit buckets, in
  * order: units above 4, 2 and 1 times the unit size (one big brain each),
  * packed units of small brains, units with LP, Prinz or LFS cells. For each,
- * 10 ints: first unit, units, neurons and synapses of its largest unit,
+ * 11 ints: first unit, units, neurons and synapses of its largest unit,
  * threads per CTA, cooperative delivery, CTAs per unit (1, or the cluster
- * size 8, 4 or 2), staged synapse meta words, dynamic shared memory bytes,
- * grid (CTAs, or clusters). Returns the count written (50). */
+ * size 8, 4 or 2), staged synapse meta words, list integration (1: the
+ * neurons that need integrating are gathered into a per-tick list and
+ * integrated at full warp width; 0: each thread integrates its own),
+ * dynamic shared memory bytes, grid (CTAs, or clusters). Returns the count
+ * written (55). */
 int nsb_gpu_buckets(void *batch, int *out);
 /* No counterpart in the reference. Sets one bucket's configuration: block
  * 128 or 256, cooperative 0/1, cluster 1 or the bucket's cluster size,
- * meta_cap a multiple of 32. Returns 0, or -1 when it cannot run (ns_error
- * says why). */
-int nsb_gpu_set_bucket(void *batch, int bucket, int block, int cooperative, int cluster, int meta_cap);
+ * meta_cap a multiple of 32, list 0/1 (one-CTA light units only; 1 for the
+ * heavy bucket). Returns 0, or -1 when it cannot run (ns_error says why). */
+int nsb_gpu_set_bucket(void *batch, int bucket, int block, int cooperative, int cluster, int meta_cap, int list);
 
 /* Replaces compile_genome (gym_adapter/compile_graph.py:10-28), which the
  * reference's SpikingPolicy applies before ns_create (gym_adapter/adapter.py:197-210):

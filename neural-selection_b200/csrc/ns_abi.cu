@@ -599,18 +599,18 @@ int nsb_gpu_buckets(void *p, int *out) {
     const auto &bs = static_cast<GpuBatch *>(p)->engine->buckets();
     int k = 0;
     for (const Bucket &B : bs) {
-        const int v[10] = {B.ub, B.units(), B.max_neurons, B.max_synapses, B.cfg.block, B.cfg.coop, B.cfg.cluster,
-                           B.cfg.meta_cap, B.smem, B.grid};
+        const int v[11] = {B.ub, B.units(), B.max_neurons, B.max_synapses, B.cfg.block, B.cfg.coop, B.cfg.cluster,
+                           B.cfg.meta_cap, B.cfg.list, B.smem, B.grid};
         std::memcpy(out + k, v, sizeof v);
-        k += 10;
+        k += 11;
     }
     return k;
 }
 
-int nsb_gpu_set_bucket(void *p, int bucket, int block, int cooperative, int cluster, int meta_cap) {
+int nsb_gpu_set_bucket(void *p, int bucket, int block, int cooperative, int cluster, int meta_cap, int list) {
     try {
         static_cast<GpuBatch *>(p)->engine->set_bucket(bucket, BucketConfig{block, cooperative ? 1 : 0, cluster,
-                                                                             meta_cap});
+                                                                             meta_cap, list});
         return 0;
     } catch (const std::exception &e) {
         g_error = e.what();

@@ -476,7 +476,11 @@ __global__ void __launch_bounds__(256, HEAVY ? 1 : NSB_MIN_CTAS) tick_kernel(Poo
                     // The warp's LP and Prinz cells, one after another, each on all 32 lanes.
                     float axon_before = 0.0f;
                     bool spiked = false;
-                    for (uint32_t pm = __ballot_sync(0xffffffffu, pending); pm; pm &= pm - 1u) {
+                    const uint32_t pend = __ballot_sync(0xffffffffu, pending);
+                    if (__popc(pend) > kWarpCellsMax && pending)
+                        axon_before = heavy_model_lane(type, P.xstate + (size_t)xidx * 16, P.xgene + (size_t)xidx * 16,
+                                                       ext, spiked, tab);
+                    for (uint32_t pm = __popc(pend) > kWarpCellsMax ? 0u : pend; pm; pm &= pm - 1u) {
                         const int L = __ffs(pm) - 1;
                         const int xi = __shfl_sync(0xffffffffu, xidx, L);
                         const uint32_t ty = __shfl_sync(0xffffffffu, type, L);
@@ -1066,6 +1070,8 @@ static void set_tick_smem(int) {
     NSB_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     allow_dynamic_smem(tick_kernel_list<false>, optin);
     allow_dynamic_smem(tick_kernel_list<true>, optin);
+    allow_dynamic_smem(tick_kernel<false, false>, optin);
+    allow_dynamic_smem(tick_kernel<false, true>, optin);
     allow_dynamic_smem(tick_kernel<true, false>, optin);
     allow_dynamic_smem(tick_kernel_cluster<false>, optin);
     allow_dynamic_smem(tick_kernel_cluster<true>, optin);
@@ -1589,7 +1595,8 @@ bool Engine::shape_bucket(Bucket &B) const {
     const BucketConfig &c = B.cfg;
     if (c.block != 128 && c.block != 256) return false;
     if (c.meta_cap < 0 || c.meta_cap % 32 != 0) return false;
-    if (B.heavy && (c.coop || c.cluster != 1)) return false;
+    if (B.heavy && (c.coop || c.cluster != 1 || !c.list)) return false;
+    if (c.list != 0 && c.list != 1) return false;
     if (c.cluster != 1 && c.cluster != B.cluster_size) return false;
     B.hw = spike_words(B.max_neurons, c.block);
     if (B.units() == 0) {
@@ -1604,6 +1611,13 @@ bool Engine::shape_bucket(Bucket &B) const {
     } else if (c.cluster > 1) {
         B.smem = cluster_smem_bytes(B.hw, c.meta_cap);
         B.grid = B.smem <= smem_optin_ ? std::min(B.units(), clusters_resident(c.cluster, c.block, B.smem)) : 0;
+    } else if (!c.list) {
+        B.smem = heavy_smem_bytes(B.hw, c.meta_cap);
+        int occ = B.smem <= smem_optin_ ? std::min(ctas_resident(tick_kernel<false, false>, c.block, B.smem),
+                                                   ctas_resident(tick_kernel<false, true>, c.block, B.smem))
+                                        : 0;
+        if (ctas_cap_ > 0) occ = std::min(occ, ctas_cap_);
+        B.grid = std::min(B.units(), sms_ * occ);
     } else {
         B.smem = tick_smem_bytes(B.hw, c.meta_cap);
         int occ = B.smem <= smem_optin_ ? std::min(ctas_resident(tick_kernel_list<false>, c.block, B.smem),
@@ -1655,6 +1669,12 @@ void Engine::launch_bucket(const Bucket &B, const Pools &P0, int *queue, const f
     else if (B.cfg.cluster > 1)
         launch_cluster(B.cfg.coop != 0, B.cfg.cluster, B.grid, B.cfg.block, B.smem, stream, P, B.ub, B.ue, queue,
                        d_input, d_mask, d_output, d_status, ticks, gain);
+    else if (!B.cfg.list && B.cfg.coop)
+        tick_kernel<false, true><<<B.grid, B.cfg.block, B.smem, stream>>>(P, B.ub, B.ue, queue, d_input, d_mask,
+                                                                           d_output, d_status, ticks, gain);
+    else if (!B.cfg.list)
+        tick_kernel<false, false><<<B.grid, B.cfg.block, B.smem, stream>>>(P, B.ub, B.ue, queue, d_input, d_mask,
+                                                                            d_output, d_status, ticks, gain);
     else
         launch_light(B.cfg.coop != 0, B.grid, B.cfg.block, B.smem, stream, P, B.ub, B.ue, queue, d_input, d_mask,
                      d_output, d_status, ticks, gain);
@@ -1846,16 +1866,18 @@ bool Engine::autotune(int ticks, float gain, cudaStream_t stream) {
     for (int b = 0; b < kBuckets; ++b) {
         Bucket &cur = buckets_[b];
         if (cur.heavy || cur.units() == 0) continue;
+        // staging depths: the default, and exactly the bucket's largest unit
+        // (less shared memory per CTA, or no global meta reads)
         std::vector<int> caps = {kMetaCap};
-        // a deeper meta stage when the bucket's largest unit has more synapses
-        const int deep = std::min((cur.max_synapses + 31) & ~31, 32768);
-        if (deep > kMetaCap) caps.push_back(deep);
+        const int fit = std::min((cur.max_synapses + 31) & ~31, 32768);
+        if (fit != kMetaCap) caps.push_back(fit);
         std::vector<BucketConfig> cands;
         for (int block : {256, 128})
             for (int coop : {0, 1})
                 for (int cap : caps) {
-                    cands.push_back(BucketConfig{block, coop, 1, cap});
-                    if (cur.cluster_size > 1) cands.push_back(BucketConfig{block, coop, cur.cluster_size, cap});
+                    cands.push_back(BucketConfig{block, coop, 1, cap, 1});
+                    cands.push_back(BucketConfig{block, coop, 1, cap, 0});
+                    if (cur.cluster_size > 1) cands.push_back(BucketConfig{block, coop, cur.cluster_size, cap, 1});
                 }
         Bucket best = cur;
         float best_ms = -1.0f;

@@ -51,6 +51,10 @@ struct BucketConfig {
     int coop = 0;            // warp-cooperative delivery
     int cluster = 1;         // CTAs per unit: 1, or the bucket's cluster size (big units only)
     int meta_cap = 6144;     // synapse meta words staged in shared memory per CTA
+    // One-CTA light units: 1 integrates from a per-tick list of the neurons
+    // that need it (full warps), 0 lets each thread integrate its own neurons
+    // (one barrier per tick).
+    int list = 1;
 };
 
 // Work units of one size class, launched together with one configuration.

@@ -279,62 +279,80 @@ static __device__ __noinline__ NeuronRegs heavy_tick(const float *g, uint32_t ty
 }
 
 // ---- LP and Prinz cells on a whole warp ------------------------------------------
-// The same arithmetic as lp_integrate and pz_substep, spread over the 32 lanes
-// of a warp: every exponential (and the one logarithm) of a derivative
-// evaluation is computed by its own lane from the same operands in the same
-// order, and each state component is then assembled by one lane exactly as
-// the one-thread code assembles it. Each value is produced by the same binary32
-// operations as there, so the results are identical bit for bit; the latency
-// of an evaluation drops from some twenty dependent exponentials to one or
-// two. All 32 lanes call these functions together (converged); w is the
-// warp's 48-float shared-memory scratch.
+// The same arithmetic as lp_integrate and pz_substep, spread over the 32
+// lanes of a warp. Each exponential (and the one logarithm) of a derivative
+// evaluation is computed by a lane of its own from the same operands in the
+// same order, and each state component is then assembled by one lane exactly
+// as the one-thread code assembles it, so the results are identical bit for
+// bit. The exponentials' operands are formed by code that is the same for
+// every lane, from per-lane constants (forms below), so the 20-odd
+// exponentials of an evaluation run at once instead of one after another.
+// All 32 lanes call these functions together (converged); w is the warp's
+// kHeavyWarpScratch floats of shared memory.
 constexpr int kHeavyWarpScratch = 48;
 
-// lp_rates on the state y (w[0..15]) for lanes 0..15: returns d[lane].
-__device__ __forceinline__ float lp_rate_warp(const float *y, float i_na, const float *sc, float *T, int lane,
-                                              const float *tab) {
-    const float va = y[0], vs = y[15], cai = y[13];
-    float t = 0.0f;
-    switch (lane) {   // the transcendental terms, one per lane
-    case 0: t = crexp(vs / 11.4866f, tab); break;
-    case 1: t = lp_sig(vs, 55.0f, -15.0f, tab); break;
-    case 2: t = crexp(-13.0f - va / 4.0f, tab); break;
-    case 3: t = crexp(va / 5.0f + 5.0f, tab); break;
-    case 4: t = crexp(-2.66666666667f - va / 18.0f, tab); break;
-    case 5: t = crexp(-5.0f - va / 5.0f, tab); break;
-    case 6: t = crexp(-10.0f - va / 5.0f, tab); break;
-    case 7: t = crexp(-1.375f - va / 40.0f, tab); break;
-    case 8: t = lp_sig(vs, 15.0f, -9.8f, tab); break;
-    case 9: t = lp_sig(vs, -40.0f, 3.2f, tab); break;
-    case 10: t = lp_sig(vs, -15.0f, -10.0f, tab); break;
-    case 11: t = lp_sig(vs, 29.1336f, -4.43083f, tab); break;
-    case 12: t = lp_sig(vs, -.6f * cai, -23.0f, tab); break;
-    case 13: t = lp_sig(vs, -16.0f - .6f * cai, -5.0f, tab); break;
-    case 14: t = lp_sig(vs, -12.0f, -26.0f, tab); break;
-    case 15: t = lp_sig(vs, -62.0f, 6.0f, tab); break;
-    case 16: t = lp_sig(vs, -40.0f, -12.0f, tab); break;
-    case 17: t = lp_sig(vs, -70.0f, 8.0f, tab); break;
-    case 18: t = lp_sig(vs, -110.0f, -21.6f, tab); break;
-    case 19: t = lp_sig(va, -26.9916223f, -5.957441281f, tab); break;
-    case 20: t = lp_sig(va, -60.57875745f, -13.25674673f, tab); break;
-    default: break;
+// Operand forms of a lane's exponential: x is the lane's voltage, m, k, c its
+// constants. LP: A (x - m) / k; B c - x / k; C x / k + c; D x / k.
+// Prinz: G (x + m) / k; P c - k * x; Q c + k * x.
+enum : int { F_A = 0, F_B, F_C, F_D, F_G, F_P, F_Q };
+struct LaneTerm {
+    int form;
+    float m, k, c;
+    int sig;       // 1: 1 / (1 + e) (the model's sigmoid gates)
+    int use_va;    // LP: the axon voltage instead of the soma's
+};
+
+// The lane's exponential term of an LP derivative evaluation (lp_rates).
+__device__ __forceinline__ LaneTerm lp_term(int lane) {
+    switch (lane) {
+    case 0: return {F_D, 0.0f, 11.4866f, 0.0f, 0, 0};
+    case 1: return {F_A, 55.0f, -15.0f, 0.0f, 1, 0};
+    case 2: return {F_B, 0.0f, 4.0f, -13.0f, 0, 1};
+    case 3: return {F_C, 0.0f, 5.0f, 5.0f, 0, 1};
+    case 4: return {F_B, 0.0f, 18.0f, -2.66666666667f, 0, 1};
+    case 5: return {F_B, 0.0f, 5.0f, -5.0f, 0, 1};
+    case 6: return {F_B, 0.0f, 5.0f, -10.0f, 0, 1};
+    case 7: return {F_B, 0.0f, 40.0f, -1.375f, 0, 1};
+    case 8: return {F_A, 15.0f, -9.8f, 0.0f, 1, 0};
+    case 9: return {F_A, -40.0f, 3.2f, 0.0f, 1, 0};
+    case 10: return {F_A, -15.0f, -10.0f, 0.0f, 1, 0};
+    case 11: return {F_A, 29.1336f, -4.43083f, 0.0f, 1, 0};
+    case 12: return {F_A, 0.0f, -23.0f, 0.0f, 1, 0};     // mid -.6 * cai
+    case 13: return {F_A, 0.0f, -5.0f, 0.0f, 1, 0};      // mid -16 - .6 * cai
+    case 14: return {F_A, -12.0f, -26.0f, 0.0f, 1, 0};
+    case 15: return {F_A, -62.0f, 6.0f, 0.0f, 1, 0};
+    case 16: return {F_A, -40.0f, -12.0f, 0.0f, 1, 0};
+    case 17: return {F_A, -70.0f, 8.0f, 0.0f, 1, 0};
+    case 18: return {F_A, -110.0f, -21.6f, 0.0f, 1, 0};
+    case 19: return {F_A, -26.9916223f, -5.957441281f, 0.0f, 1, 1};
+    case 20: return {F_A, -60.57875745f, -13.25674673f, 0.0f, 1, 1};
+    default: return {F_D, 0.0f, 1.0f, 0.0f, 0, 0};       // idle lanes
     }
-    T[lane] = t;
+}
+
+// lp_rates on the state y (16 floats) for lanes 0..15: returns d[lane].
+__device__ __forceinline__ float lp_rate_warp(const float *y, float i_na, const float *sc, float *T, int lane,
+                                              const LaneTerm &q, const float *tab) {
+    const float va = y[0], vs = y[15], cai = y[13];
+    {   // every lane: one exponential, formed the same way in every lane
+        const float x = q.use_va ? va : vs;
+        const float m = lane == 12 ? -.6f * cai : lane == 13 ? -16.0f - .6f * cai : q.m;
+        const float r = (q.form == F_A ? x - m : x) / q.k;
+        const float arg = q.form == F_B ? q.c - r : q.form == F_C ? r + q.c : r;
+        const float e = crexp(arg, tab);
+        T[lane] = q.sig ? 1.0f / (1.0f + e) : e;
+    }
     __syncwarp();
     const float *x = y;
-    float d = 0.0f, a, b;
-    switch (lane) {   // the derivative components, one per lane
-    case 0: {
+    float d = 0.0f;
+    if (lane == 0) {
         const float na = x[1] * x[1] * x[1] * x[2] * 7.15f * (va - 50.0f);
         const float kd = x[8] * x[8] * x[8] * x[8] * 1.43f * (va + 72.0f);
         const float km = .2613041227f * x[14] * (va + 80.0f);
         const float aleak = sc[3] * .001004288227f * (va + 50.0f);
         const float cpl = .004017089073f * (vs - va);
         d = (-na - kd - km - aleak + cpl) / .1148312178f;
-        break;
-    }
-    case 13:
-    case 15: {
+    } else if (lane == 13 || lane == 15) {
         const float ev = T[0];
         const float ghk = fabsf(vs) < .001f ? 11.4866f * (x[13] - 15123.5f) : vs * (x[13] * ev - 15123.5f) / (ev - 1.0f);
         const float ca = sc[0] * (x[3] * x[4] * .1247796343f + x[5] * .07142141077f) * .00155982f * ghk * .9f;
@@ -349,34 +367,30 @@ __device__ __forceinline__ float lp_rate_warp(const float *y, float i_na, const 
             const float sleak = sc[3] * .0006901584324f * (vs + 50.0f);
             d = (-ca - kca - ka - ih - sleak - cpl + (i_na - 2.0f) * .01222505828f) / .0543909161f;
         }
-        break;
-    }
-    case 1:
-        a = lp_ratio(-16.64f - .32f * va, T[2] - 1.0f, 1.28f);
-        b = lp_ratio(.28f * va + 7.0f, T[3] - 1.0f, 1.4f);
-        d = a * (1.0f - x[1]) - b * x[1];
-        break;
-    case 2:
-        a = .128f * T[4];
-        b = 4.0f / (T[5] + 1.0f);
-        d = a * (1.0f - x[2]) - b * x[2];
-        break;
-    case 8:
-        a = lp_ratio(-1.6f - .032f * va, T[6] - 1.0f, .16f);
-        b = .5f * T[7];
-        d = a * (1.0f - x[8]) - b * x[8];
-        break;
-    case 3: d = (T[8] - x[3]) * .045f; break;
-    case 4: d = (T[9] - x[4]) * .02f * T[10]; break;
-    case 5: d = (T[11] - x[5]) * .0608644f; break;
-    case 6: d = (T[12] * T[13] * cai / (2.5f + cai) - x[6]) * .6f; break;
-    case 7: d = (.7f / (.6f + cai) - x[7]) * .035f; break;
-    case 9: d = (T[14] - x[9]) * .14f; break;
-    case 10: d = (T[15] - x[10]) * .05f; break;
-    case 11: d = (T[15] - x[11]) * .0036f * T[16]; break;
-    case 12: d = (T[17] - x[12]) * .00033f / T[18]; break;
-    case 14: d = (T[19] - x[14]) * .0001386796618f * T[20]; break;
-    default: break;
+    } else if (lane == 1 || lane == 2 || lane == 8) {
+        float a, b;
+        if (lane == 1) {
+            a = lp_ratio(-16.64f - .32f * va, T[2] - 1.0f, 1.28f);
+            b = lp_ratio(.28f * va + 7.0f, T[3] - 1.0f, 1.4f);
+        } else if (lane == 2) {
+            a = .128f * T[4];
+            b = 4.0f / (T[5] + 1.0f);
+        } else {
+            a = lp_ratio(-1.6f - .032f * va, T[6] - 1.0f, .16f);
+            b = .5f * T[7];
+        }
+        d = a * (1.0f - x[lane]) - b * x[lane];
+    } else if (lane < 16) {
+        // gating variables: ((A - x) * k) [* or / B]
+        const int ia = lane == 3 ? 8 : lane == 4 ? 9 : lane == 5 ? 11 : lane == 9 ? 14 : lane == 10 ? 15
+                       : lane == 11 ? 15 : lane == 12 ? 17 : 19;
+        const float A = lane == 6 ? T[12] * T[13] * cai / (2.5f + cai) : lane == 7 ? .7f / (.6f + cai) : T[ia];
+        const float k = lane == 3 ? .045f : lane == 4 ? .02f : lane == 5 ? .0608644f : lane == 6 ? .6f
+                        : lane == 7 ? .035f : lane == 9 ? .14f : lane == 10 ? .05f : lane == 11 ? .0036f
+                        : lane == 12 ? .00033f : .0001386796618f;
+        d = (A - x[lane]) * k;
+        if (lane == 4 || lane == 11 || lane == 14) d = d * T[lane == 4 ? 10 : lane == 11 ? 16 : 20];
+        else if (lane == 12) d = d / T[18];
     }
     __syncwarp();
     return d;
@@ -384,24 +398,24 @@ __device__ __forceinline__ float lp_rate_warp(const float *y, float i_na, const 
 
 // lp_integrate on x (16 floats, any memory the warp can read and write).
 static __device__ __noinline__ void lp_integrate_warp(float *x, float i_na, const float *sc, float *w, int lane,
-                                               const float *tab) {
+                                                      const float *tab) {
     const float dt = .05f;
     float *y = w, *T = w + 16;
-    const float xj0 = lane < 16 ? x[lane] : 0.0f;
-    float xj = xj0;
+    const LaneTerm q = lp_term(lane);
+    float xj = lane < 16 ? x[lane] : 0.0f;
     if (lane < 16) y[lane] = xj;
     __syncwarp();
     for (int step = 0; step < 20; ++step) {
-        const float k1 = lp_rate_warp(y, i_na, sc, T, lane, tab);
+        const float k1 = lp_rate_warp(y, i_na, sc, T, lane, q, tab);
         if (lane < 16) y[lane] = xj + .5f * dt * k1;
         __syncwarp();
-        const float k2 = lp_rate_warp(y, i_na, sc, T, lane, tab);
+        const float k2 = lp_rate_warp(y, i_na, sc, T, lane, q, tab);
         if (lane < 16) y[lane] = xj + .5f * dt * k2;
         __syncwarp();
-        const float k3 = lp_rate_warp(y, i_na, sc, T, lane, tab);
+        const float k3 = lp_rate_warp(y, i_na, sc, T, lane, q, tab);
         if (lane < 16) y[lane] = xj + dt * k3;
         __syncwarp();
-        const float k4 = lp_rate_warp(y, i_na, sc, T, lane, tab);
+        const float k4 = lp_rate_warp(y, i_na, sc, T, lane, q, tab);
         xj += dt * (k1 + 2 * k2 + 2 * k3 + k4) / 6.0f;
         if (lane < 16) y[lane] = xj;
         __syncwarp();
@@ -410,77 +424,110 @@ static __device__ __noinline__ void lp_integrate_warp(float *x, float i_na, cons
     __syncwarp();
 }
 
-// One pz_substep on u (w[0..12]: v, ca, m[7], h[4]); returns nothing, u is
-// updated in place. T = w + 16 holds the lanes' transcendental terms.
+// The lane's exponential term of a Prinz substep (pz_substep), level 1 (all
+// from the voltage v): gates mi[0..6] (lanes 1-7), the time constants
+// mt[0..6] (8-16, the two-exponential ones split over two lanes each), gates
+// hi[0..3] (17-20) and the time constants ht[0..3] (21-26). Lane 0 takes the
+// logarithm of the calcium reversal. post: 0 none, 1 K1 - K2 g, 2 the
+// calcium factor of mi[4].
+struct PzTerm {
+    LaneTerm t;
+    int post;
+    float k1, k2;
+};
+__device__ __forceinline__ PzTerm pz_term(int lane) {
+    switch (lane) {
+    case 1: return {{F_G, 25.5f, -5.29f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
+    case 2: return {{F_G, 27.1f, -7.2f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
+    case 3: return {{F_G, 33.0f, -8.1f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
+    case 4: return {{F_G, 27.2f, -8.7f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
+    case 5: return {{F_G, 28.3f, -12.6f, 0.0f, 1, 0}, 2, 0.0f, 0.0f};
+    case 6: return {{F_G, 12.3f, -11.8f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
+    case 7: return {{F_G, 75.0f, 5.5f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
+    case 8: return {{F_G, 120.0f, -25.0f, 0.0f, 1, 0}, 1, 2.64f, 2.52f};
+    case 9: return {{F_G, 68.1f, -20.5f, 0.0f, 1, 0}, 1, 43.4f, 42.6f};
+    case 10: return {{F_G, 27.0f, 10.0f, 0.0f, 0, 0}, 0, 0.0f, 0.0f};
+    case 11: return {{F_G, 70.0f, -13.0f, 0.0f, 0, 0}, 0, 0.0f, 0.0f};
+    case 12: return {{F_G, 32.9f, -15.2f, 0.0f, 1, 0}, 1, 23.2f, 20.8f};
+    case 13: return {{F_G, 46.0f, -22.7f, 0.0f, 1, 0}, 1, 180.6f, 150.2f};
+    case 14: return {{F_G, 28.3f, -19.2f, 0.0f, 1, 0}, 1, 14.4f, 12.8f};
+    case 15: return {{F_P, 0.0f, .086f, -14.59f, 0, 0}, 0, 0.0f, 0.0f};
+    case 16: return {{F_Q, 0.0f, .0701f, -1.87f, 0, 0}, 0, 0.0f, 0.0f};
+    case 17: return {{F_G, 48.9f, 5.18f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
+    case 18: return {{F_G, 32.1f, 5.5f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
+    case 19: return {{F_G, 60.0f, 6.2f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
+    case 20: return {{F_G, 56.9f, 4.9f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
+    case 21: return {{F_G, 62.9f, -10.0f, 0.0f, 0, 0}, 0, 0.0f, 0.0f};
+    case 22: return {{F_G, 34.9f, 3.6f, 0.0f, 0, 0}, 0, 0.0f, 0.0f};
+    case 23: return {{F_G, 55.0f, -16.9f, 0.0f, 1, 0}, 1, 210.0f, 179.6f};
+    case 24: return {{F_G, 55.0f, 9.0f, 0.0f, 0, 0}, 0, 0.0f, 0.0f};
+    case 25: return {{F_G, 65.0f, -16.0f, 0.0f, 0, 0}, 0, 0.0f, 0.0f};
+    case 26: return {{F_G, 38.9f, -26.5f, 0.0f, 1, 0}, 1, 77.2f, 58.4f};
+    default: return {{F_G, 0.0f, 1.0f, 0.0f, 0, 0}, 0, 0.0f, 0.0f};   // lane 0 and idle lanes
+    }
+}
+
+// One pz_substep on u (13 floats: v, ca, m[7], h[4]) in shared memory; T
+// holds the lanes' level-1 terms.
 __device__ __forceinline__ void pz_substep_warp(float *u, const float *g, float ext, float clamp_ns, float clamp_rev,
-                                                float *T, int lane, const float *tab) {
+                                                float *T, int lane, const PzTerm &q, const float *tab) {
     const float dt = .025f;
     const float *m = u + 2, *h = u + 9;
     const float v = u[0], ca = fmaxf(u[1], 0.000001f);
-    float t = 0.0f;
-    switch (lane) {
-    case 0: t = nsx::logf_cr(3000.0f / ca); break;
-    case 1: t = pz_gate(v, 25.5f, -5.29f, tab); break;
-    case 2: t = pz_gate(v, 27.1f, -7.2f, tab); break;
-    case 3: t = pz_gate(v, 33, -8.1f, tab); break;
-    case 4: t = pz_gate(v, 27.2f, -8.7f, tab); break;
-    case 5: t = (ca / (ca + 3)) * pz_gate(v, 28.3f, -12.6f, tab); break;
-    case 6: t = pz_gate(v, 12.3f, -11.8f, tab); break;
-    case 7: t = pz_gate(v, 75, 5.5f, tab); break;
-    case 8: t = 2.64f - 2.52f * pz_gate(v, 120, -25, tab); break;
-    case 9: t = 43.4f - 42.6f * pz_gate(v, 68.1f, -20.5f, tab); break;
-    case 10: t = crexp((v + 27) / 10, tab); break;
-    case 11: t = crexp((v + 70) / -13, tab); break;
-    case 12: t = 23.2f - 20.8f * pz_gate(v, 32.9f, -15.2f, tab); break;
-    case 13: t = 180.6f - 150.2f * pz_gate(v, 46, -22.7f, tab); break;
-    case 14: t = 14.4f - 12.8f * pz_gate(v, 28.3f, -19.2f, tab); break;
-    case 15: t = crexp(-14.59f - .086f * v, tab); break;
-    case 16: t = crexp(-1.87f + .0701f * v, tab); break;
-    case 17: t = pz_gate(v, 48.9f, 5.18f, tab); break;
-    case 18: t = pz_gate(v, 32.1f, 5.5f, tab); break;
-    case 19: t = pz_gate(v, 60, 6.2f, tab); break;
-    case 20: t = pz_gate(v, 56.9f, 4.9f, tab); break;
-    case 21: t = crexp((v + 62.9f) / -10, tab); break;
-    case 22: t = crexp((v + 34.9f) / 3.6f, tab); break;
-    case 23: t = 210 - 179.6f * pz_gate(v, 55, -16.9f, tab); break;
-    case 24: t = crexp((v + 55) / 9, tab); break;
-    case 25: t = crexp((v + 65) / -16, tab); break;
-    case 26: t = 77.2f - 58.4f * pz_gate(v, 38.9f, -26.5f, tab); break;
-    default: break;
+    {   // level 1: one exponential per lane, formed the same way in every lane
+        const float p = q.t.form == F_G ? v + q.t.m : q.t.k * v;
+        const float arg = q.t.form == F_P ? q.t.c - p : q.t.form == F_Q ? q.t.c + p : p / q.t.k;
+        const float e = crexp(arg, tab);
+        float t = q.t.sig ? 1.0f / (1.0f + e) : e;
+        if (q.post == 1) t = q.k1 - q.k2 * t;
+        else if (q.post == 2) t = (ca / (ca + 3)) * t;
+        if (lane == 0) t = nsx::logf_cr(3000.0f / ca);
+        T[lane] = t;
     }
-    T[lane] = t;
     __syncwarp();
-    float nv = 0.0f, nca = 0.0f;
+    // level 2: the voltage and calcium (lane 0), m[i] (lanes 2-8) and h[i]
+    // (lanes 9-12), one exponential each
+    float arg = 0.0f, gt = 0.0f, ws = 0.0f, eca = 0.0f, c1 = 0.0f, c2 = 0.0f, base = 0.0f, cur = 0.0f;
     if (lane == 0) {
-        const float eca = (8.31451e3f * 283.0f / (2.0f * 96485.3415f)) * T[0];
+        eca = (8.31451e3f * 283.0f / (2.0f * 96485.3415f)) * T[0];
         const float c[8] = {g[0] * m[0] * m[0] * m[0] * h[0], g[1] * m[1] * m[1] * m[1] * h[1],
                             g[2] * m[2] * m[2] * m[2] * h[2], g[3] * m[3] * m[3] * m[3] * h[3],
                             g[4] * m[4] * m[4] * m[4] * m[4], g[5] * m[5] * m[5] * m[5] * m[5],
                             g[6] * m[6], g[7]};
         const float rev[8] = {50, eca, eca, -80, -80, -80, -20, -50};
-        float gt = clamp_ns, ws = ext + clamp_ns * clamp_rev;
+        gt = clamp_ns;
+        ws = ext + clamp_ns * clamp_rev;
         for (int i = 0; i < 8; ++i) { gt += c[i]; ws += c[i] * rev[i]; }
+        c1 = c[1];
+        c2 = c[2];
+        arg = -dt * gt / 628.3f;
+    } else if (lane >= 2 && lane < 13) {
+        const bool mg = lane < 9;
+        const int i = mg ? lane - 2 : lane - 9;
+        base = mg ? T[1 + i] : T[17 + i];
+        cur = mg ? m[i] : h[i];
+        float tau;
+        if (mg) {
+            if (i == 2) tau = 2.8f + 14 * (1.0f / (T[10] + T[11]));
+            else if (i == 6) tau = 2.0f / (T[15] + T[16]);
+            else tau = T[i < 2 ? 8 + i : 9 + i];
+        } else {
+            if (i == 0) tau = (1.34f / (1 + T[21])) * (1.5f + 1 / (1 + T[22]));
+            else if (i == 2) tau = 120 + 300 * (1.0f / (T[24] + T[25]));
+            else tau = T[i == 1 ? 23 : 26];
+        }
+        arg = -dt / tau;
+    }
+    const float e = crexp(arg, tab);
+    float nv = 0.0f, nca = 0.0f;
+    if (lane == 0) {
         if (fabsf(gt) < .000001f) nv = v + dt * ws / 628.3f;
-        else { const float tg = ws / gt; nv = tg + (v - tg) * crexp(-dt * gt / 628.3f, tab); }
-        const float ica = (c[1] + c[2]) * (v - eca) / 1000000.0f;
+        else { const float tg = ws / gt; nv = tg + (v - tg) * e; }
+        const float ica = (c1 + c2) * (v - eca) / 1000000.0f;
         const float cat = .05f - 14961.0f * ica;
         nca = fmaxf(.000001f, cat + (ca - cat) * c_K.prinz_ca);
-    } else if (lane >= 2 && lane < 9) {
-        const int i = lane - 2;
-        const float mi = T[1 + i];
-        float mt;
-        if (i == 2) mt = 2.8f + 14 * (1.0f / (T[10] + T[11]));
-        else if (i == 6) mt = 2.0f / (T[15] + T[16]);
-        else mt = T[i < 2 ? 8 + i : 9 + i];
-        nv = mi + (m[i] - mi) * crexp(-dt / mt, tab);
-    } else if (lane >= 9 && lane < 13) {
-        const int i = lane - 9;
-        const float hi = T[17 + i];
-        float ht;
-        if (i == 0) ht = (1.34f / (1 + T[21])) * (1.5f + 1 / (1 + T[22]));
-        else if (i == 2) ht = 120 + 300 * (1.0f / (T[24] + T[25]));
-        else ht = T[i == 1 ? 23 : 26];
-        nv = hi + (h[i] - hi) * crexp(-dt / ht, tab);
+    } else if (lane >= 2 && lane < 13) {
+        nv = base + (cur - base) * e;
     }
     __syncwarp();
     if (lane == 0) { u[0] = nv; u[1] = nca; }
@@ -491,19 +538,44 @@ __device__ __forceinline__ void pz_substep_warp(float *u, const float *g, float 
 // The Prinz cell's 40 substeps of one tick on x (13 state floats); returns
 // whether the voltage crossed 0 mV upwards in any substep (all lanes).
 static __device__ __noinline__ bool prinz_tick_warp(float *x, const float *xg, float ext, float clamp_ns,
-                                             float clamp_rev, float *w, int lane, const float *tab) {
+                                                    float clamp_rev, float *w, int lane, const float *tab) {
     float *u = w, *T = w + 16;
+    const PzTerm q = pz_term(lane);
     if (lane < 13) u[lane] = x[lane];
     __syncwarp();
     bool spiked = false;
     for (int i = 0; i < 40; ++i) {
         const float before = u[0];
-        pz_substep_warp(u, xg, ext, clamp_ns, clamp_rev, T, lane, tab);
+        pz_substep_warp(u, xg, ext, clamp_ns, clamp_rev, T, lane, q, tab);
         spiked |= before < 0 && u[0] >= 0;
     }
     if (lane < 13) x[lane] = u[lane];
     __syncwarp();
     return spiked;
+}
+
+// A warp with more LP and Prinz cells than this integrates each on its own
+// lane at once (lp_integrate, pz_substep); with fewer, one after another on
+// the whole warp.
+constexpr int kWarpCellsMax = 8;
+
+// The cell model of one LP (type 2) or Prinz (type 3) cell on its own lane,
+// between heavy_pre and heavy_post: returns the LP axon voltage before the
+// tick (type 2) and sets `spiked` (type 3).
+__device__ __forceinline__ float heavy_model_lane(uint32_t type, float *x, const float *xg, float ext, bool &spiked,
+                                                  const float *tab) {
+    if (type == 2) {
+        const float ab = x[0];
+        lp_integrate(x, ext / 1000.0f, xg, tab);
+        return ab;
+    }
+    spiked = false;
+    for (int i = 0; i < 40; ++i) {
+        const float before = x[0];
+        pz_substep(x, xg, ext, xg[8] + 0.0f, -68.0f, tab);
+        spiked |= before < 0 && x[0] >= 0;
+    }
+    return 0.0f;
 }
 
 // heavy_tick in three parts for the warp form: heavy_pre and heavy_post run

@@ -478,11 +478,41 @@ __device__ __forceinline__ void phase_release(const WorldArgs &d, const UnitMem 
     }
 }
 
-// Phase 3 for neuron n (state in s).
+// An LP or Prinz cell waiting for its warp (HEAVY builds): its slot, type,
+// external current and this tick's modulator bits.
+struct HeavyJob {
+    int pending;
+    uint32_t type;
+    int slot;
+    float ext;
+    uint32_t mod;
+};
+
+// The end of phase 3 for neuron n: motor counts, trace peak, spike ring and
+// the per-tick records plasticity reads.
+__device__ __forceinline__ void phase_neuron_tail(const UnitMem &U, int n, int cur9, const NeuronRegs &s,
+                                                  uint32_t mod, int *motor_cnt, TraceRegs &tr) {
+    const uint32_t f = U.nflag[n];
+    const bool traced = (f & WF_TRACED) != 0;
+    const int motor = (int)((f >> WF_MOTOR_SHIFT) & 7u) - 1;
+    if (motor >= 0) {
+        if (traced) tr.pk = fmaxf(tr.pk, s.v);
+        if (s.spike) atomicAdd(&motor_cnt[motor], 1);
+    }
+    const uint16_t bit = (uint16_t)(1u << cur9);
+    U.ring[n] = s.spike ? (uint16_t)(U.ring[n] | bit) : (uint16_t)(U.ring[n] & ~bit);
+    U.nspk[n] = s.spike ? 1 : 0;
+    U.nmod[n] = (uint8_t)mod;
+    U.ndepol[n] = s.depol;
+}
+
+// Phase 3 for neuron n (state in s). In HEAVY builds an LP or Prinz cell
+// stops after heavy_pre with `job` pending: heavy_cells_warp runs its model
+// on the whole warp and phase_neuron_tail finishes it.
 template <bool HEAVY>
 __device__ __forceinline__ void phase_neuron(const WorldArgs &d, const UnitMem &U, int n, int t, int64_t tick,
                                              int cur9, NeuronRegs &s, int *motor_cnt, TraceRegs &tr,
-                                             const float *tab) {
+                                             const float *tab, HeavyJob &job) {
     const uint32_t f = U.nflag[n];
     if (!(f & NF_ACTIVE)) return;
     const int slot = U.nslot[n];
@@ -529,27 +559,67 @@ __device__ __forceinline__ void phase_neuron(const WorldArgs &d, const UnitMem &
     const uint32_t type = f & NF_TYPE_MASK;
     float cur = 0.0f;
     if (f & WF_SENSE) cur = (f & WF_RECEPTOR) ? receptor_drive(g, f, s, U.cur[n]) : U.cur[n];
-    if (HEAVY && (type == 2 || type == 3 || type == 6)) {
-        const ref::NeuronGene &G = d.ngene[slot];
+    if (HEAVY && (type == 2 || type == 3)) {
+        job = HeavyJob{1, type, slot, heavy_pre(g, type, s, cur, e0, e1, e2, e3, inh), mod};
+        return;
+    }
+    if (HEAVY && type == 6) {
         float xg[16] = {};
-        if (type == 2) { xg[0] = G.lp.calcium; xg[1] = G.lp.calcium_k; xg[2] = G.lp.h; xg[3] = G.lp.leak; }
-        if (type == 3) { for (int k = 0; k < 8; ++k) xg[k] = G.prinz.g[k]; xg[8] = G.prinz_leak; }
         float gg[16];
         for (int k = 0; k < 16; ++k) gg[k] = g[k];
         s = heavy_tick(gg, type, xg, d.nstate[slot].cell, s, cur, e0, e1, e2, e3, inh, tab);
     } else {
         adex_tick(g, type, f, s, cur, e0, e1, e2, e3, inh, tab);
     }
-    const int motor = (int)((f >> WF_MOTOR_SHIFT) & 7u) - 1;
-    if (motor >= 0) {
-        if (traced) tr.pk = fmaxf(tr.pk, s.v);
-        if (s.spike) atomicAdd(&motor_cnt[motor], 1);
+    phase_neuron_tail(U, n, cur9, s, mod, motor_cnt, tr);
+}
+
+// The warp's pending LP and Prinz cells, one after another, each on all 32
+// lanes (ns_physio.cuh: lp_integrate_warp, prinz_tick_warp); the owner lane
+// then completes heavy_tick's arithmetic. All lanes call it together; w is
+// the warp's kHeavyWarpScratch + 16 floats of shared memory.
+__device__ __forceinline__ void heavy_cells_warp(const WorldArgs &d, const HeavyJob &job, NeuronRegs &s, float *w,
+                                                 int lane, const float *tab) {
+    const uint32_t pend = __ballot_sync(0xffffffffu, job.pending != 0);
+    if (__popc(pend) > kWarpCellsMax) {        // many cells: each on its own lane at once
+        if (job.pending) {
+            const ref::NeuronGene &G = d.ngene[job.slot];
+            float xg[16] = {};
+            if (job.type == 2) { xg[0] = G.lp.calcium; xg[1] = G.lp.calcium_k; xg[2] = G.lp.h; xg[3] = G.lp.leak; }
+            else { for (int k = 0; k < 8; ++k) xg[k] = G.prinz.g[k]; xg[8] = G.prinz_leak; }
+            float *x = d.nstate[job.slot].cell;
+            bool spiked = false;
+            const float ab = heavy_model_lane(job.type, x, xg, job.ext, spiked, tab);
+            heavy_post(job.type, s, x, ab, spiked);
+        }
+        return;
     }
-    const uint16_t bit = (uint16_t)(1u << cur9);
-    U.ring[n] = s.spike ? (uint16_t)(U.ring[n] | bit) : (uint16_t)(U.ring[n] & ~bit);
-    U.nspk[n] = s.spike ? 1 : 0;
-    U.nmod[n] = (uint8_t)mod;
-    U.ndepol[n] = s.depol;
+    for (uint32_t pm = pend; pm; pm &= pm - 1u) {
+        const int L = __ffs(pm) - 1;
+        const int slot = __shfl_sync(0xffffffffu, job.slot, L);
+        const uint32_t ty = __shfl_sync(0xffffffffu, job.type, L);
+        const float ex = __shfl_sync(0xffffffffu, job.ext, L);
+        const ref::NeuronGene &G = d.ngene[slot];
+        float *xg = w + kHeavyWarpScratch;
+        if (lane < 16) {
+            float v = 0.0f;
+            if (ty == 2) v = lane == 0 ? G.lp.calcium : lane == 1 ? G.lp.calcium_k : lane == 2 ? G.lp.h
+                                                      : lane == 3 ? G.lp.leak : 0.0f;
+            else v = lane < 8 ? G.prinz.g[lane] : lane == 8 ? G.prinz_leak : 0.0f;
+            xg[lane] = v;
+        }
+        __syncwarp();
+        float *x = d.nstate[slot].cell;
+        if (ty == 2) {
+            const float ab = x[0];
+            lp_integrate_warp(x, ex / 1000.0f, xg, w, lane, tab);
+            if (lane == L) heavy_post(2, s, x, ab, false);
+        } else {
+            const bool sp = prinz_tick_warp(x, xg, ex, xg[8] + 0.0f, -68.0f, w, lane, tab);
+            if (lane == L) heavy_post(3, s, x, 0.0f, sp);
+        }
+        __syncwarp();
+    }
 }
 
 __device__ __forceinline__ void phase_plastic_events(const WorldArgs &d, const UnitMem &U, int ne, int tid, int bs) {
@@ -675,6 +745,7 @@ __global__ void __launch_bounds__(kBlock, MINB) world_tick_small(WorldArgs d, Ca
     __shared__ int q_n, q_i, q_done, s_nu, s_ntot, s_etot;
     __shared__ int s_cnt[2];
     __shared__ unsigned long long s_events;
+    __shared__ float s_hscr[HEAVY ? (kBlock / 32) * (kHeavyWarpScratch + 16) : 1];   // warp scratch of LP/Prinz cells
 
     const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31, warp = tid >> 5;
     {
@@ -782,7 +853,12 @@ __global__ void __launch_bounds__(kBlock, MINB) world_tick_small(WorldArgs d, Ca
             phase_release(d, U, tick, tid, bs, tab);
             __syncthreads();
             if (tid == 0) s_cnt[0] = 0;
-            if (tid < ntot) phase_neuron<HEAVY>(d, U, tid, t, tick, cur9, s, &ua_motor[nani[tid] * kM], tr, tab);
+            HeavyJob job = {};
+            if (tid < ntot) phase_neuron<HEAVY>(d, U, tid, t, tick, cur9, s, &ua_motor[nani[tid] * kM], tr, tab, job);
+            if (HEAVY) {
+                heavy_cells_warp(d, job, s, s_hscr + warp * (kHeavyWarpScratch + 16), lane, tab);
+                if (job.pending) phase_neuron_tail(U, tid, cur9, s, job.mod, &ua_motor[nani[tid] * kM], tr);
+            }
             __syncthreads();
             phase_plastic_events(d, U, etot, tid, bs);
             __syncthreads();
@@ -877,6 +953,7 @@ __global__ void __launch_bounds__(kBigBlock, HEAVY ? 2 : 3) world_tick_big(World
     float *tab = reinterpret_cast<float *>(w_smem);
     __shared__ int s_i, s_motor[kM], s_cnt[2];
     __shared__ unsigned long long s_events;
+    __shared__ float s_hscr[HEAVY ? (kBigBlock / 32) * (kHeavyWarpScratch + 16) : 1];   // warp scratch of LP/Prinz cells
     const int tid = threadIdx.x, bs = blockDim.x;
     {
         const float *src = nsx::exp2f_table();
@@ -935,11 +1012,22 @@ __global__ void __launch_bounds__(kBigBlock, HEAVY ? 2 : 3) world_tick_big(World
             phase_release(d, U, tick, tid, bs, tab);
             __syncthreads();
             if (tid == 0) s_cnt[0] = 0;
-            for (int n = tid; n < nn; n += bs) {
-                NeuronRegs s;
-                slab_load(B, n, s);
-                TraceRegs tr = {0, 0, 0, B.trx[n], B.tri[n], __uint_as_float(B.regs[13 * MN + n])};
-                phase_neuron<HEAVY>(d, U, n, t, tick, cur9, s, s_motor, tr, tab);
+            for (int nb0 = 0; nb0 < nn; nb0 += bs) {    // the same trip count for every thread (warp cells)
+                const int n = nb0 + tid;
+                if (!HEAVY && n >= nn) break;
+                NeuronRegs s = {};
+                TraceRegs tr = {0, 0, 0, 0.0f, 0.0f, -INFINITY};
+                HeavyJob job = {};
+                if (n < nn) {
+                    slab_load(B, n, s);
+                    tr = TraceRegs{0, 0, 0, B.trx[n], B.tri[n], __uint_as_float(B.regs[13 * MN + n])};
+                    phase_neuron<HEAVY>(d, U, n, t, tick, cur9, s, s_motor, tr, tab, job);
+                }
+                if (HEAVY) {
+                    heavy_cells_warp(d, job, s, s_hscr + (tid >> 5) * (kHeavyWarpScratch + 16), tid & 31, tab);
+                    if (job.pending) phase_neuron_tail(U, n, cur9, s, job.mod, s_motor, tr);
+                }
+                if (n >= nn) continue;
                 slab_store(B, n, s);
                 if (tr.ea || tr.er || tr.ia) {
                     const int m = (int)((U.nflag[n] >> WF_MOTOR_SHIFT) & 7u) - 1;

@@ -62,7 +62,7 @@ SIGNATURES = {
     "nsb_gpu_checkpoint_import": (ct.c_int, [_vp, _vp, ct.c_longlong, _vp, ct.c_longlong, _i64]),
     "nsb_gpu_autotune": (ct.c_int, [_vp, ct.c_int, ct.c_float, _vp]),
     "nsb_gpu_buckets": (ct.c_int, [_vp, _i32]),
-    "nsb_gpu_set_bucket": (ct.c_int, [_vp, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_int]),
+    "nsb_gpu_set_bucket": (ct.c_int, [_vp, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_int]),
     "nsb_compile_genome": (ct.c_int, [ct.c_int, ct.c_int, _f, _f, ct.c_int, _i32, _f, _f, _i32, _u32, _u32, _i32,
                                       _i32]),
     "nsb_world_create": (_vp, [_vp, ct.c_int, ct.c_int]),
@@ -359,20 +359,20 @@ class GpuBatch:
 
     BUCKETS = ("huge", "large", "big", "packed", "heavy")
     BUCKET_FIELDS = ("first_unit", "units", "max_neurons", "max_synapses", "block", "cooperative", "cluster",
-                     "meta_cap", "smem_bytes", "grid")
+                     "meta_cap", "list", "smem_bytes", "grid")
 
     def buckets(self):
         """The five work-unit buckets and their launch configurations, as dicts."""
-        out = np.zeros(50, np.int32)
+        out = np.zeros(55, np.int32)
         n = self.lib.nsb_gpu_buckets(self.ptr, _p(out, _i32))
-        rows = out[:n].reshape(-1, 10)
+        rows = out[:n].reshape(-1, 11)
         return [dict(name=name, **{f: int(v) for f, v in zip(self.BUCKET_FIELDS, row)})
                 for name, row in zip(self.BUCKETS, rows)]
 
-    def set_bucket(self, bucket, block=256, cooperative=False, cluster=1, meta_cap=6144):
+    def set_bucket(self, bucket, block=256, cooperative=False, cluster=1, meta_cap=6144, list_=True):
         """Set one bucket's configuration (RuntimeError when it cannot run)."""
         if self.lib.nsb_gpu_set_bucket(self.ptr, int(bucket), int(block), 1 if cooperative else 0, int(cluster),
-                                       int(meta_cap)):
+                                       int(meta_cap), 1 if list_ else 0):
             raise RuntimeError(_err(self.lib))
 
     def close(self):

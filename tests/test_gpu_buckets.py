@@ -4,8 +4,8 @@ A batch with work units in every bucket (brains of 3,500, 2,000 and 1,200
 neurons above the 768-neuron unit, packed small brains, and brains with LP,
 Prinz and LFS cells) is stepped under many bucket configurations: 128 or
 256 threads per CTA, serial or warp-cooperative delivery, one CTA or a
-thread-block cluster per big brain, and synapse meta words staged in shared
-memory or read from global memory. Every configuration gives the oracle's
+thread-block cluster per big brain, synapse meta words staged in shared
+memory or read from global memory, and list or per-thread integration. Every configuration gives the oracle's
 results bit for bit, and the autotuner leaves the brains' state untouched.
 """
 import numpy as np
@@ -72,13 +72,14 @@ def test_every_bucket_configuration_matches_the_oracle(nsb, monkeypatch):
         assert [b["units"] > 0 for b in bk] == [True] * 5, bk
         assert [b["max_neurons"] for b in bk[:3]] == [3500, 2000, 1200]
         _check(gpu, batch, seeds, want, "default")
-        configs = [(256, 0, False, 6144), (128, 1, True, 6144), (128, 0, True, 0), (256, 1, False, 0),
-                   (128, 1, False, 32768), (256, 0, True, 32768), (128, 0, False, 64), (256, 1, True, 6144)]
-        for block, coop, clustered, cap in configs:
+        configs = [(256, 0, False, 6144, 1), (128, 1, True, 6144, 1), (128, 0, True, 0, 1), (256, 1, False, 0, 0),
+                   (128, 1, False, 32768, 1), (256, 0, True, 32768, 1), (128, 0, False, 64, 0),
+                   (256, 1, True, 6144, 1), (256, 0, False, 6144, 0), (128, 1, False, 6144, 0)]
+        for block, coop, clustered, cap, lst in configs:
             for b in range(4):
-                gpu.set_bucket(b, block, coop, (8, 4, 2, 1)[b] if clustered else 1, cap)
+                gpu.set_bucket(b, block, coop, (8, 4, 2, 1)[b] if clustered else 1, cap, lst)
             got = gpu.buckets()
-            label = f"block {block} coop {coop} clustered {clustered} meta {cap}"
+            label = f"block {block} coop {coop} clustered {clustered} meta {cap} list {lst}"
             assert all(g["block"] == block for g in got[:4]), label
             _check(gpu, batch, seeds, want, label)
         with pytest.raises(RuntimeError):
