@@ -13,6 +13,9 @@ value : neuron-ticks/s with inputs resident on the device, one persistent
 e2e   : the same metric through the reference's C ABI call ns_gpu_step with
         pinned host buffers (host->device observations, device->host motor
         outputs and status inside the timed region).
+other_configs : (N=1, default run) the same metric, device-resident, on the
+        plasticity-heavy full pools (config 4) and the plain small batch
+        (config 1), each after its own per-bucket autotune.
 reference_cuda : (N=1, default run) the reference's own CUDA forms on the
         same batch and GPU after this library's buffers are freed: the Gym
         batch kernel step_batch (gym_adapter/gpu.cu) and the world simulator's
@@ -141,9 +144,23 @@ def workload(nsb, seed, fraction=1, kind="batched_uneven"):
     profiler captures that must stay small. kind "plasticity_heavy": the same
     pools with every synapse on the triplet/dopamine profile (config 4)."""
     if kind == "plasticity_heavy":
-        return nsb.workloads.plasticity_heavy(seed=seed + 2, brains=32768 // fraction,
-                                              total_neurons=4194304 // fraction,
-                                              total_synapses=8388608 // fraction)
+        tag = "full" if fraction == 1 else f"div{fraction}"
+        cache = Path(os.environ.get("NSB_BENCH_CACHE", "/tmp")) / f"nsb_heavy_{tag}_seed{seed}.npz"
+        W = nsb.workloads
+        meta = {"ticks_per_step": 16, "steps": 1000, "pulse_period": 50, "pulse_mod": 4, "burst_fraction": 0.3}
+        if cache.exists():
+            z = np.load(cache)
+            return W.Batch(z["nr"], z["sr"], z["no"], z["so"], z["mo"], int(z["ch"]), int(z["md"]),
+                           "plasticity_heavy", z["inp"], 230.0, meta)
+        b = W.plasticity_heavy(seed=seed + 2, brains=32768 // fraction, total_neurons=4194304 // fraction,
+                               total_synapses=8388608 // fraction)
+        assert all(b.meta[k] == v for k, v in meta.items())
+        try:
+            np.savez(cache, nr=b.neuron_rows, sr=b.synapse_rows, no=b.neuron_offsets, so=b.synapse_offsets,
+                     mo=b.motors, ch=b.channels, md=b.max_delay, inp=b.inputs)
+        except OSError:
+            pass
+        return b
     if kind == "plain_small":
         # config 1: 64 brains x 48 neurons, 600 synapses each, 20 Hz receptor drive
         return nsb.workloads.plain_small(seed=seed)
@@ -413,6 +430,46 @@ def run_reference_cuda(args, rank, world, local_rank):
         print(json.dumps({"impl": "reference-cuda", "unavailable": n}), flush=True)
 
 
+def device_rate(nsb, batch, steps, warmup, gpu_index):
+    """One batch stepped device-resident from a captured CUDA graph after the
+    per-bucket autotuner, timed with CUDA events on the launching stream:
+    ms per step, neuron-ticks/s, synaptic events/s, the bucket plan and the
+    clocks seen."""
+    import torch
+    gpu = nsb.GpuBatch.from_rows(batch)
+    try:
+        if "pulse_period" in batch.meta:
+            gpu.set_modulation(batch.meta["pulse_period"], batch.meta["pulse_mod"])
+        gpu.reset(np.arange(batch.brains, dtype=np.uint32))
+        gpu.upload(batch.inputs, np.ones(batch.brains, np.uint8))
+        stream = torch.cuda.Stream()
+        s = stream.cuda_stream
+        gpu.autotune(16, batch.gain, s)
+        torch.cuda.synchronize()
+        for _ in range(max(warmup, 3)):
+            gpu.step_graph(16, batch.gain, s)
+        torch.cuda.synchronize()
+        gpu.take_events()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(gpu_index) as clk:
+            e0.record(stream)
+            for _ in range(steps):
+                gpu.step_graph(16, batch.gain, s)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        events = gpu.take_events()
+        plan = [{k: b[k] for k in ("name", "units", "block", "cooperative", "cluster", "meta_cap", "list")}
+                for b in gpu.buckets() if b["units"]]
+    finally:
+        gpu.close()
+    N = len(batch.neuron_rows)
+    return {"ms_per_step": ms / steps, "value": N * 16 * steps / (ms / 1e3), "unit": UNIT,
+            "synaptic_events_per_s": events / (ms / 1e3), "neurons": N, "synapses": len(batch.synapse_rows),
+            "brains": batch.brains, "steps": steps, "warmup": max(warmup, 3), "plan": plan, "clocks": clk.summary()}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     torch.cuda.set_device(local_rank)
@@ -445,7 +502,8 @@ def run_ours(args, rank, world, local_rank):
     # Per-bucket autotune (untimed; state restored afterwards).
     coop = gpu.autotune(16, batch.gain, s)
     torch.cuda.synchronize()
-    plan = [{k: b[k] for k in ("name", "units", "max_neurons", "block", "cooperative", "cluster", "meta_cap", "grid")}
+    plan = [{k: b[k] for k in ("name", "units", "max_neurons", "block", "cooperative", "cluster", "meta_cap", "list",
+                               "grid")}
             for b in gpu.buckets() if b["units"]]
     for _ in range(max(args.warmup, 3)):
         gpu.step_graph(16, batch.gain, s)
@@ -543,6 +601,16 @@ def run_ours(args, rank, world, local_rank):
             line["cpu_baseline"] = {"value": nt / secs, "unit": UNIT, "cores": ref.processes, "kind": ref.kind,
                                     "sample": ref.sample + "; 2 timed steps after 1 warm-up"}
     gpu.close()
+    if rank == 0 and world == 1 and not args.no_other_configs and args.fraction == 1 \
+            and args.workload == "batched_uneven":
+        # The other configurations of the same metric, device-resident, in the same run:
+        # plasticity-heavy full pools (every synapse triplet STDP + dopamine
+        # eligibility, 30 % bursting, pulses every 50 ms) and the plain small
+        # batch (64 brains x 48 neurons, 600 synapses each).
+        line["other_configs"] = {
+            "plasticity_heavy_full_pools": device_rate(nsb, workload(nsb, 2, 1, "plasticity_heavy"), 10, 3,
+                                                       local_rank),
+            "plain_small_64x48": device_rate(nsb, workload(nsb, 2, 1, "plain_small"), 50, 5, local_rank)}
     if rank == 0:
         if (world == 1 and not args.no_reference_cuda and args.fraction == 1
                 and args.workload in ("batched_uneven", "plain_small")):
@@ -1005,6 +1073,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-cuda"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="skip the plasticity-heavy and plain-small lines of the default run (N=1 only)")
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="skip timing the reference's own CUDA forms on the same batch (N=1 only)")
     ap.add_argument("--fraction", type=int, default=1, choices=[1, 2, 4, 8, 16],

@@ -271,13 +271,18 @@ NSX_COLD float expf_cr_wide(float x) { return expf_cr_tab(x, exp2_table()); }
 // The result is returned only if it is at least 2^-38 (relative) away from a
 // rounding midpoint; otherwise, and outside [-86, 88.5] (results near the
 // normal range limits, NaN, infinities), the binary64 path decides.
-NSX_HD float expf_cr_ff(float x, const float *tabf) {
-    if (!(x >= -86.0f && x <= 88.5f)) return expf_cr_wide(x);
+// expf_cr_fast is the binary32 part alone: its result stands when `ok`.
+NSX_HD float expf_cr_fast(float x, const float *tabf, bool &ok) {
+    // Branch-free, so that independent exponentials can be interleaved: an
+    // argument outside [-86, 88.5] is replaced by 0 for the arithmetic (the
+    // table index stays in range) and reported through `ok`.
+    const bool in = x >= -86.0f && x <= 88.5f;
+    const float xs = in ? x : 0.0f;
     const float shifter = 0x1.8p23f;
-    const float t = sfma(x, NSX_F_INV_LN2_128, shifter);
+    const float t = sfma(xs, NSX_F_INV_LN2_128, shifter);
     const int ki = (int)fbits(t) - 0x4B400000;
     const float kf = t - shifter;
-    const float r1 = sfma(-kf, NSX_F_LN2_128_A, x);      // exact
+    const float r1 = sfma(-kf, NSX_F_LN2_128_A, xs);     // exact
     const float p = kf * NSX_F_LN2_128_B;
     const float pe = sfma(kf, NSX_F_LN2_128_B, -p);       // exact error of p
     const float rh = r1 - p;                              // two-sum(r1, -p)
@@ -302,8 +307,14 @@ NSX_HD float expf_cr_ff(float x, const float *tabf) {
     const uint32_t yb = fbits(y);
     const float half = bitsf((yb & 0x7f800000u) - (24u << 23));   // ulp(y)/2
     const float gap = half - fabsf(d);
-    if ((yb & 0x007fffffu) == 0u || gap <= half * 0x1p-14f) return expf_cr_wide(x);
+    ok = in && (yb & 0x007fffffu) != 0u && gap > half * 0x1p-14f;
     return bitsf((uint32_t)((int)yb + (ki >> 7) * (1 << 23)));
+}
+
+NSX_HD float expf_cr_ff(float x, const float *tabf) {
+    bool ok;
+    const float y = expf_cr_fast(x, tabf, ok);
+    return ok ? y : expf_cr_wide(x);
 }
 
 // Correctly rounded exp using the built-in table of the calling side.

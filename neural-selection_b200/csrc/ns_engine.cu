@@ -599,6 +599,11 @@ __global__ void __launch_bounds__(256, NSB_MIN_CTAS) tick_kernel_list(Pools P, i
     float *l_e0 = reinterpret_cast<float *>(l_j + kListCap), *l_e1 = l_e0 + kListCap, *l_e2 = l_e1 + kListCap,
           *l_e3 = l_e2 + kListCap, *l_inh = l_e3 + kListCap;
     uint32_t *l_mn = reinterpret_cast<uint32_t *>(l_inh + kListCap);
+    // units of up to kListCap neurons: flags, incoming-segment starts and the
+    // call's AMPA scale of every neuron, staged for the call
+    uint32_t *s_nf = l_mn + kListCap;
+    int *s_ip = reinterpret_cast<int *>(s_nf + kListCap);                 // kListCap + 1
+    float *s_amp = reinterpret_cast<float *>(s_ip + kListCap + 1);
     __shared__ int s_unit, s_count[2];
     __shared__ unsigned long long s_events;
 
@@ -631,6 +636,14 @@ __global__ void __launch_bounds__(256, NSB_MIN_CTAS) tick_kernel_list(Pools P, i
             for (int k = tid; k < ne; k += bs) s_meta[k] = P.smeta[e0 + k];
         const uint32_t *meta = meta_smem ? s_meta : P.smeta + e0;
         for (int w = tid; w < P.hw; w += bs) s_fixed[w] = 0u;
+        const bool stage = nn <= kListCap;
+        if (stage) {
+            for (int j = tid; j < nn; j += bs) {
+                s_nf[j] = P.nflags[n0 + j];
+                s_ip[j] = P.inptr[n0 + j];
+            }
+            if (tid == 0) s_ip[nn] = P.inptr[n0 + nn];
+        }
         // A unit whose brains are all masked off does no work: outputs 0.
         if (!__syncthreads_or(tid < nb && s_mask[tid] != 0)) {
             for (int i = tid; i < nb * P.outputs; i += bs)
@@ -649,7 +662,9 @@ __global__ void __launch_bounds__(256, NSB_MIN_CTAS) tick_kernel_list(Pools P, i
             if (run) {
                 uint32_t *r = P.nstate + (size_t)(n0 + j) * S_WORDS;
                 h0 = r[S_HIST];
-                r[S_PAD] = __float_as_uint(crexp(__uint_as_float(r[S_LOGAMPA]), tab));
+                const float amp = crexp(__uint_as_float(r[S_LOGAMPA]), tab);
+                r[S_PAD] = __float_as_uint(amp);
+                if (stage) s_amp[j] = amp;
             }
             const uint32_t rot = run ? rotr32(h0, (uint32_t)(s_tick[bi] & 31)) : 0u;
             for (int sl = 0; sl < 32; ++sl) {
@@ -668,7 +683,7 @@ __global__ void __launch_bounds__(256, NSB_MIN_CTAS) tick_kernel_list(Pools P, i
                 for (int sl0 = c0; sl0 < min(slots, c0 + spc); ++sl0) {
                     const int j = sl0 * bs + tid;
                     const int n = n0 + j;
-                    const uint32_t flags = j < nn ? P.nflags[n] : 0u;
+                    const uint32_t flags = j < nn ? (stage ? s_nf[j] : P.nflags[n]) : 0u;
                     const int bi = (int)((flags >> NF_SLOT_SHIFT) & NF_SLOT_MASK);
                     const bool run = j < nn && s_mask[bi] != 0;
                     if (lane == 0) hist[(t & 31) * P.hw + sl0 * nwarp + warp] = 0u;   // filled in phase B
@@ -677,9 +692,15 @@ __global__ void __launch_bounds__(256, NSB_MIN_CTAS) tick_kernel_list(Pools P, i
                     float ampa = 0.0f;
                     if (run) {
                         tick0 = s_tick[bi];
-                        ib = P.inptr[n];
-                        ie = P.inptr[n + 1];
-                        ampa = __uint_as_float(P.nstate[(size_t)n * S_WORDS + S_PAD]);
+                        if (stage) {
+                            ib = s_ip[j];
+                            ie = s_ip[j + 1];
+                            ampa = s_amp[j];
+                        } else {
+                            ib = P.inptr[n];
+                            ie = P.inptr[n + 1];
+                            ampa = __uint_as_float(P.nstate[(size_t)n * S_WORDS + S_PAD]);
+                        }
                     }
                     const bool dlv = run && (flags & NF_ACTIVE);
                     Delivered d = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0u, 0};
@@ -720,7 +741,7 @@ __global__ void __launch_bounds__(256, NSB_MIN_CTAS) tick_kernel_list(Pools P, i
                 for (int k = tid; k < count; k += bs) {
                     const int j = l_j[k];
                     const int n = n0 + j;
-                    const uint32_t flags = P.nflags[n];
+                    const uint32_t flags = stage ? s_nf[j] : P.nflags[n];
                     const int bi = (int)((flags >> NF_SLOT_SHIFT) & NF_SLOT_MASK);
                     const uint32_t mn = l_mn[k];
                     const Delivered d = {l_e0[k], l_e1[k], l_e2[k], l_e3[k], l_inh[k], mn & 0xffu, (int)(mn >> 8)};
@@ -745,8 +766,9 @@ __global__ void __launch_bounds__(256, NSB_MIN_CTAS) tick_kernel_list(Pools P, i
                         ++cnt[j];
                     }
                     if ((flags & NF_PLASTIC_IN) && (s.spike || d.mod || d.narr))
-                        plasticity_events(P.sstate, P.sgene, P.slastp, P.hw, P.inptr[n], P.inptr[n + 1], e0, meta,
-                                          hist, t, s_tick[bi], s.spike != 0, d.mod, s.depol, tab);
+                        plasticity_events(P.sstate, P.sgene, P.slastp, P.hw, stage ? s_ip[j] : P.inptr[n],
+                                          stage ? s_ip[j + 1] : P.inptr[n + 1], e0, meta, hist, t, s_tick[bi],
+                                          s.spike != 0, d.mod, s.depol, tab);
                 }
                 __syncthreads();
             }
@@ -1045,7 +1067,7 @@ int spike_words(int max_unit_neurons, int block) {
 // Dynamic shared memory of the light (list) kernel.
 int tick_smem_bytes(int hw, int meta_cap) {
     return 1024 + (meta_cap + 32 * hw * 2 + ((hw + 1) & ~1)) * 4 + kMaxUnitBrains * 8 + 2 * kMaxUnitBrains * 4 +
-           8 * kEvCap * 8 + kListCap * 7 * 4;
+           8 * kEvCap * 8 + kListCap * 7 * 4 + (3 * kListCap + 1) * 4;
 }
 
 // Dynamic shared memory of the heavy kernel for hw ring words.

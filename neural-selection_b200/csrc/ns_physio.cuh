@@ -142,47 +142,90 @@ __device__ __forceinline__ float lp_sig(float v, float mid, float slope, const f
     return 1.0f / (1.0f + crexp((v - mid) / slope, tab));
 }
 __device__ __forceinline__ float lp_ratio(float num, float den, float lim) { return fabsf(den) < 1e-5f ? lim : num / den; }
+// Correctly rounded exponentials of N independent arguments: every binary32
+// fast path first, with no branch between them, so that they interleave;
+// then the binary64 path for any argument that needs it (rare).
+template <int N> __device__ __forceinline__ void crexp_n(const float (&x)[N], float (&y)[N], const float *tab) {
+    bool ok[N];
+    bool all = true;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        y[i] = nsx::expf_cr_fast(x[i], tab, ok[i]);
+        all = all && ok[i];
+    }
+    if (!all) {
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+            if (!ok[i]) y[i] = nsx::expf_cr_wide(x[i]);
+    }
+}
+
+// lp_rates with its 21 exponentials computed as one batch (crexp_n): the
+// arguments, the sigmoids 1 / (1 + e) and the derivative assembly are the
+// operations of the reference, in its order.
 static __device__ __noinline__ void lp_rates(const float *x, float i_na, const float *sc, float *d, const float *tab) {
-    const float va = x[0], vs = x[15];
+    const float va = x[0], vs = x[15], cai = x[13];
+    float A[21], E[21];
+    A[0] = vs / 11.4866f;
+    A[1] = (vs - 55.0f) / -15.0f;
+    A[2] = -13.0f - va / 4.0f;
+    A[3] = va / 5.0f + 5.0f;
+    A[4] = -2.66666666667f - va / 18.0f;
+    A[5] = -5.0f - va / 5.0f;
+    A[6] = -10.0f - va / 5.0f;
+    A[7] = -1.375f - va / 40.0f;
+    A[8] = (vs - 15.0f) / -9.8f;
+    A[9] = (vs - -40.0f) / 3.2f;
+    A[10] = (vs - -15.0f) / -10.0f;
+    A[11] = (vs - 29.1336f) / -4.43083f;
+    A[12] = (vs - -.6f * cai) / -23.0f;
+    A[13] = (vs - (-16.0f - .6f * cai)) / -5.0f;
+    A[14] = (vs - -12.0f) / -26.0f;
+    A[15] = (vs - -62.0f) / 6.0f;
+    A[16] = (vs - -40.0f) / -12.0f;
+    A[17] = (vs - -70.0f) / 8.0f;
+    A[18] = (vs - -110.0f) / -21.6f;
+    A[19] = (va - -26.9916223f) / -5.957441281f;
+    A[20] = (va - -60.57875745f) / -13.25674673f;
+    crexp_n(A, E, tab);
+    auto sig = [&](int i) { return 1.0f / (1.0f + E[i]); };
     const float na = x[1] * x[1] * x[1] * x[2] * 7.15f * (va - 50.0f);
     const float kd = x[8] * x[8] * x[8] * x[8] * 1.43f * (va + 72.0f);
     const float km = .2613041227f * x[14] * (va + 80.0f);
     const float aleak = sc[3] * .001004288227f * (va + 50.0f);
     const float cpl = .004017089073f * (vs - va);
     d[0] = (-na - kd - km - aleak + cpl) / .1148312178f;
-    const float ev = crexp(vs / 11.4866f, tab);
+    const float ev = E[0];
     const float ghk = fabsf(vs) < .001f ? 11.4866f * (x[13] - 15123.5f) : vs * (x[13] * ev - 15123.5f) / (ev - 1.0f);
     const float ca = sc[0] * (x[3] * x[4] * .1247796343f + x[5] * .07142141077f) * .00155982f * ghk * .9f;
     const float kca = sc[1] * x[6] * x[7] * 1.663612026f * (vs + 72.0f) * .9f;
-    const float amix = lp_sig(vs, 55.0f, -15.0f, tab);
+    const float amix = sig(1);
     const float ka = x[9] * x[9] * x[9] * .8008791415f * (vs + 72.0f) * (amix * x[10] + (1.0f - amix) * x[11]) * .9f;
     const float ih = sc[2] * x[12] * .0126874385f * (vs + 20.0f) * .9f;
     const float sleak = sc[3] * .0006901584324f * (vs + 50.0f);
     d[15] = (-ca - kca - ka - ih - sleak - cpl + (i_na - 2.0f) * .01222505828f) / .0543909161f;
-    float a = lp_ratio(-16.64f - .32f * va, crexp(-13.0f - va / 4.0f, tab) - 1.0f, 1.28f);
-    float b = lp_ratio(.28f * va + 7.0f, crexp(va / 5.0f + 5.0f, tab) - 1.0f, 1.4f);
+    float a = lp_ratio(-16.64f - .32f * va, E[2] - 1.0f, 1.28f);
+    float b = lp_ratio(.28f * va + 7.0f, E[3] - 1.0f, 1.4f);
     d[1] = a * (1.0f - x[1]) - b * x[1];
-    a = .128f * crexp(-2.66666666667f - va / 18.0f, tab);
-    b = 4.0f / (crexp(-5.0f - va / 5.0f, tab) + 1.0f);
+    a = .128f * E[4];
+    b = 4.0f / (E[5] + 1.0f);
     d[2] = a * (1.0f - x[2]) - b * x[2];
-    a = lp_ratio(-1.6f - .032f * va, crexp(-10.0f - va / 5.0f, tab) - 1.0f, .16f);
-    b = .5f * crexp(-1.375f - va / 40.0f, tab);
+    a = lp_ratio(-1.6f - .032f * va, E[6] - 1.0f, .16f);
+    b = .5f * E[7];
     d[8] = a * (1.0f - x[8]) - b * x[8];
-    d[3] = (lp_sig(vs, 15.0f, -9.8f, tab) - x[3]) * .045f;
-    d[4] = (lp_sig(vs, -40.0f, 3.2f, tab) - x[4]) * .02f * lp_sig(vs, -15.0f, -10.0f, tab);
-    d[5] = (lp_sig(vs, 29.1336f, -4.43083f, tab) - x[5]) * .0608644f;
-    const float cai = x[13];
-    const float kinf = lp_sig(vs, -.6f * cai, -23.0f, tab) * lp_sig(vs, -16.0f - .6f * cai, -5.0f, tab) * cai / (2.5f + cai);
+    d[3] = (sig(8) - x[3]) * .045f;
+    d[4] = (sig(9) - x[4]) * .02f * sig(10);
+    d[5] = (sig(11) - x[5]) * .0608644f;
+    const float kinf = sig(12) * sig(13) * cai / (2.5f + cai);
     d[6] = (kinf - x[6]) * .6f;
     d[7] = (.7f / (.6f + cai) - x[7]) * .035f;
-    d[9] = (lp_sig(vs, -12.0f, -26.0f, tab) - x[9]) * .14f;
-    const float ainf = lp_sig(vs, -62.0f, 6.0f, tab);
+    d[9] = (sig(14) - x[9]) * .14f;
+    const float ainf = sig(15);
     d[10] = (ainf - x[10]) * .05f;
-    d[11] = (ainf - x[11]) * .0036f * lp_sig(vs, -40.0f, -12.0f, tab);
-    d[12] = (lp_sig(vs, -70.0f, 8.0f, tab) - x[12]) * .00033f / lp_sig(vs, -110.0f, -21.6f, tab);
+    d[11] = (ainf - x[11]) * .0036f * sig(16);
+    d[12] = (sig(17) - x[12]) * .00033f / sig(18);
     d[13] = -.05049639866f * ca - .01729930764f * (cai - .02f);
-    d[14] = (lp_sig(va, -26.9916223f, -5.957441281f, tab) - x[14]) * .0001386796618f *
-            lp_sig(va, -60.57875745f, -13.25674673f, tab);
+    d[14] = (sig(19) - x[14]) * .0001386796618f * sig(20);
 }
 static __device__ __noinline__ void lp_integrate(float *x, float i_na, const float *sc, const float *tab) {
     const float dt = .05f;
@@ -206,11 +249,37 @@ __device__ __forceinline__ float pz_gate(float v, float a, float b, const float 
 __device__ __forceinline__ float pz_gate2(float v, float a, float b, float c, float d, const float *tab) {
     return 1.0f / (crexp((v + a) / b, tab) + crexp((v + c) / d, tab));
 }
+// pz_substep with its exponentials computed as two batches (crexp_n): the
+// voltage's gates and time constants, then the relaxations that use them.
 static __device__ __noinline__ void pz_substep(float *u, const float *g, float ext, float clamp_ns, float clamp_rev,
                                         const float *tab) {
     const float dt = .025f;
     float *m = u + 2, *h = u + 9;
     const float v = u[0], ca = fmaxf(u[1], 0.000001f);
+    // level 1: pz_gate(v, a, b) = 1 / (1 + exp((v + a) / b)) and the raw exponentials
+    float A[26], E[26];
+    const float ga[20] = {25.5f, 27.1f, 33, 27.2f, 28.3f, 12.3f, 75,          // mi
+                          120, 68.1f, 32.9f, 46, 28.3f,                       // mt 0 1 3 4 5
+                          48.9f, 32.1f, 60, 56.9f,                            // hi
+                          55, 38.9f,                                          // ht 1 3
+                          0, 0};
+    const float gb[20] = {-5.29f, -7.2f, -8.1f, -8.7f, -12.6f, -11.8f, 5.5f,
+                          -25, -20.5f, -15.2f, -22.7f, -19.2f,
+                          5.18f, 5.5f, 6.2f, 4.9f,
+                          -16.9f, -26.5f,
+                          1, 1};
+#pragma unroll
+    for (int i = 0; i < 18; ++i) A[i] = (v + ga[i]) / gb[i];
+    A[18] = (v + 27) / 10;           // mt 2
+    A[19] = (v + 70) / -13;
+    A[20] = -14.59f - .086f * v;     // mt 6
+    A[21] = -1.87f + .0701f * v;
+    A[22] = (v + 62.9f) / -10;       // ht 0
+    A[23] = (v + 34.9f) / 3.6f;
+    A[24] = (v + 55) / 9;            // ht 2
+    A[25] = (v + 65) / -16;
+    crexp_n(A, E, tab);
+    auto gate = [&](int i) { return 1.0f / (1.0f + E[i]); };
     const float eca = (8.31451e3f * 283.0f / (2.0f * 96485.3415f)) * nsx::logf_cr(3000.0f / ca);
     const float c[8] = {g[0] * m[0] * m[0] * m[0] * h[0], g[1] * m[1] * m[1] * m[1] * h[1],
                         g[2] * m[2] * m[2] * m[2] * h[2], g[3] * m[3] * m[3] * m[3] * h[3],
@@ -219,25 +288,28 @@ static __device__ __noinline__ void pz_substep(float *u, const float *g, float e
     const float rev[8] = {50, eca, eca, -80, -80, -80, -20, -50};
     float gt = clamp_ns, ws = ext + clamp_ns * clamp_rev;
     for (int i = 0; i < 8; ++i) { gt += c[i]; ws += c[i] * rev[i]; }
+    const float mi[7] = {gate(0), gate(1), gate(2), gate(3), (ca / (ca + 3)) * gate(4), gate(5), gate(6)};
+    const float mt[7] = {2.64f - 2.52f * gate(7), 43.4f - 42.6f * gate(8), 2.8f + 14 * (1.0f / (E[18] + E[19])),
+                         23.2f - 20.8f * gate(9), 180.6f - 150.2f * gate(10), 14.4f - 12.8f * gate(11),
+                         2.0f / (E[20] + E[21])};
+    const float hi[4] = {gate(12), gate(13), gate(14), gate(15)};
+    const float ht[4] = {(1.34f / (1 + E[22])) * (1.5f + 1 / (1 + E[23])), 210 - 179.6f * gate(16),
+                         120 + 300 * (1.0f / (E[24] + E[25])), 77.2f - 58.4f * gate(17)};
+    // level 2: the voltage's relaxation and the gates'
+    float B[12], F[12];
+    B[0] = -dt * gt / 628.3f;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) B[1 + i] = -dt / mt[i];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) B[8 + i] = -dt / ht[i];
+    crexp_n(B, F, tab);
     if (fabsf(gt) < .000001f) u[0] = v + dt * ws / 628.3f;
-    else { const float tg = ws / gt; u[0] = tg + (v - tg) * crexp(-dt * gt / 628.3f, tab); }
+    else { const float tg = ws / gt; u[0] = tg + (v - tg) * F[0]; }
     const float ica = (c[1] + c[2]) * (v - eca) / 1000000.0f;
     const float cat = .05f - 14961.0f * ica;
     u[1] = fmaxf(.000001f, cat + (ca - cat) * c_K.prinz_ca);
-    const float mi[7] = {pz_gate(v, 25.5f, -5.29f, tab), pz_gate(v, 27.1f, -7.2f, tab), pz_gate(v, 33, -8.1f, tab),
-                         pz_gate(v, 27.2f, -8.7f, tab), (ca / (ca + 3)) * pz_gate(v, 28.3f, -12.6f, tab),
-                         pz_gate(v, 12.3f, -11.8f, tab), pz_gate(v, 75, 5.5f, tab)};
-    const float mt[7] = {2.64f - 2.52f * pz_gate(v, 120, -25, tab), 43.4f - 42.6f * pz_gate(v, 68.1f, -20.5f, tab),
-                         2.8f + 14 * pz_gate2(v, 27, 10, 70, -13, tab), 23.2f - 20.8f * pz_gate(v, 32.9f, -15.2f, tab),
-                         180.6f - 150.2f * pz_gate(v, 46, -22.7f, tab), 14.4f - 12.8f * pz_gate(v, 28.3f, -19.2f, tab),
-                         2.0f / (crexp(-14.59f - .086f * v, tab) + crexp(-1.87f + .0701f * v, tab))};
-    for (int i = 0; i < 7; ++i) m[i] = mi[i] + (m[i] - mi[i]) * crexp(-dt / mt[i], tab);
-    const float hi[4] = {pz_gate(v, 48.9f, 5.18f, tab), pz_gate(v, 32.1f, 5.5f, tab), pz_gate(v, 60, 6.2f, tab),
-                         pz_gate(v, 56.9f, 4.9f, tab)};
-    const float ht[4] = {(1.34f / (1 + crexp((v + 62.9f) / -10, tab))) * (1.5f + 1 / (1 + crexp((v + 34.9f) / 3.6f, tab))),
-                         210 - 179.6f * pz_gate(v, 55, -16.9f, tab), 120 + 300 * pz_gate2(v, 55, 9, 65, -16, tab),
-                         77.2f - 58.4f * pz_gate(v, 38.9f, -26.5f, tab)};
-    for (int i = 0; i < 4; ++i) h[i] = hi[i] + (h[i] - hi[i]) * crexp(-dt / ht[i], tab);
+    for (int i = 0; i < 7; ++i) m[i] = mi[i] + (m[i] - mi[i]) * F[1 + i];
+    for (int i = 0; i < 4; ++i) h[i] = hi[i] + (h[i] - hi[i]) * F[8 + i];
 }
 
 // Heavy cell types (2 LP, 3 Prinz, 6 LFS) on their extended state x (16 floats).
@@ -326,7 +398,7 @@ __device__ __forceinline__ LaneTerm lp_term(int lane) {
     case 18: return {F_A, -110.0f, -21.6f, 0.0f, 1, 0};
     case 19: return {F_A, -26.9916223f, -5.957441281f, 0.0f, 1, 1};
     case 20: return {F_A, -60.57875745f, -13.25674673f, 0.0f, 1, 1};
-    default: return {F_D, 0.0f, 1.0f, 0.0f, 0, 0};       // idle lanes
+    default: return {F_B, 0.0f, 1e30f, -1.0f, 0, 0};     // idle lanes: exp(-1), unused
     }
 }
 
@@ -463,7 +535,7 @@ __device__ __forceinline__ PzTerm pz_term(int lane) {
     case 24: return {{F_G, 55.0f, 9.0f, 0.0f, 0, 0}, 0, 0.0f, 0.0f};
     case 25: return {{F_G, 65.0f, -16.0f, 0.0f, 0, 0}, 0, 0.0f, 0.0f};
     case 26: return {{F_G, 38.9f, -26.5f, 0.0f, 1, 0}, 1, 77.2f, 58.4f};
-    default: return {{F_G, 0.0f, 1.0f, 0.0f, 0, 0}, 0, 0.0f, 0.0f};   // lane 0 and idle lanes
+    default: return {{F_P, 0.0f, 0.0f, -1.0f, 0, 0}, 0, 0.0f, 0.0f};  // lane 0 and idle lanes: exp(-1), unused
     }
 }
 
@@ -487,7 +559,7 @@ __device__ __forceinline__ void pz_substep_warp(float *u, const float *g, float 
     __syncwarp();
     // level 2: the voltage and calcium (lane 0), m[i] (lanes 2-8) and h[i]
     // (lanes 9-12), one exponential each
-    float arg = 0.0f, gt = 0.0f, ws = 0.0f, eca = 0.0f, c1 = 0.0f, c2 = 0.0f, base = 0.0f, cur = 0.0f;
+    float arg = -1.0f, gt = 0.0f, ws = 0.0f, eca = 0.0f, c1 = 0.0f, c2 = 0.0f, base = 0.0f, cur = 0.0f;
     if (lane == 0) {
         eca = (8.31451e3f * 283.0f / (2.0f * 96485.3415f)) * T[0];
         const float c[8] = {g[0] * m[0] * m[0] * m[0] * h[0], g[1] * m[1] * m[1] * m[1] * h[1],
@@ -557,7 +629,10 @@ static __device__ __noinline__ bool prinz_tick_warp(float *x, const float *xg, f
 // A warp with more LP and Prinz cells than this integrates each on its own
 // lane at once (lp_integrate, pz_substep); with fewer, one after another on
 // the whole warp.
-constexpr int kWarpCellsMax = 8;
+#ifndef NSB_WARP_CELLS_MAX
+#define NSB_WARP_CELLS_MAX 8
+#endif
+constexpr int kWarpCellsMax = NSB_WARP_CELLS_MAX;
 
 // The cell model of one LP (type 2) or Prinz (type 3) cell on its own lane,
 // between heavy_pre and heavy_post: returns the LP axon voltage before the
