@@ -500,7 +500,7 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.Stream()
     s = stream.cuda_stream
     # Per-bucket autotune (untimed; state restored afterwards).
-    coop = gpu.autotune(16, batch.gain, s)
+    coop = gpu.autotune(16, batch.gain, s) if not args.no_autotune else gpu.buckets()[3]["cooperative"] != 0
     torch.cuda.synchronize()
     plan = [{k: b[k] for k in ("name", "units", "max_neurons", "block", "cooperative", "cluster", "meta_cap", "list",
                                "grid")}
@@ -1073,6 +1073,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-cuda"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default bucket configurations (profiler captures: fewer launches before the timed ones)")
     ap.add_argument("--no-other-configs", action="store_true",
                     help="skip the plasticity-heavy and plain-small lines of the default run (N=1 only)")
     ap.add_argument("--no-reference-cuda", action="store_true",

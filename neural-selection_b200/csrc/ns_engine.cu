@@ -1871,12 +1871,13 @@ bool Engine::autotune(int ticks, float gain, cudaStream_t stream) {
     const Pools P = pools(count_events_);
     // Times a bucket alone: one warm-up launch and three timed ones from the
     // same restored state for every candidate.
-    auto time_bucket = [&](const Bucket &B) {
+    // Times whole steps (every bucket, side by side, as a real step runs):
+    // one warm-up step and three timed ones from the same restored state.
+    auto time_step = [&]() {
         restore();
         for (int k = 0; k < 4; ++k) {
             if (k == 1) NSB_CHECK(cudaEventRecord(e0, s));
-            NSB_CHECK(cudaMemsetAsync(d_queue_, 0, 8 * sizeof(int), s));
-            launch_bucket(B, P, d_queue_, d_input_, d_mask_, ticks, gain, d_output_, d_status_, s);
+            launch_groups(P, d_queue_, d_input_, d_mask_, ticks, gain, d_output_, d_status_, s);
         }
         NSB_CHECK(cudaEventRecord(e1, s));
         NSB_CHECK(cudaEventSynchronize(e1));
@@ -1885,32 +1886,42 @@ bool Engine::autotune(int ticks, float gain, cudaStream_t stream) {
         NSB_CHECK(cudaEventElapsedTime(&ms, e0, e1));
         return ms;
     };
-    for (int b = 0; b < kBuckets; ++b) {
-        Bucket &cur = buckets_[b];
-        if (cur.heavy || cur.units() == 0) continue;
-        // staging depths: the default, and exactly the bucket's largest unit
-        // (less shared memory per CTA, or no global meta reads)
-        std::vector<int> caps = {kMetaCap};
-        const int fit = std::min((cur.max_synapses + 31) & ~31, 32768);
-        if (fit != kMetaCap) caps.push_back(fit);
-        std::vector<BucketConfig> cands;
-        for (int block : {256, 128})
-            for (int coop : {0, 1})
-                for (int cap : caps) {
-                    cands.push_back(BucketConfig{block, coop, 1, cap, 1});
-                    cands.push_back(BucketConfig{block, coop, 1, cap, 0});
-                    if (cur.cluster_size > 1) cands.push_back(BucketConfig{block, coop, cur.cluster_size, cap, 1});
-                }
-        Bucket best = cur;
-        float best_ms = -1.0f;
-        for (const BucketConfig &c : cands) {
-            Bucket B = cur;
-            B.cfg = c;
-            if (!shape_bucket(B)) continue;
-            const float ms = time_bucket(B);
-            if (best_ms < 0 || ms < best_ms) { best_ms = ms; best = B; }
+    // Coordinate descent: one bucket at a time (the packed bucket first, then
+    // the big-brain buckets), each candidate timed in the whole step, kept
+    // when it saves more than 1 %; at most two passes.
+    float best_ms = time_step();
+    const int order[4] = {kBucketPacked, 2, 1, 0};
+    for (int pass = 0; pass < 2; ++pass) {
+        bool changed = false;
+        for (int b : order) {
+            Bucket &cur = buckets_[b];
+            if (cur.heavy || cur.units() == 0) continue;
+            // staging depths: the default, and exactly the bucket's largest
+            // unit (less shared memory per CTA, or no global meta reads)
+            std::vector<int> caps = {kMetaCap};
+            const int fit = std::min((cur.max_synapses + 31) & ~31, 32768);
+            if (fit != kMetaCap) caps.push_back(fit);
+            std::vector<BucketConfig> cands;
+            for (int block : {256, 128})
+                for (int coop : {0, 1})
+                    for (int cap : caps) {
+                        cands.push_back(BucketConfig{block, coop, 1, cap, 1});
+                        cands.push_back(BucketConfig{block, coop, 1, cap, 0});
+                        if (cur.cluster_size > 1) cands.push_back(BucketConfig{block, coop, cur.cluster_size, cap, 1});
+                    }
+            for (const BucketConfig &c : cands) {
+                if (c.block == cur.cfg.block && c.coop == cur.cfg.coop && c.cluster == cur.cfg.cluster &&
+                    c.meta_cap == cur.cfg.meta_cap && c.list == cur.cfg.list)
+                    continue;
+                const Bucket saved = cur;
+                cur.cfg = c;
+                if (!shape_bucket(cur)) { cur = saved; continue; }
+                const float ms = time_step();
+                if (ms < 0.99f * best_ms) { best_ms = ms; changed = true; }
+                else cur = saved;
+            }
         }
-        cur = best;
+        if (!changed) break;
     }
     restore();
     NSB_CHECK(cudaStreamSynchronize(s));

@@ -108,12 +108,13 @@ public:
     // set_cooperative sets every light bucket.
     bool cooperative() const { return buckets_[kBucketPacked].cfg.coop != 0; }
     void set_cooperative(bool coop);
-    // Per-bucket autotuner: for each bucket of work units, times candidate
-    // configurations (threads per CTA, delivery mode, meta staging depth, and
-    // one CTA or a cluster for big brains) on the engine's own buffers, a few
-    // launches each with the state restored afterwards (so the call has no
-    // visible effect on the brains), and keeps the fastest. Returns the
-    // packed bucket's delivery mode.
+    // Per-bucket autotuner: coordinate descent over the buckets of work
+    // units; each candidate configuration of a bucket (threads per CTA,
+    // delivery mode, meta staging depth, list or per-thread integration, one
+    // CTA or a cluster for big brains) is timed in whole steps on the
+    // engine's own buffers, from the same restored state (so the call has no
+    // visible effect on the brains), and kept when it saves more than 1 %.
+    // Returns the packed bucket's delivery mode.
     bool autotune(int ticks, float gain, cudaStream_t stream);
     // The buckets and their current configurations.
     const std::vector<Bucket> &buckets() const { return buckets_; }

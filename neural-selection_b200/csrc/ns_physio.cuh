@@ -628,9 +628,11 @@ static __device__ __noinline__ bool prinz_tick_warp(float *x, const float *xg, f
 
 // A warp with more LP and Prinz cells than this integrates each on its own
 // lane at once (lp_integrate, pz_substep); with fewer, one after another on
-// the whole warp.
+// the whole warp. Measured on B200, the lanes' own integration (its
+// exponentials batched, crexp_n) is faster for every count in the Gym
+// engine, so the warp form is off there by default.
 #ifndef NSB_WARP_CELLS_MAX
-#define NSB_WARP_CELLS_MAX 8
+#define NSB_WARP_CELLS_MAX 0
 #endif
 constexpr int kWarpCellsMax = NSB_WARP_CELLS_MAX;
 
