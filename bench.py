@@ -84,6 +84,18 @@ def traffic_per_launch():
     return None
 
 
+def warp_instructions_per_neuron_tick():
+    """Warp instructions the light tick kernel issues per neuron-tick, from
+    the committed ncu summary of the benchmark's 1/8 slice."""
+    p = ROOT / "profiles" / "tick_kernel_list_div8_full_set.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("warp_instructions_per_neuron_tick:"):
+            return float(line.split(":")[1].split()[0])
+    return None
+
+
 class ClockSampler:
     """nvidia-smi SM clocks and throttle reasons sampled every 200 ms."""
     FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -590,6 +602,16 @@ def run_ours(args, rank, world, local_rank):
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
                 "gpu_launches": launches_per_step * args.steps,
                 "clocks": clocks}
+        wi = warp_instructions_per_neuron_tick()
+        if wi is not None and clocks and args.workload == "batched_uneven":
+            # Issue roofline: the kernel is bound by instruction issue, not HBM.
+            # Peak = SMs x 4 schedulers x one warp instruction per cycle at the SM clock seen.
+            sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
+            peak_issue = sms * 4 * clocks["sm_mhz"] * 1e6
+            line["roofline_issue"] = {"bound": "issue", "warp_inst_per_neuron_tick": wi,
+                                      "achieved": wi * value / world / 1e9, "peak": peak_issue / 1e9,
+                                      "unit": "G warp-instructions/s", "frac": wi * value / world / peak_issue,
+                                      "source": "profiles/tick_kernel_list_div8_full_set.md (ncu, 1/8 slice)"}
         if not args.no_cpu_baseline:
             ref = CpuReference(batch, 8, os.cpu_count() or 1)
             ref.step(16)
