@@ -456,6 +456,8 @@ def device_rate(nsb, batch, steps, warmup, gpu_index):
         gpu.upload(batch.inputs, np.ones(batch.brains, np.uint8))
         stream = torch.cuda.Stream()
         s = stream.cuda_stream
+        for _ in range(5):                 # the autotuner sees running activity, not the reset
+            gpu.step_graph(16, batch.gain, s)
         gpu.autotune(16, batch.gain, s)
         torch.cuda.synchronize()
         for _ in range(max(warmup, 3)):
@@ -511,7 +513,12 @@ def run_ours(args, rank, world, local_rank):
     gpu.upload(batch.inputs, np.ones(batch.brains, np.uint8))
     stream = torch.cuda.Stream()
     s = stream.cuda_stream
-    # Per-bucket autotune (untimed; state restored afterwards).
+    # Per-bucket autotune (untimed; state restored afterwards), after a few
+    # steps so that it sees the population's running activity, not its reset.
+    if not args.no_autotune:
+        for _ in range(5):
+            gpu.step_graph(16, batch.gain, s)
+        torch.cuda.synchronize()
     coop = gpu.autotune(16, batch.gain, s) if not args.no_autotune else gpu.buckets()[3]["cooperative"] != 0
     torch.cuda.synchronize()
     plan = [{k: b[k] for k in ("name", "units", "max_neurons", "block", "cooperative", "cluster", "meta_cap", "list",

@@ -578,8 +578,11 @@ __global__ void __launch_bounds__(256, HEAVY ? 1 : NSB_MIN_CTAS) tick_kernel(Poo
 // kListCap neurons run the two phases per chunk of kListCap neurons.
 constexpr int kListCap = 768;
 
+#ifndef NSB_LIST_MIN_CTAS
+#define NSB_LIST_MIN_CTAS NSB_MIN_CTAS
+#endif
 template <bool COOP>
-__global__ void __launch_bounds__(256, NSB_MIN_CTAS) tick_kernel_list(Pools P, int unit_begin, int unit_end,
+__global__ void __launch_bounds__(256, NSB_LIST_MIN_CTAS) tick_kernel_list(Pools P, int unit_begin, int unit_end,
                                                                       int *queue, const float *__restrict__ input,
                                                                       const uint8_t *__restrict__ mask,
                                                                       float *__restrict__ output,

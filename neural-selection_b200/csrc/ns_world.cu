@@ -574,6 +574,14 @@ __device__ __forceinline__ void phase_neuron(const WorldArgs &d, const UnitMem &
     phase_neuron_tail(U, n, cur9, s, mod, motor_cnt, tr);
 }
 
+// World animals keep their neurons in list order, so their LP and Prinz cells
+// are spread over the warps, a few each; measured on B200 the warp form is
+// faster there than each cell on its own lane.
+#ifndef NSB_WORLD_WARP_CELLS_MAX
+#define NSB_WORLD_WARP_CELLS_MAX 32
+#endif
+constexpr int kWorldWarpCellsMax = NSB_WORLD_WARP_CELLS_MAX;
+
 // The warp's pending LP and Prinz cells, one after another, each on all 32
 // lanes (ns_physio.cuh: lp_integrate_warp, prinz_tick_warp); the owner lane
 // then completes heavy_tick's arithmetic. All lanes call it together; w is
@@ -581,7 +589,7 @@ __device__ __forceinline__ void phase_neuron(const WorldArgs &d, const UnitMem &
 __device__ __forceinline__ void heavy_cells_warp(const WorldArgs &d, const HeavyJob &job, NeuronRegs &s, float *w,
                                                  int lane, const float *tab) {
     const uint32_t pend = __ballot_sync(0xffffffffu, job.pending != 0);
-    if (__popc(pend) > kWarpCellsMax) {        // many cells: each on its own lane at once
+    if (__popc(pend) > kWorldWarpCellsMax) {   // many cells: each on its own lane at once
         if (job.pending) {
             const ref::NeuronGene &G = d.ngene[job.slot];
             float xg[16] = {};
@@ -704,7 +712,10 @@ __device__ __forceinline__ void atomic_fmax(float *p, float v) {
 
 extern __shared__ __align__(16) unsigned char w_smem[];
 
-constexpr int kClaim = 4;   // animals taken from the living list per claim
+// Animals taken from the living list per claim, in the light and heavy builds
+// alike: a CTA keeps what it claims, so larger claims let a few CTAs take a
+// population whose animals are mostly of one build.
+constexpr int kClaim = 4;
 
 // Small units: animals with at most kBlock neurons and kUnitEdges live
 // synapses, packed in claim order. The light instantiation takes the animals
@@ -767,11 +778,11 @@ __global__ void __launch_bounds__(kBlock, MINB) world_tick_small(WorldArgs d, Ca
             for (;;) {
                 if (q_i >= q_n && !q_done) {
                     int base = 0;
-                    if (lane == 0) base = atomicAdd(queue, HEAVY ? 32 : kClaim);
+                    if (lane == 0) base = atomicAdd(queue, kClaim);
                     base = __shfl_sync(0xffffffffu, base, 0);
                     bool ok = false;
                     int a = -1, nn = 0, nl = 0;
-                    if (lane < (HEAVY ? 32 : kClaim) && base + lane < n_alive) {
+                    if (lane < (kClaim) && base + lane < n_alive) {
                         a = alive[base + lane];
                         if (!compiled(d, c, a)) {
                             if (!HEAVY) atomicOr(status, ST_LIST);    // compile failed (its own bit is set too)
@@ -793,7 +804,7 @@ __global__ void __launch_bounds__(kBlock, MINB) world_tick_small(WorldArgs d, Ca
                         q_a[pos] = a; q_nn[pos] = nn; q_nl[pos] = nl;
                     }
                     __syncwarp();
-                    if (lane == 0) { q_n = __popc(mk); q_i = 0; if (base + (HEAVY ? 32 : kClaim) >= n_alive) q_done = 1; }
+                    if (lane == 0) { q_n = __popc(mk); q_i = 0; if (base + (kClaim) >= n_alive) q_done = 1; }
                     __syncwarp();
                     continue;
                 }
