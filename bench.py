@@ -534,11 +534,13 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local_rank) as clk:
+        torch.cuda.nvtx.range_push("timed")       # profiler captures: ncu --nvtx --nvtx-include timed/
         e0.record(stream)
         for _ in range(args.steps):
             gpu.step_graph(16, batch.gain, s)
         e1.record(stream)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
     ms = e0.elapsed_time(e1)
     events = gpu.take_events()
     if dist:
