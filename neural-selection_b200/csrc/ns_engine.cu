@@ -1326,7 +1326,7 @@ Plan make_plan(const std::vector<BrainSpec> &brains, int channels, int outputs, 
         const int un0 = ncur, ue0 = ecur;
         unitb[ui] = make_int2((int)brain_order.size(), (int)ub.size());
         // Neuron order inside the unit: active before inactive, then by cell
-        // class (type 0 | types 1,4 | type 5 | LP/Prinz/LFS), then by which
+        // class (type 0 | types 1,4 | type 5 | LP | Prinz | LFS), then by which
         // dendritic branches receive excitatory synapses, so that a warp's
         // lanes take the same path through the integrator.
         struct Key { int inactive, cls, bmask, slot, j; };
@@ -1344,7 +1344,9 @@ Plan make_plan(const std::vector<BrainSpec> &brains, int channels, int outputs, 
             }
             for (int j = 0; j < B.count; ++j) {
                 const unsigned char t = B.genes[j].type;
-                const int cls = is_heavy_type(t) ? 3 : (t == 0 ? 0 : (t == 5 ? 2 : 1));
+                // LP, Prinz and LFS cells each in a class of their own, so a
+                // warp's cells run one model at a time instead of diverging
+                const int cls = t == 2 ? 3 : t == 3 ? 4 : t == 6 ? 5 : (t == 0 ? 0 : (t == 5 ? 2 : 1));
                 keys.push_back({B.genes[j].active ? 0 : 1, cls, t == 0 ? bmask[j] : 0, slot, j});
             }
         }
