@@ -1895,6 +1895,24 @@ bool Engine::autotune(int ticks, float gain, cudaStream_t stream) {
     // the big-brain buckets), each candidate timed in the whole step, kept
     // when it saves more than 1 %; at most two passes.
     float best_ms = time_step();
+    // First the whole-batch switches: every light bucket on per-thread
+    // integration, and every big-brain bucket on one CTA per brain (a
+    // descent one bucket at a time can stop short of these).
+    for (int sw = 0; sw < 2; ++sw) {
+        const std::vector<Bucket> saved = buckets_;
+        bool ok = true, any = false;
+        for (int b = 0; b < kBuckets && ok; ++b) {
+            Bucket &B = buckets_[b];
+            if (B.heavy || B.units() == 0) continue;
+            if (sw == 0 && B.cfg.list) { B.cfg.list = 0; B.cfg.cluster = 1; any = true; }
+            if (sw == 1 && B.cfg.cluster > 1) { B.cfg.cluster = 1; any = true; }
+            ok = shape_bucket(B);
+        }
+        if (!any || !ok) { buckets_ = saved; continue; }
+        const float ms = time_step();
+        if (ms < 0.99f * best_ms) best_ms = ms;
+        else buckets_ = saved;
+    }
     const int order[4] = {kBucketPacked, 2, 1, 0};
     for (int pass = 0; pass < 2; ++pass) {
         bool changed = false;

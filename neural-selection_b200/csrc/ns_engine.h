@@ -108,8 +108,10 @@ public:
     // set_cooperative sets every light bucket.
     bool cooperative() const { return buckets_[kBucketPacked].cfg.coop != 0; }
     void set_cooperative(bool coop);
-    // Per-bucket autotuner: coordinate descent over the buckets of work
-    // units; each candidate configuration of a bucket (threads per CTA,
+    // Per-bucket autotuner: two whole-batch switches (every light bucket on
+    // per-thread integration; every big brain on one CTA), then coordinate
+    // descent over the buckets of work units; each candidate configuration
+    // of a bucket (threads per CTA,
     // delivery mode, meta staging depth, list or per-thread integration, one
     // CTA or a cluster for big brains) is timed in whole steps on the
     // engine's own buffers, from the same restored state (so the call has no
