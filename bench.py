@@ -73,13 +73,14 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_per_launch():
-    """DRAM bytes per tick-kernel launch from the committed ncu summary."""
+def traffic_per_step():
+    """DRAM bytes of one step's tick-kernel launches (every bucket) from the
+    committed ncu summary of the full-pool workload."""
     p = ROOT / "profiles" / "tick_kernel_full_pools.txt"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
-        if line.startswith("dram_bytes_per_launch:"):
+        if line.startswith("dram_bytes_per_step:"):
             return float(line.split(":")[1].split()[0])
     return None
 
@@ -585,7 +586,7 @@ def run_ours(args, rank, world, local_rank):
         peak, peak_kind = peaks()
         algo = ALGO_BYTES_PER_NEURON * N + ALGO_BYTES_PER_SYNAPSE * E
         achieved = algo / (ms_step / 1e3) / 1e9
-        traffic = traffic_per_launch() if args.workload == "batched_uneven" else None
+        traffic = traffic_per_step() if args.workload == "batched_uneven" else None
         if traffic is not None:
             traffic /= args.fraction
         clocks = clk.summary()

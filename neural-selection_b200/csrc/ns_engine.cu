@@ -1174,18 +1174,23 @@ void prepare_tick_kernels(int smem) {
     NSB_CHECK(cudaMemcpyToSymbol(c_K, &K, sizeof(PhysConst)));
 }
 
+int serve_smem_bytes(int hw, int meta_cap) { return heavy_smem_bytes(hw, meta_cap); }
+
 int tick_occupancy(int block, int smem) {
-    int occ = 0, occ2 = 0;
-    NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tick_kernel_list<false>, block, smem));
-    NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, tick_kernel_list<true>, block, smem));
-    return std::max(std::min(occ, occ2), 1);
+    int occ = 0;
+    NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tick_kernel<false, true>, block, smem));
+    return std::max(occ, 1);
 }
 
+// The serving loop's units hold one brain each, of up to 4,096 dense
+// neurons: the per-thread kernel with warp-cooperative delivery steps them
+// fastest (the autotuner's choice for that population in static batches).
 void launch_tick_light(const Pools &P, int n_units, int grid, int block, int smem, int *queue, const float *input,
                        const uint8_t *mask, float *output, int *status, int ticks, float gain, cudaStream_t stream) {
     NSB_CHECK(cudaMemsetAsync(queue, 0, sizeof(int), stream));
-    if (n_units > 0) launch_light(true, grid, block, smem, stream, P, 0, n_units, queue, input, mask, output, status,
-                                  ticks, gain);
+    if (n_units > 0)
+        tick_kernel<false, true><<<grid, block, smem, stream>>>(P, 0, n_units, queue, input, mask, output, status,
+                                                                ticks, gain);
     NSB_CHECK(cudaGetLastError());
 }
 
@@ -1809,15 +1814,18 @@ void Engine::step_device(const float *d_input, const uint8_t *d_mask, int ticks,
 void Engine::step_host(const float *input, const uint8_t *mask, int ticks, float gain, float *output, int *status) {
     if (ticks < 1 || ticks > 10000 || !std::isfinite(gain) || gain < 0)
         throw std::runtime_error("Invalid neural integration interval");
-    for (int i = 0; i < n_brains_; ++i)
-        if (mask[i])
-            for (int j = 0; j < channels_; ++j) {
-                const float v = input[(size_t)i * channels_ + j];
-                if (!std::isfinite(v) || v < 0 || v > 1) throw std::runtime_error("Invalid encoded observation");
-            }
+    // An observation outside [0, 1] is invalid; NaN and the infinities fail
+    // one of the two comparisons. The row test has no branch, so it vectorises.
+    for (int i = 0; i < n_brains_; ++i) {
+        if (!mask[i]) continue;
+        const float *row = input + (size_t)i * channels_;
+        bool ok = true;
+        for (int j = 0; j < channels_; ++j) ok &= (row[j] >= 0.0f) & (row[j] <= 1.0f);
+        if (!ok) throw std::runtime_error("Invalid encoded observation");
+    }
     NSB_CHECK(cudaMemcpyAsync(d_input_, input, (size_t)n_brains_ * channels_ * sizeof(float), cudaMemcpyHostToDevice, stream_));
     NSB_CHECK(cudaMemcpyAsync(d_mask_, mask, n_brains_, cudaMemcpyHostToDevice, stream_));
-    launch(d_input_, d_mask_, ticks, gain, d_output_, d_status_, stream_);
+    step_graph(ticks, gain, stream_);          // the step's launches, replayed from the captured graph
     NSB_CHECK(cudaMemcpyAsync(output, d_output_, (size_t)n_brains_ * outputs_ * sizeof(float), cudaMemcpyDeviceToHost, stream_));
     NSB_CHECK(cudaMemcpyAsync(status, d_status_, n_brains_ * sizeof(int), cudaMemcpyDeviceToHost, stream_));
     NSB_CHECK(cudaStreamSynchronize(stream_));

@@ -100,9 +100,13 @@ int tick_smem_bytes(int hw, int meta_cap = kMetaCap);
 // Binds the physiology constants and the tick kernels' shared-memory limit on
 // the current device (idempotent).
 void prepare_tick_kernels(int smem);
-// Resident CTAs per SM of the light tick kernel.
+// Dynamic shared memory of the serving loop's tick kernel (per-thread
+// integration, warp-cooperative delivery).
+int serve_smem_bytes(int hw, int meta_cap = kMetaCap);
+// Resident CTAs per SM of the serving loop's tick kernel.
 int tick_occupancy(int block, int smem);
-// Light tick kernel over units [0, n_units) of P (queue reset on `stream`).
+// The serving loop's tick kernel over units [0, n_units) of P (queue reset on
+// `stream`).
 void launch_tick_light(const Pools &P, int n_units, int grid, int block, int smem, int *queue, const float *input,
                        const uint8_t *mask, float *output, int *status, int ticks, float gain, cudaStream_t stream);
 

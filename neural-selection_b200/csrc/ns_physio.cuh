@@ -163,7 +163,8 @@ template <int N> __device__ __forceinline__ void crexp_n(const float (&x)[N], fl
 // lp_rates with its 21 exponentials computed as one batch (crexp_n): the
 // arguments, the sigmoids 1 / (1 + e) and the derivative assembly are the
 // operations of the reference, in its order.
-static __device__ __noinline__ void lp_rates(const float *x, float i_na, const float *sc, float *d, const float *tab) {
+__device__ __forceinline__ void lp_rates(const float (&x)[16], float i_na, const float (&sc)[4], float (&d)[16],
+                                         const float *tab) {
     const float va = x[0], vs = x[15], cai = x[13];
     float A[21], E[21];
     A[0] = vs / 11.4866f;
@@ -227,19 +228,44 @@ static __device__ __noinline__ void lp_rates(const float *x, float i_na, const f
     d[13] = -.05049639866f * ca - .01729930764f * (cai - .02f);
     d[14] = (sig(19) - x[14]) * .0001386796618f * sig(20);
 }
-static __device__ __noinline__ void lp_integrate(float *x, float i_na, const float *sc, const float *tab) {
+// lp_integrate on the state xs (16 floats in memory): 20 classical RK4 steps
+// of 0.05 ms with the state, the four scales and the stage sums in registers.
+// The four stages run as one loop over a single copy of lp_rates. The stage
+// sum k1 + 2 k2 + 2 k3 + k4 accumulates left to right, the order of the
+// reference's expression, so every rounding is the same.
+static __device__ __noinline__ void lp_integrate(float *xs, float i_na, const float *scs, const float *tab) {
     const float dt = .05f;
-    float k1[16], k2[16], k3[16], k4[16], y[16];
+    float x[16], y[16], k[16], acc[16], sc[4];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) x[j] = xs[j];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) sc[j] = scs[j];
+#pragma unroll 1
     for (int step = 0; step < 20; ++step) {
-        lp_rates(x, i_na, sc, k1, tab);
-        for (int j = 0; j < 16; ++j) y[j] = x[j] + .5f * dt * k1[j];
-        lp_rates(y, i_na, sc, k2, tab);
-        for (int j = 0; j < 16; ++j) y[j] = x[j] + .5f * dt * k2[j];
-        lp_rates(y, i_na, sc, k3, tab);
-        for (int j = 0; j < 16; ++j) y[j] = x[j] + dt * k3[j];
-        lp_rates(y, i_na, sc, k4, tab);
-        for (int j = 0; j < 16; ++j) x[j] += dt * (k1[j] + 2 * k2[j] + 2 * k3[j] + k4[j]) / 6.0f;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) y[j] = x[j];
+#pragma unroll 1
+        for (int st = 0; st < 4; ++st) {
+            lp_rates(y, i_na, sc, k, tab);
+            if (st == 0) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) acc[j] = k[j];
+            } else if (st < 3) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) acc[j] = acc[j] + 2 * k[j];
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) acc[j] = acc[j] + k[j];
+            }
+            const float c = st < 2 ? .5f * dt : dt;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) y[j] = x[j] + c * k[j];
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) x[j] += dt * acc[j] / 6.0f;
     }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) xs[j] = x[j];
 }
 
 // ---- Prinz pacemaker (prinz_cell.cuh:45-121); u = {v, ca, m[7], h[4]} -------------
@@ -251,8 +277,8 @@ __device__ __forceinline__ float pz_gate2(float v, float a, float b, float c, fl
 }
 // pz_substep with its exponentials computed as two batches (crexp_n): the
 // voltage's gates and time constants, then the relaxations that use them.
-static __device__ __noinline__ void pz_substep(float *u, const float *g, float ext, float clamp_ns, float clamp_rev,
-                                        const float *tab) {
+__device__ __forceinline__ void pz_substep(float (&u)[13], const float (&g)[9], float ext, float clamp_ns,
+                                           float clamp_rev, const float *tab) {
     const float dt = .025f;
     float *m = u + 2, *h = u + 9;
     const float v = u[0], ca = fmaxf(u[1], 0.000001f);
@@ -287,6 +313,7 @@ static __device__ __noinline__ void pz_substep(float *u, const float *g, float e
                         g[6] * m[6], g[7]};
     const float rev[8] = {50, eca, eca, -80, -80, -80, -20, -50};
     float gt = clamp_ns, ws = ext + clamp_ns * clamp_rev;
+#pragma unroll
     for (int i = 0; i < 8; ++i) { gt += c[i]; ws += c[i] * rev[i]; }
     const float mi[7] = {gate(0), gate(1), gate(2), gate(3), (ca / (ca + 3)) * gate(4), gate(5), gate(6)};
     const float mt[7] = {2.64f - 2.52f * gate(7), 43.4f - 42.6f * gate(8), 2.8f + 14 * (1.0f / (E[18] + E[19])),
@@ -308,8 +335,32 @@ static __device__ __noinline__ void pz_substep(float *u, const float *g, float e
     const float ica = (c[1] + c[2]) * (v - eca) / 1000000.0f;
     const float cat = .05f - 14961.0f * ica;
     u[1] = fmaxf(.000001f, cat + (ca - cat) * c_K.prinz_ca);
+#pragma unroll
     for (int i = 0; i < 7; ++i) m[i] = mi[i] + (m[i] - mi[i]) * F[1 + i];
+#pragma unroll
     for (int i = 0; i < 4; ++i) h[i] = hi[i] + (h[i] - hi[i]) * F[8 + i];
+}
+
+// The Prinz cell's 40 substeps of one tick on xs (13 state floats in memory),
+// with the state and conductances in registers; returns whether the voltage
+// crossed 0 mV upwards in any substep.
+static __device__ __noinline__ bool prinz_tick(float *xs, const float *gs, float ext, float clamp_ns, float clamp_rev,
+                                               const float *tab) {
+    float u[13], g[9];
+#pragma unroll
+    for (int j = 0; j < 13; ++j) u[j] = xs[j];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) g[j] = gs[j];
+    bool spiked = false;
+#pragma unroll 1
+    for (int i = 0; i < 40; ++i) {
+        const float before = u[0];
+        pz_substep(u, g, ext, clamp_ns, clamp_rev, tab);
+        spiked |= before < 0 && u[0] >= 0;
+    }
+#pragma unroll
+    for (int j = 0; j < 13; ++j) xs[j] = u[j];
+    return spiked;
 }
 
 // Heavy cell types (2 LP, 3 Prinz, 6 LFS) on their extended state x (16 floats).
@@ -335,12 +386,7 @@ static __device__ __noinline__ NeuronRegs heavy_tick(const float *g, uint32_t ty
         s.total += (int)s.spike;
     } else {
         const float ext = cur + exc * (0.0f - s.v) + s.inh * (-75.0f - s.v);
-        bool spiked = false;
-        for (int i = 0; i < 40; ++i) {
-            const float before = x[0];
-            pz_substep(x, xg, ext, xg[8] + clamp_leak, clamp_rev, tab);
-            spiked |= before < 0 && x[0] >= 0;
-        }
+        const bool spiked = prinz_tick(x, xg, ext, xg[8] + clamp_leak, clamp_rev, tab);
         s.spike = spiked ? 1u : 0u;
         s.total += (int)s.spike;
         s.v = x[0];
@@ -646,12 +692,7 @@ __device__ __forceinline__ float heavy_model_lane(uint32_t type, float *x, const
         lp_integrate(x, ext / 1000.0f, xg, tab);
         return ab;
     }
-    spiked = false;
-    for (int i = 0; i < 40; ++i) {
-        const float before = x[0];
-        pz_substep(x, xg, ext, xg[8] + 0.0f, -68.0f, tab);
-        spiked |= before < 0 && x[0] >= 0;
-    }
+    spiked = prinz_tick(x, xg, ext, xg[8] + 0.0f, -68.0f, tab);
     return 0.0f;
 }
 

@@ -189,7 +189,7 @@ Server::Server(const ServeConfig &cfg) : cfg_(cfg) {
     NSB_CHECK(cudaGetDevice(&dev_));
     NSB_CHECK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev_));
     hw_ = spike_words(std::max(cfg.max_brain_neurons, unit_cap_), cfg.block);
-    smem_ = tick_smem_bytes(hw_);
+    smem_ = serve_smem_bytes(hw_);
     prepare_tick_kernels(smem_);
     grid_cap_ = sms_ * tick_occupancy(cfg.block, smem_);
 
