@@ -177,6 +177,7 @@ Engine &brain_engine(HostBrain &b) {
         cfg.max_delay = b.max_delay;
         cfg.block = 128;
         if (const char *cl = std::getenv("NSB_CLUSTER")) cfg.cluster_big = std::atoi(cl);
+        if (const char *wc = std::getenv("NSB_WARP_CELLS")) cfg.warp_cells = std::atoi(wc);
         b.engine = std::make_unique<Engine>(specs, b.channels, (int)b.motors.size(), cfg);
         // A brain stepped before any reset starts from its host records
         // (value-initialised by ns_create, as in the reference).
@@ -302,6 +303,7 @@ static void *gpu_create(void **handles, int count, int max_delay_floor, int bloc
     if (block) cfg.block = block;
     if (const char *slots = std::getenv("NSB_UNIT_SLOTS")) cfg.unit_slots = std::max(1, std::atoi(slots));
     if (const char *cl = std::getenv("NSB_CLUSTER")) cfg.cluster_big = std::atoi(cl);
+    if (const char *wc = std::getenv("NSB_WARP_CELLS")) cfg.warp_cells = std::atoi(wc);
     auto batch = std::make_unique<GpuBatch>();
     batch->engine = std::make_unique<Engine>(specs, channels, outputs, cfg);
     batch->channels = channels;

@@ -325,6 +325,18 @@ __device__ __forceinline__ void finish_synapses(const Pools &P, int ib, int ie, 
 
 extern __shared__ __align__(16) unsigned char g_smem[];
 
+// A heavy unit's pool of pending LP and Prinz cells (one entry per thread at
+// most). The counter alternates between two words from call to call, so that
+// each pooling needs only its two barriers: a call reads n[p] between them and
+// clears n[p ^ 1], which the previous call read and the next call fills.
+template <int NT> struct UnitHeavyPool {
+    int n[2];
+    int xidx[NT];
+    float ext[NT];
+    float res[NT];       // LP: the axon voltage before the tick; Prinz: 1 when it spiked
+    uint8_t type[NT];
+};
+
 // One launch steps every unit of [unit_begin, unit_end) through `ticks`
 // ticks. Units are pulled from `queue` (reset to 0 before the launch).
 template <bool HEAVY, bool COOP>
@@ -344,11 +356,14 @@ __global__ void __launch_bounds__(256, HEAVY ? 1 : NSB_MIN_CTAS) tick_kernel(Poo
     float *s_heavy = reinterpret_cast<float *>(s_evv + 8 * kEvCap);       // 8 warps x kHeavyWarpScratch
     __shared__ int s_unit;
     __shared__ unsigned long long s_events;
+    __shared__ UnitHeavyPool<HEAVY ? 256 : 1> s_pool;
 
     const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarp = bs >> 5;
+    int hcall = 0;   // poolings so far (HEAVY)
     {
         const float *src = nsx::exp2f_table();
         for (int i = tid; i < 256; i += bs) tab[i] = src[i];
+        if (HEAVY && tid == 0) s_pool.n[0] = s_pool.n[1] = 0;
     }
     for (;;) {
         if (tid == 0) { s_unit = unit_begin + atomicAdd(queue, 1); s_events = 0; }
@@ -473,29 +488,55 @@ __global__ void __launch_bounds__(256, HEAVY ? 1 : NSB_MIN_CTAS) tick_kernel(Poo
                     }
                 }
                 if (HEAVY) {
-                    // The warp's LP and Prinz cells, one after another, each on all 32 lanes.
+                    // The unit's pending LP and Prinz cells: a warp that owned
+                    // several would step them one after another while the rest
+                    // of the CTA waited, so the CTA pools them and the warps take
+                    // the pool round-robin, each cell on all 32 lanes; with more
+                    // than wc cells per warp on average, each cell runs on its
+                    // owner lane at once instead.
                     float axon_before = 0.0f;
                     bool spiked = false;
-                    const uint32_t pend = __ballot_sync(0xffffffffu, pending);
-                    if (__popc(pend) > kWarpCellsMax && pending)
-                        axon_before = heavy_model_lane(type, P.xstate + (size_t)xidx * 16, P.xgene + (size_t)xidx * 16,
-                                                       ext, spiked, tab);
-                    for (uint32_t pm = __popc(pend) > kWarpCellsMax ? 0u : pend; pm; pm &= pm - 1u) {
-                        const int L = __ffs(pm) - 1;
-                        const int xi = __shfl_sync(0xffffffffu, xidx, L);
-                        const uint32_t ty = __shfl_sync(0xffffffffu, type, L);
-                        const float ex = __shfl_sync(0xffffffffu, ext, L);
-                        float *x = P.xstate + (size_t)xi * 16;
-                        const float *xg = P.xgene + (size_t)xi * 16;
-                        if (ty == 2) {
-                            const float ab = x[0];
-                            lp_integrate_warp(x, ex / 1000.0f, xg, s_heavy + warp * kHeavyWarpScratch, lane, tab);
-                            if (lane == L) axon_before = ab;
-                        } else {
-                            const bool sp = prinz_tick_warp(x, xg, ex, xg[8] + 0.0f, -68.0f,
-                                                            s_heavy + warp * kHeavyWarpScratch, lane, tab);
-                            if (lane == L) spiked = sp;
+                    const int p = hcall & 1;
+                    ++hcall;
+                    int k = 0;
+                    if (pending) {
+                        k = atomicAdd(&s_pool.n[p], 1);
+                        s_pool.xidx[k] = xidx;
+                        s_pool.ext[k] = ext;
+                        s_pool.type[k] = (uint8_t)type;
+                    }
+                    __syncthreads();
+                    const int np = s_pool.n[p];
+                    if (tid == 0) s_pool.n[p ^ 1] = 0;
+                    const int wc = P.warp_cells >= 0 ? P.warp_cells : kWarpCellsMax;
+                    const bool lanes = np > wc * nwarp;
+                    if (lanes) {
+                        if (pending)
+                            axon_before = heavy_model_lane(type, P.xstate + (size_t)xidx * 16,
+                                                           P.xgene + (size_t)xidx * 16, ext, spiked, tab);
+                    } else {
+                        for (int e = warp; e < np; e += nwarp) {
+                            const int xi = s_pool.xidx[e];
+                            const uint32_t ty = s_pool.type[e];
+                            const float ex = s_pool.ext[e];
+                            float *x = P.xstate + (size_t)xi * 16;
+                            const float *xg = P.xgene + (size_t)xi * 16;
+                            if (ty == 2) {
+                                const float ab = x[0];
+                                lp_integrate_warp(x, ex / 1000.0f, xg, s_heavy + warp * kHeavyWarpScratch, lane, tab);
+                                if (lane == 0) s_pool.res[e] = ab;
+                            } else {
+                                const bool sp = prinz_tick_warp(x, xg, ex, xg[8] + 0.0f, -68.0f,
+                                                                s_heavy + warp * kHeavyWarpScratch, lane, tab);
+                                if (lane == 0) s_pool.res[e] = sp ? 1.0f : 0.0f;
+                            }
+                            __syncwarp();
                         }
+                    }
+                    __syncthreads();
+                    if (pending && !lanes) {
+                        axon_before = type == 2 ? s_pool.res[k] : 0.0f;
+                        spiked = type == 3 && s_pool.res[k] != 0.0f;
                     }
                     if (pending) {
                         heavy_post(type, s, P.xstate + (size_t)xidx * 16, axon_before, spiked);
@@ -1205,7 +1246,7 @@ template <class T> T *Engine::alloc(size_t n) {
 static bool excitatory_type(unsigned char t) { return t == 0 || t == 4 || t == 5; }
 
 Plan make_plan(const std::vector<BrainSpec> &brains, int channels, int outputs, int max_delay, int unit_cap,
-               bool cluster_big) {
+               bool cluster_big, int heavy_target) {
     Plan p;
     const int n_brains = (int)brains.size();
     // ---- validate and size ----
@@ -1228,17 +1269,25 @@ Plan make_plan(const std::vector<BrainSpec> &brains, int channels, int outputs, 
 
     // ---- work units ------------------------------------------------------------
     // Brains with LP/Prinz/LFS cells go to units of their own (stepped by the
-    // heavy kernel). Within each group a brain above the CTA size is a unit of
-    // its own; smaller brains are packed best-fit decreasing.
+    // heavy kernel). Within each group a brain above the group's unit capacity
+    // is a unit of its own; smaller brains are packed best-fit decreasing. The
+    // heavy kernel runs one CTA per SM and its cell models are long chains per
+    // lane, so its units are sized to spread the heavy neurons over
+    // heavy_target SMs rather than filled to unit_cap.
     auto is_heavy_type = [](unsigned char t) { return t == 2 || t == 3 || t == 6; };
     std::vector<char> brain_heavy(n_brains, 0);
+    long long heavy_neurons = 0;
     for (int b = 0; b < n_brains; ++b)
         for (int j = 0; j < brains[b].count; ++j)
-            if (is_heavy_type(brains[b].genes[j].type)) { brain_heavy[b] = 1; break; }
+            if (is_heavy_type(brains[b].genes[j].type)) { brain_heavy[b] = 1; heavy_neurons += brains[b].count; break; }
+    const int heavy_cap = heavy_target > 0
+        ? (int)std::min<long long>(unit_cap, std::max<long long>(1, (heavy_neurons + heavy_target - 1) / heavy_target))
+        : unit_cap;
     std::vector<std::vector<int>> unit_brains;
     std::vector<int> unit_fill;
     std::vector<char> unit_heavy;
     for (int group = 0; group < 2; ++group) {
+        const int cap = group ? heavy_cap : unit_cap;
         std::vector<int> order;
         for (int b = 0; b < n_brains; ++b)
             if (brain_heavy[b] == group) order.push_back(b);
@@ -1246,7 +1295,7 @@ Plan make_plan(const std::vector<BrainSpec> &brains, int channels, int outputs, 
         std::multimap<int, int> open;   // remaining capacity -> unit
         for (int b : order) {
             const int n = brains[b].count;
-            if (n > unit_cap) {
+            if (n > cap) {
                 unit_brains.push_back({b}); unit_fill.push_back(n); unit_heavy.push_back((char)group);
                 continue;
             }
@@ -1256,11 +1305,11 @@ Plan make_plan(const std::vector<BrainSpec> &brains, int channels, int outputs, 
                 open.erase(it);
                 unit_brains[uidx].push_back(b);
                 unit_fill[uidx] += n;
-                const int rem = unit_cap - unit_fill[uidx];
+                const int rem = cap - unit_fill[uidx];
                 if (rem > 0 && (int)unit_brains[uidx].size() < kMaxUnitBrains) open.emplace(rem, uidx);
             } else {
                 unit_brains.push_back({b}); unit_fill.push_back(n); unit_heavy.push_back((char)group);
-                const int rem = unit_cap - n;
+                const int rem = cap - n;
                 if (rem > 0) open.emplace(rem, (int)unit_brains.size() - 1);
             }
         }
@@ -1477,19 +1526,20 @@ Engine::Engine(const std::vector<BrainSpec> &brains, int channels, int outputs, 
     n_brains_ = (int)brains.size();
     channels_ = channels; outputs_ = outputs; max_delay_ = cfg.max_delay; block_ = cfg.block;
     count_events_ = cfg.count_events;
+    warp_cells_ = cfg.warp_cells;
     unit_cap_ = block_ * (cfg.unit_slots > 0 ? cfg.unit_slots : 3);
     int dev0 = 0, sms0 = 0;
     NSB_CHECK(cudaGetDevice(&dev0));
     NSB_CHECK(cudaDeviceGetAttribute(&sms0, cudaDevAttrMultiProcessorCount, dev0));
-    Plan p = make_plan(brains, channels, outputs, max_delay_, unit_cap_, cfg.cluster_big == 1);
+    Plan p = make_plan(brains, channels, outputs, max_delay_, unit_cap_, cfg.cluster_big == 1, sms0);
     if (cfg.unit_slots <= 0 && p.n_light_units < sms0 * NSB_MIN_CTAS) {
         // A batch too small to fill the GPU: one neuron per thread, so each
         // unit's tick is one neuron update long instead of three.
         unit_cap_ = block_;
-        p = make_plan(brains, channels, outputs, max_delay_, unit_cap_, cfg.cluster_big == 1);
+        p = make_plan(brains, channels, outputs, max_delay_, unit_cap_, cfg.cluster_big == 1, sms0);
     }
     if (cfg.cluster_big < 0 && p.n_big_units > 0 && p.n_light_units < sms0 * NSB_MIN_CTAS)
-        p = make_plan(brains, channels, outputs, max_delay_, unit_cap_, true);
+        p = make_plan(brains, channels, outputs, max_delay_, unit_cap_, true, sms0);
     n_neurons_ = p.n_neurons; n_synapses_ = p.n_synapses; n_units_ = p.n_units; n_light_units_ = p.n_light_units;
     n_big_units_ = p.n_big_units; n_heavy_ = p.n_heavy; max_unit_neurons_ = p.max_unit_neurons;
     max_unit_brains_ = p.max_unit_brains;
@@ -1686,6 +1736,7 @@ Pools Engine::pools(bool events) const {
     P.events = events ? d_events_ : nullptr;
     P.pulse_period = pulse_period_;
     P.pulse_mod = pulse_mod_;
+    P.warp_cells = warp_cells_;
     return P;
 }
 

@@ -38,6 +38,10 @@ struct EngineConfig {
     // big brain spread over up to 8 SMs; in full batches the one-CTA path
     // has the higher throughput).
     int cluster_big = -1;
+    // LP and Prinz cells per warp up to which a heavy unit steps them one
+    // after another on the whole warp instead of each on its own lane; -1: the
+    // build's default (per lane). Both forms give the same bits.
+    int warp_cells = -1;
 };
 
 struct Stats {
@@ -171,6 +175,7 @@ private:
     cudaStream_t bstream_[kBuckets] = {};
     cudaEvent_t fork_ = nullptr, join_[kBuckets] = {};
     bool count_events_ = true;
+    int warp_cells_ = -1;        // EngineConfig::warp_cells
     bool coop_ = false;
     int pulse_period_ = 0;
     uint32_t pulse_mod_ = 0;

@@ -52,6 +52,10 @@ struct Pools {
     // reads them from global memory); the launch's dynamic shared memory is
     // sized for it.
     int meta_cap = kMetaCap;
+    // Heavy units: a warp with more LP and Prinz cells than this steps each on
+    // its own lane, with fewer one after another on the whole warp; -1: the
+    // build's default (kWarpCellsMax).
+    int warp_cells = -1;
 };
 
 // Host plan of a set of brains: work units and every pool record, indexed
@@ -82,10 +86,12 @@ struct Plan {
 
 // Packs brains into units of at most unit_cap neurons (best-fit decreasing;
 // a larger brain is a unit of its own; brains with LP/Prinz/LFS cells in
-// separate, heavy units) and lays out their records. Throws
+// separate, heavy units) and lays out their records. With heavy_target > 0
+// the heavy units hold about 1/heavy_target of the heavy brains' neurons each
+// (at most unit_cap), so that they spread over that many SMs. Throws
 // std::runtime_error on invalid input with the reference's messages.
 Plan make_plan(const std::vector<BrainSpec> &brains, int channels, int outputs, int max_delay, int unit_cap,
-               bool cluster_big = false);
+               bool cluster_big = false, int heavy_target = 0);
 // Cluster sizes of the three big-brain groups, in queue order.
 constexpr int kClusterSizes[3] = {8, 4, 2};
 

@@ -142,6 +142,29 @@ __device__ __forceinline__ float lp_sig(float v, float mid, float slope, const f
     return 1.0f / (1.0f + crexp((v - mid) / slope, tab));
 }
 __device__ __forceinline__ float lp_ratio(float num, float den, float lim) { return fabsf(den) < 1e-5f ? lim : num / den; }
+
+// N independent quotients a[i] / b[i] (IEEE division). The compiled division
+// was measured against straight-line alternatives on B200 (a binary64
+// Newton-Raphson quotient rounded once; a binary32 Markstein quotient proved by
+// its exact remainder): both gave the same bits and both were slower, since
+// every reciprocal goes through the special-function unit and the proof adds
+// a dozen dependent operations per quotient.
+template <int N> __device__ __forceinline__ void fdiv_n(const float (&a)[N], const float (&b)[N], float (&q)[N]) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) q[i] = a[i] / b[i];
+}
+
+// Exponentials in the LP and Prinz models. A batch whose binary64 fallback
+// (expf_cr_wide, an out-of-line call) sits inside the integration loop was
+// measured 2.7 times slower per exponential on B200 than the same binary32
+// fast paths alone, although the fallback almost never runs: the call's
+// register contract weighs on the whole loop. So the models' hot loops use
+// the fast paths alone (exp_n<false>), which report in `ok` whether every
+// result stands; an integration step with any undecided exponential (about
+// one argument in 8,000) is recomputed from its saved state by an out-of-line
+// copy of the same step that uses crexp_n (exp_n<true>). The results are the
+// correctly rounded ones either way.
+//
 // Correctly rounded exponentials of N independent arguments: every binary32
 // fast path first, with no branch between them, so that they interleave;
 // then the binary64 path for any argument that needs it (rare).
@@ -159,110 +182,206 @@ template <int N> __device__ __forceinline__ void crexp_n(const float (&x)[N], fl
             if (!ok[i]) y[i] = nsx::expf_cr_wide(x[i]);
     }
 }
+// SAFE: crexp_n. Otherwise the binary32 fast paths alone; `ok` is cleared when
+// any of them is undecided (its result then must not be used).
+template <bool SAFE, int N>
+__device__ __forceinline__ void exp_n(const float (&x)[N], float (&y)[N], const float *tab, bool &ok) {
+    if (SAFE) {
+        crexp_n(x, y, tab);
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            bool oi;
+            y[i] = nsx::expf_cr_fast(x[i], tab, oi);
+            ok = ok && oi;
+        }
+    }
+}
+template <bool SAFE> __device__ __forceinline__ float exp1(float x, const float *tab, bool &ok) {
+    if (SAFE) return crexp(x, tab);
+    bool oi;
+    const float y = nsx::expf_cr_fast(x, tab, oi);
+    ok = ok && oi;
+    return y;
+}
 
-// lp_rates with its 21 exponentials computed as one batch (crexp_n): the
-// arguments, the sigmoids 1 / (1 + e) and the derivative assembly are the
-// operations of the reference, in its order.
+// lp_rates with its 21 exponentials computed as one batch (crexp_n) and its
+// 40 quotients as three (fdiv_n: the exponents' arguments; the sigmoids and
+// ratios; the three that use those). Every argument, sigmoid and assembly is
+// the reference's operation in its order; x / 4 and x / 8 are written as the
+// products by 0.25 and 0.125, which round the same exact value.
+template <bool SAFE>
 __device__ __forceinline__ void lp_rates(const float (&x)[16], float i_na, const float (&sc)[4], float (&d)[16],
-                                         const float *tab) {
+                                         const float *tab, bool &ok) {
     const float va = x[0], vs = x[15], cai = x[13];
+    float N1[17], D1[17], Q1[17];
+    N1[0] = vs;                          D1[0] = 11.4866f;
+    N1[1] = vs - 55.0f;                  D1[1] = -15.0f;
+    N1[2] = va;                          D1[2] = 5.0f;
+    N1[3] = va;                          D1[3] = 18.0f;
+    N1[4] = va;                          D1[4] = 40.0f;
+    N1[5] = vs - 15.0f;                  D1[5] = -9.8f;
+    N1[6] = vs - -40.0f;                 D1[6] = 3.2f;
+    N1[7] = vs - -15.0f;                 D1[7] = -10.0f;
+    N1[8] = vs - 29.1336f;               D1[8] = -4.43083f;
+    N1[9] = vs - -.6f * cai;             D1[9] = -23.0f;
+    N1[10] = vs - (-16.0f - .6f * cai);  D1[10] = -5.0f;
+    N1[11] = vs - -12.0f;                D1[11] = -26.0f;
+    N1[12] = vs - -62.0f;                D1[12] = 6.0f;
+    N1[13] = vs - -40.0f;                D1[13] = -12.0f;
+    N1[14] = vs - -110.0f;               D1[14] = -21.6f;
+    N1[15] = va - -26.9916223f;          D1[15] = -5.957441281f;
+    N1[16] = va - -60.57875745f;         D1[16] = -13.25674673f;
+    fdiv_n(N1, D1, Q1);
     float A[21], E[21];
-    A[0] = vs / 11.4866f;
-    A[1] = (vs - 55.0f) / -15.0f;
-    A[2] = -13.0f - va / 4.0f;
-    A[3] = va / 5.0f + 5.0f;
-    A[4] = -2.66666666667f - va / 18.0f;
-    A[5] = -5.0f - va / 5.0f;
-    A[6] = -10.0f - va / 5.0f;
-    A[7] = -1.375f - va / 40.0f;
-    A[8] = (vs - 15.0f) / -9.8f;
-    A[9] = (vs - -40.0f) / 3.2f;
-    A[10] = (vs - -15.0f) / -10.0f;
-    A[11] = (vs - 29.1336f) / -4.43083f;
-    A[12] = (vs - -.6f * cai) / -23.0f;
-    A[13] = (vs - (-16.0f - .6f * cai)) / -5.0f;
-    A[14] = (vs - -12.0f) / -26.0f;
-    A[15] = (vs - -62.0f) / 6.0f;
-    A[16] = (vs - -40.0f) / -12.0f;
-    A[17] = (vs - -70.0f) / 8.0f;
-    A[18] = (vs - -110.0f) / -21.6f;
-    A[19] = (va - -26.9916223f) / -5.957441281f;
-    A[20] = (va - -60.57875745f) / -13.25674673f;
-    crexp_n(A, E, tab);
-    auto sig = [&](int i) { return 1.0f / (1.0f + E[i]); };
+    A[0] = Q1[0];
+    A[1] = Q1[1];
+    A[2] = -13.0f - va * 0.25f;          // va / 4
+    A[3] = Q1[2] + 5.0f;
+    A[4] = -2.66666666667f - Q1[3];
+    A[5] = -5.0f - Q1[2];
+    A[6] = -10.0f - Q1[2];
+    A[7] = -1.375f - Q1[4];
+    A[8] = Q1[5];
+    A[9] = Q1[6];
+    A[10] = Q1[7];
+    A[11] = Q1[8];
+    A[12] = Q1[9];
+    A[13] = Q1[10];
+    A[14] = Q1[11];
+    A[15] = Q1[12];
+    A[16] = Q1[13];
+    A[17] = (vs - -70.0f) * 0.125f;      // (vs + 70) / 8
+    A[18] = Q1[14];
+    A[19] = Q1[15];
+    A[20] = Q1[16];
+    exp_n<SAFE>(A, E, tab, ok);
     const float na = x[1] * x[1] * x[1] * x[2] * 7.15f * (va - 50.0f);
     const float kd = x[8] * x[8] * x[8] * x[8] * 1.43f * (va + 72.0f);
     const float km = .2613041227f * x[14] * (va + 80.0f);
     const float aleak = sc[3] * .001004288227f * (va + 50.0f);
     const float cpl = .004017089073f * (vs - va);
-    d[0] = (-na - kd - km - aleak + cpl) / .1148312178f;
     const float ev = E[0];
-    const float ghk = fabsf(vs) < .001f ? 11.4866f * (x[13] - 15123.5f) : vs * (x[13] * ev - 15123.5f) / (ev - 1.0f);
+    // the sigmoids 1 / (1 + E[i]) of i = 1, 8..20 (Q2[0], Q2[i - 7]), the GHK
+    // quotient, the rate ratios, the calcium-dependent quotient and d[0]
+    float N2[21], D2[21], Q2[21];
+    N2[0] = 1.0f;                                D2[0] = 1.0f + E[1];
+#pragma unroll
+    for (int i = 8; i <= 20; ++i) { N2[i - 7] = 1.0f; D2[i - 7] = 1.0f + E[i]; }
+    N2[14] = vs * (x[13] * ev - 15123.5f);       D2[14] = ev - 1.0f;
+    N2[15] = -16.64f - .32f * va;                D2[15] = E[2] - 1.0f;
+    N2[16] = .28f * va + 7.0f;                   D2[16] = E[3] - 1.0f;
+    N2[17] = 4.0f;                               D2[17] = E[5] + 1.0f;
+    N2[18] = -1.6f - .032f * va;                 D2[18] = E[6] - 1.0f;
+    N2[19] = .7f;                                D2[19] = .6f + cai;
+    N2[20] = -na - kd - km - aleak + cpl;        D2[20] = .1148312178f;
+    fdiv_n(N2, D2, Q2);
+    auto sig = [&](int i) { return i == 1 ? Q2[0] : Q2[i - 7]; };
+    d[0] = Q2[20];
+    const float ghk = fabsf(vs) < .001f ? 11.4866f * (x[13] - 15123.5f) : Q2[14];
     const float ca = sc[0] * (x[3] * x[4] * .1247796343f + x[5] * .07142141077f) * .00155982f * ghk * .9f;
     const float kca = sc[1] * x[6] * x[7] * 1.663612026f * (vs + 72.0f) * .9f;
     const float amix = sig(1);
     const float ka = x[9] * x[9] * x[9] * .8008791415f * (vs + 72.0f) * (amix * x[10] + (1.0f - amix) * x[11]) * .9f;
     const float ih = sc[2] * x[12] * .0126874385f * (vs + 20.0f) * .9f;
     const float sleak = sc[3] * .0006901584324f * (vs + 50.0f);
-    d[15] = (-ca - kca - ka - ih - sleak - cpl + (i_na - 2.0f) * .01222505828f) / .0543909161f;
-    float a = lp_ratio(-16.64f - .32f * va, E[2] - 1.0f, 1.28f);
-    float b = lp_ratio(.28f * va + 7.0f, E[3] - 1.0f, 1.4f);
+    float N3[3], D3[3], Q3[3];
+    N3[0] = -ca - kca - ka - ih - sleak - cpl + (i_na - 2.0f) * .01222505828f;   D3[0] = .0543909161f;
+    N3[1] = sig(12) * sig(13) * cai;                                              D3[1] = 2.5f + cai;
+    N3[2] = (sig(17) - x[12]) * .00033f;                                          D3[2] = sig(18);
+    fdiv_n(N3, D3, Q3);
+    d[15] = Q3[0];
+    float a = fabsf(D2[15]) < 1e-5f ? 1.28f : Q2[15];
+    float b = fabsf(D2[16]) < 1e-5f ? 1.4f : Q2[16];
     d[1] = a * (1.0f - x[1]) - b * x[1];
     a = .128f * E[4];
-    b = 4.0f / (E[5] + 1.0f);
+    b = Q2[17];
     d[2] = a * (1.0f - x[2]) - b * x[2];
-    a = lp_ratio(-1.6f - .032f * va, E[6] - 1.0f, .16f);
+    a = fabsf(D2[18]) < 1e-5f ? .16f : Q2[18];
     b = .5f * E[7];
     d[8] = a * (1.0f - x[8]) - b * x[8];
     d[3] = (sig(8) - x[3]) * .045f;
     d[4] = (sig(9) - x[4]) * .02f * sig(10);
     d[5] = (sig(11) - x[5]) * .0608644f;
-    const float kinf = sig(12) * sig(13) * cai / (2.5f + cai);
+    const float kinf = Q3[1];
     d[6] = (kinf - x[6]) * .6f;
-    d[7] = (.7f / (.6f + cai) - x[7]) * .035f;
+    d[7] = (Q2[19] - x[7]) * .035f;
     d[9] = (sig(14) - x[9]) * .14f;
     const float ainf = sig(15);
     d[10] = (ainf - x[10]) * .05f;
     d[11] = (ainf - x[11]) * .0036f * sig(16);
-    d[12] = (sig(17) - x[12]) * .00033f / sig(18);
+    d[12] = Q3[2];
     d[13] = -.05049639866f * ca - .01729930764f * (cai - .02f);
     d[14] = (sig(19) - x[14]) * .0001386796618f * sig(20);
 }
-// lp_integrate on the state xs (16 floats in memory): 20 classical RK4 steps
-// of 0.05 ms with the state, the four scales and the stage sums in registers.
-// The four stages run as one loop over a single copy of lp_rates. The stage
-// sum k1 + 2 k2 + 2 k3 + k4 accumulates left to right, the order of the
+// One classical RK4 step of 0.05 ms from x into xn: lp_rates at x, x + dt/2 k1,
+// x + dt/2 k2 and x + dt k3, as one loop over a single copy of lp_rates. The
+// stage sum k1 + 2 k2 + 2 k3 + k4 accumulates left to right, the order of the
 // reference's expression, so every rounding is the same.
-static __device__ __noinline__ void lp_integrate(float *xs, float i_na, const float *scs, const float *tab) {
+template <bool SAFE>
+__device__ __forceinline__ void lp_rk4(const float (&x)[16], float (&xn)[16], float i_na, const float (&sc)[4],
+                                       const float *tab, bool &ok) {
     const float dt = .05f;
-    float x[16], y[16], k[16], acc[16], sc[4];
+    float y[16], k[16], acc[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) y[j] = x[j];
+#pragma unroll 1
+    for (int st = 0; st < 4; ++st) {
+        lp_rates<SAFE>(y, i_na, sc, k, tab, ok);
+        if (st == 0) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[j] = k[j];
+        } else if (st < 3) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[j] = acc[j] + 2 * k[j];
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[j] = acc[j] + k[j];
+        }
+        const float c = st < 2 ? .5f * dt : dt;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) y[j] = x[j] + c * k[j];
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) xn[j] = x[j] + dt * acc[j] / 6.0f;
+}
+
+// The RK4 step with every exponential decided (crexp_n), on the state xs in
+// memory: the rare recomputation of a step whose fast paths left one undecided.
+static __device__ __noinline__ void lp_rk4_safe(float *xs, float i_na, const float *scs, const float *tab) {
+    float x[16], xn[16], sc[4];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) x[j] = xs[j];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) sc[j] = scs[j];
+    bool ok = true;
+    lp_rk4<true>(x, xn, i_na, sc, tab, ok);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) xs[j] = xn[j];
+}
+
+// lp_integrate on the state xs (16 floats in memory): 20 RK4 steps with the
+// state and the four scales in registers.
+static __device__ __noinline__ void lp_integrate(float *xs, float i_na, const float *scs, const float *tab) {
+    float x[16], sc[4];
 #pragma unroll
     for (int j = 0; j < 16; ++j) x[j] = xs[j];
 #pragma unroll
     for (int j = 0; j < 4; ++j) sc[j] = scs[j];
 #pragma unroll 1
     for (int step = 0; step < 20; ++step) {
+        float xn[16];
+        bool ok = true;
+        lp_rk4<false>(x, xn, i_na, sc, tab, ok);
+        if (!ok) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) y[j] = x[j];
-#pragma unroll 1
-        for (int st = 0; st < 4; ++st) {
-            lp_rates(y, i_na, sc, k, tab);
-            if (st == 0) {
+            for (int j = 0; j < 16; ++j) xs[j] = x[j];
+            lp_rk4_safe(xs, i_na, scs, tab);
 #pragma unroll
-                for (int j = 0; j < 16; ++j) acc[j] = k[j];
-            } else if (st < 3) {
-#pragma unroll
-                for (int j = 0; j < 16; ++j) acc[j] = acc[j] + 2 * k[j];
-            } else {
-#pragma unroll
-                for (int j = 0; j < 16; ++j) acc[j] = acc[j] + k[j];
-            }
-            const float c = st < 2 ? .5f * dt : dt;
-#pragma unroll
-            for (int j = 0; j < 16; ++j) y[j] = x[j] + c * k[j];
+            for (int j = 0; j < 16; ++j) xn[j] = xs[j];
         }
 #pragma unroll
-        for (int j = 0; j < 16; ++j) x[j] += dt * acc[j] / 6.0f;
+        for (int j = 0; j < 16; ++j) x[j] = xn[j];
     }
 #pragma unroll
     for (int j = 0; j < 16; ++j) xs[j] = x[j];
@@ -275,38 +394,60 @@ __device__ __forceinline__ float pz_gate(float v, float a, float b, const float 
 __device__ __forceinline__ float pz_gate2(float v, float a, float b, float c, float d, const float *tab) {
     return 1.0f / (crexp((v + a) / b, tab) + crexp((v + c) / d, tab));
 }
-// pz_substep with its exponentials computed as two batches (crexp_n): the
-// voltage's gates and time constants, then the relaxations that use them.
+// pz_substep with its exponentials computed as two batches (crexp_n: the
+// voltage's gates and time constants, then the relaxations that use them) and
+// its quotients as three (fdiv_n: the exponents' arguments and the calcium
+// quotients; the gates and time constants; the relaxation rates, the voltage's
+// target and the calcium current). Every operation is the reference's, in its
+// order; (v + 65) / -16 is written as the product by -0.0625, which rounds the
+// same exact value.
+template <bool SAFE>
 __device__ __forceinline__ void pz_substep(float (&u)[13], const float (&g)[9], float ext, float clamp_ns,
-                                           float clamp_rev, const float *tab) {
+                                           float clamp_rev, const float *tab, bool &ok) {
     const float dt = .025f;
     float *m = u + 2, *h = u + 9;
     const float v = u[0], ca = fmaxf(u[1], 0.000001f);
     // level 1: pz_gate(v, a, b) = 1 / (1 + exp((v + a) / b)) and the raw exponentials
-    float A[26], E[26];
-    const float ga[20] = {25.5f, 27.1f, 33, 27.2f, 28.3f, 12.3f, 75,          // mi
+    const float ga[18] = {25.5f, 27.1f, 33, 27.2f, 28.3f, 12.3f, 75,          // mi
                           120, 68.1f, 32.9f, 46, 28.3f,                       // mt 0 1 3 4 5
                           48.9f, 32.1f, 60, 56.9f,                            // hi
-                          55, 38.9f,                                          // ht 1 3
-                          0, 0};
-    const float gb[20] = {-5.29f, -7.2f, -8.1f, -8.7f, -12.6f, -11.8f, 5.5f,
+                          55, 38.9f};                                         // ht 1 3
+    const float gb[18] = {-5.29f, -7.2f, -8.1f, -8.7f, -12.6f, -11.8f, 5.5f,
                           -25, -20.5f, -15.2f, -22.7f, -19.2f,
                           5.18f, 5.5f, 6.2f, 4.9f,
-                          -16.9f, -26.5f,
-                          1, 1};
+                          -16.9f, -26.5f};
+    float N1[25], D1[25], Q1[25];
 #pragma unroll
-    for (int i = 0; i < 18; ++i) A[i] = (v + ga[i]) / gb[i];
-    A[18] = (v + 27) / 10;           // mt 2
-    A[19] = (v + 70) / -13;
+    for (int i = 0; i < 18; ++i) { N1[i] = v + ga[i]; D1[i] = gb[i]; }
+    N1[18] = v + 27;       D1[18] = 10;          // mt 2
+    N1[19] = v + 70;       D1[19] = -13;
+    N1[20] = v + 62.9f;    D1[20] = -10;         // ht 0
+    N1[21] = v + 34.9f;    D1[21] = 3.6f;
+    N1[22] = v + 55;       D1[22] = 9;           // ht 2
+    N1[23] = 3000.0f;      D1[23] = ca;          // calcium reversal
+    N1[24] = ca;           D1[24] = ca + 3;      // calcium factor of mi[4]
+    fdiv_n(N1, D1, Q1);
+    float A[26], E[26];
+#pragma unroll
+    for (int i = 0; i < 20; ++i) A[i] = Q1[i];
     A[20] = -14.59f - .086f * v;     // mt 6
     A[21] = -1.87f + .0701f * v;
-    A[22] = (v + 62.9f) / -10;       // ht 0
-    A[23] = (v + 34.9f) / 3.6f;
-    A[24] = (v + 55) / 9;            // ht 2
-    A[25] = (v + 65) / -16;
-    crexp_n(A, E, tab);
-    auto gate = [&](int i) { return 1.0f / (1.0f + E[i]); };
-    const float eca = (8.31451e3f * 283.0f / (2.0f * 96485.3415f)) * nsx::logf_cr(3000.0f / ca);
+    A[22] = Q1[20];
+    A[23] = Q1[21];
+    A[24] = Q1[22];
+    A[25] = (v + 65) * -0.0625f;     // (v + 65) / -16
+    exp_n<SAFE>(A, E, tab, ok);
+    float N2[23], D2[23], Q2[23];
+#pragma unroll
+    for (int i = 0; i < 18; ++i) { N2[i] = 1.0f; D2[i] = 1.0f + E[i]; }
+    N2[18] = 1.0f;         D2[18] = E[18] + E[19];
+    N2[19] = 2.0f;         D2[19] = E[20] + E[21];
+    N2[20] = 1.34f;        D2[20] = 1 + E[22];
+    N2[21] = 1;            D2[21] = 1 + E[23];
+    N2[22] = 1.0f;         D2[22] = E[24] + E[25];
+    fdiv_n(N2, D2, Q2);
+    auto gate = [&](int i) { return Q2[i]; };
+    const float eca = (8.31451e3f * 283.0f / (2.0f * 96485.3415f)) * nsx::logf_cr(Q1[23]);
     const float c[8] = {g[0] * m[0] * m[0] * m[0] * h[0], g[1] * m[1] * m[1] * m[1] * h[1],
                         g[2] * m[2] * m[2] * m[2] * h[2], g[3] * m[3] * m[3] * m[3] * h[3],
                         g[4] * m[4] * m[4] * m[4] * m[4], g[5] * m[5] * m[5] * m[5] * m[5],
@@ -315,30 +456,52 @@ __device__ __forceinline__ void pz_substep(float (&u)[13], const float (&g)[9], 
     float gt = clamp_ns, ws = ext + clamp_ns * clamp_rev;
 #pragma unroll
     for (int i = 0; i < 8; ++i) { gt += c[i]; ws += c[i] * rev[i]; }
-    const float mi[7] = {gate(0), gate(1), gate(2), gate(3), (ca / (ca + 3)) * gate(4), gate(5), gate(6)};
-    const float mt[7] = {2.64f - 2.52f * gate(7), 43.4f - 42.6f * gate(8), 2.8f + 14 * (1.0f / (E[18] + E[19])),
-                         23.2f - 20.8f * gate(9), 180.6f - 150.2f * gate(10), 14.4f - 12.8f * gate(11),
-                         2.0f / (E[20] + E[21])};
+    const float mi[7] = {gate(0), gate(1), gate(2), gate(3), Q1[24] * gate(4), gate(5), gate(6)};
+    const float mt[7] = {2.64f - 2.52f * gate(7), 43.4f - 42.6f * gate(8), 2.8f + 14 * Q2[18],
+                         23.2f - 20.8f * gate(9), 180.6f - 150.2f * gate(10), 14.4f - 12.8f * gate(11), Q2[19]};
     const float hi[4] = {gate(12), gate(13), gate(14), gate(15)};
-    const float ht[4] = {(1.34f / (1 + E[22])) * (1.5f + 1 / (1 + E[23])), 210 - 179.6f * gate(16),
-                         120 + 300 * (1.0f / (E[24] + E[25])), 77.2f - 58.4f * gate(17)};
+    const float ht[4] = {Q2[20] * (1.5f + Q2[21]), 210 - 179.6f * gate(16), 120 + 300 * Q2[22],
+                         77.2f - 58.4f * gate(17)};
     // level 2: the voltage's relaxation and the gates'
+    float N3[15], D3[15], Q3[15];
+    N3[0] = -dt * gt;      D3[0] = 628.3f;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) { N3[1 + i] = -dt; D3[1 + i] = mt[i]; }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { N3[8 + i] = -dt; D3[8 + i] = ht[i]; }
+    N3[12] = dt * ws;                     D3[12] = 628.3f;
+    N3[13] = ws;                          D3[13] = gt;
+    N3[14] = (c[1] + c[2]) * (v - eca);   D3[14] = 1000000.0f;
+    fdiv_n(N3, D3, Q3);
     float B[12], F[12];
-    B[0] = -dt * gt / 628.3f;
 #pragma unroll
-    for (int i = 0; i < 7; ++i) B[1 + i] = -dt / mt[i];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) B[8 + i] = -dt / ht[i];
-    crexp_n(B, F, tab);
-    if (fabsf(gt) < .000001f) u[0] = v + dt * ws / 628.3f;
-    else { const float tg = ws / gt; u[0] = tg + (v - tg) * F[0]; }
-    const float ica = (c[1] + c[2]) * (v - eca) / 1000000.0f;
+    for (int i = 0; i < 12; ++i) B[i] = Q3[i];
+    exp_n<SAFE>(B, F, tab, ok);
+    if (fabsf(gt) < .000001f) u[0] = v + Q3[12];
+    else { const float tg = Q3[13]; u[0] = tg + (v - tg) * F[0]; }
+    const float ica = Q3[14];
     const float cat = .05f - 14961.0f * ica;
     u[1] = fmaxf(.000001f, cat + (ca - cat) * c_K.prinz_ca);
 #pragma unroll
     for (int i = 0; i < 7; ++i) m[i] = mi[i] + (m[i] - mi[i]) * F[1 + i];
 #pragma unroll
     for (int i = 0; i < 4; ++i) h[i] = hi[i] + (h[i] - hi[i]) * F[8 + i];
+}
+
+// The substep with every exponential decided (crexp_n), on the state xs in
+// memory: the rare recomputation of a substep whose fast paths left one
+// undecided.
+static __device__ __noinline__ void pz_substep_safe(float *xs, const float *gs, float ext, float clamp_ns,
+                                                    float clamp_rev, const float *tab) {
+    float u[13], g[9];
+#pragma unroll
+    for (int j = 0; j < 13; ++j) u[j] = xs[j];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) g[j] = gs[j];
+    bool ok = true;
+    pz_substep<true>(u, g, ext, clamp_ns, clamp_rev, tab, ok);
+#pragma unroll
+    for (int j = 0; j < 13; ++j) xs[j] = u[j];
 }
 
 // The Prinz cell's 40 substeps of one tick on xs (13 state floats in memory),
@@ -355,7 +518,18 @@ static __device__ __noinline__ bool prinz_tick(float *xs, const float *gs, float
 #pragma unroll 1
     for (int i = 0; i < 40; ++i) {
         const float before = u[0];
-        pz_substep(u, g, ext, clamp_ns, clamp_rev, tab);
+        float uo[13];
+#pragma unroll
+        for (int j = 0; j < 13; ++j) uo[j] = u[j];
+        bool ok = true;
+        pz_substep<false>(u, g, ext, clamp_ns, clamp_rev, tab, ok);
+        if (!ok) {
+#pragma unroll
+            for (int j = 0; j < 13; ++j) xs[j] = uo[j];
+            pz_substep_safe(xs, gs, ext, clamp_ns, clamp_rev, tab);
+#pragma unroll
+            for (int j = 0; j < 13; ++j) u[j] = xs[j];
+        }
         spiked |= before < 0 && u[0] >= 0;
     }
 #pragma unroll
@@ -448,237 +622,365 @@ __device__ __forceinline__ LaneTerm lp_term(int lane) {
     }
 }
 
-// lp_rates on the state y (16 floats) for lanes 0..15: returns d[lane].
-__device__ __forceinline__ float lp_rate_warp(const float *y, float i_na, const float *sc, float *T, int lane,
-                                              const LaneTerm &q, const float *tab) {
-    const float va = y[0], vs = y[15], cai = y[13];
-    {   // every lane: one exponential, formed the same way in every lane
-        const float x = q.use_va ? va : vs;
+// lp_rates on a warp: lane i < 21 forms the i-th exponential of lp_rates and,
+// for the gates, its sigmoid 1 / (1 + e), each exactly as lp_rates forms it;
+// shuffles give every lane all 21 values, and every lane then assembles all
+// 16 derivatives with lp_rates' operations (the same values in every lane,
+// so the assembly runs converged, with no divergence and no shared memory).
+template <bool SAFE>
+__device__ __forceinline__ void lp_rates_warp(const float (&x)[16], float i_na, const float (&sc)[4], float (&d)[16],
+                                              int lane, const LaneTerm &q, const float *tab, bool &ok) {
+    const float va = x[0], vs = x[15], cai = x[13];
+    float t;
+    {
+        const float xs = q.use_va ? va : vs;
         const float m = lane == 12 ? -.6f * cai : lane == 13 ? -16.0f - .6f * cai : q.m;
-        const float r = (q.form == F_A ? x - m : x) / q.k;
+        const float r = (q.form == F_A ? xs - m : xs) / q.k;
         const float arg = q.form == F_B ? q.c - r : q.form == F_C ? r + q.c : r;
-        const float e = crexp(arg, tab);
-        T[lane] = q.sig ? 1.0f / (1.0f + e) : e;
+        const float e = exp1<SAFE>(arg, tab, ok);
+        t = q.sig ? 1.0f / (1.0f + e) : e;
     }
-    __syncwarp();
-    const float *x = y;
-    float d = 0.0f;
-    if (lane == 0) {
-        const float na = x[1] * x[1] * x[1] * x[2] * 7.15f * (va - 50.0f);
-        const float kd = x[8] * x[8] * x[8] * x[8] * 1.43f * (va + 72.0f);
-        const float km = .2613041227f * x[14] * (va + 80.0f);
-        const float aleak = sc[3] * .001004288227f * (va + 50.0f);
-        const float cpl = .004017089073f * (vs - va);
-        d = (-na - kd - km - aleak + cpl) / .1148312178f;
-    } else if (lane == 13 || lane == 15) {
-        const float ev = T[0];
-        const float ghk = fabsf(vs) < .001f ? 11.4866f * (x[13] - 15123.5f) : vs * (x[13] * ev - 15123.5f) / (ev - 1.0f);
-        const float ca = sc[0] * (x[3] * x[4] * .1247796343f + x[5] * .07142141077f) * .00155982f * ghk * .9f;
-        if (lane == 13) {
-            d = -.05049639866f * ca - .01729930764f * (cai - .02f);
-        } else {
-            const float cpl = .004017089073f * (vs - va);
-            const float kca = sc[1] * x[6] * x[7] * 1.663612026f * (vs + 72.0f) * .9f;
-            const float amix = T[1];
-            const float ka = x[9] * x[9] * x[9] * .8008791415f * (vs + 72.0f) * (amix * x[10] + (1.0f - amix) * x[11]) * .9f;
-            const float ih = sc[2] * x[12] * .0126874385f * (vs + 20.0f) * .9f;
-            const float sleak = sc[3] * .0006901584324f * (vs + 50.0f);
-            d = (-ca - kca - ka - ih - sleak - cpl + (i_na - 2.0f) * .01222505828f) / .0543909161f;
-        }
-    } else if (lane == 1 || lane == 2 || lane == 8) {
-        float a, b;
-        if (lane == 1) {
-            a = lp_ratio(-16.64f - .32f * va, T[2] - 1.0f, 1.28f);
-            b = lp_ratio(.28f * va + 7.0f, T[3] - 1.0f, 1.4f);
-        } else if (lane == 2) {
-            a = .128f * T[4];
-            b = 4.0f / (T[5] + 1.0f);
-        } else {
-            a = lp_ratio(-1.6f - .032f * va, T[6] - 1.0f, .16f);
-            b = .5f * T[7];
-        }
-        d = a * (1.0f - x[lane]) - b * x[lane];
-    } else if (lane < 16) {
-        // gating variables: ((A - x) * k) [* or / B]
-        const int ia = lane == 3 ? 8 : lane == 4 ? 9 : lane == 5 ? 11 : lane == 9 ? 14 : lane == 10 ? 15
-                       : lane == 11 ? 15 : lane == 12 ? 17 : 19;
-        const float A = lane == 6 ? T[12] * T[13] * cai / (2.5f + cai) : lane == 7 ? .7f / (.6f + cai) : T[ia];
-        const float k = lane == 3 ? .045f : lane == 4 ? .02f : lane == 5 ? .0608644f : lane == 6 ? .6f
-                        : lane == 7 ? .035f : lane == 9 ? .14f : lane == 10 ? .05f : lane == 11 ? .0036f
-                        : lane == 12 ? .00033f : .0001386796618f;
-        d = (A - x[lane]) * k;
-        if (lane == 4 || lane == 11 || lane == 14) d = d * T[lane == 4 ? 10 : lane == 11 ? 16 : 20];
-        else if (lane == 12) d = d / T[18];
-    }
-    __syncwarp();
-    return d;
+    // T[i] = E[i] for i = 0, 2..7 and sig(i) for i = 1, 8..20 (lp_rates' names)
+    float T[21];
+#pragma unroll
+    for (int i = 0; i < 21; ++i) T[i] = __shfl_sync(0xffffffffu, t, i);
+    const float na = x[1] * x[1] * x[1] * x[2] * 7.15f * (va - 50.0f);
+    const float kd = x[8] * x[8] * x[8] * x[8] * 1.43f * (va + 72.0f);
+    const float km = .2613041227f * x[14] * (va + 80.0f);
+    const float aleak = sc[3] * .001004288227f * (va + 50.0f);
+    const float cpl = .004017089073f * (vs - va);
+    const float ev = T[0];
+    float N2[7], D2[7], Q2[7];
+    N2[0] = vs * (x[13] * ev - 15123.5f);       D2[0] = ev - 1.0f;
+    N2[1] = -16.64f - .32f * va;                D2[1] = T[2] - 1.0f;
+    N2[2] = .28f * va + 7.0f;                   D2[2] = T[3] - 1.0f;
+    N2[3] = 4.0f;                               D2[3] = T[5] + 1.0f;
+    N2[4] = -1.6f - .032f * va;                 D2[4] = T[6] - 1.0f;
+    N2[5] = .7f;                                D2[5] = .6f + cai;
+    N2[6] = -na - kd - km - aleak + cpl;        D2[6] = .1148312178f;
+    fdiv_n(N2, D2, Q2);
+    d[0] = Q2[6];
+    const float ghk = fabsf(vs) < .001f ? 11.4866f * (x[13] - 15123.5f) : Q2[0];
+    const float ca = sc[0] * (x[3] * x[4] * .1247796343f + x[5] * .07142141077f) * .00155982f * ghk * .9f;
+    const float kca = sc[1] * x[6] * x[7] * 1.663612026f * (vs + 72.0f) * .9f;
+    const float amix = T[1];
+    const float ka = x[9] * x[9] * x[9] * .8008791415f * (vs + 72.0f) * (amix * x[10] + (1.0f - amix) * x[11]) * .9f;
+    const float ih = sc[2] * x[12] * .0126874385f * (vs + 20.0f) * .9f;
+    const float sleak = sc[3] * .0006901584324f * (vs + 50.0f);
+    float N3[3], D3[3], Q3[3];
+    N3[0] = -ca - kca - ka - ih - sleak - cpl + (i_na - 2.0f) * .01222505828f;   D3[0] = .0543909161f;
+    N3[1] = T[12] * T[13] * cai;                                                  D3[1] = 2.5f + cai;
+    N3[2] = (T[17] - x[12]) * .00033f;                                            D3[2] = T[18];
+    fdiv_n(N3, D3, Q3);
+    d[15] = Q3[0];
+    float a = fabsf(D2[1]) < 1e-5f ? 1.28f : Q2[1];
+    float b = fabsf(D2[2]) < 1e-5f ? 1.4f : Q2[2];
+    d[1] = a * (1.0f - x[1]) - b * x[1];
+    a = .128f * T[4];
+    b = Q2[3];
+    d[2] = a * (1.0f - x[2]) - b * x[2];
+    a = fabsf(D2[4]) < 1e-5f ? .16f : Q2[4];
+    b = .5f * T[7];
+    d[8] = a * (1.0f - x[8]) - b * x[8];
+    d[3] = (T[8] - x[3]) * .045f;
+    d[4] = (T[9] - x[4]) * .02f * T[10];
+    d[5] = (T[11] - x[5]) * .0608644f;
+    d[6] = (Q3[1] - x[6]) * .6f;
+    d[7] = (Q2[5] - x[7]) * .035f;
+    d[9] = (T[14] - x[9]) * .14f;
+    d[10] = (T[15] - x[10]) * .05f;
+    d[11] = (T[15] - x[11]) * .0036f * T[16];
+    d[12] = Q3[2];
+    d[13] = -.05049639866f * ca - .01729930764f * (cai - .02f);
+    d[14] = (T[19] - x[14]) * .0001386796618f * T[20];
 }
 
-// lp_integrate on x (16 floats, any memory the warp can read and write).
-static __device__ __noinline__ void lp_integrate_warp(float *x, float i_na, const float *sc, float *w, int lane,
-                                                      const float *tab) {
+// lp_rk4 on the whole warp (lp_rates_warp); every lane computes xn.
+template <bool SAFE>
+__device__ __forceinline__ void lp_rk4_warp(const float (&x)[16], float (&xn)[16], float i_na, const float (&sc)[4],
+                                            int lane, const LaneTerm &q, const float *tab, bool &ok) {
     const float dt = .05f;
-    float *y = w, *T = w + 16;
-    const LaneTerm q = lp_term(lane);
-    float xj = lane < 16 ? x[lane] : 0.0f;
-    if (lane < 16) y[lane] = xj;
-    __syncwarp();
-    for (int step = 0; step < 20; ++step) {
-        const float k1 = lp_rate_warp(y, i_na, sc, T, lane, q, tab);
-        if (lane < 16) y[lane] = xj + .5f * dt * k1;
-        __syncwarp();
-        const float k2 = lp_rate_warp(y, i_na, sc, T, lane, q, tab);
-        if (lane < 16) y[lane] = xj + .5f * dt * k2;
-        __syncwarp();
-        const float k3 = lp_rate_warp(y, i_na, sc, T, lane, q, tab);
-        if (lane < 16) y[lane] = xj + dt * k3;
-        __syncwarp();
-        const float k4 = lp_rate_warp(y, i_na, sc, T, lane, q, tab);
-        xj += dt * (k1 + 2 * k2 + 2 * k3 + k4) / 6.0f;
-        if (lane < 16) y[lane] = xj;
-        __syncwarp();
+    float y[16], k[16], acc[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) y[j] = x[j];
+#pragma unroll 1
+    for (int st = 0; st < 4; ++st) {
+        lp_rates_warp<SAFE>(y, i_na, sc, k, lane, q, tab, ok);
+        if (st == 0) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[j] = k[j];
+        } else if (st < 3) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[j] = acc[j] + 2 * k[j];
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[j] = acc[j] + k[j];
+        }
+        const float c = st < 2 ? .5f * dt : dt;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) y[j] = x[j] + c * k[j];
     }
-    if (lane < 16) x[lane] = xj;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) xn[j] = x[j] + dt * acc[j] / 6.0f;
+}
+
+// The warp's RK4 step with every exponential decided, on xs in memory (lane 0
+// writes the result); all 32 lanes call it together.
+static __device__ __noinline__ void lp_rk4_warp_safe(float *xs, float i_na, const float *scs, int lane,
+                                                     const float *tab) {
+    const LaneTerm q = lp_term(lane);
+    float x[16], xn[16], sc[4];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) x[j] = xs[j];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) sc[j] = scs[j];
+    bool ok = true;
+    lp_rk4_warp<true>(x, xn, i_na, sc, lane, q, tab, ok);
+    __syncwarp();
+    if (lane == 0) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) xs[j] = xn[j];
+    }
     __syncwarp();
 }
 
-// The lane's exponential term of a Prinz substep (pz_substep), level 1 (all
-// from the voltage v): gates mi[0..6] (lanes 1-7), the time constants
-// mt[0..6] (8-16, the two-exponential ones split over two lanes each), gates
-// hi[0..3] (17-20) and the time constants ht[0..3] (21-26). Lane 0 takes the
-// logarithm of the calcium reversal. post: 0 none, 1 K1 - K2 g, 2 the
-// calcium factor of mi[4].
+// lp_integrate on the whole warp: every lane holds the state and the scales
+// in registers and runs lp_integrate's 20 RK4 steps (a step with an undecided
+// exponential in any lane is recomputed by lp_rk4_warp_safe); lane 0 writes
+// the state back. All 32 lanes call it together. The scratch argument `w` is
+// unused (kept for the callers' interface).
+static __device__ __noinline__ void lp_integrate_warp(float *xs, float i_na, const float *scs, float *w, int lane,
+                                                      const float *tab) {
+    (void)w;
+    const LaneTerm q = lp_term(lane);
+    float x[16], sc[4];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) x[j] = xs[j];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) sc[j] = scs[j];
+#pragma unroll 1
+    for (int step = 0; step < 20; ++step) {
+        float xn[16];
+        bool ok = true;
+        lp_rk4_warp<false>(x, xn, i_na, sc, lane, q, tab, ok);
+        if (__any_sync(0xffffffffu, !ok)) {
+            __syncwarp();
+            if (lane == 0) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) xs[j] = x[j];
+            }
+            __syncwarp();
+            lp_rk4_warp_safe(xs, i_na, scs, lane, tab);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) xn[j] = xs[j];
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) x[j] = xn[j];
+    }
+    __syncwarp();
+    if (lane == 0) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) xs[j] = x[j];
+    }
+    __syncwarp();
+}
+
+// The lane's term of a Prinz substep, level 1 (pz_substep's A, E and the
+// quotients on them): lanes 0-17 the gates pz_gate (1 / (1 + e) of
+// (v + a) / b), 18, 19 and 24, 25 the raw exponentials of the two-exponential
+// time constants, 20 and 21 those of mt[6] (c - k v, c + k v), 22 and 23 the
+// factors 1.34 / (1 + e) and 1 / (1 + e) of ht[0]; lane 26 takes the
+// logarithm of 3000 / ca and lane 27 the quotient ca / (ca + 3).
 struct PzTerm {
-    LaneTerm t;
-    int post;
-    float k1, k2;
+    int form;       // F_G: (v + a) / b; F_P: c - k v; F_Q: c + k v
+    float a, b;     // F_G: a, b; F_P, F_Q: c, k
+    float num;      // the numerator over 1 + e; 0: the raw exponential
 };
 __device__ __forceinline__ PzTerm pz_term(int lane) {
     switch (lane) {
-    case 1: return {{F_G, 25.5f, -5.29f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
-    case 2: return {{F_G, 27.1f, -7.2f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
-    case 3: return {{F_G, 33.0f, -8.1f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
-    case 4: return {{F_G, 27.2f, -8.7f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
-    case 5: return {{F_G, 28.3f, -12.6f, 0.0f, 1, 0}, 2, 0.0f, 0.0f};
-    case 6: return {{F_G, 12.3f, -11.8f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
-    case 7: return {{F_G, 75.0f, 5.5f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
-    case 8: return {{F_G, 120.0f, -25.0f, 0.0f, 1, 0}, 1, 2.64f, 2.52f};
-    case 9: return {{F_G, 68.1f, -20.5f, 0.0f, 1, 0}, 1, 43.4f, 42.6f};
-    case 10: return {{F_G, 27.0f, 10.0f, 0.0f, 0, 0}, 0, 0.0f, 0.0f};
-    case 11: return {{F_G, 70.0f, -13.0f, 0.0f, 0, 0}, 0, 0.0f, 0.0f};
-    case 12: return {{F_G, 32.9f, -15.2f, 0.0f, 1, 0}, 1, 23.2f, 20.8f};
-    case 13: return {{F_G, 46.0f, -22.7f, 0.0f, 1, 0}, 1, 180.6f, 150.2f};
-    case 14: return {{F_G, 28.3f, -19.2f, 0.0f, 1, 0}, 1, 14.4f, 12.8f};
-    case 15: return {{F_P, 0.0f, .086f, -14.59f, 0, 0}, 0, 0.0f, 0.0f};
-    case 16: return {{F_Q, 0.0f, .0701f, -1.87f, 0, 0}, 0, 0.0f, 0.0f};
-    case 17: return {{F_G, 48.9f, 5.18f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
-    case 18: return {{F_G, 32.1f, 5.5f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
-    case 19: return {{F_G, 60.0f, 6.2f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
-    case 20: return {{F_G, 56.9f, 4.9f, 0.0f, 1, 0}, 0, 0.0f, 0.0f};
-    case 21: return {{F_G, 62.9f, -10.0f, 0.0f, 0, 0}, 0, 0.0f, 0.0f};
-    case 22: return {{F_G, 34.9f, 3.6f, 0.0f, 0, 0}, 0, 0.0f, 0.0f};
-    case 23: return {{F_G, 55.0f, -16.9f, 0.0f, 1, 0}, 1, 210.0f, 179.6f};
-    case 24: return {{F_G, 55.0f, 9.0f, 0.0f, 0, 0}, 0, 0.0f, 0.0f};
-    case 25: return {{F_G, 65.0f, -16.0f, 0.0f, 0, 0}, 0, 0.0f, 0.0f};
-    case 26: return {{F_G, 38.9f, -26.5f, 0.0f, 1, 0}, 1, 77.2f, 58.4f};
-    default: return {{F_P, 0.0f, 0.0f, -1.0f, 0, 0}, 0, 0.0f, 0.0f};  // lane 0 and idle lanes: exp(-1), unused
+    case 0: return {F_G, 25.5f, -5.29f, 1.0f};
+    case 1: return {F_G, 27.1f, -7.2f, 1.0f};
+    case 2: return {F_G, 33.0f, -8.1f, 1.0f};
+    case 3: return {F_G, 27.2f, -8.7f, 1.0f};
+    case 4: return {F_G, 28.3f, -12.6f, 1.0f};
+    case 5: return {F_G, 12.3f, -11.8f, 1.0f};
+    case 6: return {F_G, 75.0f, 5.5f, 1.0f};
+    case 7: return {F_G, 120.0f, -25.0f, 1.0f};
+    case 8: return {F_G, 68.1f, -20.5f, 1.0f};
+    case 9: return {F_G, 32.9f, -15.2f, 1.0f};
+    case 10: return {F_G, 46.0f, -22.7f, 1.0f};
+    case 11: return {F_G, 28.3f, -19.2f, 1.0f};
+    case 12: return {F_G, 48.9f, 5.18f, 1.0f};
+    case 13: return {F_G, 32.1f, 5.5f, 1.0f};
+    case 14: return {F_G, 60.0f, 6.2f, 1.0f};
+    case 15: return {F_G, 56.9f, 4.9f, 1.0f};
+    case 16: return {F_G, 55.0f, -16.9f, 1.0f};
+    case 17: return {F_G, 38.9f, -26.5f, 1.0f};
+    case 18: return {F_G, 27.0f, 10.0f, 0.0f};
+    case 19: return {F_G, 70.0f, -13.0f, 0.0f};
+    case 20: return {F_P, -14.59f, .086f, 0.0f};
+    case 21: return {F_Q, -1.87f, .0701f, 0.0f};
+    case 22: return {F_G, 62.9f, -10.0f, 1.34f};
+    case 23: return {F_G, 34.9f, 3.6f, 1.0f};
+    case 24: return {F_G, 55.0f, 9.0f, 0.0f};
+    case 25: return {F_G, 65.0f, -16.0f, 0.0f};
+    default: return {F_P, -1.0f, 0.0f, 0.0f};    // lanes 26-31: exp(-1), unused
     }
 }
 
-// One pz_substep on u (13 floats: v, ca, m[7], h[4]) in shared memory; T
-// holds the lanes' level-1 terms.
-__device__ __forceinline__ void pz_substep_warp(float *u, const float *g, float ext, float clamp_ns, float clamp_rev,
-                                                float *T, int lane, const PzTerm &q, const float *tab) {
+// One pz_substep on the whole warp: every lane holds u (v, ca, m[7], h[4]) and
+// g in registers. Level 1: lane i forms pz_substep's i-th exponential and the
+// quotient on it (PzTerm), lanes 26 and 27 the calcium terms; shuffles give
+// every lane all 28. Every lane then assembles the gates, time constants and
+// currents with pz_substep's operations; level 2: lane i < 12 forms the i-th
+// relaxation exponential, lanes 12-14 the voltage target and the calcium
+// current; shuffles again, and every lane updates u the same way.
+template <bool SAFE>
+__device__ __forceinline__ void pz_substep_warp(float (&u)[13], const float (&g)[9], float ext, float clamp_ns,
+                                                float clamp_rev, int lane, const PzTerm &q, const float *tab,
+                                                bool &ok) {
     const float dt = .025f;
-    const float *m = u + 2, *h = u + 9;
+    float *m = u + 2, *h = u + 9;
     const float v = u[0], ca = fmaxf(u[1], 0.000001f);
-    {   // level 1: one exponential per lane, formed the same way in every lane
-        const float p = q.t.form == F_G ? v + q.t.m : q.t.k * v;
-        const float arg = q.t.form == F_P ? q.t.c - p : q.t.form == F_Q ? q.t.c + p : p / q.t.k;
-        const float e = crexp(arg, tab);
-        float t = q.t.sig ? 1.0f / (1.0f + e) : e;
-        if (q.post == 1) t = q.k1 - q.k2 * t;
-        else if (q.post == 2) t = (ca / (ca + 3)) * t;
-        if (lane == 0) t = nsx::logf_cr(3000.0f / ca);
-        T[lane] = t;
+    float t;
+    {
+        const float n = lane == 26 ? 3000.0f : lane == 27 ? ca : v + q.a;
+        const float dd = lane == 26 ? ca : lane == 27 ? ca + 3 : q.form == F_G ? q.b : 1.0f;
+        const float r = n / dd;
+        const float arg = lane >= 26 ? -1.0f : q.form == F_G ? r : q.form == F_P ? q.a - q.b * v : q.a + q.b * v;
+        const float e = exp1<SAFE>(arg, tab, ok);
+        const float s = q.num / (1 + e);
+        t = lane == 27 ? r : q.num != 0.0f ? s : e;
+        if (lane == 26) t = nsx::logf_cr(r);
     }
+    float T[28];
+#pragma unroll
+    for (int i = 0; i < 28; ++i) T[i] = __shfl_sync(0xffffffffu, t, i);
+    float N1[3], D1[3], Q1[3];
+    N1[0] = 1.0f;  D1[0] = T[18] + T[19];
+    N1[1] = 2.0f;  D1[1] = T[20] + T[21];
+    N1[2] = 1.0f;  D1[2] = T[24] + T[25];
+    fdiv_n(N1, D1, Q1);
+    const float eca = (8.31451e3f * 283.0f / (2.0f * 96485.3415f)) * T[26];
+    const float c[8] = {g[0] * m[0] * m[0] * m[0] * h[0], g[1] * m[1] * m[1] * m[1] * h[1],
+                        g[2] * m[2] * m[2] * m[2] * h[2], g[3] * m[3] * m[3] * m[3] * h[3],
+                        g[4] * m[4] * m[4] * m[4] * m[4], g[5] * m[5] * m[5] * m[5] * m[5],
+                        g[6] * m[6], g[7]};
+    const float rev[8] = {50, eca, eca, -80, -80, -80, -20, -50};
+    float gt = clamp_ns, ws = ext + clamp_ns * clamp_rev;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) { gt += c[i]; ws += c[i] * rev[i]; }
+    const float mi[7] = {T[0], T[1], T[2], T[3], T[27] * T[4], T[5], T[6]};
+    const float mt[7] = {2.64f - 2.52f * T[7], 43.4f - 42.6f * T[8], 2.8f + 14 * Q1[0],
+                         23.2f - 20.8f * T[9], 180.6f - 150.2f * T[10], 14.4f - 12.8f * T[11], Q1[1]};
+    const float hi[4] = {T[12], T[13], T[14], T[15]};
+    const float ht[4] = {T[22] * (1.5f + T[23]), 210 - 179.6f * T[16], 120 + 300 * Q1[2], 77.2f - 58.4f * T[17]};
+    // level 2: lane 0 the voltage's relaxation, 1-7 and 8-11 the gates',
+    // 12-14 the voltage target's two forms and the calcium current
+    float f;
+    {
+        float n = -dt, dd = 628.3f;
+        if (lane == 0) n = -dt * gt;
+        else if (lane == 12) n = dt * ws;
+        else if (lane == 13) { n = ws; dd = gt; }
+        else if (lane == 14) { n = (c[1] + c[2]) * (v - eca); dd = 1000000.0f; }
+#pragma unroll
+        for (int i = 0; i < 7; ++i) dd = lane == 1 + i ? mt[i] : dd;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) dd = lane == 8 + i ? ht[i] : dd;
+        const float r = n / dd;
+        const float e = exp1<SAFE>(lane < 12 ? r : -1.0f, tab, ok);
+        f = lane < 12 ? e : r;
+    }
+    float F[15];
+#pragma unroll
+    for (int i = 0; i < 15; ++i) F[i] = __shfl_sync(0xffffffffu, f, i);
+    if (fabsf(gt) < .000001f) u[0] = v + F[12];
+    else { const float tg = F[13]; u[0] = tg + (v - tg) * F[0]; }
+    const float ica = F[14];
+    const float cat = .05f - 14961.0f * ica;
+    u[1] = fmaxf(.000001f, cat + (ca - cat) * c_K.prinz_ca);
+#pragma unroll
+    for (int i = 0; i < 7; ++i) m[i] = mi[i] + (m[i] - mi[i]) * F[1 + i];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) h[i] = hi[i] + (h[i] - hi[i]) * F[8 + i];
+}
+
+// The warp's substep with every exponential decided, on xs in memory (lane 0
+// writes the result); all 32 lanes call it together.
+static __device__ __noinline__ void pz_substep_warp_safe(float *xs, const float *xg, float ext, float clamp_ns,
+                                                         float clamp_rev, int lane, const float *tab) {
+    const PzTerm q = pz_term(lane);
+    float u[13], g[9];
+#pragma unroll
+    for (int j = 0; j < 13; ++j) u[j] = xs[j];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) g[j] = xg[j];
+    bool ok = true;
+    pz_substep_warp<true>(u, g, ext, clamp_ns, clamp_rev, lane, q, tab, ok);
     __syncwarp();
-    // level 2: the voltage and calcium (lane 0), m[i] (lanes 2-8) and h[i]
-    // (lanes 9-12), one exponential each
-    float arg = -1.0f, gt = 0.0f, ws = 0.0f, eca = 0.0f, c1 = 0.0f, c2 = 0.0f, base = 0.0f, cur = 0.0f;
     if (lane == 0) {
-        eca = (8.31451e3f * 283.0f / (2.0f * 96485.3415f)) * T[0];
-        const float c[8] = {g[0] * m[0] * m[0] * m[0] * h[0], g[1] * m[1] * m[1] * m[1] * h[1],
-                            g[2] * m[2] * m[2] * m[2] * h[2], g[3] * m[3] * m[3] * m[3] * h[3],
-                            g[4] * m[4] * m[4] * m[4] * m[4], g[5] * m[5] * m[5] * m[5] * m[5],
-                            g[6] * m[6], g[7]};
-        const float rev[8] = {50, eca, eca, -80, -80, -80, -20, -50};
-        gt = clamp_ns;
-        ws = ext + clamp_ns * clamp_rev;
-        for (int i = 0; i < 8; ++i) { gt += c[i]; ws += c[i] * rev[i]; }
-        c1 = c[1];
-        c2 = c[2];
-        arg = -dt * gt / 628.3f;
-    } else if (lane >= 2 && lane < 13) {
-        const bool mg = lane < 9;
-        const int i = mg ? lane - 2 : lane - 9;
-        base = mg ? T[1 + i] : T[17 + i];
-        cur = mg ? m[i] : h[i];
-        float tau;
-        if (mg) {
-            if (i == 2) tau = 2.8f + 14 * (1.0f / (T[10] + T[11]));
-            else if (i == 6) tau = 2.0f / (T[15] + T[16]);
-            else tau = T[i < 2 ? 8 + i : 9 + i];
-        } else {
-            if (i == 0) tau = (1.34f / (1 + T[21])) * (1.5f + 1 / (1 + T[22]));
-            else if (i == 2) tau = 120 + 300 * (1.0f / (T[24] + T[25]));
-            else tau = T[i == 1 ? 23 : 26];
-        }
-        arg = -dt / tau;
+#pragma unroll
+        for (int j = 0; j < 13; ++j) xs[j] = u[j];
     }
-    const float e = crexp(arg, tab);
-    float nv = 0.0f, nca = 0.0f;
-    if (lane == 0) {
-        if (fabsf(gt) < .000001f) nv = v + dt * ws / 628.3f;
-        else { const float tg = ws / gt; nv = tg + (v - tg) * e; }
-        const float ica = (c1 + c2) * (v - eca) / 1000000.0f;
-        const float cat = .05f - 14961.0f * ica;
-        nca = fmaxf(.000001f, cat + (ca - cat) * c_K.prinz_ca);
-    } else if (lane >= 2 && lane < 13) {
-        nv = base + (cur - base) * e;
-    }
-    __syncwarp();
-    if (lane == 0) { u[0] = nv; u[1] = nca; }
-    else if (lane >= 2 && lane < 13) u[lane] = nv;
     __syncwarp();
 }
 
-// The Prinz cell's 40 substeps of one tick on x (13 state floats); returns
-// whether the voltage crossed 0 mV upwards in any substep (all lanes).
+// The Prinz cell's 40 substeps of one tick on x (13 state floats) on the whole
+// warp (a substep with an undecided exponential in any lane is recomputed by
+// pz_substep_warp_safe); lane 0 writes the state back. Returns whether the
+// voltage crossed 0 mV upwards in any substep (all lanes). The scratch
+// argument `w` is unused (kept for the callers' interface).
 static __device__ __noinline__ bool prinz_tick_warp(float *x, const float *xg, float ext, float clamp_ns,
                                                     float clamp_rev, float *w, int lane, const float *tab) {
-    float *u = w, *T = w + 16;
+    (void)w;
     const PzTerm q = pz_term(lane);
-    if (lane < 13) u[lane] = x[lane];
-    __syncwarp();
+    float u[13], g[9];
+#pragma unroll
+    for (int j = 0; j < 13; ++j) u[j] = x[j];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) g[j] = xg[j];
     bool spiked = false;
+#pragma unroll 1
     for (int i = 0; i < 40; ++i) {
         const float before = u[0];
-        pz_substep_warp(u, xg, ext, clamp_ns, clamp_rev, T, lane, q, tab);
+        float uo[13];
+#pragma unroll
+        for (int j = 0; j < 13; ++j) uo[j] = u[j];
+        bool ok = true;
+        pz_substep_warp<false>(u, g, ext, clamp_ns, clamp_rev, lane, q, tab, ok);
+        if (__any_sync(0xffffffffu, !ok)) {
+            __syncwarp();
+            if (lane == 0) {
+#pragma unroll
+                for (int j = 0; j < 13; ++j) x[j] = uo[j];
+            }
+            __syncwarp();
+            pz_substep_warp_safe(x, xg, ext, clamp_ns, clamp_rev, lane, tab);
+#pragma unroll
+            for (int j = 0; j < 13; ++j) u[j] = x[j];
+        }
         spiked |= before < 0 && u[0] >= 0;
     }
-    if (lane < 13) x[lane] = u[lane];
+    __syncwarp();
+    if (lane == 0) {
+#pragma unroll
+        for (int j = 0; j < 13; ++j) x[j] = u[j];
+    }
     __syncwarp();
     return spiked;
 }
 
-// A warp with more LP and Prinz cells than this integrates each on its own
-// lane at once (lp_integrate, pz_substep); with fewer, one after another on
-// the whole warp. Measured on B200, the lanes' own integration (its
-// exponentials batched, crexp_n) is faster for every count in the Gym
-// engine, so the warp form is off there by default.
+// A heavy unit steps its pooled LP and Prinz cells on whole warps, one after
+// another per warp (lp_integrate_warp, prinz_tick_warp), when the pool holds at
+// most this many cells per warp on average; with more, each cell runs on its
+// own lane at once (lp_integrate, prinz_tick). Measured on B200, one cell-tick
+// costs about 142 k (LP) and 97 k (Prinz) cycles on a warp and about 435 k on
+// a lane, and a warp whose lanes hold both kinds runs the two one after the
+// other; on whole warps the pool also spreads evenly. The Gym batches measured
+// were fastest on whole warps up to about eight cells per warp.
 #ifndef NSB_WARP_CELLS_MAX
-#define NSB_WARP_CELLS_MAX 0
+#define NSB_WARP_CELLS_MAX 8
 #endif
 constexpr int kWarpCellsMax = NSB_WARP_CELLS_MAX;
 

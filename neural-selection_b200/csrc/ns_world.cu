@@ -37,6 +37,7 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -96,6 +97,7 @@ struct WorldArgs {
     float *tr_en, *tr_in, *tr_pk;
     int trace, sil_senses, sil_contact;
     int P, ncap, ecap;
+    int warp_cells;    // LP and Prinz cells per warp, on average, up to which heavy_cells_cta uses whole warps
 };
 
 // Compiled-brain cache, one entry per animal slot. Region layout at arena +
@@ -507,7 +509,7 @@ __device__ __forceinline__ void phase_neuron_tail(const UnitMem &U, int n, int c
 }
 
 // Phase 3 for neuron n (state in s). In HEAVY builds an LP or Prinz cell
-// stops after heavy_pre with `job` pending: heavy_cells_warp runs its model
+// stops after heavy_pre with `job` pending: heavy_cells_cta runs its model
 // on the whole warp and phase_neuron_tail finishes it.
 template <bool HEAVY>
 __device__ __forceinline__ void phase_neuron(const WorldArgs &d, const UnitMem &U, int n, int t, int64_t tick,
@@ -574,39 +576,68 @@ __device__ __forceinline__ void phase_neuron(const WorldArgs &d, const UnitMem &
     phase_neuron_tail(U, n, cur9, s, mod, motor_cnt, tr);
 }
 
-// World animals keep their neurons in list order, so their LP and Prinz cells
-// are spread over the warps, a few each; measured on B200 the warp form is
-// faster there than each cell on its own lane.
+// A world step's time is set by its slowest warp: a warp that owns five LP
+// cells and steps them one after another takes five times as long as one that
+// owns one, while the rest of its CTA waits at the next barrier. So the CTA
+// pools its pending LP and Prinz cells (heavy_cells_cta): the warps take the
+// pool round-robin and step each cell on all 32 lanes (lp_integrate_warp,
+// prinz_tick_warp), or, with more than kWorldWarpCellsMax cells per warp on
+// average (where one cell per lane at once costs less), every cell runs on
+// its owner lane (heavy_model_lane).
 #ifndef NSB_WORLD_WARP_CELLS_MAX
-#define NSB_WORLD_WARP_CELLS_MAX 32
+#define NSB_WORLD_WARP_CELLS_MAX 3
 #endif
 constexpr int kWorldWarpCellsMax = NSB_WORLD_WARP_CELLS_MAX;
 
-// The warp's pending LP and Prinz cells, one after another, each on all 32
-// lanes (ns_physio.cuh: lp_integrate_warp, prinz_tick_warp); the owner lane
-// then completes heavy_tick's arithmetic. All lanes call it together; w is
-// the warp's kHeavyWarpScratch + 16 floats of shared memory.
-__device__ __forceinline__ void heavy_cells_warp(const WorldArgs &d, const HeavyJob &job, NeuronRegs &s, float *w,
-                                                 int lane, const float *tab) {
-    const uint32_t pend = __ballot_sync(0xffffffffu, job.pending != 0);
-    if (__popc(pend) > kWorldWarpCellsMax) {   // many cells: each on its own lane at once
+// The CTA's pool of pending LP and Prinz cells (one entry per thread at most).
+// The counter alternates between two words from call to call, so that each
+// call needs only its two barriers: a call reads n[p] between them and clears
+// n[p ^ 1], which the previous call read and the next call fills.
+template <int NT> struct HeavyPool {
+    int n[2];
+    int slot[NT];
+    float ext[NT];
+    float res[NT];       // LP: the axon voltage before the tick; Prinz: 1 when it spiked
+    uint8_t type[NT];
+};
+
+// The cell model of pending cells between heavy_pre and heavy_post. All
+// threads of the CTA call it together, `call` counting the calls (the same in
+// every thread); w is the warp's kHeavyWarpScratch + 16 floats of shared
+// memory. The owner thread then completes heavy_tick's arithmetic.
+template <int NT>
+__device__ __forceinline__ void heavy_cells_cta(const WorldArgs &d, const HeavyJob &job, NeuronRegs &s,
+                                                HeavyPool<NT> &pool, float *w, int tid, int call,
+                                                const float *tab) {
+    const int lane = tid & 31, warp = tid >> 5, nwarps = NT / 32, p = call & 1;
+    int k = 0;
+    if (job.pending) {
+        k = atomicAdd(&pool.n[p], 1);
+        pool.slot[k] = job.slot;
+        pool.ext[k] = job.ext;
+        pool.type[k] = (uint8_t)job.type;
+    }
+    __syncthreads();
+    const int n = pool.n[p];
+    if (tid == 0) pool.n[p ^ 1] = 0;
+    if (n > d.warp_cells * nwarps) {   // many cells: each on its owner lane at once
         if (job.pending) {
             const ref::NeuronGene &G = d.ngene[job.slot];
             float xg[16] = {};
             if (job.type == 2) { xg[0] = G.lp.calcium; xg[1] = G.lp.calcium_k; xg[2] = G.lp.h; xg[3] = G.lp.leak; }
-            else { for (int k = 0; k < 8; ++k) xg[k] = G.prinz.g[k]; xg[8] = G.prinz_leak; }
+            else { for (int q = 0; q < 8; ++q) xg[q] = G.prinz.g[q]; xg[8] = G.prinz_leak; }
             float *x = d.nstate[job.slot].cell;
             bool spiked = false;
             const float ab = heavy_model_lane(job.type, x, xg, job.ext, spiked, tab);
             heavy_post(job.type, s, x, ab, spiked);
         }
+        __syncthreads();
         return;
     }
-    for (uint32_t pm = pend; pm; pm &= pm - 1u) {
-        const int L = __ffs(pm) - 1;
-        const int slot = __shfl_sync(0xffffffffu, job.slot, L);
-        const uint32_t ty = __shfl_sync(0xffffffffu, job.type, L);
-        const float ex = __shfl_sync(0xffffffffu, job.ext, L);
+    for (int e = warp; e < n; e += nwarps) {
+        const int slot = pool.slot[e];
+        const uint32_t ty = pool.type[e];
+        const float ex = pool.ext[e];
         const ref::NeuronGene &G = d.ngene[slot];
         float *xg = w + kHeavyWarpScratch;
         if (lane < 16) {
@@ -621,13 +652,17 @@ __device__ __forceinline__ void heavy_cells_warp(const WorldArgs &d, const Heavy
         if (ty == 2) {
             const float ab = x[0];
             lp_integrate_warp(x, ex / 1000.0f, xg, w, lane, tab);
-            if (lane == L) heavy_post(2, s, x, ab, false);
+            if (lane == 0) pool.res[e] = ab;
         } else {
             const bool sp = prinz_tick_warp(x, xg, ex, xg[8] + 0.0f, -68.0f, w, lane, tab);
-            if (lane == L) heavy_post(3, s, x, 0.0f, sp);
+            if (lane == 0) pool.res[e] = sp ? 1.0f : 0.0f;
         }
         __syncwarp();
     }
+    __syncthreads();
+    if (job.pending)
+        heavy_post(job.type, s, d.nstate[job.slot].cell, job.type == 2 ? pool.res[k] : 0.0f,
+                   job.type == 3 && pool.res[k] != 0.0f);
 }
 
 __device__ __forceinline__ void phase_plastic_events(const WorldArgs &d, const UnitMem &U, int ne, int tid, int bs) {
@@ -724,6 +759,13 @@ constexpr int kClaim = 4;
 // MINB: CTAs per SM the register budget is sized for (the light kernel is
 // built for 3, at 79 registers, and for 2, at about 100, which steps each
 // unit faster when there are few units per CTA slot).
+// CTAs per SM of the heavy instantiations (their LP and Prinz cell models
+// need the registers).
+#ifndef NSB_WORLD_HEAVY_MINB
+#define NSB_WORLD_HEAVY_MINB 2
+#endif
+constexpr int kHeavyMinb = NSB_WORLD_HEAVY_MINB;
+
 template <bool HEAVY, int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) world_tick_small(WorldArgs d, Cache c, int64_t first_tick,
                                                               const int *alive, const int *nalive, int *queue,
@@ -757,13 +799,15 @@ __global__ void __launch_bounds__(kBlock, MINB) world_tick_small(WorldArgs d, Ca
     __shared__ int s_cnt[2];
     __shared__ unsigned long long s_events;
     __shared__ float s_hscr[HEAVY ? (kBlock / 32) * (kHeavyWarpScratch + 16) : 1];   // warp scratch of LP/Prinz cells
+    __shared__ HeavyPool<HEAVY ? kBlock : 32> s_pool;
 
     const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    int hcall = 0;
     {
         const float *src = nsx::exp2f_table();
         for (int i = tid; i < 256; i += bs) tab[i] = src[i];
     }
-    if (tid == 0) { q_n = 0; q_i = 0; q_done = 0; }
+    if (tid == 0) { q_n = 0; q_i = 0; q_done = 0; s_pool.n[0] = s_pool.n[1] = 0; }
     __syncthreads();
     const int n_alive = *nalive;
     UnitMem U;
@@ -867,7 +911,7 @@ __global__ void __launch_bounds__(kBlock, MINB) world_tick_small(WorldArgs d, Ca
             HeavyJob job = {};
             if (tid < ntot) phase_neuron<HEAVY>(d, U, tid, t, tick, cur9, s, &ua_motor[nani[tid] * kM], tr, tab, job);
             if (HEAVY) {
-                heavy_cells_warp(d, job, s, s_hscr + warp * (kHeavyWarpScratch + 16), lane, tab);
+                heavy_cells_cta(d, job, s, s_pool, s_hscr + warp * (kHeavyWarpScratch + 16), tid, hcall++, tab);
                 if (job.pending) phase_neuron_tail(U, tid, cur9, s, job.mod, &ua_motor[nani[tid] * kM], tr);
             }
             __syncthreads();
@@ -958,17 +1002,20 @@ __device__ __forceinline__ void slab_store(const BigSlab &B, int n, const Neuron
 // Big animals of one class (HEAVY: with an active LP, Prinz or LFS cell),
 // one per 256-thread CTA; each class has its own claim counter.
 template <bool HEAVY>
-__global__ void __launch_bounds__(kBigBlock, HEAVY ? 2 : 3) world_tick_big(WorldArgs d, Cache c, int64_t first_tick,
+__global__ void __launch_bounds__(kBigBlock, HEAVY ? kHeavyMinb : 3) world_tick_big(WorldArgs d, Cache c, int64_t first_tick,
                                                                           const int *big, const int *big_count,
                                                                           int *queue, BigSlab slab, Counters *stats) {
     float *tab = reinterpret_cast<float *>(w_smem);
     __shared__ int s_i, s_motor[kM], s_cnt[2];
     __shared__ unsigned long long s_events;
     __shared__ float s_hscr[HEAVY ? (kBigBlock / 32) * (kHeavyWarpScratch + 16) : 1];   // warp scratch of LP/Prinz cells
+    __shared__ HeavyPool<HEAVY ? kBigBlock : 32> s_pool;
     const int tid = threadIdx.x, bs = blockDim.x;
+    int hcall = 0;
     {
         const float *src = nsx::exp2f_table();
         for (int i = tid; i < 256; i += bs) tab[i] = src[i];
+        if (tid == 0) s_pool.n[0] = s_pool.n[1] = 0;
     }
     BigSlab B = slab;
     const size_t sn = (size_t)blockIdx.x, MN = (size_t)slab.max_n, ME = (size_t)slab.max_e;
@@ -1035,7 +1082,8 @@ __global__ void __launch_bounds__(kBigBlock, HEAVY ? 2 : 3) world_tick_big(World
                     phase_neuron<HEAVY>(d, U, n, t, tick, cur9, s, s_motor, tr, tab, job);
                 }
                 if (HEAVY) {
-                    heavy_cells_warp(d, job, s, s_hscr + (tid >> 5) * (kHeavyWarpScratch + 16), tid & 31, tab);
+                    heavy_cells_cta(d, job, s, s_pool, s_hscr + (tid >> 5) * (kHeavyWarpScratch + 16), tid, hcall++,
+                                    tab);
                     if (job.pending) phase_neuron_tail(U, n, cur9, s, job.mod, s_motor, tr);
                 }
                 if (n >= nn) continue;
@@ -1142,6 +1190,8 @@ public:
         d_.tr_en = p.trace_exc_ns; d_.tr_in = p.trace_inh_ns; d_.tr_pk = p.trace_peak_mv;
         d_.trace = p.trace_animal; d_.sil_senses = p.silence_senses; d_.sil_contact = p.silence_contact;
         d_.P = p.animal_capacity; d_.ncap = p.neuron_capacity; d_.ecap = p.synapse_capacity;
+        d_.warp_cells = kWorldWarpCellsMax;
+        if (const char *wc = std::getenv("NSB_WORLD_WARP_CELLS")) d_.warp_cells = std::atoi(wc);
         int dev = 0;
         NSB_CHECK(cudaGetDevice(&dev));
         NSB_CHECK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
@@ -1160,9 +1210,9 @@ public:
                                        small_smem_));
         NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, world_tick_small<false, 2>, kBlock, small_smem_));
         small2_grid_ = sms_ * std::max(occ, 1);
-        NSB_CHECK(cudaFuncSetAttribute(world_tick_small<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        NSB_CHECK(cudaFuncSetAttribute(world_tick_small<true, kHeavyMinb>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        small_smem_));
-        NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, world_tick_small<true, 2>, kBlock, small_smem_));
+        NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, world_tick_small<true, kHeavyMinb>, kBlock, small_smem_));
         heavy_grid_ = sms_ * std::max(occ, 1);
         NSB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, world_tick_big<false>, kBigBlock, 1024));
         big_grid_ = sms_ * std::max(occ, 1);
@@ -1242,7 +1292,7 @@ public:
         else
             world_tick_small<false, 3><<<small_grid_, kBlock, small_smem_, st>>>(
                 d_, c_, first_tick, alive_, ints_ + 5, ints_ + 1, big_, ints_ + 8, ints_ + 4, stats_);
-        world_tick_small<true, 2><<<heavy_grid_, kBlock, small_smem_, st>>>(d_, c_, first_tick, alive_, ints_ + 5,
+        world_tick_small<true, kHeavyMinb><<<heavy_grid_, kBlock, small_smem_, st>>>(d_, c_, first_tick, alive_, ints_ + 5,
                                                                            ints_ + 6, big_, ints_ + 8, ints_ + 4, stats_);
         world_tick_big<false><<<big_grid_, kBigBlock, 1024, st>>>(d_, c_, first_tick, big_, ints_ + 8, ints_ + 3, b_,
                                                                  stats_);

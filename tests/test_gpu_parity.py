@@ -94,6 +94,17 @@ def test_parity_mix_every_profile_and_cell_type(nsb, delivery):
     gpu.close()
 
 
+@pytest.mark.parametrize("warp_cells", ["0", "4", "32"])
+def test_lp_and_prinz_cells_in_every_form(nsb, monkeypatch, warp_cells):
+    """A heavy unit's pooled LP and Prinz cells stepped each on its own lane
+    (0), and on whole warps, a share of the pool each (4, 32): every form
+    gives the oracle's bits."""
+    monkeypatch.setenv("NSB_WARP_CELLS", warp_cells)
+    batch = nsb.workloads.parity_mix(seed=7, brains=12, heavy_types=True)
+    gpu, _ = run_parity(nsb, batch, calls=4)
+    gpu.close()
+
+
 @pytest.mark.parametrize("delivery", [False, True])
 def test_plasticity_heavy_triplet_dopamine(nsb, delivery):
     """Every synapse on profile 6 (triplet STDP into a dopamine eligibility

@@ -143,7 +143,12 @@ def _run_both(nsb, pools, first_step, steps):
     return got, ref, st
 
 
-def test_world_stage_matches_oracle(nsb, oracle_built):
+@pytest.mark.parametrize("warp_cells", [None, "0"])
+def test_world_stage_matches_oracle(nsb, oracle_built, monkeypatch, warp_cells):
+    """The world stage on a mixed population against the oracle; LP and Prinz
+    cells on the whole warp (the default) and each on its own lane (0)."""
+    if warp_cells is not None:
+        monkeypatch.setenv("NSB_WORLD_WARP_CELLS", warp_cells)
     pools, slots = _population(nsb)
     before = pools.copy()
     got, ref, st = _run_both(nsb, pools, 5, 6)
