@@ -151,6 +151,10 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# Workloads the reference's own CUDA forms are timed on as well.
+SMALL_OR_MAIN = ("batched_uneven", "plain_small", "heavy_smoke", "heavy_founders")
+
+
 def workload(nsb, seed, fraction=1, kind="batched_uneven"):
     """The full-pool workload, or with --fraction D a 1/D slice of it (brains,
     neuron and synapse pools all divided by D; same size distribution) for
@@ -177,6 +181,13 @@ def workload(nsb, seed, fraction=1, kind="batched_uneven"):
     if kind == "plain_small":
         # config 1: 64 brains x 48 neurons, 600 synapses each, 20 Hz receptor drive
         return nsb.workloads.plain_small(seed=seed)
+    if kind == "heavy_smoke":
+        # 4 brains of every cell type with 43 LP and Prinz cells among them
+        return nsb.workloads.parity_mix(seed=seed + 1, brains=4)
+    if kind == "heavy_founders":
+        # 256 world founders with LP, Prinz and LFS cells (3 % each of hidden
+        # cells), stepped as one batch
+        return nsb.workloads.world_founders(seed=seed, founders=256, heavy_types=True)
     if kind == "serving_population":
         # the serving genomes (config 5) stepped as one static batch of 5,000
         # genomes (about 4.1 M neurons, 33 M synapses), every channel at 0.5
@@ -421,7 +432,7 @@ def run_reference_cuda(args, rank, world, local_rank):
     import torch
     torch.cuda.set_device(local_rank)
     nsb = load_package()
-    batch = workload(nsb, 2, 1, args.workload if args.workload in ("batched_uneven", "plain_small") else "batched_uneven")
+    batch = workload(nsb, 2, 1, args.workload if args.workload in SMALL_OR_MAIN else "batched_uneven")
     steps = max(3, min(args.steps, 20))
     forms, notes = reference_cuda_forms(batch, steps, args.warmup, local_rank)
     N = len(batch.neuron_rows)
@@ -595,6 +606,8 @@ def run_ours(args, rank, world, local_rank):
                 "scaling": "strong" if args.strong and world > 1 else "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (Philox4x32-10, seed 2 + rank)",
                 "config": {"workload": ("plain_small_64x48" if args.workload == "plain_small" else
+                                        "lp_prinz_smoke_4_brains" if args.workload == "heavy_smoke" else
+                                        "heavy_world_founders_256" if args.workload == "heavy_founders" else
                                         f"{args.workload}_full_pools" if args.fraction == 1 else
                                         f"{args.workload}_1/{args.fraction}_pools"), "brains": batch.brains, "neurons": N,
                            "synapses": E, "ticks_per_step": 16, "delays_ms": f"1-{batch.max_delay}",
@@ -642,10 +655,11 @@ def run_ours(args, rank, world, local_rank):
         line["other_configs"] = {
             "plasticity_heavy_full_pools": device_rate(nsb, workload(nsb, 2, 1, "plasticity_heavy"), 10, 3,
                                                        local_rank),
-            "plain_small_64x48": device_rate(nsb, workload(nsb, 2, 1, "plain_small"), 50, 5, local_rank)}
+            "plain_small_64x48": device_rate(nsb, workload(nsb, 2, 1, "plain_small"), 50, 5, local_rank),
+            "lp_prinz_smoke_4_brains": device_rate(nsb, workload(nsb, 2, 1, "heavy_smoke"), 20, 3, local_rank)}
     if rank == 0:
         if (world == 1 and not args.no_reference_cuda and args.fraction == 1
-                and args.workload in ("batched_uneven", "plain_small")):
+                and args.workload in SMALL_OR_MAIN):
             # The reference's own CUDA forms on the same batch and GPU, after
             # this library's buffers are freed (none of its code runs there).
             torch.cuda.synchronize()
@@ -1114,7 +1128,8 @@ def main():
     ap.add_argument("--fraction", type=int, default=1, choices=[1, 2, 4, 8, 16],
                     help="run a 1/D slice of the full pools (profiler captures only)")
     ap.add_argument("--workload", default="batched_uneven",
-                    choices=["batched_uneven", "plasticity_heavy", "serving_population", "plain_small"],
+                    choices=["batched_uneven", "plasticity_heavy", "serving_population", "plain_small", "heavy_smoke",
+                             "heavy_founders"],
                     help="full-pool workload: batched uneven brains (default) or the plasticity-heavy variant")
     ap.add_argument("--strong", action="store_true",
                     help="N > 1: split one full-pool population across the ranks (default: one replica per rank)")

@@ -154,6 +154,23 @@ template <int N> __device__ __forceinline__ void fdiv_n(const float (&a)[N], con
     for (int i = 0; i < N; ++i) q[i] = a[i] / b[i];
 }
 
+// N independent quotients on a warp: lane i < N divides a[i] by b[i] (the
+// operands are the same in every lane) and shuffles give every lane all N,
+// so the IEEE divisions run at once instead of one after another. All 32
+// lanes call it together.
+template <int N>
+__device__ __forceinline__ void fdiv_warp(const float (&a)[N], const float (&b)[N], float (&q)[N], int lane) {
+    float n = a[0], d = b[0];
+#pragma unroll
+    for (int i = 1; i < N; ++i) {
+        n = lane == i ? a[i] : n;
+        d = lane == i ? b[i] : d;
+    }
+    const float r = n / d;
+#pragma unroll
+    for (int i = 0; i < N; ++i) q[i] = __shfl_sync(0xffffffffu, r, i);
+}
+
 // Exponentials in the LP and Prinz models. A batch whose binary64 fallback
 // (expf_cr_wide, an out-of-line call) sits inside the integration loop was
 // measured 2.7 times slower per exponential on B200 than the same binary32
@@ -626,7 +643,8 @@ __device__ __forceinline__ LaneTerm lp_term(int lane) {
 // for the gates, its sigmoid 1 / (1 + e), each exactly as lp_rates forms it;
 // shuffles give every lane all 21 values, and every lane then assembles all
 // 16 derivatives with lp_rates' operations (the same values in every lane,
-// so the assembly runs converged, with no divergence and no shared memory).
+// so the assembly runs converged, with no divergence and no shared memory),
+// its ten quotients spread over the lanes in two rounds (fdiv_warp).
 template <bool SAFE>
 __device__ __forceinline__ void lp_rates_warp(const float (&x)[16], float i_na, const float (&sc)[4], float (&d)[16],
                                               int lane, const LaneTerm &q, const float *tab, bool &ok) {
@@ -658,7 +676,7 @@ __device__ __forceinline__ void lp_rates_warp(const float (&x)[16], float i_na, 
     N2[4] = -1.6f - .032f * va;                 D2[4] = T[6] - 1.0f;
     N2[5] = .7f;                                D2[5] = .6f + cai;
     N2[6] = -na - kd - km - aleak + cpl;        D2[6] = .1148312178f;
-    fdiv_n(N2, D2, Q2);
+    fdiv_warp(N2, D2, Q2, lane);
     d[0] = Q2[6];
     const float ghk = fabsf(vs) < .001f ? 11.4866f * (x[13] - 15123.5f) : Q2[0];
     const float ca = sc[0] * (x[3] * x[4] * .1247796343f + x[5] * .07142141077f) * .00155982f * ghk * .9f;
@@ -671,7 +689,7 @@ __device__ __forceinline__ void lp_rates_warp(const float (&x)[16], float i_na, 
     N3[0] = -ca - kca - ka - ih - sleak - cpl + (i_na - 2.0f) * .01222505828f;   D3[0] = .0543909161f;
     N3[1] = T[12] * T[13] * cai;                                                  D3[1] = 2.5f + cai;
     N3[2] = (T[17] - x[12]) * .00033f;                                            D3[2] = T[18];
-    fdiv_n(N3, D3, Q3);
+    fdiv_warp(N3, D3, Q3, lane);
     d[15] = Q3[0];
     float a = fabsf(D2[1]) < 1e-5f ? 1.28f : Q2[1];
     float b = fabsf(D2[2]) < 1e-5f ? 1.4f : Q2[2];
@@ -860,7 +878,7 @@ __device__ __forceinline__ void pz_substep_warp(float (&u)[13], const float (&g)
     N1[0] = 1.0f;  D1[0] = T[18] + T[19];
     N1[1] = 2.0f;  D1[1] = T[20] + T[21];
     N1[2] = 1.0f;  D1[2] = T[24] + T[25];
-    fdiv_n(N1, D1, Q1);
+    fdiv_warp(N1, D1, Q1, lane);
     const float eca = (8.31451e3f * 283.0f / (2.0f * 96485.3415f)) * T[26];
     const float c[8] = {g[0] * m[0] * m[0] * m[0] * h[0], g[1] * m[1] * m[1] * m[1] * h[1],
                         g[2] * m[2] * m[2] * m[2] * h[2], g[3] * m[3] * m[3] * m[3] * h[3],
