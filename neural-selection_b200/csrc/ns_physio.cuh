@@ -138,10 +138,9 @@ static __device__ __noinline__ void lfs_tick(const float *g, NeuronRegs &s, floa
 }
 
 // ---- LP cell (lp_cell.cuh:28-113) --------------------------------------------------
-__device__ __forceinline__ float lp_sig(float v, float mid, float slope, const float *tab) {
-    return 1.0f / (1.0f + crexp((v - mid) / slope, tab));
-}
-__device__ __forceinline__ float lp_ratio(float num, float den, float lim) { return fabsf(den) < 1e-5f ? lim : num / den; }
+// The reference's sigmoid gates are 1 / (1 + exp((v - mid) / slope)) and its
+// rate ratios num / den, or a limit when |den| < 1e-5; lp_rates and
+// lp_rates_warp evaluate them in place, in batches.
 
 // N independent quotients a[i] / b[i] (IEEE division). The compiled division
 // was measured against straight-line alternatives on B200 (a binary64
@@ -405,12 +404,9 @@ static __device__ __noinline__ void lp_integrate(float *xs, float i_na, const fl
 }
 
 // ---- Prinz pacemaker (prinz_cell.cuh:45-121); u = {v, ca, m[7], h[4]} -------------
-__device__ __forceinline__ float pz_gate(float v, float a, float b, const float *tab) {
-    return 1.0f / (1.0f + crexp((v + a) / b, tab));
-}
-__device__ __forceinline__ float pz_gate2(float v, float a, float b, float c, float d, const float *tab) {
-    return 1.0f / (crexp((v + a) / b, tab) + crexp((v + c) / d, tab));
-}
+// The reference's gates pz_gate(v, a, b) = 1 / (1 + exp((v + a) / b)) and its
+// two-exponential time constants 1 / (exp((v + a) / b) + exp((v + c) / d))
+// are evaluated in place by pz_substep and pz_substep_warp, in batches.
 // pz_substep with its exponentials computed as two batches (crexp_n: the
 // voltage's gates and time constants, then the relaxations that use them) and
 // its quotients as three (fdiv_n: the exponents' arguments and the calcium
