@@ -640,7 +640,7 @@ __device__ __forceinline__ LaneTerm lp_term(int lane) {
 // shuffles give every lane all 21 values, and every lane then assembles all
 // 16 derivatives with lp_rates' operations (the same values in every lane,
 // so the assembly runs converged, with no divergence and no shared memory),
-// its ten quotients spread over the lanes in two rounds (fdiv_warp).
+// nine of its ten quotients spread over the lanes in one round (fdiv_warp).
 template <bool SAFE>
 __device__ __forceinline__ void lp_rates_warp(const float (&x)[16], float i_na, const float (&sc)[4], float (&d)[16],
                                               int lane, const LaneTerm &q, const float *tab, bool &ok) {
@@ -664,7 +664,8 @@ __device__ __forceinline__ void lp_rates_warp(const float (&x)[16], float i_na, 
     const float aleak = sc[3] * .001004288227f * (va + 50.0f);
     const float cpl = .004017089073f * (vs - va);
     const float ev = T[0];
-    float N2[7], D2[7], Q2[7];
+    // every quotient but d[15]'s (which needs the first) in one round
+    float N2[9], D2[9], Q2[9];
     N2[0] = vs * (x[13] * ev - 15123.5f);       D2[0] = ev - 1.0f;
     N2[1] = -16.64f - .32f * va;                D2[1] = T[2] - 1.0f;
     N2[2] = .28f * va + 7.0f;                   D2[2] = T[3] - 1.0f;
@@ -672,6 +673,8 @@ __device__ __forceinline__ void lp_rates_warp(const float (&x)[16], float i_na, 
     N2[4] = -1.6f - .032f * va;                 D2[4] = T[6] - 1.0f;
     N2[5] = .7f;                                D2[5] = .6f + cai;
     N2[6] = -na - kd - km - aleak + cpl;        D2[6] = .1148312178f;
+    N2[7] = T[12] * T[13] * cai;                D2[7] = 2.5f + cai;
+    N2[8] = (T[17] - x[12]) * .00033f;          D2[8] = T[18];
     fdiv_warp(N2, D2, Q2, lane);
     d[0] = Q2[6];
     const float ghk = fabsf(vs) < .001f ? 11.4866f * (x[13] - 15123.5f) : Q2[0];
@@ -681,12 +684,7 @@ __device__ __forceinline__ void lp_rates_warp(const float (&x)[16], float i_na, 
     const float ka = x[9] * x[9] * x[9] * .8008791415f * (vs + 72.0f) * (amix * x[10] + (1.0f - amix) * x[11]) * .9f;
     const float ih = sc[2] * x[12] * .0126874385f * (vs + 20.0f) * .9f;
     const float sleak = sc[3] * .0006901584324f * (vs + 50.0f);
-    float N3[3], D3[3], Q3[3];
-    N3[0] = -ca - kca - ka - ih - sleak - cpl + (i_na - 2.0f) * .01222505828f;   D3[0] = .0543909161f;
-    N3[1] = T[12] * T[13] * cai;                                                  D3[1] = 2.5f + cai;
-    N3[2] = (T[17] - x[12]) * .00033f;                                            D3[2] = T[18];
-    fdiv_warp(N3, D3, Q3, lane);
-    d[15] = Q3[0];
+    d[15] = (-ca - kca - ka - ih - sleak - cpl + (i_na - 2.0f) * .01222505828f) / .0543909161f;
     float a = fabsf(D2[1]) < 1e-5f ? 1.28f : Q2[1];
     float b = fabsf(D2[2]) < 1e-5f ? 1.4f : Q2[2];
     d[1] = a * (1.0f - x[1]) - b * x[1];
@@ -699,12 +697,12 @@ __device__ __forceinline__ void lp_rates_warp(const float (&x)[16], float i_na, 
     d[3] = (T[8] - x[3]) * .045f;
     d[4] = (T[9] - x[4]) * .02f * T[10];
     d[5] = (T[11] - x[5]) * .0608644f;
-    d[6] = (Q3[1] - x[6]) * .6f;
+    d[6] = (Q2[7] - x[6]) * .6f;
     d[7] = (Q2[5] - x[7]) * .035f;
     d[9] = (T[14] - x[9]) * .14f;
     d[10] = (T[15] - x[10]) * .05f;
     d[11] = (T[15] - x[11]) * .0036f * T[16];
-    d[12] = Q3[2];
+    d[12] = Q2[8];
     d[13] = -.05049639866f * ca - .01729930764f * (cai - .02f);
     d[14] = (T[19] - x[14]) * .0001386796618f * T[20];
 }
