@@ -33,3 +33,21 @@ def test_uneven_small_is_deterministic(nsb):
     b = nsb.workloads.batched_uneven(brains=64, total_neurons=8192, total_synapses=16384)
     assert np.array_equal(a.synapse_rows, b.synapse_rows)
     assert len(a.synapse_rows) == 16384 and a.synapse_rows[:, 4].max() == 16
+
+
+def test_lp_prinz_bench_batches(nsb):
+    """The LP/Prinz batches the benchmark times (bench.py --workload
+    heavy_smoke / heavy_founders): their sizes and cell counts, and, in the
+    founders, warps of list order that own several LP cells (the case the
+    heavy kernels' per-CTA pool balances)."""
+    W = nsb.workloads
+    smoke = W.parity_mix(seed=3, brains=4)
+    t = smoke.neuron_rows[:, 0].astype(int)
+    assert smoke.brains == 4 and len(t) == 182
+    assert int(((t == 2) | (t == 3)).sum()) == 43
+    founders = W.world_founders(seed=2, founders=256, heavy_types=True)
+    t = founders.neuron_rows[:, 0].astype(int)
+    assert founders.brains == 256 and len(t) == 16310
+    assert 200 < (t == 2).sum() < 330 and 200 < (t == 3).sum() < 330 and (t == 6).sum() > 150
+    lp_per_warp = [int((t[w:w + 32] == 2).sum()) for w in range(0, len(t), 32)]
+    assert max(lp_per_warp) >= 4
