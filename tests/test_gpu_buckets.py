@@ -82,6 +82,11 @@ def test_every_bucket_configuration_matches_the_oracle(nsb, monkeypatch):
             label = f"block {block} coop {coop} clustered {clustered} meta {cap} list {lst}"
             assert all(g["block"] == block for g in got[:4]), label
             _check(gpu, batch, seeds, want, label)
+        # heavy units on 128-thread CTAs: four warps share the LP/Prinz pool
+        gpu.set_bucket(4, 128, 0, 1, 6144, 1)
+        assert gpu.buckets()[4]["block"] == 128
+        _check(gpu, batch, seeds, want, "heavy block 128")
+        gpu.set_bucket(4, 256, 0, 1, 6144, 1)
         with pytest.raises(RuntimeError):
             gpu.set_bucket(3, 256, 0, 2, 6144)          # packed units have no cluster form
         with pytest.raises(RuntimeError):
