@@ -162,6 +162,27 @@ def test_world_stage_matches_oracle(nsb, oracle_built, monkeypatch, warp_cells):
     assert got.motors.sum() > 0 and got.trace_exc_arrivals.sum() > 0
 
 
+@pytest.mark.parametrize("warp_cells", [None, "0"])
+def test_world_stage_big_animals_with_lp_and_prinz_cells(nsb, oracle_built, monkeypatch, warp_cells):
+    """Animals above the small units' 256 neurons with LP, Prinz and LFS cells
+    (the big-animal kernel's heavy build, whose CTA pools the cells of each
+    256-neuron slot) beside small heavy founders, against the oracle: whole
+    warps (the default) and each cell on its own lane (0)."""
+    if warp_cells is not None:
+        monkeypatch.setenv("NSB_WORLD_WARP_CELLS", warp_cells)
+    W, wl = nsb.world, nsb.workloads
+    batch = wl.concat([wl.world_founders(seed=21, founders=3, lo=300, hi=700, heavy_types=True),
+                       wl.world_founders(seed=22, founders=5, heavy_types=True)], "world_big_heavy")
+    t = batch.neuron_rows[:, 0].astype(int)
+    assert ((t == 2) | (t == 3)).sum() > 20 and np.diff(batch.neuron_offsets).max() > 256
+    seeds = np.arange(batch.brains, dtype=np.uint32) * 5 + 1
+    pools = W.place_population(batch, *W.records_from_gpu(batch, seeds), scatter_seed=7)
+    got, ref, st = _run_both(nsb, pools, 3, 4)
+    _compare(got, ref)
+    assert st["animals"] == batch.brains
+    assert got.motors.sum() > 0 or got.neuron_state["total"].sum() > 0
+
+
 def test_world_stage_steady_population(nsb, oracle_built):
     """Config-2 founders (32-96 neurons, 4-12 synapses per neuron), packed
     slots: the compiled brains are reused across steps."""
